@@ -1,0 +1,128 @@
+"""Writes seeded synthetic systems in the formats the reference oracle reads,
+and runs the compiled reference driver (oracle/_ref/ref_driver).
+
+Test infrastructure, not product: only tests/, ``__graft_entry__.smoke()`` and
+the ``cpu_baseline`` / ``--impl reference`` legs of bench.py use this module.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+from typing import Dict, Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DRIVER = os.path.join(HERE, "_ref", "ref_driver")
+
+
+def write_species(sp, path: str) -> None:
+    """Plain-text species read by oracle/shim/SpeciesReader.cpp."""
+    with open(path, "w") as f:
+        f.write(f"symbol {sp.name}\natomic_number {sp.atomic_number}\n")
+        f.write(f"mass {sp.mass}\nvalence_charge {sp.zval}\n")
+        projs = sp.projectors()
+        f.write(f"lmax {max([l for l, _ in projs], default=0)}\n")
+        f.write(f"mesh_spacing {sp.mesh_spacing}\n")
+        v = sp.local_potential()
+        f.write(f"local_potential {v.size}\n")
+        f.write("\n".join(f"{x:.17e}" for x in v) + "\n")
+        for l, p in projs:
+            f.write(f"projector {l} 0 {p.size}\n")
+            f.write("\n".join(f"{x:.17e}" for x in p) + "\n")
+        for l, d in sp.dmatrix():
+            f.write(f"d_ij {l} 0 0 {d:.17e}\n")
+        f.write("end\n")
+
+
+def write_coeffs(path: str, hkl: np.ndarray, c: np.ndarray) -> None:
+    nb, ngw = c.shape
+    with open(path, "wb") as f:
+        np.array([ngw, nb], dtype=np.int32).tofile(f)
+        np.ascontiguousarray(hkl, dtype=np.int32).tofile(f)
+        out = np.empty((nb, ngw, 2))
+        out[..., 0] = c.real
+        out[..., 1] = c.imag
+        out.tofile(f)
+
+
+def write_system(sysdef, workdir: str, c: Optional[np.ndarray] = None) -> str:
+    """Write system.txt (+ species + coefficients) into workdir."""
+    os.makedirs(workdir, exist_ok=True)
+    hkl = sysdef.miller()
+    if c is None:
+        c = sysdef.coefficients(hkl)
+    write_coeffs(os.path.join(workdir, "coeffs.bin"), hkl, c)
+    lines = ["cell " + " ".join(f"{x:.17e}" for x in sysdef.cell.ravel()),
+             f"ecut_ry {sysdef.ecut_ry:.17e}", f"nel {sysdef.nel}",
+             f"xc {sysdef.xc}"]
+    for sp in sysdef.species:
+        p = os.path.join(workdir, f"{sp.name}.sp")
+        write_species(sp, p)
+        lines.append(f"species {sp.name} {p}")
+    count = {}
+    for isp, pos in sysdef.atoms:
+        name = sysdef.species[isp].name
+        count[name] = count.get(name, 0) + 1
+        lines.append(f"atom {name}{count[name]} {name} "
+                     + " ".join(f"{x:.17e}" for x in pos))
+    lines.append(f"coeffs {os.path.join(workdir, 'coeffs.bin')}")
+    path = os.path.join(workdir, "system.txt")
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+    return path
+
+
+def run_reference(sysdef, workdir: str, nsteps: int, dump_steps: int = 0,
+                  forces: bool = False, wf_dyn: str = "PSDA",
+                  threads: Optional[int] = None, c=None) -> Dict:
+    """Run the compiled reference on sysdef; returns parsed outputs."""
+    if not os.path.exists(REF_DRIVER):
+        raise FileNotFoundError("oracle/_ref/ref_driver not built "
+                                "(make -C oracle)")
+    path = write_system(sysdef, workdir, c)
+    env = dict(os.environ)
+    if threads:
+        env["OMP_NUM_THREADS"] = str(threads)
+        env["OPENBLAS_NUM_THREADS"] = str(threads)
+    subprocess.run([REF_DRIVER, path, str(nsteps), workdir, str(dump_steps),
+                    "1" if forces else "0", wf_dyn], check=True, env=env,
+                   stdout=subprocess.DEVNULL)
+    return load_outputs(workdir)
+
+
+def load_outputs(workdir: str) -> Dict:
+    out: Dict = {}
+    meta = {}
+    with open(os.path.join(workdir, "meta.txt")) as f:
+        for line in f:
+            k, v = line.split()
+            meta[k] = float(v) if "." in v else int(v)
+    out["meta"] = meta
+    e = np.loadtxt(os.path.join(workdir, "energies.txt"), ndmin=2)
+    names = ["step", "ekin", "econf", "eps", "enl", "ecoul", "exc", "esr",
+             "eself", "ehart", "etotal", "eigenvalue_sum", "t_charge",
+             "t_vhxc", "t_energy", "t_wf_update"]
+    out["energies"] = {n: e[:, i] for i, n in enumerate(names)}
+    nst, ngw = meta["nst"], meta["ngw"]
+    grid = (meta["np2v"], meta["np1v"], meta["np0v"])
+    s = 0
+    while os.path.exists(os.path.join(workdir, f"step{s}_rhor.bin")):
+        pre = os.path.join(workdir, f"step{s}_")
+        d = {}
+        d["rhor"] = np.fromfile(pre + "rhor.bin").reshape(grid)
+        d["vr"] = np.fromfile(pre + "vr.bin").reshape(grid)
+        for k in ("hc", "c"):
+            a = np.fromfile(pre + f"{k}.bin").reshape(nst, ngw, 2)
+            d[k] = a[..., 0] + 1j * a[..., 1]
+        out[f"step{s}"] = d
+        s += 1
+    for s in range(int(e[-1, 0]) + 1):
+        fp = os.path.join(workdir, f"step{s}_fion.txt")
+        if os.path.exists(fp):
+            out[f"fion{s}"] = np.loadtxt(fp).reshape(-1, 3)
+    fc = os.path.join(workdir, "final_c.bin")
+    if os.path.exists(fc):
+        a = np.fromfile(fc).reshape(nst, ngw, 2)
+        out["final_c"] = a[..., 0] + 1j * a[..., 1]
+    return out

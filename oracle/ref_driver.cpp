@@ -1,0 +1,273 @@
+// Oracle driver: runs the reference Qbox electronic step, single task, on the
+// seeded synthetic inputs written by oracle/inputs.py, and dumps energies and
+// arrays for the parity tests.  Test infrastructure, not product: it links the
+// reference sources compiled by oracle/Makefile into oracle/_ref/.
+//
+// The loop is the SCF loop of src/BOSampleStepper.cpp:795-977 with nite=0 and
+// wf_dyn=PSDA:  ChargeDensity::update_density (:805) -> update_vhxc(false)
+// (:891) -> EnergyFunctional::energy(true,...) (:941) -> eigenvalue_sum =
+// Wavefunction::dot (:954) -> PSDAWavefunctionStepper::update (:960).
+// Input coefficients are keyed by Miller index so the reference's rod order
+// (src/Basis.cpp:544-597) never leaks into the inputs.
+//
+// usage: ref_driver <system.txt> <nsteps> <outdir> [dump_steps=0]
+//                   [forces=0] [threads-note]
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <iomanip>
+#include <map>
+#include <sstream>
+#include <string>
+#include <vector>
+#include <sys/time.h>
+
+#include "MPIdata.h"
+#include "Sample.h"
+#include "Species.h"
+#include "SpeciesReader.h"
+#include "Atom.h"
+#include "Wavefunction.h"
+#include "SlaterDet.h"
+#include "ChargeDensity.h"
+#include "EnergyFunctional.h"
+#include "Preconditioner.h"
+#include "PSDAWavefunctionStepper.h"
+#include "JDWavefunctionStepper.h"
+#include "FourierTransform.h"
+#include "Basis.h"
+#include "Timer.h"
+
+using namespace std;
+
+static double wall(void)
+{ struct timeval tv; gettimeofday(&tv, 0); return tv.tv_sec + 1e-6 * tv.tv_usec; }
+
+struct Key { int h, k, l; bool operator<(const Key& o) const
+  { return h != o.h ? h < o.h : ( k != o.k ? k < o.k : l < o.l ); } };
+
+static void write_bin(const string& path, const void* p, size_t bytes)
+{
+  FILE* f = fopen(path.c_str(), "wb");
+  if ( !f ) { cerr << "cannot write " << path << endl; exit(1); }
+  fwrite(p, 1, bytes, f);
+  fclose(f);
+}
+
+int main(int argc, char** argv)
+{
+  if ( argc < 4 )
+  {
+    cerr << "usage: ref_driver system.txt nsteps outdir [dump_steps] [forces]"
+         << endl;
+    return 2;
+  }
+  const string sysfile = argv[1];
+  const int nsteps = atoi(argv[2]);
+  const string outdir = argv[3];
+  const int dump_steps = argc > 4 ? atoi(argv[4]) : 0;
+  const int want_forces = argc > 5 ? atoi(argv[5]) : 0;
+  const string wf_dyn = argc > 6 ? argv[6] : "PSDA";
+
+  MPIdata::set(1,1,1,1);
+  Sample s;
+  s.ctrl.xc = "LDA";
+  s.ctrl.ecuts = 0.0;
+  s.ctrl.ecutprec = 0.0;
+  s.ctrl.polarization = "OFF";
+  s.ctrl.fermi_temp = 0.0;
+  for ( int i = 0; i < 6; i++ ) s.ctrl.ext_stress[i] = 0.0;
+  s.ctrl.e_field = D3vector(0,0,0);
+  s.ctrl.alpha_PBE0 = 0.25;
+  s.ctrl.alpha_RSH = 0.0; s.ctrl.beta_RSH = 0.0; s.ctrl.mu_RSH = 0.0;
+  s.ctrl.stress = "OFF";
+  s.ctrl.wf_diag = "F";
+
+  // ---- system file ----
+  ifstream in(sysfile.c_str());
+  if ( !in ) { cerr << "cannot open " << sysfile << endl; return 1; }
+  string key, coeff_file;
+  double a[9] = {0};
+  double ecut_ry = 0.0;
+  int nel = 0;
+  int atom_count = 0;
+  while ( in >> key )
+  {
+    if ( key == "cell" ) for ( int i = 0; i < 9; i++ ) in >> a[i];
+    else if ( key == "ecut_ry" ) in >> ecut_ry;
+    else if ( key == "nel" ) in >> nel;
+    else if ( key == "xc" ) in >> s.ctrl.xc;
+    else if ( key == "species" )
+    {
+      string name, path; in >> name >> path;
+      Species* sp = new Species(name);
+      SpeciesReader rdr;
+      rdr.uri_to_species(path, *sp);
+      s.atoms.addSpecies(sp, name);
+    }
+    else if ( key == "atom" )
+    {
+      string name, spname; double x, y, z;
+      in >> name >> spname >> x >> y >> z;
+      s.atoms.addAtom(new Atom(name, spname, D3vector(x,y,z), D3vector(0,0,0)));
+      atom_count++;
+    }
+    else if ( key == "coeffs" ) in >> coeff_file;
+    else { cerr << "unknown key " << key << endl; return 1; }
+  }
+  UnitCell cell(D3vector(a[0],a[1],a[2]), D3vector(a[3],a[4],a[5]),
+                D3vector(a[6],a[7],a[8]));
+  s.atoms.set_cell(cell);
+  s.wf.resize(cell, cell, 0.5 * ecut_ry);
+  s.wf.set_nel(nel);
+  s.wf.update_occ(0.0);
+
+  SlaterDet& sd = *s.wf.sd(0,0);
+  const Basis& basis = sd.basis();
+  const int ngw = basis.localsize();
+  const int nst = sd.nst();
+  ComplexMatrix& c = sd.c();
+  const int mloc = c.mloc();
+
+  // ---- coefficients, keyed by Miller index ----
+  FILE* fc = fopen(coeff_file.c_str(), "rb");
+  if ( !fc ) { cerr << "cannot open " << coeff_file << endl; return 1; }
+  int hdr[2];
+  if ( fread(hdr, sizeof(int), 2, fc) != 2 ) return 1;
+  const int ngw_in = hdr[0], nb_in = hdr[1];
+  if ( ngw_in != ngw || nb_in != nst )
+  {
+    cerr << "basis mismatch: file ngw=" << ngw_in << " nb=" << nb_in
+         << " reference ngw=" << ngw << " nst=" << nst << endl;
+    return 1;
+  }
+  vector<int> hkl(3*ngw);
+  if ( fread(&hkl[0], sizeof(int), 3*ngw, fc) != (size_t)(3*ngw) ) return 1;
+  vector<double> cin(2*(size_t)ngw*nst);
+  if ( fread(&cin[0], sizeof(double), cin.size(), fc) != cin.size() ) return 1;
+  fclose(fc);
+  map<Key,int> row_of;
+  for ( int i = 0; i < ngw; i++ )
+    row_of[Key{hkl[3*i],hkl[3*i+1],hkl[3*i+2]}] = i;
+  vector<int> perm(ngw);  // perm[ig] = input row of reference coefficient ig
+  for ( int ig = 0; ig < ngw; ig++ )
+  {
+    Key k{basis.idx(3*ig), basis.idx(3*ig+1), basis.idx(3*ig+2)};
+    map<Key,int>::iterator it = row_of.find(k);
+    if ( it == row_of.end() ) { cerr << "Miller index missing" << endl; return 1; }
+    perm[ig] = it->second;
+  }
+  for ( int n = 0; n < nst; n++ )
+    for ( int ig = 0; ig < ngw; ig++ )
+    {
+      const size_t src = 2*((size_t)n*ngw + perm[ig]);
+      c[ig + (size_t)n*mloc] = complex<double>(cin[src], cin[src+1]);
+    }
+  s.wf.gram();
+
+  // ---- set up the energy functional and the stepper ----
+  ChargeDensity cd(s.wf);
+  EnergyFunctional ef(s, cd);
+  Preconditioner prec(s.wf, ef, s.ctrl.ecutprec);
+  TimerMap tmap;
+  WavefunctionStepper* stepper = 0;
+  if ( wf_dyn == "JD" )
+    stepper = new JDWavefunctionStepper(s.wf, prec, ef, tmap);
+  else
+    stepper = new PSDAWavefunctionStepper(s.wf, prec, tmap);
+  Wavefunction dwf(s.wf);
+  vector<vector<double> > fion;
+  valarray<double> sigma(6);
+  fion.resize(s.atoms.nsp());
+  for ( int is = 0; is < s.atoms.nsp(); is++ )
+    fion[is].resize(3*s.atoms.na(is));
+
+  const FourierTransform& vft = *cd.vft();
+  const int np012 = vft.np012();
+
+  ofstream eo((outdir + "/energies.txt").c_str());
+  eo << setprecision(17);
+  eo << "# step ekin econf eps enl ecoul exc esr eself ehart etotal "
+        "eigenvalue_sum t_charge t_vhxc t_energy t_wf_update\n";
+  {
+    ofstream meta((outdir + "/meta.txt").c_str());
+    meta << "ngw " << ngw << "\nnst " << nst << "\nnp0v " << vft.np0()
+         << "\nnp1v " << vft.np1() << "\nnp2v " << vft.np2()
+         << "\nng_v " << cd.vbasis()->localsize()
+         << "\nnrods " << basis.nrods() << "\nomega " << cell.volume()
+         << "\nnatoms " << atom_count << "\n";
+  }
+
+  stepper->preprocess();
+  for ( int itscf = 0; itscf < nsteps; itscf++ )
+  {
+    const double t0 = wall();
+    cd.update_density();
+    const double t1 = wall();
+    ef.update_vhxc(false);
+    const double t2 = wall();
+    const bool last = ( itscf == nsteps - 1 );
+    const bool fstep = want_forces && ( last || itscf < dump_steps );
+    ef.energy(true, dwf, fstep, fion, false, sigma);
+    const double t3 = wall();
+    const double eigsum = real(s.wf.dot(dwf));
+    if ( itscf < dump_steps )
+    {
+      ostringstream pre; pre << outdir << "/step" << itscf << "_";
+      write_bin(pre.str() + "rhor.bin", &cd.rhor[0][0], np012 * sizeof(double));
+      write_bin(pre.str() + "vr.bin", &ef.v_r[0][0], np012 * sizeof(double));
+      // C and H*C in the input (sorted Miller) order
+      vector<double> out(2*(size_t)ngw*nst);
+      const ComplexMatrix& hc = dwf.sd(0,0)->c();
+      for ( int n = 0; n < nst; n++ )
+        for ( int ig = 0; ig < ngw; ig++ )
+        {
+          const complex<double> v = hc[ig + (size_t)n*mloc];
+          const size_t dst = 2*((size_t)n*ngw + perm[ig]);
+          out[dst] = v.real(); out[dst+1] = v.imag();
+        }
+      write_bin(pre.str() + "hc.bin", &out[0], out.size()*sizeof(double));
+      for ( int n = 0; n < nst; n++ )
+        for ( int ig = 0; ig < ngw; ig++ )
+        {
+          const complex<double> v = c[ig + (size_t)n*mloc];
+          const size_t dst = 2*((size_t)n*ngw + perm[ig]);
+          out[dst] = v.real(); out[dst+1] = v.imag();
+        }
+      write_bin(pre.str() + "c.bin", &out[0], out.size()*sizeof(double));
+    }
+    if ( fstep )
+    {
+      ostringstream fn; fn << outdir << "/step" << itscf << "_fion.txt";
+      ofstream fo(fn.str().c_str());
+      fo << setprecision(17);
+      for ( int is = 0; is < s.atoms.nsp(); is++ )
+        for ( int i = 0; i < 3*s.atoms.na(is); i++ )
+          fo << fion[is][i] << "\n";
+    }
+    stepper->update(dwf);
+    const double t4 = wall();
+    eo << itscf << " " << ef.ekin() << " " << ef.econf() << " " << ef.eps()
+       << " " << ef.enl() << " " << ef.ecoul() << " " << ef.exc() << " "
+       << ef.esr() << " " << ef.eself() << " " << ef.ehart() << " "
+       << ef.etotal() << " " << eigsum << " " << (t1-t0) << " " << (t2-t1)
+       << " " << (t3-t2) << " " << (t4-t3) << "\n";
+    eo.flush();
+  }
+  // final wavefunctions
+  {
+    vector<double> out(2*(size_t)ngw*nst);
+    for ( int n = 0; n < nst; n++ )
+      for ( int ig = 0; ig < ngw; ig++ )
+      {
+        const complex<double> v = c[ig + (size_t)n*mloc];
+        const size_t dst = 2*((size_t)n*ngw + perm[ig]);
+        out[dst] = v.real(); out[dst+1] = v.imag();
+      }
+    write_bin(outdir + "/final_c.bin", &out[0], out.size()*sizeof(double));
+  }
+  delete stepper;
+  return 0;
+}
