@@ -1,0 +1,783 @@
+"""CPU restatement (numpy, FP64) of the reference's Kohn-Sham electronic step.
+
+TEST INFRASTRUCTURE - this is the oracle, not the product.  Only tests/,
+``__graft_entry__.smoke()`` and bench.py's ``cpu_baseline`` leg may use it,
+and only as the checker.  Its results are pinned against the reference itself
+built single-task (oracle/_ref, see oracle/Makefile) by tests/test_oracle.py
+and the committed fixtures in tests/golden/.
+
+Each function cites the reference file:line it restates.  The reference keeps
+Gamma-point wavefunctions on the half sphere of G vectors and represents them
+as real matrices of twice the number of rows ("DoubleMatrix proxy"); every
+inner product therefore carries the factor 2 for +G/-G and a correction that
+removes the double-counted G=0 row.  Here coefficients are kept as complex
+arrays c[n, ig] in sorted Miller order, and the same conventions are written
+out explicitly.
+
+Grids are numpy arrays of shape (np2, np1, np0) indexed [z, y, x], which is
+the reference's memory order x + np0*(y + np1*z) (src/BasisMapping.cpp:206-216).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional
+
+import numpy as np
+
+FPI = 4.0 * math.pi
+RCPS = 1.5           # Gaussian pseudocharge radius, src/AtomSet.cpp:43-44
+
+
+# --------------------------------------------------------------------------
+# basis and FFT sizes
+# --------------------------------------------------------------------------
+def factorizable(n: int) -> bool:
+    """src/Basis.cpp:105-133: n = 2^a 3^{0,1,2} 5^{0,1} 7^{0,1} 11^{0,1}."""
+    for p in (11, 7, 5, 3, 3):
+        if n % p == 0:
+            n //= p
+    while n % 2 == 0:
+        n //= 2
+    return n == 1
+
+
+def reciprocal(cell: np.ndarray) -> np.ndarray:
+    return 2.0 * math.pi * np.linalg.inv(cell).T
+
+
+def fft_size_for(cell: np.ndarray, ecut: float) -> List[int]:
+    """src/Basis.cpp:332-341,513-521: np_i = smallest factorizable even
+    number >= 2*hmax_i with hmax_i = int(1.5 + sqrt(2 ecut)/(2 pi) |a_i|)."""
+    fac = math.sqrt(2.0 * ecut) / (2.0 * math.pi)
+    out = []
+    for i in range(3):
+        hmax = int(1.5 + fac * np.linalg.norm(cell[i]))
+        n = 2 * hmax
+        while not factorizable(n):
+            n += 2
+        out.append(n)
+    return out
+
+
+def dense_grid(cell: np.ndarray, ecut: float) -> List[int]:
+    """src/ChargeDensity.cpp:36-49: vbasis at 4*ecut, grid np+2 rounded up to
+    a factorizable size; the wavefunction FFTs use the same grid (:98)."""
+    out = []
+    for n in fft_size_for(cell, 4.0 * ecut):
+        n += 2
+        while not factorizable(n):
+            n += 2
+        out.append(n)
+    return out
+
+
+def half_sphere(cell: np.ndarray, ecut: float) -> np.ndarray:
+    """Sorted (h,k,l) of {G: |G|^2 < 2 ecut} on the Gamma half sphere
+    (rods of src/Basis.cpp:357-447)."""
+    b = reciprocal(cell)
+    fac = math.sqrt(2.0 * ecut) / (2.0 * math.pi)
+    m = [int(1.5 + fac * np.linalg.norm(cell[i])) for i in range(3)]
+    h, k, l = np.meshgrid(np.arange(0, m[0] + 1), np.arange(-m[1], m[1] + 1),
+                          np.arange(-m[2], m[2] + 1), indexing="ij")
+    h, k, l = h.ravel(), k.ravel(), l.ravel()
+    keep = (h > 0) | ((h == 0) & (k > 0)) | ((h == 0) & (k == 0) & (l >= 0))
+    h, k, l = h[keep], k[keep], l[keep]
+    gx = h * b[0, 0] + k * b[1, 0] + l * b[2, 0]
+    gy = h * b[0, 1] + k * b[1, 1] + l * b[2, 1]
+    gz = h * b[0, 2] + k * b[1, 2] + l * b[2, 2]
+    inside = gx * gx + gy * gy + gz * gz < 2.0 * ecut
+    hkl = np.stack([h[inside], k[inside], l[inside]], 1).astype(np.int64)
+    order = np.lexsort((hkl[:, 2], hkl[:, 1], hkl[:, 0]))
+    return hkl[order]
+
+
+@dataclass
+class Basis:
+    """G vectors of a Gamma half-sphere basis (src/Basis.cpp:646-690)."""
+    cell: np.ndarray
+    ecut: float
+    hkl: np.ndarray = field(init=False)
+    gx: np.ndarray = field(init=False)   # (ng, 3)
+    g2: np.ndarray = field(init=False)
+    g: np.ndarray = field(init=False)
+    g2i: np.ndarray = field(init=False)
+    gi: np.ndarray = field(init=False)
+
+    def __post_init__(self):
+        self.hkl = half_sphere(self.cell, self.ecut)
+        b = reciprocal(self.cell)
+        self.gx = self.hkl @ b
+        self.g2 = (self.gx ** 2).sum(1)
+        self.g = np.sqrt(self.g2)
+        with np.errstate(divide="ignore"):
+            self.gi = np.where(self.g > 0, 1.0 / np.where(self.g > 0, self.g, 1), 0.0)
+        self.g2i = self.gi * self.gi
+
+    @property
+    def size(self) -> int:
+        return self.hkl.shape[0]
+
+    def g0(self) -> int:
+        return int(np.flatnonzero((self.hkl == 0).all(1))[0])
+
+
+class Grid:
+    """Complex 3-D FFT on the dense grid for a half-sphere basis
+    (src/FourierTransform.cpp:147-239; forward scales by 1/N, src:733-744)."""
+
+    def __init__(self, basis: Basis, shape: List[int]):
+        self.n0, self.n1, self.n2 = shape
+        self.N = self.n0 * self.n1 * self.n2
+        h, k, l = basis.hkl[:, 0], basis.hkl[:, 1], basis.hkl[:, 2]
+        self.ip = ((l % self.n2) * self.n1 + (k % self.n1)) * self.n0 + (h % self.n0)
+        self.im = (((-l) % self.n2) * self.n1 + ((-k) % self.n1)) * self.n0 + ((-h) % self.n0)
+        self.shape = (self.n2, self.n1, self.n0)
+
+    def backward(self, c: np.ndarray, c2: Optional[np.ndarray] = None) -> np.ndarray:
+        """src/BasisMapping.cpp:628-700 + fz_inv/fxy_inv: one or two real
+        functions packed as c1 + i c2; returns the complex grid."""
+        z = np.zeros(self.N, complex)
+        if c2 is None:
+            z[self.ip] = c
+            z[self.im] = np.conj(c)
+        else:
+            z[self.ip] = c + 1j * c2
+            z[self.im] = np.conj(c) + 1j * np.conj(c2)
+        return np.fft.ifftn(z.reshape(self.shape)) * self.N
+
+    def forward(self, f: np.ndarray, two: bool = False):
+        """src/BasisMapping.cpp:703-750 + fxy/fz: grid -> coefficients."""
+        z = (np.fft.fftn(f.reshape(self.shape)) / self.N).ravel()
+        if not two:
+            return z[self.ip]
+        zp, zm = z[self.ip], np.conj(z[self.im])
+        return 0.5 * (zp + zm), -0.5j * (zp - zm)
+
+
+# --------------------------------------------------------------------------
+# species: radial tables -> G-space splines (src/Species.cpp:510-1055)
+# --------------------------------------------------------------------------
+def simpsn(t: np.ndarray) -> float:
+    """src/Species.cpp:34-48 (end-corrected trapezoid weights)."""
+    n = t.size
+    c = (17.0 / 48.0, 59.0 / 48.0, 43.0 / 48.0, 49.0 / 48.0)
+    s = sum(c[i] * (t[i] + t[n - 1 - i]) for i in range(4))
+    return s + t[4:n - 4].sum()
+
+
+def sinft(y: np.ndarray) -> np.ndarray:
+    """src/sinft.cpp: y_k = sum_{j=1}^{n-1} y_j sin(pi j k / n), computed as
+    the reference does through a length-2n complex FFT of the odd extension."""
+    n = y.size
+    z = np.zeros(2 * n, complex)
+    z[1:n] = y[1:]
+    z[2 * n - np.arange(1, n)] = -y[1:]
+    return -0.5 * np.fft.fft(z)[:n].imag
+
+
+def cosft1(y: np.ndarray) -> np.ndarray:
+    """src/sinft.cpp cosft1: y has n+1 entries; returns n values
+    0.5*Re(FFT of the even extension)."""
+    n = y.size - 1
+    z = np.zeros(2 * n, complex)
+    z[0] = y[0]
+    z[1:n + 1] = y[1:n + 1]
+    z[2 * n - np.arange(1, n + 1)] = y[1:n + 1]
+    return 0.5 * np.fft.fft(z)[:n].real
+
+
+def spline(x, y, yp_left, yp_right, nat_left, nat_right):
+    """src/spline.cpp spline(): second derivatives of a cubic spline."""
+    n = x.size
+    d = np.empty(n); e = np.empty(n); f = np.empty(n); y2 = np.empty(n)
+    third, sixth = 1.0 / 3.0, 1.0 / 6.0
+    if nat_left == 0:
+        h = x[1] - x[0]
+        d[0], e[0], f[0] = third * h, sixth * h, 0.0
+        y2[0] = (y[1] - y[0]) / h - yp_left
+    else:
+        d[0], e[0], f[0], y2[0] = 1.0, 0.0, 0.0, 0.0
+    if nat_right == 0:
+        h = x[n - 1] - x[n - 2]
+        d[n - 1], e[n - 1], f[n - 1] = third * h, 0.0, sixth * h
+        y2[n - 1] = yp_right - (y[n - 1] - y[n - 2]) / h
+    else:
+        d[n - 1], e[n - 1], f[n - 1], y2[n - 1] = 1.0, 0.0, 0.0, 0.0
+    hp = x[2:] - x[1:-1]
+    hm = x[1:-1] - x[:-2]
+    d[1:-1] = third * (hp + hm)
+    e[1:-1] = sixth * hp
+    f[1:-1] = sixth * hm
+    y2[1:-1] = (y[2:] - y[1:-1]) / hp - (y[1:-1] - y[:-2]) / hm
+    # tridiagonal solve, src/spline.cpp tridsolve()
+    for i in range(1, n):
+        f[i] /= d[i - 1]
+        d[i] -= f[i] * e[i - 1]
+    for i in range(1, n):
+        y2[i] -= f[i] * y2[i - 1]
+    y2[n - 1] /= d[n - 1]
+    for i in range(n - 2, -1, -1):
+        y2[i] = (y2[i] - e[i] * y2[i + 1]) / d[i]
+    return y2
+
+
+def splintd(xa, ya, y2a, x):
+    """src/spline.cpp splint/splintd, vectorised: value and derivative."""
+    n = xa.size
+    kl = np.clip(np.searchsorted(xa, x, side="right") - 1, 0, n - 2)
+    kh = kl + 1
+    h = xa[kh] - xa[kl]
+    a = (xa[kh] - x) / h
+    b = (x - xa[kl]) / h
+    y = a * ya[kl] + b * ya[kh] + h * h * (1.0 / 6.0) * (
+        (a ** 3 - a) * y2a[kl] + (b ** 3 - b) * y2a[kh])
+    dy = (ya[kh] - ya[kl]) / h + h * (((1.0 / 6.0) - 0.5 * a * a) * y2a[kl]
+                                      + (0.5 * b * b - (1.0 / 6.0)) * y2a[kh])
+    return y, dy
+
+
+class Species:
+    """G-space tables of one SLPP species (src/Species.cpp:510-1055,
+    evaluation :1133-1192)."""
+
+    def __init__(self, sp):
+        self.zval = float(sp.zval)
+        dr = sp.mesh_spacing
+        ndft = 1
+        while ndft * dr < 40.0:
+            ndft *= 2
+        self.ndft = ndft
+        r = np.arange(ndft) * dr
+        vloc_in = sp.local_potential()
+        npts = vloc_in.size
+        vlocr = np.empty(ndft)
+        vlocr[:npts] = vloc_in
+        vlocr[npts:] = -self.zval / r[npts:]
+        z = self.zval
+        vlocr[0] += (z / RCPS) * (2.0 / math.sqrt(math.pi))
+        from math import erf
+        vlocr[1:] += (z / r[1:]) * np.array([erf(x / RCPS) for x in r[1:]])
+        vlocr *= FPI * r * dr
+        v0 = simpsn(vlocr * r)
+        vg = sinft(vlocr)
+        fac = math.pi / (ndft * dr)
+        self.gspl = np.arange(ndft) * fac
+        vg[0] = v0
+        vg[1:] /= self.gspl[1:]
+        self.vlocg = vg
+        self.vlocg2 = spline(self.gspl, vg, 0.0, 0.0, 0, 1)
+        self.proj = []     # (l, table, second derivatives)
+        self.dmat = dict(sp.dmatrix())
+        for l, phi_in in sp.projectors():
+            phi = np.zeros(ndft)
+            phi[:npts] = phi_in
+            vnlr = FPI * dr * phi
+            if l == 0:
+                v0 = simpsn(vnlr * r * r)
+                t = sinft(vnlr * r)
+                t[0] = v0
+                t[1:] /= self.gspl[1:]
+                t2 = spline(self.gspl, t, 0.0, 0.0, 0, 1)
+            elif l == 1:
+                s = sinft(vnlr)
+                fint = np.zeros(ndft)
+                fint[1:] = s[1:] / self.gspl[1:] ** 2
+                yy = np.zeros(ndft + 1)
+                yy[:ndft] = vnlr * r
+                c = cosft1(yy)
+                t = np.zeros(ndft)
+                t[1:] = fint[1:] - c[1:] / self.gspl[1:]
+                t2 = spline(self.gspl, t, 0.0, 0.0, 1, 1)
+            else:
+                raise NotImplementedError("l > 1 projectors")
+            self.proj.append((l, t, t2))
+        self.nlm = sum(2 * l + 1 for l, _, _ in self.proj)
+        self.eself = z * z / (math.sqrt(2.0 * math.pi) * RCPS)
+
+    def dvlocg(self, g):
+        v, dv = splintd(self.gspl, self.vlocg, self.vlocg2, g)
+        out = g > self.gspl[-1]
+        return np.where(out, 0.0, v), np.where(out, 0.0, dv)
+
+    def vnlg(self, iop, g):
+        l, t, t2 = self.proj[iop]
+        v, dv = splintd(self.gspl, t, t2, g)
+        out = g > self.gspl[-1]
+        return np.where(out, 0.0, v), np.where(out, 0.0, dv)
+
+    def rhopsg(self, g):
+        return -self.zval * np.exp(-0.25 * RCPS * RCPS * g * g)
+
+
+# --------------------------------------------------------------------------
+# XC functionals (src/LDAFunctional.cpp:92-160, src/PBEFunctional.cpp:168-280)
+# --------------------------------------------------------------------------
+def lda_pz(rho):
+    """Perdew-Zunger LDA, unpolarized (src/LDAFunctional.cpp:92-150)."""
+    c1 = 0.6203504908994001
+    c3 = -0.610887057711
+    A, B, b1, b2, G = 0.0311, -0.048, 1.0529, 0.3334, -0.1423
+    D = G / (1.0 + b1 + b2) - B
+    C = -A - D - G * ((b1 / 2.0 + b2) / ((1.0 + b1 + b2) * (1.0 + b1 + b2)))
+    ee = np.zeros_like(rho)
+    vv = np.zeros_like(rho)
+    pos = rho > 0.0
+    r = rho[pos]
+    rs = c1 / np.cbrt(r)
+    vx = c3 / rs
+    ex = 0.75 * vx
+    lo = rs < 1.0
+    ec = np.empty_like(rs); vc = np.empty_like(rs)
+    lr = np.log(rs[lo]); rl = rs[lo]
+    ec[lo] = A * lr + B + C * rl * lr + D * rl
+    vc[lo] = A * lr + (B - A / 3.0) + (2.0 / 3.0) * C * rl * lr + ((2.0 * D - C) / 3.0) * rl
+    rh = rs[~lo]
+    sq = np.sqrt(rh)
+    den = 1.0 + b1 * sq + b2 * rh
+    ec[~lo] = G / den
+    vc[~lo] = ec[~lo] * (1.0 + (7.0 / 6.0) * b1 * sq + (4.0 / 3.0) * b2 * rh) / den
+    ee[pos] = ex + ec
+    vv[pos] = vx + vc
+    return ee, vv
+
+
+def pbe(rho, grad):
+    """PBE exchange-correlation (src/PBEFunctional.cpp:168-280, gcor2 :488)."""
+    third, third4 = 1.0 / 3.0, 4.0 / 3.0
+    ax = -0.7385587663820224058
+    um, uk = 0.2195149727645171, 0.804
+    ul = um / uk
+    pi32third = 3.09366772628014
+    alpha = 1.91915829267751
+    seven_sixth = 7.0 / 6.0
+    four_over_pi = 1.27323954473516
+    gamma = 0.03109069086965489
+    bet = 0.06672455060314922
+    delt = bet / gamma
+    exc = np.zeros_like(rho); v1 = np.zeros_like(rho); v2 = np.zeros_like(rho)
+    m = rho >= 1.e-18
+    r = rho[m]; gr = grad[m]
+    rh13 = r ** third
+    exunif = ax * rh13
+    fk = pi32third * rh13
+    s = gr / (2.0 * fk * r)
+    s2 = s * s
+    p0 = 1.0 + ul * s2
+    fxpbe = 1.0 + uk - uk / p0
+    ex = exunif * fxpbe
+    fs = 2.0 * uk * ul / (p0 * p0)
+    vx1 = third4 * exunif * (fxpbe - s2 * fs)
+    vx2 = -exunif * fs / (r * 4.0 * fk * fk)
+    rs = alpha / fk
+    twoks = 2.0 * np.sqrt(four_over_pi * fk)
+    t = gr / (twoks * r)
+    rtrs = np.sqrt(rs)
+    a_, a1, b1, b2, b3, b4 = 0.0310907, 0.2137, 7.5957, 3.5876, 1.6382, 0.49294
+    q0 = -2.0 * a_ * (1.0 + a1 * rtrs * rtrs)
+    q1 = 2.0 * a_ * rtrs * (b1 + rtrs * (b2 + rtrs * (b3 + rtrs * b4)))
+    q2 = np.log(1.0 + 1.0 / q1)
+    ec = q0 * q2
+    q3 = a_ * (b1 / rtrs + 2.0 * b2 + rtrs * (3.0 * b3 + 4.0 * b4 * rtrs))
+    ecrs = -2.0 * a_ * a1 * q2 - q0 * q3 / (q1 * (1.0 + q1))
+    vc = ec - rs * ecrs * third
+    pon = -ec / gamma
+    b = delt / (np.exp(pon) - 1.0)
+    b2_ = b * b
+    t2 = t * t
+    t4 = t2 * t2
+    q4 = 1.0 + b * t2
+    q5 = q4 + b2_ * t4
+    h = gamma * np.log(1.0 + delt * q4 * t2 / q5)
+    t6 = t4 * t2
+    rsthrd = rs * third
+    fac = delt / b + 1.0
+    bec = b2_ * fac / bet
+    q8 = q5 * q5 + delt * q4 * q5 * t2
+    q9 = 1.0 + 2.0 * b * t2
+    hb = -bet * b * t6 * (2.0 + b * t2) / q8
+    hrs = -rsthrd * hb * bec * ecrs
+    ht = 2.0 * bet * q9 / q8
+    vc1 = vc + h + hrs - t2 * ht * seven_sixth
+    vc2 = -ht / (r * twoks * twoks)
+    exc[m] = ex + ec + h
+    v1[m] = vx1 + vc1
+    v2[m] = vx2 + vc2
+    return exc, v1, v2
+
+
+# --------------------------------------------------------------------------
+# the electronic step
+# --------------------------------------------------------------------------
+def fold_in_ws(v: np.ndarray, cell: np.ndarray) -> np.ndarray:
+    """src/UnitCell.cpp:157-187 (13 neighbour vectors, 1e-10 tolerance)."""
+    a = cell
+    an = [a[0], a[1], a[2], a[0] + a[1], a[0] - a[1], a[1] + a[2], a[1] - a[2],
+          a[2] + a[0], a[2] - a[0], a[0] + a[1] + a[2], a[0] - a[1] - a[2],
+          a[0] + a[1] - a[2], a[0] - a[1] + a[2]]
+    v = v.copy()
+    eps = 1.e-10
+    for _ in range(10):
+        done = True
+        for ai in an:
+            h = 0.5 * ai @ ai
+            sp = v @ ai
+            if sp > h + eps:
+                done = False
+                while v @ ai > h + eps:
+                    v -= ai
+            elif sp < -h - eps:
+                done = False
+                while v @ ai < -h - eps:
+                    v += ai
+        if done:
+            break
+    return v
+
+
+def esr_forces(system, zv, positions):
+    """Pseudocharge repulsion E_sr and its forces
+    (src/EnergyFunctional.cpp:1112-1192)."""
+    cell = system.cell
+    b = reciprocal(cell)
+    d = [2.0 * math.pi / np.linalg.norm(b[i]) for i in range(3)]
+    nsp = len(positions)
+    esr = 0.0
+    f = [np.zeros_like(p) for p in positions]
+    from math import erfc
+    for is1 in range(nsp):
+        for is2 in range(is1, nsp):
+            rc12 = math.sqrt(2.0 * RCPS * RCPS)
+            nc = [int(8.0 * rc12 / d[i]) for i in range(3)]
+            for ia1 in range(len(positions[is1])):
+                ia2min = ia1 if is1 == is2 else 0
+                for ia2 in range(ia2min, len(positions[is2])):
+                    same = is1 == is2 and ia1 == ia2
+                    v12 = fold_in_ws(positions[is1][ia1] - positions[is2][ia2], cell)
+                    for i0 in range(-nc[0], nc[0] + 1):
+                        for i1 in range(-nc[1], nc[1] + 1):
+                            for i2 in range(-nc[2], nc[2] + 1):
+                                if same and i0 == 0 and i1 == 0 and i2 == 0:
+                                    continue
+                                fac = 0.5 if same else 1.0
+                                x = v12 + i0 * cell[0] + i1 * cell[1] + i2 * cell[2]
+                                r12 = math.sqrt(x @ x)
+                                arg = r12 / rc12
+                                term = zv[is1] * zv[is2] * erfc(arg) / r12
+                                esr += fac * term
+                                de = 2.0 * zv[is1] * zv[is2] * math.exp(-arg * arg) / (
+                                    rc12 * math.sqrt(math.pi))
+                                dedr = -fac * (term + de) / (r12 * r12)
+                                f[is1][ia1] -= dedr * x
+                                f[is2][ia2] += dedr * x
+    return esr, f
+
+
+class ElectronicStep:
+    """State and operators of the reference's SCF iteration with nite=0
+    (src/BOSampleStepper.cpp:795-977) on one Gamma-point SlaterDet."""
+
+    def __init__(self, system, c: Optional[np.ndarray] = None):
+        self.system = system
+        cell = np.array(system.cell, float)
+        self.cell = cell
+        self.omega = abs(np.linalg.det(cell))
+        self.wb = Basis(cell, system.ecut)
+        self.vb = Basis(cell, 4.0 * system.ecut)
+        shape = dense_grid(cell, system.ecut)
+        self.grid_shape = shape
+        self.wgrid = Grid(self.wb, shape)
+        self.vgrid = Grid(self.vb, shape)
+        self.N = self.wgrid.N
+        self.nst = system.nbands
+        self.occ = np.full(self.nst, 2.0)
+        self.xc = system.xc
+        self.species = [Species(sp) for sp in system.species]
+        self.positions = [system.positions(i) for i in range(len(system.species))]
+        if c is None:
+            c = system.coefficients(self.wb.hkl)
+        self.c = np.array(c, complex)
+        self.g0 = self.wb.g0()
+        self._setup_tables()
+        self.gram()
+        self.c_last = None
+        self.dc_last = None
+        self.extrapolate = False
+
+    # ---- setup (src/EnergyFunctional.cpp:1047-1245, NonLocal update_twnl)
+    def _setup_tables(self):
+        vb, wb = self.vb, self.wb
+        om = self.omega
+        self.vion_g = np.zeros(vb.size, complex)
+        self.rhops_t = np.zeros(vb.size, complex)
+        self.sfac = []
+        self.vps = []
+        self.rhops = []
+        for isp, sp in enumerate(self.species):
+            tau = self.positions[isp]
+            phase = -(vb.gx @ tau.T)             # (ng, na)
+            s = np.exp(1j * phase).sum(1)        # S(G) = sum_a exp(-i G.tau)
+            self.sfac.append(s)
+            v, dv = sp.dvlocg(vb.g)
+            vps = v / om
+            rhops = sp.rhopsg(vb.g) / om
+            self.vps.append(vps); self.rhops.append(rhops)
+            self.vion_g += s * vps
+            self.rhops_t += s * rhops
+        zv = [sp.zval for sp in self.species]
+        self.esr, self.fion_esr = esr_forces(self.system, zv, self.positions)
+        self.eself = sum(sp.eself * len(self.positions[i])
+                         for i, sp in enumerate(self.species))
+        # nonlocal projectors twnl (src/NonLocalPotential.cpp:235-560)
+        s14pi = math.sqrt(1.0 / FPI)
+        s34pi = math.sqrt(3.0 / FPI)
+        self.nl = []
+        for isp, sp in enumerate(self.species):
+            if not sp.proj:
+                continue
+            tw = []
+            lp = []
+            dfac = []
+            for iop, (l, _, _) in enumerate(sp.proj):
+                v, dv = sp.vnlg(iop, wb.g)
+                if l == 0:
+                    tw.append(s14pi * v); lp.append(0); dfac.append(sp.dmat[0])
+                else:
+                    for j in range(3):
+                        tw.append(s34pi * wb.gx[:, j] * wb.gi * v)
+                        lp.append(1); dfac.append(sp.dmat[1])
+            self.nl.append((isp, np.array(tw), np.array(lp), np.array(dfac)))
+
+    def anl(self, isp, tw, lp):
+        """Projector x phase, A[ipr, ia, G] (src/NonLocalPotential.cpp:1316-1394)."""
+        tau = self.positions[isp]
+        e = np.exp(-1j * (self.wb.gx @ tau.T)).T    # (na, ng) exp(-i G.tau)
+        a = tw[:, None, :] * e[None, :, :]
+        a[lp == 1] *= -1j
+        return a
+
+    # ---- SlaterDet operations
+    def real_dot(self, x, y):
+        """2 Re sum_G conj(x) y - Re x(0) Re y(0): the DoubleMatrix proxy
+        gemm('t','n',2.0) + ger(-1.0) pattern (src/SlaterDet.cpp:809-813)."""
+        m = 2.0 * (x.conj() @ y.T).real
+        m -= np.outer(x[:, self.g0].real, y[:, self.g0].real)
+        return m
+
+    def cleanup(self):
+        """src/SlaterDet.cpp:1341-1356: Im c(G=0) = 0."""
+        self.c[:, self.g0] = self.c[:, self.g0].real
+
+    def gram(self):
+        """src/SlaterDet.cpp:480-534: S = 2C^T C - c0 c0^T, S = L L^T,
+        C <- C L^-T."""
+        self.cleanup()
+        s = self.real_dot(self.c, self.c)
+        L = np.linalg.cholesky(s)
+        self.c = np.linalg.solve(L, self.c)
+
+    def ortho_align(self, c_last):
+        """src/SlaterDet.cpp:768-876."""
+        self.cleanup()
+        ctmp = self.c.copy()
+        L = np.linalg.cholesky(self.real_dot(self.c, self.c))
+        x = self.real_dot(self.c, c_last)           # B = C^T C_last (x2, fix)
+        x = np.linalg.solve(L, x)                   # L^-1 B
+        x = polar(x, 1.e-6, 20)
+        x = np.linalg.solve(L.T, x)                 # L^-T Q
+        self.c = x.T @ ctmp                         # C <- C_tmp X
+
+    # ---- density (src/SlaterDet.cpp:225-298, src/ChargeDensity.cpp:136-198)
+    def update_density(self):
+        rho = np.zeros(self.N)
+        om_inv = 1.0 / self.omega
+        n = 0
+        while n + 1 < self.nst:
+            f = self.wgrid.backward(self.c[n], self.c[n + 1]).ravel()
+            rho += om_inv * self.occ[n] * f.real ** 2 + om_inv * self.occ[n + 1] * f.imag ** 2
+            n += 2
+        if self.nst % 2:
+            f = self.wgrid.backward(self.c[-1]).ravel()
+            rho += om_inv * self.occ[-1] * f.real ** 2
+        self.rhor = rho
+        self.total_charge = rho.sum() * self.omega / self.N
+        self.rhog = self.vgrid.forward(self.omega * rho)
+
+    # ---- potentials (src/EnergyFunctional.cpp:231-394, XCPotential:124-465)
+    def update_vhxc(self):
+        vb, om = self.vb, self.omega
+        rhoelg = self.rhog / om
+        self.rhoelg = rhoelg
+        rho = self.rhor
+        if self.xc == "LDA":
+            e, v = lda_pz(rho)
+            vxc = v
+            self.exc = (rho * e).sum() * om / self.N
+        else:
+            grads = []
+            for j in range(3):
+                t = 1j * vb.gx[:, j] / om * self.rhog
+                grads.append(self.vgrid.backward(t).real.ravel())
+            grad = np.sqrt(grads[0] ** 2 + grads[1] ** 2 + grads[2] ** 2)
+            e, v1, v2 = pbe(rho, grad)
+            vxt = np.zeros(self.N)
+            for j in range(3):
+                t = self.vgrid.forward(grads[j] * v2)
+                t = t * (1j * vb.gx[:, j])
+                vxt += self.vgrid.backward(t).real.ravel()
+            vxc = v1 + vxt
+            self.exc = (rho * e).sum() * om / self.N
+        g0 = vb.g0()
+        eps = 2.0 * (np.conj(rhoelg) * self.vion_g).real.sum()
+        eps -= (np.conj(rhoelg[g0]) * self.vion_g[g0]).real
+        self.eps = eps * om
+        rt = rhoelg + self.rhops_t
+        self.rhogt = rt
+        self.ehart = om * FPI * (np.abs(rt) ** 2 * vb.g2i).sum()
+        vloc_g = self.vion_g + FPI * rt * vb.g2i
+        self.v_r = vxc + self.vgrid.backward(vloc_g).real.ravel()
+
+    # ---- nonlocal (src/NonLocalPotential.cpp:1258-1640)
+    def nonlocal_energy(self, hc: Optional[np.ndarray], forces=False):
+        enl = 0.0
+        om_inv = 1.0 / self.omega
+        fion = [np.zeros_like(p) for p in self.positions]
+        for isp, tw, lp, dfac in self.nl:
+            a = self.anl(isp, tw, lp)                   # (npr, na, ng)
+            npr, na, ng = a.shape
+            af = a.reshape(npr * na, ng)
+            F = self.real_dot(af, self.c)               # (npr*na, nst)
+            DF = F * np.repeat(dfac, na)[:, None]
+            enl += om_inv * (F * DF * self.occ[None, :]).sum()
+            if hc is not None:
+                hc += (om_inv * DF).T @ af
+            if forces:
+                for j in range(3):
+                    daf = af * (-1j * self.wb.gx[:, j])[None, :]
+                    dF = self.real_dot(daf, self.c)
+                    t = (self.occ[None, :] * DF * dF).sum(1).reshape(npr, na)
+                    fion[isp][:, j] -= 2.0 * om_inv * t.sum(0)
+        return enl, fion
+
+    # ---- energy and H*psi (src/EnergyFunctional.cpp:397-1044)
+    def energy(self, compute_hpsi=True, forces=False):
+        wb = self.wb
+        psi2 = (self.occ[:, None] * np.abs(self.c) ** 2).sum(0)
+        self.ekin = (psi2 * wb.g2).sum()
+        hc = np.zeros_like(self.c) if compute_hpsi else None
+        self.enl, fnl = self.nonlocal_energy(hc, forces)
+        self.ecoul = self.ehart + self.esr - self.eself
+        self.etotal = self.ekin + self.eps + self.enl + self.ecoul + self.exc
+        if compute_hpsi:
+            hc += 0.5 * wb.g2[None, :] * self.c
+            self.rs_mul_add(self.v_r, hc)
+            self.hc = hc
+        if forces:
+            self.fion = self._local_forces(fnl)
+        return self.etotal
+
+    def rs_mul_add(self, v, hc):
+        """src/SlaterDet.cpp:410-477: hc += FFT_fwd(v FFT_bwd(c))."""
+        n = 0
+        while n + 1 < self.nst:
+            f = self.wgrid.backward(self.c[n], self.c[n + 1]).ravel() * v
+            c1, c2 = self.wgrid.forward(f, two=True)
+            hc[n] += c1
+            hc[n + 1] += c2
+            n += 2
+        if self.nst % 2:
+            f = self.wgrid.backward(self.c[-1]).ravel() * v
+            hc[-1] += self.wgrid.forward(f)
+
+    def _local_forces(self, fnl):
+        """src/EnergyFunctional.cpp:841-930."""
+        vb = self.vb
+        out = []
+        for isp, sp in enumerate(self.species):
+            vtemp = FPI * self.rhops[isp] * vb.g2i * np.conj(self.rhogt) \
+                + self.vps[isp] * np.conj(self.rhoelg)
+            tau = self.positions[isp]
+            e = np.exp(-1j * (vb.gx @ tau.T))        # (ng, na)
+            tmp = e.real * vtemp.imag[:, None] + e.imag * vtemp.real[:, None]
+            f_loc = -2.0 * self.omega * (tmp.T @ vb.gx)
+            out.append(fnl[isp] + self.fion_esr[isp] + f_loc)
+        return out
+
+    def eigenvalue_sum(self):
+        """Wavefunction::dot (src/SlaterDet.cpp:1122-1153)."""
+        d = 2.0 * (np.conj(self.c) * self.hc).real.sum()
+        d -= (self.c[:, self.g0].real * self.hc[:, self.g0].real).sum()
+        return d
+
+    # ---- PSDA (src/PSDAWavefunctionStepper.cpp:46-249, Preconditioner)
+    def psda_update(self):
+        hc = self.hc
+        a = self.real_dot(self.c, hc)              # A = C^T HC (x2, fix)
+        hc = hc - a.T @ self.c                     # HC - C A
+        # preconditioner (src/Preconditioner.cpp:88-143, diag :49-85)
+        p2 = np.abs(self.c) ** 2
+        snorm = p2.sum(1) - 0.5 * p2[:, self.g0]
+        sek = (p2 * self.wb.g2[None, :]).sum(1)
+        bn, be = 2.0 * snorm, 2.0 * sek
+        ekin = np.where(0.5 * bn > 0.0, 0.5 * be / np.where(bn != 0, bn, 1), 0.0)
+        ekin = np.where(ekin == 0.0, 1.0, ekin)
+        e = 0.5 * self.wb.g2[None, :]
+        with np.errstate(divide="ignore"):
+            kdiag = np.where(e < ekin[:, None], 0.5 / ekin[:, None], 0.5 / e)
+        dc = -kdiag * hc
+        x = self.c
+        if self.extrapolate:
+            df = dc - self.dc_last
+            av = 2.0 * (dc.real * df.real + dc.imag * df.imag).sum()
+            bv = 2.0 * (df.real ** 2 + df.imag ** 2).sum()
+            f0, d0 = dc[:, self.g0], df[:, self.g0]
+            av -= (f0.real * d0.real + f0.imag * d0.imag).sum()
+            bv -= (d0.real ** 2 + d0.imag ** 2).sum()
+            theta = -av / bv if bv != 0.0 else 0.0
+            if theta < -1.0:
+                theta = 0.0
+            theta = min(2.0, theta)
+            self.theta = theta
+            xbar = x + theta * (x - self.c_last)
+            fbar = dc + theta * (dc - self.dc_last)
+            newc = xbar + fbar
+        else:
+            self.theta = 0.0
+            newc = x + dc
+        self.c_last = x.copy()
+        self.dc_last = dc
+        self.c = newc
+        self.ortho_align(self.c_last)
+        self.extrapolate = True
+
+    def step(self, forces=False) -> Dict[str, float]:
+        self.update_density()
+        self.update_vhxc()
+        self.energy(True, forces)
+        eig = self.eigenvalue_sum()
+        out = dict(ekin=self.ekin, eps=self.eps, enl=self.enl,
+                   ehart=self.ehart, ecoul=self.ecoul, exc=self.exc,
+                   esr=self.esr, eself=self.eself, etotal=self.etotal,
+                   eigenvalue_sum=eig)
+        self.psda_update()
+        return out
+
+
+def polar(x, tol, maxiter):
+    """src/Matrix.cpp:2446-2540: Bjorck-Bowie iteration while
+    ||I - X^T X||_F < 1, else the Higham step X <- (X + X^-T)/2."""
+    n = x.shape[0]
+    eye = np.eye(n)
+    for _ in range(maxiter):
+        q = eye - x.T @ x
+        qn = math.sqrt((q * q).sum())
+        if qn < 1.0:
+            t = eye + 0.75 * q
+            qt = q @ t
+            t = eye + 0.5 * qt
+            x = x @ t
+        else:
+            x = 0.5 * (x + np.linalg.inv(x.T))
+        if qn <= tol:      # the update above still runs on the last pass
+            break
+    return x

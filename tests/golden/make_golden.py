@@ -1,0 +1,74 @@
+"""Generates the golden fixtures in tests/golden/ by running the reference Qbox
+electronic step, compiled single-task by oracle/Makefile (oracle/_ref).
+
+    make -C oracle && python tests/golden/make_golden.py
+
+Each fixture holds, for a seeded synthetic system: every energy term of each
+SCF step, the ionic forces at the first and last step, the grid sizes and
+basis size, a fixed sample of the density and local potential on the grid,
+H*psi and wavefunction coefficients of a few bands (all G for small bases,
+a fixed sample of G otherwise), and per-band norms.
+The fixtures pin the numpy oracle (oracle/qbox_np.py) in tests/test_oracle.py.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, os.path.join(ROOT, "qbox-public_b200"))
+sys.path.insert(0, ROOT)
+
+from qbx import systems            # noqa: E402
+from oracle import inputs          # noqa: E402
+
+CASES = {"si8": 20, "si64": 3, "h2o32": 2}
+NSAMPLE = 2048
+NBANDS_FULL = 4
+
+
+def make(name: str, nsteps: int, workdir: str) -> str:
+    s = systems.get(name)
+    out = inputs.run_reference(s, workdir, nsteps, dump_steps=1, forces=True,
+                               threads=os.cpu_count())
+    meta = out["meta"]
+    e = out["energies"]
+    rng = np.random.default_rng(12345)
+    N = meta["np0v"] * meta["np1v"] * meta["np2v"]
+    idx = np.sort(rng.choice(N, NSAMPLE, replace=False))
+    st = out["step0"]
+    ngw = meta["ngw"]
+    gidx = np.arange(ngw) if ngw <= 2000 else np.sort(
+        rng.choice(ngw, 512, replace=False))
+    fx = dict(
+        grid=np.array([meta["np0v"], meta["np1v"], meta["np2v"]]),
+        ngw=meta["ngw"], nst=meta["nst"], ng_v=meta["ng_v"],
+        omega=meta["omega"], nsteps=nsteps,
+        sample_idx=idx,
+        rhor_sample=st["rhor"].ravel()[idx],
+        vr_sample=st["vr"].ravel()[idx],
+        rhor_sum=st["rhor"].sum(), vr_sum=st["vr"].sum(),
+        g_idx=gidx,
+        hc_bands=st["hc"][:NBANDS_FULL, gidx],
+        hc_norm2=(np.abs(st["hc"]) ** 2).sum(1),
+        final_c_bands=out["final_c"][:NBANDS_FULL, gidx],
+        final_c_norm2=(np.abs(out["final_c"]) ** 2).sum(1),
+        fion_first=out["fion0"], fion_last=out[f"fion{nsteps - 1}"],
+    )
+    for k in ("ekin", "eps", "enl", "ehart", "ecoul", "exc", "esr", "eself",
+              "etotal", "eigenvalue_sum"):
+        fx["e_" + k] = e[k]
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)),
+                        f"ref_{name}.npz")
+    np.savez_compressed(path, **fx)
+    return path
+
+
+if __name__ == "__main__":
+    import tempfile
+    names = sys.argv[1:] or list(CASES)
+    for n in names:
+        with tempfile.TemporaryDirectory() as td:
+            print(make(n, CASES[n], td))

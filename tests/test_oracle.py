@@ -1,0 +1,88 @@
+"""The numpy oracle (oracle/qbox_np.py) against the reference's own outputs.
+
+The fixtures in tests/golden/ were produced by the reference Qbox sources
+compiled single-task (tests/golden/make_golden.py).  These tests pin the
+oracle that the GPU parity tests compare against.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden
+from qbx import systems
+from oracle import qbox_np
+
+TERMS = ("ekin", "eps", "enl", "ehart", "exc", "esr", "eself", "etotal",
+         "eigenvalue_sum")
+
+
+def _check_step0(es, g):
+    n = np.prod(g["grid"])
+    assert es.N == n
+    assert tuple(es.grid_shape) == tuple(g["grid"])
+    assert es.wb.size == g["ngw"] and es.vb.size == g["ng_v"]
+    np.testing.assert_allclose(es.rhor[g["sample_idx"]], g["rhor_sample"],
+                               rtol=0, atol=1e-13)
+    np.testing.assert_allclose(es.v_r[g["sample_idx"]], g["vr_sample"],
+                               rtol=0, atol=1e-11)
+    np.testing.assert_allclose(es.hc[:4, g["g_idx"]], g["hc_bands"], atol=1e-13)
+    np.testing.assert_allclose((np.abs(es.hc) ** 2).sum(1), g["hc_norm2"],
+                               rtol=1e-11)
+
+
+@pytest.mark.parametrize("name,nsteps", [("si8", 20), ("si64", 3),
+                                         ("h2o32", 1)])
+def test_oracle_matches_reference(name, nsteps):
+    g = golden(name)
+    es = qbox_np.ElectronicStep(systems.get(name))
+    for it in range(nsteps):
+        last = it == nsteps - 1
+        r = es.step(forces=(it == 0 or last))
+        if it == 0:
+            _check_step0(es, g)
+            np.testing.assert_allclose(np.concatenate(es.fion), g["fion_first"],
+                                       atol=1e-12)
+        for k in TERMS:
+            ref = g["e_" + k][it]
+            assert abs(r[k] - ref) < 1e-9 * max(1.0, abs(ref)), (it, k, r[k], ref)
+    if nsteps == int(g["nsteps"]):
+        np.testing.assert_allclose(np.concatenate(es.fion), g["fion_last"],
+                                   atol=1e-12)
+        np.testing.assert_allclose(es.c[:4, g["g_idx"]], g["final_c_bands"],
+                                   atol=1e-12)
+
+
+def test_invariants_si8():
+    """Known-answer invariants of the reference (src/SlaterDet.cpp:1272-1314
+    orthonormality; src/ChargeDensity.cpp:173-191 total charge)."""
+    s = systems.si8()
+    es = qbox_np.ElectronicStep(s)
+    for _ in range(3):
+        es.step()
+        ov = es.real_dot(es.c, es.c)
+        assert np.abs(ov - np.eye(s.nbands)).max() < 1e-12
+        assert abs(es.total_charge - s.nel) < 1e-10
+
+
+def test_fft_roundtrip_and_gaussian():
+    """forward(backward(c)) = c on the sphere, and the analytic transform of
+    a Gaussian (src/testFourierTransform.cpp:157-162)."""
+    s = systems.si8()
+    es = qbox_np.ElectronicStep(s)
+    c = es.c[0]
+    f = es.wgrid.backward(c)
+    assert np.abs(f.imag).max() < 1e-12
+    np.testing.assert_allclose(es.wgrid.forward(f.ravel()), c, atol=1e-14)
+    # Gaussian exp(-a r^2) at the origin of the 20.52-bohr cell: periodic
+    # images and the truncation at |G|^2 < 8 ecut are both below 1e-12
+    s = systems.si64()
+    es = qbox_np.ElectronicStep(s)
+    a = 1.0
+    vb = es.vb
+    ghat = (np.pi / a) ** 1.5 * np.exp(-vb.g2 / (4 * a)) / es.omega
+    f = es.vgrid.backward(ghat).real
+    n0, n1, n2 = es.grid_shape
+    x = np.arange(n0) / n0
+    L = s.cell[0, 0]
+    d = np.minimum(x, 1 - x) * L
+    r2 = d[None, None, :] ** 2 + d[None, :, None] ** 2 + d[:, None, None] ** 2
+    np.testing.assert_allclose(f, np.exp(-a * r2), atol=1e-11)
