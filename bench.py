@@ -1,0 +1,345 @@
+"""Benchmark: ms per electronic step of the 512-atom Si-like cell on one B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (si512): 512-atom diamond-lattice cell a=41.04 bohr of the synthetic
+Si-like species, atoms displaced by U(-0.05,0.05) bohr (seed 5), Gamma point,
+25 Ry, 1024 bands, PBE; coefficients complex N(0,1) from seed 5, then
+orthonormalised.  A step is one SCF iteration with nite=0: update_density,
+update_vhxc, energy(true) (H*psi), eigenvalue_sum and one PSDA update with
+ortho_align.  The wavefunctions (1.2 GB) are larger than L2, so no flush is
+needed between steps.
+
+The headline `value` is the mixed-precision path (FP32 staged FFTs); the FP64
+path is timed in the same run (`fp64_ms_per_step`), and `dE_per_atom` is the
+total-energy difference between the two after the same steps.  `e2e` runs
+the same step through the C ABI with the wavefunctions in pinned host memory:
+each step uploads C, runs the step and downloads C and the energies.
+
+Under torchrun each rank runs an independent replica on its own GPU (the
+electronic step of one cell does not shard in this build).  `--impl
+reference` times the reference's own CPU build (oracle/_ref) on a band sample
+of the same cell and scales it to 1024 bands (see `cpu_baseline.sample`).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "qbox-public_b200")
+for p in (PKG, ROOT):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+METRIC = ("ms per electronic step, mixed vs FP64 on GPU, 512-atom Si-like, "
+          "ΔE≤1e-6 Ha/atom")
+WORKLOAD = ("si512: 512-atom Si-like diamond cell a=41.04 bohr, Gamma, 25 Ry, "
+            "1024 bands, PBE, 140^3 grid, 72919 PW/band")
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.out, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.out.flush()
+        self.out.seek(0)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out.read().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.out.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------- reference arm
+def reference_step_ms(nsteps: int, nbands_sample: int, threads: int):
+    """Time the reference (oracle/_ref) on a band sample of si512 and scale
+    each phase to 1024 bands: density and H*psi linearly in the bands (FFTs
+    and nonlocal projections), the PSDA update quadratically (band-band
+    GEMMs), update_vhxc not at all."""
+    from qbx import systems
+    from oracle import inputs
+    full = systems.si512()
+    s = full.band_sample(nbands_sample)
+    with tempfile.TemporaryDirectory() as td:
+        out = inputs.run_reference(s, td, nsteps, threads=threads)
+    e = out["energies"]
+    k = max(1, nsteps - 1)              # the first step carries warm-up costs
+    tc = statistics.median(e["t_charge"][-k:])
+    tv = statistics.median(e["t_vhxc"][-k:])
+    te = statistics.median(e["t_energy"][-k:])
+    tw = statistics.median(e["t_wf_update"][-k:])
+    f = full.nbands / nbands_sample
+    ms = 1e3 * (tc * f + tv + te * f + tw * f * f)
+    sample = (f"{nbands_sample} of {full.nbands} bands of si512 for {nsteps} steps, "
+              f"median of the last {k}; per-phase scaling to 1024 bands "
+              f"(density {tc:.2f}s, vhxc {tv:.2f}s, energy {te:.2f}s, "
+              f"wf_update {tw:.2f}s per sample step)")
+    return ms, sample
+
+
+def run_reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    ref = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+    if not os.path.exists(ref):
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/ref_driver not built (make -C oracle)"}))
+        return
+    nsteps = max(2, min(args.warmup + args.steps, 4))
+    ms, sample = reference_step_ms(nsteps, 32, threads)
+    line = {
+        "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": WORKLOAD, "precision": "FP64 (reference CPU build)"},
+        "cpu_baseline": {"value": ms, "unit": "ms", "cores": threads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ------------------------------------------------------------ our arm
+def algorithmic_bytes_xy_vpsi(ctx, npairs: int, cbytes: int) -> float:
+    """Per H*psi: for every band pair the plane pass reads and writes every
+    stick value once (2 S c) and reads the potential once (N x 8 bytes)."""
+    n0, n1, n2 = ctx.grid
+    nvec = 2 * nrods(ctx) - 1
+    S = nvec * n2
+    return npairs * (2.0 * S * cbytes + 8.0 * n0 * n1 * n2)
+
+
+def nrods(ctx) -> int:
+    hkl = ctx.miller()
+    return len({(int(h), int(k)) for h, k, _ in hkl})
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    from qbx import capi, systems
+
+    rank, world, local = dist_env()
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = local
+
+    s = systems.si512()
+    hkl = s.miller()
+    c0 = s.coefficients(hkl)
+    natoms = len(s.atoms)
+
+    def timed(ctx, nsteps, profile=False, e2e_bufs=None):
+        stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        if profile:
+            ctx.profile(True)
+        n0 = ctx.launch_count()
+        start.record(stream)
+        r = None
+        for _ in range(nsteps):
+            if e2e_bufs is not None:
+                ctx.set_coeffs_async(e2e_bufs[0])
+            r = ctx.scf_step()
+            if e2e_bufs is not None:
+                ctx.get_coeffs_async(e2e_bufs[1])
+        end.record(stream)
+        end.synchronize()
+        torch.cuda.synchronize()
+        ms = start.elapsed_time(end) / nsteps
+        launches = ctx.launch_count() - n0
+        return ms, r, launches
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], device=f"cuda:{dev}", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- mixed precision (headline)
+    mix = capi.from_system(s, device=dev, precision=capi.MIXED, coeffs=c0)
+    for _ in range(args.warmup):
+        mix.scf_step()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    ms_mix, r_mix, launches = timed(mix, args.steps, profile=True)
+    clk = clocks.stop()
+    prof = {}
+    for name in ("update_density", "update_vhxc", "energy", "vpsi", "psda_update",
+                 "xy_vpsi", "xy_density", "zfft_bwd", "zfft_fwd", "grid_fft",
+                 "gemm_nl_project", "gemm_nl_apply", "gemm_residual", "overlap_cholesky",
+                 "gemm_overlap_last", "gemm_rotate", "polar"):
+        t, n = mix.profile_get(name)
+        prof[name] = {"ms_per_step": t / args.steps, "launches_per_step": n / args.steps}
+    mix.profile(False)
+    npairs = (s.nbands + 1) // 2
+    # one xy_vpsi launch per batch of band pairs
+    t_xy, n_xy = prof["xy_vpsi"]["ms_per_step"], prof["xy_vpsi"]["launches_per_step"]
+    bytes_hpsi = algorithmic_bytes_xy_vpsi(mix, npairs, 8)
+    per_launch_bytes = bytes_hpsi / max(1e-9, n_xy)
+    per_launch_ms = t_xy / max(1e-9, n_xy)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9
+    roofline = {"kernel": "k_xy<float, OP_VPSI> (plane pass of H*psi)", "bound": "hbm",
+                "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved / hbm_peak,
+                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                "traffic": None,
+                "algorithmic_bytes_per_launch": per_launch_bytes,
+                "launch_ms": per_launch_ms}
+    # GEMM share (FP64 cuBLAS in this build) against the dense FP64 rate
+    gemm_ms = sum(prof[k]["ms_per_step"] for k in
+                  ("gemm_nl_project", "gemm_nl_apply", "gemm_residual", "overlap_cholesky",
+                   "gemm_overlap_last", "gemm_rotate"))
+    K = 2 * mix.ngw
+    n = s.nbands
+    npj = 4 * natoms
+    gemm_flop = 2 * (2.0 * K * npj * n) + 2 * (2.0 * K * n * n) + K * n * n + 2 * (2.0 * K * n * n)
+
+    # ---- FP64 path on the same start
+    f64 = capi.from_system(s, device=dev, precision=capi.FP64, coeffs=c0)
+    for _ in range(args.warmup):
+        f64.scf_step()
+    ms_f64, r_f64, _ = timed(f64, args.steps)
+    de_atom = abs(r_mix["etotal"] - r_f64["etotal"]) / natoms
+    f64.close()
+
+    # ---- end to end through the C ABI with pinned host buffers
+    nb = 2 * mix.ngw * s.nbands * 8
+    pin_in = torch.empty(nb // 8, dtype=torch.float64, pin_memory=True)
+    pin_out = torch.empty(nb // 8, dtype=torch.float64, pin_memory=True)
+    cur = mix.get_coeffs()
+    pin_in.numpy()[:] = cur.view(np.float64).ravel()
+    ne2e = max(2, min(args.steps, 5))
+    ms_e2e, _, _ = timed(mix, ne2e, e2e_bufs=(pin_in.numpy(), pin_out.numpy()))
+    mix.close()
+
+    ms_mix = max_over_ranks(ms_mix)
+    ms_f64 = max_over_ranks(ms_f64)
+    ms_e2e = max_over_ranks(ms_e2e)
+
+    if rank == 0:
+        cpu = None
+        if os.environ.get("QBX_BENCH_NO_CPU") != "1":
+            ref = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+            if os.path.exists(ref):
+                threads = os.cpu_count() or 1
+                cms, sample = reference_step_ms(2, 32, threads)
+                cpu = {"value": cms, "unit": "ms", "cores": threads, "kind": "reference",
+                       "sample": sample}
+        line = {
+            "metric": METRIC, "value": ms_mix, "unit": "ms", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mix,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 FFT + f64 GEMM/Cholesky/reductions", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "precision": "mixed",
+                       "l2": "inputs larger than L2 (1.19 GB wavefunctions per step)",
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "fp64_ms_per_step": ms_f64,
+            "mixed_vs_fp64_speedup": ms_f64 / ms_mix,
+            "dE_per_atom": de_atom,
+            "etotal_mixed": r_mix["etotal"], "etotal_fp64": r_f64["etotal"],
+            "roofline": roofline,
+            "gemm": {"ms_per_step": gemm_ms, "flop_per_step": gemm_flop,
+                     "tflops": gemm_flop / (gemm_ms * 1e-3) / 1e12 if gemm_ms else None,
+                     "precision": "fp64 (cuBLAS)"},
+            "profile": prof,
+            "cpu_baseline": cpu,
+            "e2e": {"value": ms_e2e, "unit": "ms", "h2d_bytes_per_step": nb,
+                    "d2h_bytes_per_step": nb},
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

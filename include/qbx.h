@@ -1,0 +1,157 @@
+/*
+ * qbx.h - C ABI of the B200 Kohn-Sham electronic step.
+ *
+ * One qbx_context holds one Gamma-point Slater determinant on one GPU (the
+ * reference's Context collapsed to one process).  The entry points mirror
+ * the reference Qbox classes on the electronic-step path; each names the
+ * reference interface it replaces.  All arrays are host pointers unless the
+ * name says otherwise; all sizes are element counts.  Every call returns 0
+ * on success or a positive error code; qbx_last_error() gives the message.
+ *
+ * Conventions (as in the reference):
+ *  - units are Hartree atomic units; ecut is in Hartree (the reference's
+ *    `set ecut` value in Rydberg divided by 2, src/Ecut.h:40-50);
+ *  - coefficients are complex doubles (re, im interleaved), band-major:
+ *    c[2*(n*ngw + ig) + {0,1}], ig over the half sphere of G vectors;
+ *  - the default coefficient order is sorted Miller index (h,k,l), the order
+ *    returned by qbx_basis_miller(); any other order can be used by passing
+ *    the caller's Miller indices to qbx_set_coeff_order();
+ *  - real-space grids are np0*np1*np2 doubles, x fastest
+ *    (src/BasisMapping.cpp:206-216);
+ *  - energies[QBX_NENERGY] = { ekin, eps, enl, ehart, ecoul, exc, esr, eself,
+ *    etotal, eigenvalue_sum, total_charge, theta }.
+ */
+#ifndef QBX_H
+#define QBX_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct qbx_context qbx_context;
+
+#define QBX_FP64 0   /* FP64 FFTs and FP64 GEMMs                        */
+#define QBX_MIXED 1  /* FP32 FFTs; FP64 storage, reductions, Cholesky   */
+#define QBX_NENERGY 12
+
+int qbx_version(void);
+
+/* Context::Context / MPIdata::set(1,1,1,1): one process, one GPU. */
+int qbx_create(qbx_context** ctx, int device, int precision);
+void qbx_destroy(qbx_context* ctx);
+const char* qbx_last_error(const qbx_context* ctx);
+int qbx_set_precision(qbx_context* ctx, int precision);
+
+/* Basis::resize (src/Basis.cpp:255-643) for the wavefunctions at ecut and
+ * the density at 4*ecut, the dense FFT grid of ChargeDensity
+ * (src/ChargeDensity.cpp:36-49), and Wavefunction::set_nel / update_occ for
+ * nst doubly occupied bands.  xc is "LDA" or "PBE".  cell holds a0,a1,a2. */
+int qbx_set_cell(qbx_context* ctx, const double cell[9], double ecut, int nst,
+                 const char* xc);
+/* Sizes: wavefunction and density basis sizes and the grid. */
+int qbx_basis_sizes(const qbx_context* ctx, int* ngw, int* ngv, int np[3]);
+/* Miller indices (3*ngw ints) of the wavefunction basis, default order. */
+int qbx_basis_miller(const qbx_context* ctx, int* hkl);
+/* Use the caller's coefficient order: hkl = 3*ngw Miller indices, one per
+ * coefficient row as the caller stores them (NULL restores the default). */
+int qbx_set_coeff_order(qbx_context* ctx, const int* hkl);
+
+/* Species::initialize_slpp (src/Species.cpp:510-1055) from the radial
+ * tables of a semilocal norm-conserving species: local potential vlocal on
+ * a uniform mesh r_i = i*mesh_spacing, nproj projectors proj[iop*nmesh+i]
+ * of angular momentum proj_l[iop] (0 or 1) with diagonal D-matrix entries
+ * dmat[iop].  Returns the species index in *isp. */
+int qbx_add_species(qbx_context* ctx, int zval, double mesh_spacing, int nmesh,
+                    const double* vlocal, int nproj, const int* proj_l,
+                    const double* proj, const double* dmat, int* isp);
+
+/* EnergyFunctional::atoms_moved (src/EnergyFunctional.cpp:1047-1197) and
+ * NonLocalPotential::update_twnl: structure factors, local potential,
+ * pseudocharges, E_sr and projectors for positions tau (bohr, 3 per atom,
+ * species-major; na[isp] atoms of each species added so far). */
+int qbx_set_atoms(qbx_context* ctx, const int* na, const double* tau);
+
+/* SlaterDet coefficients (src/SlaterDet.h:35-109): upload / download.
+ * qbx_set_coeffs starts a new stepper history (as a freshly loaded
+ * wavefunction does); the _async forms keep it, for callers that keep the
+ * SlaterDet in host memory and stream it through every step. */
+int qbx_set_coeffs(qbx_context* ctx, const double* c);
+int qbx_get_coeffs(qbx_context* ctx, double* c);
+/* Upload/download without synchronising the host (pinned buffers). */
+int qbx_set_coeffs_async(qbx_context* ctx, const double* c);
+int qbx_get_coeffs_async(qbx_context* ctx, double* c);
+
+/* SlaterDet::gram (src/SlaterDet.cpp:480-534). */
+int qbx_gram(qbx_context* ctx);
+
+/* ChargeDensity::update_density (src/ChargeDensity.cpp:136-198). */
+int qbx_update_density(qbx_context* ctx, double* total_charge);
+int qbx_get_density(qbx_context* ctx, double* rhor);
+
+/* EnergyFunctional::update_vhxc (src/EnergyFunctional.cpp:231-394). */
+int qbx_update_vhxc(qbx_context* ctx);
+int qbx_get_vr(qbx_context* ctx, double* vr);
+
+/* EnergyFunctional::energy(compute_hpsi, dwf, compute_forces, fion, ...)
+ * (src/EnergyFunctional.cpp:397-1044) including NonLocalPotential::energy
+ * (src/NonLocalPotential.cpp:1258-2069) and SlaterDet::rs_mul_add
+ * (src/SlaterDet.cpp:410-477).  fion (3 per atom) may be NULL. */
+int qbx_energy(qbx_context* ctx, int compute_hpsi, int compute_forces,
+               double* energies, double* fion);
+int qbx_get_hpsi(qbx_context* ctx, double* hc);
+
+/* Wavefunction::dot(dwf) (src/SlaterDet.cpp:1122-1153). */
+int qbx_eigenvalue_sum(qbx_context* ctx, double* eigsum);
+
+/* PSDAWavefunctionStepper::update (src/PSDAWavefunctionStepper.cpp:46-249),
+ * ending with SlaterDet::ortho_align (src/SlaterDet.cpp:768-876). */
+int qbx_psda_update(qbx_context* ctx);
+int qbx_psda_reset(qbx_context* ctx);
+
+/* One electronic step of the SCF loop with nite = 0
+ * (src/BOSampleStepper.cpp:795-977): update_density, update_vhxc,
+ * energy(true,...), eigenvalue_sum, PSDA update. */
+int qbx_scf_step(qbx_context* ctx, int compute_forces, double* energies,
+                 double* fion);
+
+/* FourierTransform::backward(c1, c2, f) on the density grid
+ * (src/FourierTransform.cpp:193-205): two bands n1, n2 of the current
+ * wavefunctions to the complex grid f (2*np012 doubles, host). */
+int qbx_ft_backward_pair(qbx_context* ctx, int n1, int n2, double* f);
+
+int qbx_synchronize(qbx_context* ctx);
+
+/* Timer/TimerMap equivalent (src/Timer.h:21-76): CUDA-event timing of the
+ * library's named regions on its stream ("xy_vpsi", "gemm_nl_project",
+ * "update_density", ...).  qbx_profile(ctx, 1) clears and starts recording;
+ * qbx_profile_get returns the total milliseconds and count of one region. */
+int qbx_profile(qbx_context* ctx, int on);
+int qbx_profile_get(qbx_context* ctx, const char* name, double* ms,
+                    long* count);
+/* Number of kernels of this library launched on the context so far. */
+int qbx_launch_count(qbx_context* ctx, long* n);
+/* The cudaStream_t all work of the context is ordered on. */
+void* qbx_stream(qbx_context* ctx);
+
+/* Host-only setup helpers (no GPU needed), exposing the same host code the
+ * context uses.  Basis::resize + ChargeDensity grid: basis sizes, grid and
+ * (if hkl != NULL) the 3*ngw Miller indices in the default order. */
+int qbx_host_basis(const double cell[9], double ecut, int* ngw, int* ngv,
+                   int np[3], int* hkl);
+/* Species::initialize_slpp + Species::dvlocg / vnlg (src/Species.cpp:
+ * 1133-1185) evaluated at ng values of |G|: vloc[ng], dvloc[ng],
+ * vnl[nproj*ng]. */
+int qbx_host_species_eval(int zval, double mesh_spacing, int nmesh,
+                          const double* vlocal, int nproj, const int* proj_l,
+                          const double* proj, int ng, const double* g,
+                          double* vloc, double* dvloc, double* vnl);
+/* E_sr and its forces (src/EnergyFunctional.cpp:1112-1192); fion has 3 per
+ * atom, species-major. */
+int qbx_host_esr(const double cell[9], int nsp, const int* na,
+                 const double* zv, const double* tau, double* esr,
+                 double* fion);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

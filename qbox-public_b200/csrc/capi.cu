@@ -1,0 +1,613 @@
+// C ABI of the library (declared in include/qbx.h).  Each entry point wraps
+// one operation of the reference's class API on the electronic-step path,
+// converts exceptions to status codes and keeps the message for
+// qbx_last_error().
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <new>
+#include <stdexcept>
+#include <tuple>
+
+#include "../../include/qbx.h"
+#include "qbx_internal.h"
+
+struct qbx_context {
+  qbx::Context c;
+  std::vector<int> perm;          // caller row -> internal row
+  int* d_perm = nullptr;
+};
+
+namespace qbx {
+void gram(Context& ctx);
+void ortho_align(Context& ctx);
+void update_density(Context& ctx);
+void update_vhxc(Context& ctx);
+void energy(Context& ctx, bool hpsi, bool forces);
+void psda_update(Context& ctx);
+}
+
+using namespace qbx;
+
+namespace {
+
+template <typename F>
+int guarded(qbx_context* h, F f) {
+  if (!h) return 1;
+  try {
+    QBX_CUDA(cudaSetDevice(h->c.device));
+    f(h->c);
+    h->c.last_error.clear();
+    return 0;
+  } catch (const Error& e) {
+    h->c.last_error = e.msg;
+    return e.code > 0 ? e.code : 1;
+  } catch (const std::bad_alloc&) {
+    h->c.last_error = "host allocation failed";
+    return 5;
+  } catch (const std::exception& e) {
+    h->c.last_error = e.what();
+    return 6;
+  }
+}
+
+void free_cell(Context& c) {
+  free_sticks(c.dws);
+  free_sticks(c.dvs);
+  double** bufs[] = {&c.d_gx_w, &c.d_g2_w, &c.d_gx_v, &c.d_g2i_v, &c.d_c, &c.d_hc, &c.d_c_last,
+                     &c.d_dc_last, &c.d_ctmp, &c.d_occ, &c.d_rhor, &c.d_vr, &c.d_vxc,
+                     &c.d_exc, &c.d_vx2, &c.d_grad, &c.d_rhog, &c.d_vion, &c.d_rhops,
+                     &c.d_vtmp_g, &c.d_vtmp_g2, &c.d_nn, &c.d_nn2, &c.d_nn3, &c.d_nn4,
+                     &c.d_solver_work, &c.d_red, &c.d_scalars, &c.d_prec};
+  for (double** b : bufs) dfree(*b);
+  dfree(c.d_ipiv);
+  dfree(c.d_info);
+  if (c.d_grid) { cudaFree(c.d_grid); c.d_grid = nullptr; }
+  if (c.d_zbuf) { cudaFree(c.d_zbuf); c.d_zbuf = nullptr; }
+  c.have_cell = false;
+}
+
+void free_atoms(Context& c) {
+  double** bufs[] = {&c.d_anl, &c.d_fnl, &c.d_dfnl, &c.d_pdfac, &c.d_sfac, &c.d_vps,
+                     &c.d_rhops_sp, &c.d_fion};
+  for (double** b : bufs) dfree(*b);
+  dfree(c.d_patom);
+  c.nproj = 0;
+}
+
+void fill_energies(const Context& c, double* e) {
+  if (!e) return;
+  const double v[QBX_NENERGY] = {c.ekin, c.eps, c.enl, c.ehart, c.ecoul, c.exc, c.esr, c.eself,
+                                 c.etotal, c.eigsum, c.total_charge, c.theta};
+  std::memcpy(e, v, sizeof(v));
+}
+
+__global__ void k_permute(const double2* __restrict__ in, const int* __restrict__ perm, int ngw,
+                          int nst, int to_internal, double2* __restrict__ out) {
+  const size_t n = (size_t)ngw * nst;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const size_t b = t / ngw;
+    const int i = (int)(t - b * ngw);
+    if (to_internal) out[b * ngw + perm[i]] = in[t];
+    else out[t] = in[b * ngw + perm[i]];
+  }
+}
+
+// density weights occ/Omega are kept in d_wdens (a slice of the scalar pool)
+void upload_weights(Context& c) {
+  std::vector<double> w(c.nst);
+  for (int n = 0; n < c.nst; n++) w[n] = c.occ[n] / c.wb.omega;
+  h2d_sync(c.d_scalars + 16, w.data(), sizeof(double) * c.nst);
+}
+
+void check_ready(const Context& c, bool atoms) {
+  QBX_REQUIRE(c.have_cell, 7, "qbx_set_cell has not been called");
+  if (atoms) QBX_REQUIRE(c.d_vion != nullptr && !c.tau.empty(), 7, "qbx_set_atoms has not been called");
+}
+
+}  // namespace
+
+// density weights live after the 16 scalar slots
+namespace qbx {
+double* density_weights(Context& c) { return c.d_scalars + 16; }
+}
+
+extern "C" {
+
+int qbx_version(void) { return 1; }
+
+int qbx_create(qbx_context** out, int device, int precision) {
+  if (!out) return 1;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return 8;
+  if (device < 0 || device >= ndev) return 9;
+  if (precision != QBX_FP64 && precision != QBX_MIXED) return 1;
+  qbx_context* h = new (std::nothrow) qbx_context();
+  if (!h) return 5;
+  h->c.device = device;
+  h->c.precision = precision;
+  const int rc = guarded(h, [&](Context& c) {
+    QBX_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+    QBX_BLAS(cublasCreate(&c.blas));
+    QBX_BLAS(cublasSetStream(c.blas, c.stream));
+    QBX_SOLVER(cusolverDnCreate(&c.solver));
+    QBX_SOLVER(cusolverDnSetStream(c.solver, c.stream));
+  });
+  if (rc) { delete h; return rc; }
+  *out = h;
+  return 0;
+}
+
+void qbx_destroy(qbx_context* h) {
+  if (!h) return;
+  cudaSetDevice(h->c.device);
+  if (h->c.stream) cudaStreamSynchronize(h->c.stream);
+  free_atoms(h->c);
+  free_cell(h->c);
+  dfree(h->d_perm);
+  if (h->c.blas) cublasDestroy(h->c.blas);
+  if (h->c.solver) cusolverDnDestroy(h->c.solver);
+  if (h->c.stream) cudaStreamDestroy(h->c.stream);
+  delete h;
+}
+
+const char* qbx_last_error(const qbx_context* h) {
+  return h ? h->c.last_error.c_str() : "null context";
+}
+
+int qbx_set_precision(qbx_context* h, int precision) {
+  return guarded(h, [&](Context& c) {
+    QBX_REQUIRE(precision == QBX_FP64 || precision == QBX_MIXED, 1, "unknown precision");
+    if (c.have_cell && precision != c.precision) {
+      // the stick buffer holds the precision's complex type
+      c.precision = precision;
+      const size_t per_pair = (size_t)c.wb.n2 * c.wb.nvec *
+                              (precision == QBX_MIXED ? sizeof(float2) : sizeof(double2));
+      if (c.d_zbuf) cudaFree(c.d_zbuf);
+      c.d_zbuf = nullptr;
+      QBX_CUDA(cudaMalloc(&c.d_zbuf, per_pair * c.pair_batch));
+      c.zbuf_bytes = per_pair * c.pair_batch;
+    }
+    c.precision = precision;
+  });
+}
+
+int qbx_set_cell(qbx_context* h, const double cell[9], double ecut, int nst, const char* xc) {
+  return guarded(h, [&](Context& c) {
+    QBX_REQUIRE(cell && ecut > 0.0 && nst > 0, 1, "bad cell, ecut or band count");
+    const std::string x = xc ? xc : "LDA";
+    QBX_REQUIRE(x == "LDA" || x == "PBE", 1, "xc must be LDA or PBE");
+    free_atoms(c);
+    free_cell(c);
+    c.xc = x;
+    build_basis(c.wb, cell, ecut);
+    build_basis(c.vb, cell, 4.0 * ecut);
+    int np[3];
+    dense_grid(cell, ecut, np);
+    set_grid(c.wb, np[0], np[1], np[2]);
+    set_grid(c.vb, np[0], np[1], np[2]);
+    upload_sticks(c.dws, c.wb);
+    upload_sticks(c.dvs, c.vb);
+    c.nst = nst;
+    c.occ.assign(nst, 2.0);
+    c.extrapolate = false;
+    const int ngw = c.wb.ng, ngv = c.vb.ng;
+    const size_t N = c.N();
+    c.d_gx_w = dupload(c.wb.gx);
+    c.d_g2_w = dupload(c.wb.g2);
+    c.d_gx_v = dupload(c.vb.gx);
+    c.d_g2i_v = dupload(c.vb.g2i);
+    const size_t wf = 2 * (size_t)ngw * nst;
+    c.d_c = dalloc<double>(wf);
+    c.d_hc = dalloc<double>(wf);
+    c.d_c_last = dalloc<double>(wf);
+    c.d_dc_last = dalloc<double>(wf);
+    c.d_ctmp = dalloc<double>(wf);
+    QBX_CUDA(cudaMemset(c.d_c, 0, wf * sizeof(double)));
+    c.d_occ = dupload(c.occ);
+    c.d_prec = dalloc<double>(nst);
+    c.d_rhor = dalloc<double>(N);
+    c.d_vr = dalloc<double>(N);
+    c.d_vxc = dalloc<double>(N);
+    c.d_exc = dalloc<double>(N);
+    c.d_vx2 = dalloc<double>(N);
+    c.d_grad = dalloc<double>(3 * N);
+    QBX_CUDA(cudaMalloc(&c.d_grid, N * sizeof(double2)));
+    c.d_rhog = dalloc<double>(2 * (size_t)ngv);
+    c.d_vion = nullptr;
+    c.d_rhops = dalloc<double>(2 * (size_t)ngv);
+    c.d_vtmp_g = dalloc<double>(2 * (size_t)ngv);
+    c.d_vtmp_g2 = dalloc<double>(2 * (size_t)ngv);
+    const size_t nn = (size_t)nst * nst;
+    c.d_nn = dalloc<double>(nn);
+    c.d_nn2 = dalloc<double>(nn);
+    c.d_nn3 = dalloc<double>(nn);
+    c.d_nn4 = dalloc<double>(3 * nn);
+    c.d_ipiv = dalloc<int>(nst);
+    c.d_info = dalloc<int>(1);
+    int lw1 = 0, lw2 = 0;
+    QBX_SOLVER(cusolverDnDpotrf_bufferSize(c.solver, CUBLAS_FILL_MODE_LOWER, nst, c.d_nn, nst, &lw1));
+    QBX_SOLVER(cusolverDnDgetrf_bufferSize(c.solver, nst, nst, c.d_nn, nst, &lw2));
+    c.solver_lwork = std::max(lw1, lw2);
+    c.d_solver_work = dalloc<double>(std::max(1, c.solver_lwork));
+    c.d_red = dalloc<double>(4 * 1024);
+    c.d_scalars = dalloc<double>(16 + nst);
+    upload_weights(c);
+    // staged FFT stick buffer: bounded to ~4 GB per batch of band pairs
+    const int npairs = (nst + 1) / 2;
+    const size_t per_pair = (size_t)c.wb.n2 * c.wb.nvec *
+                            (c.precision == QBX_MIXED ? sizeof(float2) : sizeof(double2));
+    c.pair_batch = (int)std::max<size_t>(1, std::min<size_t>(npairs, ((size_t)4 << 30) / per_pair));
+    QBX_CUDA(cudaMalloc(&c.d_zbuf, per_pair * c.pair_batch));
+    c.zbuf_bytes = per_pair * c.pair_batch;
+    c.species.clear();
+    c.tau.clear();
+    QBX_CUDA(cudaDeviceSynchronize());   // memsets above ran on the legacy stream
+    c.have_cell = true;
+  });
+}
+
+int qbx_basis_sizes(const qbx_context* h, int* ngw, int* ngv, int np[3]) {
+  if (!h || !h->c.have_cell) return 7;
+  if (ngw) *ngw = h->c.wb.ng;
+  if (ngv) *ngv = h->c.vb.ng;
+  if (np) { np[0] = h->c.wb.n0; np[1] = h->c.wb.n1; np[2] = h->c.wb.n2; }
+  return 0;
+}
+
+int qbx_basis_miller(const qbx_context* h, int* hkl) {
+  if (!h || !h->c.have_cell || !hkl) return 7;
+  std::memcpy(hkl, h->c.wb.hkl.data(), sizeof(int) * h->c.wb.hkl.size());
+  return 0;
+}
+
+int qbx_set_coeff_order(qbx_context* h, const int* hkl) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, false);
+    dfree(h->d_perm);
+    h->perm.clear();
+    if (!hkl) return;
+    const int ngw = c.wb.ng;
+    std::map<std::tuple<int, int, int>, int> pos;
+    for (int i = 0; i < ngw; i++)
+      pos[std::make_tuple(c.wb.hkl[3 * i], c.wb.hkl[3 * i + 1], c.wb.hkl[3 * i + 2])] = i;
+    h->perm.resize(ngw);
+    std::vector<char> seen(ngw, 0);
+    for (int i = 0; i < ngw; i++) {
+      auto it = pos.find(std::make_tuple(hkl[3 * i], hkl[3 * i + 1], hkl[3 * i + 2]));
+      QBX_REQUIRE(it != pos.end(), 14, "Miller index not in the basis");
+      QBX_REQUIRE(!seen[it->second], 14, "repeated Miller index");
+      seen[it->second] = 1;
+      h->perm[i] = it->second;
+    }
+    h->d_perm = dupload(h->perm);
+  });
+}
+
+int qbx_add_species(qbx_context* h, int zval, double mesh_spacing, int nmesh, const double* vlocal,
+                    int nproj, const int* proj_l, const double* proj, const double* dmat,
+                    int* isp) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, false);
+    QBX_REQUIRE(zval > 0 && vlocal && nmesh > 8, 1, "bad species data");
+    QBX_REQUIRE(nproj == 0 || (proj_l && proj), 1, "missing projector data");
+    SpeciesTables s;
+    species_from_radial(s, zval, mesh_spacing, nmesh, vlocal, nproj, proj_l, proj, dmat);
+    c.species.push_back(s);
+    if (isp) *isp = (int)c.species.size() - 1;
+  });
+}
+
+int qbx_set_atoms(qbx_context* h, const int* na, const double* tau) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, false);
+    QBX_REQUIRE(!c.species.empty(), 7, "no species defined");
+    const int nsp = (int)c.species.size();
+    free_atoms(c);
+    c.tau.assign(nsp, std::vector<double>());
+    int off = 0, nel = 0, natoms = 0;
+    for (int is = 0; is < nsp; is++) {
+      QBX_REQUIRE(na[is] >= 0, 1, "negative atom count");
+      c.tau[is].assign(tau + 3 * off, tau + 3 * (off + na[is]));
+      off += na[is];
+      nel += (int)c.species[is].zval * na[is];
+    }
+    natoms = off;
+    (void)nel;   // a net charge is allowed, as in the reference
+    // projector columns: species, then projector (l,m), then atom
+    c.nproj = 0;
+    c.proj_dfac.clear();
+    std::vector<int> patom;
+    int atom0 = 0;
+    for (int is = 0; is < nsp; is++) {
+      const SpeciesTables& sp = c.species[is];
+      for (size_t iop = 0; iop < sp.proj_l.size(); iop++)
+        for (int m = 0; m < 2 * sp.proj_l[iop] + 1; m++)
+          for (int ia = 0; ia < na[is]; ia++) {
+            c.proj_dfac.push_back(sp.proj_d[iop]);
+            patom.push_back(atom0 + ia);
+            c.nproj++;
+          }
+      atom0 += na[is];
+    }
+    const int ngw = c.wb.ng, ngv = c.vb.ng;
+    if (c.nproj) {
+      c.d_anl = dalloc<double>(2 * (size_t)ngw * c.nproj);
+      c.d_fnl = dalloc<double>((size_t)c.nproj * c.nst);
+      c.d_dfnl = dalloc<double>((size_t)c.nproj * c.nst);
+      c.d_pdfac = dupload(c.proj_dfac);
+      c.d_patom = dupload(patom);
+    }
+    c.d_fion = dalloc<double>(3 * std::max(1, natoms));
+    // species tables on the density sphere (EnergyFunctional::cell_moved,
+    // src/EnergyFunctional.cpp:1200-1245)
+    std::vector<double> vps((size_t)ngv * nsp), rhops((size_t)ngv * nsp);
+    for (int is = 0; is < nsp; is++)
+      for (int ig = 0; ig < ngv; ig++) {
+        double v, dv;
+        c.species[is].dvlocg(c.vb.g[ig], v, dv);
+        vps[(size_t)is * ngv + ig] = v / c.vb.omega;
+        rhops[(size_t)is * ngv + ig] = c.species[is].rhopsg(c.vb.g[ig]) / c.vb.omega;
+      }
+    c.d_vps = dupload(vps);
+    c.d_rhops_sp = dupload(rhops);
+    c.d_sfac = dalloc<double>(2 * (size_t)ngv * nsp);
+    if (!c.d_vion) c.d_vion = dalloc<double>(2 * (size_t)ngv);
+    launch_setup_atoms(c);
+    std::vector<double> zv(nsp);
+    c.eself = 0.0;
+    for (int is = 0; is < nsp; is++) {
+      zv[is] = c.species[is].zval;
+      c.eself += na[is] * c.species[is].eself();
+    }
+    c.esr = esr_energy_forces(c.wb.cell, c.tau, zv, 1.5, c.fion_esr);
+    QBX_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+static int set_coeffs_impl(qbx_context* h, const double* src, bool sync, bool reset) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, false);
+    const size_t wf = 2 * (size_t)c.wb.ng * c.nst;
+    if (h->d_perm) {
+      QBX_CUDA(cudaMemcpyAsync(c.d_ctmp, src, wf * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+      k_permute<<<1184, 256, 0, c.stream>>>((const double2*)c.d_ctmp, h->d_perm, c.wb.ng, c.nst, 1,
+                                            (double2*)c.d_c);
+      QBX_LAUNCHED(c);
+    } else {
+      QBX_CUDA(cudaMemcpyAsync(c.d_c, src, wf * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    }
+    if (reset) c.extrapolate = false;
+    if (sync) QBX_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+static int get_coeffs_impl(qbx_context* h, const double* dsrc, double* dst, bool sync) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, false);
+    const size_t wf = 2 * (size_t)c.wb.ng * c.nst;
+    if (h->d_perm) {
+      k_permute<<<1184, 256, 0, c.stream>>>((const double2*)dsrc, h->d_perm, c.wb.ng, c.nst, 0,
+                                            (double2*)c.d_ctmp);
+      QBX_LAUNCHED(c);
+      QBX_CUDA(cudaMemcpyAsync(dst, c.d_ctmp, wf * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    } else {
+      QBX_CUDA(cudaMemcpyAsync(dst, dsrc, wf * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    }
+    if (sync) QBX_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+int qbx_set_coeffs(qbx_context* h, const double* c) { return set_coeffs_impl(h, c, true, true); }
+int qbx_set_coeffs_async(qbx_context* h, const double* c) { return set_coeffs_impl(h, c, false, false); }
+int qbx_get_coeffs(qbx_context* h, double* c) {
+  return h ? get_coeffs_impl(h, h->c.d_c, c, true) : 1;
+}
+int qbx_get_coeffs_async(qbx_context* h, double* c) {
+  return h ? get_coeffs_impl(h, h->c.d_c, c, false) : 1;
+}
+int qbx_get_hpsi(qbx_context* h, double* hc) {
+  return h ? get_coeffs_impl(h, h->c.d_hc, hc, true) : 1;
+}
+
+int qbx_gram(qbx_context* h) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, false);
+    gram(c);
+    QBX_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+int qbx_update_density(qbx_context* h, double* total_charge) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, true);
+    update_density(c);
+    if (total_charge) *total_charge = c.total_charge;
+  });
+}
+
+int qbx_get_density(qbx_context* h, double* rhor) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, false);
+    QBX_CUDA(cudaMemcpyAsync(rhor, c.d_rhor, c.N() * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    QBX_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+int qbx_update_vhxc(qbx_context* h) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, true);
+    update_vhxc(c);
+  });
+}
+
+int qbx_get_vr(qbx_context* h, double* vr) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, false);
+    QBX_CUDA(cudaMemcpyAsync(vr, c.d_vr, c.N() * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    QBX_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+int qbx_energy(qbx_context* h, int hpsi, int forces, double* energies, double* fion) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, true);
+    energy(c, hpsi != 0, forces != 0);
+    QBX_CUDA(cudaStreamSynchronize(c.stream));
+    fill_energies(c, energies);
+    if (forces && fion) std::memcpy(fion, c.fion.data(), sizeof(double) * c.fion.size());
+  });
+}
+
+int qbx_eigenvalue_sum(qbx_context* h, double* eig) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, true);
+    c.eigsum = launch_eigsum(c);
+    if (eig) *eig = c.eigsum;
+  });
+}
+
+int qbx_psda_update(qbx_context* h) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, true);
+    psda_update(c);
+    QBX_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+int qbx_psda_reset(qbx_context* h) {
+  return guarded(h, [&](Context& c) { c.extrapolate = false; });
+}
+
+int qbx_scf_step(qbx_context* h, int forces, double* energies, double* fion) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, true);
+    update_density(c);
+    update_vhxc(c);
+    energy(c, true, forces != 0);
+    c.eigsum = launch_eigsum(c);
+    fill_energies(c, energies);
+    if (forces && fion) std::memcpy(fion, c.fion.data(), sizeof(double) * c.fion.size());
+    psda_update(c);
+    QBX_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+int qbx_ft_backward_pair(qbx_context* h, int n1, int n2, double* f) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, false);
+    QBX_REQUIRE(n1 >= 0 && n1 < c.nst && n2 < c.nst, 1, "band index out of range");
+    const size_t N = c.N();
+    const double* c1 = c.d_c + 2 * (size_t)n1 * c.wb.ng;
+    const double* c2 = n2 >= 0 ? c.d_c + 2 * (size_t)n2 * c.wb.ng : nullptr;
+    wb_backward_pair(c, c1, c2, c.d_grad);   // complex grid in the first 2N of d_grad
+    QBX_CUDA(cudaMemcpyAsync(f, c.d_grad, 2 * N * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    QBX_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+int qbx_profile(qbx_context* h, int on) {
+  return guarded(h, [&](Context& c) {
+    QBX_CUDA(cudaStreamSynchronize(c.stream));
+    c.prof.reset();
+    c.prof.on = (on != 0);
+  });
+}
+
+int qbx_profile_get(qbx_context* h, const char* name, double* ms, long* count) {
+  return guarded(h, [&](Context& c) {
+    QBX_CUDA(cudaStreamSynchronize(c.stream));
+    c.prof.resolve();
+    double t = 0.0;
+    long n = 0;
+    for (size_t i = 0; i < c.prof.names.size(); i++)
+      if (c.prof.names[i] == name) { t = c.prof.ms[i]; n = c.prof.count[i]; }
+    if (ms) *ms = t;
+    if (count) *count = n;
+  });
+}
+
+int qbx_launch_count(qbx_context* h, long* n) {
+  if (!h) return 1;
+  if (n) *n = h->c.nlaunch;
+  return 0;
+}
+
+void* qbx_stream(qbx_context* h) { return h ? (void*)h->c.stream : nullptr; }
+
+int qbx_synchronize(qbx_context* h) {
+  return guarded(h, [&](Context& c) { QBX_CUDA(cudaStreamSynchronize(c.stream)); });
+}
+
+int qbx_host_basis(const double cell[9], double ecut, int* ngw, int* ngv, int np[3], int* hkl) {
+  try {
+    Basis w, v;
+    build_basis(w, cell, ecut);
+    build_basis(v, cell, 4.0 * ecut);
+    int g[3];
+    dense_grid(cell, ecut, g);
+    if (ngw) *ngw = w.ng;
+    if (ngv) *ngv = v.ng;
+    if (np) { np[0] = g[0]; np[1] = g[1]; np[2] = g[2]; }
+    if (hkl) std::memcpy(hkl, w.hkl.data(), sizeof(int) * w.hkl.size());
+    return 0;
+  } catch (const Error& e) {
+    return e.code;
+  } catch (...) {
+    return 6;
+  }
+}
+
+int qbx_host_species_eval(int zval, double mesh_spacing, int nmesh, const double* vlocal,
+                          int nproj, const int* proj_l, const double* proj, int ng,
+                          const double* g, double* vloc, double* dvloc, double* vnl) {
+  try {
+    SpeciesTables s;
+    species_from_radial(s, zval, mesh_spacing, nmesh, vlocal, nproj, proj_l, proj, nullptr);
+    for (int i = 0; i < ng; i++) {
+      double v, dv;
+      s.dvlocg(g[i], v, dv);
+      if (vloc) vloc[i] = v;
+      if (dvloc) dvloc[i] = dv;
+      for (int p = 0; p < nproj && vnl; p++) {
+        s.dvnlg(p, g[i], v, dv);
+        vnl[(size_t)p * ng + i] = v;
+      }
+    }
+    return 0;
+  } catch (const Error& e) {
+    return e.code;
+  } catch (...) {
+    return 6;
+  }
+}
+
+int qbx_host_esr(const double cell[9], int nsp, const int* na, const double* zv,
+                 const double* tau, double* esr, double* fion) {
+  try {
+    std::vector<std::vector<double>> t(nsp), f;
+    std::vector<double> z(zv, zv + nsp);
+    int off = 0;
+    for (int is = 0; is < nsp; is++) {
+      t[is].assign(tau + 3 * off, tau + 3 * (off + na[is]));
+      off += na[is];
+    }
+    const double e = esr_energy_forces(cell, t, z, 1.5, f);
+    if (esr) *esr = e;
+    if (fion) {
+      int k = 0;
+      for (int is = 0; is < nsp; is++)
+        for (double x : f[is]) fion[k++] = x;
+    }
+    return 0;
+  } catch (const Error& e) {
+    return e.code;
+  } catch (...) {
+    return 6;
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,670 @@
+// Staged 3-D FFTs of the electronic step on sm_100a.
+//
+// Wavefunction transforms (the hot path) never build the full 3-D grid in
+// HBM.  A band pair psi_1 + i psi_2 (the reference's two-real-functions
+// packing, src/BasisMapping.cpp:667-750) goes through three kernels:
+//
+//   k_zfft_bwd : gather the coefficients of a few rods, expand them into
+//                z-sticks (+G and -G columns), inverse FFT along z in shared
+//                memory, write the sticks plane-major  zbuf[pair][z][stick].
+//   k_xy       : one CTA per z-plane: scatter that plane's stick values into
+//                a compact (x-column x y) tile in shared memory, inverse FFT
+//                along y on the occupied columns only, then row by row the
+//                inverse FFT along x, and the fused real-space operation:
+//                  OP_DENSITY: rho += f1/Omega psi_1^2 + f2/Omega psi_2^2
+//                  OP_VPSI:    psi *= V(r), forward x FFT, back into the tile;
+//                              forward y FFT, write the plane's sticks back.
+//   k_zfft_fwd : forward z FFT of the sticks, unpack the two bands
+//                (src/BasisMapping.cpp:722-750), scale by 1/N and write
+//                hc = 1/2|G|^2 c + result   (kinetic term fused).
+//
+// Per band pair the HBM traffic is the coefficients, the sticks written and
+// read in each direction and the potential plane: the staged floor.
+//
+// Density-basis transforms (a handful per step) use the full grid with three
+// strided line-FFT passes (k_line_fft).
+//
+// All 1-D FFTs are mixed-radix (2,3,4,5,7,11) self-sorting Stockham passes
+// over shared memory with a twiddle table exp(+2 pi i k/n) built in FP64.
+#include <cstdio>
+#include <vector>
+
+#include "qbx_internal.h"
+
+namespace qbx {
+
+template <typename T> struct Cplx;
+template <> struct Cplx<float> { using t = float2; };
+template <> struct Cplx<double> { using t = double2; };
+
+template <typename C> __device__ __forceinline__ C mk(double x, double y) {
+  C r; r.x = x; r.y = y; return r;
+}
+template <typename C> __device__ __forceinline__ C cadd(C a, C b) {
+  C r; r.x = a.x + b.x; r.y = a.y + b.y; return r;
+}
+template <typename C> __device__ __forceinline__ C csub(C a, C b) {
+  C r; r.x = a.x - b.x; r.y = a.y - b.y; return r;
+}
+template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
+  C r; r.x = a.x * b.x - a.y * b.y; r.y = a.x * b.y + a.y * b.x; return r;
+}
+// multiply by DIR * i
+template <int DIR, typename C> __device__ __forceinline__ C muli(C a) {
+  C r;
+  if (DIR > 0) { r.x = -a.y; r.y = a.x; } else { r.x = a.y; r.y = -a.x; }
+  return r;
+}
+template <int DIR, typename C> __device__ __forceinline__ C twid(const C* tw, int k) {
+  C w = tw[k];
+  if (DIR < 0) w.y = -w.y;
+  return w;
+}
+
+// R-point DFT, out[k] = sum_q v[q] exp(DIR 2 pi i q k / R); roots from the
+// length-n table at stride n/R.
+template <int R, int DIR, typename C>
+__device__ __forceinline__ void small_dft(C* v, const C* tw, int rs) {
+  if (R == 2) {
+    const C a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  } else if (R == 4) {
+    const C a = cadd(v[0], v[2]), b = csub(v[0], v[2]);
+    const C c = cadd(v[1], v[3]), d = muli<DIR>(csub(v[1], v[3]));
+    v[0] = cadd(a, c);
+    v[2] = csub(a, c);
+    v[1] = cadd(b, d);
+    v[3] = csub(b, d);
+  } else {
+    C out[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      C acc = v[0];
+#pragma unroll
+      for (int q = 1; q < R; ++q) acc = cadd(acc, cmul(v[q], twid<DIR>(tw, ((q * k) % R) * rs)));
+      out[k] = acc;
+    }
+#pragma unroll
+    for (int k = 0; k < R; ++k) v[k] = out[k];
+  }
+}
+
+// One Stockham pass over nlines contiguous lines of length n (line stride ls).
+template <int R, int DIR, typename C>
+__device__ __forceinline__ void stockham_pass(const C* __restrict__ src, C* __restrict__ dst,
+                                              int n, int nlines, int ls, int Ns, const C* tw) {
+  const int nb = n / R;
+  const int total = nlines * nb;
+  const int tws = n / (Ns * R);
+  const int rs = n / R;
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    const int line = t / nb;
+    const int i = t - line * nb;
+    const C* s = src + line * ls;
+    C* d = dst + line * ls;
+    const int j = i % Ns;
+    C v[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) v[q] = s[i + q * nb];
+    if (Ns > 1) {
+#pragma unroll
+      for (int q = 1; q < R; ++q) v[q] = cmul(v[q], twid<DIR>(tw, q * j * tws));
+    }
+    small_dft<R, DIR>(v, tw, rs);
+    const int base = (i / Ns) * Ns * R + j;
+#pragma unroll
+    for (int q = 0; q < R; ++q) d[base + q * Ns] = v[q];
+  }
+}
+
+// FFT of nlines lines held in a (ping) with b as the pong buffer; every
+// thread of the CTA participates.  Returns the buffer holding the result.
+template <int DIR, typename C>
+__device__ C* fft_lines(C* a, C* b, int nlines, int ls, const RadixPlan& p, const C* tw) {
+  int Ns = 1;
+  for (int s = 0; s < p.nstage; ++s) {
+    const int r = p.radix[s];
+    switch (r) {
+      case 2: stockham_pass<2, DIR>(a, b, p.n, nlines, ls, Ns, tw); break;
+      case 3: stockham_pass<3, DIR>(a, b, p.n, nlines, ls, Ns, tw); break;
+      case 4: stockham_pass<4, DIR>(a, b, p.n, nlines, ls, Ns, tw); break;
+      case 5: stockham_pass<5, DIR>(a, b, p.n, nlines, ls, Ns, tw); break;
+      case 7: stockham_pass<7, DIR>(a, b, p.n, nlines, ls, Ns, tw); break;
+      default: stockham_pass<11, DIR>(a, b, p.n, nlines, ls, Ns, tw); break;
+    }
+    __syncthreads();
+    C* t = a; a = b; b = t;
+    Ns *= r;
+  }
+  return a;
+}
+
+template <typename C>
+__device__ __forceinline__ void load_twiddles(C* dst, const double2* src, int n) {
+  for (int k = threadIdx.x; k < n; k += blockDim.x) dst[k] = mk<C>(src[k].x, src[k].y);
+}
+
+// --------------------------------------------------------- z backward
+// zbuf layout: [pair][z][stick], stick fastest.
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_zfft_bwd(const double2* __restrict__ c, int ngw, int nst, int pair0,
+           DeviceSticks g, const double2* __restrict__ twz,
+           typename Cplx<T>::t* __restrict__ zbuf, int rods_per_cta) {
+  using C = typename Cplx<T>::t;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  const int n2 = g.n2;
+  C* A = tw + n2;
+  C* B = A + 2 * rods_per_cta * n2;
+  const int r0 = blockIdx.x * rods_per_cta;
+  const int r1 = min(g.nrods, r0 + rods_per_cta);
+  const int s0 = (r0 == 0) ? 0 : 2 * r0 - 1;
+  const int nl = (2 * r1 - 1) - s0;
+  const int pl = blockIdx.y;
+  const int b1 = 2 * (pair0 + pl);
+  const double2* c1 = c + (size_t)b1 * ngw;
+  const double2* c2 = (b1 + 1 < nst) ? c + (size_t)(b1 + 1) * ngw : nullptr;
+  load_twiddles(tw, twz, n2);
+  const int half = (n2 + 1) / 2;
+  for (int t = threadIdx.x; t < nl * n2; t += blockDim.x) {
+    const int line = t / n2, z = t - line * n2;
+    const int s = s0 + line;
+    const int r = (s + 1) >> 1;
+    const int lz = z < half ? z : z - n2;
+    bool minus;
+    int l;
+    if (r == 0) { minus = (lz <= 0); l = minus ? -lz : lz; }
+    else { minus = ((s & 1) == 0); l = minus ? -lz : lz; }
+    const int lmin = g.rod_lmin[r];
+    double vx = 0.0, vy = 0.0;
+    if (l >= lmin && l < lmin + g.rod_size[r]) {
+      const int ig = g.rod_first[r] + (l - lmin);
+      const double2 p = c1[ig];
+      const double2 q = c2 ? c2[ig] : make_double2(0.0, 0.0);
+      // +G: c1 + i c2 ; -G: conj(c1) + i conj(c2)
+      if (!minus) { vx = p.x - q.y; vy = p.y + q.x; }
+      else        { vx = p.x + q.y; vy = q.x - p.y; }
+    }
+    A[line * n2 + z] = mk<C>(vx, vy);
+  }
+  __syncthreads();
+  C* res = fft_lines<+1>(A, B, nl, n2, g.pz, tw);
+  C* out = zbuf + (size_t)pl * n2 * g.nvec;
+  for (int t = threadIdx.x; t < nl * n2; t += blockDim.x) {
+    const int line = t % nl, z = t / nl;
+    out[(size_t)z * g.nvec + s0 + line] = res[line * n2 + z];
+  }
+}
+
+// --------------------------------------------------------- z forward
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_zfft_fwd(const typename Cplx<T>::t* __restrict__ zbuf, int ngw, int nst, int pair0,
+           DeviceSticks g, const double2* __restrict__ twz, double scale,
+           const double2* __restrict__ c, const double* __restrict__ g2,
+           double2* __restrict__ hc, int rods_per_cta) {
+  using C = typename Cplx<T>::t;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  const int n2 = g.n2;
+  C* A = tw + n2;
+  C* B = A + 2 * rods_per_cta * n2;
+  const int r0 = blockIdx.x * rods_per_cta;
+  const int r1 = min(g.nrods, r0 + rods_per_cta);
+  const int s0 = (r0 == 0) ? 0 : 2 * r0 - 1;
+  const int nl = (2 * r1 - 1) - s0;
+  const int pl = blockIdx.y;
+  const int b1 = 2 * (pair0 + pl);
+  const bool two = (b1 + 1 < nst);
+  load_twiddles(tw, twz, n2);
+  const C* in = zbuf + (size_t)pl * n2 * g.nvec;
+  for (int t = threadIdx.x; t < nl * n2; t += blockDim.x) {
+    const int line = t % nl, z = t / nl;
+    A[line * n2 + z] = in[(size_t)z * g.nvec + s0 + line];
+  }
+  __syncthreads();
+  C* res = fft_lines<-1>(A, B, nl, n2, g.pz, tw);
+  const int ig0 = g.rod_first[r0];
+  const int ig1 = g.rod_first[r1 - 1] + g.rod_size[r1 - 1];
+  for (int ig = ig0 + threadIdx.x; ig < ig1; ig += blockDim.x) {
+    int r = r0;
+    while (r + 1 < r1 && g.rod_first[r + 1] <= ig) ++r;
+    const int l = g.rod_lmin[r] + (ig - g.rod_first[r]);
+    const int zp = ((l % n2) + n2) % n2;
+    const int zm = ((-l % n2) + n2) % n2;
+    const int sp = (r == 0) ? 0 : 2 * r - 1 - s0;
+    const int sm = (r == 0) ? 0 : 2 * r - s0;
+    const C P = res[sp * n2 + zp];
+    const C M = res[sm * n2 + zm];
+    // c1 = (Z(G) + conj Z(-G))/2, c2 = -i (Z(G) - conj Z(-G))/2
+    const double px = P.x, py = P.y, mx = M.x, my = M.y;
+    const double c1x = 0.5 * (px + mx) * scale, c1y = 0.5 * (py - my) * scale;
+    const double c2x = 0.5 * (py + my) * scale, c2y = 0.5 * (mx - px) * scale;
+    const double kin = 0.5 * g2[ig];
+    const size_t i1 = (size_t)b1 * ngw + ig;
+    const double2 a = c[i1];
+    hc[i1] = make_double2(kin * a.x + c1x, kin * a.y + c1y);
+    if (two) {
+      const size_t i2 = i1 + ngw;
+      const double2 b = c[i2];
+      hc[i2] = make_double2(kin * b.x + c2x, kin * b.y + c2y);
+    }
+  }
+}
+
+// ------------------------------------------------------------ xy plane
+enum { OP_DENSITY = 0, OP_VPSI = 1 };
+
+template <int DIR, typename C>
+__device__ void y_pass(C* P, C* S, int ncol, int n1, int cc, const RadixPlan& py, const C* twy) {
+  for (int c0 = 0; c0 < ncol; c0 += cc) {
+    const int nc = min(cc, ncol - c0);
+    C* blk = P + c0 * n1;
+    C* res = fft_lines<DIR>(blk, S, nc, n1, py, twy);
+    if (res != blk) {
+      for (int t = threadIdx.x; t < nc * n1; t += blockDim.x) blk[t] = res[t];
+      __syncthreads();
+    }
+  }
+}
+
+template <typename T, int OP>
+__global__ void __launch_bounds__(512)
+k_xy(typename Cplx<T>::t* __restrict__ zbuf, int npairs, int pairs_per_cta,
+     DeviceSticks g, const double2* __restrict__ twx, const double2* __restrict__ twy,
+     const double* __restrict__ v, double* __restrict__ rho,
+     const double* __restrict__ w, int pair0, int nst, int cc, int rr) {
+  using C = typename Cplx<T>::t;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int n0 = g.n0, n1 = g.n1, ncol = g.ncol, nvec = g.nvec;
+  C* tx = reinterpret_cast<C*>(smem_raw);
+  C* ty = tx + n0;
+  C* P = ty + n1;
+  C* S = P + ncol * n1;
+  const int z = blockIdx.x;
+  load_twiddles(tx, twx, n0);
+  load_twiddles(ty, twy, n1);
+  const int pbeg = blockIdx.y * pairs_per_cta;
+  const int pend = min(npairs, pbeg + pairs_per_cta);
+  for (int pl = pbeg; pl < pend; ++pl) {
+    C* zp = zbuf + ((size_t)pl * g.n2 + z) * nvec;
+    for (int t = threadIdx.x; t < ncol * n1; t += blockDim.x) P[t] = mk<C>(0.0, 0.0);
+    __syncthreads();
+    for (int s = threadIdx.x; s < nvec; s += blockDim.x)
+      P[g.stick_col[s] * n1 + g.stick_y[s]] = zp[s];
+    __syncthreads();
+    y_pass<+1>(P, S, ncol, n1, cc, g.py, ty);
+    double w1 = 0.0, w2 = 0.0;
+    if (OP == OP_DENSITY) {
+      const int b1 = 2 * (pair0 + pl);
+      w1 = w[b1];
+      w2 = (b1 + 1 < nst) ? w[b1 + 1] : 0.0;
+    }
+    for (int y0 = 0; y0 < n1; y0 += rr) {
+      const int nr = min(rr, n1 - y0);
+      C* R1 = S;
+      C* R2 = S + rr * n0;
+      for (int t = threadIdx.x; t < nr * n0; t += blockDim.x) R1[t] = mk<C>(0.0, 0.0);
+      __syncthreads();
+      for (int t = threadIdx.x; t < nr * ncol; t += blockDim.x) {
+        const int r = t / ncol, cidx = t - r * ncol;
+        R1[r * n0 + g.col_x[cidx]] = P[cidx * n1 + y0 + r];
+      }
+      __syncthreads();
+      C* res = fft_lines<+1>(R1, R2, nr, n0, g.px, tx);
+      const size_t rowbase = ((size_t)z * n1 + y0) * n0;
+      if (OP == OP_DENSITY) {
+        for (int t = threadIdx.x; t < nr * n0; t += blockDim.x) {
+          const C val = res[t];
+          const double a = val.x, b = val.y;
+          atomicAdd(&rho[rowbase + t], w1 * a * a + w2 * b * b);
+        }
+        __syncthreads();
+      } else {
+        for (int t = threadIdx.x; t < nr * n0; t += blockDim.x) {
+          const double vv = v[rowbase + t];
+          C val = res[t];
+          val.x *= vv; val.y *= vv;
+          res[t] = val;
+        }
+        __syncthreads();
+        C* other = (res == R1) ? R2 : R1;
+        C* res2 = fft_lines<-1>(res, other, nr, n0, g.px, tx);
+        for (int t = threadIdx.x; t < nr * ncol; t += blockDim.x) {
+          const int r = t / ncol, cidx = t - r * ncol;
+          P[cidx * n1 + y0 + r] = res2[r * n0 + g.col_x[cidx]];
+        }
+        __syncthreads();
+      }
+    }
+    if (OP == OP_VPSI) {
+      y_pass<-1>(P, S, ncol, n1, cc, g.py, ty);
+      for (int s = threadIdx.x; s < nvec; s += blockDim.x)
+        zp[s] = P[g.stick_col[s] * n1 + g.stick_y[s]];
+      __syncthreads();
+    }
+  }
+}
+
+// ------------------------------------------------ full-grid line passes
+// In-place FFT of all lines along one axis of an n0 x n1 x n2 grid (x
+// fastest).  A CTA takes L lines; for the y and z axes these are L adjacent
+// x so that global accesses stay coalesced.
+template <int DIR>
+__global__ void __launch_bounds__(256)
+k_line_fft(double2* __restrict__ grid, int n0, int n1, int n2, int axis, RadixPlan p,
+           const double2* __restrict__ tw_g, int L) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* tw = reinterpret_cast<double2*>(smem_raw);
+  const int n = p.n;
+  double2* A = tw + n;
+  double2* B = A + L * n;
+  load_twiddles(tw, tw_g, n);
+  // line set of this CTA
+  size_t base;
+  size_t estride, lstride;
+  int nl;
+  if (axis == 0) {
+    const int nlines = n1 * n2;
+    const int l0 = blockIdx.x * L;
+    nl = min(L, nlines - l0);
+    base = (size_t)l0 * n0;
+    estride = 1; lstride = n0;
+  } else if (axis == 1) {
+    const int xt = (n0 + L - 1) / L;
+    const int zb = blockIdx.x / xt, x0 = (blockIdx.x % xt) * L;
+    nl = min(L, n0 - x0);
+    base = (size_t)x0 + (size_t)n0 * n1 * zb;
+    estride = n0; lstride = 1;
+  } else {
+    const int xt = (n0 + L - 1) / L;
+    const int yb = blockIdx.x / xt, x0 = (blockIdx.x % xt) * L;
+    nl = min(L, n0 - x0);
+    base = (size_t)x0 + (size_t)n0 * yb;
+    estride = (size_t)n0 * n1; lstride = 1;
+  }
+  for (int t = threadIdx.x; t < nl * n; t += blockDim.x) {
+    int line, e;
+    if (axis == 0) { line = t / n; e = t - line * n; }
+    else { line = t % nl; e = t / nl; }
+    A[line * n + e] = grid[base + e * estride + line * lstride];
+  }
+  __syncthreads();
+  double2* res = fft_lines<DIR>(A, B, nl, n, p, tw);
+  for (int t = threadIdx.x; t < nl * n; t += blockDim.x) {
+    int line, e;
+    if (axis == 0) { line = t / n; e = t - line * n; }
+    else { line = t % nl; e = t / nl; }
+    grid[base + e * estride + line * lstride] = res[line * n + e];
+  }
+}
+
+__global__ void k_scatter_sphere(const double2* __restrict__ c, const int* __restrict__ ip,
+                                 const int* __restrict__ im, int ng, double2* __restrict__ grid) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ng; i += gridDim.x * blockDim.x) {
+    const double2 v = c[i];
+    grid[ip[i]] = v;
+    grid[im[i]] = make_double2(v.x, -v.y);
+  }
+}
+
+__global__ void k_scatter_pair(const double2* __restrict__ c1, const double2* __restrict__ c2,
+                               const int* __restrict__ ip, const int* __restrict__ im, int ng,
+                               double2* __restrict__ grid) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ng; i += gridDim.x * blockDim.x) {
+    const double2 p = c1[i];
+    const double2 q = c2 ? c2[i] : make_double2(0.0, 0.0);
+    grid[ip[i]] = make_double2(p.x - q.y, p.y + q.x);
+    grid[im[i]] = make_double2(p.x + q.y, q.x - p.y);
+  }
+}
+
+__global__ void k_gather_sphere(const double2* __restrict__ grid, const int* __restrict__ ip,
+                                int ng, double scale, double2* __restrict__ c) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ng; i += gridDim.x * blockDim.x) {
+    const double2 v = grid[ip[i]];
+    c[i] = make_double2(v.x * scale, v.y * scale);
+  }
+}
+
+__global__ void k_real_to_grid(const double* __restrict__ f, double scale, size_t n,
+                               double2* __restrict__ grid) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    grid[i] = make_double2(f[i] * scale, 0.0);
+}
+
+__global__ void k_grid_real(const double2* __restrict__ grid, size_t n, double* __restrict__ f) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    f[i] = grid[i].x;
+}
+
+// ------------------------------------------------------------ launchers
+static std::vector<double2> twiddle_table(int n) {
+  std::vector<double2> t(n);
+  for (int k = 0; k < n; k++) {
+    const double a = 2.0 * M_PI * (double)k / (double)n;
+    t[k] = make_double2(cos(a), sin(a));
+  }
+  return t;
+}
+
+struct TwiddleCache {
+  int n[3] = {0, 0, 0};
+  double2* d[3] = {nullptr, nullptr, nullptr};
+};
+static TwiddleCache g_tw[16];   // per device
+
+static const double2* twiddles(int dev, int axis, int n) {
+  TwiddleCache& c = g_tw[dev & 15];
+  if (c.n[axis] != n) {
+    if (c.d[axis]) cudaFree(c.d[axis]);
+    std::vector<double2> t = twiddle_table(n);
+    c.d[axis] = dalloc<double2>(n);
+    h2d_sync(c.d[axis], t.data(), n * sizeof(double2));
+    c.n[axis] = n;
+  }
+  return c.d[axis];
+}
+
+void upload_sticks(DeviceSticks& d, const Basis& b) {
+  free_sticks(d);
+  d.n0 = b.n0; d.n1 = b.n1; d.n2 = b.n2;
+  d.nrods = b.nrods; d.nvec = b.nvec; d.ncol = b.ncol;
+  d.rod_first = dupload(b.rod_first);
+  d.rod_lmin = dupload(b.rod_lmin);
+  d.rod_size = dupload(b.rod_size);
+  d.stick_y = dupload(b.stick_y);
+  d.stick_col = dupload(b.stick_col);
+  d.col_x = dupload(b.col_x);
+  d.ip = dupload(b.ip);
+  d.im = dupload(b.im);
+  d.px = make_plan(b.n0);
+  d.py = make_plan(b.n1);
+  d.pz = make_plan(b.n2);
+}
+
+void free_sticks(DeviceSticks& d) {
+  dfree(d.rod_first); dfree(d.rod_lmin); dfree(d.rod_size);
+  dfree(d.stick_y); dfree(d.stick_col); dfree(d.col_x);
+  dfree(d.ip); dfree(d.im);
+}
+
+static const int kRodsPerCta = 8;
+
+template <typename T>
+static size_t zsmem(int n2) {
+  return sizeof(typename Cplx<T>::t) * (size_t)n2 * (1 + 4 * kRodsPerCta);
+}
+
+template <typename T>
+struct XYConfig {
+  size_t smem;
+  int cc, rr;
+};
+
+static int max_smem_optin(int dev) {
+  int v = 0;
+  QBX_CUDA(cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  return v;
+}
+
+template <typename T>
+static XYConfig<T> xy_config(const DeviceSticks& g, int dev) {
+  using C = typename Cplx<T>::t;
+  const size_t fixed = sizeof(C) * ((size_t)g.n0 + g.n1 + (size_t)g.ncol * g.n1);
+  const size_t limit = (size_t)max_smem_optin(dev);
+  // FP32 tiles leave room for two CTAs per SM
+  size_t budget = sizeof(T) == 4 ? std::min(limit, (size_t)112 * 1024) : limit;
+  if (budget < fixed + sizeof(C) * 2 * g.n0) budget = limit;
+  QBX_REQUIRE(budget >= fixed + sizeof(C) * 2 * g.n0, 20,
+              "FFT plane tile does not fit in shared memory");
+  const size_t scratch = budget - fixed;
+  XYConfig<T> c;
+  c.cc = (int)std::min<size_t>(g.ncol, scratch / (sizeof(C) * g.n1));
+  c.rr = (int)std::min<size_t>(g.n1, scratch / (sizeof(C) * 2 * g.n0));
+  const size_t need = std::max(sizeof(C) * (size_t)c.cc * g.n1, sizeof(C) * 2 * (size_t)c.rr * g.n0);
+  c.smem = fixed + need;
+  QBX_REQUIRE(c.cc >= 1 && c.rr >= 1, 20, "FFT plane tile does not fit in shared memory");
+  return c;
+}
+
+template <typename T>
+static void staged_batch(Context& ctx, int op, const double* c, const double* v, double* rho,
+                         const double* w, double* hc, int pair0, int npairs) {
+  using C = typename Cplx<T>::t;
+  const DeviceSticks& g = ctx.dws;
+  cudaStream_t st = ctx.stream;
+  C* zbuf = (C*)ctx.d_zbuf;
+  const double2* twz = twiddles(ctx.device, 2, g.n2);
+  const double2* twx = twiddles(ctx.device, 0, g.n0);
+  const double2* twy = twiddles(ctx.device, 1, g.n1);
+  const int ngw = ctx.wb.ng;
+  dim3 zgrid((g.nrods + kRodsPerCta - 1) / kRodsPerCta, npairs);
+  const size_t zs = zsmem<T>(g.n2);
+  QBX_CUDA(cudaFuncSetAttribute(k_zfft_bwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zs));
+  {
+    ProfScope ps(ctx, "zfft_bwd");
+    k_zfft_bwd<T><<<zgrid, 256, zs, st>>>((const double2*)c, ngw, ctx.nst, pair0, g, twz, zbuf,
+                                           kRodsPerCta);
+    QBX_LAUNCHED(ctx);
+  }
+  XYConfig<T> xc = xy_config<T>(g, ctx.device);
+  int sms = 0;
+  QBX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device));
+  // enough (plane, pair-chunk) CTAs to cover every SM a couple of times
+  int chunks = std::max(1, (3 * sms + g.n2 - 1) / g.n2);
+  chunks = std::min(chunks, npairs);
+  const int ppc = (npairs + chunks - 1) / chunks;
+  chunks = (npairs + ppc - 1) / ppc;
+  dim3 xgrid(g.n2, chunks);
+  if (op == OP_DENSITY) {
+    QBX_CUDA(cudaFuncSetAttribute(k_xy<T, OP_DENSITY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)xc.smem));
+    ProfScope ps(ctx, "xy_density");
+    k_xy<T, OP_DENSITY><<<xgrid, 512, xc.smem, st>>>(zbuf, npairs, ppc, g, twx, twy, nullptr, rho, w,
+                                                   pair0, ctx.nst, xc.cc, xc.rr);
+    QBX_LAUNCHED(ctx);
+  } else {
+    QBX_CUDA(cudaFuncSetAttribute(k_xy<T, OP_VPSI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)xc.smem));
+    {
+      ProfScope ps(ctx, "xy_vpsi");
+      k_xy<T, OP_VPSI><<<xgrid, 512, xc.smem, st>>>(zbuf, npairs, ppc, g, twx, twy, v, nullptr,
+                                                  nullptr, pair0, ctx.nst, xc.cc, xc.rr);
+      QBX_LAUNCHED(ctx);
+    }
+    QBX_CUDA(cudaFuncSetAttribute(k_zfft_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zs));
+    const double scale = 1.0 / ((double)g.n0 * g.n1 * g.n2);
+    ProfScope ps(ctx, "zfft_fwd");
+    k_zfft_fwd<T><<<zgrid, 256, zs, st>>>(zbuf, ngw, ctx.nst, pair0, g, twz, scale,
+                                           (const double2*)c, ctx.d_g2_w, (double2*)hc, kRodsPerCta);
+    QBX_LAUNCHED(ctx);
+  }
+}
+
+static void staged(Context& ctx, int op, const double* c, const double* v, double* rho,
+                   const double* w, double* hc) {
+  const int npairs = (ctx.nst + 1) / 2;
+  for (int p0 = 0; p0 < npairs; p0 += ctx.pair_batch) {
+    const int np = std::min(ctx.pair_batch, npairs - p0);
+    if (ctx.precision == MIXED)
+      staged_batch<float>(ctx, op, c, v, rho, w, hc, p0, np);
+    else
+      staged_batch<double>(ctx, op, c, v, rho, w, hc, p0, np);
+  }
+}
+
+void launch_density(Context& ctx, const double* c, double* rho) {
+  QBX_CUDA(cudaMemsetAsync(rho, 0, ctx.N() * sizeof(double), ctx.stream));
+  staged(ctx, OP_DENSITY, c, nullptr, rho, density_weights(ctx), nullptr);
+}
+
+void launch_vpsi(Context& ctx, const double* c, const double* v, double* hc) {
+  staged(ctx, OP_VPSI, c, v, nullptr, nullptr, hc);
+}
+
+// full-grid transform of the grid held in ctx.d_grid
+static void grid_fft(Context& ctx, int dir) {
+  ProfScope ps(ctx, "grid_fft");
+  const Basis& b = ctx.vb;
+  const int n[3] = {b.n0, b.n1, b.n2};
+  const int L = 16;
+  for (int axis = 0; axis < 3; axis++) {
+    const RadixPlan p = make_plan(n[axis]);
+    const double2* tw = twiddles(ctx.device, axis, n[axis]);
+    int nblocks;
+    if (axis == 0) nblocks = (b.n1 * b.n2 + L - 1) / L;
+    else if (axis == 1) nblocks = ((b.n0 + L - 1) / L) * b.n2;
+    else nblocks = ((b.n0 + L - 1) / L) * b.n1;
+    const size_t smem = sizeof(double2) * (size_t)n[axis] * (1 + 2 * L);
+    if (dir > 0) {
+      QBX_CUDA(cudaFuncSetAttribute(k_line_fft<+1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k_line_fft<+1><<<nblocks, 256, smem, ctx.stream>>>((double2*)ctx.d_grid, b.n0, b.n1, b.n2, axis, p, tw, L);
+    } else {
+      QBX_CUDA(cudaFuncSetAttribute(k_line_fft<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k_line_fft<-1><<<nblocks, 256, smem, ctx.stream>>>((double2*)ctx.d_grid, b.n0, b.n1, b.n2, axis, p, tw, L);
+    }
+    QBX_LAUNCHED(ctx);
+  }
+}
+
+static int nblk(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 16); }
+
+void vb_backward(Context& ctx, const double* coef, double* real_out) {
+  const size_t N = ctx.N();
+  QBX_CUDA(cudaMemsetAsync(ctx.d_grid, 0, N * sizeof(double2), ctx.stream));
+  k_scatter_sphere<<<nblk(ctx.vb.ng), 256, 0, ctx.stream>>>((const double2*)coef, ctx.dvs.ip,
+                                                            ctx.dvs.im, ctx.vb.ng, (double2*)ctx.d_grid);
+  QBX_LAUNCHED(ctx);
+  grid_fft(ctx, +1);
+  k_grid_real<<<nblk(N), 256, 0, ctx.stream>>>((const double2*)ctx.d_grid, N, real_out);
+  QBX_LAUNCHED(ctx);
+}
+
+void vb_forward_real(Context& ctx, const double* f, double scale, double* coef) {
+  const size_t N = ctx.N();
+  k_real_to_grid<<<nblk(N), 256, 0, ctx.stream>>>(f, scale, N, (double2*)ctx.d_grid);
+  QBX_LAUNCHED(ctx);
+  grid_fft(ctx, -1);
+  k_gather_sphere<<<nblk(ctx.vb.ng), 256, 0, ctx.stream>>>((const double2*)ctx.d_grid, ctx.dvs.ip,
+                                                           ctx.vb.ng, 1.0 / (double)N, (double2*)coef);
+  QBX_LAUNCHED(ctx);
+}
+
+void wb_backward_pair(Context& ctx, const double* c1, const double* c2, double* grid_out) {
+  const size_t N = ctx.N();
+  QBX_CUDA(cudaMemsetAsync(ctx.d_grid, 0, N * sizeof(double2), ctx.stream));
+  k_scatter_pair<<<nblk(ctx.wb.ng), 256, 0, ctx.stream>>>((const double2*)c1, (const double2*)c2,
+                                                          ctx.dws.ip, ctx.dws.im, ctx.wb.ng,
+                                                          (double2*)ctx.d_grid);
+  QBX_LAUNCHED(ctx);
+  grid_fft(ctx, +1);
+  QBX_CUDA(cudaMemcpyAsync(grid_out, ctx.d_grid, N * sizeof(double2), cudaMemcpyDeviceToDevice,
+                           ctx.stream));
+}
+
+}  // namespace qbx

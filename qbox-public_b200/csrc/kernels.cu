@@ -1,0 +1,736 @@
+// Pointwise, G-space and reduction kernels of the electronic step.
+//
+// Everything here is memory-bound elementwise work in FP64: the exchange-
+// correlation functionals on the real-space grid, the Hartree/local-potential
+// algebra on the density sphere, kinetic energy and eigenvalue-sum
+// reductions, the preconditioned steepest-descent update with Anderson
+// extrapolation, and the per-geometry structure factors and projectors.
+// Reductions are deterministic: fixed-size partial sums per CTA, then one CTA
+// adds the partials in order.
+#include <cmath>
+#include <vector>
+
+#include "qbx_internal.h"
+
+namespace qbx {
+
+static const int kRedBlocks = 592;   // 4 x 148 SMs
+static const int kThreads = 256;
+
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < (int)(blockDim.x >> 5); i++) r += sh[i];
+  return r;   // valid in thread 0
+}
+
+// sum of up to 4 quantities produced by functor F(i, out[4]) over i < n
+template <int K, typename F>
+__global__ void __launch_bounds__(kThreads) k_reduce(F f, size_t n, double* partial) {
+  __shared__ double sh[32];
+  double acc[K];
+#pragma unroll
+  for (int k = 0; k < K; k++) acc[k] = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    f(i, acc);
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    const double s = block_sum(acc[k], sh);
+    if (threadIdx.x == 0) partial[k * gridDim.x + blockIdx.x] = s;
+  }
+}
+
+template <int K>
+__global__ void k_reduce_final(const double* partial, int nb, double* out) {
+  __shared__ double sh[32];
+  for (int k = 0; k < K; k++) {
+    double a = 0.0;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) a += partial[k * nb + i];
+    const double s = block_sum(a, sh);
+    if (threadIdx.x == 0) out[k] = s;
+  }
+}
+
+template <int K, typename F>
+static void reduce(Context& ctx, F f, size_t n, double* host_out) {
+  const int nb = (int)std::max<size_t>(1, std::min<size_t>(kRedBlocks, (n + kThreads - 1) / kThreads));
+  k_reduce<K><<<nb, kThreads, 0, ctx.stream>>>(f, n, ctx.d_red);
+  QBX_LAUNCHED(ctx);
+  k_reduce_final<K><<<1, kThreads, 0, ctx.stream>>>(ctx.d_red, nb, ctx.d_scalars);
+  QBX_LAUNCHED(ctx);
+  QBX_CUDA(cudaMemcpyAsync(host_out, ctx.d_scalars, K * sizeof(double), cudaMemcpyDeviceToHost,
+                           ctx.stream));
+  QBX_CUDA(cudaStreamSynchronize(ctx.stream));
+}
+
+static int blocks_for(size_t n) {
+  return (int)std::max<size_t>(1, std::min<size_t>((n + kThreads - 1) / kThreads, 148 * 32));
+}
+
+struct SumF {
+  const double* x;
+  __device__ void operator()(size_t i, double* a) const { a[0] += x[i]; }
+};
+
+double dsum(Context& ctx, const double* x, size_t n) {
+  double r;
+  reduce<1>(ctx, SumF{x}, n, &r);
+  return r;
+}
+
+// ------------------------------------------------------------------- XC
+// Perdew-Zunger LDA (src/LDAFunctional.cpp:92-150), unpolarized.
+__device__ void lda_pz(double rh, double& ee, double& vv) {
+  const double c1 = 0.6203504908994001, c3 = -0.610887057711;
+  const double A = 0.0311, B = -0.048, b1 = 1.0529, b2 = 0.3334, G = -0.1423;
+  const double D = G / (1.0 + b1 + b2) - B;
+  const double C = -A - D - G * ((b1 / 2.0 + b2) / ((1.0 + b1 + b2) * (1.0 + b1 + b2)));
+  ee = 0.0; vv = 0.0;
+  if (rh > 0.0) {
+    const double rs = c1 / cbrt(rh);
+    const double vx = c3 / rs, ex = 0.75 * vx;
+    double ec, vc;
+    if (rs < 1.0) {
+      const double lr = log(rs);
+      ec = A * lr + B + C * rs * lr + D * rs;
+      vc = A * lr + (B - A / 3.0) + (2.0 / 3.0) * C * rs * lr + ((2.0 * D - C) / 3.0) * rs;
+    } else {
+      const double sq = sqrt(rs), den = 1.0 + b1 * sq + b2 * rs;
+      ec = G / den;
+      vc = ec * (1.0 + (7.0 / 6.0) * b1 * sq + (4.0 / 3.0) * b2 * rs) / den;
+    }
+    ee = ex + ec;
+    vv = vx + vc;
+  }
+}
+
+// PBE (src/PBEFunctional.cpp:168-280; PW92 local correlation via gcor2).
+__device__ void pbe(double rho, double grad, double& exc, double& v1, double& v2) {
+  const double third = 1.0 / 3.0, third4 = 4.0 / 3.0;
+  const double ax = -0.7385587663820224058, um = 0.2195149727645171, uk = 0.804;
+  const double ul = um / uk, pi32third = 3.09366772628014, alpha = 1.91915829267751;
+  const double seven_sixth = 7.0 / 6.0, four_over_pi = 1.27323954473516;
+  const double gamma = 0.03109069086965489, bet = 0.06672455060314922;
+  const double delt = bet / gamma;
+  exc = 0.0; v1 = 0.0; v2 = 0.0;
+  if (rho < 1.e-18) return;
+  const double rh13 = pow(rho, third);
+  const double exunif = ax * rh13;
+  const double fk = pi32third * rh13;
+  const double s = grad / (2.0 * fk * rho);
+  const double s2 = s * s;
+  const double p0 = 1.0 + ul * s2;
+  const double fxpbe = 1.0 + uk - uk / p0;
+  const double ex = exunif * fxpbe;
+  const double fs = 2.0 * uk * ul / (p0 * p0);
+  const double vx1 = third4 * exunif * (fxpbe - s2 * fs);
+  const double vx2 = -exunif * fs / (rho * 4.0 * fk * fk);
+  const double rs = alpha / fk;
+  const double twoks = 2.0 * sqrt(four_over_pi * fk);
+  const double t = grad / (twoks * rho);
+  const double rtrs = sqrt(rs);
+  const double a = 0.0310907, a1 = 0.2137, bb1 = 7.5957, bb2 = 3.5876, bb3 = 1.6382, bb4 = 0.49294;
+  const double q0 = -2.0 * a * (1.0 + a1 * rtrs * rtrs);
+  const double q1 = 2.0 * a * rtrs * (bb1 + rtrs * (bb2 + rtrs * (bb3 + rtrs * bb4)));
+  const double q2 = log(1.0 + 1.0 / q1);
+  const double ec = q0 * q2;
+  const double q3 = a * (bb1 / rtrs + 2.0 * bb2 + rtrs * (3.0 * bb3 + 4.0 * bb4 * rtrs));
+  const double ecrs = -2.0 * a * a1 * q2 - q0 * q3 / (q1 * (1.0 + q1));
+  const double vc = ec - rs * ecrs * third;
+  const double pon = -ec / gamma;
+  const double b = delt / (exp(pon) - 1.0);
+  const double b2 = b * b, t2 = t * t, t4 = t2 * t2;
+  const double q4 = 1.0 + b * t2;
+  const double q5 = q4 + b2 * t4;
+  const double h = gamma * log(1.0 + delt * q4 * t2 / q5);
+  const double t6 = t4 * t2, rsthrd = rs * third;
+  const double fac = delt / b + 1.0;
+  const double bec = b2 * fac / bet;
+  const double q8 = q5 * q5 + delt * q4 * q5 * t2;
+  const double q9 = 1.0 + 2.0 * b * t2;
+  const double hb = -bet * b * t6 * (2.0 + b * t2) / q8;
+  const double hrs = -rsthrd * hb * bec * ecrs;
+  const double ht = 2.0 * bet * q9 / q8;
+  const double vc1 = vc + h + hrs - t2 * ht * seven_sixth;
+  const double vc2 = -ht / (rho * twoks * twoks);
+  exc = ex + ec + h;
+  v1 = vx1 + vc1;
+  v2 = vx2 + vc2;
+}
+
+__global__ void k_lda(const double* __restrict__ rho, size_t n, double* __restrict__ vxc,
+                      double* __restrict__ erho) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    double e, v;
+    lda_pz(rho[i], e, v);
+    vxc[i] = v;
+    erho[i] = rho[i] * e;
+  }
+}
+
+__global__ void k_pbe(const double* __restrict__ rho, const double* __restrict__ grad, size_t n,
+                      double* __restrict__ v1, double* __restrict__ v2, double* __restrict__ erho) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const double gx = grad[i], gy = grad[n + i], gz = grad[2 * n + i];
+    const double g = sqrt(gx * gx + gy * gy + gz * gz);
+    double e, a, b;
+    pbe(rho[i], g, e, a, b);
+    v1[i] = a;
+    v2[i] = b;
+    erho[i] = rho[i] * e;
+  }
+}
+
+// out(G) = i gx_j(G) scale in(G)
+__global__ void k_mul_igx(const double2* __restrict__ in, const double* __restrict__ gxj, int ng,
+                          double scale, double2* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ng; i += gridDim.x * blockDim.x) {
+    const double2 v = in[i];
+    const double g = gxj[i] * scale;
+    out[i] = make_double2(-g * v.y, g * v.x);
+  }
+}
+
+__global__ void k_mul(const double* __restrict__ a, const double* __restrict__ b, size_t n,
+                      double* __restrict__ out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    out[i] = a[i] * b[i];
+}
+
+__global__ void k_axpy(double* __restrict__ y, const double* __restrict__ x, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    y[i] += x[i];
+}
+
+// XCPotential::update (src/XCPotential.cpp:124-465): vxc and E_xc.
+void launch_xc(Context& ctx) {
+  const size_t N = ctx.N();
+  const double om = ctx.vb.omega;
+  const int nb = blocks_for(N);
+  if (ctx.xc == "LDA") {
+    k_lda<<<nb, kThreads, 0, ctx.stream>>>(ctx.d_rhor, N, ctx.d_vxc, ctx.d_exc);
+    QBX_LAUNCHED(ctx);
+    ctx.exc = dsum(ctx, ctx.d_exc, N) * om / (double)N;
+    return;
+  }
+  // PBE: grad rho by three backward transforms of i G_j rho(G)/Omega
+  const int ngv = ctx.vb.ng;
+  for (int j = 0; j < 3; j++) {
+    k_mul_igx<<<blocks_for(ngv), kThreads, 0, ctx.stream>>>(
+        (const double2*)ctx.d_rhog, ctx.d_gx_v + (size_t)j * ngv, ngv, 1.0 / om,
+        (double2*)ctx.d_vtmp_g);
+    QBX_LAUNCHED(ctx);
+    vb_backward(ctx, ctx.d_vtmp_g, ctx.d_grad + j * N);
+  }
+  k_pbe<<<nb, kThreads, 0, ctx.stream>>>(ctx.d_rhor, ctx.d_grad, N, ctx.d_vxc, ctx.d_vx2,
+                                         ctx.d_exc);
+  QBX_LAUNCHED(ctx);
+  ctx.exc = dsum(ctx, ctx.d_exc, N) * om / (double)N;
+  // vxc += sum_j backward(i G_j forward(grad_j vxc2))
+  for (int j = 0; j < 3; j++) {
+    k_mul<<<nb, kThreads, 0, ctx.stream>>>(ctx.d_grad + j * N, ctx.d_vx2, N, ctx.d_exc);
+    QBX_LAUNCHED(ctx);
+    vb_forward_real(ctx, ctx.d_exc, 1.0, ctx.d_vtmp_g);
+    k_mul_igx<<<blocks_for(ngv), kThreads, 0, ctx.stream>>>(
+        (const double2*)ctx.d_vtmp_g, ctx.d_gx_v + (size_t)j * ngv, ngv, 1.0,
+        (double2*)ctx.d_vtmp_g);
+    QBX_LAUNCHED(ctx);
+    vb_backward(ctx, ctx.d_vtmp_g, ctx.d_exc);
+    k_axpy<<<nb, kThreads, 0, ctx.stream>>>(ctx.d_vxc, ctx.d_exc, N);
+    QBX_LAUNCHED(ctx);
+  }
+}
+
+// ---------------------------------------------------- Hartree and local
+struct EpsEhF {
+  const double2* rhog; const double2* vion; const double2* rhops; const double* g2i;
+  double om_inv;
+  __device__ void operator()(size_t i, double* a) const {
+    const double2 r = make_double2(rhog[i].x * om_inv, rhog[i].y * om_inv);
+    const double2 v = vion[i];
+    const double f = (i == 0) ? 1.0 : 2.0;     // G=0 counted once
+    a[0] += f * (r.x * v.x + r.y * v.y);
+    const double2 t = make_double2(r.x + rhops[i].x, r.y + rhops[i].y);
+    a[1] += (t.x * t.x + t.y * t.y) * g2i[i];
+  }
+};
+
+__global__ void k_vlocal_g(const double2* __restrict__ rhog, const double2* __restrict__ vion,
+                           const double2* __restrict__ rhops, const double* __restrict__ g2i,
+                           int ng, double om_inv, double2* __restrict__ vloc,
+                           double2* __restrict__ rhogt) {
+  const double fpi = 4.0 * M_PI;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ng; i += gridDim.x * blockDim.x) {
+    const double2 t = make_double2(rhog[i].x * om_inv + rhops[i].x, rhog[i].y * om_inv + rhops[i].y);
+    rhogt[i] = t;
+    vloc[i] = make_double2(vion[i].x + fpi * t.x * g2i[i], vion[i].y + fpi * t.y * g2i[i]);
+  }
+}
+
+// EnergyFunctional::update_vhxc (src/EnergyFunctional.cpp:231-394) minus XC
+void launch_vhxc_gspace(Context& ctx) {
+  const int ngv = ctx.vb.ng;
+  const double om = ctx.vb.omega;
+  double s[2];
+  reduce<2>(ctx, EpsEhF{(const double2*)ctx.d_rhog, (const double2*)ctx.d_vion,
+                        (const double2*)ctx.d_rhops, ctx.d_g2i_v, 1.0 / om},
+            (size_t)ngv, s);
+  ctx.eps = s[0] * om;
+  ctx.ehart = om * 4.0 * M_PI * s[1];
+  k_vlocal_g<<<blocks_for(ngv), kThreads, 0, ctx.stream>>>(
+      (const double2*)ctx.d_rhog, (const double2*)ctx.d_vion, (const double2*)ctx.d_rhops,
+      ctx.d_g2i_v, ngv, 1.0 / om, (double2*)ctx.d_vtmp_g, (double2*)ctx.d_vtmp_g2);
+  QBX_LAUNCHED(ctx);
+  vb_backward(ctx, ctx.d_vtmp_g, ctx.d_vr);
+  k_axpy<<<blocks_for(ctx.N()), kThreads, 0, ctx.stream>>>(ctx.d_vr, ctx.d_vxc, ctx.N());
+  QBX_LAUNCHED(ctx);
+}
+
+// ------------------------------------------------- wavefunction sums
+struct EkinF {
+  const double2* c; const double* g2; const double* occ; int ngw;
+  __device__ void operator()(size_t i, double* a) const {
+    const int n = (int)(i / ngw), ig = (int)(i - (size_t)n * ngw);
+    const double2 v = c[i];
+    a[0] += occ[n] * (v.x * v.x + v.y * v.y) * g2[ig];
+  }
+};
+
+double launch_ekin(Context& ctx) {
+  double r;
+  reduce<1>(ctx, EkinF{(const double2*)ctx.d_c, ctx.d_g2_w, ctx.d_occ, ctx.wb.ng},
+            (size_t)ctx.wb.ng * ctx.nst, &r);
+  return r;
+}
+
+struct EigF {
+  const double2* c; const double2* hc; int ngw;
+  __device__ void operator()(size_t i, double* a) const {
+    const int n = (int)(i / ngw), ig = (int)(i - (size_t)n * ngw);
+    const double2 x = c[i], y = hc[i];
+    // 2 Re(conj(c) hc) on the half sphere, G=0 real part counted once
+    a[0] += (ig == 0) ? (2.0 * x.y * y.y + x.x * y.x) : 2.0 * (x.x * y.x + x.y * y.y);
+    (void)n;
+  }
+};
+
+double launch_eigsum(Context& ctx) {
+  double r;
+  reduce<1>(ctx, EigF{(const double2*)ctx.d_c, (const double2*)ctx.d_hc, ctx.wb.ng},
+            (size_t)ctx.wb.ng * ctx.nst, &r);
+  return r;
+}
+
+// Preconditioner::update (src/Preconditioner.cpp:88-143): per-band kinetic
+// energy ekin_n = (sum |c|^2 G^2) / (sum |c|^2 - |c_0|^2 / 2), one CTA per band.
+__global__ void k_prec(const double2* __restrict__ c, const double* __restrict__ g2, int ngw,
+                       double* __restrict__ ekin) {
+  __shared__ double sh[32];
+  const int n = blockIdx.x;
+  const double2* p = c + (size_t)n * ngw;
+  double sn = 0.0, se = 0.0;
+  for (int ig = threadIdx.x; ig < ngw; ig += blockDim.x) {
+    const double2 v = p[ig];
+    const double psi2 = v.x * v.x + v.y * v.y;
+    sn += psi2;
+    se += psi2 * g2[ig];
+  }
+  const double tn = block_sum(sn, sh);
+  const double te = block_sum(se, sh);
+  if (threadIdx.x == 0) {
+    const double c0 = p[0].x * p[0].x + p[0].y * p[0].y;
+    const double bn = 2.0 * (tn - 0.5 * c0), be = 2.0 * te;
+    double e = (0.5 * bn > 0.0) ? 0.5 * be / bn : 0.0;
+    if (e == 0.0) e = 1.0;
+    ekin[n] = e;
+  }
+}
+
+void launch_precond_update(Context& ctx) {
+  k_prec<<<ctx.nst, kThreads, 0, ctx.stream>>>((const double2*)ctx.d_c, ctx.d_g2_w, ctx.wb.ng,
+                                               ctx.d_prec);
+  QBX_LAUNCHED(ctx);
+}
+
+// dc = -K(G) r(G), K = 0.5/max(ekin_n, |G|^2/2) (Preconditioner::diag,
+// src/Preconditioner.cpp:49-85); dc overwrites the residual in hc.
+__global__ void k_precondition(double2* __restrict__ hc, const double* __restrict__ g2,
+                               const double* __restrict__ ekin, int ngw, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const int b = (int)(i / ngw), ig = (int)(i - (size_t)b * ngw);
+    const double e = 0.5 * g2[ig];
+    const double en = ekin[b];
+    const double k = (e < en) ? 0.5 / en : 0.5 / e;
+    const double2 r = hc[i];
+    hc[i] = make_double2(-k * r.x, -k * r.y);
+  }
+}
+
+struct AndersonF {
+  const double2* f; const double2* fl; int ngw;
+  __device__ void operator()(size_t i, double* a) const {
+    const int ig = (int)(i % (size_t)ngw);
+    const double2 x = f[i], y = fl[i];
+    const double dx = x.x - y.x, dy = x.y - y.y;
+    const double w = (ig == 0) ? 1.0 : 2.0;
+    a[0] += w * (x.x * dx + x.y * dy);
+    a[1] += w * (dx * dx + dy * dy);
+  }
+};
+
+__global__ void k_psda_update(double2* __restrict__ c, double2* __restrict__ c_last,
+                              double2* __restrict__ dc_last, const double2* __restrict__ dc,
+                              size_t n, double theta, int extrapolate) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const double2 x = c[i], f = dc[i];
+    double2 nc;
+    if (extrapolate) {
+      const double2 xl = c_last[i], fl = dc_last[i];
+      nc.x = x.x + theta * (x.x - xl.x) + f.x + theta * (f.x - fl.x);
+      nc.y = x.y + theta * (x.y - xl.y) + f.y + theta * (f.y - fl.y);
+    } else {
+      nc.x = x.x + f.x;
+      nc.y = x.y + f.y;
+    }
+    c[i] = nc;
+    c_last[i] = x;
+    dc_last[i] = f;
+  }
+}
+
+// PSDAWavefunctionStepper::update after the residual (src/PSDAWavefunction
+// Stepper.cpp:82-212): precondition, Anderson theta, step.
+void launch_psda_elementwise(Context& ctx) {
+  const size_t n = (size_t)ctx.wb.ng * ctx.nst;
+  k_precondition<<<blocks_for(n), kThreads, 0, ctx.stream>>>((double2*)ctx.d_hc, ctx.d_g2_w,
+                                                              ctx.d_prec, ctx.wb.ng, n);
+  QBX_LAUNCHED(ctx);
+  double theta = 0.0;
+  if (ctx.extrapolate) {
+    double ab[2];
+    reduce<2>(ctx, AndersonF{(const double2*)ctx.d_hc, (const double2*)ctx.d_dc_last, ctx.wb.ng},
+              n, ab);
+    if (ab[1] != 0.0) theta = -ab[0] / ab[1];
+    if (theta < -1.0) theta = 0.0;
+    theta = std::min(2.0, theta);
+  }
+  ctx.theta = theta;
+  k_psda_update<<<blocks_for(n), kThreads, 0, ctx.stream>>>(
+      (double2*)ctx.d_c, (double2*)ctx.d_c_last, (double2*)ctx.d_dc_last,
+      (const double2*)ctx.d_hc, n, theta, ctx.extrapolate ? 1 : 0);
+  QBX_LAUNCHED(ctx);
+}
+
+__global__ void k_cleanup(double2* c, int ngw, int nst) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n < nst) c[(size_t)n * ngw].y = 0.0;
+}
+
+// SlaterDet::cleanup (src/SlaterDet.cpp:1341-1356): Im c(G=0) = 0
+void launch_cleanup(Context& ctx, double* c) {
+  k_cleanup<<<(ctx.nst + 255) / 256, 256, 0, ctx.stream>>>((double2*)c, ctx.wb.ng, ctx.nst);
+  QBX_LAUNCHED(ctx);
+}
+
+// m(i,j) += alpha x_i y_j  (column-major, ld ldm)
+__global__ void k_rank1(double* m, int ldm, const double* x, int ldx, const double* y, int ldy,
+                        int nrow, int ncol, double alpha, int lower_only) {
+  const size_t n = (size_t)nrow * ncol;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(t % nrow), j = (int)(t / nrow);
+    if (lower_only && i < j) continue;
+    m[i + (size_t)j * ldm] += alpha * x[(size_t)i * ldx] * y[(size_t)j * ldy];
+  }
+}
+
+void launch_rank1_fix(Context& ctx, double* m, int ldm, const double* x, int ldx,
+                      const double* y, int ldy, int nrow, int ncol, double alpha,
+                      bool lower_only) {
+  k_rank1<<<blocks_for((size_t)nrow * ncol), kThreads, 0, ctx.stream>>>(
+      m, ldm, x, ldx, y, ldy, nrow, ncol, alpha, lower_only ? 1 : 0);
+  QBX_LAUNCHED(ctx);
+}
+
+// ------------------------------------------------------------ nonlocal
+struct EnlF {
+  double* f; const double* dfac; const double* occ; int np; double om_inv;
+  __device__ void operator()(size_t i, double* a) const {
+    const int p = (int)(i % np), n = (int)(i / np);
+    const double F = f[i];
+    const double DF = dfac[p] * F;
+    a[0] += occ[n] * F * DF * om_inv;
+  }
+};
+
+__global__ void k_fnl_scale(double* f, const double* dfac, int np, size_t n, double om_inv) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    f[i] *= dfac[i % np] * om_inv;
+}
+
+// E_nl and fnl <- D F / Omega (src/NonLocalPotential.cpp:1469-1597)
+double launch_enl(Context& ctx) {
+  const size_t n = (size_t)ctx.nproj * ctx.nst;
+  double e;
+  reduce<1>(ctx, EnlF{ctx.d_fnl, ctx.d_pdfac, ctx.d_occ, ctx.nproj, 1.0 / ctx.wb.omega}, n, &e);
+  k_fnl_scale<<<blocks_for(n), kThreads, 0, ctx.stream>>>(ctx.d_fnl, ctx.d_pdfac, ctx.nproj, n,
+                                                          1.0 / ctx.wb.omega);
+  QBX_LAUNCHED(ctx);
+  return e;
+}
+
+// c'(G) = G_j (i c(G)) for the force projections dF_j = 2 A^T c'
+__global__ void k_igj_c(const double2* __restrict__ c, const double* __restrict__ gxj, int ngw,
+                        size_t n, double2* __restrict__ out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const double g = gxj[i % ngw];
+    const double2 v = c[i];
+    out[i] = make_double2(-g * v.y, g * v.x);
+  }
+}
+
+// fion[atom, j] -= 2 sum_n occ_n fnl(p,n) dF(p,n) over the atom's projectors
+__global__ void k_nl_force(const double* __restrict__ fnl, const double* __restrict__ dfnl,
+                           const double* __restrict__ occ, const int* __restrict__ patom, int np,
+                           int nst, int j, double* __restrict__ fion) {
+  __shared__ double sh[32];
+  const int p = blockIdx.x;
+  double s = 0.0;
+  for (int n = threadIdx.x; n < nst; n += blockDim.x)
+    s += occ[n] * fnl[p + (size_t)n * np] * dfnl[p + (size_t)n * np];
+  const double t = block_sum(s, sh);
+  if (threadIdx.x == 0) atomicAdd(&fion[3 * patom[p] + j], -2.0 * t);
+}
+
+void launch_nl_forces(Context& ctx, double* fion) {
+  const int ngw = ctx.wb.ng;
+  const size_t n = (size_t)ngw * ctx.nst;
+  const double two = 2.0, zero = 0.0;
+  for (int j = 0; j < 3; j++) {
+    k_igj_c<<<blocks_for(n), kThreads, 0, ctx.stream>>>((const double2*)ctx.d_c,
+                                                        ctx.d_gx_w + (size_t)j * ngw, ngw, n,
+                                                        (double2*)ctx.d_ctmp);
+    QBX_LAUNCHED(ctx);
+    QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_T, CUBLAS_OP_N, ctx.nproj, ctx.nst, 2 * ngw, &two,
+                         ctx.d_anl, 2 * ngw, ctx.d_ctmp, 2 * ngw, &zero, ctx.d_dfnl, ctx.nproj));
+    k_nl_force<<<ctx.nproj, kThreads, 0, ctx.stream>>>(ctx.d_fnl, ctx.d_dfnl, ctx.d_occ,
+                                                       ctx.d_patom, ctx.nproj, ctx.nst, j, fion);
+    QBX_LAUNCHED(ctx);
+  }
+}
+
+// Forces of the local pseudopotential and the Hartree term of the Gaussian
+// pseudocharges (src/EnergyFunctional.cpp:841-930), one CTA per atom.
+__global__ void k_local_force(const double* __restrict__ gx, const double2* __restrict__ rhogt,
+                              const double2* __restrict__ rhog, const double* __restrict__ vps,
+                              const double* __restrict__ rhops, const double* __restrict__ g2i,
+                              int ng, double om_inv, const double* __restrict__ tau, double fac,
+                              int atom0, double* __restrict__ fion) {
+  __shared__ double sh[32];
+  const int ia = blockIdx.x;
+  const double tx = tau[3 * ia], ty = tau[3 * ia + 1], tz = tau[3 * ia + 2];
+  const double fpi = 4.0 * M_PI;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  for (int i = threadIdx.x; i < ng; i += blockDim.x) {
+    const double x = gx[i], y = gx[ng + i], z = gx[2 * ng + i];
+    const double2 rt = rhogt[i];
+    const double2 re = make_double2(rhog[i].x * om_inv, rhog[i].y * om_inv);
+    const double t = fpi * rhops[i] * g2i[i];
+    // vtemp = t conj(rhogt) + vps conj(rhoelg)
+    const double vr = t * rt.x + vps[i] * re.x;
+    const double vi = -t * rt.y - vps[i] * re.y;
+    double sn, cs;
+    sincos(x * tx + y * ty + z * tz, &sn, &cs);
+    // exp(-i G.tau) = cs - i sn
+    const double tmp = cs * vi + (-sn) * vr;
+    s0 += tmp * x; s1 += tmp * y; s2 += tmp * z;
+  }
+  const double a0 = block_sum(s0, sh);
+  const double a1 = block_sum(s1, sh);
+  const double a2 = block_sum(s2, sh);
+  if (threadIdx.x == 0) {
+    fion[3 * (atom0 + ia)] += fac * a0;
+    fion[3 * (atom0 + ia) + 1] += fac * a1;
+    fion[3 * (atom0 + ia) + 2] += fac * a2;
+  }
+}
+
+void launch_local_forces(Context& ctx, double* fion) {
+  const int ngv = ctx.vb.ng;
+  int atom0 = 0;
+  double* d_tau = nullptr;
+  for (size_t is = 0; is < ctx.species.size(); is++) {
+    const int na = (int)ctx.tau[is].size() / 3;
+    if (na == 0) continue;
+    d_tau = dupload(ctx.tau[is]);
+    k_local_force<<<na, kThreads, 0, ctx.stream>>>(
+        ctx.d_gx_v, (const double2*)ctx.d_vtmp_g2, (const double2*)ctx.d_rhog,
+        ctx.d_vps + is * (size_t)ngv, ctx.d_rhops_sp + is * (size_t)ngv, ctx.d_g2i_v, ngv,
+        1.0 / ctx.vb.omega, d_tau, -2.0 * ctx.vb.omega, atom0, fion);
+    QBX_LAUNCHED(ctx);
+    QBX_CUDA(cudaStreamSynchronize(ctx.stream));
+    dfree(d_tau);
+    atom0 += na;
+  }
+}
+
+// ---------------------------------------------------- small n x n helpers
+__global__ void k_identity_axpy(double* t, const double* q, int n, double alpha) {
+  const size_t nn = (size_t)n * n;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nn;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(i % n), c = (int)(i / n);
+    t[i] = (r == c ? 1.0 : 0.0) + (alpha != 0.0 ? alpha * q[i] : 0.0);
+  }
+}
+void launch_identity_axpy(Context& ctx, double* t, const double* q, int n, double alpha) {
+  k_identity_axpy<<<blocks_for((size_t)n * n), kThreads, 0, ctx.stream>>>(t, q, n, alpha);
+  QBX_LAUNCHED(ctx);
+}
+
+__global__ void k_symmetrize_lower(double* q, int n) {
+  const size_t nn = (size_t)n * n;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nn;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(i % n), c = (int)(i / n);
+    if (r < c) q[i] = q[c + (size_t)r * n];
+  }
+}
+void launch_symmetrize_lower(Context& ctx, double* q, int n) {
+  k_symmetrize_lower<<<blocks_for((size_t)n * n), kThreads, 0, ctx.stream>>>(q, n);
+  QBX_LAUNCHED(ctx);
+}
+
+__global__ void k_avg(double* x, const double* t, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    x[i] = 0.5 * (x[i] + t[i]);
+}
+void launch_avg_transpose(Context& ctx, double* x, const double* t, int n) {
+  k_avg<<<blocks_for((size_t)n * n), kThreads, 0, ctx.stream>>>(x, t, (size_t)n * n);
+  QBX_LAUNCHED(ctx);
+}
+
+struct Sq {
+  const double* q;
+  __device__ void operator()(size_t i, double* a) const { a[0] += q[i] * q[i]; }
+};
+double launch_frob(Context& ctx, const double* q, int n) {
+  double r;
+  reduce<1>(ctx, Sq{q}, (size_t)n * n, &r);
+  return sqrt(r);
+}
+
+// ------------------------------------------------------ per-geometry setup
+// S(G) = sum_a exp(-i G.tau_a) on the density sphere
+__global__ void k_sfac(const double* __restrict__ gx, int ng, const double* __restrict__ tau,
+                       int na, double2* __restrict__ s) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ng; i += gridDim.x * blockDim.x) {
+    const double x = gx[i], y = gx[ng + i], z = gx[2 * ng + i];
+    double re = 0.0, im = 0.0;
+    for (int a = 0; a < na; a++) {
+      double sn, cs;
+      sincos(x * tau[3 * a] + y * tau[3 * a + 1] + z * tau[3 * a + 2], &sn, &cs);
+      re += cs;
+      im -= sn;
+    }
+    s[i] = make_double2(re, im);
+  }
+}
+
+__global__ void k_vion(const double2* __restrict__ s, const double* __restrict__ vps,
+                       const double* __restrict__ rhops, int ng, double2* __restrict__ vion,
+                       double2* __restrict__ rhopst) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ng; i += gridDim.x * blockDim.x) {
+    const double2 v = s[i];
+    vion[i].x += v.x * vps[i];
+    vion[i].y += v.y * vps[i];
+    rhopst[i].x += v.x * rhops[i];
+    rhopst[i].y += v.y * rhops[i];
+  }
+}
+
+// anl(G) = twnl(G) (-i)^l exp(-i G.tau) for one projector column per atom
+__global__ void k_anl(const double* __restrict__ gx, int ngw, const double* __restrict__ twnl,
+                      const double* __restrict__ tau, int na, int l, double2* __restrict__ anl) {
+  const int ia = blockIdx.y;
+  const double tx = tau[3 * ia], ty = tau[3 * ia + 1], tz = tau[3 * ia + 2];
+  double2* out = anl + (size_t)ia * ngw;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ngw; i += gridDim.x * blockDim.x) {
+    double sn, cs;
+    sincos(gx[i] * tx + gx[ngw + i] * ty + gx[2 * ngw + i] * tz, &sn, &cs);
+    const double t = twnl[i];
+    // exp(-i G.tau) = (cs, -sn); times -i for l = 1: (-sn, -cs)
+    out[i] = (l == 0) ? make_double2(t * cs, -t * sn) : make_double2(-t * sn, -t * cs);
+  }
+}
+
+void launch_setup_atoms(Context& ctx) {
+  const Basis& vb = ctx.vb;
+  const Basis& wb = ctx.wb;
+  const int ngv = vb.ng, ngw = wb.ng;
+  const int nsp = (int)ctx.species.size();
+  QBX_CUDA(cudaMemsetAsync(ctx.d_vion, 0, 2 * sizeof(double) * ngv, ctx.stream));
+  QBX_CUDA(cudaMemsetAsync(ctx.d_rhops, 0, 2 * sizeof(double) * ngv, ctx.stream));
+  int col = 0;
+  for (int is = 0; is < nsp; is++) {
+    const SpeciesTables& sp = ctx.species[is];
+    const int na = (int)ctx.tau[is].size() / 3;
+    double* d_tau = dupload(ctx.tau[is]);
+    double2* sf = (double2*)ctx.d_sfac + (size_t)is * ngv;
+    k_sfac<<<blocks_for(ngv), kThreads, 0, ctx.stream>>>(ctx.d_gx_v, ngv, d_tau, na, sf);
+    QBX_LAUNCHED(ctx);
+    k_vion<<<blocks_for(ngv), kThreads, 0, ctx.stream>>>(sf, ctx.d_vps + (size_t)is * ngv,
+                                                         ctx.d_rhops_sp + (size_t)is * ngv, ngv,
+                                                         (double2*)ctx.d_vion,
+                                                         (double2*)ctx.d_rhops);
+    QBX_LAUNCHED(ctx);
+    // projectors: twnl on the host (spline of V_nl times Y_lm), phases here
+    const double s14pi = std::sqrt(1.0 / (4.0 * M_PI));
+    const double s34pi = std::sqrt(3.0 / (4.0 * M_PI));
+    for (size_t iop = 0; iop < sp.proj_l.size(); iop++) {
+      const int l = sp.proj_l[iop];
+      std::vector<double> v(ngw);
+      for (int ig = 0; ig < ngw; ig++) {
+        double val, dv;
+        sp.dvnlg((int)iop, wb.g[ig], val, dv);
+        v[ig] = val;
+      }
+      const int nm = 2 * l + 1;
+      for (int m = 0; m < nm; m++) {
+        std::vector<double> tw(ngw);
+        for (int ig = 0; ig < ngw; ig++) {
+          if (l == 0) tw[ig] = s14pi * v[ig];
+          else tw[ig] = s34pi * wb.gx[(size_t)m * ngw + ig] * wb.gi[ig] * v[ig];
+        }
+        double* d_tw = dupload(tw);
+        dim3 grid((ngw + kThreads - 1) / kThreads, na);
+        k_anl<<<grid, kThreads, 0, ctx.stream>>>(ctx.d_gx_w, ngw, d_tw, d_tau, na, l,
+                                                  (double2*)ctx.d_anl + (size_t)col * ngw);
+        QBX_LAUNCHED(ctx);
+        QBX_CUDA(cudaStreamSynchronize(ctx.stream));
+        dfree(d_tw);
+        col += na;
+      }
+    }
+    QBX_CUDA(cudaStreamSynchronize(ctx.stream));
+    dfree(d_tau);
+  }
+  QBX_REQUIRE(col == ctx.nproj, 30, "projector count mismatch");
+}
+
+}  // namespace qbx

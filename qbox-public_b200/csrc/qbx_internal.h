@@ -1,0 +1,359 @@
+// Internal declarations of the B200 Kohn-Sham electronic-step library.
+//
+// One qbx_context owns one Gamma-point SlaterDet on one GPU: the plane-wave
+// basis and its staged-FFT stick geometry, species G-space tables, the
+// structure factors and projectors of the current atomic positions, and the
+// device-resident wavefunctions C, H*C and the stepper history.  Host code
+// here builds geometry and tables (the role of the reference's Basis,
+// BasisMapping and Species classes); every per-step operation runs on the GPU.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cublas_v2.h>
+#include <cusolverDn.h>
+
+#include <complex>
+#include <string>
+#include <vector>
+
+namespace qbx {
+
+// ------------------------------------------------------------------ errors
+struct Error {
+  int code;
+  std::string msg;
+};
+
+#define QBX_CUDA(call)                                                       \
+  do {                                                                       \
+    cudaError_t e_ = (call);                                                 \
+    if (e_ != cudaSuccess)                                                   \
+      throw ::qbx::Error{2, std::string(#call) + ": " + cudaGetErrorString(e_)}; \
+  } while (0)
+#define QBX_BLAS(call)                                                       \
+  do {                                                                       \
+    cublasStatus_t s_ = (call);                                              \
+    if (s_ != CUBLAS_STATUS_SUCCESS)                                         \
+      throw ::qbx::Error{3, std::string(#call) + " failed: " + std::to_string((int)s_)}; \
+  } while (0)
+#define QBX_SOLVER(call)                                                     \
+  do {                                                                       \
+    cusolverStatus_t s_ = (call);                                            \
+    if (s_ != CUSOLVER_STATUS_SUCCESS)                                       \
+      throw ::qbx::Error{4, std::string(#call) + " failed: " + std::to_string((int)s_)}; \
+  } while (0)
+#define QBX_REQUIRE(cond, code, text)                                        \
+  do { if (!(cond)) throw ::qbx::Error{code, text}; } while (0)
+// after every kernel launch of this library: check it and count it
+#define QBX_LAUNCHED(ctx)                                                    \
+  do { QBX_CUDA(cudaGetLastError()); (ctx).nlaunch++; } while (0)
+
+// ------------------------------------------------------------ FFT geometry
+// A mixed-radix plan for one 1-D length (radices 2,3,4,5,7,8,11).
+struct RadixPlan {
+  int n = 0;
+  int nstage = 0;
+  int radix[12] = {0};
+};
+RadixPlan make_plan(int n);
+
+// Half-sphere basis on the dense grid, ordered rod by rod: rods are the
+// z-columns (h,k) of the half sphere in sorted (h,k) order, rod (0,0) first;
+// coefficients of one rod are contiguous with l ascending.  Sticks are the
+// columns of the full grid that carry data: rod 0 -> stick 0 (holds +l and
+// -l), rod r>0 -> stick 2r-1 at (h,k) and stick 2r at (-h,-k).
+struct Basis {
+  double cell[9];          // rows a0,a1,a2
+  double recip[9];         // rows b0,b1,b2 (2 pi inverse transpose)
+  double omega = 0;
+  double ecut = 0;         // Hartree
+  int ng = 0;
+  std::vector<int> hkl;    // 3*ng, internal order
+  std::vector<double> gx;  // 3*ng (x block, y block, z block)
+  std::vector<double> g2, g, gi, g2i;
+  int g0 = 0;              // index of G=0 (always 0 in the internal order)
+  // rods
+  int nrods = 0;
+  std::vector<int> rod_h, rod_k, rod_lmin, rod_size, rod_first;
+  // grid
+  int n0 = 0, n1 = 0, n2 = 0;
+  int nvec = 0;                           // sticks = 2*nrods-1
+  std::vector<int> stick_x, stick_y;      // grid column of each stick
+  int ncol = 0;                           // distinct x columns of sticks
+  std::vector<int> stick_col;             // compact column of each stick
+  std::vector<int> col_x;                 // grid x of each compact column
+  std::vector<int> ip, im;                // grid index of +G and -G
+};
+
+void build_basis(Basis& b, const double cell[9], double ecut);
+void set_grid(Basis& b, int n0, int n1, int n2);
+bool factorizable(int n);
+int fft_size(const double cell[9], double ecut, int dir);
+void dense_grid(const double cell[9], double ecut_wf, int np[3]);
+
+// Device copy of the stick geometry used by the staged FFT kernels.
+struct DeviceSticks {
+  int n0, n1, n2, nrods, nvec, ncol;
+  int* rod_first;    // nrods
+  int* rod_lmin;     // nrods
+  int* rod_size;     // nrods
+  int* stick_y;      // nvec
+  int* stick_col;    // nvec
+  int* col_x;        // ncol
+  int* ip;           // ng
+  int* im;           // ng
+  RadixPlan px, py, pz;
+};
+
+// -------------------------------------------------------------- species
+// G-space tables of one species, as the reference's Species holds them after
+// initialize() (cubic splines of V_loc(G) and of each projector on a uniform
+// G mesh).
+struct SpeciesTables {
+  double zval = 0, rcps = 1.5;
+  int ndft = 0;
+  std::vector<double> gspl, vlocg, vlocg2;
+  std::vector<int> proj_l;                    // one entry per radial projector
+  std::vector<double> proj_d;                 // D matrix (diagonal, per l)
+  std::vector<std::vector<double>> vnlg, vnlg2;
+  int nlm() const {
+    int n = 0;
+    for (int l : proj_l) n += 2 * l + 1;
+    return n;
+  }
+  double eself() const;
+  void dvlocg(double g, double& v, double& dv) const;
+  void dvnlg(int iop, double g, double& v, double& dv) const;
+  double rhopsg(double g) const;
+};
+void species_from_radial(SpeciesTables& s, int zval, double mesh_spacing,
+                         int nmesh, const double* vlocal, int nproj,
+                         const int* proj_l, const double* proj,
+                         const double* proj_d);
+
+double esr_energy_forces(const double cell[9],
+                         const std::vector<std::vector<double>>& tau,
+                         const std::vector<double>& zv, double rcps,
+                         std::vector<std::vector<double>>& f);
+
+// ---------------------------------------------------------------- context
+enum Precision { FP64 = 0, MIXED = 1 };
+
+// CUDA-event timing of tagged regions on the context's stream.  When
+// enabled, each region records an event pair; qbx_profile_get() resolves the
+// pairs into per-tag total milliseconds and counts.
+struct Profiler {
+  bool on = false;
+  std::vector<std::string> names;
+  std::vector<double> ms;
+  std::vector<long> count;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+  std::vector<cudaEvent_t> pool;
+  int tag(const std::string& n) {
+    for (size_t i = 0; i < names.size(); i++)
+      if (names[i] == n) return (int)i;
+    names.push_back(n); ms.push_back(0.0); count.push_back(0);
+    return (int)names.size() - 1;
+  }
+  cudaEvent_t get() {
+    if (pool.empty()) {
+      cudaEvent_t e;
+      QBX_CUDA(cudaEventCreate(&e));
+      return e;
+    }
+    cudaEvent_t e = pool.back();
+    pool.pop_back();
+    return e;
+  }
+  void resolve() {
+    for (auto& p : pending) {
+      float t = 0.f;
+      QBX_CUDA(cudaEventElapsedTime(&t, p.second.first, p.second.second));
+      ms[p.first] += t;
+      count[p.first] += 1;
+      pool.push_back(p.second.first);
+      pool.push_back(p.second.second);
+    }
+    pending.clear();
+  }
+  void reset() {
+    resolve();
+    for (auto& m : ms) m = 0.0;
+    for (auto& c : count) c = 0;
+  }
+};
+
+struct Context {
+  int device = 0;
+  int precision = FP64;
+  std::string last_error;
+  cudaStream_t stream = nullptr;
+  cublasHandle_t blas = nullptr;
+  cusolverDnHandle_t solver = nullptr;
+  bool have_cell = false;
+
+  Basis wb, vb;                 // wavefunction basis, density basis (4 ecut)
+  DeviceSticks dws{}, dvs{};
+  std::string xc = "LDA";
+
+  // species and atoms
+  std::vector<SpeciesTables> species;
+  std::vector<std::vector<double>> tau;   // per species, 3*na
+  double esr = 0, eself = 0;
+  std::vector<std::vector<double>> fion_esr;
+  int nproj = 0;                // total projector columns (sum nlm*na)
+  std::vector<int> proj_species, proj_atom, proj_lm;   // per column
+  std::vector<double> proj_dfac;                       // D per column
+
+  // wavefunctions
+  int nst = 0;
+  std::vector<double> occ;
+  bool extrapolate = false;
+
+  // device buffers (double unless noted)
+  double* d_gx_w = nullptr;     // 3*ngw
+  double* d_g2_w = nullptr;     // ngw
+  double* d_gx_v = nullptr;     // 3*ngv
+  double* d_g2i_v = nullptr;    // ngv
+  double* d_c = nullptr;        // 2*ngw*nst  (complex, band-major)
+  double* d_hc = nullptr;
+  double* d_c_last = nullptr;
+  double* d_dc_last = nullptr;
+  double* d_ctmp = nullptr;     // scratch copy of C
+  double* d_occ = nullptr;      // nst
+  double* d_anl = nullptr;      // 2*ngw*nproj  (complex projectors x phase)
+  double* d_fnl = nullptr;      // nproj*nst
+  double* d_dfnl = nullptr;     // nproj*nst
+  double* d_pdfac = nullptr;    // nproj
+  int* d_patom = nullptr;       // nproj (global atom index)
+  double* d_rhor = nullptr;     // N
+  double* d_vr = nullptr;       // N
+  double* d_vxc = nullptr;      // N
+  double* d_exc = nullptr;      // N (energy density scratch)
+  double* d_vx2 = nullptr;      // N (PBE vxc2)
+  double* d_grad = nullptr;     // 3N
+  double* d_rhog = nullptr;     // 2*ngv (complex)
+  double* d_vion = nullptr;     // 2*ngv
+  double* d_rhops = nullptr;    // 2*ngv (sum of S*rhops)
+  double* d_vtmp_g = nullptr;   // 2*ngv scratch
+  double* d_vtmp_g2 = nullptr;  // 2*ngv scratch
+  double* d_sfac = nullptr;     // 2*ngv*nsp
+  double* d_vps = nullptr;      // ngv*nsp
+  double* d_rhops_sp = nullptr; // ngv*nsp
+  void* d_grid = nullptr;       // N complex (double2) scratch for vbasis FFTs
+  void* d_zbuf = nullptr;       // staged FFT stick buffer
+  size_t zbuf_bytes = 0;
+  int pair_batch = 0;
+  double* d_nn = nullptr;       // nst*nst matrices (4 of them)
+  double* d_nn2 = nullptr;
+  double* d_nn3 = nullptr;
+  double* d_nn4 = nullptr;
+  int* d_ipiv = nullptr;
+  int* d_info = nullptr;
+  double* d_solver_work = nullptr;
+  int solver_lwork = 0;
+  double* d_red = nullptr;      // reduction partials
+  double* d_scalars = nullptr;  // small device scalars
+  double* d_prec = nullptr;     // nst ekin per band
+  double* d_fion = nullptr;     // 3*natoms
+
+  // energies of the last evaluation
+  double ekin = 0, eps = 0, enl = 0, ehart = 0, exc = 0, ecoul = 0,
+         etotal = 0, total_charge = 0, eigsum = 0, theta = 0;
+  std::vector<double> fion;     // 3*natoms, species-major like the reference
+
+  long nlaunch = 0;              // kernels of this library launched so far
+  Profiler prof;
+
+  size_t N() const { return (size_t)vb.n0 * vb.n1 * vb.n2; }
+};
+
+// Records the tagged region [construction, destruction) on ctx.stream when
+// the profiler is on.
+struct ProfScope {
+  Context& c;
+  int t = -1;
+  cudaEvent_t a = nullptr, b = nullptr;
+  ProfScope(Context& ctx, const char* name) : c(ctx) {
+    if (!c.prof.on) return;
+    t = c.prof.tag(name);
+    a = c.prof.get();
+    b = c.prof.get();
+    QBX_CUDA(cudaEventRecord(a, c.stream));
+  }
+  ~ProfScope() {
+    if (t < 0) return;
+    if (cudaEventRecord(b, c.stream) == cudaSuccess)
+      c.prof.pending.push_back({t, {a, b}});
+  }
+};
+
+// device memory helpers
+template <typename T>
+inline T* dalloc(size_t n) {
+  if (n == 0) return nullptr;
+  void* p = nullptr;
+  QBX_CUDA(cudaMalloc(&p, n * sizeof(T)));
+  return (T*)p;
+}
+template <typename T>
+inline void dfree(T*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+// Host-to-device copy that has fully landed when it returns.  Kernels run on
+// a non-blocking stream, which does not order itself after the legacy
+// stream's copies, and a pageable cudaMemcpy may return before its DMA ends;
+// the device synchronisation closes both gaps.  Setup paths only.
+inline void h2d_sync(void* dst, const void* src, size_t bytes) {
+  if (bytes == 0) return;
+  QBX_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
+  QBX_CUDA(cudaDeviceSynchronize());
+}
+template <typename T>
+inline T* dupload(const std::vector<T>& v) {
+  T* p = dalloc<T>(v.size());
+  h2d_sync(p, v.data(), v.size() * sizeof(T));
+  return p;
+}
+
+// ---------------------------------------------------- kernel launchers
+// staged wavefunction FFTs (fft.cu)
+void upload_sticks(DeviceSticks& d, const Basis& b);
+void free_sticks(DeviceSticks& d);
+// rho(r) += sum_n occ_n/omega |psi_n(r)|^2 over all bands of c
+void launch_density(Context& ctx, const double* c, double* rho);
+// hc = 1/2 |G|^2 c + FFT_fwd(v FFT_bwd(c))  (hc overwritten)
+void launch_vpsi(Context& ctx, const double* c, const double* v, double* hc);
+// vbasis transforms on the full grid
+void vb_backward(Context& ctx, const double* coef, double* real_out);   // real part
+void vb_forward_real(Context& ctx, const double* f, double scale, double* coef);
+// wavefunction-basis single transforms through the full-grid path (tests)
+void wb_backward_pair(Context& ctx, const double* c1, const double* c2, double* grid_out);
+
+// occ_n / Omega per band (device), used by the density kernels
+double* density_weights(Context& ctx);
+
+// pointwise kernels (kernels.cu)
+double dsum(Context& ctx, const double* x, size_t n);
+void launch_xc(Context& ctx);                  // fills d_vxc, ctx.exc
+void launch_vhxc_gspace(Context& ctx);         // eps, ehart, vlocal_g
+void launch_setup_atoms(Context& ctx);         // sfac, vion, rhops, anl
+double launch_ekin(Context& ctx);
+double launch_eigsum(Context& ctx);
+void launch_precond_update(Context& ctx);      // d_prec
+void launch_psda_elementwise(Context& ctx);    // residual->step, sets theta
+void launch_cleanup(Context& ctx, double* c);  // Im c(G=0) = 0
+void launch_rank1_fix(Context& ctx, double* m, int ldm, const double* x, int ldx,
+                      const double* y, int ldy, int nrow, int ncol, double alpha,
+                      bool lower_only);
+double launch_enl(Context& ctx);                // enl; fnl <- DF/omega
+void launch_local_forces(Context& ctx, double* fion);
+void launch_nl_forces(Context& ctx, double* fion);
+void launch_identity_axpy(Context& ctx, double* t, const double* q, int n,
+                          double alpha);       // t = I + alpha*q
+void launch_symmetrize_lower(Context& ctx, double* q, int n);
+void launch_avg_transpose(Context& ctx, double* x, const double* t, int n);
+double launch_frob(Context& ctx, const double* q, int n);
+
+}  // namespace qbx

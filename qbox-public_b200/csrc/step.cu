@@ -1,0 +1,196 @@
+// The electronic step on one GPU: ChargeDensity::update_density,
+// EnergyFunctional::update_vhxc / energy, the PSDA stepper and
+// SlaterDet::gram / ortho_align, orchestrated from the host over the
+// kernels of fft.cu and kernels.cu and the dense linear algebra of cuBLAS and
+// cuSOLVER (FP64).
+//
+// Matrices follow the reference's "DoubleMatrix proxy" view of a Gamma-point
+// SlaterDet: C (ngw complex rows x nst columns, column-major) is read as a
+// real 2*ngw x nst matrix, so C^T C counts +G and -G once each except the
+// G=0 row, which the rank-1 corrections below remove
+// (src/SlaterDet.cpp:480-534,768-876).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "qbx_internal.h"
+
+namespace qbx {
+
+static void require_potrf(Context& ctx, const char* what) {
+  int info = 0;
+  QBX_CUDA(cudaMemcpyAsync(&info, ctx.d_info, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+  QBX_CUDA(cudaStreamSynchronize(ctx.stream));
+  QBX_REQUIRE(info == 0, 40, std::string(what) + ": matrix not positive definite (info=" +
+                                 std::to_string(info) + ")");
+}
+
+// S = 2 C^T C - c0 c0^T, lower triangle, then S = L L^T in place
+static void overlap_cholesky(Context& ctx, const double* c, double* S) {
+  ProfScope ps(ctx, "overlap_cholesky");
+  const int n = ctx.nst, K = 2 * ctx.wb.ng;
+  const double two = 2.0, zero = 0.0;
+  QBX_BLAS(cublasDsyrk(ctx.blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, n, K, &two, c, K, &zero, S, n));
+  launch_rank1_fix(ctx, S, n, c, K, c, K, n, n, -1.0, true);
+  QBX_SOLVER(cusolverDnDpotrf(ctx.solver, CUBLAS_FILL_MODE_LOWER, n, S, n, ctx.d_solver_work,
+                              ctx.solver_lwork, ctx.d_info));
+  require_potrf(ctx, "Cholesky of the overlap matrix");
+}
+
+// SlaterDet::gram (src/SlaterDet.cpp:480-534): C <- C L^-T
+void gram(Context& ctx) {
+  launch_cleanup(ctx, ctx.d_c);
+  overlap_cholesky(ctx, ctx.d_c, ctx.d_nn);
+  const double one = 1.0;
+  QBX_BLAS(cublasDtrsm(ctx.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T,
+                       CUBLAS_DIAG_NON_UNIT, 2 * ctx.wb.ng, ctx.nst, &one, ctx.d_nn, ctx.nst,
+                       ctx.d_c, 2 * ctx.wb.ng));
+}
+
+// DoubleMatrix::polar (src/Matrix.cpp:2446-2540) on x (n x n, in place):
+// Bjorck-Bowie steps x <- x (I + q/2 (I + 3q/4)), q = I - x^T x, while
+// ||q||_F < 1, Higham steps x <- (x + x^-T)/2 otherwise; stops after the
+// step in which ||q||_F <= tol.
+static void polar(Context& ctx, double* x, double tol, int maxiter) {
+  ProfScope ps(ctx, "polar");
+  const int n = ctx.nst;
+  double* q = ctx.d_nn3;
+  double* t = ctx.d_nn4;
+  double* qt = ctx.d_nn4 + (size_t)n * n;
+  double* xp = ctx.d_nn4 + 2 * (size_t)n * n;
+  const double one = 1.0, zero = 0.0, mone = -1.0;
+  for (int iter = 0; iter < maxiter; iter++) {
+    launch_identity_axpy(ctx, q, q, n, 0.0);   // q = I
+    QBX_BLAS(cublasDsyrk(ctx.blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, n, n, &mone, x, n, &one, q, n));
+    launch_symmetrize_lower(ctx, q, n);
+    const double qn = launch_frob(ctx, q, n);
+    if (qn < 1.0) {
+      launch_identity_axpy(ctx, t, q, n, 0.75);
+      QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &one, q, n, t, n, &zero, qt, n));
+      launch_identity_axpy(ctx, t, qt, n, 0.5);
+      QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &one, x, n, t, n, &zero, xp, n));
+      QBX_CUDA(cudaMemcpyAsync(x, xp, sizeof(double) * n * n, cudaMemcpyDeviceToDevice, ctx.stream));
+    } else {
+      // t = (x^T)^-1 via LU of x^T and a solve against the identity
+      QBX_BLAS(cublasDgeam(ctx.blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, &one, x, n, &zero, x, n, qt, n));
+      QBX_SOLVER(cusolverDnDgetrf(ctx.solver, n, n, qt, n, ctx.d_solver_work, ctx.d_ipiv, ctx.d_info));
+      launch_identity_axpy(ctx, t, t, n, 0.0);
+      QBX_SOLVER(cusolverDnDgetrs(ctx.solver, CUBLAS_OP_N, n, n, qt, n, ctx.d_ipiv, t, n, ctx.d_info));
+      launch_avg_transpose(ctx, x, t, n);
+    }
+    if (qn <= tol) break;
+  }
+}
+
+// SlaterDet::ortho_align (src/SlaterDet.cpp:768-876)
+void ortho_align(Context& ctx) {
+  const int n = ctx.nst, K = 2 * ctx.wb.ng;
+  const double one = 1.0, two = 2.0, zero = 0.0;
+  launch_cleanup(ctx, ctx.d_c);
+  QBX_CUDA(cudaMemcpyAsync(ctx.d_ctmp, ctx.d_c, sizeof(double) * (size_t)K * n,
+                           cudaMemcpyDeviceToDevice, ctx.stream));
+  double* L = ctx.d_nn;
+  double* X = ctx.d_nn2;
+  overlap_cholesky(ctx, ctx.d_c, L);
+  // B = 2 C^T C_last - c0 c_last0^T
+  {
+    ProfScope ps(ctx, "gemm_overlap_last");
+    QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, ctx.d_c, K,
+                         ctx.d_c_last, K, &zero, X, n));
+  }
+  launch_rank1_fix(ctx, X, n, ctx.d_c, K, ctx.d_c_last, K, n, n, -1.0, false);
+  QBX_BLAS(cublasDtrsm(ctx.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
+                       CUBLAS_DIAG_NON_UNIT, n, n, &one, L, n, X, n));
+  polar(ctx, X, 1.e-6, 20);
+  QBX_BLAS(cublasDtrsm(ctx.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T,
+                       CUBLAS_DIAG_NON_UNIT, n, n, &one, L, n, X, n));
+  ProfScope ps(ctx, "gemm_rotate");
+  QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, K, n, n, &one, ctx.d_ctmp, K, X, n, &zero,
+                       ctx.d_c, K));
+}
+
+// ChargeDensity::update_density (src/ChargeDensity.cpp:136-198)
+void update_density(Context& ctx) {
+  ProfScope ps(ctx, "update_density");
+  launch_density(ctx, ctx.d_c, ctx.d_rhor);
+  const size_t N = ctx.N();
+  ctx.total_charge = dsum(ctx, ctx.d_rhor, N) * ctx.vb.omega / (double)N;
+  vb_forward_real(ctx, ctx.d_rhor, ctx.vb.omega, ctx.d_rhog);
+}
+
+// EnergyFunctional::update_vhxc (src/EnergyFunctional.cpp:231-394)
+void update_vhxc(Context& ctx) {
+  ProfScope ps(ctx, "update_vhxc");
+  launch_xc(ctx);
+  launch_vhxc_gspace(ctx);
+}
+
+// NonLocalPotential::energy (src/NonLocalPotential.cpp:1258-1640):
+// F = 2 A^T C - a0 c0^T, E_nl, and H C += A (D F / Omega)
+static void nonlocal(Context& ctx, bool hpsi) {
+  ctx.enl = 0.0;
+  if (ctx.nproj == 0) return;
+  const int n = ctx.nst, K = 2 * ctx.wb.ng, np = ctx.nproj;
+  const double one = 1.0, two = 2.0, zero = 0.0;
+  {
+    ProfScope ps(ctx, "gemm_nl_project");
+    QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_T, CUBLAS_OP_N, np, n, K, &two, ctx.d_anl, K, ctx.d_c,
+                         K, &zero, ctx.d_fnl, np));
+  }
+  launch_rank1_fix(ctx, ctx.d_fnl, np, ctx.d_anl, K, ctx.d_c, K, np, n, -1.0, false);
+  ctx.enl = launch_enl(ctx);
+  if (hpsi) {
+    ProfScope ps(ctx, "gemm_nl_apply");
+    QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, K, n, np, &one, ctx.d_anl, K, ctx.d_fnl,
+                         np, &one, ctx.d_hc, K));
+  }
+}
+
+// EnergyFunctional::energy (src/EnergyFunctional.cpp:397-1044)
+void energy(Context& ctx, bool hpsi, bool forces) {
+  ProfScope ps(ctx, "energy");
+  ctx.ekin = launch_ekin(ctx);
+  if (hpsi) {
+    ProfScope pv(ctx, "vpsi");
+    launch_vpsi(ctx, ctx.d_c, ctx.d_vr, ctx.d_hc);   // hc = 1/2 G^2 c + V psi
+  }
+  nonlocal(ctx, hpsi);
+  ctx.ecoul = ctx.ehart + ctx.esr - ctx.eself;
+  ctx.etotal = ctx.ekin + ctx.eps + ctx.enl + ctx.ecoul + ctx.exc;
+  if (forces) {
+    int natoms = 0;
+    for (auto& t : ctx.tau) natoms += (int)t.size() / 3;
+    QBX_CUDA(cudaMemsetAsync(ctx.d_fion, 0, sizeof(double) * 3 * natoms, ctx.stream));
+    launch_local_forces(ctx, ctx.d_fion);
+    if (ctx.nproj) launch_nl_forces(ctx, ctx.d_fion);
+    ctx.fion.assign(3 * natoms, 0.0);
+    QBX_CUDA(cudaMemcpyAsync(ctx.fion.data(), ctx.d_fion, sizeof(double) * 3 * natoms,
+                             cudaMemcpyDeviceToHost, ctx.stream));
+    QBX_CUDA(cudaStreamSynchronize(ctx.stream));
+    int a = 0;
+    for (size_t is = 0; is < ctx.tau.size(); is++)
+      for (size_t i = 0; i < ctx.tau[is].size(); i++) ctx.fion[a++] += ctx.fion_esr[is][i];
+  }
+}
+
+// PSDAWavefunctionStepper::update (src/PSDAWavefunctionStepper.cpp:46-249)
+void psda_update(Context& ctx) {
+  ProfScope ps(ctx, "psda_update");
+  const int n = ctx.nst, K = 2 * ctx.wb.ng;
+  const double one = 1.0, two = 2.0, zero = 0.0, mone = -1.0;
+  double* A = ctx.d_nn;
+  {
+    ProfScope pg(ctx, "gemm_residual");
+    QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, ctx.d_c, K, ctx.d_hc, K,
+                         &zero, A, n));
+    launch_rank1_fix(ctx, A, n, ctx.d_c, K, ctx.d_hc, K, n, n, -1.0, false);
+    QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, K, n, n, &mone, ctx.d_c, K, A, n, &one,
+                         ctx.d_hc, K));
+  }
+  launch_precond_update(ctx);
+  launch_psda_elementwise(ctx);
+  ortho_align(ctx);
+  ctx.extrapolate = true;
+}
+
+}  // namespace qbx

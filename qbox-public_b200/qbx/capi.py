@@ -1,0 +1,374 @@
+"""ctypes binding of libqbx.so (the C ABI declared in include/qbx.h).
+
+Loading fails loudly when the CUDA library has not been built: there is no
+CPU path behind this module.  ``Context`` mirrors the reference's objects on
+the electronic-step path (Wavefunction/SlaterDet coefficients,
+ChargeDensity::update_density, EnergyFunctional::update_vhxc/energy,
+PSDAWavefunctionStepper::update) on one GPU.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libqbx.so")
+
+FP64 = 0
+MIXED = 1
+NENERGY = 12
+ENERGY_NAMES = ("ekin", "eps", "enl", "ehart", "ecoul", "exc", "esr", "eself",
+                "etotal", "eigenvalue_sum", "total_charge", "theta")
+
+# every entry point of include/qbx.h
+SYMBOLS = (
+    "qbx_version", "qbx_create", "qbx_destroy", "qbx_last_error",
+    "qbx_set_precision", "qbx_set_cell", "qbx_basis_sizes", "qbx_basis_miller",
+    "qbx_set_coeff_order", "qbx_add_species", "qbx_set_atoms",
+    "qbx_set_coeffs", "qbx_get_coeffs", "qbx_set_coeffs_async",
+    "qbx_get_coeffs_async", "qbx_gram", "qbx_update_density",
+    "qbx_get_density", "qbx_update_vhxc", "qbx_get_vr", "qbx_energy",
+    "qbx_get_hpsi", "qbx_eigenvalue_sum", "qbx_psda_update", "qbx_psda_reset",
+    "qbx_scf_step", "qbx_ft_backward_pair", "qbx_synchronize",
+    "qbx_host_basis", "qbx_host_species_eval", "qbx_host_esr",
+    "qbx_profile", "qbx_profile_get", "qbx_launch_count", "qbx_stream",
+)
+
+_lib = None
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_D = ctypes.c_double
+_DP = ctypes.POINTER(ctypes.c_double)
+_IP = ctypes.POINTER(ctypes.c_int)
+
+
+class QbxError(RuntimeError):
+    pass
+
+
+def load(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Load libqbx.so; raises if it is missing (build it with qbx.build)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise QbxError(f"{path} is not built; run qbox-public_b200/qbx/build.py")
+    lib = ctypes.CDLL(path)
+    sig = {
+        "qbx_version": (_I, []),
+        "qbx_create": (_I, [ctypes.POINTER(_P), _I, _I]),
+        "qbx_destroy": (None, [_P]),
+        "qbx_last_error": (ctypes.c_char_p, [_P]),
+        "qbx_set_precision": (_I, [_P, _I]),
+        "qbx_set_cell": (_I, [_P, _DP, _D, _I, ctypes.c_char_p]),
+        "qbx_basis_sizes": (_I, [_P, _IP, _IP, _IP]),
+        "qbx_basis_miller": (_I, [_P, _IP]),
+        "qbx_set_coeff_order": (_I, [_P, _IP]),
+        "qbx_add_species": (_I, [_P, _I, _D, _I, _DP, _I, _IP, _DP, _DP, _IP]),
+        "qbx_set_atoms": (_I, [_P, _IP, _DP]),
+        "qbx_set_coeffs": (_I, [_P, _DP]),
+        "qbx_get_coeffs": (_I, [_P, _DP]),
+        "qbx_set_coeffs_async": (_I, [_P, _DP]),
+        "qbx_get_coeffs_async": (_I, [_P, _DP]),
+        "qbx_gram": (_I, [_P]),
+        "qbx_update_density": (_I, [_P, _DP]),
+        "qbx_get_density": (_I, [_P, _DP]),
+        "qbx_update_vhxc": (_I, [_P]),
+        "qbx_get_vr": (_I, [_P, _DP]),
+        "qbx_energy": (_I, [_P, _I, _I, _DP, _DP]),
+        "qbx_get_hpsi": (_I, [_P, _DP]),
+        "qbx_eigenvalue_sum": (_I, [_P, _DP]),
+        "qbx_psda_update": (_I, [_P]),
+        "qbx_psda_reset": (_I, [_P]),
+        "qbx_scf_step": (_I, [_P, _I, _DP, _DP]),
+        "qbx_ft_backward_pair": (_I, [_P, _I, _I, _DP]),
+        "qbx_synchronize": (_I, [_P]),
+        "qbx_host_basis": (_I, [_DP, _D, _IP, _IP, _IP, _IP]),
+        "qbx_host_species_eval": (_I, [_I, _D, _I, _DP, _I, _IP, _DP, _I, _DP,
+                                       _DP, _DP, _DP]),
+        "qbx_host_esr": (_I, [_DP, _I, _IP, _DP, _DP, _DP, _DP]),
+        "qbx_profile": (_I, [_P, _I]),
+        "qbx_profile_get": (_I, [_P, ctypes.c_char_p, _DP, ctypes.POINTER(ctypes.c_long)]),
+        "qbx_launch_count": (_I, [_P, ctypes.POINTER(ctypes.c_long)]),
+        "qbx_stream": (_P, [_P]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _dp(a: Optional[np.ndarray]):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_DP)
+
+
+def _ip(a: Optional[np.ndarray]):
+    if a is None:
+        return None
+    assert a.dtype == np.int32 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_IP)
+
+
+class Context:
+    """One Gamma-point Slater determinant and its Hamiltonian on one GPU."""
+
+    def __init__(self, device: int = 0, precision: int = FP64):
+        self.lib = load()
+        h = _P()
+        rc = self.lib.qbx_create(ctypes.byref(h), device, precision)
+        if rc:
+            raise QbxError(f"qbx_create failed with code {rc}")
+        self.h = h
+        self.precision = precision
+        self.natoms = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.qbx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ok(self, rc: int, what: str):
+        if rc:
+            msg = self.lib.qbx_last_error(self.h)
+            raise QbxError(f"{what}: code {rc}: {msg.decode() if msg else ''}")
+
+    # ---- setup
+    def set_cell(self, cell, ecut: float, nst: int, xc: str = "LDA"):
+        a = np.ascontiguousarray(np.asarray(cell, float).ravel())
+        self._ok(self.lib.qbx_set_cell(self.h, _dp(a), float(ecut), int(nst),
+                                       xc.encode()), "set_cell")
+        self.nst = nst
+        ngw, ngv = _I(), _I()
+        npg = (ctypes.c_int * 3)()
+        self._ok(self.lib.qbx_basis_sizes(self.h, ctypes.byref(ngw),
+                                          ctypes.byref(ngv), npg), "basis_sizes")
+        self.ngw, self.ngv = ngw.value, ngv.value
+        self.grid = (npg[0], npg[1], npg[2])
+
+    def set_precision(self, precision: int):
+        self._ok(self.lib.qbx_set_precision(self.h, precision), "set_precision")
+        self.precision = precision
+
+    def miller(self) -> np.ndarray:
+        out = np.empty((self.ngw, 3), np.int32)
+        self._ok(self.lib.qbx_basis_miller(self.h, _ip(out)), "basis_miller")
+        return out
+
+    def set_coeff_order(self, hkl: Optional[np.ndarray]):
+        a = None if hkl is None else np.ascontiguousarray(hkl, np.int32)
+        self._ok(self.lib.qbx_set_coeff_order(self.h, _ip(a)), "set_coeff_order")
+
+    def add_species(self, zval, mesh_spacing, vlocal, projectors: Sequence, dmat):
+        v = np.ascontiguousarray(vlocal, float)
+        nproj = len(projectors)
+        pl = np.array([l for l, _ in projectors], np.int32)
+        pr = (np.ascontiguousarray(np.stack([p for _, p in projectors]), float)
+              if nproj else np.zeros(1))
+        dm = np.ascontiguousarray(np.array(dmat, float) if nproj else np.zeros(1))
+        isp = _I()
+        self._ok(self.lib.qbx_add_species(self.h, int(zval), float(mesh_spacing),
+                                          v.size, _dp(v), nproj,
+                                          _ip(pl) if nproj else None, _dp(pr),
+                                          _dp(dm), ctypes.byref(isp)), "add_species")
+        return isp.value
+
+    def set_atoms(self, counts: Sequence[int], tau: np.ndarray):
+        na = np.ascontiguousarray(np.array(counts, np.int32))
+        t = np.ascontiguousarray(np.asarray(tau, float).reshape(-1))
+        self._ok(self.lib.qbx_set_atoms(self.h, _ip(na), _dp(t)), "set_atoms")
+        self.natoms = int(na.sum())
+
+    # ---- coefficients
+    def set_coeffs(self, c: np.ndarray):
+        a = np.ascontiguousarray(c, np.complex128).view(np.float64)
+        self._ok(self.lib.qbx_set_coeffs(self.h, _dp(a)), "set_coeffs")
+
+    def get_coeffs(self) -> np.ndarray:
+        out = np.empty((self.nst, self.ngw), np.complex128)
+        self._ok(self.lib.qbx_get_coeffs(self.h, _dp(out.view(np.float64))), "get_coeffs")
+        return out
+
+    def get_hpsi(self) -> np.ndarray:
+        out = np.empty((self.nst, self.ngw), np.complex128)
+        self._ok(self.lib.qbx_get_hpsi(self.h, _dp(out.view(np.float64))), "get_hpsi")
+        return out
+
+    # ---- operations
+    def gram(self):
+        self._ok(self.lib.qbx_gram(self.h), "gram")
+
+    def update_density(self) -> float:
+        q = _D()
+        self._ok(self.lib.qbx_update_density(self.h, ctypes.byref(q)), "update_density")
+        return q.value
+
+    def density(self) -> np.ndarray:
+        out = np.empty(self.grid[0] * self.grid[1] * self.grid[2])
+        self._ok(self.lib.qbx_get_density(self.h, _dp(out)), "get_density")
+        return out
+
+    def update_vhxc(self):
+        self._ok(self.lib.qbx_update_vhxc(self.h), "update_vhxc")
+
+    def vr(self) -> np.ndarray:
+        out = np.empty(self.grid[0] * self.grid[1] * self.grid[2])
+        self._ok(self.lib.qbx_get_vr(self.h, _dp(out)), "get_vr")
+        return out
+
+    def energy(self, hpsi=True, forces=False):
+        e = np.zeros(NENERGY)
+        f = np.zeros(3 * max(1, self.natoms)) if forces else None
+        self._ok(self.lib.qbx_energy(self.h, int(hpsi), int(forces), _dp(e), _dp(f)),
+                 "energy")
+        out = dict(zip(ENERGY_NAMES, e))
+        if forces:
+            out["fion"] = f[:3 * self.natoms].reshape(-1, 3)
+        return out
+
+    def eigenvalue_sum(self) -> float:
+        v = _D()
+        self._ok(self.lib.qbx_eigenvalue_sum(self.h, ctypes.byref(v)), "eigenvalue_sum")
+        return v.value
+
+    def psda_update(self):
+        self._ok(self.lib.qbx_psda_update(self.h), "psda_update")
+
+    def psda_reset(self):
+        self._ok(self.lib.qbx_psda_reset(self.h), "psda_reset")
+
+    def scf_step(self, forces=False):
+        e = np.zeros(NENERGY)
+        f = np.zeros(3 * max(1, self.natoms)) if forces else None
+        self._ok(self.lib.qbx_scf_step(self.h, int(forces), _dp(e), _dp(f)), "scf_step")
+        out = dict(zip(ENERGY_NAMES, e))
+        if forces:
+            out["fion"] = f[:3 * self.natoms].reshape(-1, 3)
+        return out
+
+    def ft_backward_pair(self, n1: int, n2: int) -> np.ndarray:
+        n = self.grid[0] * self.grid[1] * self.grid[2]
+        out = np.empty(n, np.complex128)
+        self._ok(self.lib.qbx_ft_backward_pair(self.h, n1, n2, _dp(out.view(np.float64))),
+                 "ft_backward_pair")
+        return out.reshape(self.grid[2], self.grid[1], self.grid[0])
+
+    def synchronize(self):
+        self._ok(self.lib.qbx_synchronize(self.h), "synchronize")
+
+    # ---- timing
+    def profile(self, on: bool = True):
+        self._ok(self.lib.qbx_profile(self.h, int(on)), "profile")
+
+    def profile_get(self, name: str):
+        ms = _D()
+        n = ctypes.c_long()
+        self._ok(self.lib.qbx_profile_get(self.h, name.encode(), ctypes.byref(ms),
+                                          ctypes.byref(n)), "profile_get")
+        return ms.value, n.value
+
+    def launch_count(self) -> int:
+        n = ctypes.c_long()
+        self._ok(self.lib.qbx_launch_count(self.h, ctypes.byref(n)), "launch_count")
+        return n.value
+
+    def stream(self) -> int:
+        return self.lib.qbx_stream(self.h)
+
+    def set_coeffs_async(self, c_pinned: np.ndarray):
+        self._ok(self.lib.qbx_set_coeffs_async(self.h, _dp(c_pinned)), "set_coeffs_async")
+
+    def get_coeffs_async(self, out_pinned: np.ndarray):
+        self._ok(self.lib.qbx_get_coeffs_async(self.h, _dp(out_pinned)), "get_coeffs_async")
+
+
+def from_system(system, device: int = 0, precision: int = FP64,
+                coeffs: Optional[np.ndarray] = None, gram: bool = True) -> Context:
+    """Build a context for a qbx.systems.System and upload its seeded
+    coefficients (keyed by sorted Miller index)."""
+    ctx = Context(device, precision)
+    ctx.set_cell(system.cell, system.ecut, system.nbands, system.xc)
+    hkl = system.miller()
+    if hkl.shape[0] != ctx.ngw:
+        raise QbxError(f"basis size {ctx.ngw} differs from the generator's {hkl.shape[0]}")
+    if not np.array_equal(ctx.miller(), hkl):
+        ctx.set_coeff_order(hkl)
+    for sp in system.species:
+        ctx.add_species(sp.zval, sp.mesh_spacing, sp.local_potential(),
+                        sp.projectors(), [d for _, d in sp.dmatrix()])
+    counts = [len(system.positions(i)) for i in range(len(system.species))]
+    tau = np.concatenate([system.positions(i) for i in range(len(system.species))])
+    ctx.set_atoms(counts, tau)
+    if coeffs is None:
+        coeffs = system.coefficients(hkl)
+    ctx.set_coeffs(coeffs)
+    if gram:
+        ctx.gram()
+    return ctx
+
+
+# ---------------------------------------------------------- host-only helpers
+def host_basis(cell, ecut: float):
+    """(ngw, ngv, grid, hkl) from the library's host basis builder."""
+    lib = load()
+    a = np.ascontiguousarray(np.asarray(cell, float).ravel())
+    ngw, ngv = _I(), _I()
+    npg = (ctypes.c_int * 3)()
+    rc = lib.qbx_host_basis(_dp(a), float(ecut), ctypes.byref(ngw), ctypes.byref(ngv), npg, None)
+    if rc:
+        raise QbxError(f"qbx_host_basis failed: {rc}")
+    hkl = np.empty((ngw.value, 3), np.int32)
+    rc = lib.qbx_host_basis(_dp(a), float(ecut), None, None, None, _ip(hkl))
+    if rc:
+        raise QbxError(f"qbx_host_basis failed: {rc}")
+    return ngw.value, ngv.value, (npg[0], npg[1], npg[2]), hkl
+
+
+def host_species_eval(sp, g: np.ndarray):
+    """V_loc(G), dV_loc/dG and V_nl(G) per projector from the library."""
+    lib = load()
+    v = np.ascontiguousarray(sp.local_potential(), float)
+    projs = sp.projectors()
+    nproj = len(projs)
+    pl = np.array([l for l, _ in projs], np.int32)
+    pr = (np.ascontiguousarray(np.stack([p for _, p in projs]), float)
+          if nproj else np.zeros(1))
+    g = np.ascontiguousarray(g, float)
+    vl = np.empty(g.size)
+    dvl = np.empty(g.size)
+    vnl = np.empty(max(1, nproj) * g.size)
+    rc = lib.qbx_host_species_eval(int(sp.zval), float(sp.mesh_spacing), v.size, _dp(v),
+                                   nproj, _ip(pl) if nproj else None, _dp(pr), g.size,
+                                   _dp(g), _dp(vl), _dp(dvl), _dp(vnl))
+    if rc:
+        raise QbxError(f"qbx_host_species_eval failed: {rc}")
+    return vl, dvl, vnl[:nproj * g.size].reshape(nproj, g.size)
+
+
+def host_esr(system):
+    lib = load()
+    a = np.ascontiguousarray(np.asarray(system.cell, float).ravel())
+    nsp = len(system.species)
+    na = np.array([len(system.positions(i)) for i in range(nsp)], np.int32)
+    zv = np.array([float(sp.zval) for sp in system.species])
+    tau = np.ascontiguousarray(np.concatenate([system.positions(i) for i in range(nsp)]))
+    e = _D()
+    f = np.empty(3 * int(na.sum()))
+    rc = lib.qbx_host_esr(_dp(a), nsp, _ip(na), _dp(zv), _dp(tau), ctypes.byref(e), _dp(f))
+    if rc:
+        raise QbxError(f"qbx_host_esr failed: {rc}")
+    return e.value, f.reshape(-1, 3)

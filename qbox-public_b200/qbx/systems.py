@@ -94,6 +94,7 @@ class System:
     nbands: int
     xc: str
     seed: int
+    nel_override: Optional[int] = None   # electrons when not the ions' total
 
     @property
     def ecut(self) -> float:      # Hartree
@@ -101,7 +102,15 @@ class System:
 
     @property
     def nel(self) -> int:
+        if self.nel_override is not None:
+            return self.nel_override
         return sum(self.species[i].zval for i, _ in self.atoms)
+
+    def band_sample(self, nbands: int) -> "System":
+        """Same cell, atoms and cutoff with only nbands doubly occupied
+        bands (a bounded timing sample of the full system)."""
+        return dataclasses.replace(self, nbands=nbands, nel_override=2 * nbands,
+                                   name=f"{self.name}_b{nbands}")
 
     def positions(self, isp: int) -> np.ndarray:
         return np.array([p for i, p in self.atoms if i == isp]).reshape(-1, 3)
