@@ -132,6 +132,14 @@ int qbx_profile_get(qbx_context* ctx, const char* name, double* ms,
 int qbx_launch_count(qbx_context* ctx, long* n);
 /* The cudaStream_t all work of the context is ordered on. */
 void* qbx_stream(qbx_context* ctx);
+/* Mixed path only: 0 = split BF16 products through cuBLAS, 1 = through the
+ * library's tcgen05 kernel (default; shapes it does not cover use cuBLAS). */
+int qbx_set_gemm_backend(qbx_context* ctx, int backend);
+/* One split-precision product D (m x n) = A^T B of host FP64 matrices A
+ * (k x m) and B (k x n), column-major, through backend 0 (cuBLAS) or 1
+ * (tcgen05), for checking the products on their own. */
+int qbx_split_gemm_tn(qbx_context* ctx, int m, int n, int k, const double* a,
+                      const double* b, double* d, int backend);
 
 /* Host-only setup helpers (no GPU needed), exposing the same host code the
  * context uses.  Basis::resize + ChargeDensity grid: basis sizes, grid and

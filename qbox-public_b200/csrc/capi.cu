@@ -4,6 +4,7 @@
 // qbx_last_error().
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <new>
@@ -53,6 +54,7 @@ int guarded(qbx_context* h, F f) {
 }
 
 void free_cell(Context& c) {
+  free_mixed(c);
   free_sticks(c.dws);
   free_sticks(c.dvs);
   double** bufs[] = {&c.d_gx_w, &c.d_g2_w, &c.d_gx_v, &c.d_g2i_v, &c.d_c, &c.d_hc, &c.d_c_last,
@@ -129,6 +131,7 @@ int qbx_create(qbx_context** out, int device, int precision) {
   if (!h) return 5;
   h->c.device = device;
   h->c.precision = precision;
+  if (const char* e = std::getenv("QBX_GEMM_BACKEND")) h->c.gemm_backend = std::atoi(e) == 0 ? 0 : 1;
   const int rc = guarded(h, [&](Context& c) {
     QBX_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
     QBX_BLAS(cublasCreate(&c.blas));
@@ -172,6 +175,7 @@ int qbx_set_precision(qbx_context* h, int precision) {
       c.zbuf_bytes = per_pair * c.pair_batch;
     }
     c.precision = precision;
+    alloc_mixed(c);
   });
 }
 
@@ -247,6 +251,7 @@ int qbx_set_cell(qbx_context* h, const double cell[9], double ecut, int nst, con
     c.tau.clear();
     QBX_CUDA(cudaDeviceSynchronize());   // memsets above ran on the legacy stream
     c.have_cell = true;
+    alloc_mixed(c);
   });
 }
 
@@ -364,6 +369,7 @@ int qbx_set_atoms(qbx_context* h, const int* na, const double* tau) {
       c.eself += na[is] * c.species[is].eself();
     }
     c.esr = esr_energy_forces(c.wb.cell, c.tau, zv, 1.5, c.fion_esr);
+    alloc_mixed(c);
     QBX_CUDA(cudaStreamSynchronize(c.stream));
   });
 }
@@ -493,6 +499,7 @@ int qbx_scf_step(qbx_context* h, int forces, double* energies, double* fion) {
     if (forces && fion) std::memcpy(fion, c.fion.data(), sizeof(double) * c.fion.size());
     psda_update(c);
     QBX_CUDA(cudaStreamSynchronize(c.stream));
+    QBX_REQUIRE(tc_check_error(c) == 0, 55, "tcgen05 GEMM pipeline wait timed out");
   });
 }
 
@@ -537,6 +544,56 @@ int qbx_launch_count(qbx_context* h, long* n) {
 }
 
 void* qbx_stream(qbx_context* h) { return h ? (void*)h->c.stream : nullptr; }
+
+int qbx_split_gemm_tn(qbx_context* h, int m, int n, int k, const double* a, const double* b,
+                      double* d, int backend) {
+  return guarded(h, [&](Context& c) {
+    QBX_REQUIRE(m > 0 && n > 0 && k > 0 && a && b && d, 1, "bad GEMM arguments");
+    const int ldp = (k + 63) / 64 * 64;
+    double *da = dalloc<double>((size_t)k * m), *db = dalloc<double>((size_t)k * n);
+    double* dd = dalloc<double>((size_t)m * n);
+    void *ah, *al, *bh, *bl;
+    QBX_CUDA(cudaMalloc(&ah, (size_t)ldp * m * 2));
+    QBX_CUDA(cudaMalloc(&al, (size_t)ldp * m * 2));
+    QBX_CUDA(cudaMalloc(&bh, (size_t)ldp * n * 2));
+    QBX_CUDA(cudaMalloc(&bl, (size_t)ldp * n * 2));
+    h2d_sync(da, a, sizeof(double) * k * m);
+    h2d_sync(db, b, sizeof(double) * k * n);
+    split_bf16_2d(c, da, k, m, k, ah, al, ldp);
+    split_bf16_2d(c, db, k, n, k, bh, bl, ldp);
+    const int saved = c.gemm_backend;
+    const size_t saved_acc = c.acc32_elems;
+    void* saved_ptr = c.d_acc32;
+    void* acc = nullptr;
+    QBX_CUDA(cudaMalloc(&acc, (size_t)m * n * sizeof(float)));
+    c.d_acc32 = acc;
+    c.acc32_elems = (size_t)m * n;
+    c.gemm_backend = backend;
+    try {
+      QBX_REQUIRE(backend == 0 || tc_gemm_supported(c, true, false, m, n, k), 54,
+                  "shape not supported by the tcgen05 GEMM");
+      split_gemm(c, true, false, m, n, k, 1.0, ah, al, ldp, bh, bl, ldp, 0.0, dd);
+      QBX_CUDA(cudaMemcpyAsync(d, dd, sizeof(double) * m * n, cudaMemcpyDeviceToHost, c.stream));
+      QBX_CUDA(cudaStreamSynchronize(c.stream));
+      QBX_REQUIRE(tc_check_error(c) == 0, 55, "tcgen05 GEMM pipeline wait timed out");
+    } catch (...) {
+      c.gemm_backend = saved; c.d_acc32 = saved_ptr; c.acc32_elems = saved_acc;
+      cudaFree(acc); cudaFree(ah); cudaFree(al); cudaFree(bh); cudaFree(bl);
+      dfree(da); dfree(db); dfree(dd);
+      throw;
+    }
+    c.gemm_backend = saved; c.d_acc32 = saved_ptr; c.acc32_elems = saved_acc;
+    cudaFree(acc); cudaFree(ah); cudaFree(al); cudaFree(bh); cudaFree(bl);
+    dfree(da); dfree(db); dfree(dd);
+  });
+}
+
+int qbx_set_gemm_backend(qbx_context* h, int backend) {
+  return guarded(h, [&](Context& c) {
+    QBX_REQUIRE(backend == 0 || backend == 1, 1, "backend must be 0 (cuBLAS) or 1 (tcgen05)");
+    c.gemm_backend = backend;
+  });
+}
 
 int qbx_synchronize(qbx_context* h) {
   return guarded(h, [&](Context& c) { QBX_CUDA(cudaStreamSynchronize(c.stream)); });

@@ -262,6 +262,25 @@ struct Context {
          etotal = 0, total_charge = 0, eigsum = 0, theta = 0;
   std::vector<double> fion;     // 3*natoms, species-major like the reference
 
+  // mixed precision: BF16 hi/lo splits of the GEMM operands
+  int gemm_backend = 1;         // 0: cuBLAS BF16 products, 1: own tcgen05 kernel
+  void* d_acc32 = nullptr;      // FP32 product accumulator
+  size_t acc32_elems = 0;
+  void* cs_hi[2] = {nullptr, nullptr};   // splits of C (0: at energy, 1: after the step)
+  void* cs_lo[2] = {nullptr, nullptr};
+  void* hs_hi = nullptr;        // split of H C
+  void* hs_lo = nullptr;
+  void* as_hi = nullptr;        // split of the projectors
+  void* as_lo = nullptr;
+  void* ss_hi = nullptr;        // split of a small matrix (fnl, A, X)
+  void* ss_lo = nullptr;
+  int ldp = 0;                  // padded leading dimension of the K-row splits
+  float* c32 = nullptr;         // FP32 copy of C (tall updates)
+  float* a32 = nullptr;         // FP32 copy of the projectors
+  float* s32 = nullptr;         // FP32 copy of a small matrix
+  void* d_tc_ws = nullptr;      // split-K partials of the tcgen05 GEMM
+  size_t tc_ws_elems = 0;
+  void* d_tc_err = nullptr;     // wait-timeout flag of the tcgen05 GEMM
   long nlaunch = 0;              // kernels of this library launched so far
   Profiler prof;
 
@@ -355,5 +374,25 @@ void launch_identity_axpy(Context& ctx, double* t, const double* q, int n,
 void launch_symmetrize_lower(Context& ctx, double* q, int n);
 void launch_avg_transpose(Context& ctx, double* x, const double* t, int n);
 double launch_frob(Context& ctx, const double* q, int n);
+
+// split-precision products (split_gemm.cu, tc_gemm.cu)
+void split_bf16(Context& ctx, const double* x, size_t n, void* hi, void* lo);
+void overlap_diag_f64(Context& ctx, const double* c, int K, int n, double* S);
+// C = alpha * op(A) op(B) + beta * C, C column-major with ld m
+void split_gemm(Context& ctx, bool ta, bool tb, int m, int n, int k, double alpha,
+                const void* ahi, const void* alo, int lda, const void* bhi, const void* blo,
+                int ldb, double beta, double* C);
+bool tc_gemm_supported(const Context& ctx, bool ta, bool tb, int m, int n, int k);
+void tc_split_gemm(Context& ctx, bool ta, bool tb, int m, int n, int k, double alpha,
+                   const void* ahi, const void* alo, int lda, const void* bhi, const void* blo,
+                   int ldb, double beta, double* C);
+int tc_check_error(Context& ctx);   // nonzero if a tcgen05 GEMM wait ran out
+void split_bf16_2d(Context& ctx, const double* x, int rows, int cols, int ldx, void* hi, void* lo,
+                   int ldp);
+void to_f32(Context& ctx, const double* x, int rows, int cols, int ldx, float* y, int ldy);
+void f32emu_gemm_nn(Context& ctx, int m, int n, int k, double alpha, const float* A, int lda,
+                    const float* B, int ldb, double beta, double* C);
+void alloc_mixed(Context& ctx);
+void free_mixed(Context& ctx);
 
 }  // namespace qbx

@@ -1,0 +1,164 @@
+// Split-precision GEMMs of the mixed path.
+//
+// An FP64 operand x is written as x = hi + lo with hi = bf16(x) and
+// lo = bf16(x - hi) (about 16 significant bits together).  A product is then
+// formed from three BF16 tensor-core products accumulated in FP32,
+//     A B  ~  A_hi B_hi + A_hi B_lo + A_lo B_hi,
+// whose relative error is ~2^-16 per term and random in sign, so inner
+// products over the 145 838 plane-wave rows keep ~1e-8 absolute accuracy off
+// the diagonal.  On the diagonal of C^T C the dropped A_lo B_lo term has a
+// fixed sign; the overlap matrix therefore gets its diagonal from an FP64
+// reduction (|c_n|^2 summed exactly) before the FP64 Cholesky.
+//
+// The products themselves run through GemmBackend: cuBLAS BF16 GEMMs with
+// FP32 output here, or the library's own tcgen05 kernel (tc_gemm.cu).
+#include <algorithm>
+
+#include "qbx_internal.h"
+#include <cuda_bf16.h>
+
+namespace qbx {
+
+__global__ void k_split_bf16(const double* __restrict__ x, size_t n, __nv_bfloat16* __restrict__ hi,
+                             __nv_bfloat16* __restrict__ lo) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const double v = x[i];
+    const __nv_bfloat16 h = __double2bfloat16(v);
+    hi[i] = h;
+    lo[i] = __double2bfloat16(v - (double)__bfloat162float(h));
+  }
+}
+
+// out = alpha * acc + beta * out  (column-major, both ld = m)
+__global__ void k_acc_to_f64(const float* __restrict__ acc, size_t n, double alpha, double beta,
+                             double* __restrict__ out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    out[i] = alpha * (double)acc[i] + (beta != 0.0 ? beta * out[i] : 0.0);
+}
+
+// diag(S)_n = 2 sum_G |c_n(G)|^2 - c_n(0)^2 in FP64 (one CTA per band)
+__global__ void k_diag_overlap(const double* __restrict__ c, int K, int n, double* __restrict__ S) {
+  __shared__ double sh[32];
+  const int b = blockIdx.x;
+  const double* p = c + (size_t)b * K;
+  double s = 0.0;
+  for (int i = threadIdx.x; i < K; i += blockDim.x) s += p[i] * p[i];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += sh[w];
+    S[b + (size_t)b * n] = 2.0 * t - p[0] * p[0];
+  }
+}
+
+static int nblocks(size_t n) {
+  return (int)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, 148 * 32));
+}
+
+// column-major rows x cols (ld ldx) -> hi/lo with leading dimension ldp >=
+// rows; the padding rows are zero
+__global__ void k_split_bf16_2d(const double* __restrict__ x, int rows, int cols, int ldx,
+                                __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo,
+                                int ldp) {
+  const size_t n = (size_t)ldp * cols;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const int c = (int)(t / ldp), r = (int)(t - (size_t)c * ldp);
+    double v = 0.0;
+    if (r < rows) v = x[(size_t)c * ldx + r];
+    const __nv_bfloat16 h = __double2bfloat16(v);
+    hi[t] = h;
+    lo[t] = __double2bfloat16(v - (double)__bfloat162float(h));
+  }
+}
+
+void split_bf16_2d(Context& ctx, const double* x, int rows, int cols, int ldx, void* hi, void* lo,
+                   int ldp) {
+  const size_t n = (size_t)ldp * cols;
+  k_split_bf16_2d<<<nblocks(n), 256, 0, ctx.stream>>>(x, rows, cols, ldx, (__nv_bfloat16*)hi,
+                                                      (__nv_bfloat16*)lo, ldp);
+  QBX_LAUNCHED(ctx);
+}
+
+void split_bf16(Context& ctx, const double* x, size_t n, void* hi, void* lo) {
+  k_split_bf16<<<nblocks(n), 256, 0, ctx.stream>>>(x, n, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo);
+  QBX_LAUNCHED(ctx);
+}
+
+void overlap_diag_f64(Context& ctx, const double* c, int K, int n, double* S) {
+  k_diag_overlap<<<n, 256, 0, ctx.stream>>>(c, K, n, S);
+  QBX_LAUNCHED(ctx);
+}
+
+// D (m x n, FP32, ld m) = sum of the three split products of op(A) op(B),
+// A and B given as hi/lo BF16 pairs.  ta/tb: true = transpose (the operand
+// is stored K-major, i.e. column-major with ld = k).
+static void cublas_split(Context& ctx, bool ta, bool tb, int m, int n, int k, const void* ahi,
+                         const void* alo, int lda, const void* bhi, const void* blo, int ldb,
+                         float* D) {
+  const float one = 1.0f, zero = 0.0f;
+  const cublasOperation_t oa = ta ? CUBLAS_OP_T : CUBLAS_OP_N;
+  const cublasOperation_t ob = tb ? CUBLAS_OP_T : CUBLAS_OP_N;
+  const void* as[3] = {ahi, ahi, alo};
+  const void* bs[3] = {bhi, blo, bhi};
+  for (int t = 0; t < 3; t++)
+    QBX_BLAS(cublasGemmEx(ctx.blas, oa, ob, m, n, k, &one, as[t], CUDA_R_16BF, lda, bs[t],
+                          CUDA_R_16BF, ldb, t == 0 ? &zero : &one, D, CUDA_R_32F, m,
+                          CUBLAS_COMPUTE_32F, CUBLAS_GEMM_DEFAULT));
+}
+
+void split_gemm(Context& ctx, bool ta, bool tb, int m, int n, int k, double alpha,
+                const void* ahi, const void* alo, int lda, const void* bhi, const void* blo,
+                int ldb, double beta, double* C) {
+  if (ctx.gemm_backend == 1 && tc_gemm_supported(ctx, ta, tb, m, n, k)) {
+    tc_split_gemm(ctx, ta, tb, m, n, k, alpha, ahi, alo, lda, bhi, blo, ldb, beta, C);
+    return;
+  }
+  float* D = (float*)ctx.d_acc32;
+  QBX_REQUIRE((size_t)m * n <= ctx.acc32_elems, 50, "split GEMM accumulator too small");
+  cublas_split(ctx, ta, tb, m, n, k, ahi, alo, lda, bhi, blo, ldb, D);
+  const size_t nn = (size_t)m * n;
+  k_acc_to_f64<<<nblocks(nn), 256, 0, ctx.stream>>>(D, nn, alpha, beta, C);
+  QBX_LAUNCHED(ctx);
+}
+
+// ---- FP32-accurate products for the tall updates (C A, A_nl F, C (I-X)):
+// FP64 operands rounded to FP32, products on the tensor cores through
+// cuBLAS's BF16x9 emulation of FP32, FP32 result added into the FP64
+// output.  Relative error ~1e-7 per element instead of ~1e-5 for BF16x3.
+__global__ void k_to_f32(const double* __restrict__ x, int rows, int cols, int ldx,
+                         float* __restrict__ y, int ldy) {
+  const size_t n = (size_t)rows * cols;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const int c = (int)(t / rows), r = (int)(t - (size_t)c * rows);
+    y[(size_t)c * ldy + r] = (float)x[(size_t)c * ldx + r];
+  }
+}
+
+void to_f32(Context& ctx, const double* x, int rows, int cols, int ldx, float* y, int ldy) {
+  const size_t n = (size_t)rows * cols;
+  k_to_f32<<<nblocks(n), 256, 0, ctx.stream>>>(x, rows, cols, ldx, y, ldy);
+  QBX_LAUNCHED(ctx);
+}
+
+// C (m x n, ld m) = alpha A B + beta C with A (m x k, ld lda) and B (k x n,
+// ld ldb) given in FP32.
+void f32emu_gemm_nn(Context& ctx, int m, int n, int k, double alpha, const float* A, int lda,
+                    const float* B, int ldb, double beta, double* C) {
+  float* D = (float*)ctx.d_acc32;
+  QBX_REQUIRE((size_t)m * n <= ctx.acc32_elems, 50, "FP32 product accumulator too small");
+  const float one = 1.0f, zero = 0.0f;
+  QBX_BLAS(cublasGemmEx(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, m, n, k, &one, A, CUDA_R_32F, lda, B,
+                        CUDA_R_32F, ldb, &zero, D, CUDA_R_32F, m,
+                        CUBLAS_COMPUTE_32F_EMULATED_16BFX9, CUBLAS_GEMM_DEFAULT));
+  const size_t nn = (size_t)m * n;
+  k_acc_to_f64<<<nblocks(nn), 256, 0, ctx.stream>>>(D, nn, alpha, beta, C);
+  QBX_LAUNCHED(ctx);
+}
+
+}  // namespace qbx

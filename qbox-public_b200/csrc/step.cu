@@ -17,6 +17,8 @@
 
 namespace qbx {
 
+static bool mixed(const Context& ctx) { return ctx.precision == MIXED; }
+
 static void require_potrf(Context& ctx, const char* what) {
   int info = 0;
   QBX_CUDA(cudaMemcpyAsync(&info, ctx.d_info, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
@@ -25,13 +27,23 @@ static void require_potrf(Context& ctx, const char* what) {
                                  std::to_string(info) + ")");
 }
 
-// S = 2 C^T C - c0 c0^T, lower triangle, then S = L L^T in place
-static void overlap_cholesky(Context& ctx, const double* c, double* S) {
+// S = 2 C^T C - c0 c0^T, lower triangle, then S = L L^T in place.  In the
+// mixed path the product uses the BF16 split of c in slot `split` and the
+// diagonal is recomputed exactly in FP64.
+static void overlap_cholesky(Context& ctx, const double* c, double* S, int split = -1) {
   ProfScope ps(ctx, "overlap_cholesky");
   const int n = ctx.nst, K = 2 * ctx.wb.ng;
   const double two = 2.0, zero = 0.0;
-  QBX_BLAS(cublasDsyrk(ctx.blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, n, K, &two, c, K, &zero, S, n));
-  launch_rank1_fix(ctx, S, n, c, K, c, K, n, n, -1.0, true);
+  if (split >= 0) {
+    split_gemm(ctx, true, false, n, n, K, 2.0, ctx.cs_hi[split], ctx.cs_lo[split], ctx.ldp,
+               ctx.cs_hi[split], ctx.cs_lo[split], ctx.ldp, 0.0, S);
+    launch_rank1_fix(ctx, S, n, c, K, c, K, n, n, -1.0, true);
+    overlap_diag_f64(ctx, c, K, n, S);
+  } else {
+    QBX_BLAS(cublasDsyrk(ctx.blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, n, K, &two, c, K, &zero,
+                         S, n));
+    launch_rank1_fix(ctx, S, n, c, K, c, K, n, n, -1.0, true);
+  }
   QBX_SOLVER(cusolverDnDpotrf(ctx.solver, CUBLAS_FILL_MODE_LOWER, n, S, n, ctx.d_solver_work,
                               ctx.solver_lwork, ctx.d_info));
   require_potrf(ctx, "Cholesky of the overlap matrix");
@@ -87,16 +99,24 @@ void ortho_align(Context& ctx) {
   const int n = ctx.nst, K = 2 * ctx.wb.ng;
   const double one = 1.0, two = 2.0, zero = 0.0;
   launch_cleanup(ctx, ctx.d_c);
-  QBX_CUDA(cudaMemcpyAsync(ctx.d_ctmp, ctx.d_c, sizeof(double) * (size_t)K * n,
-                           cudaMemcpyDeviceToDevice, ctx.stream));
   double* L = ctx.d_nn;
   double* X = ctx.d_nn2;
-  overlap_cholesky(ctx, ctx.d_c, L);
+  const bool mx = mixed(ctx);
+  if (!mx)
+    QBX_CUDA(cudaMemcpyAsync(ctx.d_ctmp, ctx.d_c, sizeof(double) * (size_t)K * n,
+                             cudaMemcpyDeviceToDevice, ctx.stream));
+  // in the mixed path slot 0 holds the split of C_last (made in energy())
+  if (mx) split_bf16_2d(ctx, ctx.d_c, K, n, K, ctx.cs_hi[1], ctx.cs_lo[1], ctx.ldp);
+  overlap_cholesky(ctx, ctx.d_c, L, mx ? 1 : -1);
   // B = 2 C^T C_last - c0 c_last0^T
   {
     ProfScope ps(ctx, "gemm_overlap_last");
-    QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, ctx.d_c, K,
-                         ctx.d_c_last, K, &zero, X, n));
+    if (mx)
+      split_gemm(ctx, true, false, n, n, K, 2.0, ctx.cs_hi[1], ctx.cs_lo[1], ctx.ldp,
+                 ctx.cs_hi[0], ctx.cs_lo[0], ctx.ldp, 0.0, X);
+    else
+      QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, ctx.d_c, K,
+                           ctx.d_c_last, K, &zero, X, n));
   }
   launch_rank1_fix(ctx, X, n, ctx.d_c, K, ctx.d_c_last, K, n, n, -1.0, false);
   QBX_BLAS(cublasDtrsm(ctx.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
@@ -105,8 +125,18 @@ void ortho_align(Context& ctx) {
   QBX_BLAS(cublasDtrsm(ctx.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T,
                        CUBLAS_DIAG_NON_UNIT, n, n, &one, L, n, X, n));
   ProfScope ps(ctx, "gemm_rotate");
-  QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, K, n, n, &one, ctx.d_ctmp, K, X, n, &zero,
-                       ctx.d_c, K));
+  if (mx) {
+    // C <- C - C (I - X): the split-precision error only touches the
+    // correction, so C stays orthonormal to the accuracy of the overlap.
+    double* T = ctx.d_nn3;
+    launch_identity_axpy(ctx, T, X, n, -1.0);
+    to_f32(ctx, T, n, n, n, ctx.s32, n);
+    to_f32(ctx, ctx.d_c, K, n, K, ctx.c32, K);
+    f32emu_gemm_nn(ctx, K, n, n, -1.0, ctx.c32, K, ctx.s32, n, 1.0, ctx.d_c);
+  } else {
+    QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, K, n, n, &one, ctx.d_ctmp, K, X, n,
+                         &zero, ctx.d_c, K));
+  }
 }
 
 // ChargeDensity::update_density (src/ChargeDensity.cpp:136-198)
@@ -132,23 +162,36 @@ static void nonlocal(Context& ctx, bool hpsi) {
   if (ctx.nproj == 0) return;
   const int n = ctx.nst, K = 2 * ctx.wb.ng, np = ctx.nproj;
   const double one = 1.0, two = 2.0, zero = 0.0;
+  const bool mx = mixed(ctx);
   {
     ProfScope ps(ctx, "gemm_nl_project");
-    QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_T, CUBLAS_OP_N, np, n, K, &two, ctx.d_anl, K, ctx.d_c,
-                         K, &zero, ctx.d_fnl, np));
+    if (mx)
+      split_gemm(ctx, true, false, np, n, K, 2.0, ctx.as_hi, ctx.as_lo, ctx.ldp, ctx.cs_hi[0],
+                 ctx.cs_lo[0], ctx.ldp, 0.0, ctx.d_fnl);
+    else
+      QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_T, CUBLAS_OP_N, np, n, K, &two, ctx.d_anl, K,
+                           ctx.d_c, K, &zero, ctx.d_fnl, np));
   }
   launch_rank1_fix(ctx, ctx.d_fnl, np, ctx.d_anl, K, ctx.d_c, K, np, n, -1.0, false);
   ctx.enl = launch_enl(ctx);
   if (hpsi) {
     ProfScope ps(ctx, "gemm_nl_apply");
-    QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, K, n, np, &one, ctx.d_anl, K, ctx.d_fnl,
-                         np, &one, ctx.d_hc, K));
+    if (mx) {
+      to_f32(ctx, ctx.d_fnl, np, n, np, ctx.s32, np);
+      f32emu_gemm_nn(ctx, K, n, np, 1.0, ctx.a32, K, ctx.s32, np, 1.0, ctx.d_hc);
+    } else {
+      QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, K, n, np, &one, ctx.d_anl, K,
+                           ctx.d_fnl, np, &one, ctx.d_hc, K));
+    }
   }
 }
 
 // EnergyFunctional::energy (src/EnergyFunctional.cpp:397-1044)
 void energy(Context& ctx, bool hpsi, bool forces) {
   ProfScope ps(ctx, "energy");
+  if (mixed(ctx))
+    split_bf16_2d(ctx, ctx.d_c, 2 * ctx.wb.ng, ctx.nst, 2 * ctx.wb.ng, ctx.cs_hi[0], ctx.cs_lo[0],
+                  ctx.ldp);
   ctx.ekin = launch_ekin(ctx);
   if (hpsi) {
     ProfScope pv(ctx, "vpsi");
@@ -181,16 +224,72 @@ void psda_update(Context& ctx) {
   double* A = ctx.d_nn;
   {
     ProfScope pg(ctx, "gemm_residual");
-    QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, ctx.d_c, K, ctx.d_hc, K,
-                         &zero, A, n));
-    launch_rank1_fix(ctx, A, n, ctx.d_c, K, ctx.d_hc, K, n, n, -1.0, false);
-    QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, K, n, n, &mone, ctx.d_c, K, A, n, &one,
-                         ctx.d_hc, K));
+    if (mixed(ctx)) {
+      split_bf16_2d(ctx, ctx.d_hc, K, n, K, ctx.hs_hi, ctx.hs_lo, ctx.ldp);
+      split_gemm(ctx, true, false, n, n, K, 2.0, ctx.cs_hi[0], ctx.cs_lo[0], ctx.ldp, ctx.hs_hi,
+                 ctx.hs_lo, ctx.ldp, 0.0, A);
+      launch_rank1_fix(ctx, A, n, ctx.d_c, K, ctx.d_hc, K, n, n, -1.0, false);
+      to_f32(ctx, A, n, n, n, ctx.s32, n);
+      to_f32(ctx, ctx.d_c, K, n, K, ctx.c32, K);
+      f32emu_gemm_nn(ctx, K, n, n, -1.0, ctx.c32, K, ctx.s32, n, 1.0, ctx.d_hc);
+    } else {
+      QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, ctx.d_c, K, ctx.d_hc,
+                           K, &zero, A, n));
+      launch_rank1_fix(ctx, A, n, ctx.d_c, K, ctx.d_hc, K, n, n, -1.0, false);
+      QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, K, n, n, &mone, ctx.d_c, K, A, n,
+                           &one, ctx.d_hc, K));
+    }
   }
   launch_precond_update(ctx);
   launch_psda_elementwise(ctx);
   ortho_align(ctx);
   ctx.extrapolate = true;
+}
+
+void free_mixed(Context& ctx) {
+  void** bufs[] = {&ctx.d_acc32, &ctx.cs_hi[0], &ctx.cs_lo[0], &ctx.cs_hi[1], &ctx.cs_lo[1],
+                   &ctx.hs_hi, &ctx.hs_lo, &ctx.as_hi, &ctx.as_lo, &ctx.ss_hi, &ctx.ss_lo,
+                   &ctx.d_tc_ws, &ctx.d_tc_err};
+  for (void** b : bufs)
+    if (*b) { cudaFree(*b); *b = nullptr; }
+  dfree(ctx.c32);
+  dfree(ctx.a32);
+  dfree(ctx.s32);
+  ctx.acc32_elems = 0;
+  ctx.tc_ws_elems = 0;
+}
+
+// Buffers of the split-precision products; the projector split is rebuilt
+// whenever the projectors change.
+void alloc_mixed(Context& ctx) {
+  free_mixed(ctx);
+  if (ctx.precision != MIXED || !ctx.have_cell) return;
+  const size_t K = 2 * (size_t)ctx.wb.ng, n = ctx.nst, np = ctx.nproj;
+  ctx.ldp = (int)((K + 63) / 64 * 64);
+  const size_t wf = (size_t)ctx.ldp * n;
+  const size_t small = std::max(np * n, n * n);
+  ctx.acc32_elems = std::max(wf, std::max(np * n, std::max(K * np, n * n)));
+  QBX_CUDA(cudaMalloc(&ctx.d_acc32, ctx.acc32_elems * sizeof(float)));
+  for (int s = 0; s < 2; s++) {
+    QBX_CUDA(cudaMalloc(&ctx.cs_hi[s], wf * 2));
+    QBX_CUDA(cudaMalloc(&ctx.cs_lo[s], wf * 2));
+  }
+  QBX_CUDA(cudaMalloc(&ctx.hs_hi, wf * 2));
+  QBX_CUDA(cudaMalloc(&ctx.hs_lo, wf * 2));
+  QBX_CUDA(cudaMalloc(&ctx.ss_hi, std::max<size_t>(small, 1) * 2));
+  QBX_CUDA(cudaMalloc(&ctx.ss_lo, std::max<size_t>(small, 1) * 2));
+  ctx.c32 = dalloc<float>(K * n);
+  ctx.s32 = dalloc<float>(std::max<size_t>(small, 1));
+  if (np) {
+    QBX_CUDA(cudaMalloc(&ctx.as_hi, (size_t)ctx.ldp * np * 2));
+    QBX_CUDA(cudaMalloc(&ctx.as_lo, (size_t)ctx.ldp * np * 2));
+    ctx.a32 = dalloc<float>(K * np);
+    if (ctx.d_anl) {
+      split_bf16_2d(ctx, ctx.d_anl, (int)K, (int)np, (int)K, ctx.as_hi, ctx.as_lo, ctx.ldp);
+      to_f32(ctx, ctx.d_anl, (int)K, (int)np, (int)K, ctx.a32, (int)K);
+    }
+  }
+  QBX_CUDA(cudaStreamSynchronize(ctx.stream));
 }
 
 }  // namespace qbx

@@ -1,0 +1,341 @@
+// tcgen05 split-precision GEMM for sm_100a.
+//
+//   D(m, n) = sum_k A(k, m) B(k, n)   over the three split terms
+//             A_hi B_hi + A_hi B_lo + A_lo B_hi   (BF16 in, FP32 accumulate)
+//
+// A and B are K-major (column-major with the contraction index contiguous),
+// as the wavefunction and projector matrices of a SlaterDet are.  These are
+// the inner products of the electronic step: projections F = A_nl^T C, the
+// residual C^T (H C), the overlap C^T C and C^T C_last.
+//
+// One CTA computes a 128 x 128 FP32 tile of one split-K slice:
+//   warp 0  - TMA producer: per 64-wide K block one pipeline stage receives
+//             the four 128x64 BF16 tiles A_hi, A_lo, B_hi, B_lo
+//             (128-byte swizzle); mbarrier expect_tx per stage;
+//   warp 1  - allocates 128 TMEM columns; one elected thread issues the
+//             12 tcgen05.mma (3 terms x 4 K-steps of 16) per stage and
+//             commits the stage back to the producer;
+//   warps 4-7 - epilogue: tcgen05.ld of the accumulator (each warp its 32
+//             TMEM lanes) and coalesced FP32 stores of the partial tile.
+// The split-K partials are summed in FP64 by k_reduce_splits.  Every
+// mbarrier wait is bounded; a wait that runs out sets an error flag that
+// the host turns into an error, and the CTA still releases its TMEM.
+#include <cuda.h>
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "qbx_internal.h"
+
+namespace qbx {
+
+namespace tc {
+
+constexpr int BM = 128, BN = 128, BK = 64;
+constexpr int STAGES = 3;
+constexpr int TILE_BYTES = BM * BK * 2;           // 16 KB per operand tile
+constexpr int STAGE_BYTES = 4 * TILE_BYTES;       // A_hi, A_lo, B_hi, B_lo
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /* align */ + 256 /* barriers */;
+constexpr int THREADS = 256;
+constexpr uint32_t TMEM_COLS = 128;
+constexpr long long WAIT_LIMIT = 1ll << 24;       // bounded spins per wait
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+// bounded wait for the phase with the given parity to complete
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t a = smem_u32(bar);
+  for (long long it = 0; it < WAIT_LIMIT; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar,
+                                            int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes "
+      "[%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(dst)),
+      "l"((uint64_t)map), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+
+// K-major operand tile in shared memory, 128-byte swizzle, rows of 128 bytes,
+// 8-row groups 1024 bytes apart (the canonical UMMA K-major SW128 layout).
+__device__ __forceinline__ uint64_t smem_desc(const void* tile) {
+  const uint64_t addr = smem_u32(tile);
+  return ((addr & 0x3FFFF) >> 4) | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
+}
+
+// kind::f16 instruction descriptor: F32 accumulate, BF16 A and B, both
+// K-major, N = BN, M = BM.
+__host__ __device__ constexpr uint32_t idesc_bf16() {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+         ((uint32_t)(BM >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc_bf16()), "r"(acc)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          smem_u32(bar))
+      : "memory");
+}
+
+__global__ void __launch_bounds__(THREADS, 1)
+k_tc_split_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant__ CUtensorMap ma_lo,
+                const __grid_constant__ CUtensorMap mb_hi, const __grid_constant__ CUtensorMap mb_lo,
+                int M, int N, int nkb, int kb_per_split, float* __restrict__ ws,
+                int* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t* full = (uint64_t*)(base + STAGES * STAGE_BYTES);
+  uint64_t* empty = full + STAGES;
+  uint64_t* accum = empty + STAGES;
+  uint32_t* tmem_slot = (uint32_t*)(accum + 1);
+  __shared__ int s_fail;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int kb0 = blockIdx.z * kb_per_split;
+  const int kb1 = min(nkb, kb0 + kb_per_split);
+  const int niter = max(0, kb1 - kb0);
+
+  if (threadIdx.x == 0) {
+    s_fail = 0;
+    for (int s = 0; s < STAGES; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(accum, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // ---------------- TMA producer
+    for (int it = 0; it < niter; ++it) {
+      const int s = it % STAGES;
+      const uint32_t ph = (uint32_t)((it / STAGES) & 1);
+      if (!mbar_wait(&empty[s], ph ^ 1u)) { atomicExch(err, 1); s_fail = 1; break; }
+      unsigned char* st = base + s * STAGE_BYTES;
+      mbar_expect_tx(&full[s], STAGE_BYTES);
+      const int kx = (kb0 + it) * BK;
+      tma_load_2d(st + 0 * TILE_BYTES, &ma_hi, &full[s], kx, m0);
+      tma_load_2d(st + 1 * TILE_BYTES, &ma_lo, &full[s], kx, m0);
+      tma_load_2d(st + 2 * TILE_BYTES, &mb_hi, &full[s], kx, n0);
+      tma_load_2d(st + 3 * TILE_BYTES, &mb_lo, &full[s], kx, n0);
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---------------- MMA issuer
+    for (int it = 0; it < niter; ++it) {
+      const int s = it % STAGES;
+      const uint32_t ph = (uint32_t)((it / STAGES) & 1);
+      if (!mbar_wait(&full[s], ph)) { atomicExch(err, 2); s_fail = 1; break; }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      unsigned char* st = base + s * STAGE_BYTES;
+      const uint64_t dah = smem_desc(st + 0 * TILE_BYTES);
+      const uint64_t dal = smem_desc(st + 1 * TILE_BYTES);
+      const uint64_t dbh = smem_desc(st + 2 * TILE_BYTES);
+      const uint64_t dbl = smem_desc(st + 3 * TILE_BYTES);
+#pragma unroll
+      for (int k = 0; k < BK / 16; ++k) {
+        const uint64_t off = (uint64_t)(k * 32) >> 4;      // 16 BF16 = 32 bytes
+        const uint32_t first = (it == 0 && k == 0) ? 0u : 1u;
+        umma_bf16(tmem, dah + off, dbh + off, first);
+        umma_bf16(tmem, dah + off, dbl + off, 1u);
+        umma_bf16(tmem, dal + off, dbh + off, 1u);
+      }
+      umma_commit(&empty[s]);
+    }
+    umma_commit(accum);
+  } else if (warp >= 4) {
+    // ---------------- epilogue
+    const int wq = warp - 4;                       // TMEM lanes 32*wq .. 32*wq+31
+    const int row = m0 + wq * 32 + lane;
+    const bool ok = mbar_wait(accum, 0u);
+    if (!ok) { atomicExch(err, 3); s_fail = 1; }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    float* out = ws + (size_t)blockIdx.z * M * N;
+#pragma unroll 1
+    for (int c0 = 0; c0 < BN; c0 += 16) {
+      uint32_t r[16];
+      const uint32_t taddr = tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)c0;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+          "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+            "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+            "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (ok && niter > 0 && row < M) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int col = n0 + c0 + j;
+          if (col < N) out[(size_t)col * M + row] = __uint_as_float(r[j]);
+        }
+      } else if (row < M) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int col = n0 + c0 + j;
+          if (col < N) out[(size_t)col * M + row] = 0.0f;
+        }
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  }
+  __syncthreads();
+  if (warp == 1) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(TMEM_COLS)
+                 : "memory");
+  }
+}
+
+// out(i) = alpha * sum_s ws(s, i) + beta * out(i), summed in FP64
+__global__ void k_reduce_splits(const float* __restrict__ ws, int nsplit, size_t n, double alpha,
+                                double beta, double* __restrict__ out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int z = 0; z < nsplit; z++) s += (double)ws[(size_t)z * n + i];
+    out[i] = alpha * s + (beta != 0.0 ? beta * out[i] : 0.0);
+  }
+}
+
+}  // namespace tc
+
+// ------------------------------------------------------------------ host
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    QBX_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+    QBX_REQUIRE(p && q == cudaDriverEntryPointSuccess, 52, "cuTensorMapEncodeTiled unavailable");
+    fn = (EncodeTiledFn)p;
+  }
+  return fn;
+}
+
+// K-major BF16 matrix: rows = k (contiguous, ld elements), cols = m; box
+// 64 (k) x 128 (m rows), 128-byte swizzle.
+static CUtensorMap kmajor_map(const void* ptr, int k, int cols, int ld) {
+  CUtensorMap map;
+  const cuuint64_t dims[2] = {(cuuint64_t)k, (cuuint64_t)cols};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)tc::BK, (cuuint32_t)tc::BM};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr),
+                                 dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                 CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  QBX_REQUIRE(r == CUDA_SUCCESS, 53, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+  return map;
+}
+
+bool tc_gemm_supported(const Context& ctx, bool ta, bool tb, int m, int n, int k) {
+  // transposed-A x plain-B products on whole 128 x 128 tiles, with 16-byte
+  // aligned leading dimensions (checked by the caller's padding)
+  (void)ctx;
+  return ta && !tb && m % tc::BM == 0 && n % tc::BN == 0 && k >= tc::BK;
+}
+
+void tc_split_gemm(Context& ctx, bool ta, bool tb, int m, int n, int k, double alpha,
+                   const void* ahi, const void* alo, int lda, const void* bhi, const void* blo,
+                   int ldb, double beta, double* C) {
+  QBX_REQUIRE(tc_gemm_supported(ctx, ta, tb, m, n, k), 54, "shape not supported by tcgen05 GEMM");
+  QBX_REQUIRE((lda * 2) % 16 == 0 && (ldb * 2) % 16 == 0, 54, "leading dimension not 16-byte aligned");
+  QBX_REQUIRE(((uintptr_t)ahi | (uintptr_t)alo | (uintptr_t)bhi | (uintptr_t)blo) % 16 == 0, 54,
+              "operand not 16-byte aligned");
+  const CUtensorMap mah = kmajor_map(ahi, k, m, lda);
+  const CUtensorMap mal = kmajor_map(alo, k, m, lda);
+  const CUtensorMap mbh = kmajor_map(bhi, k, n, ldb);
+  const CUtensorMap mbl = kmajor_map(blo, k, n, ldb);
+  const int nkb = (k + tc::BK - 1) / tc::BK;
+  const int tiles = (m / tc::BM) * (n / tc::BN);
+  int sms = 148;
+  QBX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device));
+  // split K so that about two CTAs per SM are in flight; the partials (FP32)
+  // are summed in FP64 afterwards
+  int splits = std::max(1, std::min(nkb, (2 * sms + tiles - 1) / tiles));
+  const size_t need = (size_t)splits * m * n;
+  if (need > ctx.tc_ws_elems) {
+    if (ctx.d_tc_ws) cudaFree(ctx.d_tc_ws);
+    QBX_CUDA(cudaMalloc(&ctx.d_tc_ws, need * sizeof(float)));
+    ctx.tc_ws_elems = need;
+  }
+  if (!ctx.d_tc_err) {
+    QBX_CUDA(cudaMalloc(&ctx.d_tc_err, sizeof(int)));
+    QBX_CUDA(cudaMemsetAsync(ctx.d_tc_err, 0, sizeof(int), ctx.stream));
+  }
+  const int kbps = (nkb + splits - 1) / splits;
+  splits = (nkb + kbps - 1) / kbps;
+  QBX_CUDA(cudaFuncSetAttribute(tc::k_tc_split_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                tc::SMEM_BYTES));
+  dim3 grid(m / tc::BM, n / tc::BN, splits);
+  tc::k_tc_split_gemm<<<grid, tc::THREADS, tc::SMEM_BYTES, ctx.stream>>>(
+      mah, mal, mbh, mbl, m, n, nkb, kbps, (float*)ctx.d_tc_ws, (int*)ctx.d_tc_err);
+  QBX_LAUNCHED(ctx);
+  // C = alpha * (sum of the split-K partials, in FP64) + beta * C
+  const size_t nn = (size_t)m * n;
+  const int nb = (int)std::min<size_t>((nn + 255) / 256, (size_t)sms * 16);
+  tc::k_reduce_splits<<<nb, 256, 0, ctx.stream>>>((const float*)ctx.d_tc_ws, splits, nn, alpha,
+                                                  beta, C);
+  QBX_LAUNCHED(ctx);
+}
+
+int tc_check_error(Context& ctx) {
+  if (!ctx.d_tc_err) return 0;
+  int e = 0;
+  QBX_CUDA(cudaMemcpyAsync(&e, ctx.d_tc_err, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+  QBX_CUDA(cudaStreamSynchronize(ctx.stream));
+  return e;
+}
+
+}  // namespace qbx

@@ -35,6 +35,7 @@ SYMBOLS = (
     "qbx_scf_step", "qbx_ft_backward_pair", "qbx_synchronize",
     "qbx_host_basis", "qbx_host_species_eval", "qbx_host_esr",
     "qbx_profile", "qbx_profile_get", "qbx_launch_count", "qbx_stream",
+    "qbx_set_gemm_backend", "qbx_split_gemm_tn",
 )
 
 _lib = None
@@ -95,6 +96,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "qbx_profile_get": (_I, [_P, ctypes.c_char_p, _DP, ctypes.POINTER(ctypes.c_long)]),
         "qbx_launch_count": (_I, [_P, ctypes.POINTER(ctypes.c_long)]),
         "qbx_stream": (_P, [_P]),
+        "qbx_set_gemm_backend": (_I, [_P, _I]),
+        "qbx_split_gemm_tn": (_I, [_P, _I, _I, _I, _DP, _DP, _DP, _I]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -285,6 +288,21 @@ class Context:
         n = ctypes.c_long()
         self._ok(self.lib.qbx_launch_count(self.h, ctypes.byref(n)), "launch_count")
         return n.value
+
+    def set_gemm_backend(self, backend: int):
+        self._ok(self.lib.qbx_set_gemm_backend(self.h, backend), "set_gemm_backend")
+
+    def split_gemm_tn(self, a: np.ndarray, b: np.ndarray, backend: int) -> np.ndarray:
+        """A^T B through the split-precision product (a: k x m, b: k x n)."""
+        k, m = a.shape
+        _, n = b.shape
+        # column-major k x m is the C-ordered m x k array a.T
+        at = np.ascontiguousarray(np.asarray(a, float).T)
+        bt = np.ascontiguousarray(np.asarray(b, float).T)
+        out = np.empty((n, m))          # column-major m x n
+        self._ok(self.lib.qbx_split_gemm_tn(self.h, m, n, k, _dp(at), _dp(bt), _dp(out),
+                                            backend), "split_gemm_tn")
+        return out.T
 
     def stream(self) -> int:
         return self.lib.qbx_stream(self.h)
