@@ -67,6 +67,8 @@ void free_cell(Context& c) {
   dfree(c.d_info);
   if (c.d_grid) { cudaFree(c.d_grid); c.d_grid = nullptr; }
   if (c.d_zbuf) { cudaFree(c.d_zbuf); c.d_zbuf = nullptr; }
+  if (c.d_zfast) { cudaFree(c.d_zfast); c.d_zfast = nullptr; }
+  dfree(c.d_vr32);
   c.have_cell = false;
 }
 
@@ -247,6 +249,22 @@ int qbx_set_cell(qbx_context* h, const double cell[9], double ecut, int nst, con
     c.pair_batch = (int)std::max<size_t>(1, std::min<size_t>(npairs, ((size_t)4 << 30) / per_pair));
     QBX_CUDA(cudaMalloc(&c.d_zbuf, per_pair * c.pair_batch));
     c.zbuf_bytes = per_pair * c.pair_batch;
+    // the specialised FFTs work through a smaller stick buffer that can stay
+    // in L2 between the z and plane kernels (64 MB unless overridden)
+    {
+      size_t mb = 64;
+      if (const char* e = std::getenv("QBX_FAST_ZBUF_MB")) mb = std::max(1, std::atoi(e));
+      const size_t pp64 = (size_t)c.wb.n2 * c.wb.nvec * sizeof(double2);
+      c.zfast_bytes = std::max(mb << 20, pp64);
+      QBX_CUDA(cudaMalloc(&c.d_zfast, c.zfast_bytes));
+      c.d_vr32 = dalloc<float>(N);
+      c.fast_fft = true;
+      if (const char* e = std::getenv("QBX_FAST_FFT")) c.fast_fft = std::atoi(e) != 0;
+      if (const char* e = std::getenv("QBX_FAST_WARPS")) c.fast_warps = std::max(1, std::min(16, std::atoi(e)));
+      if (const char* e = std::getenv("QBX_FAST_RODS")) c.fast_rods = std::max(1, std::min(32, std::atoi(e)));
+      if (const char* e = std::getenv("QBX_FAST_CHUNKS")) c.fast_chunks = std::max(1, std::atoi(e));
+      if (const char* e = std::getenv("QBX_FAST_BATCH")) c.fast_batch = std::max(0, std::atoi(e));
+    }
     c.species.clear();
     c.tau.clear();
     QBX_CUDA(cudaDeviceSynchronize());   // memsets above ran on the legacy stream

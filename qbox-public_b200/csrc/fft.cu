@@ -29,6 +29,7 @@
 #include <cstdio>
 #include <vector>
 
+#include "fft_fast.cuh"
 #include "qbx_internal.h"
 
 namespace qbx {
@@ -586,8 +587,65 @@ static void staged_batch(Context& ctx, int op, const double* c, const double* v,
   }
 }
 
+static int nblk(size_t n);
+
+__global__ void k_to_float(const double* __restrict__ x, size_t n, float* __restrict__ y) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    y[i] = (float)x[i];
+}
+
+// The specialised kernels of fft_fast_*.cu in batches of band pairs through
+// ctx.d_zfast; false when the grid has none.
+static bool staged_fast(Context& ctx, int op, const double* c, const double* v, double* rho,
+                        const double* w, double* hc) {
+  if (!ctx.fast_fft || !ctx.d_zfast) return false;
+  const DeviceSticks& g = ctx.dws;
+  fast::StagedArgs a{};
+  a.op = (op == OP_DENSITY) ? fast::XY_DENSITY : fast::XY_VPSI;
+  a.c = c;
+  a.rho = rho;
+  a.w = w;
+  a.hc = hc;
+  a.nst = ctx.nst;
+  a.zbuf = ctx.d_zfast;
+  a.twx = twiddles(ctx.device, 0, g.n0);
+  a.twy = twiddles(ctx.device, 1, g.n1);
+  a.twz = twiddles(ctx.device, 2, g.n2);
+  a.rods_per_cta = ctx.fast_rods;
+  a.xy_warps = ctx.fast_warps;
+  a.density_chunks = ctx.fast_chunks;
+  a.v = v;
+  if (op == OP_VPSI && ctx.precision == MIXED) {
+    const size_t N = ctx.N();
+    k_to_float<<<nblk(N), 256, 0, ctx.stream>>>(v, N, ctx.d_vr32);
+    QBX_LAUNCHED(ctx);
+    a.v = ctx.d_vr32;
+  }
+  const size_t limit = (size_t)max_smem_optin(ctx.device);
+  const int npairs = (ctx.nst + 1) / 2;
+  const size_t per_pair = (ctx.precision == MIXED ? sizeof(float2) : sizeof(double2)) *
+                          (size_t)g.n2 * g.nvec;
+  int batch = (int)std::min<size_t>(npairs, ctx.zfast_bytes / per_pair);
+  if (ctx.fast_batch > 0) batch = std::min(batch, ctx.fast_batch);
+  QBX_REQUIRE(batch >= 1, 21, "stick buffer of the specialised FFTs holds no band pair");
+  bool first = true;
+  for (int p0 = 0; p0 < npairs; p0 += batch) {
+    a.pair0 = p0;
+    a.npairs = std::min(batch, npairs - p0);
+    const bool ok = fast_staged_a(ctx, a, limit) || fast_staged_b(ctx, a, limit);
+    if (!ok) {
+      QBX_REQUIRE(first, 21, "specialised FFT kernels unavailable after the first batch");
+      return false;
+    }
+    first = false;
+  }
+  return true;
+}
+
 static void staged(Context& ctx, int op, const double* c, const double* v, double* rho,
                    const double* w, double* hc) {
+  if (staged_fast(ctx, op, c, v, rho, w, hc)) return;
   const int npairs = (ctx.nst + 1) / 2;
   for (int p0 = 0; p0 < npairs; p0 += ctx.pair_batch) {
     const int np = std::min(ctx.pair_batch, npairs - p0);

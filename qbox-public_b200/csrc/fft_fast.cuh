@@ -1,0 +1,387 @@
+// Staged wavefunction FFT kernels specialised on the grid lengths.
+//
+// Same three-kernel structure as the generic path in fft.cu (z sticks ->
+// plane tile -> z sticks, band pairs packed as psi_1 + i psi_2), with every
+// 1-D transform a warp-synchronous register FFT of compile-time length
+// (fft_reg.cuh) and the surrounding data movement fused into the first and
+// last radix stages:
+//
+//   kz_bwd  : the first z stage reads the two bands' coefficients of the
+//             stick's rod straight from HBM (+G: c1 + i c2, -G: conj(c1) +
+//             i conj(c2)); the sticks of the CTA are then written
+//             plane-major, coalesced across sticks.
+//   kxy     : one CTA per (z plane, pair chunk).  The plane's sticks are
+//             scattered into a compact tile P[column][y] (odd row pitch, so
+//             strided lane accesses spread over the banks), y is transformed
+//             column by column in place, then each warp takes whole x rows:
+//             the first x stage reads the row straight out of P (zeros off
+//             the occupied columns), and the last stage either accumulates
+//             f1/Omega psi_1^2 + f2/Omega psi_2^2 (density) or multiplies by
+//             V(r) into the warp's line, after which the forward x transform
+//             writes only the occupied columns back into P; the forward y
+//             pass and a coalesced gather return the sticks.
+//   kz_fwd  : coalesced read of the sticks, forward z transform, unpack of
+//             the two bands (src/BasisMapping.cpp:722-750), 1/N scale and
+//             the kinetic term: hc = 1/2 |G|^2 c + result.
+//
+// Mixed precision accumulates the density of a CTA's pairs in an FP32 plane
+// in shared memory and adds it to the FP64 grid once per CTA; FP64 adds each
+// pair's contribution with FP64 atomics.
+#pragma once
+
+#include <algorithm>
+
+#include "fft_reg.cuh"
+#include "qbx_internal.h"
+
+namespace qbx {
+namespace fast {
+
+using reg::BufLoad;
+using reg::BufStore;
+using reg::cmk;
+
+constexpr int kZThreads = 256;
+// CTA size of the plane kernel: FP64 lines need about twice the registers
+// of FP32 lines in the radix-7/11 stages
+template <typename T> struct XYThreads { static constexpr int v = 512; };
+template <> struct XYThreads<double> { static constexpr int v = 256; };
+
+template <typename C>
+__device__ __forceinline__ void load_tw(C* dst, const double2* src, int n) {
+  for (int k = threadIdx.x; k < n; k += blockDim.x) dst[k] = cmk<C>(src[k].x, src[k].y);
+}
+
+__host__ __device__ constexpr int pitch(int n) { return (n % 2 == 0) ? n + 1 : n; }
+
+// ------------------------------------------------------------ z backward
+template <typename T, int N2>
+__global__ void __launch_bounds__(kZThreads)
+kz_bwd(const double2* __restrict__ c, int ngw, int nst, int pair0, DeviceSticks g,
+       const double2* __restrict__ twz, typename reg::CT<T>::c* __restrict__ zbuf,
+       int rods_per_cta) {
+  using C = typename reg::CT<T>::c;
+  constexpr int LD = pitch(N2);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  C* lines = tw + N2;
+  const int r0 = blockIdx.x * rods_per_cta;
+  const int r1 = min(g.nrods, r0 + rods_per_cta);
+  const int s0 = (r0 == 0) ? 0 : 2 * r0 - 1;
+  const int nl = (2 * r1 - 1) - s0;
+  const int pl = blockIdx.y;
+  const int b1 = 2 * (pair0 + pl);
+  const double2* c1 = c + (size_t)b1 * ngw;
+  const double2* c2 = (b1 + 1 < nst) ? c + (size_t)(b1 + 1) * ngw : nullptr;
+  load_tw(tw, twz, N2);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  constexpr int half = (N2 + 1) / 2;
+  for (int line = warp; line < nl; line += nw) {
+    const int s = s0 + line;
+    const int r = (s + 1) >> 1;
+    const int lmin = g.rod_lmin[r], size = g.rod_size[r], first = g.rod_first[r];
+    const bool rod0 = (r == 0);
+    const bool mstick = ((s & 1) == 0);   // the -G stick of a rod r > 0
+    auto ld = [&](int z) -> C {
+      const int lz = z < half ? z : z - N2;
+      const bool minus = rod0 ? (lz <= 0) : mstick;
+      const int l = minus ? -lz : lz;
+      double vx = 0.0, vy = 0.0;
+      if (l >= lmin && l < lmin + size) {
+        const double2 p = c1[first + (l - lmin)];
+        const double2 q = c2 ? c2[first + (l - lmin)] : make_double2(0.0, 0.0);
+        if (!minus) { vx = p.x - q.y; vy = p.y + q.x; }
+        else        { vx = p.x + q.y; vy = q.x - p.y; }
+      }
+      return cmk<C>(vx, vy);
+    };
+    C* buf = lines + line * LD;
+    reg::warp_fft<N2, +1>(buf, tw, lane, ld, BufStore<C>{buf});
+  }
+  __syncthreads();
+  C* out = zbuf + (size_t)pl * N2 * g.nvec;
+  for (int t = threadIdx.x; t < nl * N2; t += blockDim.x) {
+    const int line = t % nl, z = t / nl;
+    out[(size_t)z * g.nvec + s0 + line] = lines[line * LD + z];
+  }
+}
+
+// ------------------------------------------------------------ z forward
+template <typename T, int N2>
+__global__ void __launch_bounds__(kZThreads)
+kz_fwd(const typename reg::CT<T>::c* __restrict__ zbuf, int ngw, int nst, int pair0,
+       DeviceSticks g, const double2* __restrict__ twz, double scale,
+       const double2* __restrict__ c, const double* __restrict__ g2, double2* __restrict__ hc,
+       int rods_per_cta) {
+  using C = typename reg::CT<T>::c;
+  constexpr int LD = pitch(N2);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  C* lines = tw + N2;
+  const int r0 = blockIdx.x * rods_per_cta;
+  const int r1 = min(g.nrods, r0 + rods_per_cta);
+  const int s0 = (r0 == 0) ? 0 : 2 * r0 - 1;
+  const int nl = (2 * r1 - 1) - s0;
+  const int pl = blockIdx.y;
+  const int b1 = 2 * (pair0 + pl);
+  const bool two = (b1 + 1 < nst);
+  load_tw(tw, twz, N2);
+  const C* in = zbuf + (size_t)pl * N2 * g.nvec;
+  for (int t = threadIdx.x; t < nl * N2; t += blockDim.x) {
+    const int line = t % nl, z = t / nl;
+    lines[line * LD + z] = in[(size_t)z * g.nvec + s0 + line];
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int line = warp; line < nl; line += nw) {
+    C* buf = lines + line * LD;
+    reg::warp_fft<N2, -1>(buf, tw, lane, BufLoad<C>{buf}, BufStore<C>{buf});
+  }
+  __syncthreads();
+  // one warp per rod: unpack the pair and add the kinetic term
+  for (int r = r0 + warp; r < r1; r += nw) {
+    const int lmin = g.rod_lmin[r], size = g.rod_size[r], first = g.rod_first[r];
+    const int sp = (r == 0) ? 0 : 2 * r - 1 - s0;
+    const int sm = (r == 0) ? 0 : 2 * r - s0;
+    for (int e = lane; e < size; e += 32) {
+      const int l = lmin + e;
+      const int zp = ((l % N2) + N2) % N2;
+      const int zm = ((-l % N2) + N2) % N2;
+      const C P = lines[sp * LD + zp];
+      const C M = lines[sm * LD + zm];
+      // c1 = (Z(G) + conj Z(-G))/2, c2 = -i (Z(G) - conj Z(-G))/2
+      const double px = P.x, py = P.y, mx = M.x, my = M.y;
+      const double c1x = 0.5 * (px + mx) * scale, c1y = 0.5 * (py - my) * scale;
+      const double c2x = 0.5 * (py + my) * scale, c2y = 0.5 * (mx - px) * scale;
+      const int ig = first + e;
+      const double kin = 0.5 * g2[ig];
+      const size_t i1 = (size_t)b1 * ngw + ig;
+      const double2 a = c[i1];
+      hc[i1] = make_double2(kin * a.x + c1x, kin * a.y + c1y);
+      if (two) {
+        const size_t i2 = i1 + ngw;
+        const double2 b = c[i2];
+        hc[i2] = make_double2(kin * b.x + c2x, kin * b.y + c2y);
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------ xy plane
+enum { XY_DENSITY = 0, XY_VPSI = 1 };
+
+// density accumulator in shared memory: FP32 plane for the mixed path
+template <typename T> struct UseSmemAcc { static constexpr bool v = false; };
+template <> struct UseSmemAcc<float> { static constexpr bool v = true; };
+
+template <typename T, int N0, int N1, int OP>
+__host__ size_t xy_smem_bytes(int ncol, int nwarps) {
+  using C = typename reg::CT<T>::c;
+  size_t b = sizeof(C) * ((size_t)N0 + N1 + (size_t)ncol * pitch(N1) + (size_t)nwarps * N0);
+  if (OP == XY_DENSITY && UseSmemAcc<T>::v) b += sizeof(float) * (size_t)N0 * N1;
+  b += sizeof(int) * N0;
+  return b;
+}
+
+// shared memory: [twx N0][twy N1][P ncol x pitch(N1)][one line of N0 per
+// warp][FP32 density plane N1 x N0, mixed density only][xmap N0 ints]
+template <typename T, int N0, int N1, int OP>
+__global__ void __launch_bounds__(XYThreads<T>::v)
+kxy(typename reg::CT<T>::c* __restrict__ zbuf, int npairs, int pairs_per_cta, DeviceSticks g,
+    const double2* __restrict__ twx_g, const double2* __restrict__ twy_g,
+    const T* __restrict__ v, double* __restrict__ rho, const double* __restrict__ w, int pair0,
+    int nst) {
+  using C = typename reg::CT<T>::c;
+  constexpr int LD = pitch(N1);
+  constexpr bool SACC = (OP == XY_DENSITY) && UseSmemAcc<T>::v;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int ncol = g.ncol, nvec = g.nvec;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  C* twx = reinterpret_cast<C*>(smem_raw);
+  C* twy = twx + N0;
+  C* P = twy + N1;
+  C* lines = P + (size_t)ncol * LD;
+  float* acc = reinterpret_cast<float*>(lines + (size_t)nw * N0);
+  int* xmap = reinterpret_cast<int*>(acc + (SACC ? (size_t)N0 * N1 : 0));
+  C* line = lines + (size_t)warp * N0;
+  const int z = blockIdx.x;
+  load_tw(twx, twx_g, N0);
+  load_tw(twy, twy_g, N1);
+  for (int x = threadIdx.x; x < N0; x += blockDim.x) xmap[x] = -1;
+  if constexpr (SACC)
+    for (int t = threadIdx.x; t < N0 * N1; t += blockDim.x) acc[t] = 0.f;
+  __syncthreads();
+  for (int cidx = threadIdx.x; cidx < ncol; cidx += blockDim.x) xmap[g.col_x[cidx]] = cidx;
+  const int pbeg = blockIdx.y * pairs_per_cta;
+  const int pend = min(npairs, pbeg + pairs_per_cta);
+  for (int pl = pbeg; pl < pend; ++pl) {
+    C* zp = zbuf + ((size_t)pl * g.n2 + z) * nvec;
+    // tile: zero, then scatter the plane's sticks
+    for (int t = threadIdx.x; t < ncol * LD; t += blockDim.x) P[t] = cmk<C>(0.0, 0.0);
+    __syncthreads();
+    for (int s = threadIdx.x; s < nvec; s += blockDim.x)
+      P[g.stick_col[s] * LD + g.stick_y[s]] = zp[s];
+    __syncthreads();
+    // backward y, in place, one warp per occupied column
+    for (int cidx = warp; cidx < ncol; cidx += nw) {
+      C* col = P + cidx * LD;
+      reg::warp_fft<N1, +1>(col, twy, lane, BufLoad<C>{col}, BufStore<C>{col});
+    }
+    __syncthreads();
+    double w1 = 0.0, w2 = 0.0;
+    if (OP == XY_DENSITY) {
+      const int b1 = 2 * (pair0 + pl);
+      w1 = w[b1];
+      w2 = (b1 + 1 < nst) ? w[b1 + 1] : 0.0;
+    }
+    // x rows, one warp per row; the first stage reads the row out of P
+    for (int y = warp; y < N1; y += nw) {
+      auto ldP = [&](int x) -> C {
+        const int cidx = xmap[x];
+        return cidx >= 0 ? P[cidx * LD + y] : cmk<C>(0.0, 0.0);
+      };
+      const size_t rowbase = ((size_t)z * N1 + y) * N0;
+      if constexpr (OP == XY_DENSITY) {
+        if constexpr (SACC) {
+          const float f1 = (float)w1, f2 = (float)w2;
+          float* arow = acc + y * N0;
+          auto st = [&](int x, C val) {
+            arow[x] += f1 * (float)val.x * (float)val.x + f2 * (float)val.y * (float)val.y;
+          };
+          reg::warp_fft<N0, +1>(line, twx, lane, ldP, st);
+        } else {
+          auto st = [&](int x, C val) {
+            atomicAdd(&rho[rowbase + x], w1 * (double)val.x * (double)val.x +
+                                             w2 * (double)val.y * (double)val.y);
+          };
+          reg::warp_fft<N0, +1>(line, twx, lane, ldP, st);
+        }
+      } else {
+        const T* vrow = v + rowbase;
+        auto stv = [&](int x, C val) {
+          const T vv = vrow[x];
+          val.x *= vv;
+          val.y *= vv;
+          line[x] = val;
+        };
+        reg::warp_fft<N0, +1>(line, twx, lane, ldP, stv);
+        auto stP = [&](int x, C val) {
+          const int cidx = xmap[x];
+          if (cidx >= 0) P[cidx * LD + y] = val;
+        };
+        reg::warp_fft<N0, -1>(line, twx, lane, BufLoad<C>{line}, stP);
+      }
+    }
+    __syncthreads();
+    if (OP == XY_VPSI) {
+      for (int cidx = warp; cidx < ncol; cidx += nw) {
+        C* col = P + cidx * LD;
+        reg::warp_fft<N1, -1>(col, twy, lane, BufLoad<C>{col}, BufStore<C>{col});
+      }
+      __syncthreads();
+      for (int s = threadIdx.x; s < nvec; s += blockDim.x)
+        zp[s] = P[g.stick_col[s] * LD + g.stick_y[s]];
+      __syncthreads();
+    }
+  }
+  if constexpr (SACC) {
+    __syncthreads();
+    const size_t pbase = (size_t)z * N1 * N0;
+    for (int t = threadIdx.x; t < N0 * N1; t += blockDim.x) atomicAdd(&rho[pbase + t], (double)acc[t]);
+  }
+}
+
+// ------------------------------------------------------------ launch
+// Arguments of one batch of band pairs through the specialised kernels.
+struct StagedArgs {
+  int op;                  // XY_DENSITY or XY_VPSI
+  const double* c;         // coefficients (device, default order)
+  const void* v;           // V(r): float (mixed) or double (FP64); VPSI only
+  double* rho;             // density grid (DENSITY)
+  const double* w;         // occ/Omega per band (DENSITY)
+  double* hc;              // output H*psi (VPSI)
+  int nst, pair0, npairs;
+  void* zbuf;
+  const double2 *twx, *twy, *twz;
+  int rods_per_cta;        // z kernels
+  int xy_warps;            // requested warps per kxy CTA
+  int density_chunks;      // CTAs per plane in the density pass
+};
+
+template <typename T, int N>
+void run_cubic(Context& ctx, const StagedArgs& a) {
+  using C = typename reg::CT<T>::c;
+  const DeviceSticks& g = ctx.dws;
+  cudaStream_t st = ctx.stream;
+  const int ngw = ctx.wb.ng;
+  const int rpc = a.rods_per_cta;
+  const size_t zs = sizeof(C) * ((size_t)N + (size_t)2 * rpc * pitch(N));
+  dim3 zgrid((g.nrods + rpc - 1) / rpc, a.npairs);
+  QBX_CUDA(cudaFuncSetAttribute(kz_bwd<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zs));
+  {
+    ProfScope ps(ctx, "zfft_bwd");
+    kz_bwd<T, N><<<zgrid, kZThreads, zs, st>>>((const double2*)a.c, ngw, a.nst, a.pair0, g, a.twz,
+                                               (C*)a.zbuf, rpc);
+    QBX_LAUNCHED(ctx);
+  }
+  const int nw = std::min(a.xy_warps, XYThreads<T>::v / 32);
+  if (a.op == XY_DENSITY) {
+    const size_t sm = xy_smem_bytes<T, N, N, XY_DENSITY>(g.ncol, nw);
+    QBX_CUDA(cudaFuncSetAttribute(kxy<T, N, N, XY_DENSITY>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    int chunks = std::max(1, std::min(a.npairs, a.density_chunks));
+    const int ppc = (a.npairs + chunks - 1) / chunks;
+    chunks = (a.npairs + ppc - 1) / ppc;
+    ProfScope ps(ctx, "xy_density");
+    kxy<T, N, N, XY_DENSITY><<<dim3(N, chunks), 32 * nw, sm, st>>>(
+        (C*)a.zbuf, a.npairs, ppc, g, a.twx, a.twy, nullptr, a.rho, a.w, a.pair0, a.nst);
+    QBX_LAUNCHED(ctx);
+    return;
+  }
+  const size_t sm = xy_smem_bytes<T, N, N, XY_VPSI>(g.ncol, nw);
+  QBX_CUDA(cudaFuncSetAttribute(kxy<T, N, N, XY_VPSI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sm));
+  {
+    ProfScope ps(ctx, "xy_vpsi");
+    kxy<T, N, N, XY_VPSI><<<dim3(N, a.npairs), 32 * nw, sm, st>>>(
+        (C*)a.zbuf, a.npairs, 1, g, a.twx, a.twy, (const T*)a.v, nullptr, nullptr, a.pair0, a.nst);
+    QBX_LAUNCHED(ctx);
+  }
+  QBX_CUDA(cudaFuncSetAttribute(kz_fwd<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zs));
+  const double scale = 1.0 / ((double)N * N * N);
+  ProfScope ps(ctx, "zfft_fwd");
+  kz_fwd<T, N><<<zgrid, kZThreads, zs, st>>>((const C*)a.zbuf, ngw, a.nst, a.pair0, g, a.twz, scale,
+                                             (const double2*)a.c, ctx.d_g2_w, (double2*)a.hc, rpc);
+  QBX_LAUNCHED(ctx);
+}
+
+template <typename T, int N>
+size_t smem_need(const Context& ctx, const StagedArgs& a) {
+  const int nw = std::min(a.xy_warps, XYThreads<T>::v / 32);
+  const size_t x = std::max(xy_smem_bytes<T, N, N, XY_DENSITY>(ctx.dws.ncol, nw),
+                            xy_smem_bytes<T, N, N, XY_VPSI>(ctx.dws.ncol, nw));
+  const size_t z = sizeof(typename reg::CT<T>::c) * ((size_t)N + (size_t)2 * a.rods_per_cta * pitch(N));
+  return std::max(x, z);
+}
+
+}  // namespace fast
+
+// Specialised staged transforms for cubic grids of the lengths compiled in
+// fft_fast_a.cu / fft_fast_b.cu; each returns false when it has no kernel
+// for the grid, or when its shared memory would not fit.
+bool fast_staged_a(Context& ctx, const fast::StagedArgs& a, size_t smem_limit);
+bool fast_staged_b(Context& ctx, const fast::StagedArgs& a, size_t smem_limit);
+
+}  // namespace qbx
+
+#define QBX_FAST_CASE(N)                                                      \
+  case N:                                                                     \
+    if (ctx.precision == MIXED) {                                             \
+      if (fast::smem_need<float, N>(ctx, a) > smem_limit) return false;       \
+      fast::run_cubic<float, N>(ctx, a);                                      \
+    } else {                                                                  \
+      if (fast::smem_need<double, N>(ctx, a) > smem_limit) return false;      \
+      fast::run_cubic<double, N>(ctx, a);                                     \
+    }                                                                         \
+    return true;

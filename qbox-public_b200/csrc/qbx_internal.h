@@ -275,9 +275,20 @@ struct Context {
   void* ss_hi = nullptr;        // split of a small matrix (fnl, A, X)
   void* ss_lo = nullptr;
   int ldp = 0;                  // padded leading dimension of the K-row splits
-  float* c32 = nullptr;         // FP32 copy of C (tall updates)
-  float* a32 = nullptr;         // FP32 copy of the projectors
-  float* s32 = nullptr;         // FP32 copy of a small matrix
+  float* c32 = nullptr;         // TF32 hi/lo split of C (tall updates)
+  float* c32lo = nullptr;
+  float* d_vr32 = nullptr;      // FP32 copy of V(r) for the mixed H*psi pass
+  void* d_zfast = nullptr;      // stick buffer of the specialised staged FFTs
+  size_t zfast_bytes = 0;
+  int fast_batch = 0;           // band pairs per launch (0: as many as fit)
+  int fast_rods = 16;           // rods per CTA of the z kernels
+  int fast_warps = 16;          // warps per CTA of the plane kernel
+  int fast_chunks = 8;          // CTAs per plane in the density pass
+  bool fast_fft = true;         // use the specialised kernels when compiled
+  float* a32 = nullptr;         // TF32 hi/lo split of the projectors
+  float* a32lo = nullptr;
+  float* s32 = nullptr;         // TF32 hi/lo split of a small matrix
+  float* s32lo = nullptr;
   void* d_tc_ws = nullptr;      // split-K partials of the tcgen05 GEMM
   size_t tc_ws_elems = 0;
   void* d_tc_err = nullptr;     // wait-timeout flag of the tcgen05 GEMM
@@ -389,9 +400,11 @@ void tc_split_gemm(Context& ctx, bool ta, bool tb, int m, int n, int k, double a
 int tc_check_error(Context& ctx);   // nonzero if a tcgen05 GEMM wait ran out
 void split_bf16_2d(Context& ctx, const double* x, int rows, int cols, int ldx, void* hi, void* lo,
                    int ldp);
-void to_f32(Context& ctx, const double* x, int rows, int cols, int ldx, float* y, int ldy);
-void f32emu_gemm_nn(Context& ctx, int m, int n, int k, double alpha, const float* A, int lda,
-                    const float* B, int ldb, double beta, double* C);
+void split_tf32(Context& ctx, const double* x, int rows, int cols, int ldx, float* hi, float* lo,
+                int ldy);
+void tf32x3_gemm_nn(Context& ctx, int m, int n, int k, double alpha, const float* Ahi,
+                    const float* Alo, int lda, const float* Bhi, const float* Blo, int ldb,
+                    double beta, double* C);
 void alloc_mixed(Context& ctx);
 void free_mixed(Context& ctx);
 

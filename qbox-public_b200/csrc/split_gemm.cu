@@ -126,36 +126,56 @@ void split_gemm(Context& ctx, bool ta, bool tb, int m, int n, int k, double alph
   QBX_LAUNCHED(ctx);
 }
 
-// ---- FP32-accurate products for the tall updates (C A, A_nl F, C (I-X)):
-// FP64 operands rounded to FP32, products on the tensor cores through
-// cuBLAS's BF16x9 emulation of FP32, FP32 result added into the FP64
-// output.  Relative error ~1e-7 per element instead of ~1e-5 for BF16x3.
-__global__ void k_to_f32(const double* __restrict__ x, int rows, int cols, int ldx,
-                         float* __restrict__ y, int ldy) {
+// ---- FP32-accurate products for the tall updates (C A, A_nl F, C (I-X)).
+// An FP64 operand is split into two TF32 values, x ~ hi + lo with
+// hi = tf32(x) and lo = tf32(x - hi) (about 22 significant bits together),
+// and the product is formed from three TF32 tensor-core products
+// accumulated in FP32, A_lo B_hi + A_hi B_lo + A_hi B_hi (the small terms
+// first), then added into the FP64 output: relative error ~3e-7 per element,
+// that of an FP32 product, against ~1e-5 for three BF16 products.
+
+// round an FP32 value to TF32 (10 explicit mantissa bits), nearest with
+// ties away from zero; finite inputs only
+__device__ __forceinline__ float tf32_round(float x) {
+  unsigned u = __float_as_uint(x);
+  u = (u + 0x1000u) & 0xffffe000u;
+  return __uint_as_float(u);
+}
+
+__global__ void k_split_tf32(const double* __restrict__ x, int rows, int cols, int ldx,
+                             float* __restrict__ hi, float* __restrict__ lo, int ldy) {
   const size_t n = (size_t)rows * cols;
   for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n;
        t += (size_t)gridDim.x * blockDim.x) {
     const int c = (int)(t / rows), r = (int)(t - (size_t)c * rows);
-    y[(size_t)c * ldy + r] = (float)x[(size_t)c * ldx + r];
+    const double v = x[(size_t)c * ldx + r];
+    const float h = tf32_round((float)v);
+    hi[(size_t)c * ldy + r] = h;
+    lo[(size_t)c * ldy + r] = tf32_round((float)(v - (double)h));
   }
 }
 
-void to_f32(Context& ctx, const double* x, int rows, int cols, int ldx, float* y, int ldy) {
+void split_tf32(Context& ctx, const double* x, int rows, int cols, int ldx, float* hi, float* lo,
+                int ldy) {
   const size_t n = (size_t)rows * cols;
-  k_to_f32<<<nblocks(n), 256, 0, ctx.stream>>>(x, rows, cols, ldx, y, ldy);
+  k_split_tf32<<<nblocks(n), 256, 0, ctx.stream>>>(x, rows, cols, ldx, hi, lo, ldy);
   QBX_LAUNCHED(ctx);
 }
 
 // C (m x n, ld m) = alpha A B + beta C with A (m x k, ld lda) and B (k x n,
-// ld ldb) given in FP32.
-void f32emu_gemm_nn(Context& ctx, int m, int n, int k, double alpha, const float* A, int lda,
-                    const float* B, int ldb, double beta, double* C) {
+// ld ldb) given as TF32 hi/lo splits.
+void tf32x3_gemm_nn(Context& ctx, int m, int n, int k, double alpha, const float* Ahi,
+                    const float* Alo, int lda, const float* Bhi, const float* Blo, int ldb,
+                    double beta, double* C) {
   float* D = (float*)ctx.d_acc32;
   QBX_REQUIRE((size_t)m * n <= ctx.acc32_elems, 50, "FP32 product accumulator too small");
   const float one = 1.0f, zero = 0.0f;
-  QBX_BLAS(cublasGemmEx(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, m, n, k, &one, A, CUDA_R_32F, lda, B,
-                        CUDA_R_32F, ldb, &zero, D, CUDA_R_32F, m,
-                        CUBLAS_COMPUTE_32F_EMULATED_16BFX9, CUBLAS_GEMM_DEFAULT));
+  const float* as[3] = {Alo, Ahi, Ahi};
+  const float* bs[3] = {Bhi, Blo, Bhi};
+  for (int t = 0; t < 3; t++)
+    QBX_BLAS(cublasGemmEx(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, m, n, k, &one, as[t], CUDA_R_32F,
+                          lda, bs[t], CUDA_R_32F, ldb, t == 0 ? &zero : &one, D, CUDA_R_32F, m,
+                          CUBLAS_COMPUTE_32F_FAST_TF32, CUBLAS_GEMM_DEFAULT));
   const size_t nn = (size_t)m * n;
   k_acc_to_f64<<<nblocks(nn), 256, 0, ctx.stream>>>(D, nn, alpha, beta, C);
   QBX_LAUNCHED(ctx);

@@ -1,0 +1,64 @@
+"""The specialised staged FFTs (fft_fast_*.cu: compile-time lengths,
+warp-synchronous radix stages) against the generic runtime-radix kernels of
+fft.cu and against the oracle, through the C ABI.
+
+QBX_FAST_FFT=0 at qbx_set_cell selects the generic kernels for a context.
+Tolerances: FP64 1e-12 of the largest value (the same arithmetic in another
+order); mixed precision 2e-6 of the largest value.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from qbx import capi, systems
+from oracle import qbox_np
+
+pytestmark = pytest.mark.gpu
+
+
+def _ctx(s, precision, fast):
+    os.environ["QBX_FAST_FFT"] = "1" if fast else "0"
+    try:
+        return capi.from_system(s, precision=precision)
+    finally:
+        os.environ.pop("QBX_FAST_FFT", None)
+
+
+def _run(ctx):
+    ctx.update_density()
+    rho = ctx.density()
+    ctx.update_vhxc()
+    e = ctx.energy(hpsi=True)
+    return rho, ctx.get_hpsi(), e
+
+
+@pytest.mark.parametrize("name", ["si8", "si64", "h2o32"])
+@pytest.mark.parametrize("precision", [capi.FP64, capi.MIXED])
+def test_fast_matches_generic(name, precision):
+    s = systems.get(name)
+    a = _ctx(s, precision, True)
+    b = _ctx(s, precision, False)
+    ra, ha, ea = _run(a)
+    rb, hb, eb = _run(b)
+    tol = 1e-12 if precision == capi.FP64 else 2e-6
+    np.testing.assert_allclose(ra, rb, rtol=0, atol=tol * np.abs(rb).max())
+    np.testing.assert_allclose(ha, hb, rtol=0, atol=tol * np.abs(hb).max())
+    etol = (1e-9 if precision == capi.FP64 else 1e-6) * len(s.atoms)
+    assert abs(ea["etotal"] - eb["etotal"]) < etol
+    a.close()
+    b.close()
+
+
+def test_fast_fp64_matches_oracle_si64():
+    s = systems.si64()
+    es = qbox_np.ElectronicStep(s)
+    es.update_density()
+    es.update_vhxc()
+    es.energy(True)
+    ctx = _ctx(s, capi.FP64, True)
+    rho, hc, e = _run(ctx)
+    np.testing.assert_allclose(rho, es.rhor, rtol=0, atol=1e-12 * np.abs(es.rhor).max())
+    np.testing.assert_allclose(hc, es.hc, rtol=0, atol=1e-11)
+    assert abs(e["etotal"] - es.etotal) < 1e-8
+    ctx.close()

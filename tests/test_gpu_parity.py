@@ -115,7 +115,9 @@ def test_mixed_si64_within_budget(backend):
     same coefficients (the FP64 trajectory's), so the energy difference is
     the error the mixed step itself makes: 1e-6 Ha/atom in the total energy,
     1e-4 Ha/bohr in the forces, and the mixed ortho_align leaves C
-    orthonormal to 1e-7.  (Whole trajectories started from random
+    orthonormal to 1e-6 (its rotation is an FP32-accurate product, so the
+    overlap of the new C is exact to a few FP32 roundings; the next step's
+    overlap Cholesky is FP64).  (Whole trajectories started from random
     coefficients are compared on the 8-atom cell, where they converge; far
     from the ground state the PSDA step amplifies any difference in C to
     first order in the energy.)"""
@@ -132,7 +134,7 @@ def test_mixed_si64_within_budget(backend):
     np.testing.assert_allclose(rb["fion"], ra["fion"], atol=1e-4)
     cb = b.get_coeffs()
     ov = 2.0 * (cb.conj() @ cb.T).real - np.outer(cb[:, 0].real, cb[:, 0].real)
-    assert np.abs(ov - np.eye(s.nbands)).max() < 1e-7
+    assert np.abs(ov - np.eye(s.nbands)).max() < 1e-6
     a.close()
     b.close()
 
