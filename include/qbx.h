@@ -24,6 +24,8 @@
 #ifndef QBX_H
 #define QBX_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -140,6 +142,31 @@ int qbx_set_gemm_backend(qbx_context* ctx, int backend);
  * (tcgen05), for checking the products on their own. */
 int qbx_split_gemm_tn(qbx_context* ctx, int m, int n, int k, const double* a,
                       const double* b, double* d, int backend);
+
+/* Size of the device array behind qbx_density_static: 32 MiB. */
+#define QBX_STATIC_SCRATCH_BYTES ((size_t)32 << 20)
+
+/* No counterpart in the reference.  ChargeDensity-style density of nst bands
+ * for callers that cannot allocate device memory when they need it (code in
+ * a host callback or a plug-in where cudaMalloc is not allowed, or a process
+ * whose device memory another framework has already divided up).  d_c is a
+ * DEVICE array of nst bands (band-major, 2*ngw doubles each, in the default
+ * order of qbx_basis_miller; qbx_set_coeff_order does not apply); d_rho is a
+ * DEVICE array of np0*np1*np2 doubles that receives
+ * sum_n occ_n/Omega |psi_n(r)|^2 (overwritten).  occ is a HOST array of nst
+ * occupations, or NULL for 2 per band.  The z-stick scratch, twiddle and
+ * weight tables come from one static device array of QBX_STATIC_SCRATCH_BYTES
+ * that every GPU loading the library holds until exit; the call allocates
+ * nothing and returns error 62 when one band pair's z-sticks do not fit:
+ * np2 * (2*nrods-1) complex values per pair (FP32 in the mixed precision,
+ * FP64 otherwise) must fit in 31 MiB, about 4 M values in FP32.  The first
+ * call on a device looks up the array's device address
+ * (cudaGetSymbolAddress), so make it before any stream capture.  All calls
+ * share the array and it keeps the last call's contents; calls that overlap
+ * on one GPU race.  Runs on the context's stream and returns after it has
+ * finished. */
+int qbx_density_static(qbx_context* ctx, const double* d_c, int nst,
+                       const double* occ, double* d_rho);
 
 /* Host-only setup helpers (no GPU needed), exposing the same host code the
  * context uses.  Basis::resize + ChargeDensity grid: basis sizes, grid and

@@ -116,6 +116,7 @@ void check_ready(const Context& c, bool atoms) {
 // density weights live after the 16 scalar slots
 namespace qbx {
 double* density_weights(Context& c) { return c.d_scalars + 16; }
+Context& context_of(qbx_context* h) { return h->c; }
 }
 
 extern "C" {

@@ -726,3 +726,59 @@ void wb_backward_pair(Context& ctx, const double* c1, const double* c2, double* 
 }
 
 }  // namespace qbx
+
+namespace qbx {
+
+// Density of nst bands of c (device, default order) added into rho, with the
+// stick buffer and the three twiddle tables supplied by the caller instead
+// of the context's own.  Batches of band pairs are sized to zbuf_bytes.
+template <typename T>
+static void density_buffers_t(Context& ctx, const double* c, int nst, const double* w,
+                              double* rho, void* zbuf, size_t zbuf_bytes, const double2* twx,
+                              const double2* twy, const double2* twz) {
+  using C = typename Cplx<T>::t;
+  const DeviceSticks& g = ctx.dws;
+  cudaStream_t st = ctx.stream;
+  const size_t per_pair = sizeof(C) * (size_t)g.n2 * g.nvec;
+  const int npairs_all = (nst + 1) / 2;
+  const int batch = (int)std::min<size_t>(npairs_all, zbuf_bytes / per_pair);
+  QBX_REQUIRE(batch >= 1, 60, "stick buffer smaller than one band pair");
+  const size_t zs = zsmem<T>(g.n2);
+  QBX_CUDA(cudaFuncSetAttribute(k_zfft_bwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zs));
+  XYConfig<T> xc = xy_config<T>(g, ctx.device);
+  QBX_CUDA(cudaFuncSetAttribute(k_xy<T, OP_DENSITY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)xc.smem));
+  int sms = 0;
+  QBX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device));
+  for (int p0 = 0; p0 < npairs_all; p0 += batch) {
+    const int npairs = std::min(batch, npairs_all - p0);
+    dim3 zgrid((g.nrods + kRodsPerCta - 1) / kRodsPerCta, npairs);
+    k_zfft_bwd<T><<<zgrid, 256, zs, st>>>((const double2*)c, ctx.wb.ng, nst, p0, g, twz, (C*)zbuf,
+                                           kRodsPerCta);
+    QBX_LAUNCHED(ctx);
+    int chunks = std::max(1, (3 * sms + g.n2 - 1) / g.n2);
+    chunks = std::min(chunks, npairs);
+    const int ppc = (npairs + chunks - 1) / chunks;
+    chunks = (npairs + ppc - 1) / ppc;
+    dim3 xgrid(g.n2, chunks);
+    k_xy<T, OP_DENSITY><<<xgrid, 512, xc.smem, st>>>((C*)zbuf, npairs, ppc, g, twx, twy, nullptr,
+                                                     rho, w, p0, nst, xc.cc, xc.rr);
+    QBX_LAUNCHED(ctx);
+  }
+}
+
+size_t density_stick_bytes_per_pair(const Context& ctx) {
+  const size_t e = ctx.precision == MIXED ? sizeof(float2) : sizeof(double2);
+  return e * (size_t)ctx.dws.n2 * ctx.dws.nvec;
+}
+
+void density_with_buffers(Context& ctx, const double* c, int nst, const double* w, double* rho,
+                          void* zbuf, size_t zbuf_bytes, const double2* twx, const double2* twy,
+                          const double2* twz) {
+  if (ctx.precision == MIXED)
+    density_buffers_t<float>(ctx, c, nst, w, rho, zbuf, zbuf_bytes, twx, twy, twz);
+  else
+    density_buffers_t<double>(ctx, c, nst, w, rho, zbuf, zbuf_bytes, twx, twy, twz);
+}
+
+}  // namespace qbx

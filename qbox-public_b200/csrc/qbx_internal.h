@@ -409,3 +409,12 @@ void alloc_mixed(Context& ctx);
 void free_mixed(Context& ctx);
 
 }  // namespace qbx
+
+namespace qbx {
+// Density pass with caller-supplied stick buffer and twiddle tables
+// (exp(+2 pi i k/n) for the x, y and z lengths); adds into rho.
+size_t density_stick_bytes_per_pair(const Context& ctx);
+void density_with_buffers(Context& ctx, const double* c, int nst, const double* w, double* rho,
+                          void* zbuf, size_t zbuf_bytes, const double2* twx, const double2* twy,
+                          const double2* twz);
+}  // namespace qbx

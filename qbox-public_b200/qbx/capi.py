@@ -35,7 +35,7 @@ SYMBOLS = (
     "qbx_scf_step", "qbx_ft_backward_pair", "qbx_synchronize",
     "qbx_host_basis", "qbx_host_species_eval", "qbx_host_esr",
     "qbx_profile", "qbx_profile_get", "qbx_launch_count", "qbx_stream",
-    "qbx_set_gemm_backend", "qbx_split_gemm_tn",
+    "qbx_set_gemm_backend", "qbx_split_gemm_tn", "qbx_density_static",
 )
 
 _lib = None
@@ -98,6 +98,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "qbx_stream": (_P, [_P]),
         "qbx_set_gemm_backend": (_I, [_P, _I]),
         "qbx_split_gemm_tn": (_I, [_P, _I, _I, _I, _DP, _DP, _DP, _I]),
+        "qbx_density_static": (_I, [_P, ctypes.c_void_p, _I, _DP, ctypes.c_void_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -303,6 +304,16 @@ class Context:
         self._ok(self.lib.qbx_split_gemm_tn(self.h, m, n, k, _dp(at), _dp(bt), _dp(out),
                                             backend), "split_gemm_tn")
         return out.T
+
+    def density_static(self, c_dev_ptr: int, nst: int, rho_dev_ptr: int,
+                       occ: Optional[np.ndarray] = None):
+        """qbx_density_static: density of nst bands held in device memory
+        (default coefficient order) into a device grid, using the library's
+        static scratch array; pointers are raw device addresses."""
+        o = None if occ is None else np.ascontiguousarray(occ, dtype=float)
+        self._ok(self.lib.qbx_density_static(self.h, ctypes.c_void_p(c_dev_ptr), nst,
+                                             _dp(o), ctypes.c_void_p(rho_dev_ptr)),
+                 "density_static")
 
     def stream(self) -> int:
         return self.lib.qbx_stream(self.h)
