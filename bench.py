@@ -337,13 +337,32 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_profile_case(args):
+    """A small case for ncu captures: warm-up plus one mixed electronic step
+    of the 512-atom cell with a band sample (the per-launch work of the plane
+    kernels is that of the full run; the device holds a few GB)."""
+    from qbx import capi, systems
+    s = systems.si512().band_sample(args.profile_bands)
+    ctx = capi.from_system(s, precision=capi.MIXED)
+    for _ in range(args.warmup + 1):
+        ctx.scf_step()
+    ctx.synchronize()
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--profile-bands", type=int, default=0,
+                    help="run only warm-up + one mixed step of si512 with this many bands "
+                         "(a small case for profilers); prints nothing")
     args = ap.parse_args()
+    if args.profile_bands:
+        run_profile_case(args)
+        return
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -404,7 +404,8 @@ void split_tf32(Context& ctx, const double* x, int rows, int cols, int ldx, floa
                 int ldy);
 void tf32x3_gemm_nn(Context& ctx, int m, int n, int k, double alpha, const float* Ahi,
                     const float* Alo, int lda, const float* Bhi, const float* Blo, int ldb,
-                    double beta, double* C);
+                    double beta, double* C, int ldc);
+inline int pad4(int n) { return (n + 3) / 4 * 4; }
 void alloc_mixed(Context& ctx);
 void free_mixed(Context& ctx);
 

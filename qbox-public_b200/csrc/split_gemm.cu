@@ -162,22 +162,37 @@ void split_tf32(Context& ctx, const double* x, int rows, int cols, int ldx, floa
   QBX_LAUNCHED(ctx);
 }
 
-// C (m x n, ld m) = alpha A B + beta C with A (m x k, ld lda) and B (k x n,
-// ld ldb) given as TF32 hi/lo splits.
+// out (rows x cols, ld ldo) = alpha * acc (ld lda) + beta * out
+__global__ void k_acc2d_to_f64(const float* __restrict__ acc, int lda, int rows, int cols,
+                               double alpha, double beta, double* __restrict__ out, int ldo) {
+  const size_t n = (size_t)rows * cols;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const int c = (int)(t / rows), r = (int)(t - (size_t)c * rows);
+    double* o = out + (size_t)c * ldo + r;
+    *o = alpha * (double)acc[(size_t)c * lda + r] + (beta != 0.0 ? beta * *o : 0.0);
+  }
+}
+
+// C (m x n, ld ldc) = alpha A B + beta C with A (m x k, ld lda) and B (k x n,
+// ld ldb) given as TF32 hi/lo splits.  Leading dimensions of the FP32
+// operands should be multiples of 4 (16-byte rows) for the fast TF32
+// kernels; the FP32 product is kept with ld = m rounded up to 4.
 void tf32x3_gemm_nn(Context& ctx, int m, int n, int k, double alpha, const float* Ahi,
                     const float* Alo, int lda, const float* Bhi, const float* Blo, int ldb,
-                    double beta, double* C) {
+                    double beta, double* C, int ldc) {
   float* D = (float*)ctx.d_acc32;
-  QBX_REQUIRE((size_t)m * n <= ctx.acc32_elems, 50, "FP32 product accumulator too small");
+  const int ldd = (m + 3) / 4 * 4;
+  QBX_REQUIRE((size_t)ldd * n <= ctx.acc32_elems, 50, "FP32 product accumulator too small");
   const float one = 1.0f, zero = 0.0f;
   const float* as[3] = {Alo, Ahi, Ahi};
   const float* bs[3] = {Bhi, Blo, Bhi};
   for (int t = 0; t < 3; t++)
     QBX_BLAS(cublasGemmEx(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, m, n, k, &one, as[t], CUDA_R_32F,
-                          lda, bs[t], CUDA_R_32F, ldb, t == 0 ? &zero : &one, D, CUDA_R_32F, m,
+                          lda, bs[t], CUDA_R_32F, ldb, t == 0 ? &zero : &one, D, CUDA_R_32F, ldd,
                           CUBLAS_COMPUTE_32F_FAST_TF32, CUBLAS_GEMM_DEFAULT));
   const size_t nn = (size_t)m * n;
-  k_acc_to_f64<<<nblocks(nn), 256, 0, ctx.stream>>>(D, nn, alpha, beta, C);
+  k_acc2d_to_f64<<<nblocks(nn), 256, 0, ctx.stream>>>(D, ldd, m, n, alpha, beta, C, ldc);
   QBX_LAUNCHED(ctx);
 }
 

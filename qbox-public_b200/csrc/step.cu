@@ -130,9 +130,10 @@ void ortho_align(Context& ctx) {
     // correction, so C stays orthonormal to the accuracy of the overlap.
     double* T = ctx.d_nn3;
     launch_identity_axpy(ctx, T, X, n, -1.0);
-    split_tf32(ctx, T, n, n, n, ctx.s32, ctx.s32lo, n);
-    split_tf32(ctx, ctx.d_c, K, n, K, ctx.c32, ctx.c32lo, K);
-    tf32x3_gemm_nn(ctx, K, n, n, -1.0, ctx.c32, ctx.c32lo, K, ctx.s32, ctx.s32lo, n, 1.0, ctx.d_c);
+    split_tf32(ctx, T, n, n, n, ctx.s32, ctx.s32lo, pad4(n));
+    split_tf32(ctx, ctx.d_c, K, n, K, ctx.c32, ctx.c32lo, ctx.ldp);
+    tf32x3_gemm_nn(ctx, K, n, n, -1.0, ctx.c32, ctx.c32lo, ctx.ldp, ctx.s32, ctx.s32lo, pad4(n),
+                   1.0, ctx.d_c, K);
   } else {
     QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, K, n, n, &one, ctx.d_ctmp, K, X, n,
                          &zero, ctx.d_c, K));
@@ -177,9 +178,9 @@ static void nonlocal(Context& ctx, bool hpsi) {
   if (hpsi) {
     ProfScope ps(ctx, "gemm_nl_apply");
     if (mx) {
-      split_tf32(ctx, ctx.d_fnl, np, n, np, ctx.s32, ctx.s32lo, np);
-      tf32x3_gemm_nn(ctx, K, n, np, 1.0, ctx.a32, ctx.a32lo, K, ctx.s32, ctx.s32lo, np, 1.0,
-                     ctx.d_hc);
+      split_tf32(ctx, ctx.d_fnl, np, n, np, ctx.s32, ctx.s32lo, pad4(np));
+      tf32x3_gemm_nn(ctx, K, n, np, 1.0, ctx.a32, ctx.a32lo, ctx.ldp, ctx.s32, ctx.s32lo, pad4(np),
+                     1.0, ctx.d_hc, K);
     } else {
       QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, K, n, np, &one, ctx.d_anl, K,
                            ctx.d_fnl, np, &one, ctx.d_hc, K));
@@ -230,10 +231,10 @@ void psda_update(Context& ctx) {
       split_gemm(ctx, true, false, n, n, K, 2.0, ctx.cs_hi[0], ctx.cs_lo[0], ctx.ldp, ctx.hs_hi,
                  ctx.hs_lo, ctx.ldp, 0.0, A);
       launch_rank1_fix(ctx, A, n, ctx.d_c, K, ctx.d_hc, K, n, n, -1.0, false);
-      split_tf32(ctx, A, n, n, n, ctx.s32, ctx.s32lo, n);
-      split_tf32(ctx, ctx.d_c, K, n, K, ctx.c32, ctx.c32lo, K);
-      tf32x3_gemm_nn(ctx, K, n, n, -1.0, ctx.c32, ctx.c32lo, K, ctx.s32, ctx.s32lo, n, 1.0,
-                     ctx.d_hc);
+      split_tf32(ctx, A, n, n, n, ctx.s32, ctx.s32lo, pad4(n));
+      split_tf32(ctx, ctx.d_c, K, n, K, ctx.c32, ctx.c32lo, ctx.ldp);
+      tf32x3_gemm_nn(ctx, K, n, n, -1.0, ctx.c32, ctx.c32lo, ctx.ldp, ctx.s32, ctx.s32lo, pad4(n),
+                     1.0, ctx.d_hc, K);
     } else {
       QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, ctx.d_c, K, ctx.d_hc,
                            K, &zero, A, n));
@@ -283,18 +284,19 @@ void alloc_mixed(Context& ctx) {
   QBX_CUDA(cudaMalloc(&ctx.hs_lo, wf * 2));
   QBX_CUDA(cudaMalloc(&ctx.ss_hi, std::max<size_t>(small, 1) * 2));
   QBX_CUDA(cudaMalloc(&ctx.ss_lo, std::max<size_t>(small, 1) * 2));
-  ctx.c32 = dalloc<float>(K * n);
-  ctx.c32lo = dalloc<float>(K * n);
-  ctx.s32 = dalloc<float>(std::max<size_t>(small, 1));
-  ctx.s32lo = dalloc<float>(std::max<size_t>(small, 1));
+  ctx.c32 = dalloc<float>((size_t)ctx.ldp * n);
+  ctx.c32lo = dalloc<float>((size_t)ctx.ldp * n);
+  const size_t small4 = std::max<size_t>((size_t)pad4((int)std::max(np, n)) * n, 1);
+  ctx.s32 = dalloc<float>(small4);
+  ctx.s32lo = dalloc<float>(small4);
   if (np) {
     QBX_CUDA(cudaMalloc(&ctx.as_hi, (size_t)ctx.ldp * np * 2));
     QBX_CUDA(cudaMalloc(&ctx.as_lo, (size_t)ctx.ldp * np * 2));
-    ctx.a32 = dalloc<float>(K * np);
-    ctx.a32lo = dalloc<float>(K * np);
+    ctx.a32 = dalloc<float>((size_t)ctx.ldp * np);
+    ctx.a32lo = dalloc<float>((size_t)ctx.ldp * np);
     if (ctx.d_anl) {
       split_bf16_2d(ctx, ctx.d_anl, (int)K, (int)np, (int)K, ctx.as_hi, ctx.as_lo, ctx.ldp);
-      split_tf32(ctx, ctx.d_anl, (int)K, (int)np, (int)K, ctx.a32, ctx.a32lo, (int)K);
+      split_tf32(ctx, ctx.d_anl, (int)K, (int)np, (int)K, ctx.a32, ctx.a32lo, ctx.ldp);
     }
   }
   QBX_CUDA(cudaStreamSynchronize(ctx.stream));

@@ -38,7 +38,8 @@ constexpr int TILE_BYTES = BM * BK * 2;           // 16 KB per operand tile
 constexpr int STAGE_BYTES = 4 * TILE_BYTES;       // A_hi, A_lo, B_hi, B_lo
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /* align */ + 256 /* barriers */;
 constexpr int THREADS = 256;
-constexpr uint32_t TMEM_COLS = 128;
+constexpr uint32_t TMEM_COLS = 2 * BN;           // two accumulators, used in turn
+constexpr int CHUNK = 8;                          // K blocks per accumulator fill
 constexpr long long WAIT_LIMIT = 1ll << 24;       // bounded spins per wait
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -104,6 +105,10 @@ __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t
       : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 __device__ __forceinline__ void umma_commit(uint64_t* bar) {
   asm volatile(
       "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
@@ -111,6 +116,12 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
       : "memory");
 }
 
+// Accumulation: the MMA warp fills one of two 128-column TMEM accumulators
+// with CHUNK K blocks (512 products of each split term per element) and
+// commits it; the epilogue warps add that accumulator into FP32 registers
+// and hand it back, while the MMA warp fills the other one.  FP32 chains
+// thus stay short (CHUNK*4 MMA steps in TMEM, then one register add per
+// chunk) instead of one TMEM chain over the whole K slice.
 __global__ void __launch_bounds__(THREADS, 1)
 k_tc_split_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant__ CUtensorMap ma_lo,
                 const __grid_constant__ CUtensorMap mb_hi, const __grid_constant__ CUtensorMap mb_lo,
@@ -120,23 +131,26 @@ k_tc_split_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant
   unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint64_t* full = (uint64_t*)(base + STAGES * STAGE_BYTES);
   uint64_t* empty = full + STAGES;
-  uint64_t* accum = empty + STAGES;
-  uint32_t* tmem_slot = (uint32_t*)(accum + 1);
-  __shared__ int s_fail;
+  uint64_t* tfull = empty + STAGES;      // accumulator b filled
+  uint64_t* tfree = tfull + 2;           // accumulator b drained by the epilogue
+  uint32_t* tmem_slot = (uint32_t*)(tfree + 2);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
   const int kb0 = blockIdx.z * kb_per_split;
   const int kb1 = min(nkb, kb0 + kb_per_split);
   const int niter = max(0, kb1 - kb0);
+  const int nchunk = (niter + CHUNK - 1) / CHUNK;
 
   if (threadIdx.x == 0) {
-    s_fail = 0;
     for (int s = 0; s < STAGES; s++) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(accum, 1);
+    for (int b = 0; b < 2; b++) {
+      mbar_init(&tfull[b], 1);
+      mbar_init(&tfree[b], 4);           // one arrival per epilogue warp
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) {
@@ -155,7 +169,7 @@ k_tc_split_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant
     for (int it = 0; it < niter; ++it) {
       const int s = it % STAGES;
       const uint32_t ph = (uint32_t)((it / STAGES) & 1);
-      if (!mbar_wait(&empty[s], ph ^ 1u)) { atomicExch(err, 1); s_fail = 1; break; }
+      if (!mbar_wait(&empty[s], ph ^ 1u)) { atomicExch(err, 1); break; }
       unsigned char* st = base + s * STAGE_BYTES;
       mbar_expect_tx(&full[s], STAGE_BYTES);
       const int kx = (kb0 + it) * BK;
@@ -167,61 +181,76 @@ k_tc_split_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant
   } else if (warp == 1 && lane == 0) {
     // ---------------- MMA issuer
     for (int it = 0; it < niter; ++it) {
+      const int c = it / CHUNK, b = c & 1;
+      const bool chunk_start = (it % CHUNK) == 0;
+      if (chunk_start && c >= 2 && !mbar_wait(&tfree[b], (uint32_t)(((c >> 1) - 1) & 1))) {
+        atomicExch(err, 4);
+        break;
+      }
       const int s = it % STAGES;
       const uint32_t ph = (uint32_t)((it / STAGES) & 1);
-      if (!mbar_wait(&full[s], ph)) { atomicExch(err, 2); s_fail = 1; break; }
+      if (!mbar_wait(&full[s], ph)) { atomicExch(err, 2); break; }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       unsigned char* st = base + s * STAGE_BYTES;
       const uint64_t dah = smem_desc(st + 0 * TILE_BYTES);
       const uint64_t dal = smem_desc(st + 1 * TILE_BYTES);
       const uint64_t dbh = smem_desc(st + 2 * TILE_BYTES);
       const uint64_t dbl = smem_desc(st + 3 * TILE_BYTES);
+      const uint32_t tacc = tmem + (uint32_t)(b * BN);
 #pragma unroll
       for (int k = 0; k < BK / 16; ++k) {
         const uint64_t off = (uint64_t)(k * 32) >> 4;      // 16 BF16 = 32 bytes
-        const uint32_t first = (it == 0 && k == 0) ? 0u : 1u;
-        umma_bf16(tmem, dah + off, dbh + off, first);
-        umma_bf16(tmem, dah + off, dbl + off, 1u);
-        umma_bf16(tmem, dal + off, dbh + off, 1u);
+        const uint32_t accumulate = (chunk_start && k == 0) ? 0u : 1u;
+        umma_bf16(tacc, dah + off, dbh + off, accumulate);
+        umma_bf16(tacc, dah + off, dbl + off, 1u);
+        umma_bf16(tacc, dal + off, dbh + off, 1u);
       }
       umma_commit(&empty[s]);
+      if ((it % CHUNK) == CHUNK - 1 || it == niter - 1) umma_commit(&tfull[b]);
     }
-    umma_commit(accum);
   } else if (warp >= 4) {
-    // ---------------- epilogue
+    // ---------------- epilogue: drain each chunk into FP32 registers
     const int wq = warp - 4;                       // TMEM lanes 32*wq .. 32*wq+31
     const int row = m0 + wq * 32 + lane;
-    const bool ok = mbar_wait(accum, 0u);
-    if (!ok) { atomicExch(err, 3); s_fail = 1; }
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    float acc[BN];
+#pragma unroll
+    for (int j = 0; j < BN; ++j) acc[j] = 0.0f;
+    bool ok = true;
+    for (int c = 0; c < nchunk && ok; ++c) {
+      const int b = c & 1;
+      if (!mbar_wait(&tfull[b], (uint32_t)((c >> 1) & 1))) {
+        atomicExch(err, 3);
+        ok = false;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+      for (int c0 = 0; c0 < BN; c0 += 16) {
+        uint32_t r[16];
+        const uint32_t taddr = tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)(b * BN + c0);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+            "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+              "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+              "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int j = 0; j < 16; ++j) acc[c0 + j] += __uint_as_float(r[j]);
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tfree[b]);
+    }
     float* out = ws + (size_t)blockIdx.z * M * N;
-#pragma unroll 1
-    for (int c0 = 0; c0 < BN; c0 += 16) {
-      uint32_t r[16];
-      const uint32_t taddr = tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)c0;
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-          "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
-            "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
-            "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-          : "r"(taddr));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (ok && niter > 0 && row < M) {
+    if (row < M) {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const int col = n0 + c0 + j;
-          if (col < N) out[(size_t)col * M + row] = __uint_as_float(r[j]);
-        }
-      } else if (row < M) {
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const int col = n0 + c0 + j;
-          if (col < N) out[(size_t)col * M + row] = 0.0f;
-        }
+      for (int j = 0; j < BN; ++j) {
+        const int col = n0 + j;
+        if (col < N) out[(size_t)col * M + row] = ok ? acc[j] : 0.0f;
       }
     }
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   }
   __syncthreads();
   if (warp == 1) {
