@@ -265,6 +265,8 @@ int qbx_set_cell(qbx_context* h, const double cell[9], double ecut, int nst, con
       if (const char* e = std::getenv("QBX_FAST_RODS")) c.fast_rods = std::max(1, std::min(32, std::atoi(e)));
       if (const char* e = std::getenv("QBX_FAST_CHUNKS")) c.fast_chunks = std::max(1, std::atoi(e));
       if (const char* e = std::getenv("QBX_FAST_BATCH")) c.fast_batch = std::max(0, std::atoi(e));
+      if (const char* e = std::getenv("QBX_FAST_VPSI_THREADS"))
+        c.fast_vpsi_threads = std::atoi(e) == 512 ? 512 : 256;
     }
     c.species.clear();
     c.tau.clear();

@@ -30,6 +30,7 @@
 #pragma once
 
 #include <algorithm>
+#include <type_traits>
 
 #include "fft_reg.cuh"
 #include "qbx_internal.h"
@@ -42,10 +43,14 @@ using reg::BufStore;
 using reg::cmk;
 
 constexpr int kZThreads = 256;
-// CTA size of the plane kernel: FP64 lines need about twice the registers
-// of FP32 lines in the radix-7/11 stages
-template <typename T> struct XYThreads { static constexpr int v = 512; };
-template <> struct XYThreads<double> { static constexpr int v = 256; };
+// CTA shapes of the plane kernel (threads, CTAs per SM it is compiled for).
+// FP64 lines need about twice the registers of FP32 lines; the FP32 density
+// pass holds an FP32 plane in shared memory, so one CTA per SM; the FP32
+// H*psi pass comes in two shapes, one 512-thread CTA or two 256-thread CTAs
+// per SM, picked at run time.
+template <typename T, int OP> struct XYDefault { static constexpr int th = 256; };
+template <> struct XYDefault<float, 0> { static constexpr int th = 512; };
+__host__ __device__ constexpr int xy_minblocks(int th) { return th == 256 ? 2 : 1; }
 
 template <typename C>
 __device__ __forceinline__ void load_tw(C* dst, const double2* src, int n) {
@@ -186,8 +191,8 @@ __host__ size_t xy_smem_bytes(int ncol, int nwarps) {
 
 // shared memory: [twx N0][twy N1][P ncol x pitch(N1)][one line of N0 per
 // warp][FP32 density plane N1 x N0, mixed density only][xmap N0 ints]
-template <typename T, int N0, int N1, int OP>
-__global__ void __launch_bounds__(XYThreads<T>::v)
+template <typename T, int N0, int N1, int OP, int TH>
+__global__ void __launch_bounds__(TH, xy_minblocks(TH))
 kxy(typename reg::CT<T>::c* __restrict__ zbuf, int npairs, int pairs_per_cta, DeviceSticks g,
     const double2* __restrict__ twx_g, const double2* __restrict__ twy_g,
     const T* __restrict__ v, double* __restrict__ rho, const double* __restrict__ w, int pair0,
@@ -215,6 +220,7 @@ kxy(typename reg::CT<T>::c* __restrict__ zbuf, int npairs, int pairs_per_cta, De
   for (int cidx = threadIdx.x; cidx < ncol; cidx += blockDim.x) xmap[g.col_x[cidx]] = cidx;
   const int pbeg = blockIdx.y * pairs_per_cta;
   const int pend = min(npairs, pbeg + pairs_per_cta);
+  #pragma unroll 1
   for (int pl = pbeg; pl < pend; ++pl) {
     C* zp = zbuf + ((size_t)pl * g.n2 + z) * nvec;
     // tile: zero, then scatter the plane's sticks
@@ -224,6 +230,7 @@ kxy(typename reg::CT<T>::c* __restrict__ zbuf, int npairs, int pairs_per_cta, De
       P[g.stick_col[s] * LD + g.stick_y[s]] = zp[s];
     __syncthreads();
     // backward y, in place, one warp per occupied column
+    #pragma unroll 1
     for (int cidx = warp; cidx < ncol; cidx += nw) {
       C* col = P + cidx * LD;
       reg::warp_fft<N1, +1>(col, twy, lane, BufLoad<C>{col}, BufStore<C>{col});
@@ -236,6 +243,7 @@ kxy(typename reg::CT<T>::c* __restrict__ zbuf, int npairs, int pairs_per_cta, De
       w2 = (b1 + 1 < nst) ? w[b1 + 1] : 0.0;
     }
     // x rows, one warp per row; the first stage reads the row out of P
+    #pragma unroll 1
     for (int y = warp; y < N1; y += nw) {
       auto ldP = [&](int x) -> C {
         const int cidx = xmap[x];
@@ -258,24 +266,36 @@ kxy(typename reg::CT<T>::c* __restrict__ zbuf, int npairs, int pairs_per_cta, De
           reg::warp_fft<N0, +1>(line, twx, lane, ldP, st);
         }
       } else {
+        // V(r) of this row, prefetched in the order the forward transform's
+        // first stage reads the row, multiplied in as it loads
+        using FS = reg::FirstStage<N0>;
         const T* vrow = v + rowbase;
-        auto stv = [&](int x, C val) {
-          const T vv = vrow[x];
-          val.x *= vv;
-          val.y *= vv;
-          line[x] = val;
+        T vpre[FS::RD][FS::R];
+#pragma unroll
+        for (int rd = 0; rd < FS::RD; ++rd)
+#pragma unroll
+          for (int q = 0; q < FS::R; ++q) {
+            const int i = lane + 32 * rd;
+            vpre[rd][q] = (FS::NB % 32 == 0 || i < FS::NB) ? vrow[i + q * FS::NB] : T(0);
+          }
+        reg::warp_fft<N0, +1>(line, twx, lane, ldP, BufStore<C>{line});
+        auto ldv = [&](int rd, int q, int i) -> C {
+          C val = line[i];
+          val.x *= vpre[rd][q];
+          val.y *= vpre[rd][q];
+          return val;
         };
-        reg::warp_fft<N0, +1>(line, twx, lane, ldP, stv);
         auto stP = [&](int x, C val) {
           const int cidx = xmap[x];
           if (cidx >= 0) P[cidx * LD + y] = val;
         };
-        reg::warp_fft<N0, -1>(line, twx, lane, BufLoad<C>{line}, stP);
+        reg::warp_fft_rq<N0, -1>(line, twx, lane, ldv, stP);
       }
     }
     __syncthreads();
     if (OP == XY_VPSI) {
-      for (int cidx = warp; cidx < ncol; cidx += nw) {
+      #pragma unroll 1
+    for (int cidx = warp; cidx < ncol; cidx += nw) {
         C* col = P + cidx * LD;
         reg::warp_fft<N1, -1>(col, twy, lane, BufLoad<C>{col}, BufStore<C>{col});
       }
@@ -306,8 +326,22 @@ struct StagedArgs {
   const double2 *twx, *twy, *twz;
   int rods_per_cta;        // z kernels
   int xy_warps;            // requested warps per kxy CTA
+  int vpsi_threads;        // FP32 H*psi plane CTA: 256 (two per SM) or 512
   int density_chunks;      // CTAs per plane in the density pass
 };
+
+template <typename T, int N, int TH>
+void launch_vpsi_xy(Context& ctx, const StagedArgs& a) {
+  using C = typename reg::CT<T>::c;
+  const DeviceSticks& g = ctx.dws;
+  const int nw = std::min(a.xy_warps, TH / 32);
+  const size_t sm = xy_smem_bytes<T, N, N, XY_VPSI>(g.ncol, nw);
+  QBX_CUDA(cudaFuncSetAttribute(kxy<T, N, N, XY_VPSI, TH>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  kxy<T, N, N, XY_VPSI, TH><<<dim3(N, a.npairs), 32 * nw, sm, ctx.stream>>>(
+      (C*)a.zbuf, a.npairs, 1, g, a.twx, a.twy, (const T*)a.v, nullptr, nullptr, a.pair0, a.nst);
+  QBX_LAUNCHED(ctx);
+}
 
 template <typename T, int N>
 void run_cubic(Context& ctx, const StagedArgs& a) {
@@ -325,28 +359,27 @@ void run_cubic(Context& ctx, const StagedArgs& a) {
                                                (C*)a.zbuf, rpc);
     QBX_LAUNCHED(ctx);
   }
-  const int nw = std::min(a.xy_warps, XYThreads<T>::v / 32);
   if (a.op == XY_DENSITY) {
+    constexpr int TH = XYDefault<T, XY_DENSITY>::th;
+    const int nw = std::min(a.xy_warps, TH / 32);
     const size_t sm = xy_smem_bytes<T, N, N, XY_DENSITY>(g.ncol, nw);
-    QBX_CUDA(cudaFuncSetAttribute(kxy<T, N, N, XY_DENSITY>,
+    QBX_CUDA(cudaFuncSetAttribute(kxy<T, N, N, XY_DENSITY, TH>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     int chunks = std::max(1, std::min(a.npairs, a.density_chunks));
     const int ppc = (a.npairs + chunks - 1) / chunks;
     chunks = (a.npairs + ppc - 1) / ppc;
     ProfScope ps(ctx, "xy_density");
-    kxy<T, N, N, XY_DENSITY><<<dim3(N, chunks), 32 * nw, sm, st>>>(
+    kxy<T, N, N, XY_DENSITY, TH><<<dim3(N, chunks), 32 * nw, sm, st>>>(
         (C*)a.zbuf, a.npairs, ppc, g, a.twx, a.twy, nullptr, a.rho, a.w, a.pair0, a.nst);
     QBX_LAUNCHED(ctx);
     return;
   }
-  const size_t sm = xy_smem_bytes<T, N, N, XY_VPSI>(g.ncol, nw);
-  QBX_CUDA(cudaFuncSetAttribute(kxy<T, N, N, XY_VPSI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)sm));
   {
     ProfScope ps(ctx, "xy_vpsi");
-    kxy<T, N, N, XY_VPSI><<<dim3(N, a.npairs), 32 * nw, sm, st>>>(
-        (C*)a.zbuf, a.npairs, 1, g, a.twx, a.twy, (const T*)a.v, nullptr, nullptr, a.pair0, a.nst);
-    QBX_LAUNCHED(ctx);
+    if (std::is_same<T, float>::value && a.vpsi_threads == 512)
+      launch_vpsi_xy<T, N, 512>(ctx, a);
+    else
+      launch_vpsi_xy<T, N, 256>(ctx, a);
   }
   QBX_CUDA(cudaFuncSetAttribute(kz_fwd<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zs));
   const double scale = 1.0 / ((double)N * N * N);
@@ -358,9 +391,10 @@ void run_cubic(Context& ctx, const StagedArgs& a) {
 
 template <typename T, int N>
 size_t smem_need(const Context& ctx, const StagedArgs& a) {
-  const int nw = std::min(a.xy_warps, XYThreads<T>::v / 32);
-  const size_t x = std::max(xy_smem_bytes<T, N, N, XY_DENSITY>(ctx.dws.ncol, nw),
-                            xy_smem_bytes<T, N, N, XY_VPSI>(ctx.dws.ncol, nw));
+  const int nwd = std::min(a.xy_warps, XYDefault<T, XY_DENSITY>::th / 32);
+  const int nwv = std::min(a.xy_warps, (std::is_same<T, float>::value ? a.vpsi_threads : 256) / 32);
+  const size_t x = std::max(xy_smem_bytes<T, N, N, XY_DENSITY>(ctx.dws.ncol, nwd),
+                            xy_smem_bytes<T, N, N, XY_VPSI>(ctx.dws.ncol, nwv));
   const size_t z = sizeof(typename reg::CT<T>::c) * ((size_t)N + (size_t)2 * a.rods_per_cta * pitch(N));
   return std::max(x, z);
 }

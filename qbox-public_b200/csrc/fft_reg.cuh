@@ -24,6 +24,8 @@
 
 #include <cuda_runtime.h>
 
+#include <cstdint>
+
 namespace qbx {
 namespace reg {
 
@@ -160,15 +162,51 @@ template <typename C> struct BufStore {
   __device__ __forceinline__ void operator()(int i, C v) const { b[i] = v; }
 };
 
+// ------------------------------------------------------------ shared memory
+// The working line and the twiddle table are addressed through 32-bit
+// shared-window offsets that the optimiser cannot see through (see
+// warp_fft), with explicit ld/st.shared.
+__device__ __forceinline__ float2 lds(uint32_t a, float2*) {
+  float2 v;
+  asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ double2 lds(uint32_t a, double2*) {
+  double2 v;
+  asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ void sts(uint32_t a, float2 v) {
+  asm volatile("st.shared.v2.f32 [%0], {%1, %2};" ::"r"(a), "f"(v.x), "f"(v.y) : "memory");
+}
+__device__ __forceinline__ void sts(uint32_t a, double2 v) {
+  asm volatile("st.shared.v2.f64 [%0], {%1, %2};" ::"r"(a), "d"(v.x), "d"(v.y) : "memory");
+}
+__device__ __forceinline__ void warp_sync_mem() {
+  asm volatile("" ::: "memory");
+  __syncwarp();
+  asm volatile("" ::: "memory");
+}
+
 // ------------------------------------------------------------ stages
+// First-stage geometry of a length-N line: lane + 32*rd is the butterfly,
+// q its input; input index = butterfly + q * NB.
+template <int N> struct FirstStage {
+  static constexpr int R = stage_radix(N, 0);
+  static constexpr int NB = N / R;
+  static constexpr int RD = (NB + 31) / 32;
+};
+
 template <int N, int S, int DIR, typename C, typename LD, typename ST>
-__device__ __forceinline__ void wstage(C* buf, const C* tw, int lane, const LD& ld, const ST& st) {
+__device__ __forceinline__ void wstage(uint32_t sbuf, uint32_t stw, int lane, const LD& ld,
+                                       const ST& st) {
   constexpr int R = stage_radix(N, S);
   constexpr int NS = stage_ns(N, S);
   constexpr int NB = N / R;
   constexpr int RD = (NB + 31) / 32;
   constexpr bool FIRST = (S == 0);
   constexpr bool LAST = (S == stage_count(N) - 1);
+  constexpr uint32_t E = sizeof(C);
   C v[RD][R];
 #pragma unroll
   for (int rd = 0; rd < RD; ++rd) {
@@ -176,12 +214,12 @@ __device__ __forceinline__ void wstage(C* buf, const C* tw, int lane, const LD& 
     if (NB % 32 == 0 || i < NB) {
 #pragma unroll
       for (int q = 0; q < R; ++q) {
-        if constexpr (FIRST) v[rd][q] = ld(i + q * NB);
-        else v[rd][q] = buf[i + q * NB];
+        if constexpr (FIRST) v[rd][q] = ld(rd, q, i + q * NB);
+        else v[rd][q] = lds(sbuf + (uint32_t)(i + q * NB) * E, (C*)nullptr);
       }
     }
   }
-  __syncwarp();
+  warp_sync_mem();
 #pragma unroll
   for (int rd = 0; rd < RD; ++rd) {
     const int i = lane + 32 * rd;
@@ -191,7 +229,7 @@ __device__ __forceinline__ void wstage(C* buf, const C* tw, int lane, const LD& 
         constexpr int TS = N / (NS * R);
 #pragma unroll
         for (int q = 1; q < R; ++q) {
-          const C w = tw[q * j * TS];
+          const C w = lds(stw + (uint32_t)(q * j * TS) * E, (C*)nullptr);
           v[rd][q] = DIR > 0 ? cmul(v[rd][q], w) : cmulc(v[rd][q], w);
         }
       }
@@ -200,30 +238,53 @@ __device__ __forceinline__ void wstage(C* buf, const C* tw, int lane, const LD& 
 #pragma unroll
       for (int q = 0; q < R; ++q) {
         if constexpr (LAST) st(base + q * NS, v[rd][q]);
-        else buf[base + q * NS] = v[rd][q];
+        else sts(sbuf + (uint32_t)(base + q * NS) * E, v[rd][q]);
       }
     }
   }
-  __syncwarp();
+  warp_sync_mem();
 }
 
 template <int N, int S, int DIR, typename C, typename LD, typename ST>
-__device__ __forceinline__ void wstages(C* buf, const C* tw, int lane, const LD& ld, const ST& st) {
-  wstage<N, S, DIR>(buf, tw, lane, ld, st);
-  if constexpr (S + 1 < stage_count(N)) wstages<N, S + 1, DIR>(buf, tw, lane, ld, st);
+__device__ __forceinline__ void wstages(uint32_t sbuf, uint32_t stw, int lane, const LD& ld,
+                                        const ST& st) {
+  wstage<N, S, DIR, C>(sbuf, stw, lane, ld, st);
+  if constexpr (S + 1 < stage_count(N)) wstages<N, S + 1, DIR, C>(sbuf, stw, lane, ld, st);
 }
 
-// Transform one line with the warp.  buf (N values) is the working line;
-// ld(i) supplies input i to the first stage, st(k, value) takes output k
-// from the last stage.
+// Adapts a loader of the form ld(i) to the first stage's ld(rd, q, i).
+template <typename LD> struct IndexLoad {
+  const LD& f;
+  __device__ __forceinline__ auto operator()(int, int, int i) const { return f(i); }
+};
+
+// Transform one line with the warp.  buf (N values, shared memory) is the
+// working line; ld(i) supplies input i to the first stage, st(k, value)
+// takes output k from the last stage.
 template <int N, int DIR, typename C, typename LD, typename ST>
 __device__ __forceinline__ void warp_fft(C* buf, const C* tw, int lane, const LD& ld, const ST& st) {
   static_assert(plan_ok(N), "FFT length must factor into 2, 3, 5, 7, 11");
-  // Hide the table address from the optimiser: otherwise it keeps every
-  // lane's twiddles of every stage in registers across the callers' loops,
-  // which costs more registers (and occupancy) than the shared loads.
-  asm volatile("" : "+l"(tw));
-  wstages<N, 0, DIR>(buf, tw, lane, ld, st);
+  uint32_t sbuf = (uint32_t)__cvta_generic_to_shared(buf);
+  uint32_t stw = (uint32_t)__cvta_generic_to_shared(tw);
+  // Hide the addresses and the lane from the optimiser: otherwise it keeps
+  // every lane's twiddle and line offsets of every stage in registers across
+  // the callers' loops, which costs more registers (and occupancy) than
+  // recomputing them.
+  asm volatile("" : "+r"(sbuf), "+r"(stw), "+r"(lane));
+  wstages<N, 0, DIR, C>(sbuf, stw, lane, IndexLoad<LD>{ld}, st);
+}
+
+// As warp_fft, with a first-stage loader that also receives the butterfly
+// round rd and input q (for values the caller prefetched into registers in
+// FirstStage<N> order).
+template <int N, int DIR, typename C, typename LD, typename ST>
+__device__ __forceinline__ void warp_fft_rq(C* buf, const C* tw, int lane, const LD& ld,
+                                            const ST& st) {
+  static_assert(plan_ok(N), "FFT length must factor into 2, 3, 5, 7, 11");
+  uint32_t sbuf = (uint32_t)__cvta_generic_to_shared(buf);
+  uint32_t stw = (uint32_t)__cvta_generic_to_shared(tw);
+  asm volatile("" : "+r"(sbuf), "+r"(stw), "+r"(lane));
+  wstages<N, 0, DIR, C>(sbuf, stw, lane, ld, st);
 }
 
 }  // namespace reg

@@ -282,7 +282,8 @@ struct Context {
   size_t zfast_bytes = 0;
   int fast_batch = 0;           // band pairs per launch (0: as many as fit)
   int fast_rods = 16;           // rods per CTA of the z kernels
-  int fast_warps = 16;          // warps per CTA of the plane kernel
+  int fast_warps = 16;          // warps per CTA of the plane kernel (at most)
+  int fast_vpsi_threads = 256;  // FP32 H*psi plane CTA size (256 or 512)
   int fast_chunks = 8;          // CTAs per plane in the density pass
   bool fast_fft = true;         // use the specialised kernels when compiled
   float* a32 = nullptr;         // TF32 hi/lo split of the projectors
