@@ -135,6 +135,9 @@ int qbx_create(qbx_context** out, int device, int precision) {
   h->c.device = device;
   h->c.precision = precision;
   if (const char* e = std::getenv("QBX_GEMM_BACKEND")) h->c.gemm_backend = std::atoi(e) == 0 ? 0 : 1;
+  // tall updates: TF32 splits by default; BF16 splits (QBX_TALL_KIND=0) are
+  // ~20% faster but leave C orthonormal only to ~1e-5
+  if (const char* e = std::getenv("QBX_TALL_KIND")) h->c.tall_kind = std::atoi(e) == 0 ? 0 : 1;
   const int rc = guarded(h, [&](Context& c) {
     QBX_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
     QBX_BLAS(cublasCreate(&c.blas));
@@ -265,8 +268,8 @@ int qbx_set_cell(qbx_context* h, const double cell[9], double ecut, int nst, con
       if (const char* e = std::getenv("QBX_FAST_RODS")) c.fast_rods = std::max(1, std::min(32, std::atoi(e)));
       if (const char* e = std::getenv("QBX_FAST_CHUNKS")) c.fast_chunks = std::max(1, std::atoi(e));
       if (const char* e = std::getenv("QBX_FAST_BATCH")) c.fast_batch = std::max(0, std::atoi(e));
-      if (const char* e = std::getenv("QBX_FAST_VPSI_THREADS"))
-        c.fast_vpsi_threads = std::atoi(e) == 512 ? 512 : 256;
+      if (const char* e = std::getenv("QBX_FAST_VPSI_SHAPE"))
+        c.fast_vpsi_shape = std::max(0, std::min(2, std::atoi(e)));
     }
     c.species.clear();
     c.tau.clear();
@@ -570,42 +573,61 @@ int qbx_split_gemm_tn(qbx_context* h, int m, int n, int k, const double* a, cons
                       double* d, int backend) {
   return guarded(h, [&](Context& c) {
     QBX_REQUIRE(m > 0 && n > 0 && k > 0 && a && b && d, 1, "bad GEMM arguments");
-    const int ldp = (k + 63) / 64 * 64;
+    QBX_REQUIRE(backend >= 0 && backend <= 2, 1, "backend must be 0, 1 or 2");
     double *da = dalloc<double>((size_t)k * m), *db = dalloc<double>((size_t)k * n);
     double* dd = dalloc<double>((size_t)m * n);
-    void *ah, *al, *bh, *bl;
-    QBX_CUDA(cudaMalloc(&ah, (size_t)ldp * m * 2));
-    QBX_CUDA(cudaMalloc(&al, (size_t)ldp * m * 2));
-    QBX_CUDA(cudaMalloc(&bh, (size_t)ldp * n * 2));
-    QBX_CUDA(cudaMalloc(&bl, (size_t)ldp * n * 2));
-    h2d_sync(da, a, sizeof(double) * k * m);
-    h2d_sync(db, b, sizeof(double) * k * n);
-    split_bf16_2d(c, da, k, m, k, ah, al, ldp);
-    split_bf16_2d(c, db, k, n, k, bh, bl, ldp);
+    void *ah = nullptr, *al = nullptr, *bh = nullptr, *bl = nullptr, *acc = nullptr;
     const int saved = c.gemm_backend;
     const size_t saved_acc = c.acc32_elems;
     void* saved_ptr = c.d_acc32;
-    void* acc = nullptr;
-    QBX_CUDA(cudaMalloc(&acc, (size_t)m * n * sizeof(float)));
-    c.d_acc32 = acc;
-    c.acc32_elems = (size_t)m * n;
-    c.gemm_backend = backend;
+    auto cleanup = [&]() {
+      c.gemm_backend = saved; c.d_acc32 = saved_ptr; c.acc32_elems = saved_acc;
+      if (acc) cudaFree(acc);
+      if (ah) cudaFree(ah);
+      if (al) cudaFree(al);
+      if (bh) cudaFree(bh);
+      if (bl) cudaFree(bl);
+      dfree(da); dfree(db); dfree(dd);
+    };
     try {
-      QBX_REQUIRE(backend == 0 || tc_gemm_supported(c, true, false, m, n, k), 54,
-                  "shape not supported by the tcgen05 GEMM");
-      split_gemm(c, true, false, m, n, k, 1.0, ah, al, ldp, bh, bl, ldp, 0.0, dd);
+      h2d_sync(da, a, sizeof(double) * k * m);
+      h2d_sync(db, b, sizeof(double) * k * n);
+      if (backend == 2) {
+        // TF32 splits through the tcgen05 kind::tf32 kernel
+        const int ldk = pad4(k);
+        QBX_CUDA(cudaMalloc(&ah, (size_t)ldk * m * 4));
+        QBX_CUDA(cudaMalloc(&al, (size_t)ldk * m * 4));
+        QBX_CUDA(cudaMalloc(&bh, (size_t)ldk * n * 4));
+        QBX_CUDA(cudaMalloc(&bl, (size_t)ldk * n * 4));
+        split_tf32(c, da, k, m, k, (float*)ah, (float*)al, ldk);
+        split_tf32(c, db, k, n, k, (float*)bh, (float*)bl, ldk);
+        QBX_CUDA(cudaMemsetAsync(dd, 0, sizeof(double) * m * n, c.stream));
+        tc_tf32_gemm_tn(c, m, n, k, 1.0, (const float*)ah, (const float*)al, ldk,
+                        (const float*)bh, (const float*)bl, ldk, 0.0, dd, m);
+      } else {
+        const int ldp = (k + 63) / 64 * 64;
+        QBX_CUDA(cudaMalloc(&ah, (size_t)ldp * m * 2));
+        QBX_CUDA(cudaMalloc(&al, (size_t)ldp * m * 2));
+        QBX_CUDA(cudaMalloc(&bh, (size_t)ldp * n * 2));
+        QBX_CUDA(cudaMalloc(&bl, (size_t)ldp * n * 2));
+        split_bf16_2d(c, da, k, m, k, ah, al, ldp);
+        split_bf16_2d(c, db, k, n, k, bh, bl, ldp);
+        QBX_CUDA(cudaMalloc(&acc, (size_t)m * n * sizeof(float)));
+        c.d_acc32 = acc;
+        c.acc32_elems = (size_t)m * n;
+        c.gemm_backend = backend;
+        QBX_REQUIRE(backend == 0 || tc_gemm_supported(c, true, false, m, n, k), 54,
+                    "shape not supported by the tcgen05 GEMM");
+        split_gemm(c, true, false, m, n, k, 1.0, ah, al, ldp, bh, bl, ldp, 0.0, dd);
+      }
       QBX_CUDA(cudaMemcpyAsync(d, dd, sizeof(double) * m * n, cudaMemcpyDeviceToHost, c.stream));
       QBX_CUDA(cudaStreamSynchronize(c.stream));
       QBX_REQUIRE(tc_check_error(c) == 0, 55, "tcgen05 GEMM pipeline wait timed out");
     } catch (...) {
-      c.gemm_backend = saved; c.d_acc32 = saved_ptr; c.acc32_elems = saved_acc;
-      cudaFree(acc); cudaFree(ah); cudaFree(al); cudaFree(bh); cudaFree(bl);
-      dfree(da); dfree(db); dfree(dd);
+      cleanup();
       throw;
     }
-    c.gemm_backend = saved; c.d_acc32 = saved_ptr; c.acc32_elems = saved_acc;
-    cudaFree(acc); cudaFree(ah); cudaFree(al); cudaFree(bh); cudaFree(bl);
-    dfree(da); dfree(db); dfree(dd);
+    cleanup();
   });
 }
 

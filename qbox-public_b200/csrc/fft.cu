@@ -614,7 +614,7 @@ static bool staged_fast(Context& ctx, int op, const double* c, const double* v, 
   a.twz = twiddles(ctx.device, 2, g.n2);
   a.rods_per_cta = ctx.fast_rods;
   a.xy_warps = ctx.fast_warps;
-  a.vpsi_threads = ctx.fast_vpsi_threads;
+  a.vpsi_shape = ctx.fast_vpsi_shape;
   a.density_chunks = ctx.fast_chunks;
   a.v = v;
   if (op == OP_VPSI && ctx.precision == MIXED) {

@@ -48,9 +48,15 @@ constexpr int kZThreads = 256;
 // pass holds an FP32 plane in shared memory, so one CTA per SM; the FP32
 // H*psi pass comes in two shapes, one 512-thread CTA or two 256-thread CTAs
 // per SM, picked at run time.
-template <typename T, int OP> struct XYDefault { static constexpr int th = 256; };
-template <> struct XYDefault<float, 0> { static constexpr int th = 512; };
-__host__ __device__ constexpr int xy_minblocks(int th) { return th == 256 ? 2 : 1; }
+template <typename T, int OP> struct XYDefault { static constexpr int shape = 3; };
+template <> struct XYDefault<float, 0> { static constexpr int shape = 1; };
+// Plane CTA shapes: 0 = 256 threads, two CTAs per SM; 1 = 512 threads, one
+// per SM; 2 = 512 threads compiled for two per SM (64 registers per
+// thread); 3 = 256 threads, one per SM (the FP64 kernels)
+__host__ __device__ constexpr int xy_threads(int shape) {
+  return (shape == 0 || shape == 3) ? 256 : 512;
+}
+__host__ __device__ constexpr int xy_minblocks(int shape) { return (shape == 0 || shape == 2) ? 2 : 1; }
 
 template <typename C>
 __device__ __forceinline__ void load_tw(C* dst, const double2* src, int n) {
@@ -191,8 +197,8 @@ __host__ size_t xy_smem_bytes(int ncol, int nwarps) {
 
 // shared memory: [twx N0][twy N1][P ncol x pitch(N1)][one line of N0 per
 // warp][FP32 density plane N1 x N0, mixed density only][xmap N0 ints]
-template <typename T, int N0, int N1, int OP, int TH>
-__global__ void __launch_bounds__(TH, xy_minblocks(TH))
+template <typename T, int N0, int N1, int OP, int SHAPE>
+__global__ void __launch_bounds__(xy_threads(SHAPE), xy_minblocks(SHAPE))
 kxy(typename reg::CT<T>::c* __restrict__ zbuf, int npairs, int pairs_per_cta, DeviceSticks g,
     const double2* __restrict__ twx_g, const double2* __restrict__ twy_g,
     const T* __restrict__ v, double* __restrict__ rho, const double* __restrict__ w, int pair0,
@@ -326,19 +332,19 @@ struct StagedArgs {
   const double2 *twx, *twy, *twz;
   int rods_per_cta;        // z kernels
   int xy_warps;            // requested warps per kxy CTA
-  int vpsi_threads;        // FP32 H*psi plane CTA: 256 (two per SM) or 512
+  int vpsi_shape;          // FP32 H*psi plane CTA shape (xy_threads / xy_minblocks)
   int density_chunks;      // CTAs per plane in the density pass
 };
 
-template <typename T, int N, int TH>
+template <typename T, int N, int SH>
 void launch_vpsi_xy(Context& ctx, const StagedArgs& a) {
   using C = typename reg::CT<T>::c;
   const DeviceSticks& g = ctx.dws;
-  const int nw = std::min(a.xy_warps, TH / 32);
+  const int nw = std::min(a.xy_warps, xy_threads(SH) / 32);
   const size_t sm = xy_smem_bytes<T, N, N, XY_VPSI>(g.ncol, nw);
-  QBX_CUDA(cudaFuncSetAttribute(kxy<T, N, N, XY_VPSI, TH>,
+  QBX_CUDA(cudaFuncSetAttribute(kxy<T, N, N, XY_VPSI, SH>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  kxy<T, N, N, XY_VPSI, TH><<<dim3(N, a.npairs), 32 * nw, sm, ctx.stream>>>(
+  kxy<T, N, N, XY_VPSI, SH><<<dim3(N, a.npairs), 32 * nw, sm, ctx.stream>>>(
       (C*)a.zbuf, a.npairs, 1, g, a.twx, a.twy, (const T*)a.v, nullptr, nullptr, a.pair0, a.nst);
   QBX_LAUNCHED(ctx);
 }
@@ -360,26 +366,29 @@ void run_cubic(Context& ctx, const StagedArgs& a) {
     QBX_LAUNCHED(ctx);
   }
   if (a.op == XY_DENSITY) {
-    constexpr int TH = XYDefault<T, XY_DENSITY>::th;
-    const int nw = std::min(a.xy_warps, TH / 32);
+    constexpr int SH = XYDefault<T, XY_DENSITY>::shape;
+    const int nw = std::min(a.xy_warps, xy_threads(SH) / 32);
     const size_t sm = xy_smem_bytes<T, N, N, XY_DENSITY>(g.ncol, nw);
-    QBX_CUDA(cudaFuncSetAttribute(kxy<T, N, N, XY_DENSITY, TH>,
+    QBX_CUDA(cudaFuncSetAttribute(kxy<T, N, N, XY_DENSITY, SH>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     int chunks = std::max(1, std::min(a.npairs, a.density_chunks));
     const int ppc = (a.npairs + chunks - 1) / chunks;
     chunks = (a.npairs + ppc - 1) / ppc;
     ProfScope ps(ctx, "xy_density");
-    kxy<T, N, N, XY_DENSITY, TH><<<dim3(N, chunks), 32 * nw, sm, st>>>(
+    kxy<T, N, N, XY_DENSITY, SH><<<dim3(N, chunks), 32 * nw, sm, st>>>(
         (C*)a.zbuf, a.npairs, ppc, g, a.twx, a.twy, nullptr, a.rho, a.w, a.pair0, a.nst);
     QBX_LAUNCHED(ctx);
     return;
   }
   {
     ProfScope ps(ctx, "xy_vpsi");
-    if (std::is_same<T, float>::value && a.vpsi_threads == 512)
-      launch_vpsi_xy<T, N, 512>(ctx, a);
-    else
-      launch_vpsi_xy<T, N, 256>(ctx, a);
+    if constexpr (std::is_same<T, float>::value) {
+      if (a.vpsi_shape == 1) launch_vpsi_xy<T, N, 1>(ctx, a);
+      else if (a.vpsi_shape == 2) launch_vpsi_xy<T, N, 2>(ctx, a);
+      else launch_vpsi_xy<T, N, 0>(ctx, a);
+    } else {
+      launch_vpsi_xy<T, N, 3>(ctx, a);
+    }
   }
   QBX_CUDA(cudaFuncSetAttribute(kz_fwd<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zs));
   const double scale = 1.0 / ((double)N * N * N);
@@ -391,8 +400,8 @@ void run_cubic(Context& ctx, const StagedArgs& a) {
 
 template <typename T, int N>
 size_t smem_need(const Context& ctx, const StagedArgs& a) {
-  const int nwd = std::min(a.xy_warps, XYDefault<T, XY_DENSITY>::th / 32);
-  const int nwv = std::min(a.xy_warps, (std::is_same<T, float>::value ? a.vpsi_threads : 256) / 32);
+  const int nwd = std::min(a.xy_warps, xy_threads(XYDefault<T, XY_DENSITY>::shape) / 32);
+  const int nwv = std::min(a.xy_warps, xy_threads(std::is_same<T, float>::value ? a.vpsi_shape : 3) / 32);
   const size_t x = std::max(xy_smem_bytes<T, N, N, XY_DENSITY>(ctx.dws.ncol, nwd),
                             xy_smem_bytes<T, N, N, XY_VPSI>(ctx.dws.ncol, nwv));
   const size_t z = sizeof(typename reg::CT<T>::c) * ((size_t)N + (size_t)2 * a.rods_per_cta * pitch(N));

@@ -283,13 +283,21 @@ struct Context {
   int fast_batch = 0;           // band pairs per launch (0: as many as fit)
   int fast_rods = 16;           // rods per CTA of the z kernels
   int fast_warps = 16;          // warps per CTA of the plane kernel (at most)
-  int fast_vpsi_threads = 256;  // FP32 H*psi plane CTA size (256 or 512)
+  int fast_vpsi_shape = 0;      // FP32 H*psi plane CTA shape (0, 1, 2)
   int fast_chunks = 8;          // CTAs per plane in the density pass
   bool fast_fft = true;         // use the specialised kernels when compiled
   float* a32 = nullptr;         // TF32 hi/lo split of the projectors
   float* a32lo = nullptr;
   float* s32 = nullptr;         // TF32 hi/lo split of a small matrix
   float* s32lo = nullptr;
+  int tall_kind = 1;            // TALL_TF32 (default) or TALL_BF16 for the tall updates
+  void* at_hi = nullptr;        // split of A_nl^T (projectors contiguous), ld tall_ld(nproj)
+  void* at_lo = nullptr;
+  void* ct_hi = nullptr;        // split of C^T (bands contiguous), ld tall_ld(nst)
+  void* ct_lo = nullptr;
+  void* tm_hi = nullptr;        // split of the small right-hand matrix, ld tall_ld(rows)
+  void* tm_lo = nullptr;
+  int tall_ld(int n) const { return tall_kind == 1 ? (n + 3) / 4 * 4 : (n + 7) / 8 * 8; }
   void* d_tc_ws = nullptr;      // split-K partials of the tcgen05 GEMM
   size_t tc_ws_elems = 0;
   void* d_tc_err = nullptr;     // wait-timeout flag of the tcgen05 GEMM
@@ -407,6 +415,24 @@ void tf32x3_gemm_nn(Context& ctx, int m, int n, int k, double alpha, const float
                     const float* Alo, int lda, const float* Bhi, const float* Blo, int ldb,
                     double beta, double* C, int ldc);
 inline int pad4(int n) { return (n + 3) / 4 * 4; }
+inline int pad8(int n) { return (n + 7) / 8 * 8; }
+// split kinds of the tall updates: BF16 hi/lo (kind::f16) or TF32 hi/lo
+// (kind::tf32, stored as FP32)
+enum { TALL_BF16 = 0, TALL_TF32 = 1 };
+// x as hi/lo of the given kind, leading dimension ldy (BF16: padding rows zero)
+void split_plain(Context& ctx, int kind, const double* x, int rows, int cols, int ldx, void* hi,
+                 void* lo, int ldy);
+// x^T as hi/lo of the given kind: x rows x cols (ld ldx) -> cols x rows (ld ldy)
+void split_t(Context& ctx, int kind, const double* x, int rows, int cols, int ldx, void* hi,
+             void* lo, int ldy);
+// C (m x n, ld ldc) = alpha A^T B + beta C with hi/lo splits A (k x m, ld
+// lda) and B (k x n, ld ldb) of the given kind, through the tcgen05 kernel
+void tc_gemm_kind_tn(Context& ctx, int kind, int m, int n, int k, double alpha, const void* ahi,
+                     const void* alo, int lda, const void* bhi, const void* blo, int ldb,
+                     double beta, double* C, int ldc);
+void tc_tf32_gemm_tn(Context& ctx, int m, int n, int k, double alpha, const float* ahi,
+                     const float* alo, int lda, const float* bhi, const float* blo, int ldb,
+                     double beta, double* C, int ldc);
 void alloc_mixed(Context& ctx);
 void free_mixed(Context& ctx);
 

@@ -162,6 +162,66 @@ void split_tf32(Context& ctx, const double* x, int rows, int cols, int ldx, floa
   QBX_LAUNCHED(ctx);
 }
 
+// Transposed split: x (rows x cols, column-major, ld ldx) -> y = x^T (cols x
+// rows, ld ldy) as hi/lo pairs of TF32 (stored as FP32) or BF16, through
+// 32 x 32 tiles in shared memory so that both the FP64 reads and the split
+// writes are coalesced.
+template <typename OUT>
+__device__ __forceinline__ void split_pair(double v, OUT& h, OUT& l);
+template <>
+__device__ __forceinline__ void split_pair<float>(double v, float& h, float& l) {
+  h = tf32_round((float)v);
+  l = tf32_round((float)(v - (double)h));
+}
+template <>
+__device__ __forceinline__ void split_pair<__nv_bfloat16>(double v, __nv_bfloat16& h,
+                                                          __nv_bfloat16& l) {
+  h = __double2bfloat16(v);
+  l = __double2bfloat16(v - (double)__bfloat162float(h));
+}
+
+template <typename OUT>
+__global__ void k_split_t(const double* __restrict__ x, int rows, int cols, int ldx,
+                          OUT* __restrict__ hi, OUT* __restrict__ lo, int ldy) {
+  __shared__ double t[32][33];
+  const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;   // 32 x 8 threads
+  for (int j = ty; j < 32; j += 8) {
+    const int r = r0 + tx, c = c0 + j;
+    t[j][tx] = (r < rows && c < cols) ? x[(size_t)c * ldx + r] : 0.0;
+  }
+  __syncthreads();
+  for (int j = ty; j < 32; j += 8) {
+    const int c = c0 + tx, r = r0 + j;      // y(c, r) at r * ldy + c
+    if (c < cols && r < rows) {
+      OUT h, l;
+      split_pair<OUT>(t[tx][j], h, l);
+      hi[(size_t)r * ldy + c] = h;
+      lo[(size_t)r * ldy + c] = l;
+    }
+  }
+}
+
+void split_plain(Context& ctx, int kind, const double* x, int rows, int cols, int ldx, void* hi,
+                 void* lo, int ldy) {
+  if (kind == TALL_TF32)
+    split_tf32(ctx, x, rows, cols, ldx, (float*)hi, (float*)lo, ldy);
+  else
+    split_bf16_2d(ctx, x, rows, cols, ldx, hi, lo, ldy);
+}
+
+void split_t(Context& ctx, int kind, const double* x, int rows, int cols, int ldx, void* hi,
+             void* lo, int ldy) {
+  dim3 grid((rows + 31) / 32, (cols + 31) / 32);
+  QBX_REQUIRE(grid.y <= 65535, 50, "too many columns for the transposed split");
+  if (kind == TALL_TF32)
+    k_split_t<float><<<grid, 256, 0, ctx.stream>>>(x, rows, cols, ldx, (float*)hi, (float*)lo, ldy);
+  else
+    k_split_t<__nv_bfloat16><<<grid, 256, 0, ctx.stream>>>(
+        x, rows, cols, ldx, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo, ldy);
+  QBX_LAUNCHED(ctx);
+}
+
 // out (rows x cols, ld ldo) = alpha * acc (ld lda) + beta * out
 __global__ void k_acc2d_to_f64(const float* __restrict__ acc, int lda, int rows, int cols,
                                double alpha, double beta, double* __restrict__ out, int ldo) {

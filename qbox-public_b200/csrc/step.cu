@@ -94,6 +94,26 @@ static void polar(Context& ctx, double* x, double tol, int maxiter) {
   }
 }
 
+// out += alpha * c * M for the FP64 wavefunction block c (K x n) and an n x n
+// matrix M: the tcgen05 kernel on the transposed split of c (BF16 or TF32
+// hi/lo, ctx.tall_kind), or three cuBLAS TF32 products on its plain split.
+// out may be c itself: both read the split copy of c.
+static void tall_update(Context& ctx, const double* c, const double* M, double alpha, double* out) {
+  const int n = ctx.nst, K = 2 * ctx.wb.ng;
+  if (ctx.gemm_backend == 1) {
+    const int kind = ctx.tall_kind, ld = ctx.tall_ld(n);
+    split_plain(ctx, kind, M, n, n, n, ctx.tm_hi, ctx.tm_lo, ld);   // M is K-major as stored
+    split_t(ctx, kind, c, K, n, K, ctx.ct_hi, ctx.ct_lo, ld);
+    tc_gemm_kind_tn(ctx, kind, K, n, n, alpha, ctx.ct_hi, ctx.ct_lo, ld, ctx.tm_hi, ctx.tm_lo, ld,
+                    1.0, out, K);
+  } else {
+    split_tf32(ctx, M, n, n, n, ctx.s32, ctx.s32lo, pad4(n));
+    split_tf32(ctx, c, K, n, K, ctx.c32, ctx.c32lo, ctx.ldp);
+    tf32x3_gemm_nn(ctx, K, n, n, alpha, ctx.c32, ctx.c32lo, ctx.ldp, ctx.s32, ctx.s32lo, pad4(n),
+                   1.0, out, K);
+  }
+}
+
 // SlaterDet::ortho_align (src/SlaterDet.cpp:768-876)
 void ortho_align(Context& ctx) {
   const int n = ctx.nst, K = 2 * ctx.wb.ng;
@@ -130,10 +150,7 @@ void ortho_align(Context& ctx) {
     // correction, so C stays orthonormal to the accuracy of the overlap.
     double* T = ctx.d_nn3;
     launch_identity_axpy(ctx, T, X, n, -1.0);
-    split_tf32(ctx, T, n, n, n, ctx.s32, ctx.s32lo, pad4(n));
-    split_tf32(ctx, ctx.d_c, K, n, K, ctx.c32, ctx.c32lo, ctx.ldp);
-    tf32x3_gemm_nn(ctx, K, n, n, -1.0, ctx.c32, ctx.c32lo, ctx.ldp, ctx.s32, ctx.s32lo, pad4(n),
-                   1.0, ctx.d_c, K);
+    tall_update(ctx, ctx.d_c, T, -1.0, ctx.d_c);
   } else {
     QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, K, n, n, &one, ctx.d_ctmp, K, X, n,
                          &zero, ctx.d_c, K));
@@ -178,9 +195,17 @@ static void nonlocal(Context& ctx, bool hpsi) {
   if (hpsi) {
     ProfScope ps(ctx, "gemm_nl_apply");
     if (mx) {
-      split_tf32(ctx, ctx.d_fnl, np, n, np, ctx.s32, ctx.s32lo, pad4(np));
-      tf32x3_gemm_nn(ctx, K, n, np, 1.0, ctx.a32, ctx.a32lo, ctx.ldp, ctx.s32, ctx.s32lo, pad4(np),
-                     1.0, ctx.d_hc, K);
+      if (ctx.gemm_backend == 1) {
+        // F (np x n) is already K-major for this product: a plain split
+        const int kind = ctx.tall_kind, ld = ctx.tall_ld(np);
+        split_plain(ctx, kind, ctx.d_fnl, np, n, np, ctx.tm_hi, ctx.tm_lo, ld);
+        tc_gemm_kind_tn(ctx, kind, K, n, np, 1.0, ctx.at_hi, ctx.at_lo, ld, ctx.tm_hi, ctx.tm_lo,
+                        ld, 1.0, ctx.d_hc, K);
+      } else {
+        split_tf32(ctx, ctx.d_fnl, np, n, np, ctx.s32, ctx.s32lo, pad4(np));
+        tf32x3_gemm_nn(ctx, K, n, np, 1.0, ctx.a32, ctx.a32lo, ctx.ldp, ctx.s32, ctx.s32lo,
+                       pad4(np), 1.0, ctx.d_hc, K);
+      }
     } else {
       QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, K, n, np, &one, ctx.d_anl, K,
                            ctx.d_fnl, np, &one, ctx.d_hc, K));
@@ -231,10 +256,7 @@ void psda_update(Context& ctx) {
       split_gemm(ctx, true, false, n, n, K, 2.0, ctx.cs_hi[0], ctx.cs_lo[0], ctx.ldp, ctx.hs_hi,
                  ctx.hs_lo, ctx.ldp, 0.0, A);
       launch_rank1_fix(ctx, A, n, ctx.d_c, K, ctx.d_hc, K, n, n, -1.0, false);
-      split_tf32(ctx, A, n, n, n, ctx.s32, ctx.s32lo, pad4(n));
-      split_tf32(ctx, ctx.d_c, K, n, K, ctx.c32, ctx.c32lo, ctx.ldp);
-      tf32x3_gemm_nn(ctx, K, n, n, -1.0, ctx.c32, ctx.c32lo, ctx.ldp, ctx.s32, ctx.s32lo, pad4(n),
-                     1.0, ctx.d_hc, K);
+      tall_update(ctx, ctx.d_c, A, -1.0, ctx.d_hc);
     } else {
       QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, ctx.d_c, K, ctx.d_hc,
                            K, &zero, A, n));
@@ -261,6 +283,9 @@ void free_mixed(Context& ctx) {
   dfree(ctx.a32lo);
   dfree(ctx.s32);
   dfree(ctx.s32lo);
+  void** tall[] = {&ctx.at_hi, &ctx.at_lo, &ctx.ct_hi, &ctx.ct_lo, &ctx.tm_hi, &ctx.tm_lo};
+  for (void** b : tall)
+    if (*b) { cudaFree(*b); *b = nullptr; }
   ctx.acc32_elems = 0;
   ctx.tc_ws_elems = 0;
 }
@@ -289,14 +314,25 @@ void alloc_mixed(Context& ctx) {
   const size_t small4 = std::max<size_t>((size_t)pad4((int)std::max(np, n)) * n, 1);
   ctx.s32 = dalloc<float>(small4);
   ctx.s32lo = dalloc<float>(small4);
+  // tall-update splits: room for either kind (TF32 4 bytes at ld pad4,
+  // BF16 2 bytes at ld pad8)
+  auto tall_bytes = [](size_t rows, size_t cols) { return (size_t)pad8((int)rows) * cols * 4; };
+  QBX_CUDA(cudaMalloc(&ctx.ct_hi, tall_bytes(n, K)));
+  QBX_CUDA(cudaMalloc(&ctx.ct_lo, tall_bytes(n, K)));
+  QBX_CUDA(cudaMalloc(&ctx.tm_hi, tall_bytes(std::max(np, n), n)));
+  QBX_CUDA(cudaMalloc(&ctx.tm_lo, tall_bytes(std::max(np, n), n)));
   if (np) {
     QBX_CUDA(cudaMalloc(&ctx.as_hi, (size_t)ctx.ldp * np * 2));
     QBX_CUDA(cudaMalloc(&ctx.as_lo, (size_t)ctx.ldp * np * 2));
     ctx.a32 = dalloc<float>((size_t)ctx.ldp * np);
     ctx.a32lo = dalloc<float>((size_t)ctx.ldp * np);
+    QBX_CUDA(cudaMalloc(&ctx.at_hi, tall_bytes(np, K)));
+    QBX_CUDA(cudaMalloc(&ctx.at_lo, tall_bytes(np, K)));
     if (ctx.d_anl) {
       split_bf16_2d(ctx, ctx.d_anl, (int)K, (int)np, (int)K, ctx.as_hi, ctx.as_lo, ctx.ldp);
       split_tf32(ctx, ctx.d_anl, (int)K, (int)np, (int)K, ctx.a32, ctx.a32lo, ctx.ldp);
+      split_t(ctx, ctx.tall_kind, ctx.d_anl, (int)K, (int)np, (int)K, ctx.at_hi, ctx.at_lo,
+              ctx.tall_ld((int)np));
     }
   }
   QBX_CUDA(cudaStreamSynchronize(ctx.stream));

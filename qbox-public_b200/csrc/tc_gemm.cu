@@ -1,12 +1,20 @@
 // tcgen05 split-precision GEMM for sm_100a.
 //
 //   D(m, n) = sum_k A(k, m) B(k, n)   over the three split terms
-//             A_hi B_hi + A_hi B_lo + A_lo B_hi   (BF16 in, FP32 accumulate)
+//             A_hi B_hi + A_hi B_lo + A_lo B_hi   (FP32 accumulate)
+//
+// in two operand kinds: BF16 splits (kind::f16, 16 significant bits) for
+// the inner products over the plane-wave rows, and TF32 splits
+// (kind::tf32, 22 bits) for the tall updates.
 //
 // A and B are K-major (column-major with the contraction index contiguous),
-// as the wavefunction and projector matrices of a SlaterDet are.  These are
-// the inner products of the electronic step: projections F = A_nl^T C, the
-// residual C^T (H C), the overlap C^T C and C^T C_last.
+// as the wavefunction and projector matrices of a SlaterDet are.  The inner
+// products of the electronic step (projections F = A_nl^T C, the residual
+// C^T (H C), the overlaps C^T C and C^T C_last) use the BF16 kind with split
+// K and an FP64 sum of the partials.  The tall updates H C += A_nl F,
+// H C -= C A and C -= C (I - X) contract over bands or projectors: their A
+// operand is the transposed split of A_nl or C (bands contiguous), and the
+// epilogue adds alpha * D into the FP64 output directly.
 //
 // One CTA computes a 128 x 128 FP32 tile of one split-K slice:
 //   warp 0  - TMA producer: per 64-wide K block one pipeline stage receives
@@ -17,7 +25,7 @@
 //             commits the stage back to the producer;
 //   warps 4-7 - epilogue: tcgen05.ld of the accumulator (each warp its 32
 //             TMEM lanes) and coalesced FP32 stores of the partial tile.
-// The split-K partials are summed in FP64 by k_reduce_splits.  Every
+// Split-K partials are summed in FP64 by k_reduce_splits2d.  Every
 // mbarrier wait is bounded; a wait that runs out sets an error flag that
 // the host turns into an error, and the CTA still releases its TMEM.
 #include <cuda.h>
@@ -32,9 +40,13 @@ namespace qbx {
 
 namespace tc {
 
-constexpr int BM = 128, BN = 128, BK = 64;
+constexpr int BM = 128, BN = 128;
+constexpr int KIND_BF16 = 0, KIND_TF32 = 1;
+// K elements per 128-byte tile row: 64 BF16 or 32 TF32
+__host__ __device__ constexpr int bk_of(int kind) { return kind == KIND_BF16 ? 64 : 32; }
+constexpr int BK = 64;                            // BF16 (kept for callers' checks)
 constexpr int STAGES = 3;
-constexpr int TILE_BYTES = BM * BK * 2;           // 16 KB per operand tile
+constexpr int TILE_BYTES = BM * 128;              // 16 KB per operand tile
 constexpr int STAGE_BYTES = 4 * TILE_BYTES;       // A_hi, A_lo, B_hi, B_lo
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /* align */ + 256 /* barriers */;
 constexpr int THREADS = 256;
@@ -89,20 +101,32 @@ __device__ __forceinline__ uint64_t smem_desc(const void* tile) {
   return ((addr & 0x3FFFF) >> 4) | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
 }
 
-// kind::f16 instruction descriptor: F32 accumulate, BF16 A and B, both
-// K-major, N = BN, M = BM.
-__host__ __device__ constexpr uint32_t idesc_bf16() {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+// Instruction descriptor: F32 accumulate (bits 4-5 = 1), A and B formats
+// (bits 7-9, 10-12: BF16 = 1 for kind::f16, TF32 = 2 for kind::tf32), both
+// K-major, N >> 3 at bit 17, M >> 4 at bit 24.
+__host__ __device__ constexpr uint32_t idesc_of(int kind) {
+  const uint32_t fmt = kind == KIND_BF16 ? 1u : 2u;
+  return (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(BN >> 3) << 17) |
          ((uint32_t)(BM >> 4) << 24);
 }
 
-__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t acc) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-      "l"(da), "l"(db), "r"(idesc_bf16()), "r"(acc)
-      : "memory");
+template <int KIND>
+__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t acc) {
+  if constexpr (KIND == KIND_BF16) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(idesc_of(KIND_BF16)), "r"(acc)
+        : "memory");
+  } else {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(idesc_of(KIND_TF32)), "r"(acc)
+        : "memory");
+  }
 }
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
@@ -122,10 +146,15 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
 // and hand it back, while the MMA warp fills the other one.  FP32 chains
 // thus stay short (CHUNK*4 MMA steps in TMEM, then one register add per
 // chunk) instead of one TMEM chain over the whole K slice.
+// Output: with ws != nullptr the FP32 tile of split-K slice z goes to
+// ws[z][col * M + row]; otherwise (no K split) C[col * ldc + row] =
+// alpha * D + beta * C in FP64.  Rows >= M and columns >= N are not stored.
+template <int KIND>
 __global__ void __launch_bounds__(THREADS, 1)
 k_tc_split_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant__ CUtensorMap ma_lo,
                 const __grid_constant__ CUtensorMap mb_hi, const __grid_constant__ CUtensorMap mb_lo,
                 int M, int N, int nkb, int kb_per_split, float* __restrict__ ws,
+                double* __restrict__ C, int ldc, double alpha, double beta,
                 int* __restrict__ err) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -136,7 +165,9 @@ k_tc_split_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant
   uint32_t* tmem_slot = (uint32_t*)(tfree + 2);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  // without a K split the N tiles of one M tile are adjacent in the grid, so
+  // the CTAs that share an A tile run together and A streams from HBM once
+  const int m0 = (ws ? blockIdx.x : blockIdx.y) * BM, n0 = (ws ? blockIdx.y : blockIdx.x) * BN;
   const int kb0 = blockIdx.z * kb_per_split;
   const int kb1 = min(nkb, kb0 + kb_per_split);
   const int niter = max(0, kb1 - kb0);
@@ -172,7 +203,7 @@ k_tc_split_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant
       if (!mbar_wait(&empty[s], ph ^ 1u)) { atomicExch(err, 1); break; }
       unsigned char* st = base + s * STAGE_BYTES;
       mbar_expect_tx(&full[s], STAGE_BYTES);
-      const int kx = (kb0 + it) * BK;
+      const int kx = (kb0 + it) * bk_of(KIND);
       tma_load_2d(st + 0 * TILE_BYTES, &ma_hi, &full[s], kx, m0);
       tma_load_2d(st + 1 * TILE_BYTES, &ma_lo, &full[s], kx, m0);
       tma_load_2d(st + 2 * TILE_BYTES, &mb_hi, &full[s], kx, n0);
@@ -197,13 +228,14 @@ k_tc_split_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant
       const uint64_t dbh = smem_desc(st + 2 * TILE_BYTES);
       const uint64_t dbl = smem_desc(st + 3 * TILE_BYTES);
       const uint32_t tacc = tmem + (uint32_t)(b * BN);
+      // 4 MMAs of 32 bytes of K each (16 BF16 or 8 TF32)
 #pragma unroll
-      for (int k = 0; k < BK / 16; ++k) {
-        const uint64_t off = (uint64_t)(k * 32) >> 4;      // 16 BF16 = 32 bytes
+      for (int k = 0; k < 4; ++k) {
+        const uint64_t off = (uint64_t)(k * 32) >> 4;
         const uint32_t accumulate = (chunk_start && k == 0) ? 0u : 1u;
-        umma_bf16(tacc, dah + off, dbh + off, accumulate);
-        umma_bf16(tacc, dah + off, dbl + off, 1u);
-        umma_bf16(tacc, dal + off, dbh + off, 1u);
+        umma<KIND>(tacc, dah + off, dbh + off, accumulate);
+        umma<KIND>(tacc, dah + off, dbl + off, 1u);
+        umma<KIND>(tacc, dal + off, dbh + off, 1u);
       }
       umma_commit(&empty[s]);
       if ((it % CHUNK) == CHUNK - 1 || it == niter - 1) umma_commit(&tfull[b]);
@@ -243,12 +275,23 @@ k_tc_split_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant
       __syncwarp();
       if (lane == 0) mbar_arrive(&tfree[b]);
     }
-    float* out = ws + (size_t)blockIdx.z * M * N;
-    if (row < M) {
+    if (ws) {
+      float* out = ws + (size_t)blockIdx.z * M * N;
+      if (row < M) {
+#pragma unroll
+        for (int j = 0; j < BN; ++j) {
+          const int col = n0 + j;
+          if (col < N) out[(size_t)col * M + row] = ok ? acc[j] : 0.0f;
+        }
+      }
+    } else if (row < M && ok) {
 #pragma unroll
       for (int j = 0; j < BN; ++j) {
         const int col = n0 + j;
-        if (col < N) out[(size_t)col * M + row] = ok ? acc[j] : 0.0f;
+        if (col < N) {
+          double* o = C + (size_t)col * ldc + row;
+          *o = alpha * (double)acc[j] + (beta != 0.0 ? beta * *o : 0.0);
+        }
       }
     }
   }
@@ -258,17 +301,6 @@ k_tc_split_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                  "r"(TMEM_COLS)
                  : "memory");
-  }
-}
-
-// out(i) = alpha * sum_s ws(s, i) + beta * out(i), summed in FP64
-__global__ void k_reduce_splits(const float* __restrict__ ws, int nsplit, size_t n, double alpha,
-                                double beta, double* __restrict__ out) {
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x) {
-    double s = 0.0;
-    for (int z = 0; z < nsplit; z++) s += (double)ws[(size_t)z * n + i];
-    out[i] = alpha * s + (beta != 0.0 ? beta * out[i] : 0.0);
   }
 }
 
@@ -292,20 +324,37 @@ static EncodeTiledFn encode_fn() {
   return fn;
 }
 
-// K-major BF16 matrix: rows = k (contiguous, ld elements), cols = m; box
-// 64 (k) x 128 (m rows), 128-byte swizzle.
-static CUtensorMap kmajor_map(const void* ptr, int k, int cols, int ld) {
+// K-major matrix of BF16 or TF32 (FP32) elements: rows = k (contiguous, ld
+// elements), cols = m; box of one 128-byte row of K by 128 columns, 128-byte
+// swizzle.  Columns past `cols` and K past `k` read as zero.
+static CUtensorMap kmajor_map(const void* ptr, int k, int cols, int ld, int kind) {
   CUtensorMap map;
+  const size_t es = kind == tc::KIND_BF16 ? 2 : 4;
   const cuuint64_t dims[2] = {(cuuint64_t)k, (cuuint64_t)cols};
-  const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
-  const cuuint32_t box[2] = {(cuuint32_t)tc::BK, (cuuint32_t)tc::BM};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * es};
+  const cuuint32_t box[2] = {(cuuint32_t)tc::bk_of(kind), (cuuint32_t)tc::BM};
   const cuuint32_t estr[2] = {1, 1};
-  const CUresult r = encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr),
-                                 dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                                 CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  const CUresult r = encode_fn()(
+      &map, kind == tc::KIND_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+      2, const_cast<void*>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+      CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   QBX_REQUIRE(r == CUDA_SUCCESS, 53, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
   return map;
+}
+
+// out(col * ldc + row) = alpha * sum_s ws(s, col * M + row) + beta * out, in FP64
+__global__ void k_reduce_splits2d(const float* __restrict__ ws, int nsplit, int M, int N,
+                                  double alpha, double beta, double* __restrict__ out, int ldc) {
+  const size_t n = (size_t)M * N;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int z = 0; z < nsplit; z++) s += (double)ws[(size_t)z * n + i];
+    const size_t col = i / M, row = i - col * M;
+    double* o = out + col * ldc + row;
+    *o = alpha * s + (beta != 0.0 ? beta * *o : 0.0);
+  }
 }
 
 bool tc_gemm_supported(const Context& ctx, bool ta, bool tb, int m, int n, int k) {
@@ -315,48 +364,89 @@ bool tc_gemm_supported(const Context& ctx, bool ta, bool tb, int m, int n, int k
   return ta && !tb && m % tc::BM == 0 && n % tc::BN == 0 && k >= tc::BK;
 }
 
-void tc_split_gemm(Context& ctx, bool ta, bool tb, int m, int n, int k, double alpha,
-                   const void* ahi, const void* alo, int lda, const void* bhi, const void* blo,
-                   int ldb, double beta, double* C) {
-  QBX_REQUIRE(tc_gemm_supported(ctx, ta, tb, m, n, k), 54, "shape not supported by tcgen05 GEMM");
-  QBX_REQUIRE((lda * 2) % 16 == 0 && (ldb * 2) % 16 == 0, 54, "leading dimension not 16-byte aligned");
+// C (m x n, ld ldc) = alpha * A^T B + beta * C, A (k x m) and B (k x n)
+// K-major splits of the given kind.  The K dimension is split across CTAs
+// only when the output has too few tiles to fill the GPU.
+static void tc_gemm_tn(Context& ctx, int kind, int m, int n, int k, double alpha, const void* ahi,
+                       const void* alo, int lda, const void* bhi, const void* blo, int ldb,
+                       double beta, double* C, int ldc) {
+  const size_t es = kind == tc::KIND_BF16 ? 2 : 4;
+  QBX_REQUIRE(m > 0 && n > 0 && k > 0 && ldc >= m, 54, "bad tcgen05 GEMM shape");
+  QBX_REQUIRE((lda * es) % 16 == 0 && (ldb * es) % 16 == 0, 54,
+              "leading dimension not 16-byte aligned");
   QBX_REQUIRE(((uintptr_t)ahi | (uintptr_t)alo | (uintptr_t)bhi | (uintptr_t)blo) % 16 == 0, 54,
               "operand not 16-byte aligned");
-  const CUtensorMap mah = kmajor_map(ahi, k, m, lda);
-  const CUtensorMap mal = kmajor_map(alo, k, m, lda);
-  const CUtensorMap mbh = kmajor_map(bhi, k, n, ldb);
-  const CUtensorMap mbl = kmajor_map(blo, k, n, ldb);
-  const int nkb = (k + tc::BK - 1) / tc::BK;
-  const int tiles = (m / tc::BM) * (n / tc::BN);
+  const CUtensorMap mah = kmajor_map(ahi, k, m, lda, kind);
+  const CUtensorMap mal = kmajor_map(alo, k, m, lda, kind);
+  const CUtensorMap mbh = kmajor_map(bhi, k, n, ldb, kind);
+  const CUtensorMap mbl = kmajor_map(blo, k, n, ldb, kind);
+  const int bk = tc::bk_of(kind);
+  const int nkb = (k + bk - 1) / bk;
+  const int tm = (m + tc::BM - 1) / tc::BM, tn = (n + tc::BN - 1) / tc::BN;
+  const int tiles = tm * tn;
   int sms = 148;
   QBX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device));
   // split K so that about two CTAs per SM are in flight; the partials (FP32)
   // are summed in FP64 afterwards
   int splits = std::max(1, std::min(nkb, (2 * sms + tiles - 1) / tiles));
-  const size_t need = (size_t)splits * m * n;
-  if (need > ctx.tc_ws_elems) {
-    if (ctx.d_tc_ws) cudaFree(ctx.d_tc_ws);
-    QBX_CUDA(cudaMalloc(&ctx.d_tc_ws, need * sizeof(float)));
-    ctx.tc_ws_elems = need;
+  const int kbps = (nkb + splits - 1) / splits;
+  splits = (nkb + kbps - 1) / kbps;
+  if (splits > 1) {
+    const size_t need = (size_t)splits * m * n;
+    if (need > ctx.tc_ws_elems) {
+      if (ctx.d_tc_ws) cudaFree(ctx.d_tc_ws);
+      ctx.d_tc_ws = nullptr;
+      ctx.tc_ws_elems = 0;
+      QBX_CUDA(cudaMalloc(&ctx.d_tc_ws, need * sizeof(float)));
+      ctx.tc_ws_elems = need;
+    }
   }
   if (!ctx.d_tc_err) {
     QBX_CUDA(cudaMalloc(&ctx.d_tc_err, sizeof(int)));
     QBX_CUDA(cudaMemsetAsync(ctx.d_tc_err, 0, sizeof(int), ctx.stream));
   }
-  const int kbps = (nkb + splits - 1) / splits;
-  splits = (nkb + kbps - 1) / kbps;
-  QBX_CUDA(cudaFuncSetAttribute(tc::k_tc_split_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                tc::SMEM_BYTES));
-  dim3 grid(m / tc::BM, n / tc::BN, splits);
-  tc::k_tc_split_gemm<<<grid, tc::THREADS, tc::SMEM_BYTES, ctx.stream>>>(
-      mah, mal, mbh, mbl, m, n, nkb, kbps, (float*)ctx.d_tc_ws, (int*)ctx.d_tc_err);
+  float* ws = splits > 1 ? (float*)ctx.d_tc_ws : nullptr;
+  QBX_REQUIRE(splits > 1 ? tn <= 65535 : tm <= 65535, 54, "too many tiles for the grid");
+  dim3 grid = splits > 1 ? dim3(tm, tn, splits) : dim3(tn, tm, 1);
+  if (kind == tc::KIND_BF16) {
+    QBX_CUDA(cudaFuncSetAttribute(tc::k_tc_split_gemm<tc::KIND_BF16>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
+    tc::k_tc_split_gemm<tc::KIND_BF16><<<grid, tc::THREADS, tc::SMEM_BYTES, ctx.stream>>>(
+        mah, mal, mbh, mbl, m, n, nkb, kbps, ws, C, ldc, alpha, beta, (int*)ctx.d_tc_err);
+  } else {
+    QBX_CUDA(cudaFuncSetAttribute(tc::k_tc_split_gemm<tc::KIND_TF32>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
+    tc::k_tc_split_gemm<tc::KIND_TF32><<<grid, tc::THREADS, tc::SMEM_BYTES, ctx.stream>>>(
+        mah, mal, mbh, mbl, m, n, nkb, kbps, ws, C, ldc, alpha, beta, (int*)ctx.d_tc_err);
+  }
   QBX_LAUNCHED(ctx);
-  // C = alpha * (sum of the split-K partials, in FP64) + beta * C
-  const size_t nn = (size_t)m * n;
-  const int nb = (int)std::min<size_t>((nn + 255) / 256, (size_t)sms * 16);
-  tc::k_reduce_splits<<<nb, 256, 0, ctx.stream>>>((const float*)ctx.d_tc_ws, splits, nn, alpha,
-                                                  beta, C);
-  QBX_LAUNCHED(ctx);
+  if (splits > 1) {
+    const size_t nn = (size_t)m * n;
+    const int nb = (int)std::min<size_t>((nn + 255) / 256, (size_t)sms * 16);
+    k_reduce_splits2d<<<nb, 256, 0, ctx.stream>>>((const float*)ctx.d_tc_ws, splits, m, n, alpha,
+                                                  beta, C, ldc);
+    QBX_LAUNCHED(ctx);
+  }
+}
+
+void tc_split_gemm(Context& ctx, bool ta, bool tb, int m, int n, int k, double alpha,
+                   const void* ahi, const void* alo, int lda, const void* bhi, const void* blo,
+                   int ldb, double beta, double* C) {
+  QBX_REQUIRE(tc_gemm_supported(ctx, ta, tb, m, n, k), 54, "shape not supported by tcgen05 GEMM");
+  tc_gemm_tn(ctx, tc::KIND_BF16, m, n, k, alpha, ahi, alo, lda, bhi, blo, ldb, beta, C, m);
+}
+
+void tc_gemm_kind_tn(Context& ctx, int kind, int m, int n, int k, double alpha, const void* ahi,
+                     const void* alo, int lda, const void* bhi, const void* blo, int ldb,
+                     double beta, double* C, int ldc) {
+  tc_gemm_tn(ctx, kind == TALL_TF32 ? tc::KIND_TF32 : tc::KIND_BF16, m, n, k, alpha, ahi, alo, lda,
+             bhi, blo, ldb, beta, C, ldc);
+}
+
+void tc_tf32_gemm_tn(Context& ctx, int m, int n, int k, double alpha, const float* ahi,
+                     const float* alo, int lda, const float* bhi, const float* blo, int ldb,
+                     double beta, double* C, int ldc) {
+  tc_gemm_tn(ctx, tc::KIND_TF32, m, n, k, alpha, ahi, alo, lda, bhi, blo, ldb, beta, C, ldc);
 }
 
 int tc_check_error(Context& ctx) {

@@ -41,3 +41,18 @@ def test_tcgen05_overlap_of_orthonormal_columns(ctx):
     off = s - np.diag(np.diag(s))
     assert np.abs(off).max() < 2e-7
     assert np.abs(np.diag(s) - 1.0).max() < 1e-4
+
+
+@pytest.mark.parametrize("m,n,k", [(128, 128, 32), (300, 130, 1000), (145838, 256, 1024),
+                                   (1000, 1024, 2048)])
+def test_tcgen05_tf32_split_gemm(ctx, m, n, k):
+    """TF32 hi/lo splits (kind::tf32), the form of the tall updates: ~22
+    significant bits per product term, so FP32-level accuracy; partial tiles
+    in m and n."""
+    rng = np.random.default_rng(m + 3 * n + k)
+    a = rng.standard_normal((k, m)) / np.sqrt(k)
+    b = rng.standard_normal((k, n))
+    ref = a.T @ b
+    d = ctx.split_gemm_tn(a, b, backend=2)
+    scale = np.abs(ref).max()
+    assert np.abs(d - ref).max() < 2e-6 * scale
