@@ -75,8 +75,10 @@ def write_system(sysdef, workdir: str, c: Optional[np.ndarray] = None) -> str:
 
 def run_reference(sysdef, workdir: str, nsteps: int, dump_steps: int = 0,
                   forces: bool = False, wf_dyn: str = "PSDA",
-                  threads: Optional[int] = None, c=None) -> Dict:
-    """Run the compiled reference on sysdef; returns parsed outputs."""
+                  threads: Optional[int] = None, c=None, stress: bool = False) -> Dict:
+    """Run the compiled reference on sysdef; returns parsed outputs.  With
+    stress=True (implies forces) the stress tensor of the force steps is
+    read as out["sigma"][step]."""
     if not os.path.exists(REF_DRIVER):
         raise FileNotFoundError("oracle/_ref/ref_driver not built "
                                 "(make -C oracle)")
@@ -86,7 +88,7 @@ def run_reference(sysdef, workdir: str, nsteps: int, dump_steps: int = 0,
         env["OMP_NUM_THREADS"] = str(threads)
         env["OPENBLAS_NUM_THREADS"] = str(threads)
     subprocess.run([REF_DRIVER, path, str(nsteps), workdir, str(dump_steps),
-                    "1" if forces else "0", wf_dyn], check=True, env=env,
+                    "2" if stress else ("1" if forces else "0"), wf_dyn], check=True, env=env,
                    stdout=subprocess.DEVNULL)
     return load_outputs(workdir)
 
@@ -121,6 +123,9 @@ def load_outputs(workdir: str) -> Dict:
         fp = os.path.join(workdir, f"step{s}_fion.txt")
         if os.path.exists(fp):
             out[f"fion{s}"] = np.loadtxt(fp).reshape(-1, 3)
+        fs = os.path.join(workdir, f"step{s}_sigma.txt")
+        if os.path.exists(fs):
+            out[f"sigma{s}"] = np.loadtxt(fs)
     fc = os.path.join(workdir, "final_c.bin")
     if os.path.exists(fc):
         a = np.fromfile(fc).reshape(nst, ngw, 2)

@@ -94,9 +94,12 @@ def half_sphere(cell: np.ndarray, ecut: float) -> np.ndarray:
 
 @dataclass
 class Basis:
-    """G vectors of a Gamma half-sphere basis (src/Basis.cpp:646-690)."""
+    """G vectors of a Gamma half-sphere basis (src/Basis.cpp:646-690).
+    With fixed_hkl the Miller set is given instead of cut from the sphere
+    (used to differentiate at a fixed set of plane waves under strain)."""
     cell: np.ndarray
     ecut: float
+    fixed_hkl: Optional[np.ndarray] = None
     hkl: np.ndarray = field(init=False)
     gx: np.ndarray = field(init=False)   # (ng, 3)
     g2: np.ndarray = field(init=False)
@@ -105,7 +108,7 @@ class Basis:
     gi: np.ndarray = field(init=False)
 
     def __post_init__(self):
-        self.hkl = half_sphere(self.cell, self.ecut)
+        self.hkl = half_sphere(self.cell, self.ecut) if self.fixed_hkl is None else self.fixed_hkl
         b = reciprocal(self.cell)
         self.gx = self.hkl @ b
         self.g2 = (self.gx ** 2).sum(1)
@@ -435,14 +438,19 @@ def fold_in_ws(v: np.ndarray, cell: np.ndarray) -> np.ndarray:
     return v
 
 
-def esr_forces(system, zv, positions):
-    """Pseudocharge repulsion E_sr and its forces
-    (src/EnergyFunctional.cpp:1112-1192)."""
+# Voigt order of the reference's stress components: xx yy zz xy yz xz
+VOIGT = ((0, 0), (1, 1), (2, 2), (0, 1), (1, 2), (0, 2))
+
+
+def esr_forces(system, zv, positions, with_stress=False):
+    """Pseudocharge repulsion E_sr, its forces and (with_stress) its stress
+    sigma_esr (src/EnergyFunctional.cpp:1112-1194)."""
     cell = system.cell
     b = reciprocal(cell)
     d = [2.0 * math.pi / np.linalg.norm(b[i]) for i in range(3)]
     nsp = len(positions)
     esr = 0.0
+    sig = np.zeros(6)
     f = [np.zeros_like(p) for p in positions]
     from math import erfc
     for is1 in range(nsp):
@@ -470,6 +478,12 @@ def esr_forces(system, zv, positions):
                                 dedr = -fac * (term + de) / (r12 * r12)
                                 f[is1][ia1] -= dedr * x
                                 f[is2][ia2] += dedr * x
+                                if with_stress:
+                                    for k, (i, j) in enumerate(VOIGT):
+                                        sig[k] += dedr * x[i] * x[j]
+    if with_stress:
+        omega = abs(np.linalg.det(np.asarray(cell, float)))
+        return esr, f, -sig / omega
     return esr, f
 
 
@@ -477,14 +491,16 @@ class ElectronicStep:
     """State and operators of the reference's SCF iteration with nite=0
     (src/BOSampleStepper.cpp:795-977) on one Gamma-point SlaterDet."""
 
-    def __init__(self, system, c: Optional[np.ndarray] = None):
+    def __init__(self, system, c: Optional[np.ndarray] = None, like=None):
+        """like: another ElectronicStep whose plane-wave sets and grid are
+        kept (a strained copy of a system for finite differences)."""
         self.system = system
         cell = np.array(system.cell, float)
         self.cell = cell
         self.omega = abs(np.linalg.det(cell))
-        self.wb = Basis(cell, system.ecut)
-        self.vb = Basis(cell, 4.0 * system.ecut)
-        shape = dense_grid(cell, system.ecut)
+        self.wb = Basis(cell, system.ecut, None if like is None else like.wb.hkl)
+        self.vb = Basis(cell, 4.0 * system.ecut, None if like is None else like.vb.hkl)
+        shape = dense_grid(cell, system.ecut) if like is None else list(like.grid_shape)
         self.grid_shape = shape
         self.wgrid = Grid(self.wb, shape)
         self.vgrid = Grid(self.vb, shape)
@@ -613,6 +629,7 @@ class ElectronicStep:
             e, v = lda_pz(rho)
             vxc = v
             self.exc = (rho * e).sum() * om / self.N
+            self.xc_parts = (e, v, None, None)
         else:
             grads = []
             for j in range(3):
@@ -627,6 +644,7 @@ class ElectronicStep:
                 vxt += self.vgrid.backward(t).real.ravel()
             vxc = v1 + vxt
             self.exc = (rho * e).sum() * om / self.N
+            self.xc_parts = (e, v1, v2, grads)
         g0 = vb.g0()
         eps = 2.0 * (np.conj(rhoelg) * self.vion_g).real.sum()
         eps -= (np.conj(rhoelg[g0]) * self.vion_g[g0]).real
@@ -702,6 +720,97 @@ class ElectronicStep:
             f_loc = -2.0 * self.omega * (tmp.T @ vb.gx)
             out.append(fnl[isp] + self.fion_esr[isp] + f_loc)
         return out
+
+    # ---- stress tensor (src/EnergyFunctional.cpp:397-1044 with
+    # compute_stress, src/XCPotential.cpp:467-640,
+    # src/NonLocalPotential.cpp:235-560 dtwnl and :1790-2069)
+    def dtwnl(self, isp):
+        """Strain derivatives of the projector forms, dt[ipr, ij, G]
+        (src/NonLocalPotential.cpp:266-440, Kleinman-Bylander l = 0, 1)."""
+        sp = self.species[isp]
+        wb = self.wb
+        g, gi, gx = wb.g, wb.gi, wb.gx
+        s14pi = math.sqrt(1.0 / FPI)
+        s34pi = math.sqrt(3.0 / FPI)
+        out = []
+        for iop, (l, _, _) in enumerate(sp.proj):
+            v, dv = sp.vnlg(iop, g)
+            if l == 0:
+                tmp = gi * s14pi * dv
+                out.append(np.array([tmp * gx[:, i] * gx[:, j] for i, j in VOIGT]))
+            else:
+                y = [s34pi * gx[:, m] * gi for m in range(3)]
+                for m in range(3):
+                    fac = -y[m] * (v - g * dv) * gi * gi
+                    dt = []
+                    for i, j in VOIGT:
+                        t = fac * gx[:, i] * gx[:, j]
+                        if j == m:
+                            t = t + v * y[i]
+                        dt.append(t)
+                    out.append(np.array(dt))
+        return np.array(out)                       # (npr, 6, ng)
+
+    def stress(self):
+        """sigma (6, Voigt order) and its parts at the current C, after
+        update_density, update_vhxc and energy."""
+        wb, vb, om = self.wb, self.vb, self.omega
+        parts = {}
+        # kinetic: (2/Omega) sum_G psi2(G) G_i G_j
+        psi2 = (self.occ[:, None] * np.abs(self.c) ** 2).sum(0)
+        parts["ekin"] = np.array([2.0 * (psi2 * wb.gx[:, i] * wb.gx[:, j]).sum()
+                                  for i, j in VOIGT]) / om
+        eye = np.array([1.0, 1.0, 1.0, 0.0, 0.0, 0.0])
+        # local pseudopotential
+        dvion = np.zeros(vb.size, complex)
+        for isp, sp in enumerate(self.species):
+            v, dv = sp.dvlocg(vb.g)
+            dvion += self.sfac[isp] * dv / om
+        fac = 2.0 * vb.gi * (np.conj(self.rhoelg) * dvion).real
+        parts["eps"] = eye * self.eps / om + np.array(
+            [(fac * vb.gx[:, i] * vb.gx[:, j]).sum() for i, j in VOIGT])
+        # Hartree (with the Gaussian pseudocharges)
+        temp = np.abs(self.rhogt) ** 2 * vb.g2i ** 2
+        for isp, sp in enumerate(self.species):
+            sg = self.sfac[isp]
+            temp = temp + 2.0 * 0.25 * RCPS * RCPS * (
+                self.rhogt.real * sg.real + self.rhogt.imag * sg.imag) * self.rhops[isp] * vb.g2i
+        tsum = np.array([(temp * vb.gx[:, i] * vb.gx[:, j]).sum() for i, j in VOIGT])
+        parts["ehart"] = eye * self.ehart / om - 2.0 * FPI * tsum
+        # exchange-correlation
+        e, v1, v2, grads = self.xc_parts
+        rho = self.rhor
+        dsum = (rho * (e - v1)).sum()
+        if v2 is None:
+            parts["exc"] = -eye * dsum / self.N
+        else:
+            g2 = grads[0] ** 2 + grads[1] ** 2 + grads[2] ** 2
+            sx = []
+            for i, j in VOIGT:
+                t = grads[i] * grads[j] * v2
+                if i == j:
+                    t = t + g2 * v2
+                sx.append(t.sum())
+            parts["exc"] = -(eye * dsum + np.array(sx)) / self.N
+        # nonlocal
+        tsum = np.zeros(6)
+        for isp, tw, lp, dfac in self.nl:
+            a = self.anl(isp, tw, lp)                 # (npr, na, ng)
+            npr, na, ng = a.shape
+            F = self.real_dot(a.reshape(npr * na, ng), self.c)
+            fnl = F * np.repeat(dfac, na)[:, None] / om
+            dt = self.dtwnl(isp)                      # (npr, 6, ng)
+            for k in range(6):
+                ak = self.anl(isp, dt[:, k, :], lp).reshape(npr * na, ng)
+                dF = self.real_dot(ak, self.c)
+                tsum[k] += (2.0 * self.occ[None, :] * fnl * dF).sum()
+        parts["enl"] = (eye * self.enl + tsum) / om
+        # pseudocharge repulsion
+        zv = [sp.zval for sp in self.species]
+        _, _, parts["esr"] = esr_forces(self.system, zv, self.positions, with_stress=True)
+        self.sigma_parts = parts
+        self.sigma = sum(parts.values())
+        return self.sigma
 
     def eigenvalue_sum(self):
         """Wavefunction::dot (src/SlaterDet.cpp:1122-1153)."""

@@ -11,7 +11,11 @@
 // (src/Basis.cpp:544-597) never leaks into the inputs.
 //
 // usage: ref_driver <system.txt> <nsteps> <outdir> [dump_steps=0]
-//                   [forces=0] [threads-note]
+//                   [forces=0] [wf_dyn=PSDA]
+// forces = 1: ionic forces at the dumped steps and the last step; forces = 2:
+// forces and the stress tensor (EnergyFunctional::energy with
+// compute_stress, src/EnergyFunctional.cpp:397-1044), written as
+// step<N>_sigma.txt (xx yy zz xy yz xz).
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -206,11 +210,12 @@ int main(int argc, char** argv)
     const double t0 = wall();
     cd.update_density();
     const double t1 = wall();
-    ef.update_vhxc(false);
-    const double t2 = wall();
     const bool last = ( itscf == nsteps - 1 );
     const bool fstep = want_forces && ( last || itscf < dump_steps );
-    ef.energy(true, dwf, fstep, fion, false, sigma);
+    const bool sstep = fstep && want_forces == 2;
+    ef.update_vhxc(sstep);
+    const double t2 = wall();
+    ef.energy(true, dwf, fstep, fion, sstep, sigma);
     const double t3 = wall();
     const double eigsum = real(s.wf.dot(dwf));
     if ( itscf < dump_steps )
@@ -237,6 +242,14 @@ int main(int argc, char** argv)
           out[dst] = v.real(); out[dst+1] = v.imag();
         }
       write_bin(pre.str() + "c.bin", &out[0], out.size()*sizeof(double));
+    }
+    if ( sstep )
+    {
+      ostringstream fn; fn << outdir << "/step" << itscf << "_sigma.txt";
+      ofstream so(fn.str().c_str());
+      so << setprecision(17);
+      for ( int i = 0; i < 6; i++ )
+        so << sigma[i] << "\n";
     }
     if ( fstep )
     {

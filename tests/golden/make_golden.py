@@ -4,7 +4,7 @@ electronic step, compiled single-task by oracle/Makefile (oracle/_ref).
     make -C oracle && python tests/golden/make_golden.py
 
 Each fixture holds, for a seeded synthetic system: every energy term of each
-SCF step, the ionic forces at the first and last step, the grid sizes and
+SCF step, the ionic forces and the stress tensor at the first and last step, the grid sizes and
 basis size, a fixed sample of the density and local potential on the grid,
 H*psi and wavefunction coefficients of a few bands (all G for small bases,
 a fixed sample of G otherwise), and per-band norms.
@@ -32,7 +32,7 @@ NBANDS_FULL = 4
 def make(name: str, nsteps: int, workdir: str) -> str:
     s = systems.get(name)
     out = inputs.run_reference(s, workdir, nsteps, dump_steps=1, forces=True,
-                               threads=os.cpu_count())
+                               stress=True, threads=os.cpu_count())
     meta = out["meta"]
     e = out["energies"]
     rng = np.random.default_rng(12345)
@@ -56,6 +56,7 @@ def make(name: str, nsteps: int, workdir: str) -> str:
         final_c_bands=out["final_c"][:NBANDS_FULL, gidx],
         final_c_norm2=(np.abs(out["final_c"]) ** 2).sum(1),
         fion_first=out["fion0"], fion_last=out[f"fion{nsteps - 1}"],
+        sigma_first=out["sigma0"], sigma_last=out[f"sigma{nsteps - 1}"],
     )
     for k in ("ekin", "eps", "enl", "ehart", "ecoul", "exc", "esr", "eself",
               "etotal", "eigenvalue_sum"):

@@ -4,6 +4,8 @@ The fixtures in tests/golden/ were produced by the reference Qbox sources
 compiled single-task (tests/golden/make_golden.py).  These tests pin the
 oracle that the GPU parity tests compare against.
 """
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -86,3 +88,69 @@ def test_fft_roundtrip_and_gaussian():
     d = np.minimum(x, 1 - x) * L
     r2 = d[None, None, :] ** 2 + d[None, :, None] ** 2 + d[:, None, None] ** 2
     np.testing.assert_allclose(f, np.exp(-a * r2), atol=1e-11)
+
+
+@pytest.mark.parametrize("name", ["si8", "si64", "h2o32"])
+def test_oracle_stress_matches_reference(name):
+    """Stress tensor (src/EnergyFunctional.cpp:397-1044 with compute_stress,
+    src/XCPotential.cpp:467-640, src/NonLocalPotential.cpp:1790-2069) at
+    the first step against the reference's own sigma."""
+    g = golden(name)
+    es = qbox_np.ElectronicStep(systems.get(name))
+    es.update_density()
+    es.update_vhxc()
+    es.energy(False)
+    np.testing.assert_allclose(es.stress(), g["sigma_first"], rtol=0, atol=1e-12)
+
+
+def _strained(s, es, eps):
+    m = np.eye(3) + eps
+    s2 = dataclasses.replace(s, cell=np.asarray(s.cell) @ m,
+                             atoms=[(i, p @ m) for i, p in s.atoms])
+    e2 = qbox_np.ElectronicStep(s2, c=es.c, like=es)
+    e2.update_density()
+    e2.update_vhxc()
+    return e2.energy(False)
+
+
+def test_stress_is_the_strain_derivative():
+    """sigma_ij = -(1/Omega) dE/d(eps_ij) at fixed coefficients and fixed
+    plane-wave set, by central differences with strain 1e-4 (the check of
+    test/si4stress/check_stress.sh, here without re-converging)."""
+    s = systems.si8()
+    es = qbox_np.ElectronicStep(s)
+    es.update_density()
+    es.update_vhxc()
+    es.energy(False)
+    sig = es.stress()
+    h = 1e-4
+    for k, (i, j) in enumerate(qbox_np.VOIGT):
+        eps = np.zeros((3, 3))
+        eps[i, j] += h
+        if i != j:
+            eps[j, i] += h
+        d = (_strained(s, es, eps) - _strained(s, es, -eps)) / (2 * h)
+        fd = -d / es.omega / (1 if i == j else 2)
+        assert abs(fd - sig[k]) < 1e-7, (k, fd, sig[k])
+
+
+def test_forces_are_the_position_derivative():
+    """fion = -dE/dtau at fixed coefficients, central differences 1e-3 bohr."""
+    s = systems.si8()
+    es = qbox_np.ElectronicStep(s)
+    es.update_density()
+    es.update_vhxc()
+    es.energy(False, forces=True)
+    f = np.concatenate(es.fion)
+    h = 1e-3
+    for a, j in ((0, 0), (3, 1), (5, 2)):
+        e = []
+        for sgn in (1, -1):
+            atoms = [(i, p.copy()) for i, p in s.atoms]
+            atoms[a][1][j] += sgn * h
+            s2 = dataclasses.replace(s, atoms=atoms)
+            e2 = qbox_np.ElectronicStep(s2, c=es.c, like=es)
+            e2.update_density()
+            e2.update_vhxc()
+            e.append(e2.energy(False))
+        assert abs(-(e[0] - e[1]) / (2 * h) - f[a, j]) < 1e-6, (a, j)
