@@ -112,9 +112,25 @@ int qbx_psda_reset(qbx_context* ctx);
 
 /* One electronic step of the SCF loop with nite = 0
  * (src/BOSampleStepper.cpp:795-977): update_density, update_vhxc,
- * energy(true,...), eigenvalue_sum, PSDA update. */
+ * energy(true,...), eigenvalue_sum, PSDA update.  compute_forces: bit 0
+ * computes the ionic forces (fion), bit 1 the stress tensor of the step's
+ * input state (read it with qbx_get_stress). */
 int qbx_scf_step(qbx_context* ctx, int compute_forces, double* energies,
                  double* fion);
+
+/* The stress tensor of EnergyFunctional::energy(..., compute_stress=true,
+ * sigma) (src/EnergyFunctional.cpp:440-1044, XCPotential::compute_stress
+ * src/XCPotential.cpp:467-640, NonLocalPotential::energy's stress
+ * src/NonLocalPotential.cpp:1790-2069, E_sr src/EnergyFunctional.cpp:
+ * 1112-1194) for the state of the last qbx_energy call: call it after
+ * qbx_energy and before anything that changes C or the potentials.
+ * sigma[6] in the order xx yy zz xy yz xz (Hartree/bohr^3); parts (may be
+ * NULL) receives 36 values: the ekin, eps, enl, ehart, exc and esr parts,
+ * 6 each. */
+int qbx_stress(qbx_context* ctx, double* sigma, double* parts);
+/* The stress computed by the last qbx_scf_step with bit 1 of
+ * compute_forces set (or the last qbx_stress). */
+int qbx_get_stress(qbx_context* ctx, double* sigma, double* parts);
 
 /* FourierTransform::backward(c1, c2, f) on the density grid
  * (src/FourierTransform.cpp:193-205): two bands n1, n2 of the current

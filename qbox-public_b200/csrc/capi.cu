@@ -74,9 +74,14 @@ void free_cell(Context& c) {
 
 void free_atoms(Context& c) {
   double** bufs[] = {&c.d_anl, &c.d_fnl, &c.d_dfnl, &c.d_pdfac, &c.d_sfac, &c.d_vps,
-                     &c.d_rhops_sp, &c.d_fion};
+                     &c.d_rhops_sp, &c.d_fion, &c.d_dvps, &c.d_vnl, &c.d_dvnl,
+                     &c.d_tau_all, &c.d_astress};
   for (double** b : bufs) dfree(*b);
   dfree(c.d_patom);
+  dfree(c.d_pcol);
+  if (c.sa_hi) { cudaFree(c.sa_hi); c.sa_hi = nullptr; }
+  if (c.sa_lo) { cudaFree(c.sa_lo); c.sa_lo = nullptr; }
+  c.have_stress = false;
   c.nproj = 0;
 }
 
@@ -349,17 +354,20 @@ int qbx_set_atoms(qbx_context* h, const int* na, const double* tau) {
     // projector columns: species, then projector (l,m), then atom
     c.nproj = 0;
     c.proj_dfac.clear();
-    std::vector<int> patom;
-    int atom0 = 0;
+    std::vector<int> patom, pcol;
+    int atom0 = 0, nrad = 0;
     for (int is = 0; is < nsp; is++) {
       const SpeciesTables& sp = c.species[is];
-      for (size_t iop = 0; iop < sp.proj_l.size(); iop++)
+      for (size_t iop = 0; iop < sp.proj_l.size(); iop++) {
         for (int m = 0; m < 2 * sp.proj_l[iop] + 1; m++)
           for (int ia = 0; ia < na[is]; ia++) {
             c.proj_dfac.push_back(sp.proj_d[iop]);
             patom.push_back(atom0 + ia);
+            pcol.insert(pcol.end(), {sp.proj_l[iop], m, nrad, atom0 + ia});
             c.nproj++;
           }
+        nrad++;
+      }
       atom0 += na[is];
     }
     const int ngw = c.wb.ng, ngv = c.vb.ng;
@@ -369,19 +377,38 @@ int qbx_set_atoms(qbx_context* h, const int* na, const double* tau) {
       c.d_dfnl = dalloc<double>((size_t)c.nproj * c.nst);
       c.d_pdfac = dupload(c.proj_dfac);
       c.d_patom = dupload(patom);
+      c.d_pcol = dupload(pcol);
+      // radial projector tables V_nl(|G|), dV_nl/dG on the wavefunction
+      // sphere (Species::dvnlg, src/Species.cpp:1172-1185) for the stress
+      std::vector<double> vnl((size_t)nrad * ngw), dvnl((size_t)nrad * ngw);
+      int r = 0;
+      for (int is = 0; is < nsp; is++)
+        for (size_t iop = 0; iop < c.species[is].proj_l.size(); iop++, r++)
+          for (int ig = 0; ig < ngw; ig++)
+            c.species[is].dvnlg((int)iop, c.wb.g[ig], vnl[(size_t)r * ngw + ig],
+                                dvnl[(size_t)r * ngw + ig]);
+      c.d_vnl = dupload(vnl);
+      c.d_dvnl = dupload(dvnl);
+    }
+    {
+      std::vector<double> tall;
+      for (int is = 0; is < nsp; is++) tall.insert(tall.end(), c.tau[is].begin(), c.tau[is].end());
+      c.d_tau_all = dupload(tall);
     }
     c.d_fion = dalloc<double>(3 * std::max(1, natoms));
     // species tables on the density sphere (EnergyFunctional::cell_moved,
     // src/EnergyFunctional.cpp:1200-1245)
-    std::vector<double> vps((size_t)ngv * nsp), rhops((size_t)ngv * nsp);
+    std::vector<double> vps((size_t)ngv * nsp), rhops((size_t)ngv * nsp), dvps((size_t)ngv * nsp);
     for (int is = 0; is < nsp; is++)
       for (int ig = 0; ig < ngv; ig++) {
         double v, dv;
         c.species[is].dvlocg(c.vb.g[ig], v, dv);
         vps[(size_t)is * ngv + ig] = v / c.vb.omega;
+        dvps[(size_t)is * ngv + ig] = dv / c.vb.omega;
         rhops[(size_t)is * ngv + ig] = c.species[is].rhopsg(c.vb.g[ig]) / c.vb.omega;
       }
     c.d_vps = dupload(vps);
+    c.d_dvps = dupload(dvps);
     c.d_rhops_sp = dupload(rhops);
     c.d_sfac = dalloc<double>(2 * (size_t)ngv * nsp);
     if (!c.d_vion) c.d_vion = dalloc<double>(2 * (size_t)ngv);
@@ -392,7 +419,7 @@ int qbx_set_atoms(qbx_context* h, const int* na, const double* tau) {
       zv[is] = c.species[is].zval;
       c.eself += na[is] * c.species[is].eself();
     }
-    c.esr = esr_energy_forces(c.wb.cell, c.tau, zv, 1.5, c.fion_esr);
+    c.esr = esr_energy_forces(c.wb.cell, c.tau, zv, 1.5, c.fion_esr, c.sigma_esr);
     alloc_mixed(c);
     QBX_CUDA(cudaStreamSynchronize(c.stream));
   });
@@ -515,15 +542,38 @@ int qbx_psda_reset(qbx_context* h) {
 int qbx_scf_step(qbx_context* h, int forces, double* energies, double* fion) {
   return guarded(h, [&](Context& c) {
     check_ready(c, true);
+    const bool want_f = (forces & 1) != 0, want_s = (forces & 2) != 0;
     update_density(c);
     update_vhxc(c);
-    energy(c, true, forces != 0);
+    energy(c, true, want_f);
+    if (want_s) compute_stress(c);
     c.eigsum = launch_eigsum(c);
     fill_energies(c, energies);
-    if (forces && fion) std::memcpy(fion, c.fion.data(), sizeof(double) * c.fion.size());
+    if (want_f && fion) std::memcpy(fion, c.fion.data(), sizeof(double) * c.fion.size());
     psda_update(c);
     QBX_CUDA(cudaStreamSynchronize(c.stream));
     QBX_REQUIRE(tc_check_error(c) == 0, 55, "tcgen05 GEMM pipeline wait timed out");
+  });
+}
+
+static void copy_stress(const Context& c, double* sigma, double* parts) {
+  if (sigma) std::memcpy(sigma, c.sigma, sizeof(c.sigma));
+  if (parts) std::memcpy(parts, c.sigma_parts, sizeof(c.sigma_parts));
+}
+
+int qbx_stress(qbx_context* h, double* sigma, double* parts) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, true);
+    compute_stress(c);
+    QBX_CUDA(cudaStreamSynchronize(c.stream));
+    copy_stress(c, sigma, parts);
+  });
+}
+
+int qbx_get_stress(qbx_context* h, double* sigma, double* parts) {
+  return guarded(h, [&](Context& c) {
+    QBX_REQUIRE(c.have_stress, 7, "no stress computed yet");
+    copy_stress(c, sigma, parts);
   });
 }
 

@@ -416,7 +416,11 @@ static void fold_in_ws(const double cell[9], double v[3]) {
 double esr_energy_forces(const double cell[9],
                          const std::vector<std::vector<double>>& tau,
                          const std::vector<double>& zv, double rcps,
-                         std::vector<std::vector<double>>& f) {
+                         std::vector<std::vector<double>>& f, double* sigma) {
+  // Voigt pairs xx yy zz xy yz xz; sigma_esr = -(1/Omega) sum dedr x_i x_j
+  // (src/EnergyFunctional.cpp:1173-1194)
+  static const int vi[6] = {0, 1, 2, 0, 1, 0}, vj[6] = {0, 1, 2, 1, 2, 2};
+  double sig[6] = {0, 0, 0, 0, 0, 0};
   const int nsp = (int)tau.size();
   f.assign(nsp, std::vector<double>());
   for (int is = 0; is < nsp; is++) f[is].assign(tau[is].size(), 0.0);
@@ -463,10 +467,18 @@ double esr_energy_forces(const double cell[9],
                   f[is1][3 * ia1 + j] -= dedr * x[j];
                   f[is2][3 * ia2 + j] += dedr * x[j];
                 }
+                for (int k = 0; k < 6; k++) sig[k] += dedr * x[vi[k]] * x[vj[k]];
               }
         }
       }
     }
+  if (sigma) {
+    const double* a = cell;
+    const double omega = std::fabs(a[0] * (a[4] * a[8] - a[5] * a[7]) -
+                                   a[1] * (a[3] * a[8] - a[5] * a[6]) +
+                                   a[2] * (a[3] * a[7] - a[4] * a[6]));
+    for (int k = 0; k < 6; k++) sigma[k] = -sig[k] / omega;
+  }
   return esr;
 }
 

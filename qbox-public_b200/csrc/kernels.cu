@@ -212,6 +212,15 @@ __global__ void k_axpy(double* __restrict__ y, const double* __restrict__ x, siz
     y[i] += x[i];
 }
 
+// sum of the energy density and of rho * v1
+struct SumRhoV1F {
+  const double* e; const double* rho; const double* v1;
+  __device__ void operator()(size_t i, double* a) const {
+    a[0] += e[i];
+    a[1] += rho[i] * v1[i];
+  }
+};
+
 // XCPotential::update (src/XCPotential.cpp:124-465): vxc and E_xc.
 void launch_xc(Context& ctx) {
   const size_t N = ctx.N();
@@ -235,7 +244,12 @@ void launch_xc(Context& ctx) {
   k_pbe<<<nb, kThreads, 0, ctx.stream>>>(ctx.d_rhor, ctx.d_grad, N, ctx.d_vxc, ctx.d_vx2,
                                          ctx.d_exc);
   QBX_LAUNCHED(ctx);
-  ctx.exc = dsum(ctx, ctx.d_exc, N) * om / (double)N;
+  {
+    double s2[2];
+    reduce<2>(ctx, SumRhoV1F{ctx.d_exc, ctx.d_rhor, ctx.d_vxc}, N, s2);
+    ctx.exc = s2[0] * om / (double)N;
+    ctx.xc_rhov1 = s2[1];    // sum_r rho v1, for the XC stress
+  }
   // vxc += sum_j backward(i G_j forward(grad_j vxc2))
   for (int j = 0; j < 3; j++) {
     k_mul<<<nb, kThreads, 0, ctx.stream>>>(ctx.d_grad + j * N, ctx.d_vx2, N, ctx.d_exc);
@@ -731,6 +745,211 @@ void launch_setup_atoms(Context& ctx) {
     dfree(d_tau);
   }
   QBX_REQUIRE(col == ctx.nproj, 30, "projector count mismatch");
+}
+
+// ------------------------------------------------------------ stress
+// The stress tensor of EnergyFunctional::energy with compute_stress
+// (src/EnergyFunctional.cpp:440-1044), components in the reference's Voigt
+// order xx yy zz xy yz xz.  Every part is a reduction over the state left
+// by update_density, update_vhxc and energy; the nonlocal part recomputes
+// the projections with the strain derivatives of the projector forms (one
+// K x nproj block and one GEMM per component) instead of storing them.
+__device__ __forceinline__ void voigt6(double x, double y, double z, double w, double* a) {
+  a[0] += w * x * x;
+  a[1] += w * y * y;
+  a[2] += w * z * z;
+  a[3] += w * x * y;
+  a[4] += w * y * z;
+  a[5] += w * x * z;
+}
+
+// kinetic: sum_n occ_n |c_n(G)|^2 G_i G_j (src/EnergyFunctional.cpp:440-570)
+struct EkinStressF {
+  const double2* c; const double* gx; const double* occ; int ngw;
+  __device__ void operator()(size_t i, double* a) const {
+    const int n = (int)(i / ngw), ig = (int)(i - (size_t)n * ngw);
+    const double2 v = c[i];
+    voigt6(gx[ig], gx[ngw + ig], gx[2 * ngw + ig], occ[n] * (v.x * v.x + v.y * v.y), a);
+  }
+};
+
+// local pseudopotential: 2/|G| Re(conj(rho_el) dV_ion) G_i G_j, dV_ion =
+// sum_s S_s(G) dV_s(G)/Omega (src/EnergyFunctional.cpp:574-608)
+struct EpsStressF {
+  const double2* rhog; const double2* sfac; const double* dvps; const double* g2i;
+  const double* gx; int ng, nsp; double om_inv;
+  __device__ void operator()(size_t i, double* a) const {
+    double dx = 0.0, dy = 0.0;
+    for (int s = 0; s < nsp; s++) {
+      const double2 sg = sfac[(size_t)s * ng + i];
+      const double d = dvps[(size_t)s * ng + i];
+      dx += sg.x * d;
+      dy += sg.y * d;
+    }
+    const double2 r = rhog[i];
+    const double w = 2.0 * sqrt(g2i[i]) * om_inv * (r.x * dx + r.y * dy);
+    voigt6(gx[i], gx[ng + i], gx[2 * ng + i], w, a);
+  }
+};
+
+// Hartree with the Gaussian pseudocharges: |rho_t|^2/G^4 + sum_s
+// rcps^2/2 Re(rho_t conj S_s) rhops_s/G^2 (src/EnergyFunctional.cpp:611-683)
+struct EhartStressF {
+  const double2* rhog; const double2* rhops_t; const double2* sfac; const double* rhops;
+  const double* g2i; const double* gx; int ng, nsp; double om_inv, rc2;
+  __device__ void operator()(size_t i, double* a) const {
+    const double2 r = rhog[i], p = rhops_t[i];
+    const double tx = r.x * om_inv + p.x, ty = r.y * om_inv + p.y;
+    const double gi2 = g2i[i];
+    double w = (tx * tx + ty * ty) * gi2 * gi2;
+    for (int s = 0; s < nsp; s++) {
+      const double2 sg = sfac[(size_t)s * ng + i];
+      w += 0.5 * rc2 * (tx * sg.x + ty * sg.y) * rhops[(size_t)s * ng + i] * gi2;
+    }
+    voigt6(gx[i], gx[ng + i], gx[2 * ng + i], w, a);
+  }
+};
+
+// XC, LDA: sum_r rho (e - v) with e the energy per particle
+struct LdaStressF {
+  const double* rhoe; const double* rho; const double* v;
+  __device__ void operator()(size_t i, double* a) const { a[0] += rhoe[i] - rho[i] * v[i]; }
+};
+
+// XC, GGA gradient part: v2 (|grad rho|^2 delta_ij + d_i rho d_j rho)
+// (src/XCPotential.cpp:520-640)
+struct GgaStressF {
+  const double* grad; const double* v2; size_t N;
+  __device__ void operator()(size_t i, double* a) const {
+    const double x = grad[i], y = grad[N + i], z = grad[2 * N + i];
+    const double w = v2[i], g2 = x * x + y * y + z * z;
+    a[0] += w * (g2 + x * x);
+    a[1] += w * (g2 + y * y);
+    a[2] += w * (g2 + z * z);
+    a[3] += w * x * y;
+    a[4] += w * y * z;
+    a[5] += w * x * z;
+  }
+};
+
+// Strain derivative of the projector forms times the structure phase,
+// component ij, for every projector column (src/NonLocalPotential.cpp:
+// 266-440 for l = 0, 1, phases as in anl):
+//   l = 0: dt = s14pi dV/dG G_i G_j / |G|
+//   l = 1: dt_m = -y_m (V - |G| dV/dG) G_i G_j / G^2 + [j == m] V y_i,
+//          y_m = s34pi G_m / |G|
+__global__ void k_danl(const double* __restrict__ gx, const double* __restrict__ g2, int ngw,
+                       const double* __restrict__ vnl, const double* __restrict__ dvnl,
+                       const int* __restrict__ pcol, const double* __restrict__ tau, int i,
+                       int j, double2* __restrict__ out) {
+  const int p = blockIdx.y;
+  const int l = pcol[4 * p], m = pcol[4 * p + 1], rad = pcol[4 * p + 2], at = pcol[4 * p + 3];
+  const double tx = tau[3 * at], ty = tau[3 * at + 1], tz = tau[3 * at + 2];
+  const double s14pi = sqrt(1.0 / (4.0 * M_PI)), s34pi = sqrt(3.0 / (4.0 * M_PI));
+  const double* v = vnl + (size_t)rad * ngw;
+  const double* dv = dvnl + (size_t)rad * ngw;
+  double2* o = out + (size_t)p * ngw;
+  for (int ig = blockIdx.x * blockDim.x + threadIdx.x; ig < ngw; ig += gridDim.x * blockDim.x) {
+    const double G[3] = {gx[ig], gx[ngw + ig], gx[2 * ngw + ig]};
+    const double gg = g2[ig];
+    const double gi = gg > 0.0 ? 1.0 / sqrt(gg) : 0.0;
+    double t;
+    if (l == 0) {
+      t = gi * s14pi * dv[ig] * G[i] * G[j];
+    } else {
+      const double ym = s34pi * G[m] * gi;
+      const double g = gg * gi;
+      t = -ym * (v[ig] - g * dv[ig]) * gi * gi * G[i] * G[j];
+      if (j == m) t += v[ig] * s34pi * G[i] * gi;
+    }
+    double sn, cs;
+    sincos(G[0] * tx + G[1] * ty + G[2] * tz, &sn, &cs);
+    // exp(-i G.tau) = (cs, -sn); times -i for l = 1: (-sn, -cs)
+    o[ig] = (l == 0) ? make_double2(t * cs, -t * sn) : make_double2(-t * sn, -t * cs);
+  }
+}
+
+// sum_{p,n} 2 occ_n fnl(p,n) dF(p,n), fnl = D F / Omega
+struct EnlStressF {
+  const double* fnl; const double* dfnl; const double* occ; int np;
+  __device__ void operator()(size_t i, double* a) const {
+    const int n = (int)(i / np);
+    a[0] += 2.0 * occ[n] * fnl[i] * dfnl[i];
+  }
+};
+
+void compute_stress(Context& ctx) {
+  static const int vi[6] = {0, 1, 2, 0, 1, 0}, vj[6] = {0, 1, 2, 1, 2, 2};
+  const double om = ctx.wb.omega, om_inv = 1.0 / om;
+  const int ngw = ctx.wb.ng, ngv = ctx.vb.ng, nst = ctx.nst, np = ctx.nproj;
+  const int nsp = (int)ctx.species.size();
+  const size_t N = ctx.N();
+  double* P = ctx.sigma_parts;        // ekin, eps, enl, ehart, exc, esr
+  const double eye[6] = {1, 1, 1, 0, 0, 0};
+  double t[6];
+  // kinetic
+  reduce<6>(ctx, EkinStressF{(const double2*)ctx.d_c, ctx.d_gx_w, ctx.d_occ, ngw},
+            (size_t)ngw * nst, t);
+  for (int k = 0; k < 6; k++) P[k] = 2.0 * t[k] * om_inv;
+  // local pseudopotential
+  reduce<6>(ctx, EpsStressF{(const double2*)ctx.d_rhog, (const double2*)ctx.d_sfac, ctx.d_dvps,
+                            ctx.d_g2i_v, ctx.d_gx_v, ngv, nsp, om_inv},
+            (size_t)ngv, t);
+  for (int k = 0; k < 6; k++) P[6 + k] = eye[k] * ctx.eps * om_inv + t[k];
+  // Hartree
+  reduce<6>(ctx, EhartStressF{(const double2*)ctx.d_rhog, (const double2*)ctx.d_rhops,
+                              (const double2*)ctx.d_sfac, ctx.d_rhops_sp, ctx.d_g2i_v,
+                              ctx.d_gx_v, ngv, nsp, om_inv, 1.5 * 1.5},
+            (size_t)ngv, t);
+  for (int k = 0; k < 6; k++) P[18 + k] = eye[k] * ctx.ehart * om_inv - 8.0 * M_PI * t[k];
+  // exchange-correlation
+  if (ctx.xc == "LDA") {
+    double d;
+    reduce<1>(ctx, LdaStressF{ctx.d_exc, ctx.d_rhor, ctx.d_vxc}, N, &d);
+    for (int k = 0; k < 6; k++) P[24 + k] = -eye[k] * d / (double)N;
+  } else {
+    reduce<6>(ctx, GgaStressF{ctx.d_grad, ctx.d_vx2, N}, N, t);
+    const double dsum = ctx.exc * (double)N / om - ctx.xc_rhov1;   // sum rho (e - v1)
+    for (int k = 0; k < 6; k++) P[24 + k] = -(eye[k] * dsum + t[k]) / (double)N;
+  }
+  // nonlocal
+  double tn[6] = {0, 0, 0, 0, 0, 0};
+  if (np) {
+    const int K = 2 * ngw;
+    if (!ctx.d_astress) ctx.d_astress = dalloc<double>((size_t)K * np);
+    const bool mx = ctx.precision == MIXED && ctx.gemm_backend == 1 &&
+                    tc_gemm_supported(ctx, true, false, np, nst, K);
+    if (mx && !ctx.sa_hi) {
+      QBX_CUDA(cudaMalloc(&ctx.sa_hi, (size_t)ctx.ldp * np * 2));
+      QBX_CUDA(cudaMalloc(&ctx.sa_lo, (size_t)ctx.ldp * np * 2));
+    }
+    const double two = 2.0, zero = 0.0;
+    for (int k = 0; k < 6; k++) {
+      dim3 grid((ngw + kThreads - 1) / kThreads, np);
+      k_danl<<<grid, kThreads, 0, ctx.stream>>>(ctx.d_gx_w, ctx.d_g2_w, ngw, ctx.d_vnl,
+                                                ctx.d_dvnl, ctx.d_pcol, ctx.d_tau_all, vi[k],
+                                                vj[k], (double2*)ctx.d_astress);
+      QBX_LAUNCHED(ctx);
+      // dF = 2 A_ij^T C; the G=0 row of A_ij is zero, so no correction
+      if (mx) {
+        split_bf16_2d(ctx, ctx.d_astress, K, np, K, ctx.sa_hi, ctx.sa_lo, ctx.ldp);
+        split_gemm(ctx, true, false, np, nst, K, 2.0, ctx.sa_hi, ctx.sa_lo, ctx.ldp,
+                   ctx.cs_hi[0], ctx.cs_lo[0], ctx.ldp, 0.0, ctx.d_dfnl);
+      } else {
+        QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_T, CUBLAS_OP_N, np, nst, K, &two,
+                             ctx.d_astress, K, ctx.d_c, K, &zero, ctx.d_dfnl, np));
+      }
+      reduce<1>(ctx, EnlStressF{ctx.d_fnl, ctx.d_dfnl, ctx.d_occ, np}, (size_t)np * nst, &tn[k]);
+    }
+  }
+  for (int k = 0; k < 6; k++) P[12 + k] = (eye[k] * ctx.enl + tn[k]) * om_inv;
+  for (int k = 0; k < 6; k++) P[30 + k] = ctx.sigma_esr[k];
+  for (int k = 0; k < 6; k++) {
+    double s = 0.0;
+    for (int q = 0; q < 6; q++) s += P[6 * q + k];
+    ctx.sigma[k] = s;
+  }
+  ctx.have_stress = true;
 }
 
 }  // namespace qbx

@@ -134,7 +134,7 @@ void species_from_radial(SpeciesTables& s, int zval, double mesh_spacing,
 double esr_energy_forces(const double cell[9],
                          const std::vector<std::vector<double>>& tau,
                          const std::vector<double>& zv, double rcps,
-                         std::vector<std::vector<double>>& f);
+                         std::vector<std::vector<double>>& f, double* sigma = nullptr);
 
 // ---------------------------------------------------------------- context
 enum Precision { FP64 = 0, MIXED = 1 };
@@ -261,6 +261,21 @@ struct Context {
   double ekin = 0, eps = 0, enl = 0, ehart = 0, exc = 0, ecoul = 0,
          etotal = 0, total_charge = 0, eigsum = 0, theta = 0;
   std::vector<double> fion;     // 3*natoms, species-major like the reference
+
+  // stress (EnergyFunctional::energy with compute_stress)
+  double sigma_esr[6] = {0, 0, 0, 0, 0, 0};
+  double sigma[6] = {0, 0, 0, 0, 0, 0};
+  double sigma_parts[36] = {0};  // ekin, eps, enl, ehart, exc, esr (6 each)
+  bool have_stress = false;
+  double xc_rhov1 = 0;          // sum_r rho v1 of the last PBE update (stress)
+  double* d_dvps = nullptr;     // ngv*nsp: dV_loc/dG / Omega per species
+  double* d_vnl = nullptr;      // nrad*ngw: radial projector V_nl(|G|)
+  double* d_dvnl = nullptr;     // nrad*ngw: dV_nl/dG
+  int* d_pcol = nullptr;        // 4*nproj: (l, m, radial row, atom) per column
+  double* d_tau_all = nullptr;  // 3*natoms
+  double* d_astress = nullptr;  // 2*ngw*nproj: a strain-derivative projector block
+  void* sa_hi = nullptr;        // its BF16 split (mixed path)
+  void* sa_lo = nullptr;
 
   // mixed precision: BF16 hi/lo splits of the GEMM operands
   int gemm_backend = 1;         // 0: cuBLAS BF16 products, 1: own tcgen05 kernel
@@ -389,6 +404,8 @@ void launch_rank1_fix(Context& ctx, double* m, int ldm, const double* x, int ldx
 double launch_enl(Context& ctx);                // enl; fnl <- DF/omega
 void launch_local_forces(Context& ctx, double* fion);
 void launch_nl_forces(Context& ctx, double* fion);
+// stress tensor of the state of the last energy(): ctx.sigma, ctx.sigma_parts
+void compute_stress(Context& ctx);
 void launch_identity_axpy(Context& ctx, double* t, const double* q, int n,
                           double alpha);       // t = I + alpha*q
 void launch_symmetrize_lower(Context& ctx, double* q, int n);

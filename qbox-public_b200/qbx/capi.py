@@ -36,6 +36,7 @@ SYMBOLS = (
     "qbx_host_basis", "qbx_host_species_eval", "qbx_host_esr",
     "qbx_profile", "qbx_profile_get", "qbx_launch_count", "qbx_stream",
     "qbx_set_gemm_backend", "qbx_split_gemm_tn", "qbx_density_static",
+    "qbx_stress", "qbx_get_stress",
 )
 
 _lib = None
@@ -99,6 +100,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "qbx_set_gemm_backend": (_I, [_P, _I]),
         "qbx_split_gemm_tn": (_I, [_P, _I, _I, _I, _DP, _DP, _DP, _I]),
         "qbx_density_static": (_I, [_P, ctypes.c_void_p, _I, _DP, ctypes.c_void_p]),
+        "qbx_stress": (_I, [_P, _DP, _DP]),
+        "qbx_get_stress": (_I, [_P, _DP, _DP]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -255,13 +258,16 @@ class Context:
     def psda_reset(self):
         self._ok(self.lib.qbx_psda_reset(self.h), "psda_reset")
 
-    def scf_step(self, forces=False):
+    def scf_step(self, forces=False, stress=False):
         e = np.zeros(NENERGY)
         f = np.zeros(3 * max(1, self.natoms)) if forces else None
-        self._ok(self.lib.qbx_scf_step(self.h, int(forces), _dp(e), _dp(f)), "scf_step")
+        flags = (1 if forces else 0) | (2 if stress else 0)
+        self._ok(self.lib.qbx_scf_step(self.h, flags, _dp(e), _dp(f)), "scf_step")
         out = dict(zip(ENERGY_NAMES, e))
         if forces:
             out["fion"] = f[:3 * self.natoms].reshape(-1, 3)
+        if stress:
+            out["sigma"], out["sigma_parts"] = self.last_stress()
         return out
 
     def ft_backward_pair(self, n1: int, n2: int) -> np.ndarray:
@@ -304,6 +310,23 @@ class Context:
         self._ok(self.lib.qbx_split_gemm_tn(self.h, m, n, k, _dp(at), _dp(bt), _dp(out),
                                             backend), "split_gemm_tn")
         return out.T
+
+    STRESS_PARTS = ("ekin", "eps", "enl", "ehart", "exc", "esr")
+
+    def _stress_out(self, fn, what):
+        sig = np.zeros(6)
+        parts = np.zeros(36)
+        self._ok(fn(self.h, _dp(sig), _dp(parts)), what)
+        return sig, dict(zip(self.STRESS_PARTS, parts.reshape(6, 6)))
+
+    def stress(self):
+        """qbx_stress: sigma (xx yy zz xy yz xz) of the last energy() and its
+        parts {ekin, eps, enl, ehart, exc, esr}."""
+        return self._stress_out(self.lib.qbx_stress, "stress")
+
+    def last_stress(self):
+        """qbx_get_stress: the stress of the last scf_step(stress=True)."""
+        return self._stress_out(self.lib.qbx_get_stress, "get_stress")
 
     def density_static(self, c_dev_ptr: int, nst: int, rho_dev_ptr: int,
                        occ: Optional[np.ndarray] = None):

@@ -187,3 +187,28 @@ def test_errors_are_reported():
     with pytest.raises(capi.QbxError, match="positive definite"):
         capi.from_system(s, coeffs=c)
     ctx.close()
+
+
+@pytest.mark.parametrize("name", ["si8", "si64", "h2o32"])
+def test_stress_matches_reference(name):
+    """Stress tensor of the first step (EnergyFunctional::energy with
+    compute_stress) against the reference's own sigma: 1e-9 Ha/bohr^3 in
+    FP64; the mixed path within 1e-6 relative of the largest component."""
+    g = golden(name)
+    s = systems.get(name)
+    ctx = capi.from_system(s, precision=capi.FP64)
+    r = ctx.scf_step(forces=True, stress=True)
+    np.testing.assert_allclose(r["sigma"], g["sigma_first"], rtol=0, atol=1e-9)
+    es = qbox_np.ElectronicStep(s)
+    es.update_density()
+    es.update_vhxc()
+    es.energy(False)
+    es.stress()
+    for k, v in r["sigma_parts"].items():
+        np.testing.assert_allclose(v, es.sigma_parts[k], rtol=0, atol=1e-9, err_msg=k)
+    ctx.close()
+    m = capi.from_system(s, precision=capi.MIXED)
+    rm = m.scf_step(stress=True)
+    scale = np.abs(g["sigma_first"]).max()
+    np.testing.assert_allclose(rm["sigma"], g["sigma_first"], rtol=0, atol=1e-6 * scale)
+    m.close()
