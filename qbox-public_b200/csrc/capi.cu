@@ -273,6 +273,8 @@ int qbx_set_cell(qbx_context* h, const double cell[9], double ecut, int nst, con
       if (const char* e = std::getenv("QBX_FAST_RODS")) c.fast_rods = std::max(1, std::min(32, std::atoi(e)));
       if (const char* e = std::getenv("QBX_FAST_CHUNKS")) c.fast_chunks = std::max(1, std::atoi(e));
       if (const char* e = std::getenv("QBX_FAST_BATCH")) c.fast_batch = std::max(0, std::atoi(e));
+      if (const char* e = std::getenv("QBX_FAST_LANE_SHAPE"))
+        c.fast_lane_shape = std::max(-1, std::min(2, std::atoi(e)));
       if (const char* e = std::getenv("QBX_FAST_VPSI_SHAPE"))
         c.fast_vpsi_shape = std::max(0, std::min(2, std::atoi(e)));
     }

@@ -615,6 +615,7 @@ static bool staged_fast(Context& ctx, int op, const double* c, const double* v, 
   a.rods_per_cta = ctx.fast_rods;
   a.xy_warps = ctx.fast_warps;
   a.vpsi_shape = ctx.fast_vpsi_shape;
+  a.lane_shape = ctx.fast_lane_shape;
   a.density_chunks = ctx.fast_chunks;
   a.v = v;
   if (op == OP_VPSI && ctx.precision == MIXED) {

@@ -32,6 +32,7 @@
 #include <algorithm>
 #include <type_traits>
 
+#include "fft_lane.cuh"
 #include "fft_reg.cuh"
 #include "qbx_internal.h"
 
@@ -318,6 +319,165 @@ kxy(typename reg::CT<T>::c* __restrict__ zbuf, int npairs, int pairs_per_cta, De
   }
 }
 
+// ------------------------------------------------------------ xy plane,
+// register lanes (FP32)
+// The plane pass of kxy with every line transform held in registers by a
+// group of lane::lanes_for(N) lanes (fft_lane.cuh): no line buffers, no
+// per-stage shared-memory round trips.  Loops over lines run in rounds of
+// blockDim/T groups that are uniform across the CTA, so that every lane
+// takes part in the shuffles; groups past the end carry zeros.
+// shared memory: [twx N0][twy N1][P ncol x pitch(N1)][FP32 density plane
+// N1 x N0, density only][xmap N0 ints]
+template <int N0, int N1, int OP>
+__host__ size_t xyl_smem_bytes(int ncol) {
+  size_t b = sizeof(float2) * ((size_t)N0 + N1 + (size_t)ncol * pitch(N1));
+  if (OP == XY_DENSITY) b += sizeof(float) * (size_t)N0 * N1;
+  return b + sizeof(int) * N0;
+}
+
+// CTA shapes of kxy_lane: 0 = 256 threads compiled for two CTAs per SM
+// (128 registers), 1 = 256 threads, one per SM, 2 = 512 threads, one per SM
+__host__ __device__ constexpr int lane_threads(int shape) { return shape == 2 ? 512 : 256; }
+__host__ __device__ constexpr int lane_minblocks(int shape) { return shape == 0 ? 2 : 1; }
+
+template <int N0, int N1, int OP, int SHAPE>
+__global__ void __launch_bounds__(lane_threads(SHAPE), lane_minblocks(SHAPE))
+kxy_lane(float2* __restrict__ zbuf, int npairs, int pairs_per_cta, DeviceSticks g,
+         const double2* __restrict__ twx_g, const double2* __restrict__ twy_g,
+         const float* __restrict__ v, double* __restrict__ rho, const double* __restrict__ w,
+         int pair0, int nst) {
+  using C = float2;
+  constexpr int LD = pitch(N1);
+  constexpr int TY = lane::lanes_for(N1), MY = N1 / TY;
+  constexpr int TX = lane::lanes_for(N0), MX = N0 / TX;
+  static_assert(TY > 0 && TX > 0, "no register plan for this length");
+  constexpr bool DENS = (OP == XY_DENSITY);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int ncol = g.ncol, nvec = g.nvec;
+  C* twx = reinterpret_cast<C*>(smem_raw);
+  C* twy = twx + N0;
+  C* P = twy + N1;
+  float* acc = reinterpret_cast<float*>(P + (size_t)ncol * LD);
+  int* xmap = reinterpret_cast<int*>(acc + (DENS ? (size_t)N0 * N1 : 0));
+  const int z = blockIdx.x;
+  load_tw(twx, twx_g, N0);
+  load_tw(twy, twy_g, N1);
+  for (int x = threadIdx.x; x < N0; x += blockDim.x) xmap[x] = -1;
+  if constexpr (DENS)
+    for (int t = threadIdx.x; t < N0 * N1; t += blockDim.x) acc[t] = 0.f;
+  __syncthreads();
+  for (int cidx = threadIdx.x; cidx < ncol; cidx += blockDim.x) xmap[g.col_x[cidx]] = cidx;
+  const int ty = threadIdx.x % TY, gy = threadIdx.x / TY, sy = blockDim.x / TY;
+  const int tx = threadIdx.x % TX, gx = threadIdx.x / TX, sx = blockDim.x / TX;
+  const int mry = lane::bitrev(ty, TY), mrx = lane::bitrev(tx, TX);
+  const int pbeg = blockIdx.y * pairs_per_cta;
+  const int pend = min(npairs, pbeg + pairs_per_cta);
+#pragma unroll 1
+  for (int pl = pbeg; pl < pend; ++pl) {
+    C* zp = zbuf + ((size_t)pl * g.n2 + z) * nvec;
+    for (int t = threadIdx.x; t < ncol * LD; t += blockDim.x) P[t] = cmk<C>(0.0, 0.0);
+    __syncthreads();
+    for (int s = threadIdx.x; s < nvec; s += blockDim.x)
+      P[g.stick_col[s] * LD + g.stick_y[s]] = zp[s];
+    __syncthreads();
+    // backward y on the occupied columns, natural in, m-distributed out
+#pragma unroll 1
+    for (int base = 0; base < ncol; base += sy) {
+      const int cidx = base + gy;
+      const bool ok = cidx < ncol;
+      C* col = P + (ok ? cidx : 0) * LD;
+      C val[MY];
+#pragma unroll
+      for (int k = 0; k < MY; ++k) val[k] = ok ? col[ty + TY * k] : cmk<C>(0.0, 0.0);
+      lane::line_n2r<TY, MY, +1>(val, ty, twy);
+      if (ok) {
+#pragma unroll
+        for (int k2 = 0; k2 < MY; ++k2) col[k2 + MY * mry] = val[k2];
+      }
+    }
+    __syncthreads();
+    double w1 = 0.0, w2 = 0.0;
+    if (DENS) {
+      const int b1 = 2 * (pair0 + pl);
+      w1 = w[b1];
+      w2 = (b1 + 1 < nst) ? w[b1 + 1] : 0.0;
+    }
+    const float f1 = (float)w1, f2 = (float)w2;
+    // x rows
+#pragma unroll 1
+    for (int base = 0; base < N1; base += sx) {
+      const int y = base + gx;
+      const bool ok = y < N1;
+      // the column map lookups depend only on the lane: hidden from the
+      // optimiser so that they are not kept in MX registers across rows
+      int txh = tx;
+      asm volatile("" : "+r"(txh));
+      C val[MX];
+#pragma unroll
+      for (int k = 0; k < MX; ++k) {
+        const int cidx = xmap[txh + TX * k];
+        val[k] = (ok && cidx >= 0) ? P[cidx * LD + y] : cmk<C>(0.0, 0.0);
+      }
+      lane::line_n2r<TX, MX, +1>(val, tx, twx);
+      if constexpr (DENS) {
+        if (ok) {
+          float* arow = acc + y * N0 + MX * mrx;
+#pragma unroll
+          for (int k2 = 0; k2 < MX; ++k2)
+            arow[k2] += f1 * val[k2].x * val[k2].x + f2 * val[k2].y * val[k2].y;
+        }
+      } else {
+        const float* vrow = v + ((size_t)z * N1 + (ok ? y : 0)) * N0 + MX * mrx;
+        // keep the V loads after the transform: hoisted above it they would
+        // hold MX more registers through it
+        asm volatile("" ::: "memory");
+#pragma unroll
+        for (int k2 = 0; k2 < MX; ++k2) {
+          const float vv = ok ? vrow[k2] : 0.f;
+          val[k2].x *= vv;
+          val[k2].y *= vv;
+        }
+        lane::line_r2n<TX, MX, -1>(val, tx, twx);
+        if (ok) {
+          asm volatile("" : "+r"(txh));
+#pragma unroll
+          for (int k = 0; k < MX; ++k) {
+            const int cidx = xmap[txh + TX * k];
+            if (cidx >= 0) P[cidx * LD + y] = val[k];
+          }
+        }
+      }
+    }
+    __syncthreads();
+    if constexpr (!DENS) {
+      // forward y, m-distributed in, natural out
+#pragma unroll 1
+      for (int base = 0; base < ncol; base += sy) {
+        const int cidx = base + gy;
+        const bool ok = cidx < ncol;
+        C* col = P + (ok ? cidx : 0) * LD;
+        C val[MY];
+#pragma unroll
+        for (int k2 = 0; k2 < MY; ++k2) val[k2] = ok ? col[k2 + MY * mry] : cmk<C>(0.0, 0.0);
+        lane::line_r2n<TY, MY, -1>(val, ty, twy);
+        if (ok) {
+#pragma unroll
+          for (int k = 0; k < MY; ++k) col[ty + TY * k] = val[k];
+        }
+      }
+      __syncthreads();
+      for (int s = threadIdx.x; s < nvec; s += blockDim.x)
+        zp[s] = P[g.stick_col[s] * LD + g.stick_y[s]];
+      __syncthreads();
+    }
+  }
+  if constexpr (DENS) {
+    __syncthreads();
+    const size_t pbase = (size_t)z * N1 * N0;
+    for (int t = threadIdx.x; t < N0 * N1; t += blockDim.x) atomicAdd(&rho[pbase + t], (double)acc[t]);
+  }
+}
+
 // ------------------------------------------------------------ launch
 // Arguments of one batch of band pairs through the specialised kernels.
 struct StagedArgs {
@@ -333,6 +493,7 @@ struct StagedArgs {
   int rods_per_cta;        // z kernels
   int xy_warps;            // requested warps per kxy CTA
   int vpsi_shape;          // FP32 H*psi plane CTA shape (xy_threads / xy_minblocks)
+  int lane_shape;          // FP32 register-lane plane kernel shape, -1 = not used
   int density_chunks;      // CTAs per plane in the density pass
 };
 
@@ -346,6 +507,18 @@ void launch_vpsi_xy(Context& ctx, const StagedArgs& a) {
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   kxy<T, N, N, XY_VPSI, SH><<<dim3(N, a.npairs), 32 * nw, sm, ctx.stream>>>(
       (C*)a.zbuf, a.npairs, 1, g, a.twx, a.twy, (const T*)a.v, nullptr, nullptr, a.pair0, a.nst);
+  QBX_LAUNCHED(ctx);
+}
+
+template <int N, int OP, int SH>
+void launch_lane_xy(Context& ctx, const StagedArgs& a, int chunks, int ppc) {
+  const DeviceSticks& g = ctx.dws;
+  const size_t sm = xyl_smem_bytes<N, N, OP>(g.ncol);
+  QBX_CUDA(cudaFuncSetAttribute(kxy_lane<N, N, OP, SH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sm));
+  kxy_lane<N, N, OP, SH><<<dim3(N, chunks), lane_threads(SH), sm, ctx.stream>>>(
+      (float2*)a.zbuf, a.npairs, ppc, g, a.twx, a.twy, (const float*)a.v, a.rho, a.w, a.pair0,
+      a.nst);
   QBX_LAUNCHED(ctx);
 }
 
@@ -364,6 +537,34 @@ void run_cubic(Context& ctx, const StagedArgs& a) {
     kz_bwd<T, N><<<zgrid, kZThreads, zs, st>>>((const double2*)a.c, ngw, a.nst, a.pair0, g, a.twz,
                                                (C*)a.zbuf, rpc);
     QBX_LAUNCHED(ctx);
+  }
+  constexpr bool LANE = std::is_same<T, float>::value && lane::lanes_for(N) > 0;
+  if constexpr (LANE) {
+    if (a.lane_shape >= 0) {
+      if (a.op == XY_DENSITY) {
+        int chunks = std::max(1, std::min(a.npairs, a.density_chunks));
+        const int ppc = (a.npairs + chunks - 1) / chunks;
+        chunks = (a.npairs + ppc - 1) / ppc;
+        ProfScope ps(ctx, "xy_density");
+        launch_lane_xy<N, XY_DENSITY, 2>(ctx, a, chunks, ppc);
+        return;
+      }
+      {
+        ProfScope ps(ctx, "xy_vpsi");
+        if (a.lane_shape == 0) launch_lane_xy<N, XY_VPSI, 0>(ctx, a, a.npairs, 1);
+        else if (a.lane_shape == 1) launch_lane_xy<N, XY_VPSI, 1>(ctx, a, a.npairs, 1);
+        else launch_lane_xy<N, XY_VPSI, 2>(ctx, a, a.npairs, 1);
+      }
+      QBX_CUDA(cudaFuncSetAttribute(kz_fwd<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)zs));
+      const double scale = 1.0 / ((double)N * N * N);
+      ProfScope ps(ctx, "zfft_fwd");
+      kz_fwd<T, N><<<zgrid, kZThreads, zs, st>>>((const C*)a.zbuf, ngw, a.nst, a.pair0, g, a.twz,
+                                                 scale, (const double2*)a.c, ctx.d_g2_w,
+                                                 (double2*)a.hc, rpc);
+      QBX_LAUNCHED(ctx);
+      return;
+    }
   }
   if (a.op == XY_DENSITY) {
     constexpr int SH = XYDefault<T, XY_DENSITY>::shape;
@@ -405,7 +606,12 @@ size_t smem_need(const Context& ctx, const StagedArgs& a) {
   const size_t x = std::max(xy_smem_bytes<T, N, N, XY_DENSITY>(ctx.dws.ncol, nwd),
                             xy_smem_bytes<T, N, N, XY_VPSI>(ctx.dws.ncol, nwv));
   const size_t z = sizeof(typename reg::CT<T>::c) * ((size_t)N + (size_t)2 * a.rods_per_cta * pitch(N));
-  return std::max(x, z);
+  size_t l = 0;
+  if constexpr (std::is_same<T, float>::value && lane::lanes_for(N) > 0)
+    if (a.lane_shape >= 0)
+      l = std::max(xyl_smem_bytes<N, N, XY_DENSITY>(ctx.dws.ncol),
+                   xyl_smem_bytes<N, N, XY_VPSI>(ctx.dws.ncol));
+  return std::max(std::max(x, z), l);
 }
 
 }  // namespace fast

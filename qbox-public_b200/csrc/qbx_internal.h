@@ -299,6 +299,7 @@ struct Context {
   int fast_rods = 16;           // rods per CTA of the z kernels
   int fast_warps = 16;          // warps per CTA of the plane kernel (at most)
   int fast_vpsi_shape = 0;      // FP32 H*psi plane CTA shape (0, 1, 2)
+  int fast_lane_shape = 0;      // FP32 register-lane plane kernel shape, -1 = off
   int fast_chunks = 8;          // CTAs per plane in the density pass
   bool fast_fft = true;         // use the specialised kernels when compiled
   float* a32 = nullptr;         // TF32 hi/lo split of the projectors
