@@ -818,12 +818,8 @@ class ElectronicStep:
         d -= (self.c[:, self.g0].real * self.hc[:, self.g0].real).sum()
         return d
 
-    # ---- PSDA (src/PSDAWavefunctionStepper.cpp:46-249, Preconditioner)
-    def psda_update(self):
-        hc = self.hc
-        a = self.real_dot(self.c, hc)              # A = C^T HC (x2, fix)
-        hc = hc - a.T @ self.c                     # HC - C A
-        # preconditioner (src/Preconditioner.cpp:88-143, diag :49-85)
+    # ---- preconditioner (src/Preconditioner.cpp:88-143, diag :49-85)
+    def kdiag(self):
         p2 = np.abs(self.c) ** 2
         snorm = p2.sum(1) - 0.5 * p2[:, self.g0]
         sek = (p2 * self.wb.g2[None, :]).sum(1)
@@ -832,7 +828,38 @@ class ElectronicStep:
         ekin = np.where(ekin == 0.0, 1.0, ekin)
         e = 0.5 * self.wb.g2[None, :]
         with np.errstate(divide="ignore"):
-            kdiag = np.where(e < ekin[:, None], 0.5 / ekin[:, None], 0.5 / e)
+            return np.where(e < ekin[:, None], 0.5 / ekin[:, None], 0.5 / e)
+
+    # ---- JD (src/JDWavefunctionStepper.cpp:47-376, real basis)
+    def jd_update(self):
+        """Rayleigh-Ritz on span(Y, Z): Y = C, Z = the preconditioned
+        residual made orthogonal to Y and orthonormal; a second H*psi on Z;
+        C <- the lowest nst eigenvectors of the 2 nst x 2 nst projected H."""
+        y, hy = self.c.copy(), self.hc.copy()
+        a = self.real_dot(y, hy)
+        r = hy - a.T @ y
+        z = -self.kdiag() * r
+        a = self.real_dot(y, z)
+        self.c = z - a.T @ y
+        self.gram()
+        z = self.c
+        self.energy(True)                      # H Z with the current potential
+        hz = self.hc
+        n = self.nst
+        h = np.zeros((2 * n, 2 * n))
+        h[:n, :n] = self.real_dot(y, hy)
+        h[n:, :n] = self.real_dot(z, hy)
+        h[n:, n:] = self.real_dot(z, hz)
+        h = np.tril(h) + np.tril(h, -1).T      # syevd('l') reads the lower part
+        w, q = np.linalg.eigh(h)
+        self.c = q[:n, :n].T @ y + q[n:, :n].T @ z
+
+    # ---- PSDA (src/PSDAWavefunctionStepper.cpp:46-249, Preconditioner)
+    def psda_update(self):
+        hc = self.hc
+        a = self.real_dot(self.c, hc)              # A = C^T HC (x2, fix)
+        hc = hc - a.T @ self.c                     # HC - C A
+        kdiag = self.kdiag()
         dc = -kdiag * hc
         x = self.c
         if self.extrapolate:
@@ -859,7 +886,7 @@ class ElectronicStep:
         self.ortho_align(self.c_last)
         self.extrapolate = True
 
-    def step(self, forces=False) -> Dict[str, float]:
+    def step(self, forces=False, wf_dyn="PSDA") -> Dict[str, float]:
         self.update_density()
         self.update_vhxc()
         self.energy(True, forces)
@@ -868,7 +895,10 @@ class ElectronicStep:
                    ehart=self.ehart, ecoul=self.ecoul, exc=self.exc,
                    esr=self.esr, eself=self.eself, etotal=self.etotal,
                    eigenvalue_sum=eig)
-        self.psda_update()
+        if wf_dyn == "JD":
+            self.jd_update()
+        else:
+            self.psda_update()
         return out
 
 

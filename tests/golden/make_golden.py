@@ -67,9 +67,29 @@ def make(name: str, nsteps: int, workdir: str) -> str:
     return path
 
 
+def make_jd(name: str, nsteps: int, workdir: str) -> str:
+    """The JD stepper (wf_dyn JD): the eigenvalue sum of each step and the
+    energy terms the reference holds after each update, i.e. of the
+    correction block Z (src/JDWavefunctionStepper.cpp:203-204)."""
+    s = systems.get(name)
+    out = inputs.run_reference(s, workdir, nsteps, wf_dyn="JD", threads=os.cpu_count())
+    e = out["energies"]
+    fx = dict(nsteps=nsteps)
+    for k in ("ekin", "eps", "enl", "ehart", "ecoul", "exc", "etotal", "eigenvalue_sum"):
+        fx["e_" + k] = e[k]
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), f"ref_{name}_jd.npz")
+    np.savez_compressed(path, **fx)
+    return path
+
+
+JD_CASES = {"si8": 6}
+
 if __name__ == "__main__":
     import tempfile
-    names = sys.argv[1:] or list(CASES)
+    names = sys.argv[1:] or list(CASES) + [n + "_jd" for n in JD_CASES]
     for n in names:
         with tempfile.TemporaryDirectory() as td:
-            print(make(n, CASES[n], td))
+            if n.endswith("_jd"):
+                print(make_jd(n[:-3], JD_CASES[n[:-3]], td))
+            else:
+                print(make(n, CASES[n], td))

@@ -62,3 +62,19 @@ def test_fast_fp64_matches_oracle_si64():
     np.testing.assert_allclose(hc, es.hc, rtol=0, atol=1e-11)
     assert abs(e["etotal"] - es.etotal) < 1e-8
     ctx.close()
+
+
+@pytest.mark.parametrize("precision", [capi.FP64, capi.MIXED])
+def test_autotune_keeps_results(precision):
+    """qbx_autotune times the staged-FFT configurations and keeps the
+    fastest; whatever it picks, the density and H*psi stay the same."""
+    s = systems.si64()
+    a = _ctx(s, precision, True)
+    ra, ha, ea = _run(a)
+    report = a.autotune()
+    assert "chosen:" in report
+    rb, hb, eb = _run(a)
+    tol = 1e-12 if precision == capi.FP64 else 2e-6
+    np.testing.assert_allclose(rb, ra, rtol=0, atol=tol * np.abs(ra).max())
+    np.testing.assert_allclose(hb, ha, rtol=0, atol=tol * np.abs(ha).max())
+    a.close()

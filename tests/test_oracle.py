@@ -154,3 +154,15 @@ def test_forces_are_the_position_derivative():
             e2.update_vhxc()
             e.append(e2.energy(False))
         assert abs(-(e[0] - e[1]) / (2 * h) - f[a, j]) < 1e-6, (a, j)
+
+
+def test_oracle_jd_matches_reference():
+    """JDWavefunctionStepper::update (src/JDWavefunctionStepper.cpp:47-376):
+    the eigenvalue sum of every step, and the energy of the correction block
+    Z that the reference's energy functional holds after each update."""
+    g = golden("si8_jd")
+    es = qbox_np.ElectronicStep(systems.si8())
+    for it in range(int(g["nsteps"])):
+        r = es.step(wf_dyn="JD")
+        assert abs(r["eigenvalue_sum"] - g["e_eigenvalue_sum"][it]) < 1e-9
+        assert abs(es.etotal - g["e_etotal"][it]) < 1e-9
