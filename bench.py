@@ -223,6 +223,8 @@ def run_ours(args):
 
     # ---- mixed precision (headline)
     mix = capi.from_system(s, device=dev, precision=capi.MIXED, coeffs=c0)
+    mix.scf_step()
+    tuning_mix = mix.autotune()
     for _ in range(args.warmup):
         mix.scf_step()
     clocks = ClockSampler(dev)
@@ -250,11 +252,15 @@ def run_ours(args):
         pass
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     achieved = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9
-    roofline = {"kernel": "kxy<float,140,140,VPSI> (plane pass of H*psi)", "bound": "hbm",
+    roofline = {"kernel": "kxy_lane<140,140,VPSI> (plane pass of H*psi, register-lane FFTs)",
+                "bound": "hbm",
                 "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                 "frac": achieved / hbm_peak,
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
-                "traffic": None,
+                # DRAM bytes per launch: the ncu capture of this kernel
+                # (profiles/kxy_lane_vpsi_si512.md: 336.9 MB for a 16-pair
+                # launch) scaled by the band pairs of this run's launches
+                "traffic": 336.9e6 / 16.0 * (npairs / max(1e-9, n_xy)),
                 "algorithmic_bytes_per_launch": per_launch_bytes,
                 "launch_ms": per_launch_ms}
     # GEMM share (FP64 cuBLAS in this build) against the dense FP64 rate
@@ -268,6 +274,8 @@ def run_ours(args):
 
     # ---- FP64 path on the same start
     f64 = capi.from_system(s, device=dev, precision=capi.FP64, coeffs=c0)
+    f64.scf_step()
+    f64.autotune()
     for _ in range(args.warmup):
         f64.scf_step()
     ms_f64, r_f64, _ = timed(f64, args.steps)
@@ -323,8 +331,10 @@ def run_ours(args):
             "roofline": roofline,
             "gemm": {"ms_per_step": gemm_ms, "flop_per_step": gemm_flop,
                      "tflops": gemm_flop / (gemm_ms * 1e-3) / 1e12 if gemm_ms else None,
-                     "precision": "fp64 (cuBLAS)"},
+                     "precision": "mixed: split BF16 (inner products) and TF32 (tall updates) "
+                                  "on tcgen05, FP64 Cholesky/polar (cuSOLVER/cuBLAS)"},
             "profile": prof,
+            "fft_tuning": tuning_mix.strip().splitlines()[-1],
             "cpu_baseline": cpu,
             "e2e": {"value": ms_e2e, "unit": "ms", "h2d_bytes_per_step": nb,
                     "d2h_bytes_per_step": nb},
@@ -338,15 +348,27 @@ def run_ours(args):
 
 
 def run_profile_case(args):
-    """A small case for ncu captures: warm-up plus one mixed electronic step
-    of the 512-atom cell with a band sample (the per-launch work of the plane
-    kernels is that of the full run; the device holds a few GB)."""
+    """A case for ncu: the 512-atom cell with a band sample (all 1024 bands
+    for the launch list of the headline step; 64 for full captures, whose
+    plane kernels do the same work per launch while the device holds a few
+    GB), mixed precision.  Warm-up steps run before cudaProfilerStart, so
+    `ncu --profile-from-start off` sees exactly one electronic step."""
+    import torch
     from qbx import capi, systems
-    s = systems.si512().band_sample(args.profile_bands)
+    s = systems.si512()
+    if args.profile_bands < s.nbands:
+        s = s.band_sample(args.profile_bands)
     ctx = capi.from_system(s, precision=capi.MIXED)
-    for _ in range(args.warmup + 1):
+    ctx.scf_step()
+    if args.profile_tune:
+        ctx.autotune()
+    for _ in range(args.warmup):
         ctx.scf_step()
     ctx.synchronize()
+    torch.cuda.profiler.start()
+    ctx.scf_step()
+    ctx.synchronize()
+    torch.cuda.profiler.stop()
     ctx.close()
 
 
@@ -358,7 +380,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--profile-bands", type=int, default=0,
                     help="run only warm-up + one mixed step of si512 with this many bands "
-                         "(a small case for profilers); prints nothing")
+                         "(a case for profilers); prints nothing")
+    ap.add_argument("--profile-tune", action="store_true",
+                    help="with --profile-bands: autotune the FFT configuration first")
     args = ap.parse_args()
     if args.profile_bands:
         run_profile_case(args)

@@ -110,6 +110,15 @@ int qbx_eigenvalue_sum(qbx_context* ctx, double* eigsum);
 int qbx_psda_update(qbx_context* ctx);
 int qbx_psda_reset(qbx_context* ctx);
 
+/* WavefunctionStepper choice (the reference's `set wf_dyn`, src/WfDyn.h):
+ * "PSDA" (default) or "JD"; qbx_scf_step then ends with that update. */
+int qbx_set_wf_dyn(qbx_context* ctx, const char* wf_dyn);
+/* JDWavefunctionStepper::update (src/JDWavefunctionStepper.cpp:47-376):
+ * after qbx_energy (which leaves H*C), Rayleigh-Ritz on span(C, Z) with the
+ * preconditioned residual Z; includes a second H*psi (on Z), whose energy
+ * terms the context then holds, as the reference's energy functional does. */
+int qbx_jd_update(qbx_context* ctx);
+
 /* One electronic step of the SCF loop with nite = 0
  * (src/BOSampleStepper.cpp:795-977): update_density, update_vhxc,
  * energy(true,...), eigenvalue_sum, PSDA update.  compute_forces: bit 0
@@ -184,6 +193,14 @@ int qbx_split_gemm_tn(qbx_context* ctx, int m, int n, int k, const double* a,
  * finished. */
 int qbx_density_static(qbx_context* ctx, const double* d_c, int nst,
                        const double* occ, double* d_rho);
+
+/* No counterpart in the reference (its FFT plans are fixed at build time).
+ * Chooses the staged-FFT launch configuration for this context's grid,
+ * basis and precision by timing the candidate plane kernels, CTA shapes,
+ * band-pair batches and z-stick blocking on the context's own data (after
+ * qbx_set_atoms and qbx_set_coeffs).  A summary of the timings and the
+ * choice is written to report (report_len bytes, may be NULL). */
+int qbx_autotune(qbx_context* ctx, char* report, int report_len);
 
 /* Host-only setup helpers (no GPU needed), exposing the same host code the
  * context uses.  Basis::resize + ChargeDensity grid: basis sizes, grid and

@@ -27,6 +27,7 @@ void update_density(Context& ctx);
 void update_vhxc(Context& ctx);
 void energy(Context& ctx, bool hpsi, bool forces);
 void psda_update(Context& ctx);
+void jd_update(Context& ctx);
 }
 
 using namespace qbx;
@@ -61,7 +62,8 @@ void free_cell(Context& c) {
                      &c.d_dc_last, &c.d_ctmp, &c.d_occ, &c.d_rhor, &c.d_vr, &c.d_vxc,
                      &c.d_exc, &c.d_vx2, &c.d_grad, &c.d_rhog, &c.d_vion, &c.d_rhops,
                      &c.d_vtmp_g, &c.d_vtmp_g2, &c.d_nn, &c.d_nn2, &c.d_nn3, &c.d_nn4,
-                     &c.d_solver_work, &c.d_red, &c.d_scalars, &c.d_prec};
+                     &c.d_solver_work, &c.d_red, &c.d_scalars, &c.d_prec, &c.d_jd_h,
+                     &c.d_jd_w, &c.d_jd_work};
   for (double** b : bufs) dfree(*b);
   dfree(c.d_ipiv);
   dfree(c.d_info);
@@ -261,7 +263,7 @@ int qbx_set_cell(qbx_context* h, const double cell[9], double ecut, int nst, con
     // the specialised FFTs work through a smaller stick buffer that can stay
     // in L2 between the z and plane kernels (64 MB unless overridden)
     {
-      size_t mb = 64;
+      size_t mb = 256;
       if (const char* e = std::getenv("QBX_FAST_ZBUF_MB")) mb = std::max(1, std::atoi(e));
       const size_t pp64 = (size_t)c.wb.n2 * c.wb.nvec * sizeof(double2);
       c.zfast_bytes = std::max(mb << 20, pp64);
@@ -272,9 +274,12 @@ int qbx_set_cell(qbx_context* h, const double cell[9], double ecut, int nst, con
       if (const char* e = std::getenv("QBX_FAST_WARPS")) c.fast_warps = std::max(1, std::min(16, std::atoi(e)));
       if (const char* e = std::getenv("QBX_FAST_RODS")) c.fast_rods = std::max(1, std::min(32, std::atoi(e)));
       if (const char* e = std::getenv("QBX_FAST_CHUNKS")) c.fast_chunks = std::max(1, std::atoi(e));
+      c.fast_batch = 16;
       if (const char* e = std::getenv("QBX_FAST_BATCH")) c.fast_batch = std::max(0, std::atoi(e));
       if (const char* e = std::getenv("QBX_FAST_LANE_SHAPE"))
-        c.fast_lane_shape = std::max(-1, std::min(2, std::atoi(e)));
+        c.fast_lane_shape = std::max(-1, std::min(4, std::atoi(e)));
+      if (const char* e = std::getenv("QBX_FAST_DENSITY_LANE_SHAPE"))
+        c.fast_density_lane_shape = std::atoi(e) == 3 ? 3 : 2;
       if (const char* e = std::getenv("QBX_FAST_VPSI_SHAPE"))
         c.fast_vpsi_shape = std::max(0, std::min(2, std::atoi(e)));
     }
@@ -552,9 +557,44 @@ int qbx_scf_step(qbx_context* h, int forces, double* energies, double* fion) {
     c.eigsum = launch_eigsum(c);
     fill_energies(c, energies);
     if (want_f && fion) std::memcpy(fion, c.fion.data(), sizeof(double) * c.fion.size());
-    psda_update(c);
+    if (c.wf_dyn == 1) jd_update(c);
+    else psda_update(c);
     QBX_CUDA(cudaStreamSynchronize(c.stream));
     QBX_REQUIRE(tc_check_error(c) == 0, 55, "tcgen05 GEMM pipeline wait timed out");
+  });
+}
+
+int qbx_set_wf_dyn(qbx_context* h, const char* name) {
+  return guarded(h, [&](Context& c) {
+    const std::string s = name ? name : "";
+    QBX_REQUIRE(s == "PSDA" || s == "JD", 1, "wf_dyn must be PSDA or JD");
+    c.wf_dyn = (s == "JD") ? 1 : 0;
+    c.extrapolate = false;
+  });
+}
+
+int qbx_jd_update(qbx_context* h) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, true);
+    jd_update(c);
+  });
+}
+
+int qbx_autotune(qbx_context* h, char* report, int report_len) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, true);
+    std::vector<std::pair<std::string, double>> log;
+    autotune_fft(c, &log);
+    if (report && report_len > 0) {
+      std::string r;
+      for (auto& e : log) r += e.first + ": " + std::to_string(e.second) + " ms\n";
+      r += "chosen: lane " + std::to_string(c.fast_lane_shape) + ", warp " +
+           std::to_string(c.fast_vpsi_shape) + ", density lane " +
+           std::to_string(c.fast_density_lane_shape) + ", pairs " +
+           std::to_string(c.fast_batch) + ", rods " + std::to_string(c.fast_rods) + "\n";
+      std::strncpy(report, r.c_str(), (size_t)report_len - 1);
+      report[report_len - 1] = 0;
+    }
   });
 }
 

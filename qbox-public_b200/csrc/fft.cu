@@ -616,6 +616,7 @@ static bool staged_fast(Context& ctx, int op, const double* c, const double* v, 
   a.xy_warps = ctx.fast_warps;
   a.vpsi_shape = ctx.fast_vpsi_shape;
   a.lane_shape = ctx.fast_lane_shape;
+  a.density_lane_shape = ctx.fast_density_lane_shape;
   a.density_chunks = ctx.fast_chunks;
   a.v = v;
   if (op == OP_VPSI && ctx.precision == MIXED) {
@@ -781,6 +782,114 @@ void density_with_buffers(Context& ctx, const double* c, int nst, const double* 
     density_buffers_t<float>(ctx, c, nst, w, rho, zbuf, zbuf_bytes, twx, twy, twz);
   else
     density_buffers_t<double>(ctx, c, nst, w, rho, zbuf, zbuf_bytes, twx, twy, twz);
+}
+
+}  // namespace qbx
+
+namespace qbx {
+
+// ------------------------------------------------------------ autotuner
+// Picks the staged-FFT launch configuration (plane-kernel family and CTA
+// shape for H*psi and for the density, band pairs per launch, rods per z
+// CTA) for this context's grid, basis and precision by timing the
+// candidates on the context's own wavefunctions and potential, one
+// parameter at a time in that order.  Results go to ctx.fast_*; the chosen
+// values and timings are appended to `log`.
+void autotune_fft(Context& ctx, std::vector<std::pair<std::string, double>>* log) {
+  QBX_REQUIRE(ctx.have_cell && ctx.d_zfast, 7, "autotune needs a cell");
+  const size_t N = ctx.N();
+  double* rho_tmp = dalloc<double>(N);
+  double* hc_tmp = ctx.d_ctmp;
+  cudaEvent_t e0, e1;
+  QBX_CUDA(cudaEventCreate(&e0));
+  QBX_CUDA(cudaEventCreate(&e1));
+  auto time_ms = [&](auto fn) {
+    fn();   // warm-up (function attributes, caches)
+    QBX_CUDA(cudaEventRecord(e0, ctx.stream));
+    fn();
+    QBX_CUDA(cudaEventRecord(e1, ctx.stream));
+    QBX_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    QBX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    return (double)ms;
+  };
+  auto vpsi = [&]() { launch_vpsi(ctx, ctx.d_c, ctx.d_vr, hc_tmp); };
+  auto dens = [&]() { launch_density(ctx, ctx.d_c, rho_tmp); };
+  auto note = [&](const std::string& what, double ms) {
+    if (log) log->push_back({what, ms});
+  };
+  try {
+    // 1. H*psi plane kernel: register-lane shapes (FP32 lengths with a
+    // register plan), then the warp-per-line kernel
+    {
+      std::vector<std::pair<int, int>> cand;   // (lane shape, warp shape)
+      if (ctx.precision == MIXED) {
+        for (int s : {4, 0, 3}) cand.push_back({s, ctx.fast_vpsi_shape});
+        for (int s : {0, 1}) cand.push_back({-1, s});
+      } else {
+        cand.push_back({-1, ctx.fast_vpsi_shape});
+      }
+      double best = 1e30;
+      std::pair<int, int> pick = cand[0];
+      for (auto cv : cand) {
+        ctx.fast_lane_shape = cv.first;
+        ctx.fast_vpsi_shape = cv.second;
+        const double t = time_ms(vpsi);
+        note("vpsi lane " + std::to_string(cv.first) + " warp " + std::to_string(cv.second), t);
+        if (t < best) { best = t; pick = cv; }
+      }
+      ctx.fast_lane_shape = pick.first;
+      ctx.fast_vpsi_shape = pick.second;
+    }
+    // 2. density plane kernel shape
+    if (ctx.precision == MIXED && ctx.fast_lane_shape >= 0) {
+      double best = 1e30;
+      int pick = ctx.fast_density_lane_shape;
+      for (int s : {3, 2}) {
+        ctx.fast_density_lane_shape = s;
+        const double t = time_ms(dens);
+        note("density lane " + std::to_string(s), t);
+        if (t < best) { best = t; pick = s; }
+      }
+      ctx.fast_density_lane_shape = pick;
+    }
+    // 3. band pairs per launch (the stick buffer stays in L2 for small batches)
+    {
+      const size_t per_pair = (ctx.precision == MIXED ? sizeof(float2) : sizeof(double2)) *
+                              (size_t)ctx.dws.n2 * ctx.dws.nvec;
+      const int cap = (int)std::max<size_t>(1, ctx.zfast_bytes / per_pair);
+      double best = 1e30;
+      int pick = ctx.fast_batch;
+      for (int b : {16, 32, 64, 0}) {
+        if (b > cap) continue;
+        ctx.fast_batch = b;
+        const double t = time_ms(vpsi) + time_ms(dens);
+        note("pairs per launch " + std::to_string(b == 0 ? cap : b), t);
+        if (t < best) { best = t; pick = b; }
+      }
+      ctx.fast_batch = pick;
+    }
+    // 4. rods per CTA of the z kernels
+    {
+      double best = 1e30;
+      int pick = ctx.fast_rods;
+      for (int r : {8, 16, 24}) {
+        ctx.fast_rods = r;
+        const double t = time_ms(vpsi);
+        note("rods per z CTA " + std::to_string(r), t);
+        if (t < best) { best = t; pick = r; }
+      }
+      ctx.fast_rods = pick;
+    }
+  } catch (...) {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    dfree(rho_tmp);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  dfree(rho_tmp);
 }
 
 }  // namespace qbx

@@ -335,10 +335,15 @@ __host__ size_t xyl_smem_bytes(int ncol) {
   return b + sizeof(int) * N0;
 }
 
-// CTA shapes of kxy_lane: 0 = 256 threads compiled for two CTAs per SM
-// (128 registers), 1 = 256 threads, one per SM, 2 = 512 threads, one per SM
-__host__ __device__ constexpr int lane_threads(int shape) { return shape == 2 ? 512 : 256; }
-__host__ __device__ constexpr int lane_minblocks(int shape) { return shape == 0 ? 2 : 1; }
+// CTA shapes of kxy_lane (most threads, CTAs per SM compiled for):
+// 0 = 256 x 2 (128 registers), 1 = 256 x 1, 2 = 512 x 1, 3 = 320 x 1,
+// 4 = 288 x 2 (113 registers).  Shapes 3 and 4 are launched with just
+// enough lanes for one round over the occupied columns (ncol * T rounded up
+// to a warp), which for 65 columns is 9 warps.
+__host__ __device__ constexpr int lane_threads(int shape) {
+  return shape == 2 ? 512 : shape == 3 ? 320 : shape == 4 ? 288 : 256;
+}
+__host__ __device__ constexpr int lane_minblocks(int shape) { return (shape == 0 || shape == 4) ? 2 : 1; }
 
 template <int N0, int N1, int OP, int SHAPE>
 __global__ void __launch_bounds__(lane_threads(SHAPE), lane_minblocks(SHAPE))
@@ -494,6 +499,7 @@ struct StagedArgs {
   int xy_warps;            // requested warps per kxy CTA
   int vpsi_shape;          // FP32 H*psi plane CTA shape (xy_threads / xy_minblocks)
   int lane_shape;          // FP32 register-lane plane kernel shape, -1 = not used
+  int density_lane_shape;  // its density-pass shape (2 or 3)
   int density_chunks;      // CTAs per plane in the density pass
 };
 
@@ -516,7 +522,12 @@ void launch_lane_xy(Context& ctx, const StagedArgs& a, int chunks, int ppc) {
   const size_t sm = xyl_smem_bytes<N, N, OP>(g.ncol);
   QBX_CUDA(cudaFuncSetAttribute(kxy_lane<N, N, OP, SH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sm));
-  kxy_lane<N, N, OP, SH><<<dim3(N, chunks), lane_threads(SH), sm, ctx.stream>>>(
+  int threads = lane_threads(SH);
+  if (SH == 3 || SH == 4) {
+    const int want = (g.ncol * lane::lanes_for(N) + 31) / 32 * 32;
+    threads = std::max(64, std::min(threads, want));
+  }
+  kxy_lane<N, N, OP, SH><<<dim3(N, chunks), threads, sm, ctx.stream>>>(
       (float2*)a.zbuf, a.npairs, ppc, g, a.twx, a.twy, (const float*)a.v, a.rho, a.w, a.pair0,
       a.nst);
   QBX_LAUNCHED(ctx);
@@ -546,14 +557,19 @@ void run_cubic(Context& ctx, const StagedArgs& a) {
         const int ppc = (a.npairs + chunks - 1) / chunks;
         chunks = (a.npairs + ppc - 1) / ppc;
         ProfScope ps(ctx, "xy_density");
-        launch_lane_xy<N, XY_DENSITY, 2>(ctx, a, chunks, ppc);
+        if (a.density_lane_shape == 3) launch_lane_xy<N, XY_DENSITY, 3>(ctx, a, chunks, ppc);
+        else launch_lane_xy<N, XY_DENSITY, 2>(ctx, a, chunks, ppc);
         return;
       }
       {
         ProfScope ps(ctx, "xy_vpsi");
-        if (a.lane_shape == 0) launch_lane_xy<N, XY_VPSI, 0>(ctx, a, a.npairs, 1);
-        else if (a.lane_shape == 1) launch_lane_xy<N, XY_VPSI, 1>(ctx, a, a.npairs, 1);
-        else launch_lane_xy<N, XY_VPSI, 2>(ctx, a, a.npairs, 1);
+        switch (a.lane_shape) {
+          case 1: launch_lane_xy<N, XY_VPSI, 1>(ctx, a, a.npairs, 1); break;
+          case 2: launch_lane_xy<N, XY_VPSI, 2>(ctx, a, a.npairs, 1); break;
+          case 3: launch_lane_xy<N, XY_VPSI, 3>(ctx, a, a.npairs, 1); break;
+          case 4: launch_lane_xy<N, XY_VPSI, 4>(ctx, a, a.npairs, 1); break;
+          default: launch_lane_xy<N, XY_VPSI, 0>(ctx, a, a.npairs, 1); break;
+        }
       }
       QBX_CUDA(cudaFuncSetAttribute(kz_fwd<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)zs));

@@ -447,6 +447,15 @@ void launch_psda_elementwise(Context& ctx) {
   QBX_LAUNCHED(ctx);
 }
 
+// JD correction: Z = -K R, R the residual held in hc (Preconditioner::diag)
+void launch_precondition_into(Context& ctx, const double* r, double* z) {
+  const size_t n = (size_t)ctx.wb.ng * ctx.nst;
+  QBX_CUDA(cudaMemcpyAsync(z, r, 2 * n * sizeof(double), cudaMemcpyDeviceToDevice, ctx.stream));
+  k_precondition<<<blocks_for(n), kThreads, 0, ctx.stream>>>((double2*)z, ctx.d_g2_w, ctx.d_prec,
+                                                              ctx.wb.ng, n);
+  QBX_LAUNCHED(ctx);
+}
+
 __global__ void k_cleanup(double2* c, int ngw, int nst) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n < nst) c[(size_t)n * ngw].y = 0.0;

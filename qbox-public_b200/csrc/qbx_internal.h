@@ -209,6 +209,11 @@ struct Context {
   int nst = 0;
   std::vector<double> occ;
   bool extrapolate = false;
+  int wf_dyn = 0;               // 0: PSDA, 1: JD (the reference's wf_dyn)
+  double* d_jd_h = nullptr;     // 2nst x 2nst projected Hamiltonian
+  double* d_jd_w = nullptr;     // its eigenvalues
+  double* d_jd_work = nullptr;  // syevd workspace
+  int jd_lwork = 0;
 
   // device buffers (double unless noted)
   double* d_gx_w = nullptr;     // 3*ngw
@@ -299,7 +304,8 @@ struct Context {
   int fast_rods = 16;           // rods per CTA of the z kernels
   int fast_warps = 16;          // warps per CTA of the plane kernel (at most)
   int fast_vpsi_shape = 0;      // FP32 H*psi plane CTA shape (0, 1, 2)
-  int fast_lane_shape = 0;      // FP32 register-lane plane kernel shape, -1 = off
+  int fast_lane_shape = 4;      // FP32 register-lane plane kernel shape, -1 = off
+  int fast_density_lane_shape = 3;  // its density shape (2 or 3)
   int fast_chunks = 8;          // CTAs per plane in the density pass
   bool fast_fft = true;         // use the specialised kernels when compiled
   float* a32 = nullptr;         // TF32 hi/lo split of the projectors
@@ -386,6 +392,9 @@ void vb_forward_real(Context& ctx, const double* f, double scale, double* coef);
 // wavefunction-basis single transforms through the full-grid path (tests)
 void wb_backward_pair(Context& ctx, const double* c1, const double* c2, double* grid_out);
 
+// staged-FFT launch configuration by timing on the context's own data
+void autotune_fft(Context& ctx, std::vector<std::pair<std::string, double>>* log);
+
 // occ_n / Omega per band (device), used by the density kernels
 double* density_weights(Context& ctx);
 
@@ -398,6 +407,7 @@ double launch_ekin(Context& ctx);
 double launch_eigsum(Context& ctx);
 void launch_precond_update(Context& ctx);      // d_prec
 void launch_psda_elementwise(Context& ctx);    // residual->step, sets theta
+void launch_precondition_into(Context& ctx, const double* r, double* z);   // z = -K r
 void launch_cleanup(Context& ctx, double* c);  // Im c(G=0) = 0
 void launch_rank1_fix(Context& ctx, double* m, int ldm, const double* x, int ldx,
                       const double* y, int ldy, int nrow, int ncol, double alpha,

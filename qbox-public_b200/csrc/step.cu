@@ -271,6 +271,73 @@ void psda_update(Context& ctx) {
   ctx.extrapolate = true;
 }
 
+// JDWavefunctionStepper::update (src/JDWavefunctionStepper.cpp:47-376),
+// real basis: Y = C, HY = H C; residual R = HY - Y (Y^T HY); Z = -K R made
+// orthogonal to Y and orthonormal (gram); H Z by a second energy(); the
+// 2n x 2n matrix of H on span(Y, Z) (lower blocks Y^T HY, Z^T HY, Z^T HZ)
+// diagonalised by syevd; C <- Y q_Y + Z q_Z for the lowest n eigenvectors.
+// The products are FP64 in both precisions.
+void jd_update(Context& ctx) {
+  ProfScope ps(ctx, "jd_update");
+  const int n = ctx.nst, K = 2 * ctx.wb.ng, n2 = 2 * n;
+  const double one = 1.0, two = 2.0, zero = 0.0, mone = -1.0;
+  double* Y = ctx.d_c_last;
+  double* HY = ctx.d_dc_last;
+  double* A = ctx.d_nn;
+  const size_t wf = (size_t)K * n;
+  if (!ctx.d_jd_h) {
+    ctx.d_jd_h = dalloc<double>((size_t)n2 * n2);
+    ctx.d_jd_w = dalloc<double>(n2);
+    QBX_SOLVER(cusolverDnDsyevd_bufferSize(ctx.solver, CUSOLVER_EIG_MODE_VECTOR,
+                                           CUBLAS_FILL_MODE_LOWER, n2, ctx.d_jd_h, n2,
+                                           ctx.d_jd_w, &ctx.jd_lwork));
+    ctx.d_jd_work = dalloc<double>(std::max(1, ctx.jd_lwork));
+  }
+  QBX_CUDA(cudaMemcpyAsync(Y, ctx.d_c, wf * sizeof(double), cudaMemcpyDeviceToDevice, ctx.stream));
+  QBX_CUDA(cudaMemcpyAsync(HY, ctx.d_hc, wf * sizeof(double), cudaMemcpyDeviceToDevice,
+                           ctx.stream));
+  // residual in HC
+  QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, Y, K, HY, K, &zero, A, n));
+  launch_rank1_fix(ctx, A, n, Y, K, HY, K, n, n, -1.0, false);
+  QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, K, n, n, &mone, Y, K, A, n, &one,
+                       ctx.d_hc, K));
+  launch_precond_update(ctx);                       // kinetic energies of Y
+  launch_precondition_into(ctx, ctx.d_hc, ctx.d_c); // Z = -K R
+  QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, Y, K, ctx.d_c, K, &zero,
+                       A, n));
+  launch_rank1_fix(ctx, A, n, Y, K, ctx.d_c, K, n, n, -1.0, false);
+  QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, K, n, n, &mone, Y, K, A, n, &one,
+                       ctx.d_c, K));
+  gram(ctx);
+  energy(ctx, true, false);                         // H Z into HC
+  double* H = ctx.d_jd_h;
+  QBX_CUDA(cudaMemsetAsync(H, 0, sizeof(double) * (size_t)n2 * n2, ctx.stream));
+  QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, Y, K, HY, K, &zero, H,
+                       n2));
+  launch_rank1_fix(ctx, H, n2, Y, K, HY, K, n, n, -1.0, false);
+  QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, ctx.d_c, K, HY, K, &zero,
+                       H + n, n2));
+  launch_rank1_fix(ctx, H + n, n2, ctx.d_c, K, HY, K, n, n, -1.0, false);
+  QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, ctx.d_c, K, ctx.d_hc, K,
+                       &zero, H + n + (size_t)n * n2, n2));
+  launch_rank1_fix(ctx, H + n + (size_t)n * n2, n2, ctx.d_c, K, ctx.d_hc, K, n, n, -1.0, false);
+  QBX_SOLVER(cusolverDnDsyevd(ctx.solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n2, H,
+                              n2, ctx.d_jd_w, ctx.d_jd_work, ctx.jd_lwork, ctx.d_info));
+  // C = Y q[0:n, 0:n] + Z q[n:2n, 0:n]
+  QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, K, n, n, &one, ctx.d_c, K, H + n, n2,
+                       &zero, ctx.d_hc, K));
+  QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, K, n, n, &one, Y, K, H, n2, &one,
+                       ctx.d_hc, K));
+  QBX_CUDA(cudaMemcpyAsync(ctx.d_c, ctx.d_hc, wf * sizeof(double), cudaMemcpyDeviceToDevice,
+                           ctx.stream));
+  int info = 0;
+  QBX_CUDA(cudaMemcpyAsync(&info, ctx.d_info, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+  QBX_CUDA(cudaStreamSynchronize(ctx.stream));
+  QBX_REQUIRE(info == 0, 41, "syevd of the JD projected Hamiltonian failed (info=" +
+                                 std::to_string(info) + ")");
+  ctx.extrapolate = false;
+}
+
 void free_mixed(Context& ctx) {
   void** bufs[] = {&ctx.d_acc32, &ctx.cs_hi[0], &ctx.cs_lo[0], &ctx.cs_hi[1], &ctx.cs_lo[1],
                    &ctx.hs_hi, &ctx.hs_lo, &ctx.as_hi, &ctx.as_lo, &ctx.ss_hi, &ctx.ss_lo,

@@ -36,7 +36,7 @@ SYMBOLS = (
     "qbx_host_basis", "qbx_host_species_eval", "qbx_host_esr",
     "qbx_profile", "qbx_profile_get", "qbx_launch_count", "qbx_stream",
     "qbx_set_gemm_backend", "qbx_split_gemm_tn", "qbx_density_static",
-    "qbx_stress", "qbx_get_stress",
+    "qbx_stress", "qbx_get_stress", "qbx_autotune", "qbx_set_wf_dyn", "qbx_jd_update",
 )
 
 _lib = None
@@ -101,6 +101,9 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "qbx_split_gemm_tn": (_I, [_P, _I, _I, _I, _DP, _DP, _DP, _I]),
         "qbx_density_static": (_I, [_P, ctypes.c_void_p, _I, _DP, ctypes.c_void_p]),
         "qbx_stress": (_I, [_P, _DP, _DP]),
+        "qbx_autotune": (_I, [_P, ctypes.c_char_p, _I]),
+        "qbx_set_wf_dyn": (_I, [_P, ctypes.c_char_p]),
+        "qbx_jd_update": (_I, [_P]),
         "qbx_get_stress": (_I, [_P, _DP, _DP]),
     }
     for name, (res, args) in sig.items():
@@ -310,6 +313,20 @@ class Context:
         self._ok(self.lib.qbx_split_gemm_tn(self.h, m, n, k, _dp(at), _dp(bt), _dp(out),
                                             backend), "split_gemm_tn")
         return out.T
+
+    def set_wf_dyn(self, name: str):
+        """qbx_set_wf_dyn: "PSDA" or "JD" for the update of scf_step."""
+        self._ok(self.lib.qbx_set_wf_dyn(self.h, name.encode()), "set_wf_dyn")
+
+    def jd_update(self):
+        self._ok(self.lib.qbx_jd_update(self.h), "jd_update")
+
+    def autotune(self) -> str:
+        """qbx_autotune: time the staged-FFT configurations on this context
+        and keep the fastest; returns the report."""
+        buf = ctypes.create_string_buffer(4096)
+        self._ok(self.lib.qbx_autotune(self.h, buf, 4096), "autotune")
+        return buf.value.decode()
 
     STRESS_PARTS = ("ekin", "eps", "enl", "ehart", "exc", "esr")
 

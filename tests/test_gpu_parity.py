@@ -212,3 +212,20 @@ def test_stress_matches_reference(name):
     scale = np.abs(g["sigma_first"]).max()
     np.testing.assert_allclose(rm["sigma"], g["sigma_first"], rtol=0, atol=1e-6 * scale)
     m.close()
+
+
+@pytest.mark.parametrize("precision", [capi.FP64, capi.MIXED])
+def test_jd_trajectory_matches_reference(precision):
+    """wf_dyn JD (JDWavefunctionStepper::update): the eigenvalue sum of six
+    steps from the seeded start against the reference's JD run; 1e-8 in
+    FP64, 1e-5 relative in the mixed precision."""
+    g = golden("si8_jd")
+    s = systems.si8()
+    ctx = capi.from_system(s, precision=precision)
+    ctx.set_wf_dyn("JD")
+    for it in range(int(g["nsteps"])):
+        r = ctx.scf_step()
+        ref = g["e_eigenvalue_sum"][it]
+        tol = 1e-8 if precision == capi.FP64 else 1e-5 * max(1.0, abs(ref))
+        assert abs(r["eigenvalue_sum"] - ref) < tol, (it, r["eigenvalue_sum"], ref)
+    ctx.close()
