@@ -127,6 +127,18 @@ int qbx_jd_update(qbx_context* ctx);
 int qbx_scf_step(qbx_context* ctx, int compute_forces, double* energies,
                  double* fion);
 
+/* No counterpart in the reference (one Qbox process runs one sample).  One
+ * electronic step of each of n independent contexts (different cells,
+ * cutoffs and band counts allowed), run concurrently: each context's work
+ * is ordered on its own stream and driven by its own host thread, so the
+ * GPU overlaps small systems.  energies receives n * QBX_NENERGY values (may
+ * be NULL); forces are not returned (compute_forces bit 0 is ignored, bit 1
+ * computes each context's stress for qbx_get_stress).  Returns the first
+ * failing context's status; its qbx_last_error holds the message.  The
+ * contexts must be distinct and not used by other threads meanwhile. */
+int qbx_scf_step_batch(qbx_context** ctxs, int n, int compute_forces,
+                       double* energies);
+
 /* The stress tensor of EnergyFunctional::energy(..., compute_stress=true,
  * sigma) (src/EnergyFunctional.cpp:440-1044, XCPotential::compute_stress
  * src/XCPotential.cpp:467-640, NonLocalPotential::energy's stress

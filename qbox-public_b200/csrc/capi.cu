@@ -9,6 +9,7 @@
 #include <map>
 #include <new>
 #include <stdexcept>
+#include <thread>
 #include <tuple>
 
 #include "../../include/qbx.h"
@@ -142,9 +143,11 @@ int qbx_create(qbx_context** out, int device, int precision) {
   h->c.device = device;
   h->c.precision = precision;
   if (const char* e = std::getenv("QBX_GEMM_BACKEND")) h->c.gemm_backend = std::atoi(e) == 0 ? 0 : 1;
-  // tall updates: TF32 splits by default; BF16 splits (QBX_TALL_KIND=0) are
-  // ~20% faster but leave C orthonormal only to ~1e-5
+  // tall updates: the rotation of C uses TF32 splits (BF16 splits would
+  // leave C orthonormal only to ~1e-5); the H*C updates use BF16 splits,
+  // ~20% faster, whose ~1e-5 relative error only enters the step direction
   if (const char* e = std::getenv("QBX_TALL_KIND")) h->c.tall_kind = std::atoi(e) == 0 ? 0 : 1;
+  if (const char* e = std::getenv("QBX_TALL_KIND_HC")) h->c.tall_kind_hc = std::atoi(e) == 1 ? 1 : 0;
   const int rc = guarded(h, [&](Context& c) {
     QBX_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
     QBX_BLAS(cublasCreate(&c.blas));
@@ -562,6 +565,27 @@ int qbx_scf_step(qbx_context* h, int forces, double* energies, double* fion) {
     QBX_CUDA(cudaStreamSynchronize(c.stream));
     QBX_REQUIRE(tc_check_error(c) == 0, 55, "tcgen05 GEMM pipeline wait timed out");
   });
+}
+
+int qbx_scf_step_batch(qbx_context** ctxs, int n, int compute_forces, double* energies) {
+  if (!ctxs || n <= 0) return 1;
+  for (int i = 0; i < n; i++)
+    if (!ctxs[i]) return 1;
+  // one host thread per context: each drives its own stream, so the GPU
+  // overlaps the systems' kernels; the steps' host synchronisations (energy
+  // reductions, Cholesky status) stall only their own system
+  std::vector<int> rc(n, 0);
+  std::vector<std::thread> th;
+  th.reserve(n);
+  for (int i = 0; i < n; i++)
+    th.emplace_back([&, i]() {
+      rc[i] = qbx_scf_step(ctxs[i], compute_forces,
+                           energies ? energies + (size_t)i * QBX_NENERGY : nullptr, nullptr);
+    });
+  for (auto& t : th) t.join();
+  for (int i = 0; i < n; i++)
+    if (rc[i]) return rc[i];
+  return 0;
 }
 
 int qbx_set_wf_dyn(qbx_context* h, const char* name) {

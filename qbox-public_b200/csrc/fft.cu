@@ -453,23 +453,8 @@ static std::vector<double2> twiddle_table(int n) {
   return t;
 }
 
-struct TwiddleCache {
-  int n[3] = {0, 0, 0};
-  double2* d[3] = {nullptr, nullptr, nullptr};
-};
-static TwiddleCache g_tw[16];   // per device
-
-static const double2* twiddles(int dev, int axis, int n) {
-  TwiddleCache& c = g_tw[dev & 15];
-  if (c.n[axis] != n) {
-    if (c.d[axis]) cudaFree(c.d[axis]);
-    std::vector<double2> t = twiddle_table(n);
-    c.d[axis] = dalloc<double2>(n);
-    h2d_sync(c.d[axis], t.data(), n * sizeof(double2));
-    c.n[axis] = n;
-  }
-  return c.d[axis];
-}
+// the twiddle table of one axis of a context's grid
+static const double2* twiddles(const Context& ctx, int axis) { return ctx.dws.tw[axis]; }
 
 void upload_sticks(DeviceSticks& d, const Basis& b) {
   free_sticks(d);
@@ -486,9 +471,16 @@ void upload_sticks(DeviceSticks& d, const Basis& b) {
   d.px = make_plan(b.n0);
   d.py = make_plan(b.n1);
   d.pz = make_plan(b.n2);
+  const int n[3] = {b.n0, b.n1, b.n2};
+  for (int a = 0; a < 3; a++) {
+    std::vector<double2> t = twiddle_table(n[a]);
+    d.tw[a] = dalloc<double2>(n[a]);
+    h2d_sync(d.tw[a], t.data(), n[a] * sizeof(double2));
+  }
 }
 
 void free_sticks(DeviceSticks& d) {
+  for (int a = 0; a < 3; a++) dfree(d.tw[a]);
   dfree(d.rod_first); dfree(d.rod_lmin); dfree(d.rod_size);
   dfree(d.stick_y); dfree(d.stick_col); dfree(d.col_x);
   dfree(d.ip); dfree(d.im);
@@ -540,13 +532,13 @@ static void staged_batch(Context& ctx, int op, const double* c, const double* v,
   const DeviceSticks& g = ctx.dws;
   cudaStream_t st = ctx.stream;
   C* zbuf = (C*)ctx.d_zbuf;
-  const double2* twz = twiddles(ctx.device, 2, g.n2);
-  const double2* twx = twiddles(ctx.device, 0, g.n0);
-  const double2* twy = twiddles(ctx.device, 1, g.n1);
+  const double2* twz = twiddles(ctx, 2);
+  const double2* twx = twiddles(ctx, 0);
+  const double2* twy = twiddles(ctx, 1);
   const int ngw = ctx.wb.ng;
   dim3 zgrid((g.nrods + kRodsPerCta - 1) / kRodsPerCta, npairs);
   const size_t zs = zsmem<T>(g.n2);
-  QBX_CUDA(cudaFuncSetAttribute(k_zfft_bwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zs));
+  allow_smem(k_zfft_bwd<T>, zs);
   {
     ProfScope ps(ctx, "zfft_bwd");
     k_zfft_bwd<T><<<zgrid, 256, zs, st>>>((const double2*)c, ngw, ctx.nst, pair0, g, twz, zbuf,
@@ -563,22 +555,20 @@ static void staged_batch(Context& ctx, int op, const double* c, const double* v,
   chunks = (npairs + ppc - 1) / ppc;
   dim3 xgrid(g.n2, chunks);
   if (op == OP_DENSITY) {
-    QBX_CUDA(cudaFuncSetAttribute(k_xy<T, OP_DENSITY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)xc.smem));
+    allow_smem(k_xy<T, OP_DENSITY>, xc.smem);
     ProfScope ps(ctx, "xy_density");
     k_xy<T, OP_DENSITY><<<xgrid, 512, xc.smem, st>>>(zbuf, npairs, ppc, g, twx, twy, nullptr, rho, w,
                                                    pair0, ctx.nst, xc.cc, xc.rr);
     QBX_LAUNCHED(ctx);
   } else {
-    QBX_CUDA(cudaFuncSetAttribute(k_xy<T, OP_VPSI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)xc.smem));
+    allow_smem(k_xy<T, OP_VPSI>, xc.smem);
     {
       ProfScope ps(ctx, "xy_vpsi");
       k_xy<T, OP_VPSI><<<xgrid, 512, xc.smem, st>>>(zbuf, npairs, ppc, g, twx, twy, v, nullptr,
                                                   nullptr, pair0, ctx.nst, xc.cc, xc.rr);
       QBX_LAUNCHED(ctx);
     }
-    QBX_CUDA(cudaFuncSetAttribute(k_zfft_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zs));
+    allow_smem(k_zfft_fwd<T>, zs);
     const double scale = 1.0 / ((double)g.n0 * g.n1 * g.n2);
     ProfScope ps(ctx, "zfft_fwd");
     k_zfft_fwd<T><<<zgrid, 256, zs, st>>>(zbuf, ngw, ctx.nst, pair0, g, twz, scale,
@@ -609,9 +599,9 @@ static bool staged_fast(Context& ctx, int op, const double* c, const double* v, 
   a.hc = hc;
   a.nst = ctx.nst;
   a.zbuf = ctx.d_zfast;
-  a.twx = twiddles(ctx.device, 0, g.n0);
-  a.twy = twiddles(ctx.device, 1, g.n1);
-  a.twz = twiddles(ctx.device, 2, g.n2);
+  a.twx = twiddles(ctx, 0);
+  a.twy = twiddles(ctx, 1);
+  a.twz = twiddles(ctx, 2);
   a.rods_per_cta = ctx.fast_rods;
   a.xy_warps = ctx.fast_warps;
   a.vpsi_shape = ctx.fast_vpsi_shape;
@@ -676,17 +666,17 @@ static void grid_fft(Context& ctx, int dir) {
   const int L = 16;
   for (int axis = 0; axis < 3; axis++) {
     const RadixPlan p = make_plan(n[axis]);
-    const double2* tw = twiddles(ctx.device, axis, n[axis]);
+    const double2* tw = twiddles(ctx, axis);
     int nblocks;
     if (axis == 0) nblocks = (b.n1 * b.n2 + L - 1) / L;
     else if (axis == 1) nblocks = ((b.n0 + L - 1) / L) * b.n2;
     else nblocks = ((b.n0 + L - 1) / L) * b.n1;
     const size_t smem = sizeof(double2) * (size_t)n[axis] * (1 + 2 * L);
     if (dir > 0) {
-      QBX_CUDA(cudaFuncSetAttribute(k_line_fft<+1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      allow_smem(k_line_fft<+1>, smem);
       k_line_fft<+1><<<nblocks, 256, smem, ctx.stream>>>((double2*)ctx.d_grid, b.n0, b.n1, b.n2, axis, p, tw, L);
     } else {
-      QBX_CUDA(cudaFuncSetAttribute(k_line_fft<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      allow_smem(k_line_fft<-1>, smem);
       k_line_fft<-1><<<nblocks, 256, smem, ctx.stream>>>((double2*)ctx.d_grid, b.n0, b.n1, b.n2, axis, p, tw, L);
     }
     QBX_LAUNCHED(ctx);
@@ -747,10 +737,9 @@ static void density_buffers_t(Context& ctx, const double* c, int nst, const doub
   const int batch = (int)std::min<size_t>(npairs_all, zbuf_bytes / per_pair);
   QBX_REQUIRE(batch >= 1, 60, "stick buffer smaller than one band pair");
   const size_t zs = zsmem<T>(g.n2);
-  QBX_CUDA(cudaFuncSetAttribute(k_zfft_bwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zs));
+  allow_smem(k_zfft_bwd<T>, zs);
   XYConfig<T> xc = xy_config<T>(g, ctx.device);
-  QBX_CUDA(cudaFuncSetAttribute(k_xy<T, OP_DENSITY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)xc.smem));
+  allow_smem(k_xy<T, OP_DENSITY>, xc.smem);
   int sms = 0;
   QBX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device));
   for (int p0 = 0; p0 < npairs_all; p0 += batch) {

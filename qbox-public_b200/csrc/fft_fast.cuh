@@ -509,8 +509,7 @@ void launch_vpsi_xy(Context& ctx, const StagedArgs& a) {
   const DeviceSticks& g = ctx.dws;
   const int nw = std::min(a.xy_warps, xy_threads(SH) / 32);
   const size_t sm = xy_smem_bytes<T, N, N, XY_VPSI>(g.ncol, nw);
-  QBX_CUDA(cudaFuncSetAttribute(kxy<T, N, N, XY_VPSI, SH>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  allow_smem(kxy<T, N, N, XY_VPSI, SH>, sm);
   kxy<T, N, N, XY_VPSI, SH><<<dim3(N, a.npairs), 32 * nw, sm, ctx.stream>>>(
       (C*)a.zbuf, a.npairs, 1, g, a.twx, a.twy, (const T*)a.v, nullptr, nullptr, a.pair0, a.nst);
   QBX_LAUNCHED(ctx);
@@ -520,8 +519,7 @@ template <int N, int OP, int SH>
 void launch_lane_xy(Context& ctx, const StagedArgs& a, int chunks, int ppc) {
   const DeviceSticks& g = ctx.dws;
   const size_t sm = xyl_smem_bytes<N, N, OP>(g.ncol);
-  QBX_CUDA(cudaFuncSetAttribute(kxy_lane<N, N, OP, SH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)sm));
+  allow_smem(kxy_lane<N, N, OP, SH>, sm);
   int threads = lane_threads(SH);
   if (SH == 3 || SH == 4) {
     const int want = (g.ncol * lane::lanes_for(N) + 31) / 32 * 32;
@@ -542,7 +540,7 @@ void run_cubic(Context& ctx, const StagedArgs& a) {
   const int rpc = a.rods_per_cta;
   const size_t zs = sizeof(C) * ((size_t)N + (size_t)2 * rpc * pitch(N));
   dim3 zgrid((g.nrods + rpc - 1) / rpc, a.npairs);
-  QBX_CUDA(cudaFuncSetAttribute(kz_bwd<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zs));
+  allow_smem(kz_bwd<T, N>, zs);
   {
     ProfScope ps(ctx, "zfft_bwd");
     kz_bwd<T, N><<<zgrid, kZThreads, zs, st>>>((const double2*)a.c, ngw, a.nst, a.pair0, g, a.twz,
@@ -571,8 +569,7 @@ void run_cubic(Context& ctx, const StagedArgs& a) {
           default: launch_lane_xy<N, XY_VPSI, 0>(ctx, a, a.npairs, 1); break;
         }
       }
-      QBX_CUDA(cudaFuncSetAttribute(kz_fwd<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)zs));
+      allow_smem(kz_fwd<T, N>, zs);
       const double scale = 1.0 / ((double)N * N * N);
       ProfScope ps(ctx, "zfft_fwd");
       kz_fwd<T, N><<<zgrid, kZThreads, zs, st>>>((const C*)a.zbuf, ngw, a.nst, a.pair0, g, a.twz,
@@ -586,8 +583,7 @@ void run_cubic(Context& ctx, const StagedArgs& a) {
     constexpr int SH = XYDefault<T, XY_DENSITY>::shape;
     const int nw = std::min(a.xy_warps, xy_threads(SH) / 32);
     const size_t sm = xy_smem_bytes<T, N, N, XY_DENSITY>(g.ncol, nw);
-    QBX_CUDA(cudaFuncSetAttribute(kxy<T, N, N, XY_DENSITY, SH>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    allow_smem(kxy<T, N, N, XY_DENSITY, SH>, sm);
     int chunks = std::max(1, std::min(a.npairs, a.density_chunks));
     const int ppc = (a.npairs + chunks - 1) / chunks;
     chunks = (a.npairs + ppc - 1) / ppc;
@@ -607,7 +603,7 @@ void run_cubic(Context& ctx, const StagedArgs& a) {
       launch_vpsi_xy<T, N, 3>(ctx, a);
     }
   }
-  QBX_CUDA(cudaFuncSetAttribute(kz_fwd<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zs));
+  allow_smem(kz_fwd<T, N>, zs);
   const double scale = 1.0 / ((double)N * N * N);
   ProfScope ps(ctx, "zfft_fwd");
   kz_fwd<T, N><<<zgrid, kZThreads, zs, st>>>((const C*)a.zbuf, ngw, a.nst, a.pair0, g, a.twz, scale,

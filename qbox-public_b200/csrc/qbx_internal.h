@@ -48,6 +48,25 @@ struct Error {
 #define QBX_LAUNCHED(ctx)                                                    \
   do { QBX_CUDA(cudaGetLastError()); (ctx).nlaunch++; } while (0)
 
+// Dynamic shared memory above 48 KB needs a per-kernel opt-in, and that
+// attribute is process-wide.  Host threads stepping different systems would
+// race if each set the size its own launch needs (a smaller value from one
+// thread can land between another's set and launch), so every launch opts in
+// to the device maximum less the kernel's static shared memory: the same
+// value from every thread.  The need itself is checked here.
+template <typename K>
+inline void allow_smem(K kernel, size_t need) {
+  int dev = 0, optin = 0;
+  QBX_CUDA(cudaGetDevice(&dev));
+  QBX_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  cudaFuncAttributes fa;
+  QBX_CUDA(cudaFuncGetAttributes(&fa, (const void*)kernel));
+  const size_t lim = (size_t)optin - fa.sharedSizeBytes;
+  QBX_REQUIRE(need <= lim, 20, "kernel shared memory above the device limit");
+  QBX_CUDA(cudaFuncSetAttribute((const void*)kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)lim));
+}
+
 // ------------------------------------------------------------ FFT geometry
 // A mixed-radix plan for one 1-D length (radices 2,3,4,5,7,8,11).
 struct RadixPlan {
@@ -103,6 +122,8 @@ struct DeviceSticks {
   int* ip;           // ng
   int* im;           // ng
   RadixPlan px, py, pz;
+  double2* tw[3];    // exp(+2 pi i k/n) for the x, y, z lengths (owned here,
+                     // so contexts of different grids never share tables)
 };
 
 // -------------------------------------------------------------- species
@@ -312,14 +333,17 @@ struct Context {
   float* a32lo = nullptr;
   float* s32 = nullptr;         // TF32 hi/lo split of a small matrix
   float* s32lo = nullptr;
-  int tall_kind = 1;            // TALL_TF32 (default) or TALL_BF16 for the tall updates
+  int tall_kind = 1;            // split kind of the rotation C (I - X): TF32 by default
+  int tall_kind_hc = 0;         // split kind of the H*C updates A_nl F and C A: BF16
   void* at_hi = nullptr;        // split of A_nl^T (projectors contiguous), ld tall_ld(nproj)
   void* at_lo = nullptr;
   void* ct_hi = nullptr;        // split of C^T (bands contiguous), ld tall_ld(nst)
   void* ct_lo = nullptr;
   void* tm_hi = nullptr;        // split of the small right-hand matrix, ld tall_ld(rows)
   void* tm_lo = nullptr;
-  int tall_ld(int n) const { return tall_kind == 1 ? (n + 3) / 4 * 4 : (n + 7) / 8 * 8; }
+  // leading dimension of a split of the given kind (16-byte rows)
+  static int tall_ld_of(int kind, int n) { return kind == 1 ? (n + 3) / 4 * 4 : (n + 7) / 8 * 8; }
+  int tall_ld(int n) const { return tall_ld_of(tall_kind, n); }
   void* d_tc_ws = nullptr;      // split-K partials of the tcgen05 GEMM
   size_t tc_ws_elems = 0;
   void* d_tc_err = nullptr;     // wait-timeout flag of the tcgen05 GEMM

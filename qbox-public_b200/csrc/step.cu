@@ -96,12 +96,13 @@ static void polar(Context& ctx, double* x, double tol, int maxiter) {
 
 // out += alpha * c * M for the FP64 wavefunction block c (K x n) and an n x n
 // matrix M: the tcgen05 kernel on the transposed split of c (BF16 or TF32
-// hi/lo, ctx.tall_kind), or three cuBLAS TF32 products on its plain split.
-// out may be c itself: both read the split copy of c.
-static void tall_update(Context& ctx, const double* c, const double* M, double alpha, double* out) {
+// hi/lo of the given kind), or three cuBLAS TF32 products on its plain
+// split.  out may be c itself: both read the split copy of c.
+static void tall_update(Context& ctx, int kind, const double* c, const double* M, double alpha,
+                        double* out) {
   const int n = ctx.nst, K = 2 * ctx.wb.ng;
   if (ctx.gemm_backend == 1) {
-    const int kind = ctx.tall_kind, ld = ctx.tall_ld(n);
+    const int ld = Context::tall_ld_of(kind, n);
     split_plain(ctx, kind, M, n, n, n, ctx.tm_hi, ctx.tm_lo, ld);   // M is K-major as stored
     split_t(ctx, kind, c, K, n, K, ctx.ct_hi, ctx.ct_lo, ld);
     tc_gemm_kind_tn(ctx, kind, K, n, n, alpha, ctx.ct_hi, ctx.ct_lo, ld, ctx.tm_hi, ctx.tm_lo, ld,
@@ -150,7 +151,8 @@ void ortho_align(Context& ctx) {
     // correction, so C stays orthonormal to the accuracy of the overlap.
     double* T = ctx.d_nn3;
     launch_identity_axpy(ctx, T, X, n, -1.0);
-    tall_update(ctx, ctx.d_c, T, -1.0, ctx.d_c);
+    // rotation: TF32 splits, so that C stays orthonormal to ~1e-7
+    tall_update(ctx, ctx.tall_kind, ctx.d_c, T, -1.0, ctx.d_c);
   } else {
     QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, K, n, n, &one, ctx.d_ctmp, K, X, n,
                          &zero, ctx.d_c, K));
@@ -197,7 +199,7 @@ static void nonlocal(Context& ctx, bool hpsi) {
     if (mx) {
       if (ctx.gemm_backend == 1) {
         // F (np x n) is already K-major for this product: a plain split
-        const int kind = ctx.tall_kind, ld = ctx.tall_ld(np);
+        const int kind = ctx.tall_kind_hc, ld = Context::tall_ld_of(kind, np);
         split_plain(ctx, kind, ctx.d_fnl, np, n, np, ctx.tm_hi, ctx.tm_lo, ld);
         tc_gemm_kind_tn(ctx, kind, K, n, np, 1.0, ctx.at_hi, ctx.at_lo, ld, ctx.tm_hi, ctx.tm_lo,
                         ld, 1.0, ctx.d_hc, K);
@@ -256,7 +258,7 @@ void psda_update(Context& ctx) {
       split_gemm(ctx, true, false, n, n, K, 2.0, ctx.cs_hi[0], ctx.cs_lo[0], ctx.ldp, ctx.hs_hi,
                  ctx.hs_lo, ctx.ldp, 0.0, A);
       launch_rank1_fix(ctx, A, n, ctx.d_c, K, ctx.d_hc, K, n, n, -1.0, false);
-      tall_update(ctx, ctx.d_c, A, -1.0, ctx.d_hc);
+      tall_update(ctx, ctx.tall_kind_hc, ctx.d_c, A, -1.0, ctx.d_hc);
     } else {
       QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, ctx.d_c, K, ctx.d_hc,
                            K, &zero, A, n));
@@ -398,8 +400,8 @@ void alloc_mixed(Context& ctx) {
     if (ctx.d_anl) {
       split_bf16_2d(ctx, ctx.d_anl, (int)K, (int)np, (int)K, ctx.as_hi, ctx.as_lo, ctx.ldp);
       split_tf32(ctx, ctx.d_anl, (int)K, (int)np, (int)K, ctx.a32, ctx.a32lo, ctx.ldp);
-      split_t(ctx, ctx.tall_kind, ctx.d_anl, (int)K, (int)np, (int)K, ctx.at_hi, ctx.at_lo,
-              ctx.tall_ld((int)np));
+      split_t(ctx, ctx.tall_kind_hc, ctx.d_anl, (int)K, (int)np, (int)K, ctx.at_hi, ctx.at_lo,
+              Context::tall_ld_of(ctx.tall_kind_hc, (int)np));
     }
   }
   QBX_CUDA(cudaStreamSynchronize(ctx.stream));

@@ -312,15 +312,16 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
                                   const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
+// looked up once; the function-local static's initialisation is thread-safe
+// (concurrent steps of several systems)
 static EncodeTiledFn encode_fn() {
-  static EncodeTiledFn fn = nullptr;
-  if (!fn) {
+  static const EncodeTiledFn fn = []() {
     void* p = nullptr;
     cudaDriverEntryPointQueryResult q;
     QBX_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
     QBX_REQUIRE(p && q == cudaDriverEntryPointSuccess, 52, "cuTensorMapEncodeTiled unavailable");
-    fn = (EncodeTiledFn)p;
-  }
+    return (EncodeTiledFn)p;
+  }();
   return fn;
 }
 
@@ -409,13 +410,11 @@ static void tc_gemm_tn(Context& ctx, int kind, int m, int n, int k, double alpha
   QBX_REQUIRE(splits > 1 ? tn <= 65535 : tm <= 65535, 54, "too many tiles for the grid");
   dim3 grid = splits > 1 ? dim3(tm, tn, splits) : dim3(tn, tm, 1);
   if (kind == tc::KIND_BF16) {
-    QBX_CUDA(cudaFuncSetAttribute(tc::k_tc_split_gemm<tc::KIND_BF16>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
+    allow_smem(tc::k_tc_split_gemm<tc::KIND_BF16>, tc::SMEM_BYTES);
     tc::k_tc_split_gemm<tc::KIND_BF16><<<grid, tc::THREADS, tc::SMEM_BYTES, ctx.stream>>>(
         mah, mal, mbh, mbl, m, n, nkb, kbps, ws, C, ldc, alpha, beta, (int*)ctx.d_tc_err);
   } else {
-    QBX_CUDA(cudaFuncSetAttribute(tc::k_tc_split_gemm<tc::KIND_TF32>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
+    allow_smem(tc::k_tc_split_gemm<tc::KIND_TF32>, tc::SMEM_BYTES);
     tc::k_tc_split_gemm<tc::KIND_TF32><<<grid, tc::THREADS, tc::SMEM_BYTES, ctx.stream>>>(
         mah, mal, mbh, mbl, m, n, nkb, kbps, ws, C, ldc, alpha, beta, (int*)ctx.d_tc_err);
   }

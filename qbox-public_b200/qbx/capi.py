@@ -37,6 +37,7 @@ SYMBOLS = (
     "qbx_profile", "qbx_profile_get", "qbx_launch_count", "qbx_stream",
     "qbx_set_gemm_backend", "qbx_split_gemm_tn", "qbx_density_static",
     "qbx_stress", "qbx_get_stress", "qbx_autotune", "qbx_set_wf_dyn", "qbx_jd_update",
+    "qbx_scf_step_batch",
 )
 
 _lib = None
@@ -103,6 +104,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "qbx_stress": (_I, [_P, _DP, _DP]),
         "qbx_autotune": (_I, [_P, ctypes.c_char_p, _I]),
         "qbx_set_wf_dyn": (_I, [_P, ctypes.c_char_p]),
+        "qbx_scf_step_batch": (_I, [ctypes.POINTER(_P), _I, _I, _DP]),
         "qbx_jd_update": (_I, [_P]),
         "qbx_get_stress": (_I, [_P, _DP, _DP]),
     }
@@ -363,6 +365,21 @@ class Context:
 
     def get_coeffs_async(self, out_pinned: np.ndarray):
         self._ok(self.lib.qbx_get_coeffs_async(self.h, _dp(out_pinned)), "get_coeffs_async")
+
+
+def scf_step_batch(contexts, stress: bool = False):
+    """qbx_scf_step_batch: one electronic step of every context, run
+    concurrently; returns a list of energy dicts."""
+    lib = load()
+    n = len(contexts)
+    arr = (_P * n)(*[c.h for c in contexts])
+    e = np.zeros(n * NENERGY)
+    rc = lib.qbx_scf_step_batch(arr, n, 2 if stress else 0, _dp(e))
+    if rc:
+        msgs = [lib.qbx_last_error(c.h) for c in contexts]
+        msg = next((m.decode() for m in msgs if m), "")
+        raise QbxError(f"scf_step_batch: code {rc}: {msg}")
+    return [dict(zip(ENERGY_NAMES, e[i * NENERGY:(i + 1) * NENERGY])) for i in range(n)]
 
 
 def from_system(system, device: int = 0, precision: int = FP64,

@@ -229,3 +229,20 @@ def test_jd_trajectory_matches_reference(precision):
         tol = 1e-8 if precision == capi.FP64 else 1e-5 * max(1.0, abs(ref))
         assert abs(r["eigenvalue_sum"] - ref) < tol, (it, r["eigenvalue_sum"], ref)
     ctx.close()
+
+
+def test_batch_of_systems_matches_single_steps():
+    """qbx_scf_step_batch over six systems of the 32-system batch (different
+    cells, cutoffs, grids and band counts), run concurrently, gives the
+    energies of stepping each context on its own."""
+    systs = systems.batch()[:6]
+    ctxs = [capi.from_system(s, precision=capi.FP64) for s in systs]
+    ref = [capi.from_system(s, precision=capi.FP64) for s in systs]
+    for _ in range(2):
+        eb = capi.scf_step_batch(ctxs)
+        es = [c.scf_step() for c in ref]
+        for a, b in zip(eb, es):
+            assert abs(a["etotal"] - b["etotal"]) < 1e-10 * max(1.0, abs(b["etotal"]))
+            assert abs(a["eigenvalue_sum"] - b["eigenvalue_sum"]) < 1e-9 * max(1.0, abs(b["eigenvalue_sum"]))
+    for c in ctxs + ref:
+        c.close()
