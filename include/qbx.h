@@ -129,15 +129,47 @@ int qbx_scf_step(qbx_context* ctx, int compute_forces, double* energies,
 
 /* No counterpart in the reference (one Qbox process runs one sample).  One
  * electronic step of each of n independent contexts (different cells,
- * cutoffs and band counts allowed), run concurrently: each context's work
- * is ordered on its own stream and driven by its own host thread, so the
- * GPU overlaps small systems.  energies receives n * QBX_NENERGY values (may
- * be NULL); forces are not returned (compute_forces bit 0 is ignored, bit 1
+ * cutoffs and band counts allowed), run concurrently.  When every context
+ * has its step captured as a graph (qbx_set_step_graph), one host thread
+ * launches all the graphs, each on its context's stream, and then collects
+ * the energies; otherwise each context is driven by its own host thread.
+ * Either way the GPU overlaps the systems.  energies receives
+ * n * QBX_NENERGY values (may be NULL); forces are not returned
+ * (compute_forces bit 0 only selects the forces variant of the step, bit 1
  * computes each context's stress for qbx_get_stress).  Returns the first
  * failing context's status; its qbx_last_error holds the message.  The
  * contexts must be distinct and not used by other threads meanwhile. */
 int qbx_scf_step_batch(qbx_context** ctxs, int n, int compute_forces,
                        double* energies);
+
+/* DoubleMatrix::polar (src/Matrix.cpp:2446-2540), the orthogonal polar
+ * factor used by SlaterDet::ortho_align: x (nst x nst, column-major, host)
+ * is replaced by its polar factor.  Bjorck-Bowie steps while
+ * ||I - x^T x||_F < 1, Higham steps x <- (x + x^-T)/2 otherwise, stopping
+ * after the step in which the norm is <= tol or after maxiter steps.
+ * graph != 0 runs the loop as the captured step does (a CUDA graph whose
+ * WHILE and IF/ELSE conditional nodes decide on the device).  iters (may be
+ * NULL) receives the number of steps. */
+int qbx_polar(qbx_context* ctx, double* x, double tol, int maxiter, int graph,
+              int* iters);
+
+/* No counterpart in the reference.  on != 0: qbx_scf_step (PSDA, with or
+ * without forces; not JD, not stress, not while profiling) runs as a CUDA
+ * graph.  Each configuration (first step / later steps with the Anderson
+ * extrapolation, with / without forces) runs eagerly once, which sizes every
+ * lazily grown buffer, and is captured on its second use; later steps launch
+ * the graph.  Inside, the reductions stay in device slots, the Anderson
+ * theta is formed on the device and the polar iteration of ortho_align is a
+ * conditional WHILE node; the host reads the scalars once after the graph.
+ * Changing the cell, atoms, precision, GEMM backend, stepper or FFT tuning
+ * drops the graphs.  A step that cannot be captured turns graphs off and
+ * runs eagerly; qbx_step_graph_info then reports why. */
+int qbx_set_step_graph(qbx_context* ctx, int on);
+/* captured: graphs currently instantiated (0-4); launches: graph launches
+ * so far; note (may be NULL): why capture was abandoned, empty if it was
+ * not. */
+int qbx_step_graph_info(qbx_context* ctx, int* captured, long* launches,
+                        char* note, int note_len);
 
 /* The stress tensor of EnergyFunctional::energy(..., compute_stress=true,
  * sigma) (src/EnergyFunctional.cpp:440-1044, XCPotential::compute_stress

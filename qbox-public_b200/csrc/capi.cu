@@ -29,6 +29,7 @@ void update_vhxc(Context& ctx);
 void energy(Context& ctx, bool hpsi, bool forces);
 void psda_update(Context& ctx);
 void jd_update(Context& ctx);
+int polar_entry(Context& ctx, double* x, double tol, int maxiter, bool graph);
 }
 
 using namespace qbx;
@@ -55,7 +56,17 @@ int guarded(qbx_context* h, F f) {
   }
 }
 
+// Captured steps hold the buffer pointers and launch shapes of the moment of
+// capture; anything that changes those drops them.
+void drop_graphs(Context& c) {
+  for (auto& g : c.graphs) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    g = StepGraph{};
+  }
+}
+
 void free_cell(Context& c) {
+  drop_graphs(c);
   free_mixed(c);
   free_sticks(c.dws);
   free_sticks(c.dvs);
@@ -76,6 +87,8 @@ void free_cell(Context& c) {
 }
 
 void free_atoms(Context& c) {
+  drop_graphs(c);
+  if (c.h_fion) { cudaFreeHost(c.h_fion); c.h_fion = nullptr; }
   double** bufs[] = {&c.d_anl, &c.d_fnl, &c.d_dfnl, &c.d_pdfac, &c.d_sfac, &c.d_vps,
                      &c.d_rhops_sp, &c.d_fion, &c.d_dvps, &c.d_vnl, &c.d_dvnl,
                      &c.d_tau_all, &c.d_astress};
@@ -111,7 +124,7 @@ __global__ void k_permute(const double2* __restrict__ in, const int* __restrict_
 void upload_weights(Context& c) {
   std::vector<double> w(c.nst);
   for (int n = 0; n < c.nst; n++) w[n] = c.occ[n] / c.wb.omega;
-  h2d_sync(c.d_scalars + 16, w.data(), sizeof(double) * c.nst);
+  h2d_sync(c.d_scalars + kSlots, w.data(), sizeof(double) * c.nst);
 }
 
 void check_ready(const Context& c, bool atoms) {
@@ -121,11 +134,144 @@ void check_ready(const Context& c, bool atoms) {
 
 }  // namespace
 
-// density weights live after the 16 scalar slots
+// density weights live after the scalar slots
 namespace qbx {
-double* density_weights(Context& c) { return c.d_scalars + 16; }
+double* density_weights(Context& c) { return c.d_scalars + kSlots; }
 Context& context_of(qbx_context* h) { return h->c; }
 }
+
+namespace {
+
+// The energies, eigenvalue sum and forces of a step from the read-back slots.
+void finish_step(Context& c, bool want_f, bool want_s) {
+  finish_density(c);
+  finish_vhxc(c);
+  finish_energy(c, want_f);
+  finish_eigsum(c);
+  if (want_s) finish_stress(c);
+}
+
+// BOSampleStepper's electronic step (src/BOSampleStepper.cpp:795-1114 with
+// nite = 0), every operation on c.stream.
+void step_eager(Context& c, bool want_f, bool want_s, double* energies, double* fion) {
+  update_density(c);
+  update_vhxc(c);
+  energy(c, true, want_f);
+  if (want_s) compute_stress(c);
+  launch_eigsum(c);
+  readback(c, want_f);
+  check_status(c);
+  finish_step(c, want_f, want_s);
+  fill_energies(c, energies);
+  if (want_f && fion) std::memcpy(fion, c.fion.data(), sizeof(double) * c.fion.size());
+  if (c.wf_dyn == 1) jd_update(c);
+  else psda_update(c);
+  readback(c, false);
+  check_status(c);
+  finish_theta(c);
+}
+
+// The same PSDA step captured into one graph: the reductions stay on the
+// device, the Anderson theta and the polar iteration are decided there
+// (conditional nodes), and the last nodes copy slots, status and forces to
+// the pinned mirrors.  The graph is instantiated, not launched.
+void capture_step(Context& c, bool want_f, StepGraph& g) {
+  const bool prof = c.prof.on, extrap = c.extrapolate;
+  const long n0 = c.nlaunch;
+  c.prof.on = false;
+  QBX_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeRelaxed));
+  c.capturing = true;
+  cudaGraph_t graph = nullptr;
+  try {
+    update_density(c);
+    update_vhxc(c);
+    energy(c, true, want_f);
+    launch_eigsum(c);
+    psda_update(c);
+    enqueue_readback(c, want_f);
+  } catch (...) {
+    cudaStreamEndCapture(c.stream, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    c.capturing = false;
+    c.prof.on = prof;
+    c.extrapolate = extrap;
+    c.nlaunch = n0;
+    throw;
+  }
+  c.capturing = false;
+  c.prof.on = prof;
+  c.extrapolate = extrap;
+  g.nkernels = c.nlaunch - n0;
+  c.nlaunch = n0;
+  QBX_CUDA(cudaStreamEndCapture(c.stream, &graph));
+  cudaGraphInstantiateParams ip = {};
+  const cudaError_t e = cudaGraphInstantiateWithParams(&g.exec, graph, &ip);
+  if (e != cudaSuccess) {
+    g.exec = nullptr;
+    std::string why = std::string("graph instantiation: ") + cudaGetErrorString(e) +
+                      " (result " + std::to_string((int)ip.result_out) + ")";
+    if (ip.errNode_out) {
+      cudaGraphNodeType t;
+      if (cudaGraphNodeGetType(ip.errNode_out, &t) == cudaSuccess) {
+        why += ", node type " + std::to_string((int)t);
+        if (t == cudaGraphNodeTypeKernel) {
+          cudaKernelNodeParams kp = {};
+          const char* name = nullptr;
+          if (cudaGraphKernelNodeGetParams(ip.errNode_out, &kp) == cudaSuccess &&
+              cudaFuncGetName(&name, kp.func) == cudaSuccess && name)
+            why += std::string(" ") + name;
+        } else if (t == cudaGraphNodeTypeMemcpy) {
+          cudaMemcpy3DParms mp = {};
+          if (cudaGraphMemcpyNodeGetParams(ip.errNode_out, &mp) == cudaSuccess)
+            why += ", copy kind " + std::to_string((int)mp.kind);
+        }
+      }
+    }
+    cudaGetLastError();
+    cudaGraphDestroy(graph);
+    throw Error{57, why};
+  }
+  cudaGraphDestroy(graph);
+}
+
+// The captured graph of this step's configuration, or null when the step
+// runs eagerly (graphs off, JD, stress, profiling, or the first use of the
+// configuration, which sizes the lazily grown buffers before any capture).
+StepGraph* step_graph_for(Context& c, bool want_f, bool want_s) {
+  if (!c.step_graph || c.wf_dyn != 0 || want_s || c.prof.on) return nullptr;
+  StepGraph& g = c.graphs[(c.extrapolate ? 1 : 0) + (want_f ? 2 : 0)];
+  if (g.exec) return &g;
+  if (g.uses++ == 0) return nullptr;
+  try {
+    capture_step(c, want_f, g);
+  } catch (const Error& e) {
+    // a step that cannot be captured keeps running eagerly
+    c.graph_note = e.msg;
+    c.step_graph = false;
+    return nullptr;
+  }
+  return &g;
+}
+
+void launch_step_graph(Context& c, StepGraph& g) {
+  QBX_CUDA(cudaGraphLaunch(g.exec, c.stream));
+  c.nlaunch += g.nkernels;
+  c.graph_launches++;
+}
+
+// after the graph of a step has completed
+// after the graph of a step has completed; the energies report the theta of
+// the previous update, as the eager step (which reports before updating) does
+void finish_graph_step(Context& c, bool want_f, double* energies, double* fion) {
+  check_status(c);
+  finish_step(c, want_f, false);
+  fill_energies(c, energies);
+  finish_theta(c);
+  c.extrapolate = true;
+  if (want_f && fion) std::memcpy(fion, c.fion.data(), sizeof(double) * c.fion.size());
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -153,7 +299,19 @@ int qbx_create(qbx_context** out, int device, int precision) {
     QBX_BLAS(cublasCreate(&c.blas));
     QBX_BLAS(cublasSetStream(c.blas, c.stream));
     QBX_SOLVER(cusolverDnCreate(&c.solver));
-    QBX_SOLVER(cusolverDnSetStream(c.solver, c.stream));
+    for (auto& s : c.side) QBX_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    // cuBLAS workspace owned by the context (rebound with every stream)
+    c.blas_ws_bytes = (size_t)32 << 20;
+    QBX_CUDA(cudaMalloc(&c.d_blas_ws, c.blas_ws_bytes));
+    bind_stream(c, c.stream);
+    // status words and the pinned mirrors of slots and status
+    c.d_status = dalloc<int>(kStatus);
+    QBX_CUDA(cudaMemset(c.d_status, 0, kStatus * sizeof(int)));
+    QBX_CUDA(cudaMallocHost(&c.h_scalars, kSlots * sizeof(double)));
+    QBX_CUDA(cudaMallocHost(&c.h_status, kStatus * sizeof(int)));
+    std::memset(c.h_scalars, 0, kSlots * sizeof(double));
+    std::memset(c.h_status, 0, kStatus * sizeof(int));
+    QBX_CUDA(cudaDeviceSynchronize());
   });
   if (rc) { delete h; return rc; }
   *out = h;
@@ -167,8 +325,14 @@ void qbx_destroy(qbx_context* h) {
   free_atoms(h->c);
   free_cell(h->c);
   dfree(h->d_perm);
+  dfree(h->c.d_status);
+  if (h->c.d_blas_ws) cudaFree(h->c.d_blas_ws);
+  if (h->c.h_scalars) cudaFreeHost(h->c.h_scalars);
+  if (h->c.h_status) cudaFreeHost(h->c.h_status);
   if (h->c.blas) cublasDestroy(h->c.blas);
   if (h->c.solver) cusolverDnDestroy(h->c.solver);
+  for (auto s : h->c.side)
+    if (s) cudaStreamDestroy(s);
   if (h->c.stream) cudaStreamDestroy(h->c.stream);
   delete h;
 }
@@ -191,6 +355,7 @@ int qbx_set_precision(qbx_context* h, int precision) {
       c.zbuf_bytes = per_pair * c.pair_batch;
     }
     c.precision = precision;
+    drop_graphs(c);
     alloc_mixed(c);
   });
 }
@@ -254,7 +419,8 @@ int qbx_set_cell(qbx_context* h, const double cell[9], double ecut, int nst, con
     c.solver_lwork = std::max(lw1, lw2);
     c.d_solver_work = dalloc<double>(std::max(1, c.solver_lwork));
     c.d_red = dalloc<double>(4 * 1024);
-    c.d_scalars = dalloc<double>(16 + nst);
+    c.d_scalars = dalloc<double>(kSlots + nst);
+    QBX_CUDA(cudaMemset(c.d_scalars, 0, kSlots * sizeof(double)));
     upload_weights(c);
     // staged FFT stick buffer: bounded to ~4 GB per batch of band pairs
     const int npairs = (nst + 1) / 2;
@@ -406,6 +572,7 @@ int qbx_set_atoms(qbx_context* h, const int* na, const double* tau) {
       c.d_tau_all = dupload(tall);
     }
     c.d_fion = dalloc<double>(3 * std::max(1, natoms));
+    QBX_CUDA(cudaMallocHost(&c.h_fion, 3 * std::max(1, natoms) * sizeof(double)));
     // species tables on the density sphere (EnergyFunctional::cell_moved,
     // src/EnergyFunctional.cpp:1200-1245)
     std::vector<double> vps((size_t)ngv * nsp), rhops((size_t)ngv * nsp), dvps((size_t)ngv * nsp);
@@ -484,7 +651,8 @@ int qbx_gram(qbx_context* h) {
   return guarded(h, [&](Context& c) {
     check_ready(c, false);
     gram(c);
-    QBX_CUDA(cudaStreamSynchronize(c.stream));
+    readback(c, false);
+    check_status(c);
   });
 }
 
@@ -492,6 +660,8 @@ int qbx_update_density(qbx_context* h, double* total_charge) {
   return guarded(h, [&](Context& c) {
     check_ready(c, true);
     update_density(c);
+    readback(c, false);
+    finish_density(c);
     if (total_charge) *total_charge = c.total_charge;
   });
 }
@@ -508,6 +678,8 @@ int qbx_update_vhxc(qbx_context* h) {
   return guarded(h, [&](Context& c) {
     check_ready(c, true);
     update_vhxc(c);
+    readback(c, false);
+    finish_vhxc(c);
   });
 }
 
@@ -523,7 +695,9 @@ int qbx_energy(qbx_context* h, int hpsi, int forces, double* energies, double* f
   return guarded(h, [&](Context& c) {
     check_ready(c, true);
     energy(c, hpsi != 0, forces != 0);
-    QBX_CUDA(cudaStreamSynchronize(c.stream));
+    readback(c, forces != 0);
+    check_status(c);
+    finish_energy(c, forces != 0);
     fill_energies(c, energies);
     if (forces && fion) std::memcpy(fion, c.fion.data(), sizeof(double) * c.fion.size());
   });
@@ -532,7 +706,9 @@ int qbx_energy(qbx_context* h, int hpsi, int forces, double* energies, double* f
 int qbx_eigenvalue_sum(qbx_context* h, double* eig) {
   return guarded(h, [&](Context& c) {
     check_ready(c, true);
-    c.eigsum = launch_eigsum(c);
+    launch_eigsum(c);
+    readback(c, false);
+    finish_eigsum(c);
     if (eig) *eig = c.eigsum;
   });
 }
@@ -541,7 +717,9 @@ int qbx_psda_update(qbx_context* h) {
   return guarded(h, [&](Context& c) {
     check_ready(c, true);
     psda_update(c);
-    QBX_CUDA(cudaStreamSynchronize(c.stream));
+    readback(c, false);
+    check_status(c);
+    finish_theta(c);
   });
 }
 
@@ -549,21 +727,54 @@ int qbx_psda_reset(qbx_context* h) {
   return guarded(h, [&](Context& c) { c.extrapolate = false; });
 }
 
+
 int qbx_scf_step(qbx_context* h, int forces, double* energies, double* fion) {
   return guarded(h, [&](Context& c) {
     check_ready(c, true);
     const bool want_f = (forces & 1) != 0, want_s = (forces & 2) != 0;
-    update_density(c);
-    update_vhxc(c);
-    energy(c, true, want_f);
-    if (want_s) compute_stress(c);
-    c.eigsum = launch_eigsum(c);
-    fill_energies(c, energies);
-    if (want_f && fion) std::memcpy(fion, c.fion.data(), sizeof(double) * c.fion.size());
-    if (c.wf_dyn == 1) jd_update(c);
-    else psda_update(c);
-    QBX_CUDA(cudaStreamSynchronize(c.stream));
-    QBX_REQUIRE(tc_check_error(c) == 0, 55, "tcgen05 GEMM pipeline wait timed out");
+    if (StepGraph* g = step_graph_for(c, want_f, want_s)) {
+      launch_step_graph(c, *g);
+      QBX_CUDA(cudaStreamSynchronize(c.stream));
+      finish_graph_step(c, want_f, energies, fion);
+      return;
+    }
+    step_eager(c, want_f, want_s, energies, fion);
+  });
+}
+
+int qbx_polar(qbx_context* h, double* x, double tol, int maxiter, int graph, int* iters) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, false);
+    QBX_REQUIRE(x && maxiter > 0, 1, "bad polar arguments");
+    const size_t nn = (size_t)c.nst * c.nst;
+    double* d = c.d_nn2;
+    QBX_CUDA(cudaMemcpyAsync(d, x, nn * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    const int it = polar_entry(c, d, tol, maxiter, graph != 0);
+    QBX_CUDA(cudaMemcpyAsync(x, d, nn * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    readback(c, false);
+    check_status(c);
+    if (iters) *iters = it;
+  });
+}
+
+int qbx_set_step_graph(qbx_context* h, int on) {
+  return guarded(h, [&](Context& c) {
+    c.step_graph = on != 0;
+    c.graph_note.clear();
+    drop_graphs(c);
+  });
+}
+
+int qbx_step_graph_info(qbx_context* h, int* captured, long* launches, char* note, int note_len) {
+  return guarded(h, [&](Context& c) {
+    int n = 0;
+    for (auto& g : c.graphs) n += g.exec != nullptr;
+    if (captured) *captured = n;
+    if (launches) *launches = c.graph_launches;
+    if (note && note_len > 0) {
+      std::strncpy(note, c.graph_note.c_str(), (size_t)note_len - 1);
+      note[note_len - 1] = 0;
+    }
   });
 }
 
@@ -571,9 +782,42 @@ int qbx_scf_step_batch(qbx_context** ctxs, int n, int compute_forces, double* en
   if (!ctxs || n <= 0) return 1;
   for (int i = 0; i < n; i++)
     if (!ctxs[i]) return 1;
-  // one host thread per context: each drives its own stream, so the GPU
-  // overlaps the systems' kernels; the steps' host synchronisations (energy
-  // reductions, Cholesky status) stall only their own system
+  // When every context has its step captured, one thread launches all the
+  // graphs (each on its context's stream, so the GPU runs the systems side
+  // by side), then waits for each and forms its energies.
+  {
+    const bool want_f = (compute_forces & 1) != 0;
+    std::vector<StepGraph*> gs(n, nullptr);
+    bool all = (compute_forces & 2) == 0;
+    for (int i = 0; i < n && all; i++) {
+      Context& c = ctxs[i]->c;
+      if (!c.step_graph || c.wf_dyn != 0 || c.prof.on || !c.have_cell || c.tau.empty()) {
+        all = false;
+        break;
+      }
+      gs[i] = &c.graphs[(c.extrapolate ? 1 : 0) + (want_f ? 2 : 0)];
+      all = gs[i]->exec != nullptr;
+    }
+    if (all) {
+      for (int i = 0; i < n; i++) {
+        const int rc = guarded(ctxs[i], [&](Context& c) { launch_step_graph(c, *gs[i]); });
+        if (rc) return rc;
+      }
+      int first = 0;
+      for (int i = 0; i < n; i++) {
+        const int rc = guarded(ctxs[i], [&](Context& c) {
+          QBX_CUDA(cudaStreamSynchronize(c.stream));
+          finish_graph_step(c, want_f,
+                            energies ? energies + (size_t)i * QBX_NENERGY : nullptr, nullptr);
+        });
+        if (rc && !first) first = rc;
+      }
+      return first;
+    }
+  }
+  // Otherwise one host thread per context: each drives its own stream, so
+  // the GPU overlaps the systems' kernels; the host synchronisations of an
+  // eager step stall only their own system.
   std::vector<int> rc(n, 0);
   std::vector<std::thread> th;
   th.reserve(n);
@@ -594,6 +838,7 @@ int qbx_set_wf_dyn(qbx_context* h, const char* name) {
     QBX_REQUIRE(s == "PSDA" || s == "JD", 1, "wf_dyn must be PSDA or JD");
     c.wf_dyn = (s == "JD") ? 1 : 0;
     c.extrapolate = false;
+    drop_graphs(c);
   });
 }
 
@@ -601,6 +846,8 @@ int qbx_jd_update(qbx_context* h) {
   return guarded(h, [&](Context& c) {
     check_ready(c, true);
     jd_update(c);
+    readback(c, false);
+    check_status(c);
   });
 }
 
@@ -608,6 +855,7 @@ int qbx_autotune(qbx_context* h, char* report, int report_len) {
   return guarded(h, [&](Context& c) {
     check_ready(c, true);
     std::vector<std::pair<std::string, double>> log;
+    drop_graphs(c);   // the launch shapes may change
     autotune_fft(c, &log);
     if (report && report_len > 0) {
       std::string r;
@@ -631,7 +879,9 @@ int qbx_stress(qbx_context* h, double* sigma, double* parts) {
   return guarded(h, [&](Context& c) {
     check_ready(c, true);
     compute_stress(c);
-    QBX_CUDA(cudaStreamSynchronize(c.stream));
+    readback(c, false);
+    check_status(c);
+    finish_stress(c);
     copy_stress(c, sigma, parts);
   });
 }
@@ -751,6 +1001,7 @@ int qbx_set_gemm_backend(qbx_context* h, int backend) {
   return guarded(h, [&](Context& c) {
     QBX_REQUIRE(backend == 0 || backend == 1, 1, "backend must be 0 (cuBLAS) or 1 (tcgen05)");
     c.gemm_backend = backend;
+    drop_graphs(c);
   });
 }
 

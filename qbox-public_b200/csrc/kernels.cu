@@ -57,16 +57,15 @@ __global__ void k_reduce_final(const double* partial, int nb, double* out) {
   }
 }
 
+// K sums of f over [0, n) into the scalar slots [slot, slot + K); no host
+// synchronisation (the host reads the slots after the step)
 template <int K, typename F>
-static void reduce(Context& ctx, F f, size_t n, double* host_out) {
+static void reduce(Context& ctx, F f, size_t n, int slot) {
   const int nb = (int)std::max<size_t>(1, std::min<size_t>(kRedBlocks, (n + kThreads - 1) / kThreads));
   k_reduce<K><<<nb, kThreads, 0, ctx.stream>>>(f, n, ctx.d_red);
   QBX_LAUNCHED(ctx);
-  k_reduce_final<K><<<1, kThreads, 0, ctx.stream>>>(ctx.d_red, nb, ctx.d_scalars);
+  k_reduce_final<K><<<1, kThreads, 0, ctx.stream>>>(ctx.d_red, nb, ctx.d_scalars + slot);
   QBX_LAUNCHED(ctx);
-  QBX_CUDA(cudaMemcpyAsync(host_out, ctx.d_scalars, K * sizeof(double), cudaMemcpyDeviceToHost,
-                           ctx.stream));
-  QBX_CUDA(cudaStreamSynchronize(ctx.stream));
 }
 
 static int blocks_for(size_t n) {
@@ -78,10 +77,8 @@ struct SumF {
   __device__ void operator()(size_t i, double* a) const { a[0] += x[i]; }
 };
 
-double dsum(Context& ctx, const double* x, size_t n) {
-  double r;
-  reduce<1>(ctx, SumF{x}, n, &r);
-  return r;
+void launch_sum(Context& ctx, const double* x, size_t n, int slot) {
+  reduce<1>(ctx, SumF{x}, n, slot);
 }
 
 // ------------------------------------------------------------------- XC
@@ -229,7 +226,7 @@ void launch_xc(Context& ctx) {
   if (ctx.xc == "LDA") {
     k_lda<<<nb, kThreads, 0, ctx.stream>>>(ctx.d_rhor, N, ctx.d_vxc, ctx.d_exc);
     QBX_LAUNCHED(ctx);
-    ctx.exc = dsum(ctx, ctx.d_exc, N) * om / (double)N;
+    launch_sum(ctx, ctx.d_exc, N, SLOT_EXC);
     return;
   }
   // PBE: grad rho by three backward transforms of i G_j rho(G)/Omega
@@ -244,12 +241,8 @@ void launch_xc(Context& ctx) {
   k_pbe<<<nb, kThreads, 0, ctx.stream>>>(ctx.d_rhor, ctx.d_grad, N, ctx.d_vxc, ctx.d_vx2,
                                          ctx.d_exc);
   QBX_LAUNCHED(ctx);
-  {
-    double s2[2];
-    reduce<2>(ctx, SumRhoV1F{ctx.d_exc, ctx.d_rhor, ctx.d_vxc}, N, s2);
-    ctx.exc = s2[0] * om / (double)N;
-    ctx.xc_rhov1 = s2[1];    // sum_r rho v1, for the XC stress
-  }
+  // sum e_xc and sum rho v1 (the latter for the XC stress)
+  reduce<2>(ctx, SumRhoV1F{ctx.d_exc, ctx.d_rhor, ctx.d_vxc}, N, SLOT_EXC);
   // vxc += sum_j backward(i G_j forward(grad_j vxc2))
   for (int j = 0; j < 3; j++) {
     k_mul<<<nb, kThreads, 0, ctx.stream>>>(ctx.d_grad + j * N, ctx.d_vx2, N, ctx.d_exc);
@@ -295,12 +288,9 @@ __global__ void k_vlocal_g(const double2* __restrict__ rhog, const double2* __re
 void launch_vhxc_gspace(Context& ctx) {
   const int ngv = ctx.vb.ng;
   const double om = ctx.vb.omega;
-  double s[2];
   reduce<2>(ctx, EpsEhF{(const double2*)ctx.d_rhog, (const double2*)ctx.d_vion,
                         (const double2*)ctx.d_rhops, ctx.d_g2i_v, 1.0 / om},
-            (size_t)ngv, s);
-  ctx.eps = s[0] * om;
-  ctx.ehart = om * 4.0 * M_PI * s[1];
+            (size_t)ngv, SLOT_EPS_EH);
   k_vlocal_g<<<blocks_for(ngv), kThreads, 0, ctx.stream>>>(
       (const double2*)ctx.d_rhog, (const double2*)ctx.d_vion, (const double2*)ctx.d_rhops,
       ctx.d_g2i_v, ngv, 1.0 / om, (double2*)ctx.d_vtmp_g, (double2*)ctx.d_vtmp_g2);
@@ -320,11 +310,9 @@ struct EkinF {
   }
 };
 
-double launch_ekin(Context& ctx) {
-  double r;
+void launch_ekin(Context& ctx) {
   reduce<1>(ctx, EkinF{(const double2*)ctx.d_c, ctx.d_g2_w, ctx.d_occ, ctx.wb.ng},
-            (size_t)ctx.wb.ng * ctx.nst, &r);
-  return r;
+            (size_t)ctx.wb.ng * ctx.nst, SLOT_EKIN);
 }
 
 struct EigF {
@@ -338,11 +326,9 @@ struct EigF {
   }
 };
 
-double launch_eigsum(Context& ctx) {
-  double r;
+void launch_eigsum(Context& ctx) {
   reduce<1>(ctx, EigF{(const double2*)ctx.d_c, (const double2*)ctx.d_hc, ctx.wb.ng},
-            (size_t)ctx.wb.ng * ctx.nst, &r);
-  return r;
+            (size_t)ctx.wb.ng * ctx.nst, SLOT_EIG);
 }
 
 // Preconditioner::update (src/Preconditioner.cpp:88-143): per-band kinetic
@@ -403,9 +389,20 @@ struct AndersonF {
   }
 };
 
+// theta = -<dc, dc - dc_last> / |dc - dc_last|^2 from the two sums, reset to
+// 0 below -1 and capped at 2 (src/PSDAWavefunctionStepper.cpp:129-179)
+__device__ __forceinline__ double anderson_theta(const double* ab) {
+  double theta = ab[1] != 0.0 ? -ab[0] / ab[1] : 0.0;
+  if (theta < -1.0) theta = 0.0;
+  return fmin(2.0, theta);
+}
+
 __global__ void k_psda_update(double2* __restrict__ c, double2* __restrict__ c_last,
                               double2* __restrict__ dc_last, const double2* __restrict__ dc,
-                              size_t n, double theta, int extrapolate) {
+                              size_t n, const double* __restrict__ ab, int extrapolate,
+                              double* __restrict__ theta_out) {
+  const double theta = extrapolate ? anderson_theta(ab) : 0.0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *theta_out = theta;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
     const double2 x = c[i], f = dc[i];
@@ -431,19 +428,14 @@ void launch_psda_elementwise(Context& ctx) {
   k_precondition<<<blocks_for(n), kThreads, 0, ctx.stream>>>((double2*)ctx.d_hc, ctx.d_g2_w,
                                                               ctx.d_prec, ctx.wb.ng, n);
   QBX_LAUNCHED(ctx);
-  double theta = 0.0;
-  if (ctx.extrapolate) {
-    double ab[2];
+  if (ctx.extrapolate)
     reduce<2>(ctx, AndersonF{(const double2*)ctx.d_hc, (const double2*)ctx.d_dc_last, ctx.wb.ng},
-              n, ab);
-    if (ab[1] != 0.0) theta = -ab[0] / ab[1];
-    if (theta < -1.0) theta = 0.0;
-    theta = std::min(2.0, theta);
-  }
-  ctx.theta = theta;
+              n, SLOT_ANDERSON);
+  // theta is formed on the device from the two sums
   k_psda_update<<<blocks_for(n), kThreads, 0, ctx.stream>>>(
       (double2*)ctx.d_c, (double2*)ctx.d_c_last, (double2*)ctx.d_dc_last,
-      (const double2*)ctx.d_hc, n, theta, ctx.extrapolate ? 1 : 0);
+      (const double2*)ctx.d_hc, n, ctx.d_scalars + SLOT_ANDERSON, ctx.extrapolate ? 1 : 0,
+      ctx.d_scalars + SLOT_THETA);
   QBX_LAUNCHED(ctx);
 }
 
@@ -505,14 +497,13 @@ __global__ void k_fnl_scale(double* f, const double* dfac, int np, size_t n, dou
 }
 
 // E_nl and fnl <- D F / Omega (src/NonLocalPotential.cpp:1469-1597)
-double launch_enl(Context& ctx) {
+void launch_enl(Context& ctx) {
   const size_t n = (size_t)ctx.nproj * ctx.nst;
-  double e;
-  reduce<1>(ctx, EnlF{ctx.d_fnl, ctx.d_pdfac, ctx.d_occ, ctx.nproj, 1.0 / ctx.wb.omega}, n, &e);
+  reduce<1>(ctx, EnlF{ctx.d_fnl, ctx.d_pdfac, ctx.d_occ, ctx.nproj, 1.0 / ctx.wb.omega}, n,
+            SLOT_ENL);
   k_fnl_scale<<<blocks_for(n), kThreads, 0, ctx.stream>>>(ctx.d_fnl, ctx.d_pdfac, ctx.nproj, n,
                                                           1.0 / ctx.wb.omega);
   QBX_LAUNCHED(ctx);
-  return e;
 }
 
 // c'(G) = G_j (i c(G)) for the force projections dF_j = 2 A^T c'
@@ -595,18 +586,15 @@ __global__ void k_local_force(const double* __restrict__ gx, const double2* __re
 void launch_local_forces(Context& ctx, double* fion) {
   const int ngv = ctx.vb.ng;
   int atom0 = 0;
-  double* d_tau = nullptr;
   for (size_t is = 0; is < ctx.species.size(); is++) {
     const int na = (int)ctx.tau[is].size() / 3;
     if (na == 0) continue;
-    d_tau = dupload(ctx.tau[is]);
+    // positions of this species: a slice of the species-major d_tau_all
     k_local_force<<<na, kThreads, 0, ctx.stream>>>(
         ctx.d_gx_v, (const double2*)ctx.d_vtmp_g2, (const double2*)ctx.d_rhog,
         ctx.d_vps + is * (size_t)ngv, ctx.d_rhops_sp + is * (size_t)ngv, ctx.d_g2i_v, ngv,
-        1.0 / ctx.vb.omega, d_tau, -2.0 * ctx.vb.omega, atom0, fion);
+        1.0 / ctx.vb.omega, ctx.d_tau_all + 3 * (size_t)atom0, -2.0 * ctx.vb.omega, atom0, fion);
     QBX_LAUNCHED(ctx);
-    QBX_CUDA(cudaStreamSynchronize(ctx.stream));
-    dfree(d_tau);
     atom0 += na;
   }
 }
@@ -652,10 +640,8 @@ struct Sq {
   const double* q;
   __device__ void operator()(size_t i, double* a) const { a[0] += q[i] * q[i]; }
 };
-double launch_frob(Context& ctx, const double* q, int n) {
-  double r;
-  reduce<1>(ctx, Sq{q}, (size_t)n * n, &r);
-  return sqrt(r);
+void launch_frob2(Context& ctx, const double* q, int n) {
+  reduce<1>(ctx, Sq{q}, (size_t)n * n, SLOT_FROB);
 }
 
 // ------------------------------------------------------ per-geometry setup
@@ -887,42 +873,31 @@ struct EnlStressF {
   }
 };
 
+// stress slots: kinetic, local, Hartree, XC, nonlocal sums (6 each)
+enum : int { SS_EKIN = SLOT_STRESS, SS_EPS = SLOT_STRESS + 6, SS_EHART = SLOT_STRESS + 12,
+             SS_EXC = SLOT_STRESS + 18, SS_ENL = SLOT_STRESS + 24 };
+static_assert(SS_ENL + 6 <= SLOT_SCRATCH, "stress slots overlap the scratch slots");
+
 void compute_stress(Context& ctx) {
   static const int vi[6] = {0, 1, 2, 0, 1, 0}, vj[6] = {0, 1, 2, 1, 2, 2};
-  const double om = ctx.wb.omega, om_inv = 1.0 / om;
+  const double om_inv = 1.0 / ctx.wb.omega;
   const int ngw = ctx.wb.ng, ngv = ctx.vb.ng, nst = ctx.nst, np = ctx.nproj;
   const int nsp = (int)ctx.species.size();
   const size_t N = ctx.N();
-  double* P = ctx.sigma_parts;        // ekin, eps, enl, ehart, exc, esr
-  const double eye[6] = {1, 1, 1, 0, 0, 0};
-  double t[6];
-  // kinetic
   reduce<6>(ctx, EkinStressF{(const double2*)ctx.d_c, ctx.d_gx_w, ctx.d_occ, ngw},
-            (size_t)ngw * nst, t);
-  for (int k = 0; k < 6; k++) P[k] = 2.0 * t[k] * om_inv;
-  // local pseudopotential
+            (size_t)ngw * nst, SS_EKIN);
   reduce<6>(ctx, EpsStressF{(const double2*)ctx.d_rhog, (const double2*)ctx.d_sfac, ctx.d_dvps,
                             ctx.d_g2i_v, ctx.d_gx_v, ngv, nsp, om_inv},
-            (size_t)ngv, t);
-  for (int k = 0; k < 6; k++) P[6 + k] = eye[k] * ctx.eps * om_inv + t[k];
-  // Hartree
+            (size_t)ngv, SS_EPS);
   reduce<6>(ctx, EhartStressF{(const double2*)ctx.d_rhog, (const double2*)ctx.d_rhops,
                               (const double2*)ctx.d_sfac, ctx.d_rhops_sp, ctx.d_g2i_v,
                               ctx.d_gx_v, ngv, nsp, om_inv, 1.5 * 1.5},
-            (size_t)ngv, t);
-  for (int k = 0; k < 6; k++) P[18 + k] = eye[k] * ctx.ehart * om_inv - 8.0 * M_PI * t[k];
-  // exchange-correlation
-  if (ctx.xc == "LDA") {
-    double d;
-    reduce<1>(ctx, LdaStressF{ctx.d_exc, ctx.d_rhor, ctx.d_vxc}, N, &d);
-    for (int k = 0; k < 6; k++) P[24 + k] = -eye[k] * d / (double)N;
-  } else {
-    reduce<6>(ctx, GgaStressF{ctx.d_grad, ctx.d_vx2, N}, N, t);
-    const double dsum = ctx.exc * (double)N / om - ctx.xc_rhov1;   // sum rho (e - v1)
-    for (int k = 0; k < 6; k++) P[24 + k] = -(eye[k] * dsum + t[k]) / (double)N;
-  }
-  // nonlocal
-  double tn[6] = {0, 0, 0, 0, 0, 0};
+            (size_t)ngv, SS_EHART);
+  if (ctx.xc == "LDA")
+    reduce<1>(ctx, LdaStressF{ctx.d_exc, ctx.d_rhor, ctx.d_vxc}, N, SS_EXC);
+  else
+    reduce<6>(ctx, GgaStressF{ctx.d_grad, ctx.d_vx2, N}, N, SS_EXC);
+  QBX_CUDA(cudaMemsetAsync(ctx.d_scalars + SS_ENL, 0, 6 * sizeof(double), ctx.stream));
   if (np) {
     const int K = 2 * ngw;
     if (!ctx.d_astress) ctx.d_astress = dalloc<double>((size_t)K * np);
@@ -948,11 +923,33 @@ void compute_stress(Context& ctx) {
         QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_T, CUBLAS_OP_N, np, nst, K, &two,
                              ctx.d_astress, K, ctx.d_c, K, &zero, ctx.d_dfnl, np));
       }
-      reduce<1>(ctx, EnlStressF{ctx.d_fnl, ctx.d_dfnl, ctx.d_occ, np}, (size_t)np * nst, &tn[k]);
+      reduce<1>(ctx, EnlStressF{ctx.d_fnl, ctx.d_dfnl, ctx.d_occ, np}, (size_t)np * nst,
+                SS_ENL + k);
     }
   }
-  for (int k = 0; k < 6; k++) P[12 + k] = (eye[k] * ctx.enl + tn[k]) * om_inv;
-  for (int k = 0; k < 6; k++) P[30 + k] = ctx.sigma_esr[k];
+}
+
+// The stress parts from the slots of compute_stress and the energies of the
+// same state (src/EnergyFunctional.cpp:397-1044 with compute_stress).
+void finish_stress(Context& ctx) {
+  const double om = ctx.wb.omega, om_inv = 1.0 / om;
+  const double N = (double)ctx.N();
+  const double* h = ctx.h_scalars;
+  double* P = ctx.sigma_parts;        // ekin, eps, enl, ehart, exc, esr
+  const double eye[6] = {1, 1, 1, 0, 0, 0};
+  for (int k = 0; k < 6; k++) {
+    P[k] = 2.0 * h[SS_EKIN + k] * om_inv;
+    P[6 + k] = eye[k] * ctx.eps * om_inv + h[SS_EPS + k];
+    P[12 + k] = (eye[k] * ctx.enl + h[SS_ENL + k]) * om_inv;
+    P[18 + k] = eye[k] * ctx.ehart * om_inv - 8.0 * M_PI * h[SS_EHART + k];
+    if (ctx.xc == "LDA") {
+      P[24 + k] = -eye[k] * h[SS_EXC] / N;
+    } else {
+      const double dsum = ctx.exc * N / om - ctx.xc_rhov1;   // sum rho (e - v1)
+      P[24 + k] = -(eye[k] * dsum + h[SS_EXC + k]) / N;
+    }
+    P[30 + k] = ctx.sigma_esr[k];
+  }
   for (int k = 0; k < 6; k++) {
     double s = 0.0;
     for (int q = 0; q < 6; q++) s += P[6 * q + k];

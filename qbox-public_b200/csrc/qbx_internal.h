@@ -204,6 +204,45 @@ struct Profiler {
   }
 };
 
+// Device scalar slots.  Every reduction of the electronic step writes its
+// sums into a fixed slot of ctx.d_scalars and nothing reads them back while
+// the step runs; the host copies all slots once (readback) and derives the
+// energies from that copy (finish_*).  With no host synchronisation inside,
+// a step can be captured as one CUDA graph.
+enum : int {
+  SLOT_CHARGE = 0,     // sum_r rho(r)
+  SLOT_EXC = 1,        // sum_r e_xc(r), sum_r rho v1 (PBE)
+  SLOT_EPS_EH = 3,     // sum rho*(G) vion(G), sum |rho_tot(G)|^2 / G^2
+  SLOT_EKIN = 5,
+  SLOT_ENL = 6,
+  SLOT_EIG = 7,
+  SLOT_ANDERSON = 8,   // the two sums of the Anderson theta
+  SLOT_THETA = 10,     // theta used by the last PSDA step
+  SLOT_FROB = 11,      // ||I - x^T x||_F^2 of the current polar iterate
+  SLOT_STRESS = 16,    // 30 sums of the stress tensor parts
+  SLOT_SCRATCH = 56,   // one-off sums
+  kSlots = 64
+};
+// Device status words of a step (int): solver info codes, the polar
+// iteration count and the tcgen05 wait-timeout flag.
+enum : int {
+  ST_INFO_GRAM = 0,
+  ST_INFO_ORTHO = 1,
+  ST_INFO_POLAR = 2,
+  ST_POLAR_ITERS = 3,
+  ST_TC_ERR = 4,
+  kStatus = 8
+};
+
+// One captured electronic step (PSDA, with or without forces, with or
+// without the Anderson extrapolation): an instantiated graph and the
+// number of this library's kernels it holds outside the polar loop.
+struct StepGraph {
+  cudaGraphExec_t exec = nullptr;
+  long nkernels = 0;
+  int uses = 0;        // eager runs of this configuration before capture
+};
+
 struct Context {
   int device = 0;
   int precision = FP64;
@@ -279,7 +318,11 @@ struct Context {
   double* d_solver_work = nullptr;
   int solver_lwork = 0;
   double* d_red = nullptr;      // reduction partials
-  double* d_scalars = nullptr;  // small device scalars
+  double* d_scalars = nullptr;  // kSlots scalar slots, then the density weights
+  double* h_scalars = nullptr;  // pinned host copy of the slots
+  int* d_status = nullptr;      // kStatus status words
+  int* h_status = nullptr;      // pinned host copy
+  double* h_fion = nullptr;     // pinned host copy of d_fion
   double* d_prec = nullptr;     // nst ekin per band
   double* d_fion = nullptr;     // 3*natoms
 
@@ -346,9 +389,19 @@ struct Context {
   int tall_ld(int n) const { return tall_ld_of(tall_kind, n); }
   void* d_tc_ws = nullptr;      // split-K partials of the tcgen05 GEMM
   size_t tc_ws_elems = 0;
-  void* d_tc_err = nullptr;     // wait-timeout flag of the tcgen05 GEMM
   long nlaunch = 0;              // kernels of this library launched so far
   Profiler prof;
+
+  // graph-captured steps (qbx_set_step_graph)
+  bool step_graph = false;
+  bool capturing = false;        // a step is being captured on `stream`
+  StepGraph graphs[4];           // by (extrapolate, forces)
+  cudaStream_t side[2] = {nullptr, nullptr};   // capture of conditional bodies
+  void* d_blas_ws = nullptr;     // cuBLAS workspace bound with every stream
+  size_t blas_ws_bytes = 0;
+  std::string graph_note;        // why the last capture was abandoned, if it was
+  long graph_launches = 0;       // captured steps launched so far
+  int polar_iters = 0;           // iterations of the last eager polar
 
   size_t N() const { return (size_t)vb.n0 * vb.n1 * vb.n2; }
 };
@@ -423,29 +476,50 @@ void autotune_fft(Context& ctx, std::vector<std::pair<std::string, double>>* log
 double* density_weights(Context& ctx);
 
 // pointwise kernels (kernels.cu)
-double dsum(Context& ctx, const double* x, size_t n);
-void launch_xc(Context& ctx);                  // fills d_vxc, ctx.exc
-void launch_vhxc_gspace(Context& ctx);         // eps, ehart, vlocal_g
+void launch_sum(Context& ctx, const double* x, size_t n, int slot);   // slot = sum x
+void launch_xc(Context& ctx);                  // fills d_vxc; SLOT_EXC
+void launch_vhxc_gspace(Context& ctx);         // SLOT_EPS_EH, vlocal_g
 void launch_setup_atoms(Context& ctx);         // sfac, vion, rhops, anl
-double launch_ekin(Context& ctx);
-double launch_eigsum(Context& ctx);
+void launch_ekin(Context& ctx);                // SLOT_EKIN
+void launch_eigsum(Context& ctx);              // SLOT_EIG
 void launch_precond_update(Context& ctx);      // d_prec
-void launch_psda_elementwise(Context& ctx);    // residual->step, sets theta
+void launch_psda_elementwise(Context& ctx);    // residual->step; SLOT_THETA
 void launch_precondition_into(Context& ctx, const double* r, double* z);   // z = -K r
 void launch_cleanup(Context& ctx, double* c);  // Im c(G=0) = 0
 void launch_rank1_fix(Context& ctx, double* m, int ldm, const double* x, int ldx,
                       const double* y, int ldy, int nrow, int ncol, double alpha,
                       bool lower_only);
-double launch_enl(Context& ctx);                // enl; fnl <- DF/omega
+void launch_enl(Context& ctx);                  // SLOT_ENL; fnl <- DF/omega
 void launch_local_forces(Context& ctx, double* fion);
 void launch_nl_forces(Context& ctx, double* fion);
-// stress tensor of the state of the last energy(): ctx.sigma, ctx.sigma_parts
+// stress tensor of the state of the last energy(): SLOT_STRESS; then
+// finish_stress gives ctx.sigma, ctx.sigma_parts
 void compute_stress(Context& ctx);
 void launch_identity_axpy(Context& ctx, double* t, const double* q, int n,
                           double alpha);       // t = I + alpha*q
 void launch_symmetrize_lower(Context& ctx, double* q, int n);
 void launch_avg_transpose(Context& ctx, double* x, const double* t, int n);
-double launch_frob(Context& ctx, const double* q, int n);
+void launch_frob2(Context& ctx, const double* q, int n);   // SLOT_FROB = ||q||_F^2
+
+// ------------------------------------------------ scalars of a step (scalars.cu)
+// Copies the slots and status words (and d_fion when `fion`) to their pinned
+// host mirrors on ctx.stream; no synchronisation (graph-capturable).
+void enqueue_readback(Context& ctx, bool fion);
+// enqueue_readback + wait for ctx.stream
+void readback(Context& ctx, bool fion);
+// one slot read now (synchronising; eager paths only)
+double read_slot(Context& ctx, int slot);
+// host values derived from the mirrors
+void finish_density(Context& ctx);   // total_charge
+void finish_vhxc(Context& ctx);      // exc, xc_rhov1, eps, ehart
+void finish_energy(Context& ctx, bool forces);   // ekin, enl, ecoul, etotal (+ fion)
+void finish_eigsum(Context& ctx);    // eigsum
+void finish_theta(Context& ctx);     // theta
+void finish_stress(Context& ctx);    // sigma, sigma_parts
+// throws the first nonzero status word as an error
+void check_status(Context& ctx);
+// binds cuBLAS (with the context's workspace) and cuSOLVER to stream s
+void bind_stream(Context& ctx, cudaStream_t s);
 
 // split-precision products (split_gemm.cu, tc_gemm.cu)
 void split_bf16(Context& ctx, const double* x, size_t n, void* hi, void* lo);

@@ -19,18 +19,12 @@ namespace qbx {
 
 static bool mixed(const Context& ctx) { return ctx.precision == MIXED; }
 
-static void require_potrf(Context& ctx, const char* what) {
-  int info = 0;
-  QBX_CUDA(cudaMemcpyAsync(&info, ctx.d_info, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
-  QBX_CUDA(cudaStreamSynchronize(ctx.stream));
-  QBX_REQUIRE(info == 0, 40, std::string(what) + ": matrix not positive definite (info=" +
-                                 std::to_string(info) + ")");
-}
-
 // S = 2 C^T C - c0 c0^T, lower triangle, then S = L L^T in place.  In the
 // mixed path the product uses the BF16 split of c in slot `split` and the
-// diagonal is recomputed exactly in FP64.
-static void overlap_cholesky(Context& ctx, const double* c, double* S, int split = -1) {
+// diagonal is recomputed exactly in FP64.  The factorisation's info code
+// goes to the status word `status` (checked when the step's scalars are
+// read back: a matrix that is not positive definite is an error there).
+static void overlap_cholesky(Context& ctx, const double* c, double* S, int status, int split) {
   ProfScope ps(ctx, "overlap_cholesky");
   const int n = ctx.nst, K = 2 * ctx.wb.ng;
   const double two = 2.0, zero = 0.0;
@@ -45,14 +39,13 @@ static void overlap_cholesky(Context& ctx, const double* c, double* S, int split
     launch_rank1_fix(ctx, S, n, c, K, c, K, n, n, -1.0, true);
   }
   QBX_SOLVER(cusolverDnDpotrf(ctx.solver, CUBLAS_FILL_MODE_LOWER, n, S, n, ctx.d_solver_work,
-                              ctx.solver_lwork, ctx.d_info));
-  require_potrf(ctx, "Cholesky of the overlap matrix");
+                              ctx.solver_lwork, ctx.d_status + status));
 }
 
 // SlaterDet::gram (src/SlaterDet.cpp:480-534): C <- C L^-T
 void gram(Context& ctx) {
   launch_cleanup(ctx, ctx.d_c);
-  overlap_cholesky(ctx, ctx.d_c, ctx.d_nn);
+  overlap_cholesky(ctx, ctx.d_c, ctx.d_nn, ST_INFO_GRAM, -1);
   const double one = 1.0;
   QBX_BLAS(cublasDtrsm(ctx.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T,
                        CUBLAS_DIAG_NON_UNIT, 2 * ctx.wb.ng, ctx.nst, &one, ctx.d_nn, ctx.nst,
@@ -63,6 +56,131 @@ void gram(Context& ctx) {
 // Bjorck-Bowie steps x <- x (I + q/2 (I + 3q/4)), q = I - x^T x, while
 // ||q||_F < 1, Higham steps x <- (x + x^-T)/2 otherwise; stops after the
 // step in which ||q||_F <= tol.
+
+// q = I - x^T x (full matrix) and SLOT_FROB = ||q||_F^2
+static void polar_q(Context& ctx, const double* x, double* q) {
+  const int n = ctx.nst;
+  const double one = 1.0, mone = -1.0;
+  launch_identity_axpy(ctx, q, q, n, 0.0);   // q = I
+  QBX_BLAS(cublasDsyrk(ctx.blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, n, n, &mone, x, n, &one, q, n));
+  launch_symmetrize_lower(ctx, q, n);
+  launch_frob2(ctx, q, n);
+}
+
+// x <- x (I + q/2 (I + 3q/4))
+static void polar_bjorck(Context& ctx, double* x, const double* q, double* t, double* qt,
+                         double* xp) {
+  const int n = ctx.nst;
+  const double one = 1.0, zero = 0.0;
+  launch_identity_axpy(ctx, t, q, n, 0.75);
+  QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &one, q, n, t, n, &zero, qt, n));
+  launch_identity_axpy(ctx, t, qt, n, 0.5);
+  QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &one, x, n, t, n, &zero, xp, n));
+  QBX_CUDA(cudaMemcpyAsync(x, xp, sizeof(double) * n * n, cudaMemcpyDeviceToDevice, ctx.stream));
+}
+
+// t = P I for the row interchanges of an LU factorisation (ipiv 1-based,
+// applied in order), one thread per column
+__global__ void k_pivoted_identity(double* __restrict__ t, const int* __restrict__ ipiv, int n) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  double* col = t + (size_t)j * n;
+  for (int i = 0; i < n; i++) col[i] = i == j ? 1.0 : 0.0;
+  for (int i = 0; i < n; i++) {
+    const int p = ipiv[i] - 1;
+    if (p != i && p >= 0 && p < n) {
+      const double a = col[i];
+      col[i] = col[p];
+      col[p] = a;
+    }
+  }
+}
+
+// x <- (x + x^-T)/2, x^-T by an LU factorisation of x^T (P x^T = L U) and
+// the two triangular solves of U^-1 L^-1 P.  (cuSOLVER's getrs would do the
+// same; at some sizes it allocates stream-ordered memory, which a
+// conditional graph body cannot hold.)
+static void polar_higham(Context& ctx, double* x, double* t, double* qt) {
+  const int n = ctx.nst;
+  const double one = 1.0, zero = 0.0;
+  QBX_BLAS(cublasDgeam(ctx.blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, &one, x, n, &zero, x, n, qt, n));
+  QBX_SOLVER(cusolverDnDgetrf(ctx.solver, n, n, qt, n, ctx.d_solver_work, ctx.d_ipiv,
+                              ctx.d_status + ST_INFO_POLAR));
+  k_pivoted_identity<<<(n + 127) / 128, 128, 0, ctx.stream>>>(t, ctx.d_ipiv, n);
+  QBX_LAUNCHED(ctx);
+  QBX_BLAS(cublasDtrsm(ctx.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
+                       CUBLAS_DIAG_UNIT, n, n, &one, qt, n, t, n));
+  QBX_BLAS(cublasDtrsm(ctx.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N,
+                       CUBLAS_DIAG_NON_UNIT, n, n, &one, qt, n, t, n));
+  launch_avg_transpose(ctx, x, t, n);
+}
+
+// After q of an iteration: choose the branch (1: Bjorck-Bowie, 0: Higham)
+// and whether another iteration follows, as the host loop below does.
+__global__ void k_polar_decide(const double* __restrict__ frob2, double tol, int maxiter,
+                               int* __restrict__ iters, cudaGraphConditionalHandle loop,
+                               cudaGraphConditionalHandle branch) {
+  const double qn = sqrt(*frob2);
+  const int it = *iters + 1;
+  *iters = it;
+  cudaGraphSetConditional(branch, qn < 1.0 ? 1u : 0u);
+  cudaGraphSetConditional(loop, (qn > tol && it < maxiter) ? 1u : 0u);
+}
+
+// ------------------------------------------------ conditional graph nodes
+// The graph being captured on stream s.
+static cudaGraph_t capture_graph(cudaStream_t s) {
+  cudaStreamCaptureStatus st;
+  cudaGraph_t g = nullptr;
+  QBX_CUDA(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, nullptr, nullptr));
+  QBX_REQUIRE(st == cudaStreamCaptureStatusActive && g, 56, "stream is not capturing");
+  return g;
+}
+
+// Appends a conditional node of the given type after the current capture
+// dependencies of s, makes it the only dependency, and returns its bodies.
+static cudaGraph_t* add_conditional(cudaStream_t s, cudaGraphConditionalHandle h,
+                                    cudaGraphConditionalNodeType type, unsigned size) {
+  cudaStreamCaptureStatus st;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  QBX_CUDA(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd));
+  QBX_REQUIRE(st == cudaStreamCaptureStatusActive, 56, "stream is not capturing");
+  cudaGraphNodeParams p = {};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = h;
+  p.conditional.type = type;
+  p.conditional.size = size;
+  cudaGraphNode_t node;
+  QBX_CUDA(cudaGraphAddNode(&node, g, deps, nd, &p));
+  QBX_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+  return p.conditional.phGraph_out;
+}
+
+// Runs f with ctx.stream (and cuBLAS/cuSOLVER) on s, capturing into body.
+template <typename F>
+static void capture_into(Context& ctx, cudaGraph_t body, cudaStream_t s, F f) {
+  cudaStream_t saved = ctx.stream;
+  QBX_CUDA(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0,
+                                         cudaStreamCaptureModeRelaxed));
+  ctx.stream = s;
+  bind_stream(ctx, s);
+  try {
+    f();
+  } catch (...) {
+    cudaGraph_t g;
+    cudaStreamEndCapture(s, &g);
+    ctx.stream = saved;
+    bind_stream(ctx, saved);
+    throw;
+  }
+  ctx.stream = saved;
+  bind_stream(ctx, saved);
+  cudaGraph_t g;
+  QBX_CUDA(cudaStreamEndCapture(s, &g));
+}
+
 static void polar(Context& ctx, double* x, double tol, int maxiter) {
   ProfScope ps(ctx, "polar");
   const int n = ctx.nst;
@@ -70,28 +188,78 @@ static void polar(Context& ctx, double* x, double tol, int maxiter) {
   double* t = ctx.d_nn4;
   double* qt = ctx.d_nn4 + (size_t)n * n;
   double* xp = ctx.d_nn4 + 2 * (size_t)n * n;
-  const double one = 1.0, zero = 0.0, mone = -1.0;
-  for (int iter = 0; iter < maxiter; iter++) {
-    launch_identity_axpy(ctx, q, q, n, 0.0);   // q = I
-    QBX_BLAS(cublasDsyrk(ctx.blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, n, n, &mone, x, n, &one, q, n));
-    launch_symmetrize_lower(ctx, q, n);
-    const double qn = launch_frob(ctx, q, n);
-    if (qn < 1.0) {
-      launch_identity_axpy(ctx, t, q, n, 0.75);
-      QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &one, q, n, t, n, &zero, qt, n));
-      launch_identity_axpy(ctx, t, qt, n, 0.5);
-      QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &one, x, n, t, n, &zero, xp, n));
-      QBX_CUDA(cudaMemcpyAsync(x, xp, sizeof(double) * n * n, cudaMemcpyDeviceToDevice, ctx.stream));
-    } else {
-      // t = (x^T)^-1 via LU of x^T and a solve against the identity
-      QBX_BLAS(cublasDgeam(ctx.blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, &one, x, n, &zero, x, n, qt, n));
-      QBX_SOLVER(cusolverDnDgetrf(ctx.solver, n, n, qt, n, ctx.d_solver_work, ctx.d_ipiv, ctx.d_info));
-      launch_identity_axpy(ctx, t, t, n, 0.0);
-      QBX_SOLVER(cusolverDnDgetrs(ctx.solver, CUBLAS_OP_N, n, n, qt, n, ctx.d_ipiv, t, n, ctx.d_info));
-      launch_avg_transpose(ctx, x, t, n);
+  if (!ctx.capturing) {
+    ctx.polar_iters = 0;
+    for (int iter = 0; iter < maxiter; iter++) {
+      polar_q(ctx, x, q);
+      const double qn = std::sqrt(read_slot(ctx, SLOT_FROB));
+      if (qn < 1.0) polar_bjorck(ctx, x, q, t, qt, xp);
+      else polar_higham(ctx, x, t, qt);
+      ctx.polar_iters = iter + 1;
+      if (qn <= tol) break;
     }
-    if (qn <= tol) break;
+    return;
   }
+  // Captured: a WHILE node whose body forms q, decides on the device, and
+  // runs the chosen step in an IF/ELSE node.  The loop handle is reset to 1
+  // at every launch of the graph, so the body runs at least once.
+  int* iters = ctx.d_status + ST_POLAR_ITERS;
+  QBX_CUDA(cudaMemsetAsync(iters, 0, sizeof(int), ctx.stream));
+  cudaGraphConditionalHandle loop;
+  QBX_CUDA(cudaGraphConditionalHandleCreate(&loop, capture_graph(ctx.stream), 1,
+                                            cudaGraphCondAssignDefault));
+  cudaGraph_t body = add_conditional(ctx.stream, loop, cudaGraphCondTypeWhile, 1)[0];
+  capture_into(ctx, body, ctx.side[0], [&]() {
+    polar_q(ctx, x, q);
+    cudaGraphConditionalHandle branch;
+    QBX_CUDA(cudaGraphConditionalHandleCreate(&branch, capture_graph(ctx.stream), 0, 0));
+    k_polar_decide<<<1, 1, 0, ctx.stream>>>(ctx.d_scalars + SLOT_FROB, tol, maxiter, iters, loop,
+                                            branch);
+    QBX_LAUNCHED(ctx);
+    cudaGraph_t* arms = add_conditional(ctx.stream, branch, cudaGraphCondTypeIf, 2);
+    cudaGraph_t bjorck = arms[0], higham = arms[1];
+    capture_into(ctx, bjorck, ctx.side[1], [&]() { polar_bjorck(ctx, x, q, t, qt, xp); });
+    capture_into(ctx, higham, ctx.side[1], [&]() { polar_higham(ctx, x, t, qt); });
+  });
+}
+
+// DoubleMatrix::polar as an operation of its own: x (nst x nst, device) in
+// place, eagerly or captured into a graph (the form the captured step uses)
+// and launched once.  Returns the iterations run.
+int polar_entry(Context& ctx, double* x, double tol, int maxiter, bool graph) {
+  if (!graph) {
+    polar(ctx, x, tol, maxiter);
+    return ctx.polar_iters;
+  }
+  const bool prof = ctx.prof.on;
+  ctx.prof.on = false;
+  cudaGraph_t g = nullptr;
+  QBX_CUDA(cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeRelaxed));
+  ctx.capturing = true;
+  try {
+    polar(ctx, x, tol, maxiter);
+  } catch (...) {
+    cudaStreamEndCapture(ctx.stream, &g);
+    if (g) cudaGraphDestroy(g);
+    ctx.capturing = false;
+    ctx.prof.on = prof;
+    throw;
+  }
+  ctx.capturing = false;
+  ctx.prof.on = prof;
+  QBX_CUDA(cudaStreamEndCapture(ctx.stream, &g));
+  cudaGraphExec_t ex = nullptr;
+  const cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
+  cudaGraphDestroy(g);
+  QBX_CUDA(e);
+  const cudaError_t l = cudaGraphLaunch(ex, ctx.stream);
+  const cudaError_t w = cudaStreamSynchronize(ctx.stream);
+  cudaGraphExecDestroy(ex);
+  QBX_CUDA(l);
+  QBX_CUDA(w);
+  int iters = 0;
+  QBX_CUDA(cudaMemcpy(&iters, ctx.d_status + ST_POLAR_ITERS, sizeof(int), cudaMemcpyDeviceToHost));
+  return iters;
 }
 
 // out += alpha * c * M for the FP64 wavefunction block c (K x n) and an n x n
@@ -128,7 +296,7 @@ void ortho_align(Context& ctx) {
                              cudaMemcpyDeviceToDevice, ctx.stream));
   // in the mixed path slot 0 holds the split of C_last (made in energy())
   if (mx) split_bf16_2d(ctx, ctx.d_c, K, n, K, ctx.cs_hi[1], ctx.cs_lo[1], ctx.ldp);
-  overlap_cholesky(ctx, ctx.d_c, L, mx ? 1 : -1);
+  overlap_cholesky(ctx, ctx.d_c, L, ST_INFO_ORTHO, mx ? 1 : -1);
   // B = 2 C^T C_last - c0 c_last0^T
   {
     ProfScope ps(ctx, "gemm_overlap_last");
@@ -163,8 +331,7 @@ void ortho_align(Context& ctx) {
 void update_density(Context& ctx) {
   ProfScope ps(ctx, "update_density");
   launch_density(ctx, ctx.d_c, ctx.d_rhor);
-  const size_t N = ctx.N();
-  ctx.total_charge = dsum(ctx, ctx.d_rhor, N) * ctx.vb.omega / (double)N;
+  launch_sum(ctx, ctx.d_rhor, ctx.N(), SLOT_CHARGE);   // total charge
   vb_forward_real(ctx, ctx.d_rhor, ctx.vb.omega, ctx.d_rhog);
 }
 
@@ -178,7 +345,6 @@ void update_vhxc(Context& ctx) {
 // NonLocalPotential::energy (src/NonLocalPotential.cpp:1258-1640):
 // F = 2 A^T C - a0 c0^T, E_nl, and H C += A (D F / Omega)
 static void nonlocal(Context& ctx, bool hpsi) {
-  ctx.enl = 0.0;
   if (ctx.nproj == 0) return;
   const int n = ctx.nst, K = 2 * ctx.wb.ng, np = ctx.nproj;
   const double one = 1.0, two = 2.0, zero = 0.0;
@@ -193,7 +359,7 @@ static void nonlocal(Context& ctx, bool hpsi) {
                            ctx.d_c, K, &zero, ctx.d_fnl, np));
   }
   launch_rank1_fix(ctx, ctx.d_fnl, np, ctx.d_anl, K, ctx.d_c, K, np, n, -1.0, false);
-  ctx.enl = launch_enl(ctx);
+  launch_enl(ctx);
   if (hpsi) {
     ProfScope ps(ctx, "gemm_nl_apply");
     if (mx) {
@@ -221,27 +387,19 @@ void energy(Context& ctx, bool hpsi, bool forces) {
   if (mixed(ctx))
     split_bf16_2d(ctx, ctx.d_c, 2 * ctx.wb.ng, ctx.nst, 2 * ctx.wb.ng, ctx.cs_hi[0], ctx.cs_lo[0],
                   ctx.ldp);
-  ctx.ekin = launch_ekin(ctx);
+  launch_ekin(ctx);
   if (hpsi) {
     ProfScope pv(ctx, "vpsi");
     launch_vpsi(ctx, ctx.d_c, ctx.d_vr, ctx.d_hc);   // hc = 1/2 G^2 c + V psi
   }
   nonlocal(ctx, hpsi);
-  ctx.ecoul = ctx.ehart + ctx.esr - ctx.eself;
-  ctx.etotal = ctx.ekin + ctx.eps + ctx.enl + ctx.ecoul + ctx.exc;
+  // the energies are formed on the host from the slots (finish_energy)
   if (forces) {
     int natoms = 0;
     for (auto& t : ctx.tau) natoms += (int)t.size() / 3;
     QBX_CUDA(cudaMemsetAsync(ctx.d_fion, 0, sizeof(double) * 3 * natoms, ctx.stream));
     launch_local_forces(ctx, ctx.d_fion);
     if (ctx.nproj) launch_nl_forces(ctx, ctx.d_fion);
-    ctx.fion.assign(3 * natoms, 0.0);
-    QBX_CUDA(cudaMemcpyAsync(ctx.fion.data(), ctx.d_fion, sizeof(double) * 3 * natoms,
-                             cudaMemcpyDeviceToHost, ctx.stream));
-    QBX_CUDA(cudaStreamSynchronize(ctx.stream));
-    int a = 0;
-    for (size_t is = 0; is < ctx.tau.size(); is++)
-      for (size_t i = 0; i < ctx.tau[is].size(); i++) ctx.fion[a++] += ctx.fion_esr[is][i];
   }
 }
 
@@ -343,7 +501,7 @@ void jd_update(Context& ctx) {
 void free_mixed(Context& ctx) {
   void** bufs[] = {&ctx.d_acc32, &ctx.cs_hi[0], &ctx.cs_lo[0], &ctx.cs_hi[1], &ctx.cs_lo[1],
                    &ctx.hs_hi, &ctx.hs_lo, &ctx.as_hi, &ctx.as_lo, &ctx.ss_hi, &ctx.ss_lo,
-                   &ctx.d_tc_ws, &ctx.d_tc_err};
+                   &ctx.d_tc_ws};
   for (void** b : bufs)
     if (*b) { cudaFree(*b); *b = nullptr; }
   dfree(ctx.c32);

@@ -395,6 +395,9 @@ static void tc_gemm_tn(Context& ctx, int kind, int m, int n, int k, double alpha
   if (splits > 1) {
     const size_t need = (size_t)splits * m * n;
     if (need > ctx.tc_ws_elems) {
+      // a captured step replays fixed pointers: the workspace is sized by an
+      // eager run of the same step before its capture
+      QBX_REQUIRE(!ctx.capturing, 56, "split-K workspace growth while capturing a step");
       if (ctx.d_tc_ws) cudaFree(ctx.d_tc_ws);
       ctx.d_tc_ws = nullptr;
       ctx.tc_ws_elems = 0;
@@ -402,21 +405,18 @@ static void tc_gemm_tn(Context& ctx, int kind, int m, int n, int k, double alpha
       ctx.tc_ws_elems = need;
     }
   }
-  if (!ctx.d_tc_err) {
-    QBX_CUDA(cudaMalloc(&ctx.d_tc_err, sizeof(int)));
-    QBX_CUDA(cudaMemsetAsync(ctx.d_tc_err, 0, sizeof(int), ctx.stream));
-  }
+  int* err = ctx.d_status + ST_TC_ERR;   // wait-timeout flag, sticky
   float* ws = splits > 1 ? (float*)ctx.d_tc_ws : nullptr;
   QBX_REQUIRE(splits > 1 ? tn <= 65535 : tm <= 65535, 54, "too many tiles for the grid");
   dim3 grid = splits > 1 ? dim3(tm, tn, splits) : dim3(tn, tm, 1);
   if (kind == tc::KIND_BF16) {
     allow_smem(tc::k_tc_split_gemm<tc::KIND_BF16>, tc::SMEM_BYTES);
     tc::k_tc_split_gemm<tc::KIND_BF16><<<grid, tc::THREADS, tc::SMEM_BYTES, ctx.stream>>>(
-        mah, mal, mbh, mbl, m, n, nkb, kbps, ws, C, ldc, alpha, beta, (int*)ctx.d_tc_err);
+        mah, mal, mbh, mbl, m, n, nkb, kbps, ws, C, ldc, alpha, beta, err);
   } else {
     allow_smem(tc::k_tc_split_gemm<tc::KIND_TF32>, tc::SMEM_BYTES);
     tc::k_tc_split_gemm<tc::KIND_TF32><<<grid, tc::THREADS, tc::SMEM_BYTES, ctx.stream>>>(
-        mah, mal, mbh, mbl, m, n, nkb, kbps, ws, C, ldc, alpha, beta, (int*)ctx.d_tc_err);
+        mah, mal, mbh, mbl, m, n, nkb, kbps, ws, C, ldc, alpha, beta, err);
   }
   QBX_LAUNCHED(ctx);
   if (splits > 1) {
@@ -449,9 +449,10 @@ void tc_tf32_gemm_tn(Context& ctx, int m, int n, int k, double alpha, const floa
 }
 
 int tc_check_error(Context& ctx) {
-  if (!ctx.d_tc_err) return 0;
+  if (!ctx.d_status) return 0;
   int e = 0;
-  QBX_CUDA(cudaMemcpyAsync(&e, ctx.d_tc_err, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+  QBX_CUDA(cudaMemcpyAsync(&e, ctx.d_status + ST_TC_ERR, sizeof(int), cudaMemcpyDeviceToHost,
+                           ctx.stream));
   QBX_CUDA(cudaStreamSynchronize(ctx.stream));
   return e;
 }

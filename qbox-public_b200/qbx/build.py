@@ -32,7 +32,8 @@ def _newer(src, dst):
 
 def build(verbose: bool = False) -> str:
     os.makedirs(OBJDIR, exist_ok=True)
-    headers = glob.glob(os.path.join(CSRC, "*.h")) + [os.path.join(ROOT, "include", "qbx.h")]
+    headers = (glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh"))
+               + [os.path.join(ROOT, "include", "qbx.h")])
     hdr_time = max(os.path.getmtime(h) for h in headers)
     objs = []
     procs = []

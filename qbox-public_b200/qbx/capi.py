@@ -37,7 +37,7 @@ SYMBOLS = (
     "qbx_profile", "qbx_profile_get", "qbx_launch_count", "qbx_stream",
     "qbx_set_gemm_backend", "qbx_split_gemm_tn", "qbx_density_static",
     "qbx_stress", "qbx_get_stress", "qbx_autotune", "qbx_set_wf_dyn", "qbx_jd_update",
-    "qbx_scf_step_batch",
+    "qbx_scf_step_batch", "qbx_set_step_graph", "qbx_step_graph_info", "qbx_polar",
 )
 
 _lib = None
@@ -107,6 +107,10 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "qbx_scf_step_batch": (_I, [ctypes.POINTER(_P), _I, _I, _DP]),
         "qbx_jd_update": (_I, [_P]),
         "qbx_get_stress": (_I, [_P, _DP, _DP]),
+        "qbx_set_step_graph": (_I, [_P, _I]),
+        "qbx_polar": (_I, [_P, _DP, _D, _I, _I, ctypes.POINTER(_I)]),
+        "qbx_step_graph_info": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_long),
+                                     ctypes.c_char_p, _I]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -323,6 +327,30 @@ class Context:
     def jd_update(self):
         self._ok(self.lib.qbx_jd_update(self.h), "jd_update")
 
+    def polar(self, x: np.ndarray, tol: float = 1e-6, maxiter: int = 20,
+              graph: bool = False):
+        """qbx_polar: the polar factor of an nst x nst matrix; returns
+        (factor, iterations)."""
+        a = np.asfortranarray(np.array(x, dtype=float))
+        it = _I()
+        self._ok(self.lib.qbx_polar(self.h, _dp(a.reshape(-1, order="F")), tol, maxiter,
+                                    int(graph), ctypes.byref(it)), "polar")
+        return a, it.value
+
+    def set_step_graph(self, on: bool = True):
+        """qbx_set_step_graph: run scf_step as a captured CUDA graph (from
+        the second step of each configuration on)."""
+        self._ok(self.lib.qbx_set_step_graph(self.h, int(on)), "set_step_graph")
+
+    def step_graph_info(self):
+        """qbx_step_graph_info: (graphs captured, graph launches, note)."""
+        n = _I()
+        launches = ctypes.c_long()
+        buf = ctypes.create_string_buffer(512)
+        self._ok(self.lib.qbx_step_graph_info(self.h, ctypes.byref(n), ctypes.byref(launches),
+                                              buf, 512), "step_graph_info")
+        return n.value, launches.value, buf.value.decode()
+
     def autotune(self) -> str:
         """qbx_autotune: time the staged-FFT configurations on this context
         and keep the fastest; returns the report."""
@@ -367,14 +395,14 @@ class Context:
         self._ok(self.lib.qbx_get_coeffs_async(self.h, _dp(out_pinned)), "get_coeffs_async")
 
 
-def scf_step_batch(contexts, stress: bool = False):
+def scf_step_batch(contexts, stress: bool = False, forces: bool = False):
     """qbx_scf_step_batch: one electronic step of every context, run
     concurrently; returns a list of energy dicts."""
     lib = load()
     n = len(contexts)
     arr = (_P * n)(*[c.h for c in contexts])
     e = np.zeros(n * NENERGY)
-    rc = lib.qbx_scf_step_batch(arr, n, 2 if stress else 0, _dp(e))
+    rc = lib.qbx_scf_step_batch(arr, n, (2 if stress else 0) | (1 if forces else 0), _dp(e))
     if rc:
         msgs = [lib.qbx_last_error(c.h) for c in contexts]
         msg = next((m.decode() for m in msgs if m), "")
