@@ -11,7 +11,12 @@
 // (src/Basis.cpp:544-597) never leaks into the inputs.
 //
 // usage: ref_driver <system.txt> <nsteps> <outdir> [dump_steps=0]
-//                   [forces=0] [wf_dyn=PSDA]
+//                   [forces=0] [wf_dyn=PSDA] [nitscf dt]
+// wf_dyn = MD runs the reference's own BOSampleStepper::step(nsteps)
+// (src/BOSampleStepper.cpp:165-1428) with atoms_dyn = MD, wf_dyn = PSDA,
+// nitscf electronic steps per ionic step, nite = 0 and the time step dt
+// (a.u.), no thermostat; its printed output goes to md_log.txt, the final
+// positions to md_tau.txt and the final coefficients to final_c.bin.
 // forces = 1: ionic forces at the dumped steps and the last step; forces = 2:
 // forces and the stress tensor (EnergyFunctional::energy with
 // compute_stress, src/EnergyFunctional.cpp:397-1044), written as
@@ -40,6 +45,7 @@
 #include "Preconditioner.h"
 #include "PSDAWavefunctionStepper.h"
 #include "JDWavefunctionStepper.h"
+#include "BOSampleStepper.h"
 #include "FourierTransform.h"
 #include "Basis.h"
 #include "Timer.h"
@@ -88,6 +94,24 @@ int main(int argc, char** argv)
   s.ctrl.alpha_RSH = 0.0; s.ctrl.beta_RSH = 0.0; s.ctrl.mu_RSH = 0.0;
   s.ctrl.stress = "OFF";
   s.ctrl.wf_diag = "F";
+  // every other control field BOSampleStepper and its steppers read
+  s.ctrl.timing = "OFF";
+  s.ctrl.wf_dyn = "PSDA";
+  s.ctrl.atoms_dyn = "LOCKED";
+  s.ctrl.nite = 0;
+  s.ctrl.emass = 0.0;
+  s.ctrl.tcp = "OFF"; s.ctrl.tcp_rcut = 0.0; s.ctrl.tcp_sigma = 0.0;
+  s.ctrl.gms_mix = 0.0;
+  s.ctrl.thermostat = "OFF";
+  s.ctrl.th_temp = 0.0; s.ctrl.th_time = 0.0; s.ctrl.th_width = 0.0;
+  s.ctrl.lock_cm = false;
+  s.ctrl.cell_dyn = "LOCKED"; s.ctrl.cell_lock = "OFF"; s.ctrl.cell_mass = 0.0;
+  s.ctrl.spin = "OFF"; s.ctrl.delta_spin = 0;
+  s.ctrl.dt = 0.0; s.ctrl.iprint = 1; s.ctrl.timeout = 0;
+  s.ctrl.charge_mix_coeff = 0.5; s.ctrl.charge_mix_rcut = 10.0; s.ctrl.charge_mix_ndim = 0;
+  s.ctrl.blHF[0] = s.ctrl.blHF[1] = s.ctrl.blHF[2] = 1; s.ctrl.btHF = 0.0;
+  s.ctrl.scf_tol = 0.0; s.ctrl.force_tol = 0.0; s.ctrl.stress_tol = 0.0;
+  s.ctrl.iter_cmd = ""; s.ctrl.iter_cmd_period = 1;
 
   // ---- system file ----
   ifstream in(sysfile.c_str());
@@ -170,6 +194,38 @@ int main(int argc, char** argv)
       c[ig + (size_t)n*mloc] = complex<double>(cin[src], cin[src+1]);
     }
   s.wf.gram();
+
+  if ( wf_dyn == "MD" )
+  {
+    const int nitscf = argc > 7 ? atoi(argv[7]) : 1;
+    s.ctrl.atoms_dyn = "MD";
+    s.ctrl.dt = argc > 8 ? atof(argv[8]) : 20.0;
+    ofstream log((outdir + "/md_log.txt").c_str());
+    streambuf* saved = cout.rdbuf(log.rdbuf());
+    {
+      BOSampleStepper stepper(s, nitscf, 0);
+      stepper.step(nsteps);
+    }
+    cout.rdbuf(saved);
+    vector<vector<double> > tau;
+    s.atoms.get_positions(tau);
+    ofstream to((outdir + "/md_tau.txt").c_str());
+    to << setprecision(17);
+    for ( size_t is = 0; is < tau.size(); is++ )
+      for ( size_t i = 0; i < tau[is].size(); i++ ) to << tau[is][i] << "\n";
+    vector<double> out(2*(size_t)ngw*nst);
+    for ( int n = 0; n < nst; n++ )
+      for ( int ig = 0; ig < ngw; ig++ )
+      {
+        const complex<double> v = c[ig + (size_t)n*mloc];
+        const size_t dst = 2*((size_t)n*ngw + perm[ig]);
+        out[dst] = v.real(); out[dst+1] = v.imag();
+      }
+    write_bin(outdir + "/final_c.bin", &out[0], out.size()*sizeof(double));
+    ofstream meta((outdir + "/meta.txt").c_str());
+    meta << "ngw " << ngw << "\nnst " << nst << "\nnatoms " << atom_count << "\n";
+    return 0;
+  }
 
   // ---- set up the energy functional and the stepper ----
   ChargeDensity cd(s.wf);
