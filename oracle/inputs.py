@@ -93,6 +93,39 @@ def run_reference(sysdef, workdir: str, nsteps: int, dump_steps: int = 0,
     return load_outputs(workdir)
 
 
+def run_reference_md(sysdef, workdir: str, niter: int, nitscf: int, dt: float,
+                     threads: Optional[int] = None) -> Dict:
+    """The reference's BOSampleStepper::step(niter) with atoms_dyn = MD and
+    nitscf PSDA electronic steps per ionic step.  Returns the per-ionic-step
+    energies it prints (etotal, econst, ekin_ion; 8 decimals), the final
+    positions and velocities (natoms x 3) and coefficients (full precision)."""
+    import re
+    if not os.path.exists(REF_DRIVER):
+        raise FileNotFoundError("oracle/_ref/ref_driver not built (make -C oracle)")
+    path = write_system(sysdef, workdir)
+    env = dict(os.environ)
+    if threads:
+        env["OMP_NUM_THREADS"] = str(threads)
+        env["OPENBLAS_NUM_THREADS"] = str(threads)
+    subprocess.run([REF_DRIVER, path, str(niter), workdir, "0", "0", "MD", str(nitscf),
+                    repr(float(dt))], check=True, env=env, stdout=subprocess.DEVNULL)
+    log = open(os.path.join(workdir, "md_log.txt")).read()
+
+    def tag(name):
+        return np.array([float(x) for x in re.findall(rf"<{name}>\s*(\S+)\s*</{name}>", log)])
+    meta = {}
+    with open(os.path.join(workdir, "meta.txt")) as fm:
+        for line in fm:
+            k, v = line.split()
+            meta[k] = int(v)
+    a = np.fromfile(os.path.join(workdir, "final_c.bin")).reshape(meta["nst"], meta["ngw"], 2)
+    return dict(etotal=tag("etotal"), econst=tag("econst"), ekin_ion=tag("ekin_ion"),
+                etotal_int=tag("etotal_int"),
+                tau=np.loadtxt(os.path.join(workdir, "md_tau.txt")).reshape(-1, 3),
+                vel=np.loadtxt(os.path.join(workdir, "md_vel.txt")).reshape(-1, 3),
+                final_c=a[..., 0] + 1j * a[..., 1])
+
+
 def load_outputs(workdir: str) -> Dict:
     out: Dict = {}
     meta = {}

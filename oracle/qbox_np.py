@@ -603,6 +603,29 @@ class ElectronicStep:
         x = np.linalg.solve(L.T, x)                 # L^-T Q
         self.c = x.T @ ctmp                         # C <- C_tmp X
 
+    def lowdin(self):
+        """src/SlaterDet.cpp:674-721: S = L L^T, U the orthogonal polar
+        factor of L^T, C <- C L^-T U."""
+        self.cleanup()
+        L = np.linalg.cholesky(self.real_dot(self.c, self.c))
+        u = polar(L.T.copy(), 1.e-6, 20)
+        t = np.linalg.solve(L.T, u)                 # L^-T U
+        self.c = t.T @ self.c
+
+    def align(self, cv):
+        """src/SlaterDet.cpp:979-1044, cv.align(self): cv <- cv X with X the
+        orthogonal polar factor of B = cv^T C (x2, G=0 fix).  Returns the
+        aligned cv."""
+        x = polar(self.real_dot(cv, self.c), 1.e-6, 20)
+        return x.T @ cv
+
+    def set_positions(self, positions):
+        """AtomSet::set_positions followed by EnergyFunctional::atoms_moved
+        (src/EnergyFunctional.cpp:1047-1197): structure factors, local
+        potential and pseudocharge sums, E_sr and the projector phases."""
+        self.positions = [np.array(p, float) for p in positions]
+        self._setup_tables()
+
     # ---- density (src/SlaterDet.cpp:225-298, src/ChargeDensity.cpp:136-198)
     def update_density(self):
         rho = np.zeros(self.N)
@@ -900,6 +923,73 @@ class ElectronicStep:
         else:
             self.psda_update()
         return out
+
+
+AMU = 1822.89      # atomic mass unit in electron masses, src/IonicStepper.cpp:40
+
+
+def md_run(es: "ElectronicStep", niter: int, nitscf: int, dt: float, masses):
+    """BOSampleStepper::step(niter) with atoms_dyn = MD, wf_dyn = PSDA,
+    nite = 0, no thermostat and the default (linear) wavefunction
+    extrapolation (src/BOSampleStepper.cpp:412-1420), with
+    MDIonicStepper::compute_r / compute_v (src/MDIonicStepper.cpp:8-30,
+    37-253).  masses: per species, in atomic mass units.
+
+    Returns {"ionic": [per ionic step: etotal, ekin_ion, econst, fion],
+    "scf": [per electronic step: the step() energies], "positions",
+    "velocities", "c", "cv"}."""
+    pm = [m * AMU for m in masses]
+    nsp = len(es.positions)
+    r0 = [p.copy() for p in es.positions]
+    v0 = [np.zeros_like(p) for p in r0]
+    rm = None
+    cv = np.zeros_like(es.c)
+    ionic, scf = [], []
+
+    def compute_v(f):
+        return [(r0[i] - rm[i]) / dt + dt / (2.0 * pm[i]) * f[i] for i in range(nsp)]
+
+    def ekin_of(v):
+        return sum(0.5 * pm[i] * (v[i] ** 2).sum() for i in range(nsp))
+
+    for it in range(niter):
+        # energy and forces at r0 with the current wavefunctions (:427-440)
+        es.update_density()
+        es.update_vhxc()
+        es.energy(False, forces=True)
+        f = [x.copy() for x in es.fion]
+        if it > 0:
+            v0 = compute_v(f)                        # (:466-469)
+        ek = ekin_of(v0)
+        ionic.append(dict(etotal=es.etotal, ekin_ion=ek, econst=es.etotal + ek,
+                          fion=np.concatenate(f)))
+        # r0 <- r0 + v0 dt + dt^2/(2m) f (:572), then atoms_moved
+        rp = [r0[i] + v0[i] * dt + dt * dt / (2.0 * pm[i]) * f[i] for i in range(nsp)]
+        rm, r0 = r0, rp
+        es.set_positions(r0)
+        # wavefunction extrapolation (:593-780, normal extrapolation)
+        x = es.c.copy()
+        if it == 0:
+            es.c = x + dt * cv
+            cv = x
+            es.gram()
+        else:
+            cv = es.align(cv)
+            es.c = 2.0 * x - cv
+            cv = x
+            es.lowdin()
+        es.extrapolate = False                       # wf_stepper->preprocess()
+        for _ in range(nitscf):
+            scf.append(es.step())
+    # wavefunction velocity and the forces at the last positions (:1351-1420)
+    cv = es.align(cv)
+    cv = (es.c - cv) / dt
+    es.gram()
+    es.update_density()
+    es.update_vhxc()
+    es.energy(False, forces=True)
+    v0 = compute_v([x.copy() for x in es.fion])
+    return dict(ionic=ionic, scf=scf, positions=r0, velocities=v0, c=es.c.copy(), cv=cv)
 
 
 def polar(x, tol, maxiter):

@@ -16,7 +16,8 @@
 // (src/BOSampleStepper.cpp:165-1428) with atoms_dyn = MD, wf_dyn = PSDA,
 // nitscf electronic steps per ionic step, nite = 0 and the time step dt
 // (a.u.), no thermostat; its printed output goes to md_log.txt, the final
-// positions to md_tau.txt and the final coefficients to final_c.bin.
+// positions and velocities to md_tau.txt and md_vel.txt and the final
+// coefficients to final_c.bin.
 // forces = 1: ionic forces at the dumped steps and the last step; forces = 2:
 // forces and the stress tensor (EnergyFunctional::energy with
 // compute_stress, src/EnergyFunctional.cpp:397-1044), written as
@@ -213,6 +214,13 @@ int main(int argc, char** argv)
     to << setprecision(17);
     for ( size_t is = 0; is < tau.size(); is++ )
       for ( size_t i = 0; i < tau[is].size(); i++ ) to << tau[is][i] << "\n";
+    // MDIonicStepper::compute_v stores the velocities in the AtomSet
+    vector<vector<double> > vel;
+    s.atoms.get_velocities(vel);
+    ofstream vo((outdir + "/md_vel.txt").c_str());
+    vo << setprecision(17);
+    for ( size_t is = 0; is < vel.size(); is++ )
+      for ( size_t i = 0; i < vel[is].size(); i++ ) vo << vel[is][i] << "\n";
     vector<double> out(2*(size_t)ngw*nst);
     for ( int n = 0; n < nst; n++ )
       for ( int ig = 0; ig < ngw; ig++ )

@@ -9,6 +9,8 @@ basis size, a fixed sample of the density and local potential on the grid,
 H*psi and wavefunction coefficients of a few bands (all G for small bases,
 a fixed sample of G otherwise), and per-band norms.
 The fixtures pin the numpy oracle (oracle/qbox_np.py) in tests/test_oracle.py.
+ref_<name>_jd.npz holds a JD-stepper run and ref_<name>_md.npz a molecular
+dynamics run of the reference's BOSampleStepper.
 """
 from __future__ import annotations
 
@@ -84,12 +86,34 @@ def make_jd(name: str, nsteps: int, workdir: str) -> str:
 
 JD_CASES = {"si8": 6}
 
+# MD: (ionic steps, electronic steps per ionic step, dt in a.u.)
+MD_CASES = {"si8": (3, 2, 20.0)}
+
+
+def make_md(name: str, workdir: str) -> str:
+    """Molecular dynamics (atoms_dyn MD) through the reference's own
+    BOSampleStepper: the printed energies of each ionic step, the final
+    positions and velocities, and the final coefficients of a few bands."""
+    niter, nitscf, dt = MD_CASES[name]
+    s = systems.get(name)
+    out = inputs.run_reference_md(s, workdir, niter, nitscf, dt, threads=os.cpu_count())
+    fx = dict(niter=niter, nitscf=nitscf, dt=dt, etotal=out["etotal"], econst=out["econst"],
+              ekin_ion=out["ekin_ion"], tau=out["tau"], vel=out["vel"],
+              final_c_bands=out["final_c"][:NBANDS_FULL],
+              final_c_norm2=(np.abs(out["final_c"]) ** 2).sum(1))
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), f"ref_{name}_md.npz")
+    np.savez_compressed(path, **fx)
+    return path
+
 if __name__ == "__main__":
     import tempfile
-    names = sys.argv[1:] or list(CASES) + [n + "_jd" for n in JD_CASES]
+    names = sys.argv[1:] or (list(CASES) + [n + "_jd" for n in JD_CASES]
+                             + [n + "_md" for n in MD_CASES])
     for n in names:
         with tempfile.TemporaryDirectory() as td:
-            if n.endswith("_jd"):
+            if n.endswith("_md"):
+                print(make_md(n[:-3], td))
+            elif n.endswith("_jd"):
                 print(make_jd(n[:-3], JD_CASES[n[:-3]], td))
             else:
                 print(make(n, CASES[n], td))

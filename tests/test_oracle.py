@@ -166,3 +166,27 @@ def test_oracle_jd_matches_reference():
         r = es.step(wf_dyn="JD")
         assert abs(r["eigenvalue_sum"] - g["e_eigenvalue_sum"][it]) < 1e-9
         assert abs(es.etotal - g["e_etotal"][it]) < 1e-9
+
+
+def test_oracle_md_matches_reference():
+    """qbox_np.md_run (BOSampleStepper::step with atoms_dyn MD, PSDA, linear
+    wavefunction extrapolation, velocity Verlet) against the reference's own
+    stepper: printed energies to their 8 decimals, final positions and
+    velocities and final coefficients to rounding."""
+    fx = golden("si8_md")
+    s = systems.si8()
+    es = qbox_np.ElectronicStep(s)
+    out = qbox_np.md_run(es, int(fx["niter"]), int(fx["nitscf"]), float(fx["dt"]),
+                         [sp.mass for sp in s.species])
+    et = np.array([d["etotal"] for d in out["ionic"]])
+    ec = np.array([d["econst"] for d in out["ionic"]])
+    ek = np.array([d["ekin_ion"] for d in out["ionic"]])
+    np.testing.assert_allclose(et, fx["etotal"], rtol=0, atol=6e-9)
+    np.testing.assert_allclose(ec, fx["econst"], rtol=0, atol=6e-9)
+    np.testing.assert_allclose(ek, fx["ekin_ion"], rtol=0, atol=6e-9)
+    np.testing.assert_allclose(np.concatenate(out["positions"]), fx["tau"], rtol=0, atol=1e-12)
+    np.testing.assert_allclose(np.concatenate(out["velocities"]), fx["vel"], rtol=0, atol=1e-14)
+    c = out["c"]
+    np.testing.assert_allclose(c[:fx["final_c_bands"].shape[0]], fx["final_c_bands"], rtol=0,
+                               atol=1e-11)
+    np.testing.assert_allclose((np.abs(c) ** 2).sum(1), fx["final_c_norm2"], rtol=1e-11)
