@@ -142,6 +142,32 @@ int qbx_scf_step(qbx_context* ctx, int compute_forces, double* energies,
 int qbx_scf_step_batch(qbx_context** ctxs, int n, int compute_forces,
                        double* energies);
 
+/* AtomSet::set_positions followed by EnergyFunctional::atoms_moved
+ * (src/EnergyFunctional.cpp:1047-1197): the same atoms at new positions
+ * tau (species-major, 3 per atom, bohr).  Structure factors, local
+ * potential, pseudocharges, projector phases and E_sr are updated in place,
+ * so captured steps (qbx_set_step_graph) stay valid. */
+int qbx_move_atoms(qbx_context* ctx, const double* tau);
+
+/* BOSampleStepper::step(niter) with atoms_dyn = MD
+ * (src/BOSampleStepper.cpp:412-1420): per ionic step the energy and forces
+ * at the current positions, MDIonicStepper's velocity Verlet
+ * (src/MDIonicStepper.cpp:8-273, no thermostat), qbx_move_atoms, the linear
+ * wavefunction extrapolation (first step c + dt v then gram; later steps
+ * 2c - c_prev after SlaterDet::align, then SlaterDet::lowdin) and nitscf
+ * electronic steps (qbx_scf_step, PSDA); at the end the wavefunction
+ * velocity and the forces at the last positions.  The wavefunction
+ * velocity persists in the context across calls (the reference's
+ * Sample::wfv).  mass_amu: per species (atomic mass units).  vel (may be
+ * NULL): initial velocities in, final out (3 per atom, species-major).
+ * tau_out (may be NULL): final positions.  ionic (may be NULL): niter x 3
+ * values (etotal, ekin_ion, econst = etotal + ekin_ion) of each ionic step.
+ * scf (may be NULL): niter * nitscf * QBX_NENERGY energies of the
+ * electronic steps. */
+int qbx_md_run(qbx_context* ctx, int niter, int nitscf, double dt,
+               const double* mass_amu, double* vel, double* tau_out,
+               double* ionic, double* scf);
+
 /* DoubleMatrix::polar (src/Matrix.cpp:2446-2540), the orthogonal polar
  * factor used by SlaterDet::ortho_align: x (nst x nst, column-major, host)
  * is replaced by its polar factor.  Bjorck-Bowie steps while

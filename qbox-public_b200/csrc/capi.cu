@@ -21,17 +21,6 @@ struct qbx_context {
   int* d_perm = nullptr;
 };
 
-namespace qbx {
-void gram(Context& ctx);
-void ortho_align(Context& ctx);
-void update_density(Context& ctx);
-void update_vhxc(Context& ctx);
-void energy(Context& ctx, bool hpsi, bool forces);
-void psda_update(Context& ctx);
-void jd_update(Context& ctx);
-int polar_entry(Context& ctx, double* x, double tol, int maxiter, bool graph);
-}
-
 using namespace qbx;
 
 namespace {
@@ -75,7 +64,7 @@ void free_cell(Context& c) {
                      &c.d_exc, &c.d_vx2, &c.d_grad, &c.d_rhog, &c.d_vion, &c.d_rhops,
                      &c.d_vtmp_g, &c.d_vtmp_g2, &c.d_nn, &c.d_nn2, &c.d_nn3, &c.d_nn4,
                      &c.d_solver_work, &c.d_red, &c.d_scalars, &c.d_prec, &c.d_jd_h,
-                     &c.d_jd_w, &c.d_jd_work};
+                     &c.d_jd_w, &c.d_jd_work, &c.d_wfv};
   for (double** b : bufs) dfree(*b);
   dfree(c.d_ipiv);
   dfree(c.d_info);
@@ -728,17 +717,44 @@ int qbx_psda_reset(qbx_context* h) {
 }
 
 
+}  // extern "C"
+
+namespace qbx {
+void scf_step_any(Context& c, bool want_f, bool want_s, double* energies, double* fion) {
+  if (StepGraph* g = step_graph_for(c, want_f, want_s)) {
+    launch_step_graph(c, *g);
+    QBX_CUDA(cudaStreamSynchronize(c.stream));
+    finish_graph_step(c, want_f, energies, fion);
+    return;
+  }
+  step_eager(c, want_f, want_s, energies, fion);
+}
+}  // namespace qbx
+
+extern "C" {
 int qbx_scf_step(qbx_context* h, int forces, double* energies, double* fion) {
   return guarded(h, [&](Context& c) {
     check_ready(c, true);
-    const bool want_f = (forces & 1) != 0, want_s = (forces & 2) != 0;
-    if (StepGraph* g = step_graph_for(c, want_f, want_s)) {
-      launch_step_graph(c, *g);
-      QBX_CUDA(cudaStreamSynchronize(c.stream));
-      finish_graph_step(c, want_f, energies, fion);
-      return;
-    }
-    step_eager(c, want_f, want_s, energies, fion);
+    scf_step_any(c, (forces & 1) != 0, (forces & 2) != 0, energies, fion);
+  });
+}
+
+int qbx_move_atoms(qbx_context* h, const double* tau) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, true);
+    QBX_REQUIRE(tau, 1, "null positions");
+    move_atoms(c, tau);
+  });
+}
+
+int qbx_md_run(qbx_context* h, int niter, int nitscf, double dt, const double* mass_amu,
+               double* vel, double* tau_out, double* ionic, double* scf) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, true);
+    QBX_REQUIRE(niter > 0 && nitscf >= 0 && dt != 0.0 && mass_amu, 1, "bad MD arguments");
+    for (size_t is = 0; is < c.species.size(); is++)
+      QBX_REQUIRE(mass_amu[is] > 0.0, 1, "species mass must be positive");
+    md_run(c, niter, nitscf, dt, mass_amu, vel, tau_out, ionic, scf);
   });
 }
 

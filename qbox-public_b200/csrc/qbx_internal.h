@@ -402,6 +402,7 @@ struct Context {
   std::string graph_note;        // why the last capture was abandoned, if it was
   long graph_launches = 0;       // captured steps launched so far
   int polar_iters = 0;           // iterations of the last eager polar
+  double* d_wfv = nullptr;       // wavefunction velocity of the MD extrapolation
 
   size_t N() const { return (size_t)vb.n0 * vb.n1 * vb.n2; }
 };
@@ -521,6 +522,23 @@ void check_status(Context& ctx);
 // binds cuBLAS (with the context's workspace) and cuSOLVER to stream s
 void bind_stream(Context& ctx, cudaStream_t s);
 
+// ------------------------------------------------ the step and its callers
+void gram(Context& ctx);
+void ortho_align(Context& ctx);
+void update_density(Context& ctx);
+void update_vhxc(Context& ctx);
+void energy(Context& ctx, bool hpsi, bool forces);
+void psda_update(Context& ctx);
+void jd_update(Context& ctx);
+void polar_factor(Context& ctx, double* x, double tol, int maxiter);
+int polar_entry(Context& ctx, double* x, double tol, int maxiter, bool graph);
+// one electronic step (captured graph or eager), energies/fion as qbx_scf_step
+void scf_step_any(Context& c, bool want_f, bool want_s, double* energies, double* fion);
+// molecular dynamics (md.cu)
+void move_atoms(Context& c, const double* tau);
+void md_run(Context& c, int niter, int nitscf, double dt, const double* mass_amu, double* vel,
+            double* tau_out, double* ionic, double* scf);
+
 // split-precision products (split_gemm.cu, tc_gemm.cu)
 void split_bf16(Context& ctx, const double* x, size_t n, void* hi, void* lo);
 void overlap_diag_f64(Context& ctx, const double* c, int K, int n, double* S);
@@ -560,6 +578,7 @@ void tc_tf32_gemm_tn(Context& ctx, int m, int n, int k, double alpha, const floa
                      const float* alo, int lda, const float* bhi, const float* blo, int ldb,
                      double beta, double* C, int ldc);
 void alloc_mixed(Context& ctx);
+void split_projectors(Context& ctx);   // after the projectors change (mixed)
 void free_mixed(Context& ctx);
 
 }  // namespace qbx

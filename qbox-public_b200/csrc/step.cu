@@ -223,6 +223,10 @@ static void polar(Context& ctx, double* x, double tol, int maxiter) {
   });
 }
 
+// The orthogonal polar factor of x (nst x nst, device) in place, eagerly or
+// inside a capture (the form ortho_align uses).
+void polar_factor(Context& ctx, double* x, double tol, int maxiter) { polar(ctx, x, tol, maxiter); }
+
 // DoubleMatrix::polar as an operation of its own: x (nst x nst, device) in
 // place, eagerly or captured into a graph (the form the captured step uses)
 // and launched once.  Returns the iterations run.
@@ -555,14 +559,21 @@ void alloc_mixed(Context& ctx) {
     ctx.a32lo = dalloc<float>((size_t)ctx.ldp * np);
     QBX_CUDA(cudaMalloc(&ctx.at_hi, tall_bytes(np, K)));
     QBX_CUDA(cudaMalloc(&ctx.at_lo, tall_bytes(np, K)));
-    if (ctx.d_anl) {
-      split_bf16_2d(ctx, ctx.d_anl, (int)K, (int)np, (int)K, ctx.as_hi, ctx.as_lo, ctx.ldp);
-      split_tf32(ctx, ctx.d_anl, (int)K, (int)np, (int)K, ctx.a32, ctx.a32lo, ctx.ldp);
-      split_t(ctx, ctx.tall_kind_hc, ctx.d_anl, (int)K, (int)np, (int)K, ctx.at_hi, ctx.at_lo,
-              Context::tall_ld_of(ctx.tall_kind_hc, (int)np));
-    }
+    split_projectors(ctx);
   }
   QBX_CUDA(cudaStreamSynchronize(ctx.stream));
+}
+
+// The split copies of the projectors A_nl (BF16 hi/lo for F = 2 A^T C,
+// TF32 hi/lo for the cuBLAS fallback, the transposed split of the H*C
+// update), rebuilt in place whenever the projectors change.
+void split_projectors(Context& ctx) {
+  if (ctx.precision != MIXED || !ctx.d_anl || !ctx.nproj) return;
+  const int K = 2 * ctx.wb.ng, np = ctx.nproj;
+  split_bf16_2d(ctx, ctx.d_anl, K, np, K, ctx.as_hi, ctx.as_lo, ctx.ldp);
+  split_tf32(ctx, ctx.d_anl, K, np, K, ctx.a32, ctx.a32lo, ctx.ldp);
+  split_t(ctx, ctx.tall_kind_hc, ctx.d_anl, K, np, K, ctx.at_hi, ctx.at_lo,
+          Context::tall_ld_of(ctx.tall_kind_hc, np));
 }
 
 }  // namespace qbx

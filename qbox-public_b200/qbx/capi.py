@@ -38,6 +38,7 @@ SYMBOLS = (
     "qbx_set_gemm_backend", "qbx_split_gemm_tn", "qbx_density_static",
     "qbx_stress", "qbx_get_stress", "qbx_autotune", "qbx_set_wf_dyn", "qbx_jd_update",
     "qbx_scf_step_batch", "qbx_set_step_graph", "qbx_step_graph_info", "qbx_polar",
+    "qbx_move_atoms", "qbx_md_run",
 )
 
 _lib = None
@@ -108,6 +109,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "qbx_jd_update": (_I, [_P]),
         "qbx_get_stress": (_I, [_P, _DP, _DP]),
         "qbx_set_step_graph": (_I, [_P, _I]),
+        "qbx_move_atoms": (_I, [_P, _DP]),
+        "qbx_md_run": (_I, [_P, _I, _I, _D, _DP, _DP, _DP, _DP, _DP]),
         "qbx_polar": (_I, [_P, _DP, _D, _I, _I, ctypes.POINTER(_I)]),
         "qbx_step_graph_info": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_long),
                                      ctypes.c_char_p, _I]),
@@ -336,6 +339,29 @@ class Context:
         self._ok(self.lib.qbx_polar(self.h, _dp(a.reshape(-1, order="F")), tol, maxiter,
                                     int(graph), ctypes.byref(it)), "polar")
         return a, it.value
+
+    def move_atoms(self, tau: np.ndarray):
+        """qbx_move_atoms: the same atoms at new positions (species-major)."""
+        t = np.ascontiguousarray(np.asarray(tau, float).reshape(-1))
+        self._ok(self.lib.qbx_move_atoms(self.h, _dp(t)), "move_atoms")
+
+    def md_run(self, niter: int, nitscf: int, dt: float, masses, vel=None):
+        """qbx_md_run: niter ionic steps of velocity Verlet MD with nitscf
+        electronic steps each.  Returns {"ionic": (niter, 3) etotal,
+        ekin_ion, econst; "scf": list of energy dicts; "positions",
+        "velocities": (natoms, 3)}."""
+        m = np.ascontiguousarray(np.asarray(masses, float))
+        v = np.zeros(3 * self.natoms) if vel is None else \
+            np.ascontiguousarray(np.asarray(vel, float).reshape(-1)).copy()
+        tau = np.zeros(3 * self.natoms)
+        ionic = np.zeros(3 * niter)
+        scf = np.zeros(max(1, niter * nitscf) * NENERGY)
+        self._ok(self.lib.qbx_md_run(self.h, niter, nitscf, dt, _dp(m), _dp(v), _dp(tau),
+                                     _dp(ionic), _dp(scf)), "md_run")
+        return {"ionic": ionic.reshape(niter, 3),
+                "scf": [dict(zip(ENERGY_NAMES, scf[i * NENERGY:(i + 1) * NENERGY]))
+                        for i in range(niter * nitscf)],
+                "positions": tau.reshape(-1, 3), "velocities": v.reshape(-1, 3)}
 
     def set_step_graph(self, on: bool = True):
         """qbx_set_step_graph: run scf_step as a captured CUDA graph (from
