@@ -303,6 +303,35 @@ def run_ours(args):
     pin_in.numpy()[:] = cur.view(np.float64).ravel()
     ne2e = max(2, min(args.steps, 5))
     ms_e2e, _, _ = timed(mix, ne2e, e2e_bufs=(pin_in.numpy(), pin_out.numpy()))
+
+    # ---- molecular dynamics of the same cell (dt = 20 a.u., forces every
+    # ionic step, captured electronic steps): ms per ionic step
+    md = None
+    if args.md_steps > 0:
+        masses = [sp.mass for sp in s.species]
+        mix.md_run(1, args.md_nitscf, 20.0, masses)           # warm-up (captures)
+        stream = torch.cuda.ExternalStream(mix.stream(), device=dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        out_md = mix.md_run(args.md_steps, args.md_nitscf, 20.0, masses)
+        e1.record(stream)
+        e1.synchronize()
+        md = {"ionic_steps": args.md_steps, "scf_steps_per_ionic_step": args.md_nitscf,
+              "dt_au": 20.0, "ms_per_ionic_step": e0.elapsed_time(e1) / args.md_steps,
+              "econst": [float(x) for x in out_md["ionic"][:, 2]],
+              "profile_ms_one_ionic_step": None,
+              "what": ("per ionic step: density, potential, energy and forces; velocity "
+                       "Verlet; atoms_moved; linear wavefunction extrapolation (align, "
+                       "lowdin, FP64); scf_steps_per_ionic_step captured electronic steps")}
+        # where one (eager, profiled) ionic step goes
+        mix.profile(True)
+        mix.md_run(1, args.md_nitscf, 20.0, masses)
+        md["profile_ms_one_ionic_step"] = {
+            k: mix.profile_get(k)[0] for k in ("md_forces", "md_move_atoms", "md_extrapolate",
+                                               "update_density", "energy", "psda_update")}
+        mix.profile(False)
     mix.close()
 
     ms_mix = max_over_ranks(ms_mix)
@@ -329,6 +358,7 @@ def run_ours(args):
             "fp64_ms_per_step": ms_f64,
             "step_graph": {"captured": graphs, "launches": graph_launches, "note": graph_note,
                            "eager_ms_per_step": ms_mix_eager},
+            "md": md,
             "mixed_vs_fp64_speedup": ms_f64 / ms_mix,
             "dE_per_atom": de_atom,
             "dE_definition": ("|E_mixed - E_fp64| / atoms for one electronic step of both paths "
@@ -385,6 +415,10 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--md-steps", type=int, default=2,
+                    help="ionic steps of the molecular-dynamics measurement (0: skip)")
+    ap.add_argument("--md-nitscf", type=int, default=1,
+                    help="electronic steps per ionic step in the MD measurement")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--profile-bands", type=int, default=0,
                     help="run only warm-up + one mixed step of si512 with this many bands "

@@ -130,9 +130,12 @@ int qbx_scf_step(qbx_context* ctx, int compute_forces, double* energies,
 /* No counterpart in the reference (one Qbox process runs one sample).  One
  * electronic step of each of n independent contexts (different cells,
  * cutoffs and band counts allowed), run concurrently.  When every context
- * has its step captured as a graph (qbx_set_step_graph), one host thread
- * launches all the graphs, each on its context's stream, and then collects
- * the energies; otherwise each context is driven by its own host thread.
+ * has its step captured as a graph (qbx_set_step_graph), one thread
+ * launches every context's graph on that context's stream and then collects
+ * the energies (with the environment variable QBX_BATCH_GRAPH=1 at
+ * qbx_create of ctxs[0]: the steps are captured together as the branches of
+ * one graph cached on ctxs[0], one launch per batch step); otherwise each
+ * context is driven by its own host thread.
  * Either way the GPU overlaps the systems.  energies receives
  * n * QBX_NENERGY values (may be NULL); forces are not returned
  * (compute_forces bit 0 only selects the forces variant of the step, bit 1
@@ -187,15 +190,17 @@ int qbx_polar(qbx_context* ctx, double* x, double tol, int maxiter, int graph,
  * the graph.  Inside, the reductions stay in device slots, the Anderson
  * theta is formed on the device and the polar iteration of ortho_align is a
  * conditional WHILE node; the host reads the scalars once after the graph.
- * Changing the cell, atoms, precision, GEMM backend, stepper or FFT tuning
- * drops the graphs.  A step that cannot be captured turns graphs off and
+ * Changing the cell, precision, GEMM backend, stepper or FFT tuning, or
+ * qbx_set_atoms, drops the graphs (qbx_move_atoms keeps them).  A step that cannot be captured turns graphs off and
  * runs eagerly; qbx_step_graph_info then reports why. */
 int qbx_set_step_graph(qbx_context* ctx, int on);
-/* captured: graphs currently instantiated (0-4); launches: graph launches
- * so far; note (may be NULL): why capture was abandoned, empty if it was
- * not. */
+/* captured: graphs currently instantiated (0-4); launches: this context's
+ * captured steps launched so far (alone or inside a batch graph);
+ * batch_launches: batch graphs launched with this context first in the
+ * list; note (may be NULL): why capture (or the batch graph) was abandoned,
+ * empty if it was not. */
 int qbx_step_graph_info(qbx_context* ctx, int* captured, long* launches,
-                        char* note, int note_len);
+                        long* batch_launches, char* note, int note_len);
 
 /* The stress tensor of EnergyFunctional::energy(..., compute_stress=true,
  * sigma) (src/EnergyFunctional.cpp:440-1044, XCPotential::compute_stress

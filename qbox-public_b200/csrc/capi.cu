@@ -10,6 +10,7 @@
 #include <new>
 #include <stdexcept>
 #include <thread>
+#include <atomic>
 #include <tuple>
 
 #include "../../include/qbx.h"
@@ -47,11 +48,17 @@ int guarded(qbx_context* h, F f) {
 
 // Captured steps hold the buffer pointers and launch shapes of the moment of
 // capture; anything that changes those drops them.
+void drop_batch(Context& c) {
+  if (c.batch.exec) cudaGraphExecDestroy(c.batch.exec);
+  c.batch = BatchGraph{};
+}
+
 void drop_graphs(Context& c) {
   for (auto& g : c.graphs) {
     if (g.exec) cudaGraphExecDestroy(g.exec);
     g = StepGraph{};
   }
+  drop_batch(c);
 }
 
 void free_cell(Context& c) {
@@ -80,7 +87,7 @@ void free_atoms(Context& c) {
   if (c.h_fion) { cudaFreeHost(c.h_fion); c.h_fion = nullptr; }
   double** bufs[] = {&c.d_anl, &c.d_fnl, &c.d_dfnl, &c.d_pdfac, &c.d_sfac, &c.d_vps,
                      &c.d_rhops_sp, &c.d_fion, &c.d_dvps, &c.d_vnl, &c.d_dvnl,
-                     &c.d_tau_all, &c.d_astress};
+                     &c.d_tau_all, &c.d_astress, &c.d_twnl};
   for (double** b : bufs) dfree(*b);
   dfree(c.d_patom);
   dfree(c.d_pcol);
@@ -164,13 +171,20 @@ void step_eager(Context& c, bool want_f, bool want_s, double* energies, double* 
 // device, the Anderson theta and the polar iteration are decided there
 // (conditional nodes), and the last nodes copy slots, status and forces to
 // the pinned mirrors.  The graph is instantiated, not launched.
-void capture_step(Context& c, bool want_f, StepGraph& g) {
+// The operations of one PSDA step on c.stream while that stream is being
+// captured (it may be one branch of a larger capture).  Host state the
+// recording changes (profiling, the extrapolation flag, the launch count) is
+// put back afterwards; returns the number of this library's kernels recorded.
+long record_step(Context& c, bool want_f) {
   const bool prof = c.prof.on, extrap = c.extrapolate;
   const long n0 = c.nlaunch;
   c.prof.on = false;
-  QBX_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeRelaxed));
   c.capturing = true;
-  cudaGraph_t graph = nullptr;
+  auto restore = [&]() {
+    c.capturing = false;
+    c.prof.on = prof;
+    c.extrapolate = extrap;
+  };
   try {
     update_density(c);
     update_vhxc(c);
@@ -179,20 +193,29 @@ void capture_step(Context& c, bool want_f, StepGraph& g) {
     psda_update(c);
     enqueue_readback(c, want_f);
   } catch (...) {
-    cudaStreamEndCapture(c.stream, &graph);
-    if (graph) cudaGraphDestroy(graph);
-    c.capturing = false;
-    c.prof.on = prof;
-    c.extrapolate = extrap;
+    restore();
     c.nlaunch = n0;
     throw;
   }
-  c.capturing = false;
-  c.prof.on = prof;
-  c.extrapolate = extrap;
-  g.nkernels = c.nlaunch - n0;
+  restore();
+  const long k = c.nlaunch - n0;
   c.nlaunch = n0;
+  return k;
+}
+
+void capture_step(Context& c, bool want_f, StepGraph& g) {
+  QBX_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeRelaxed));
+  cudaGraph_t graph = nullptr;
+  try {
+    g.nkernels = record_step(c, want_f);
+  } catch (...) {
+    cudaStreamEndCapture(c.stream, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    throw;
+  }
   QBX_CUDA(cudaStreamEndCapture(c.stream, &graph));
+  static std::atomic<long> next_id{1};
+  g.id = next_id.fetch_add(1);
   cudaGraphInstantiateParams ip = {};
   const cudaError_t e = cudaGraphInstantiateWithParams(&g.exec, graph, &ip);
   if (e != cudaSuccess) {
@@ -218,6 +241,7 @@ void capture_step(Context& c, bool want_f, StepGraph& g) {
     }
     cudaGetLastError();
     cudaGraphDestroy(graph);
+    g.id = 0;
     throw Error{57, why};
   }
   cudaGraphDestroy(graph);
@@ -283,6 +307,10 @@ int qbx_create(qbx_context** out, int device, int precision) {
   // ~20% faster, whose ~1e-5 relative error only enters the step direction
   if (const char* e = std::getenv("QBX_TALL_KIND")) h->c.tall_kind = std::atoi(e) == 0 ? 0 : 1;
   if (const char* e = std::getenv("QBX_TALL_KIND_HC")) h->c.tall_kind_hc = std::atoi(e) == 1 ? 1 : 0;
+  // batches of captured steps: one graph launch per context on its own
+  // stream (default; 9.8 ms for 32 small systems) or one graph with every
+  // context as a branch (15.7 ms: its conditional nodes serialise branches)
+  if (const char* e = std::getenv("QBX_BATCH_GRAPH")) h->c.batch_single_graph = std::atoi(e) != 0;
   const int rc = guarded(h, [&](Context& c) {
     QBX_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
     QBX_BLAS(cublasCreate(&c.blas));
@@ -781,12 +809,14 @@ int qbx_set_step_graph(qbx_context* h, int on) {
   });
 }
 
-int qbx_step_graph_info(qbx_context* h, int* captured, long* launches, char* note, int note_len) {
+int qbx_step_graph_info(qbx_context* h, int* captured, long* launches, long* batch_launches,
+                        char* note, int note_len) {
   return guarded(h, [&](Context& c) {
     int n = 0;
     for (auto& g : c.graphs) n += g.exec != nullptr;
     if (captured) *captured = n;
     if (launches) *launches = c.graph_launches;
+    if (batch_launches) *batch_launches = c.batch_launches;
     if (note && note_len > 0) {
       std::strncpy(note, c.graph_note.c_str(), (size_t)note_len - 1);
       note[note_len - 1] = 0;
@@ -815,6 +845,78 @@ int qbx_scf_step_batch(qbx_context** ctxs, int n, int compute_forces, double* en
       all = gs[i]->exec != nullptr;
     }
     if (all) {
+      // with QBX_BATCH_GRAPH on the first context: one graph over all
+      // members (parallel branches), cached there while the members'
+      // captures stay the same
+      Context& lead = ctxs[0]->c;
+      std::vector<long> ids(n);
+      for (int i = 0; i < n; i++) ids[i] = gs[i]->id;
+      if (lead.batch_single_graph && lead.batch.ids != ids) {
+        // one multi-stream capture: every member's stream joins the lead
+        // stream's capture through an event, records its step as a branch
+        // and joins back
+        drop_batch(lead);
+        lead.batch.ids = ids;
+        std::string why;
+        cudaGraph_t graph = nullptr;
+        std::vector<cudaEvent_t> ev(n + 1, nullptr);
+        try {
+          for (auto& e : ev) QBX_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+          QBX_CUDA(cudaSetDevice(lead.device));
+          QBX_CUDA(cudaStreamBeginCapture(lead.stream, cudaStreamCaptureModeRelaxed));
+          try {
+            QBX_CUDA(cudaEventRecord(ev[0], lead.stream));
+            for (int i = 0; i < n; i++) {
+              Context& c = ctxs[i]->c;
+              QBX_REQUIRE(c.device == lead.device, 1, "batch members on different devices");
+              if (i > 0) QBX_CUDA(cudaStreamWaitEvent(c.stream, ev[0], 0));
+              record_step(c, want_f);
+              if (i > 0) {
+                QBX_CUDA(cudaEventRecord(ev[i + 1], c.stream));
+                QBX_CUDA(cudaStreamWaitEvent(lead.stream, ev[i + 1], 0));
+              }
+            }
+          } catch (...) {
+            cudaStreamEndCapture(lead.stream, &graph);
+            if (graph) cudaGraphDestroy(graph);
+            graph = nullptr;
+            throw;
+          }
+          QBX_CUDA(cudaStreamEndCapture(lead.stream, &graph));
+          QBX_CUDA(cudaGraphInstantiate(&lead.batch.exec, graph, 0));
+        } catch (const Error& e) {
+          why = e.msg;
+        }
+        if (graph) cudaGraphDestroy(graph);
+        for (auto e : ev)
+          if (e) cudaEventDestroy(e);
+        if (!why.empty()) {
+          cudaGetLastError();
+          if (lead.batch.exec) cudaGraphExecDestroy(lead.batch.exec);
+          lead.batch.exec = nullptr;
+          lead.batch.failed = true;
+          lead.graph_note = "batch graph: " + why + "; members launched one by one";
+        }
+      }
+      if (lead.batch.exec) {
+        const int rc = guarded(ctxs[0], [&](Context& c) {
+          QBX_CUDA(cudaGraphLaunch(c.batch.exec, c.stream));
+          QBX_CUDA(cudaStreamSynchronize(c.stream));
+        });
+        if (rc) return rc;
+        int first = 0;
+        for (int i = 0; i < n; i++) {
+          const int r = guarded(ctxs[i], [&](Context& c) {
+            c.nlaunch += gs[i]->nkernels;
+            c.graph_launches++;
+            finish_graph_step(c, want_f,
+                              energies ? energies + (size_t)i * QBX_NENERGY : nullptr, nullptr);
+          });
+          if (r && !first) first = r;
+        }
+        lead.batch_launches++;
+        return first;
+      }
       for (int i = 0; i < n; i++) {
         const int rc = guarded(ctxs[i], [&](Context& c) { launch_step_graph(c, *gs[i]); });
         if (rc) return rc;

@@ -9,6 +9,7 @@
 #include <cstring>
 #include <map>
 #include <stdexcept>
+#include <thread>
 
 #include "qbx_internal.h"
 
@@ -433,45 +434,76 @@ double esr_energy_forces(const double cell[9],
   }
   double d[3];
   for (int i = 0; i < 3; i++) d[i] = 2.0 * M_PI / norm3(recip + 3 * i);
-  double esr = 0.0;
-  for (int is1 = 0; is1 < nsp; is1++)
-    for (int is2 = is1; is2 < nsp; is2++) {
-      const double rc12 = std::sqrt(rcps * rcps + rcps * rcps);
-      const int nc0 = (int)(8.0 * rc12 / d[0]);
-      const int nc1 = (int)(8.0 * rc12 / d[1]);
-      const int nc2 = (int)(8.0 * rc12 / d[2]);
-      const int na1 = (int)tau[is1].size() / 3, na2 = (int)tau[is2].size() / 3;
-      for (int ia1 = 0; ia1 < na1; ia1++) {
-        const int ia2min = (is1 == is2) ? ia1 : 0;
-        for (int ia2 = ia2min; ia2 < na2; ia2++) {
-          const bool same = (is1 == is2 && ia1 == ia2);
-          double v12[3];
-          for (int j = 0; j < 3; j++) v12[j] = tau[is1][3 * ia1 + j] - tau[is2][3 * ia2 + j];
-          fold_in_ws(cell, v12);
-          for (int i0 = -nc0; i0 <= nc0; i0++)
-            for (int i1 = -nc1; i1 <= nc1; i1++)
-              for (int i2 = -nc2; i2 <= nc2; i2++) {
-                if (same && i0 == 0 && i1 == 0 && i2 == 0) continue;
-                const double fac = same ? 0.5 : 1.0;
-                double x[3];
-                for (int j = 0; j < 3; j++)
-                  x[j] = v12[j] + i0 * cell[j] + i1 * cell[3 + j] + i2 * cell[6 + j];
-                const double r12 = norm3(x);
-                const double arg = r12 / rc12;
-                const double term = zv[is1] * zv[is2] * std::erfc(arg) / r12;
-                esr += fac * term;
-                const double de = 2.0 * zv[is1] * zv[is2] * std::exp(-arg * arg) /
-                                  (rc12 * std::sqrt(M_PI));
-                const double dedr = -fac * (term + de) / (r12 * r12);
-                for (int j = 0; j < 3; j++) {
-                  f[is1][3 * ia1 + j] -= dedr * x[j];
-                  f[is2][3 * ia2 + j] += dedr * x[j];
+  // Pairs (is1 <= is2; ia2 >= ia1 within a species) in the reference's order,
+  // the outer atom index split over host threads with private sums that are
+  // added at the end (only the summation order differs from one thread).
+  struct Part {
+    double esr = 0.0;
+    double sig[6] = {0, 0, 0, 0, 0, 0};
+    std::vector<std::vector<double>> f;
+  };
+  const double rc12 = std::sqrt(rcps * rcps + rcps * rcps);
+  const int nc0 = (int)(8.0 * rc12 / d[0]);
+  const int nc1 = (int)(8.0 * rc12 / d[1]);
+  const int nc2 = (int)(8.0 * rc12 / d[2]);
+  int natoms = 0;
+  for (int is = 0; is < nsp; is++) natoms += (int)tau[is].size() / 3;
+  const int nthreads = std::max(1, std::min<int>((int)std::thread::hardware_concurrency(),
+                                                 std::min(16, natoms / 32)));
+  std::vector<Part> parts(nthreads);
+  auto work = [&](int t) {
+    Part& P = parts[t];
+    P.f.assign(nsp, std::vector<double>());
+    for (int is = 0; is < nsp; is++) P.f[is].assign(tau[is].size(), 0.0);
+    for (int is1 = 0; is1 < nsp; is1++)
+      for (int is2 = is1; is2 < nsp; is2++) {
+        const int na1 = (int)tau[is1].size() / 3, na2 = (int)tau[is2].size() / 3;
+        for (int ia1 = t; ia1 < na1; ia1 += nthreads) {
+          const int ia2min = (is1 == is2) ? ia1 : 0;
+          for (int ia2 = ia2min; ia2 < na2; ia2++) {
+            const bool same = (is1 == is2 && ia1 == ia2);
+            double v12[3];
+            for (int j = 0; j < 3; j++) v12[j] = tau[is1][3 * ia1 + j] - tau[is2][3 * ia2 + j];
+            fold_in_ws(cell, v12);
+            for (int i0 = -nc0; i0 <= nc0; i0++)
+              for (int i1 = -nc1; i1 <= nc1; i1++)
+                for (int i2 = -nc2; i2 <= nc2; i2++) {
+                  if (same && i0 == 0 && i1 == 0 && i2 == 0) continue;
+                  const double fac = same ? 0.5 : 1.0;
+                  double x[3];
+                  for (int j = 0; j < 3; j++)
+                    x[j] = v12[j] + i0 * cell[j] + i1 * cell[3 + j] + i2 * cell[6 + j];
+                  const double r12 = norm3(x);
+                  const double arg = r12 / rc12;
+                  const double term = zv[is1] * zv[is2] * std::erfc(arg) / r12;
+                  P.esr += fac * term;
+                  const double de = 2.0 * zv[is1] * zv[is2] * std::exp(-arg * arg) /
+                                    (rc12 * std::sqrt(M_PI));
+                  const double dedr = -fac * (term + de) / (r12 * r12);
+                  for (int j = 0; j < 3; j++) {
+                    P.f[is1][3 * ia1 + j] -= dedr * x[j];
+                    P.f[is2][3 * ia2 + j] += dedr * x[j];
+                  }
+                  for (int k = 0; k < 6; k++) P.sig[k] += dedr * x[vi[k]] * x[vj[k]];
                 }
-                for (int k = 0; k < 6; k++) sig[k] += dedr * x[vi[k]] * x[vj[k]];
-              }
+          }
         }
       }
-    }
+  };
+  if (nthreads == 1) {
+    work(0);
+  } else {
+    std::vector<std::thread> th;
+    for (int t = 0; t < nthreads; t++) th.emplace_back(work, t);
+    for (auto& x : th) x.join();
+  }
+  double esr = 0.0;
+  for (const Part& P : parts) {
+    esr += P.esr;
+    for (int k = 0; k < 6; k++) sig[k] += P.sig[k];
+    for (int is = 0; is < nsp; is++)
+      for (size_t i = 0; i < f[is].size(); i++) f[is][i] += P.f[is][i];
+  }
   if (sigma) {
     const double* a = cell;
     const double omega = std::fabs(a[0] * (a[4] * a[8] - a[5] * a[7]) -

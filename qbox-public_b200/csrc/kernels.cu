@@ -539,8 +539,18 @@ void launch_nl_forces(Context& ctx, double* fion) {
                                                         ctx.d_gx_w + (size_t)j * ngw, ngw, n,
                                                         (double2*)ctx.d_ctmp);
     QBX_LAUNCHED(ctx);
-    QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_T, CUBLAS_OP_N, ctx.nproj, ctx.nst, 2 * ngw, &two,
-                         ctx.d_anl, 2 * ngw, ctx.d_ctmp, 2 * ngw, &zero, ctx.d_dfnl, ctx.nproj));
+    if (ctx.precision == MIXED) {
+      // dF_j = 2 A^T (i G_j C) as three BF16 split products (the split of
+      // H*C is free here: the step splits H*C again after the forces)
+      const int K = 2 * ngw;
+      split_bf16_2d(ctx, ctx.d_ctmp, K, ctx.nst, K, ctx.hs_hi, ctx.hs_lo, ctx.ldp);
+      split_gemm(ctx, true, false, ctx.nproj, ctx.nst, K, 2.0, ctx.as_hi, ctx.as_lo, ctx.ldp,
+                 ctx.hs_hi, ctx.hs_lo, ctx.ldp, 0.0, ctx.d_dfnl);
+    } else {
+      QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_T, CUBLAS_OP_N, ctx.nproj, ctx.nst, 2 * ngw, &two,
+                           ctx.d_anl, 2 * ngw, ctx.d_ctmp, 2 * ngw, &zero, ctx.d_dfnl,
+                           ctx.nproj));
+    }
     k_nl_force<<<ctx.nproj, kThreads, 0, ctx.stream>>>(ctx.d_fnl, ctx.d_dfnl, ctx.d_occ,
                                                        ctx.d_patom, ctx.nproj, ctx.nst, j, fion);
     QBX_LAUNCHED(ctx);
@@ -693,13 +703,39 @@ void launch_setup_atoms(Context& ctx) {
   const Basis& wb = ctx.wb;
   const int ngv = vb.ng, ngw = wb.ng;
   const int nsp = (int)ctx.species.size();
+  // projector forms twnl = Y_lm(G) V_nl(|G|) (spline of the radial form) do
+  // not depend on the positions: built once per set of atoms, one row of
+  // ngw per (species, projector, m)
+  if (!ctx.d_twnl) {
+    const double s14pi = std::sqrt(1.0 / (4.0 * M_PI));
+    const double s34pi = std::sqrt(3.0 / (4.0 * M_PI));
+    std::vector<double> tw;
+    for (int is = 0; is < nsp; is++) {
+      const SpeciesTables& sp = ctx.species[is];
+      for (size_t iop = 0; iop < sp.proj_l.size(); iop++) {
+        const int l = sp.proj_l[iop];
+        std::vector<double> v(ngw);
+        for (int ig = 0; ig < ngw; ig++) {
+          double val, dv;
+          sp.dvnlg((int)iop, wb.g[ig], val, dv);
+          v[ig] = val;
+        }
+        for (int m = 0; m < 2 * l + 1; m++)
+          for (int ig = 0; ig < ngw; ig++)
+            tw.push_back(l == 0 ? s14pi * v[ig]
+                                : s34pi * wb.gx[(size_t)m * ngw + ig] * wb.gi[ig] * v[ig]);
+      }
+    }
+    ctx.d_twnl = tw.empty() ? nullptr : dupload(tw);
+  }
   QBX_CUDA(cudaMemsetAsync(ctx.d_vion, 0, 2 * sizeof(double) * ngv, ctx.stream));
   QBX_CUDA(cudaMemsetAsync(ctx.d_rhops, 0, 2 * sizeof(double) * ngv, ctx.stream));
-  int col = 0;
+  int col = 0, row = 0, atom0 = 0;
   for (int is = 0; is < nsp; is++) {
     const SpeciesTables& sp = ctx.species[is];
     const int na = (int)ctx.tau[is].size() / 3;
-    double* d_tau = dupload(ctx.tau[is]);
+    // positions of this species: a slice of the species-major d_tau_all
+    const double* d_tau = ctx.d_tau_all + 3 * (size_t)atom0;
     double2* sf = (double2*)ctx.d_sfac + (size_t)is * ngv;
     k_sfac<<<blocks_for(ngv), kThreads, 0, ctx.stream>>>(ctx.d_gx_v, ngv, d_tau, na, sf);
     QBX_LAUNCHED(ctx);
@@ -708,36 +744,19 @@ void launch_setup_atoms(Context& ctx) {
                                                          (double2*)ctx.d_vion,
                                                          (double2*)ctx.d_rhops);
     QBX_LAUNCHED(ctx);
-    // projectors: twnl on the host (spline of V_nl times Y_lm), phases here
-    const double s14pi = std::sqrt(1.0 / (4.0 * M_PI));
-    const double s34pi = std::sqrt(3.0 / (4.0 * M_PI));
+    // projector columns of this species: twnl times the phases
     for (size_t iop = 0; iop < sp.proj_l.size(); iop++) {
       const int l = sp.proj_l[iop];
-      std::vector<double> v(ngw);
-      for (int ig = 0; ig < ngw; ig++) {
-        double val, dv;
-        sp.dvnlg((int)iop, wb.g[ig], val, dv);
-        v[ig] = val;
-      }
-      const int nm = 2 * l + 1;
-      for (int m = 0; m < nm; m++) {
-        std::vector<double> tw(ngw);
-        for (int ig = 0; ig < ngw; ig++) {
-          if (l == 0) tw[ig] = s14pi * v[ig];
-          else tw[ig] = s34pi * wb.gx[(size_t)m * ngw + ig] * wb.gi[ig] * v[ig];
-        }
-        double* d_tw = dupload(tw);
+      for (int m = 0; m < 2 * l + 1; m++, row++) {
         dim3 grid((ngw + kThreads - 1) / kThreads, na);
-        k_anl<<<grid, kThreads, 0, ctx.stream>>>(ctx.d_gx_w, ngw, d_tw, d_tau, na, l,
+        k_anl<<<grid, kThreads, 0, ctx.stream>>>(ctx.d_gx_w, ngw, ctx.d_twnl + (size_t)row * ngw,
+                                                  d_tau, na, l,
                                                   (double2*)ctx.d_anl + (size_t)col * ngw);
         QBX_LAUNCHED(ctx);
-        QBX_CUDA(cudaStreamSynchronize(ctx.stream));
-        dfree(d_tw);
         col += na;
       }
     }
-    QBX_CUDA(cudaStreamSynchronize(ctx.stream));
-    dfree(d_tau);
+    atom0 += na;
   }
   QBX_REQUIRE(col == ctx.nproj, 30, "projector count mismatch");
 }

@@ -8,8 +8,9 @@
 // place (the buffers keep their addresses, so captured electronic steps stay
 // valid); the wavefunctions are extrapolated on the device (linear, with the
 // previous wavefunctions aligned by a polar factor and the result Lowdin
-// orthonormalised); then nitscf electronic steps.  Only positions, forces
-// and energies cross to the host.
+// orthonormalised: align_to_c and lowdin of step.cu, split precision in the
+// mixed path); then nitscf electronic steps.  Only positions, forces and
+// energies cross to the host.
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -50,64 +51,6 @@ void extrapolate(Context& c, double s, int mode) {
   const size_t n = 2 * (size_t)c.wb.ng * c.nst;
   k_extrapolate<<<blocks(n), kThreads, 0, c.stream>>>(c.d_c, c.d_wfv, n, s, mode);
   QBX_LAUNCHED(c);
-}
-
-// zero the strictly upper triangle of an n x n column-major matrix
-__global__ void k_lower_only(double* __restrict__ a, int n) {
-  const size_t nn = (size_t)n * n;
-  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < nn;
-       t += (size_t)gridDim.x * blockDim.x) {
-    const int i = (int)(t % n), j = (int)(t / n);
-    if (i < j) a[t] = 0.0;
-  }
-}
-
-// C_out = C_in M (K x n times n x n), C_in copied to the scratch first when
-// it is C_out itself
-void right_multiply(Context& c, double* x, const double* M) {
-  const int n = c.nst, K = 2 * c.wb.ng;
-  const double one = 1.0, zero = 0.0;
-  QBX_CUDA(cudaMemcpyAsync(c.d_ctmp, x, sizeof(double) * (size_t)K * n, cudaMemcpyDeviceToDevice,
-                           c.stream));
-  QBX_BLAS(cublasDgemm(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, K, n, n, &one, c.d_ctmp, K, M, n, &zero,
-                       x, K));
-}
-
-// SlaterDet::align (src/SlaterDet.cpp:979-1044), the wavefunction velocity
-// buffer aligned to C: cv <- cv X, X the orthogonal polar factor of
-// B = 2 cv^T C - cv0 c0^T.
-void align_wfv(Context& c) {
-  const int n = c.nst, K = 2 * c.wb.ng;
-  const double two = 2.0, zero = 0.0;
-  double* X = c.d_nn2;
-  QBX_BLAS(cublasDgemm(c.blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, c.d_wfv, K, c.d_c, K,
-                       &zero, X, n));
-  launch_rank1_fix(c, X, n, c.d_wfv, K, c.d_c, K, n, n, -1.0, false);
-  polar_factor(c, X, 1.e-6, 20);
-  right_multiply(c, c.d_wfv, X);
-}
-
-// SlaterDet::lowdin (src/SlaterDet.cpp:674-721): S = 2 C^T C - c0 c0^T =
-// L L^T, U the orthogonal polar factor of L^T, C <- C L^-T U.
-void lowdin(Context& c) {
-  const int n = c.nst, K = 2 * c.wb.ng;
-  const double one = 1.0, two = 2.0, zero = 0.0;
-  launch_cleanup(c, c.d_c);
-  double* L = c.d_nn;
-  double* X = c.d_nn2;
-  QBX_BLAS(cublasDsyrk(c.blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, n, K, &two, c.d_c, K, &zero,
-                       L, n));
-  launch_rank1_fix(c, L, n, c.d_c, K, c.d_c, K, n, n, -1.0, true);
-  QBX_SOLVER(cusolverDnDpotrf(c.solver, CUBLAS_FILL_MODE_LOWER, n, L, n, c.d_solver_work,
-                              c.solver_lwork, c.d_status + ST_INFO_GRAM));
-  k_lower_only<<<blocks((size_t)n * n), kThreads, 0, c.stream>>>(L, n);
-  QBX_LAUNCHED(c);
-  QBX_BLAS(cublasDgeam(c.blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, &one, L, n, &zero, L, n, X, n));
-  polar_factor(c, X, 1.e-6, 20);
-  // X <- L^-T U
-  QBX_BLAS(cublasDtrsm(c.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T,
-                       CUBLAS_DIAG_NON_UNIT, n, n, &one, L, n, X, n));
-  right_multiply(c, c.d_c, X);
 }
 
 int natoms_of(const Context& c) {
@@ -168,6 +111,7 @@ void md_run(Context& c, int niter, int nitscf, double dt, const double* mass_amu
   }
   // energy and forces at the current positions with the current C
   auto forces_here = [&]() {
+    ProfScope ps(c, "md_forces");
     update_density(c);
     update_vhxc(c);
     energy(c, false, true);
@@ -202,15 +146,21 @@ void md_run(Context& c, int niter, int nitscf, double dt, const double* mass_amu
       rp[i] = r0[i] + v0[i] * dt + dt * dt / (2.0 * pm[i]) * f[i];
     rm = r0;
     r0 = rp;
-    move_atoms(c, r0.data());
+    {
+      ProfScope ps(c, "md_move_atoms");
+      move_atoms(c, r0.data());
+    }
     // wavefunction extrapolation (src/BOSampleStepper.cpp:731-779)
-    if (it == 0) {
-      extrapolate(c, dt, 0);
-      gram(c);
-    } else {
-      align_wfv(c);
-      extrapolate(c, 0.0, 1);
-      lowdin(c);
+    {
+      ProfScope ps(c, "md_extrapolate");
+      if (it == 0) {
+        extrapolate(c, dt, 0);
+        gram(c);
+      } else {
+        align_to_c(c, c.d_wfv);
+        extrapolate(c, 0.0, 1);
+        lowdin(c);
+      }
     }
     readback(c, false);
     check_status(c);
@@ -221,7 +171,7 @@ void md_run(Context& c, int niter, int nitscf, double dt, const double* mass_amu
   }
   // wavefunction velocity and the forces at the last positions
   // (src/BOSampleStepper.cpp:1351-1420)
-  align_wfv(c);
+  align_to_c(c, c.d_wfv);
   extrapolate(c, 1.0 / dt, 2);
   gram(c);
   forces_here();

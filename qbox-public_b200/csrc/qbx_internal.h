@@ -239,8 +239,18 @@ enum : int {
 // number of this library's kernels it holds outside the polar loop.
 struct StepGraph {
   cudaGraphExec_t exec = nullptr;
+  long id = 0;                   // unique per capture (process-wide), 0 = none
   long nkernels = 0;
   int uses = 0;        // eager runs of this configuration before capture
+};
+
+// One graph holding the steps of several contexts as parallel branches
+// (qbx_scf_step_batch, one multi-stream capture), cached on the first
+// context of the batch and rebuilt when the members' captured steps change.
+struct BatchGraph {
+  cudaGraphExec_t exec = nullptr;
+  std::vector<long> ids;         // StepGraph ids of the members, in order
+  bool failed = false;           // instantiation refused: launch per context
 };
 
 struct Context {
@@ -342,6 +352,7 @@ struct Context {
   double* d_dvnl = nullptr;     // nrad*ngw: dV_nl/dG
   int* d_pcol = nullptr;        // 4*nproj: (l, m, radial row, atom) per column
   double* d_tau_all = nullptr;  // 3*natoms
+  double* d_twnl = nullptr;     // projector forms Y_lm V_nl, one ngw row per (species, l, m)
   double* d_astress = nullptr;  // 2*ngw*nproj: a strain-derivative projector block
   void* sa_hi = nullptr;        // its BF16 split (mixed path)
   void* sa_lo = nullptr;
@@ -396,11 +407,14 @@ struct Context {
   bool step_graph = false;
   bool capturing = false;        // a step is being captured on `stream`
   StepGraph graphs[4];           // by (extrapolate, forces)
+  BatchGraph batch;              // batch graph led by this context
+  bool batch_single_graph = false;   // QBX_BATCH_GRAPH=1: batch steps as one graph
   cudaStream_t side[2] = {nullptr, nullptr};   // capture of conditional bodies
   void* d_blas_ws = nullptr;     // cuBLAS workspace bound with every stream
   size_t blas_ws_bytes = 0;
   std::string graph_note;        // why the last capture was abandoned, if it was
   long graph_launches = 0;       // captured steps launched so far
+  long batch_launches = 0;       // batch graphs launched with this context leading
   int polar_iters = 0;           // iterations of the last eager polar
   double* d_wfv = nullptr;       // wavefunction velocity of the MD extrapolation
 
@@ -534,6 +548,8 @@ void polar_factor(Context& ctx, double* x, double tol, int maxiter);
 int polar_entry(Context& ctx, double* x, double tol, int maxiter, bool graph);
 // one electronic step (captured graph or eager), energies/fion as qbx_scf_step
 void scf_step_any(Context& c, bool want_f, bool want_s, double* energies, double* fion);
+void align_to_c(Context& ctx, double* cv);   // SlaterDet::align of cv to C
+void lowdin(Context& ctx);                     // SlaterDet::lowdin of C
 // molecular dynamics (md.cu)
 void move_atoms(Context& c, const double* tau);
 void md_run(Context& c, int niter, int nitscf, double dt, const double* mass_amu, double* vel,

@@ -331,6 +331,79 @@ void ortho_align(Context& ctx) {
   }
 }
 
+// zero the strictly upper triangle of an n x n column-major matrix
+__global__ void k_lower_only(double* __restrict__ a, int n) {
+  const size_t nn = (size_t)n * n;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < nn;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(t % n), j = (int)(t / n);
+    if (i < j) a[t] = 0.0;
+  }
+}
+
+// x <- x M for a K x n wavefunction block x and an n x n matrix M: in the
+// mixed path x - x (I - M) through the TF32 tall update (M close to the
+// identity, so the split error only touches the correction), else one FP64
+// GEMM from a copy of x
+static void rotate(Context& ctx, double* x, const double* M) {
+  const int n = ctx.nst, K = 2 * ctx.wb.ng;
+  if (mixed(ctx)) {
+    double* T = ctx.d_nn3;
+    launch_identity_axpy(ctx, T, M, n, -1.0);
+    tall_update(ctx, ctx.tall_kind, x, T, -1.0, x);
+    return;
+  }
+  const double one = 1.0, zero = 0.0;
+  QBX_CUDA(cudaMemcpyAsync(ctx.d_ctmp, x, sizeof(double) * (size_t)K * n,
+                           cudaMemcpyDeviceToDevice, ctx.stream));
+  QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, K, n, n, &one, ctx.d_ctmp, K, M, n,
+                       &zero, x, K));
+}
+
+// SlaterDet::align (src/SlaterDet.cpp:979-1044) of the block cv to C:
+// cv <- cv X, X the orthogonal polar factor of B = 2 cv^T C - cv0 c0^T
+// (BF16 split product in the mixed path)
+void align_to_c(Context& ctx, double* cv) {
+  const int n = ctx.nst, K = 2 * ctx.wb.ng;
+  double* X = ctx.d_nn2;
+  if (mixed(ctx)) {
+    split_bf16_2d(ctx, cv, K, n, K, ctx.cs_hi[0], ctx.cs_lo[0], ctx.ldp);
+    split_bf16_2d(ctx, ctx.d_c, K, n, K, ctx.cs_hi[1], ctx.cs_lo[1], ctx.ldp);
+    split_gemm(ctx, true, false, n, n, K, 2.0, ctx.cs_hi[0], ctx.cs_lo[0], ctx.ldp,
+               ctx.cs_hi[1], ctx.cs_lo[1], ctx.ldp, 0.0, X);
+  } else {
+    const double two = 2.0, zero = 0.0;
+    QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, cv, K, ctx.d_c, K,
+                         &zero, X, n));
+  }
+  launch_rank1_fix(ctx, X, n, cv, K, ctx.d_c, K, n, n, -1.0, false);
+  polar(ctx, X, 1.e-6, 20);
+  rotate(ctx, cv, X);
+}
+
+// SlaterDet::lowdin (src/SlaterDet.cpp:674-721): S = 2 C^T C - c0 c0^T =
+// L L^T, U the orthogonal polar factor of L^T, C <- C L^-T U
+void lowdin(Context& ctx) {
+  const int n = ctx.nst;
+  const double one = 1.0, zero = 0.0;
+  const bool mx = mixed(ctx);
+  launch_cleanup(ctx, ctx.d_c);
+  double* L = ctx.d_nn;
+  double* X = ctx.d_nn2;
+  if (mx) split_bf16_2d(ctx, ctx.d_c, 2 * ctx.wb.ng, n, 2 * ctx.wb.ng, ctx.cs_hi[1], ctx.cs_lo[1],
+                        ctx.ldp);
+  overlap_cholesky(ctx, ctx.d_c, L, ST_INFO_GRAM, mx ? 1 : -1);
+  k_lower_only<<<(int)std::min<size_t>(((size_t)n * n + 255) / 256, 148 * 16), 256, 0,
+                 ctx.stream>>>(L, n);
+  QBX_LAUNCHED(ctx);
+  QBX_BLAS(cublasDgeam(ctx.blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, &one, L, n, &zero, L, n, X, n));
+  polar(ctx, X, 1.e-6, 20);
+  // X <- L^-T U
+  QBX_BLAS(cublasDtrsm(ctx.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T,
+                       CUBLAS_DIAG_NON_UNIT, n, n, &one, L, n, X, n));
+  rotate(ctx, ctx.d_c, X);
+}
+
 // ChargeDensity::update_density (src/ChargeDensity.cpp:136-198)
 void update_density(Context& ctx) {
   ProfScope ps(ctx, "update_density");

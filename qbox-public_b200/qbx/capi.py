@@ -113,7 +113,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "qbx_md_run": (_I, [_P, _I, _I, _D, _DP, _DP, _DP, _DP, _DP]),
         "qbx_polar": (_I, [_P, _DP, _D, _I, _I, ctypes.POINTER(_I)]),
         "qbx_step_graph_info": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_long),
-                                     ctypes.c_char_p, _I]),
+                                     ctypes.POINTER(ctypes.c_long), ctypes.c_char_p, _I]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -370,12 +370,18 @@ class Context:
 
     def step_graph_info(self):
         """qbx_step_graph_info: (graphs captured, graph launches, note)."""
+        n, launches, _, note = self.step_graph_info_full()
+        return n, launches, note
+
+    def step_graph_info_full(self):
+        """(graphs captured, graph launches, batch graph launches, note)."""
         n = _I()
         launches = ctypes.c_long()
+        batch = ctypes.c_long()
         buf = ctypes.create_string_buffer(512)
         self._ok(self.lib.qbx_step_graph_info(self.h, ctypes.byref(n), ctypes.byref(launches),
-                                              buf, 512), "step_graph_info")
-        return n.value, launches.value, buf.value.decode()
+                                              ctypes.byref(batch), buf, 512), "step_graph_info")
+        return n.value, launches.value, batch.value, buf.value.decode()
 
     def autotune(self) -> str:
         """qbx_autotune: time the staged-FFT configurations on this context

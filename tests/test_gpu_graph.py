@@ -64,11 +64,17 @@ def test_graph_step_with_forces():
     graph.close()
 
 
-def test_graph_batch_single_launch_path():
-    """With every context's step captured, qbx_scf_step_batch launches all
-    graphs from one thread; the energies equal stepping each eagerly."""
+@pytest.mark.parametrize("single_graph", [False, True])
+def test_graph_batch_paths(single_graph, monkeypatch):
+    """With every context's step captured, qbx_scf_step_batch launches each
+    context's graph from one thread, or (QBX_BATCH_GRAPH=1) one graph whose
+    branches are the contexts' steps; either way the energies equal
+    stepping each context eagerly."""
     systs = systems.batch()[:6]
+    if single_graph:
+        monkeypatch.setenv("QBX_BATCH_GRAPH", "1")
     ctxs = [capi.from_system(s, precision=capi.FP64) for s in systs]
+    monkeypatch.delenv("QBX_BATCH_GRAPH", raising=False)
     ref = [capi.from_system(s, precision=capi.FP64) for s in systs]
     for c in ctxs:
         c.set_step_graph(True)
@@ -81,6 +87,11 @@ def test_graph_batch_single_launch_path():
     for c in ctxs:
         captured, launches, note = c.step_graph_info()
         assert note == "" and captured >= 1 and launches >= 2, (captured, launches, note)
+    batch_launches = ctxs[0].step_graph_info_full()[2]
+    if single_graph:
+        assert batch_launches >= 2      # the steps ran as branches of one graph
+    else:
+        assert batch_launches == 0
     for c in ctxs + ref:
         c.close()
 
