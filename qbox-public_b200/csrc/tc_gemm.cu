@@ -285,12 +285,26 @@ k_tc_split_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant
         }
       }
     } else if (row < M && ok) {
+      // FP64 read-modify-write of the tile, 16 columns per group: the
+      // group's loads are issued together so their latencies overlap (one
+      // load at a time would leave the epilogue waiting 128 round trips)
+      constexpr int G = 16;
+      double* crow = C + row;
 #pragma unroll
-      for (int j = 0; j < BN; ++j) {
-        const int col = n0 + j;
-        if (col < N) {
-          double* o = C + (size_t)col * ldc + row;
-          *o = alpha * (double)acc[j] + (beta != 0.0 ? beta * *o : 0.0);
+      for (int j0 = 0; j0 < BN; j0 += G) {
+        double old[G];
+        if (beta != 0.0) {
+#pragma unroll
+          for (int j = 0; j < G; ++j) {
+            const int col = n0 + j0 + j;
+            old[j] = col < N ? crow[(size_t)col * ldc] : 0.0;
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < G; ++j) {
+          const int col = n0 + j0 + j;
+          if (col < N)
+            crow[(size_t)col * ldc] = alpha * (double)acc[j0 + j] + (beta != 0.0 ? beta * old[j] : 0.0);
         }
       }
     }
