@@ -285,11 +285,21 @@ k_tc_split_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant
         }
       }
     } else if (row < M && ok) {
+      double* crow = C + row;
+      if (beta == 1.0) {
+        // C += alpha D: fire-and-forget FP64 adds (each element has one
+        // writer, so the result does not depend on their order); no load
+        // round trips in the epilogue
+#pragma unroll
+        for (int j = 0; j < BN; ++j) {
+          const int col = n0 + j;
+          if (col < N) atomicAdd(crow + (size_t)col * ldc, alpha * (double)acc[j]);
+        }
+      } else {
       // FP64 read-modify-write of the tile, 16 columns per group: the
       // group's loads are issued together so their latencies overlap (one
       // load at a time would leave the epilogue waiting 128 round trips)
       constexpr int G = 16;
-      double* crow = C + row;
 #pragma unroll
       for (int j0 = 0; j0 < BN; j0 += G) {
         double old[G];
@@ -306,6 +316,7 @@ k_tc_split_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant
           if (col < N)
             crow[(size_t)col * ldc] = alpha * (double)acc[j0 + j] + (beta != 0.0 ? beta * old[j] : 0.0);
         }
+      }
       }
     }
   }
