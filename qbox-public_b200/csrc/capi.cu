@@ -1118,8 +1118,11 @@ int qbx_split_gemm_tn(qbx_context* h, int m, int n, int k, const double* a, cons
 int qbx_set_gemm_backend(qbx_context* h, int backend) {
   return guarded(h, [&](Context& c) {
     QBX_REQUIRE(backend == 0 || backend == 1, 1, "backend must be 0 (cuBLAS) or 1 (tcgen05)");
+    const bool changed = c.gemm_backend != backend;
     c.gemm_backend = backend;
     drop_graphs(c);
+    // the cuBLAS backend has TF32 split buffers of its own
+    if (changed && c.have_cell) alloc_mixed(c);
   });
 }
 

@@ -613,11 +613,15 @@ void alloc_mixed(Context& ctx) {
   QBX_CUDA(cudaMalloc(&ctx.hs_lo, wf * 2));
   QBX_CUDA(cudaMalloc(&ctx.ss_hi, std::max<size_t>(small, 1) * 2));
   QBX_CUDA(cudaMalloc(&ctx.ss_lo, std::max<size_t>(small, 1) * 2));
-  ctx.c32 = dalloc<float>((size_t)ctx.ldp * n);
-  ctx.c32lo = dalloc<float>((size_t)ctx.ldp * n);
-  const size_t small4 = std::max<size_t>((size_t)pad4((int)std::max(np, n)) * n, 1);
-  ctx.s32 = dalloc<float>(small4);
-  ctx.s32lo = dalloc<float>(small4);
+  // TF32 splits for the cuBLAS products: only with that backend
+  const bool cublas_tf32 = ctx.gemm_backend == 0;
+  if (cublas_tf32) {
+    ctx.c32 = dalloc<float>((size_t)ctx.ldp * n);
+    ctx.c32lo = dalloc<float>((size_t)ctx.ldp * n);
+    const size_t small4 = std::max<size_t>((size_t)pad4((int)std::max(np, n)) * n, 1);
+    ctx.s32 = dalloc<float>(small4);
+    ctx.s32lo = dalloc<float>(small4);
+  }
   // tall-update splits: room for either kind (TF32 4 bytes at ld pad4,
   // BF16 2 bytes at ld pad8)
   auto tall_bytes = [](size_t rows, size_t cols) { return (size_t)pad8((int)rows) * cols * 4; };
@@ -628,8 +632,10 @@ void alloc_mixed(Context& ctx) {
   if (np) {
     QBX_CUDA(cudaMalloc(&ctx.as_hi, (size_t)ctx.ldp * np * 2));
     QBX_CUDA(cudaMalloc(&ctx.as_lo, (size_t)ctx.ldp * np * 2));
-    ctx.a32 = dalloc<float>((size_t)ctx.ldp * np);
-    ctx.a32lo = dalloc<float>((size_t)ctx.ldp * np);
+    if (cublas_tf32) {
+      ctx.a32 = dalloc<float>((size_t)ctx.ldp * np);
+      ctx.a32lo = dalloc<float>((size_t)ctx.ldp * np);
+    }
     QBX_CUDA(cudaMalloc(&ctx.at_hi, tall_bytes(np, K)));
     QBX_CUDA(cudaMalloc(&ctx.at_lo, tall_bytes(np, K)));
     split_projectors(ctx);
@@ -644,7 +650,7 @@ void split_projectors(Context& ctx) {
   if (ctx.precision != MIXED || !ctx.d_anl || !ctx.nproj) return;
   const int K = 2 * ctx.wb.ng, np = ctx.nproj;
   split_bf16_2d(ctx, ctx.d_anl, K, np, K, ctx.as_hi, ctx.as_lo, ctx.ldp);
-  split_tf32(ctx, ctx.d_anl, K, np, K, ctx.a32, ctx.a32lo, ctx.ldp);
+  if (ctx.a32) split_tf32(ctx, ctx.d_anl, K, np, K, ctx.a32, ctx.a32lo, ctx.ldp);
   split_t(ctx, ctx.tall_kind_hc, ctx.d_anl, K, np, K, ctx.at_hi, ctx.at_lo,
           Context::tall_ld_of(ctx.tall_kind_hc, np));
 }
