@@ -665,8 +665,13 @@ static void grid_fft(Context& ctx, int dir) {
   const int n[3] = {b.n0, b.n1, b.n2};
   const int L = 16;
   for (int axis = 0; axis < 3; axis++) {
-    const RadixPlan p = make_plan(n[axis]);
     const double2* tw = twiddles(ctx, axis);
+    // compile-time lengths: warp FFTs on coalesced tiles (fft_fast.cuh)
+    if (ctx.fast_fft &&
+        (fast_grid_lines_a(ctx, (double2*)ctx.d_grid, b.n0, b.n1, b.n2, axis, dir, tw) ||
+         fast_grid_lines_b(ctx, (double2*)ctx.d_grid, b.n0, b.n1, b.n2, axis, dir, tw)))
+      continue;
+    const RadixPlan p = make_plan(n[axis]);
     int nblocks;
     if (axis == 0) nblocks = (b.n1 * b.n2 + L - 1) / L;
     else if (axis == 1) nblocks = ((b.n0 + L - 1) / L) * b.n2;

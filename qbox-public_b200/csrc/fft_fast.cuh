@@ -626,7 +626,90 @@ size_t smem_need(const Context& ctx, const StagedArgs& a) {
   return std::max(std::max(x, z), l);
 }
 
+// ------------------------------------------------------------ full grid
+// In-place FP64 FFT of every line along one axis of an n0 x n1 x n2 grid (x
+// fastest) whose length along that axis is N.  A CTA copies a tile of
+// kGridLines lines into shared memory with coalesced accesses (consecutive
+// lines for the x axis; lines at consecutive x for the y and z axes, so each
+// row of the tile is one contiguous run of the grid), its warps transform
+// the tile's lines in place with the compile-time warp FFT, and the tile is
+// copied back.
+constexpr int kGridLines = 16;
+constexpr int kGridThreads = 256;
+
+template <int N, int DIR>
+__global__ void __launch_bounds__(kGridThreads)
+k_grid_lines(double2* __restrict__ grid, int n0, int n1, int n2, int axis,
+             const double2* __restrict__ tw_g) {
+  using C = double2;
+  constexpr int L = kGridLines, LD = pitch(N);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  C* tile = tw + N;
+  load_tw(tw, tw_g, N);
+  size_t base, estride, lstride;
+  int nl;
+  if (axis == 0) {
+    const int l0 = blockIdx.x * L;
+    nl = min(L, n1 * n2 - l0);
+    base = (size_t)l0 * N;
+    estride = 1;
+    lstride = N;
+  } else {
+    const int xt = (n0 + L - 1) / L;
+    const int outer = blockIdx.x / xt, x0 = (blockIdx.x % xt) * L;
+    nl = min(L, n0 - x0);
+    base = (size_t)x0 + (axis == 1 ? (size_t)n0 * n1 * outer : (size_t)n0 * outer);
+    estride = axis == 1 ? (size_t)n0 : (size_t)n0 * n1;
+    lstride = 1;
+  }
+  // x lines: the tile is one contiguous run; y and z: runs of nl along x
+  for (int t = threadIdx.x; t < nl * N; t += blockDim.x) {
+    int line, e;
+    if (axis == 0) { line = t / N; e = t - line * N; }
+    else { line = t % nl; e = t / nl; }
+    tile[line * LD + e] = grid[base + e * estride + line * lstride];
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int l = warp; l < nl; l += nw) {
+    C* row = tile + l * LD;
+    reg::warp_fft<N, DIR>(row, tw, lane, BufLoad<C>{row}, BufStore<C>{row});
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < nl * N; t += blockDim.x) {
+    int line, e;
+    if (axis == 0) { line = t / N; e = t - line * N; }
+    else { line = t % nl; e = t / nl; }
+    grid[base + e * estride + line * lstride] = tile[line * LD + e];
+  }
+}
+
+template <int N>
+void run_grid_lines(Context& ctx, double2* grid, int n0, int n1, int n2, int axis, int dir,
+                    const double2* tw) {
+  const int L = kGridLines;
+  const int nblocks = axis == 0 ? (n1 * n2 + L - 1) / L
+                                : ((n0 + L - 1) / L) * (axis == 1 ? n2 : n1);
+  const size_t smem = sizeof(double2) * ((size_t)N + (size_t)L * pitch(N));
+  if (dir > 0) {
+    allow_smem(k_grid_lines<N, +1>, smem);
+    k_grid_lines<N, +1><<<nblocks, kGridThreads, smem, ctx.stream>>>(grid, n0, n1, n2, axis, tw);
+  } else {
+    allow_smem(k_grid_lines<N, -1>, smem);
+    k_grid_lines<N, -1><<<nblocks, kGridThreads, smem, ctx.stream>>>(grid, n0, n1, n2, axis, tw);
+  }
+  QBX_LAUNCHED(ctx);
+}
+
 }  // namespace fast
+
+// Full-grid line FFTs of the lengths compiled in fft_fast_a.cu / fft_fast_b.cu;
+// false when the length along `axis` has no specialised kernel.
+bool fast_grid_lines_a(Context& ctx, double2* grid, int n0, int n1, int n2, int axis, int dir,
+                       const double2* tw);
+bool fast_grid_lines_b(Context& ctx, double2* grid, int n0, int n1, int n2, int axis, int dir,
+                       const double2* tw);
 
 // Specialised staged transforms for cubic grids of the lengths compiled in
 // fft_fast_a.cu / fft_fast_b.cu; each returns false when it has no kernel
@@ -645,4 +728,9 @@ bool fast_staged_b(Context& ctx, const fast::StagedArgs& a, size_t smem_limit);
       if (fast::smem_need<double, N>(ctx, a) > smem_limit) return false;      \
       fast::run_cubic<double, N>(ctx, a);                                     \
     }                                                                         \
+    return true;
+
+#define QBX_GRID_CASE(N)                                                      \
+  case N:                                                                     \
+    fast::run_grid_lines<N>(ctx, grid, n0, n1, n2, axis, dir, tw);            \
     return true;

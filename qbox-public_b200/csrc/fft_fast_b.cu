@@ -21,4 +21,21 @@ bool fast_staged_b(Context& ctx, const fast::StagedArgs& a, size_t smem_limit) {
   }
 }
 
+bool fast_grid_lines_b(Context& ctx, double2* grid, int n0, int n1, int n2, int axis, int dir,
+                       const double2* tw) {
+  const int n = axis == 0 ? n0 : axis == 1 ? n1 : n2;
+  switch (n) {
+    QBX_GRID_CASE(80)
+    QBX_GRID_CASE(84)
+    QBX_GRID_CASE(96)
+    QBX_GRID_CASE(112)
+    QBX_GRID_CASE(120)
+    QBX_GRID_CASE(128)
+    QBX_GRID_CASE(140)
+    QBX_GRID_CASE(144)
+    default:
+      return false;
+  }
+}
+
 }  // namespace qbx
