@@ -468,6 +468,11 @@ void upload_sticks(DeviceSticks& d, const Basis& b) {
   d.col_x = dupload(b.col_x);
   d.ip = dupload(b.ip);
   d.im = dupload(b.im);
+  {
+    std::vector<int> cm((size_t)b.ncol * b.n1, -1);
+    for (int s = 0; s < b.nvec; s++) cm[(size_t)b.stick_col[s] * b.n1 + b.stick_y[s]] = s;
+    d.colmap = dupload(cm);
+  }
   d.px = make_plan(b.n0);
   d.py = make_plan(b.n1);
   d.pz = make_plan(b.n2);
@@ -484,6 +489,7 @@ void free_sticks(DeviceSticks& d) {
   dfree(d.rod_first); dfree(d.rod_lmin); dfree(d.rod_size);
   dfree(d.stick_y); dfree(d.stick_col); dfree(d.col_x);
   dfree(d.ip); dfree(d.im);
+  dfree(d.colmap);
 }
 
 static const int kRodsPerCta = 8;
@@ -839,7 +845,7 @@ void autotune_fft(Context& ctx, std::vector<std::pair<std::string, double>>* log
     if (ctx.precision == MIXED && ctx.fast_lane_shape >= 0) {
       double best = 1e30;
       int pick = ctx.fast_density_lane_shape;
-      for (int s : {3, 2}) {
+      for (int s : {3, 2, 5}) {
         ctx.fast_density_lane_shape = s;
         const double t = time_ms(dens);
         note("density lane " + std::to_string(s), t);

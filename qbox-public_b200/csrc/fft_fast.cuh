@@ -483,6 +483,109 @@ kxy_lane(float2* __restrict__ zbuf, int npairs, int pairs_per_cta, DeviceSticks 
   }
 }
 
+// ------------------------------------------------------------ density,
+// half planes
+// The density pass of kxy_lane over one half of a plane's rows per CTA
+// (blockIdx.z = 0, 1).  Each half transforms every occupied column along y,
+// its inputs gathered straight from the stick buffer through the
+// (column, y) -> stick map, keeps the rows it owns (whole lanes of the
+// register distribution: lane ty holds rows MY*bitrev(ty) + k), transforms
+// those rows along x and accumulates f/Omega |psi|^2 into an FP32 half
+// plane.  Half the tile and half the accumulator fit two CTAs per SM, for
+// about 1.3x the line transforms of the whole-plane kernel.
+// shared memory: [twx N0][twy N1][P ncol x pitch(N1/2)][FP32 half plane
+// N1/2 x N0][xmap N0 ints]
+template <int N0, int N1>
+__host__ size_t xyh_smem_bytes(int ncol) {
+  constexpr int H = N1 / 2;
+  return sizeof(float2) * ((size_t)N0 + N1 + (size_t)ncol * pitch(H)) +
+         sizeof(float) * (size_t)H * N0 + sizeof(int) * (size_t)N0;
+}
+
+template <int N0, int N1>
+__global__ void __launch_bounds__(288, 2)
+kxy_lane_dh(const float2* __restrict__ zbuf, int npairs, int pairs_per_cta, DeviceSticks g,
+            const double2* __restrict__ twx_g, const double2* __restrict__ twy_g,
+            double* __restrict__ rho, const double* __restrict__ w, int pair0, int nst) {
+  using C = float2;
+  constexpr int TY = lane::lanes_for(N1), MY = N1 / TY;
+  constexpr int TX = lane::lanes_for(N0), MX = N0 / TX;
+  constexpr int H = N1 / 2, LDH = pitch(H);
+  static_assert(TX > 0 && (TY == 2 || TY == 4) && N1 % 2 == 0,
+                "no half-plane plan for this length");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int ncol = g.ncol, nvec = g.nvec;
+  C* twx = reinterpret_cast<C*>(smem_raw);
+  C* twy = twx + N0;
+  C* P = twy + N1;
+  float* acc = reinterpret_cast<float*>(P + (size_t)ncol * LDH);
+  int* xmap = reinterpret_cast<int*>(acc + (size_t)H * N0);
+  const int z = blockIdx.x, y0 = blockIdx.z * H;
+  load_tw(twx, twx_g, N0);
+  load_tw(twy, twy_g, N1);
+  for (int x = threadIdx.x; x < N0; x += blockDim.x) xmap[x] = -1;
+  for (int t = threadIdx.x; t < H * N0; t += blockDim.x) acc[t] = 0.f;
+  __syncthreads();
+  for (int cidx = threadIdx.x; cidx < ncol; cidx += blockDim.x) xmap[g.col_x[cidx]] = cidx;
+  const int ty = threadIdx.x % TY, gy = threadIdx.x / TY, sy = blockDim.x / TY;
+  const int tx = threadIdx.x % TX, gx = threadIdx.x / TX, sx = blockDim.x / TX;
+  const int mry = lane::bitrev(ty, TY), mrx = lane::bitrev(tx, TX);
+  const bool keep = (MY * mry >= y0) && (MY * mry < y0 + H);
+  const int pbeg = blockIdx.y * pairs_per_cta;
+  const int pend = min(npairs, pbeg + pairs_per_cta);
+#pragma unroll 1
+  for (int pl = pbeg; pl < pend; ++pl) {
+    const C* zp = zbuf + ((size_t)pl * g.n2 + z) * nvec;
+    // backward y on the occupied columns, inputs gathered from the sticks
+#pragma unroll 1
+    for (int base = 0; base < ncol; base += sy) {
+      const int cidx = base + gy;
+      const bool ok = cidx < ncol;
+      const int* cm = g.colmap + (size_t)(ok ? cidx : 0) * N1;
+      C val[MY];
+#pragma unroll
+      for (int k = 0; k < MY; ++k) {
+        const int s = ok ? __ldg(cm + ty + TY * k) : -1;
+        val[k] = s >= 0 ? zp[s] : cmk<C>(0.0, 0.0);
+      }
+      lane::line_n2r<TY, MY, +1>(val, ty, twy);
+      if (ok && keep) {
+        C* col = P + cidx * LDH + (MY * mry - y0);
+#pragma unroll
+        for (int k2 = 0; k2 < MY; ++k2) col[k2] = val[k2];
+      }
+    }
+    __syncthreads();
+    const int b1 = 2 * (pair0 + pl);
+    const float f1 = (float)w[b1];
+    const float f2 = (b1 + 1 < nst) ? (float)w[b1 + 1] : 0.f;
+    // backward x on this half's rows
+#pragma unroll 1
+    for (int base = 0; base < H; base += sx) {
+      const int yl = base + gx;
+      const bool ok = yl < H;
+      int txh = tx;
+      asm volatile("" : "+r"(txh));
+      C val[MX];
+#pragma unroll
+      for (int k = 0; k < MX; ++k) {
+        const int cidx = xmap[txh + TX * k];
+        val[k] = (ok && cidx >= 0) ? P[cidx * LDH + yl] : cmk<C>(0.0, 0.0);
+      }
+      lane::line_n2r<TX, MX, +1>(val, tx, twx);
+      if (ok) {
+        float* arow = acc + yl * N0 + MX * mrx;
+#pragma unroll
+        for (int k2 = 0; k2 < MX; ++k2)
+          arow[k2] += f1 * val[k2].x * val[k2].x + f2 * val[k2].y * val[k2].y;
+      }
+    }
+    __syncthreads();
+  }
+  const size_t pbase = ((size_t)z * N1 + y0) * N0;
+  for (int t = threadIdx.x; t < H * N0; t += blockDim.x) atomicAdd(&rho[pbase + t], (double)acc[t]);
+}
+
 // ------------------------------------------------------------ launch
 // Arguments of one batch of band pairs through the specialised kernels.
 struct StagedArgs {
@@ -499,7 +602,7 @@ struct StagedArgs {
   int xy_warps;            // requested warps per kxy CTA
   int vpsi_shape;          // FP32 H*psi plane CTA shape (xy_threads / xy_minblocks)
   int lane_shape;          // FP32 register-lane plane kernel shape, -1 = not used
-  int density_lane_shape;  // its density-pass shape (2 or 3)
+  int density_lane_shape;  // its density-pass shape (2, 3; 5 = half planes)
   int density_chunks;      // CTAs per plane in the density pass
 };
 
@@ -531,6 +634,26 @@ void launch_lane_xy(Context& ctx, const StagedArgs& a, int chunks, int ppc) {
   QBX_LAUNCHED(ctx);
 }
 
+template <int N>
+constexpr bool density_half_ok() {
+  return N % 2 == 0 && lane::lanes_for(N) >= 2 && lane::lanes_for(N) <= 4;
+}
+
+template <int N>
+void launch_density_half(Context& ctx, const StagedArgs& a, int chunks, int ppc) {
+  if constexpr (density_half_ok<N>()) {
+    const DeviceSticks& g = ctx.dws;
+    const size_t sm = xyh_smem_bytes<N, N>(g.ncol);
+    allow_smem(kxy_lane_dh<N, N>, sm);
+    const int T = lane::lanes_for(N);
+    const int want = std::max((g.ncol * T + 31) / 32 * 32, ((N / 2) * T + 31) / 32 * 32);
+    const int threads = std::max(64, std::min(288, want));
+    kxy_lane_dh<N, N><<<dim3(N, chunks, 2), threads, sm, ctx.stream>>>(
+        (const float2*)a.zbuf, a.npairs, ppc, g, a.twx, a.twy, a.rho, a.w, a.pair0, a.nst);
+    QBX_LAUNCHED(ctx);
+  }
+}
+
 template <typename T, int N>
 void run_cubic(Context& ctx, const StagedArgs& a) {
   using C = typename reg::CT<T>::c;
@@ -555,7 +678,8 @@ void run_cubic(Context& ctx, const StagedArgs& a) {
         const int ppc = (a.npairs + chunks - 1) / chunks;
         chunks = (a.npairs + ppc - 1) / ppc;
         ProfScope ps(ctx, "xy_density");
-        if (a.density_lane_shape == 3) launch_lane_xy<N, XY_DENSITY, 3>(ctx, a, chunks, ppc);
+        if (a.density_lane_shape == 5 && density_half_ok<N>()) launch_density_half<N>(ctx, a, chunks, ppc);
+        else if (a.density_lane_shape == 3) launch_lane_xy<N, XY_DENSITY, 3>(ctx, a, chunks, ppc);
         else launch_lane_xy<N, XY_DENSITY, 2>(ctx, a, chunks, ppc);
         return;
       }

@@ -124,6 +124,7 @@ struct DeviceSticks {
   RadixPlan px, py, pz;
   double2* tw[3];    // exp(+2 pi i k/n) for the x, y, z lengths (owned here,
                      // so contexts of different grids never share tables)
+  int* colmap;       // ncol x n1: the stick at (compact column, y), -1 if none
 };
 
 // -------------------------------------------------------------- species
@@ -380,7 +381,7 @@ struct Context {
   int fast_warps = 16;          // warps per CTA of the plane kernel (at most)
   int fast_vpsi_shape = 0;      // FP32 H*psi plane CTA shape (0, 1, 2)
   int fast_lane_shape = 4;      // FP32 register-lane plane kernel shape, -1 = off
-  int fast_density_lane_shape = 3;  // its density shape (2 or 3)
+  int fast_density_lane_shape = 3;  // its density shape (2, 3; 5 = half planes)
   int fast_chunks = 8;          // CTAs per plane in the density pass
   bool fast_fft = true;         // use the specialised kernels when compiled
   float* a32 = nullptr;         // TF32 hi/lo split of the projectors

@@ -78,3 +78,21 @@ def test_autotune_keeps_results(precision):
     np.testing.assert_allclose(rb, ra, rtol=0, atol=tol * np.abs(ra).max())
     np.testing.assert_allclose(hb, ha, rtol=0, atol=tol * np.abs(ha).max())
     a.close()
+
+
+@pytest.mark.parametrize("name", ["si8", "si64", "h2o32"])
+def test_density_half_planes(name, monkeypatch):
+    """The half-plane density kernel (two CTAs per plane, y inputs gathered
+    from the sticks) gives the whole-plane kernel's density (FP32, 2e-6 of
+    the largest value)."""
+    s = systems.get(name)
+    ref = _ctx(s, capi.MIXED, True)
+    monkeypatch.setenv("QBX_FAST_DENSITY_LANE_SHAPE", "5")
+    half = _ctx(s, capi.MIXED, True)
+    monkeypatch.delenv("QBX_FAST_DENSITY_LANE_SHAPE")
+    ref.update_density()
+    half.update_density()
+    ra, rb = ref.density(), half.density()
+    np.testing.assert_allclose(rb, ra, rtol=0, atol=2e-6 * np.abs(ra).max())
+    ref.close()
+    half.close()
