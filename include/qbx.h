@@ -145,6 +145,26 @@ int qbx_scf_step(qbx_context* ctx, int compute_forces, double* energies,
 int qbx_scf_step_batch(qbx_context** ctxs, int n, int compute_forces,
                        double* energies);
 
+/* The ground-state SCF loop of BOSampleStepper::step(0) with atoms fixed
+ * (src/BOSampleStepper.cpp:781-1114) and wf_dyn = PSDA: nitscf
+ * iterations.  With nite > 0 each iteration mixes the new density into the
+ * input density (AndersonMixer with mix_ndim history vectors,
+ * src/AndersonMixer.cpp, and Kerker weights of radius mix_rcut bohr with
+ * coefficient mix_coeff, src/BOSampleStepper.cpp:318-410, 805-881; the
+ * reference's charge_mix_ndim, charge_mix_rcut, charge_mix_coeff; mix_ndim 0
+ * mixes linearly), rebuilds the potentials and runs up to nite electronic
+ * steps, stopping when the eigenvalue sum moves less than 0.01 of the
+ * Hartree energy change; with nite = 0 each iteration is one qbx_scf_step
+ * without forces.  Stops early when the last three Harris-Foulkes energies
+ * lie within scf_tol.  Outputs (each may be NULL): etotal_int[nitscf]
+ * (Harris-Foulkes estimate per iteration, :1075-1101),
+ * eigsum[nitscf * max(nite,1)] (eigenvalue sum of each electronic step),
+ * nite_done[nitscf], nitscf_done (iterations run). */
+int qbx_scf_run(qbx_context* ctx, int nitscf, int nite, double mix_coeff,
+                double mix_rcut, int mix_ndim, double scf_tol,
+                double* etotal_int, double* eigsum, int* nite_done,
+                int* nitscf_done);
+
 /* AtomSet::set_positions followed by EnergyFunctional::atoms_moved
  * (src/EnergyFunctional.cpp:1047-1197): the same atoms at new positions
  * tau (species-major, 3 per atom, bohr).  Structure factors, local

@@ -126,6 +126,38 @@ def run_reference_md(sysdef, workdir: str, niter: int, nitscf: int, dt: float,
                 final_c=a[..., 0] + 1j * a[..., 1])
 
 
+def run_reference_gs(sysdef, workdir: str, nitscf: int, nite: int, mix_coeff: float = 0.5,
+                     mix_rcut: float = 10.0, mix_ndim: int = 3,
+                     threads: Optional[int] = None) -> Dict:
+    """The reference's BOSampleStepper::step(0): nitscf SCF iterations with
+    nite PSDA steps each and charge mixing.  Returns the printed etotal_int
+    of each iteration and eigenvalue sums of each electronic step
+    (8 decimals) and the final coefficients (full precision)."""
+    import re
+    if not os.path.exists(REF_DRIVER):
+        raise FileNotFoundError("oracle/_ref/ref_driver not built (make -C oracle)")
+    path = write_system(sysdef, workdir)
+    env = dict(os.environ)
+    if threads:
+        env["OMP_NUM_THREADS"] = str(threads)
+        env["OPENBLAS_NUM_THREADS"] = str(threads)
+    subprocess.run([REF_DRIVER, path, str(nitscf), workdir, "0", "0", "GS", str(nite),
+                    repr(float(mix_coeff)), repr(float(mix_rcut)), str(int(mix_ndim))],
+                   check=True, env=env, stdout=subprocess.DEVNULL)
+    log = open(os.path.join(workdir, "gs_log.txt")).read()
+
+    def tag(name):
+        return np.array([float(x) for x in re.findall(rf"<{name}>\s*(\S+)\s*</{name}>", log)])
+    meta = {}
+    with open(os.path.join(workdir, "meta.txt")) as fm:
+        for line in fm:
+            k, v = line.split()
+            meta[k] = int(v)
+    a = np.fromfile(os.path.join(workdir, "final_c.bin")).reshape(meta["nst"], meta["ngw"], 2)
+    return dict(etotal_int=tag("etotal_int"), eigenvalue_sum=tag("eigenvalue_sum"),
+                final_c=a[..., 0] + 1j * a[..., 1])
+
+
 def load_outputs(workdir: str) -> Dict:
     out: Dict = {}
     meta = {}

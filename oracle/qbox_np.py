@@ -642,6 +642,12 @@ class ElectronicStep:
         self.total_charge = rho.sum() * self.omega / self.N
         self.rhog = self.vgrid.forward(self.omega * rho)
 
+    def update_rhor(self):
+        """ChargeDensity::update_rhor (src/ChargeDensity.cpp:201-240):
+        rho(r) = Re FFT_bwd(rho(G)) / Omega from the (mixed) rho(G)."""
+        self.rhor = self.vgrid.backward(self.rhog).real.ravel() / self.omega
+        self.total_charge = self.rhor.sum() * self.omega / self.N
+
     # ---- potentials (src/EnergyFunctional.cpp:231-394, XCPotential:124-465)
     def update_vhxc(self):
         vb, om = self.vb, self.omega
@@ -668,6 +674,8 @@ class ElectronicStep:
             vxc = v1 + vxt
             self.exc = (rho * e).sum() * om / self.N
             self.xc_parts = (e, v1, v2, grads)
+        # dxc = sum rho (e_xc - v_xc) Omega / N (src/XCPotential.cpp:199-229, 376-423)
+        self.dxc = (rho * (e - vxc)).sum() * om / self.N
         g0 = vb.g0()
         eps = 2.0 * (np.conj(rhoelg) * self.vion_g).real.sum()
         eps -= (np.conj(rhoelg[g0]) * self.vion_g[g0]).real
@@ -675,6 +683,9 @@ class ElectronicStep:
         rt = rhoelg + self.rhops_t
         self.rhogt = rt
         self.ehart = om * FPI * (np.abs(rt) ** 2 * vb.g2i).sum()
+        # electronic and pseudocharge parts (src/EnergyFunctional.cpp:320-351)
+        self.ehart_e = om * FPI * (np.abs(rhoelg) ** 2 * vb.g2i).sum()
+        self.ehart_p = om * FPI * (np.abs(self.rhops_t) ** 2 * vb.g2i).sum()
         vloc_g = self.vion_g + FPI * rt * vb.g2i
         self.v_r = vxc + self.vgrid.backward(vloc_g).real.ravel()
 
@@ -926,6 +937,126 @@ class ElectronicStep:
 
 
 AMU = 1822.89      # atomic mass unit in electron masses, src/IonicStepper.cpp:40
+
+
+class AndersonMixer:
+    """src/AndersonMixer.cpp:28-256 with diag = true, eig_ratio = 0: history
+    of nmax+1 (x, f) pairs; theta solves the least-squares system on the
+    differences to the newest f through the positive eigenvalues of its
+    normal matrix."""
+
+    def __init__(self, m: int, nmax: int):
+        self.m, self.nmax = m, nmax
+        self.x = [None] * (nmax + 1)
+        self.f = [None] * (nmax + 1)
+        self.restart()
+
+    def restart(self):
+        self.n, self.k = -1, -1
+
+    def update(self, x, f):
+        nmax = self.nmax
+        self.k = (self.k + 1) % (nmax + 1)
+        if self.n < nmax:
+            self.n += 1
+        k, n = self.k, self.n
+        self.x[k] = x.copy()
+        self.f[k] = f.copy()
+        theta = np.zeros(n)
+        if n > 0:
+            km = [(k - i + nmax) % (nmax + 1) for i in range(n)]
+            d = [self.f[k] - self.f[j] for j in km]
+            a = np.array([[d[i] @ d[j] for j in range(n)] for i in range(n)])
+            b = np.array([d[i] @ self.f[k] for i in range(n)])
+            w, u = np.linalg.eigh(a)
+            for kk in range(n):
+                if w[kk] > 0.0 * w[n - 1]:
+                    theta += (u[:, kk] @ b / w[kk]) * u[:, kk]
+        xbar = self.x[k].copy()
+        fbar = self.f[k].copy()
+        for i in range(n):
+            j = (k - i + nmax) % (nmax + 1)
+            fbar -= theta[i] * (self.f[k] - self.f[j])
+            xbar -= theta[i] * (self.x[k] - self.x[j])
+        return xbar, fbar
+
+
+def scf_run(es: "ElectronicStep", nitscf: int, nite: int, mix_coeff: float = 0.5,
+            mix_rcut: float = 10.0, mix_ndim: int = 3, scf_tol: float = 0.0):
+    """The SCF loop of BOSampleStepper::step(0) (ground state, atoms fixed,
+    src/BOSampleStepper.cpp:781-1114) with wf_dyn = PSDA: nitscf iterations,
+    each an update of the density (mixed with the Anderson mixer and the
+    Kerker weights when nite > 0, :805-881), of the potentials, and up to
+    nite electronic steps (stopping early when the eigenvalue sum moves less
+    than 0.01 of the Hartree energy change, :903-980); the Harris-Foulkes
+    estimate etotal_int per iteration (:1075-1101).
+
+    Returns {"etotal_int": [...], "eigenvalue_sum": [...], "nite_done": [...]}."""
+    vb = es.vb
+    g2 = vb.g2
+    q1 = 2.0 * math.pi / 3.0                                        # rc1 = 3 (:344-386)
+    wls = np.where(g2 != 0.0, np.sqrt(g2 / np.where(g2 != 0.0, g2 + q1 * q1, 1.0)), 1.0)
+    if mix_rcut > 0.0:
+        q0 = 2.0 * math.pi / mix_rcut
+        wk = np.where(g2 != 0.0, g2 / (g2 + q0 * q0), 1.0)         # (:391-407)
+    else:
+        wk = np.ones_like(g2)
+    mixer = AndersonMixer(2 * vb.size, mix_ndim) if mix_ndim > 0 else None
+    es.extrapolate = False                                           # preprocess (:785)
+    out = {"etotal_int": [], "eigenvalue_sum": [], "nite_done": []}
+    rhog_in = None
+    ehart = ehart_m = delta_ehart = 0.0
+    etotal = etotal_m = etotal_mm = 0.0
+    for itscf in range(nitscf):
+        es.update_density()
+        if nite > 0:
+            if itscf == 0:
+                rhog_in = es.rhog.copy()
+            else:
+                drhog = es.rhog - rhog_in
+                if mixer is not None:
+                    dr = (drhog / wls).view(np.float64)
+                    xbar, fbar = mixer.update(rhog_in.view(np.float64).copy(), dr.copy())
+                    rhobar = xbar.view(np.complex128)
+                    drhobar = fbar.view(np.complex128) * wls
+                    rhog_in = rhobar + mix_coeff * drhobar * wk
+                else:
+                    rhog_in = rhog_in + mix_coeff * drhog * wk
+                es.rhog = rhog_in.copy()
+                es.update_rhor()
+        es.update_vhxc()
+        if nite > 0:
+            es.extrapolate = False                                   # (:897)
+        if itscf == 0:
+            ehart = es.ehart
+            delta_ehart = 0.0
+        elif itscf == 1:
+            ehart_m, ehart = ehart, es.ehart
+            delta_ehart = abs(ehart - ehart_m)
+        else:
+            ehart_m, ehart = ehart, es.ehart
+            delta_ehart = min(delta_ehart, abs(ehart - ehart_m))
+        ite = 0
+        conv = False
+        eig = eig_m = 0.0
+        while not conv and ite < max(nite, 1):
+            es.energy(True)
+            if ite > 0:
+                eig_m = eig
+            eig = es.eigenvalue_sum()
+            out["eigenvalue_sum"].append(eig)
+            es.psda_update()
+            if ite > 0:
+                conv = abs(eig - eig_m) < 0.01 * delta_ehart
+            ite += 1
+        out["nite_done"].append(ite)
+        eint = 2.0 * eig - es.ehart_e + es.ehart_p + es.esr - es.eself + es.dxc
+        out["etotal_int"].append(eint)
+        etotal_mm, etotal_m, etotal = etotal_m, etotal, eint
+        d = max(abs(etotal - etotal_m), abs(etotal - etotal_mm), abs(etotal_m - etotal_mm))
+        if d < scf_tol:
+            break
+    return out
 
 
 def md_run(es: "ElectronicStep", niter: int, nitscf: int, dt: float, masses):

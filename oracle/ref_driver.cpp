@@ -12,6 +12,12 @@
 //
 // usage: ref_driver <system.txt> <nsteps> <outdir> [dump_steps=0]
 //                   [forces=0] [wf_dyn=PSDA] [nitscf dt]
+//        ref_driver <system.txt> <nitscf> <outdir> 0 0 GS <nite> <mix_coeff>
+//                   <mix_rcut> <mix_ndim>
+// wf_dyn = GS runs the reference's BOSampleStepper::step(0) (ground state,
+// atoms fixed) with nitscf SCF iterations of nite PSDA steps each and the
+// given charge mixing (charge_mix_coeff, charge_mix_rcut, charge_mix_ndim);
+// its log goes to gs_log.txt and the final coefficients to final_c.bin.
 // wf_dyn = MD runs the reference's own BOSampleStepper::step(nsteps)
 // (src/BOSampleStepper.cpp:165-1428) with atoms_dyn = MD, wf_dyn = PSDA,
 // nitscf electronic steps per ionic step, nite = 0 and the time step dt
@@ -195,6 +201,33 @@ int main(int argc, char** argv)
       c[ig + (size_t)n*mloc] = complex<double>(cin[src], cin[src+1]);
     }
   s.wf.gram();
+
+  if ( wf_dyn == "GS" )
+  {
+    const int nite = argc > 7 ? atoi(argv[7]) : 0;
+    s.ctrl.charge_mix_coeff = argc > 8 ? atof(argv[8]) : 0.5;
+    s.ctrl.charge_mix_rcut = argc > 9 ? atof(argv[9]) : 10.0;
+    s.ctrl.charge_mix_ndim = argc > 10 ? atoi(argv[10]) : 3;
+    ofstream log((outdir + "/gs_log.txt").c_str());
+    streambuf* saved = cout.rdbuf(log.rdbuf());
+    {
+      BOSampleStepper stepper(s, nsteps, nite);
+      stepper.step(0);
+    }
+    cout.rdbuf(saved);
+    vector<double> out(2*(size_t)ngw*nst);
+    for ( int n = 0; n < nst; n++ )
+      for ( int ig = 0; ig < ngw; ig++ )
+      {
+        const complex<double> v = c[ig + (size_t)n*mloc];
+        const size_t dst = 2*((size_t)n*ngw + perm[ig]);
+        out[dst] = v.real(); out[dst+1] = v.imag();
+      }
+    write_bin(outdir + "/final_c.bin", &out[0], out.size()*sizeof(double));
+    ofstream meta((outdir + "/meta.txt").c_str());
+    meta << "ngw " << ngw << "\nnst " << nst << "\nnatoms " << atom_count << "\n";
+    return 0;
+  }
 
   if ( wf_dyn == "MD" )
   {

@@ -64,6 +64,7 @@ void drop_graphs(Context& c) {
 void free_cell(Context& c) {
   drop_graphs(c);
   free_mixed(c);
+  free_mix(c);
   free_sticks(c.dws);
   free_sticks(c.dvs);
   double** bufs[] = {&c.d_gx_w, &c.d_g2_w, &c.d_gx_v, &c.d_g2i_v, &c.d_c, &c.d_hc, &c.d_c_last,
@@ -764,6 +765,18 @@ int qbx_scf_step(qbx_context* h, int forces, double* energies, double* fion) {
   return guarded(h, [&](Context& c) {
     check_ready(c, true);
     scf_step_any(c, (forces & 1) != 0, (forces & 2) != 0, energies, fion);
+  });
+}
+
+int qbx_scf_run(qbx_context* h, int nitscf, int nite, double mix_coeff, double mix_rcut,
+                int mix_ndim, double scf_tol, double* etotal_int, double* eigsum,
+                int* nite_done, int* nitscf_done) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, true);
+    QBX_REQUIRE(nitscf > 0 && nite >= 0 && mix_coeff >= 0.0 && mix_rcut >= 0.0, 1,
+                "bad SCF arguments");
+    scf_run(c, nitscf, nite, mix_coeff, mix_rcut, mix_ndim, scf_tol, etotal_int, eigsum,
+            nite_done, nitscf_done);
   });
 }
 

@@ -209,6 +209,12 @@ __global__ void k_axpy(double* __restrict__ y, const double* __restrict__ x, siz
     y[i] += x[i];
 }
 
+// sum_i x_i y_i
+struct DotF {
+  const double* x; const double* y;
+  __device__ void operator()(size_t i, double* a) const { a[0] += x[i] * y[i]; }
+};
+
 // sum of the energy density and of rho * v1
 struct SumRhoV1F {
   const double* e; const double* rho; const double* v1;
@@ -227,6 +233,7 @@ void launch_xc(Context& ctx) {
     k_lda<<<nb, kThreads, 0, ctx.stream>>>(ctx.d_rhor, N, ctx.d_vxc, ctx.d_exc);
     QBX_LAUNCHED(ctx);
     launch_sum(ctx, ctx.d_exc, N, SLOT_EXC);
+    reduce<1>(ctx, DotF{ctx.d_rhor, ctx.d_vxc}, N, SLOT_EXC + 2);   // for dxc
     return;
   }
   // PBE: grad rho by three backward transforms of i G_j rho(G)/Omega
@@ -256,6 +263,7 @@ void launch_xc(Context& ctx) {
     k_axpy<<<nb, kThreads, 0, ctx.stream>>>(ctx.d_vxc, ctx.d_exc, N);
     QBX_LAUNCHED(ctx);
   }
+  reduce<1>(ctx, DotF{ctx.d_rhor, ctx.d_vxc}, N, SLOT_EXC + 2);   // for dxc
 }
 
 // ---------------------------------------------------- Hartree and local
@@ -267,8 +275,12 @@ struct EpsEhF {
     const double2 v = vion[i];
     const double f = (i == 0) ? 1.0 : 2.0;     // G=0 counted once
     a[0] += f * (r.x * v.x + r.y * v.y);
-    const double2 t = make_double2(r.x + rhops[i].x, r.y + rhops[i].y);
-    a[1] += (t.x * t.x + t.y * t.y) * g2i[i];
+    const double2 p = rhops[i];
+    const double2 t = make_double2(r.x + p.x, r.y + p.y);
+    const double gi = g2i[i];
+    a[1] += (t.x * t.x + t.y * t.y) * gi;
+    a[2] += (r.x * r.x + r.y * r.y) * gi;      // electrons alone
+    a[3] += (p.x * p.x + p.y * p.y) * gi;      // pseudocharges alone
   }
 };
 
@@ -288,7 +300,7 @@ __global__ void k_vlocal_g(const double2* __restrict__ rhog, const double2* __re
 void launch_vhxc_gspace(Context& ctx) {
   const int ngv = ctx.vb.ng;
   const double om = ctx.vb.omega;
-  reduce<2>(ctx, EpsEhF{(const double2*)ctx.d_rhog, (const double2*)ctx.d_vion,
+  reduce<4>(ctx, EpsEhF{(const double2*)ctx.d_rhog, (const double2*)ctx.d_vion,
                         (const double2*)ctx.d_rhops, ctx.d_g2i_v, 1.0 / om},
             (size_t)ngv, SLOT_EPS_EH);
   k_vlocal_g<<<blocks_for(ngv), kThreads, 0, ctx.stream>>>(

@@ -212,17 +212,19 @@ struct Profiler {
 // a step can be captured as one CUDA graph.
 enum : int {
   SLOT_CHARGE = 0,     // sum_r rho(r)
-  SLOT_EXC = 1,        // sum_r e_xc(r), sum_r rho v1 (PBE)
-  SLOT_EPS_EH = 3,     // sum rho*(G) vion(G), sum |rho_tot(G)|^2 / G^2
-  SLOT_EKIN = 5,
-  SLOT_ENL = 6,
-  SLOT_EIG = 7,
-  SLOT_ANDERSON = 8,   // the two sums of the Anderson theta
-  SLOT_THETA = 10,     // theta used by the last PSDA step
-  SLOT_FROB = 11,      // ||I - x^T x||_F^2 of the current polar iterate
+  SLOT_EXC = 1,        // sum_r e_xc(r), sum_r rho v1 (PBE), sum_r rho v_xc
+  SLOT_EPS_EH = 4,     // sum rho*(G) vion(G); sum |G|^-2 times |rho_tot|^2,
+                       // |rho_e|^2, |rho_ps|^2 (total, electronic, pseudocharge)
+  SLOT_EKIN = 8,
+  SLOT_ENL = 9,
+  SLOT_EIG = 10,
+  SLOT_ANDERSON = 11,  // the two sums of the Anderson theta
+  SLOT_THETA = 13,     // theta used by the last PSDA step
+  SLOT_FROB = 14,      // ||I - x^T x||_F^2 of the current polar iterate
   SLOT_STRESS = 16,    // 30 sums of the stress tensor parts
   SLOT_SCRATCH = 56,   // one-off sums
-  kSlots = 64
+  SLOT_MIX = 64,       // the normal matrix and right-hand side of the charge mixer
+  kSlots = 128
 };
 // Device status words of a step (int): solver info codes, the polar
 // iteration count and the tcgen05 wait-timeout flag.
@@ -348,6 +350,13 @@ struct Context {
   double sigma_parts[36] = {0};  // ekin, eps, enl, ehart, exc, esr (6 each)
   bool have_stress = false;
   double xc_rhov1 = 0;          // sum_r rho v1 of the last PBE update (stress)
+  double dxc = 0, ehart_e = 0, ehart_p = 0;   // Harris-Foulkes terms of update_vhxc
+  // charge mixing of the SCF loop with nite > 0 (scf.cu)
+  double* d_rhog_in = nullptr;  // 2*ngv: the mixed rho(G)
+  double* d_mix = nullptr;      // 2*(ndim+1) vectors of 2*ngv: Anderson x and f history
+  double* d_wmix = nullptr;     // 2*ngv: least-squares weights, Kerker weights
+  int mix_ndim = -1;            // history length the buffers were made for
+  double mix_rcut = -1.0;
   double* d_dvps = nullptr;     // ngv*nsp: dV_loc/dG / Omega per species
   double* d_vnl = nullptr;      // nrad*ngw: radial projector V_nl(|G|)
   double* d_dvnl = nullptr;     // nrad*ngw: dV_nl/dG
@@ -551,6 +560,11 @@ int polar_entry(Context& ctx, double* x, double tol, int maxiter, bool graph);
 void scf_step_any(Context& c, bool want_f, bool want_s, double* energies, double* fion);
 void align_to_c(Context& ctx, double* cv);   // SlaterDet::align of cv to C
 void lowdin(Context& ctx);                     // SlaterDet::lowdin of C
+// SCF loop with charge mixing (scf.cu); energies as arrays of the
+// iterations (see qbx_scf_run)
+void scf_run(Context& c, int nitscf, int nite, double mix_coeff, double mix_rcut, int mix_ndim,
+             double scf_tol, double* etotal_int, double* eigsum, int* nite_done, int* nitscf_done);
+void free_mix(Context& c);
 // molecular dynamics (md.cu)
 void move_atoms(Context& c, const double* tau);
 void md_run(Context& c, int niter, int nitscf, double dt, const double* mass_amu, double* vel,

@@ -53,8 +53,12 @@ void finish_vhxc(Context& ctx) {
   const double om = ctx.vb.omega;
   ctx.exc = ctx.h_scalars[SLOT_EXC] * om / (double)ctx.N();
   ctx.xc_rhov1 = ctx.xc == "LDA" ? 0.0 : ctx.h_scalars[SLOT_EXC + 1];
+  // dxc = Omega/N sum rho (e_xc - v_xc) (src/XCPotential.cpp:199-229, 376-423)
+  ctx.dxc = ctx.exc - ctx.h_scalars[SLOT_EXC + 2] * om / (double)ctx.N();
   ctx.eps = ctx.h_scalars[SLOT_EPS_EH] * om;
   ctx.ehart = om * 4.0 * M_PI * ctx.h_scalars[SLOT_EPS_EH + 1];
+  ctx.ehart_e = om * 4.0 * M_PI * ctx.h_scalars[SLOT_EPS_EH + 2];
+  ctx.ehart_p = om * 4.0 * M_PI * ctx.h_scalars[SLOT_EPS_EH + 3];
 }
 
 // EnergyFunctional::energy (src/EnergyFunctional.cpp:397-1044): the total

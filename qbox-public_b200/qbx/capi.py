@@ -38,7 +38,7 @@ SYMBOLS = (
     "qbx_set_gemm_backend", "qbx_split_gemm_tn", "qbx_density_static",
     "qbx_stress", "qbx_get_stress", "qbx_autotune", "qbx_set_wf_dyn", "qbx_jd_update",
     "qbx_scf_step_batch", "qbx_set_step_graph", "qbx_step_graph_info", "qbx_polar",
-    "qbx_move_atoms", "qbx_md_run",
+    "qbx_move_atoms", "qbx_md_run", "qbx_scf_run",
 )
 
 _lib = None
@@ -110,6 +110,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "qbx_get_stress": (_I, [_P, _DP, _DP]),
         "qbx_set_step_graph": (_I, [_P, _I]),
         "qbx_move_atoms": (_I, [_P, _DP]),
+        "qbx_scf_run": (_I, [_P, _I, _I, _D, _D, _I, _D, _DP, _DP, _IP, _IP]),
         "qbx_md_run": (_I, [_P, _I, _I, _D, _DP, _DP, _DP, _DP, _DP]),
         "qbx_polar": (_I, [_P, _DP, _D, _I, _I, ctypes.POINTER(_I)]),
         "qbx_step_graph_info": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_long),
@@ -339,6 +340,23 @@ class Context:
         self._ok(self.lib.qbx_polar(self.h, _dp(a.reshape(-1, order="F")), tol, maxiter,
                                     int(graph), ctypes.byref(it)), "polar")
         return a, it.value
+
+    def scf_run(self, nitscf: int, nite: int, mix_coeff: float = 0.5, mix_rcut: float = 10.0,
+                mix_ndim: int = 3, scf_tol: float = 0.0):
+        """qbx_scf_run: the ground-state SCF loop with charge mixing.
+        Returns {"etotal_int": (iterations,), "eigenvalue_sum": list per
+        electronic step run, "nite_done": (iterations,)}."""
+        ns = max(nite, 1)
+        eint = np.zeros(nitscf)
+        eig = np.zeros(nitscf * ns)
+        nd = np.zeros(nitscf, np.int32)
+        done = ctypes.c_int()
+        self._ok(self.lib.qbx_scf_run(self.h, nitscf, nite, mix_coeff, mix_rcut, mix_ndim,
+                                      scf_tol, _dp(eint), _dp(eig), _ip(nd),
+                                      ctypes.byref(done)), "scf_run")
+        n = done.value
+        sums = [eig[i * ns + j] for i in range(n) for j in range(int(nd[i]))]
+        return {"etotal_int": eint[:n], "eigenvalue_sum": np.array(sums), "nite_done": nd[:n]}
 
     def move_atoms(self, tau: np.ndarray):
         """qbx_move_atoms: the same atoms at new positions (species-major)."""

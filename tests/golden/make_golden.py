@@ -9,8 +9,9 @@ basis size, a fixed sample of the density and local potential on the grid,
 H*psi and wavefunction coefficients of a few bands (all G for small bases,
 a fixed sample of G otherwise), and per-band norms.
 The fixtures pin the numpy oracle (oracle/qbox_np.py) in tests/test_oracle.py.
-ref_<name>_jd.npz holds a JD-stepper run and ref_<name>_md.npz a molecular
-dynamics run of the reference's BOSampleStepper.
+ref_<name>_jd.npz holds a JD-stepper run, ref_<name>_md.npz a molecular
+dynamics run and ref_<name>_gs.npz a ground-state SCF run with charge mixing
+of the reference's BOSampleStepper.
 """
 from __future__ import annotations
 
@@ -105,13 +106,41 @@ def make_md(name: str, workdir: str) -> str:
     np.savez_compressed(path, **fx)
     return path
 
+# SCF with charge mixing: (nitscf, nite, charge_mix_coeff, charge_mix_rcut,
+# charge_mix_ndim)
+GS_CASES = {"si8": (10, 4, 0.5, 10.0, 3), "si64": (3, 2, 0.5, 10.0, 3)}
+
+
+def make_gs(name: str, workdir: str) -> str:
+    """The ground-state SCF loop with nite > 0 and Anderson/Kerker charge
+    mixing through the reference's own BOSampleStepper: printed
+    etotal_int per SCF iteration and eigenvalue sums per electronic step,
+    final coefficients of a few bands."""
+    nitscf, nite, coeff, rcut, ndim = GS_CASES[name]
+    s = systems.get(name)
+    out = inputs.run_reference_gs(s, workdir, nitscf, nite, coeff, rcut, ndim,
+                                  threads=os.cpu_count())
+    ngw = out["final_c"].shape[1]
+    gidx = np.arange(ngw) if ngw <= 2000 else np.sort(
+        np.random.default_rng(12345).choice(ngw, 512, replace=False))
+    fx = dict(nitscf=nitscf, nite=nite, mix_coeff=coeff, mix_rcut=rcut, mix_ndim=ndim,
+              etotal_int=out["etotal_int"], eigenvalue_sum=out["eigenvalue_sum"], g_idx=gidx,
+              final_c_bands=out["final_c"][:NBANDS_FULL, gidx],
+              final_c_norm2=(np.abs(out["final_c"]) ** 2).sum(1))
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), f"ref_{name}_gs.npz")
+    np.savez_compressed(path, **fx)
+    return path
+
+
 if __name__ == "__main__":
     import tempfile
     names = sys.argv[1:] or (list(CASES) + [n + "_jd" for n in JD_CASES]
-                             + [n + "_md" for n in MD_CASES])
+                             + [n + "_md" for n in MD_CASES] + [n + "_gs" for n in GS_CASES])
     for n in names:
         with tempfile.TemporaryDirectory() as td:
-            if n.endswith("_md"):
+            if n.endswith("_gs"):
+                print(make_gs(n[:-3], td))
+            elif n.endswith("_md"):
                 print(make_md(n[:-3], td))
             elif n.endswith("_jd"):
                 print(make_jd(n[:-3], JD_CASES[n[:-3]], td))

@@ -190,3 +190,20 @@ def test_oracle_md_matches_reference():
     np.testing.assert_allclose(c[:fx["final_c_bands"].shape[0]], fx["final_c_bands"], rtol=0,
                                atol=1e-11)
     np.testing.assert_allclose((np.abs(c) ** 2).sum(1), fx["final_c_norm2"], rtol=1e-11)
+
+
+def test_oracle_scf_mixing_matches_reference():
+    """qbox_np.scf_run (BOSampleStepper::step(0) with nite > 0, Anderson and
+    Kerker charge mixing) against the reference's own stepper: printed
+    etotal_int and eigenvalue sums to their 8 decimals, final coefficients
+    to rounding."""
+    fx = golden("si8_gs")
+    s = systems.si8()
+    es = qbox_np.ElectronicStep(s)
+    out = qbox_np.scf_run(es, int(fx["nitscf"]), int(fx["nite"]), float(fx["mix_coeff"]),
+                          float(fx["mix_rcut"]), int(fx["mix_ndim"]))
+    np.testing.assert_allclose(out["etotal_int"], fx["etotal_int"], rtol=0, atol=6e-9)
+    np.testing.assert_allclose(out["eigenvalue_sum"], fx["eigenvalue_sum"], rtol=0, atol=6e-9)
+    g = fx["g_idx"]
+    np.testing.assert_allclose(es.c[:fx["final_c_bands"].shape[0], g], fx["final_c_bands"],
+                               rtol=0, atol=1e-11)
