@@ -46,10 +46,8 @@ WORKLOAD = ("si512: 512-atom Si-like diamond cell a=41.04 bohr, Gamma, 25 Ry, "
 
 
 def dist_env():
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return rank, world, local
+    from qbx import replicas
+    return replicas.dist_env()
 
 
 # ---------------------------------------------------------------- clocks
@@ -176,12 +174,10 @@ def run_ours(args):
     import torch
     from qbx import capi, systems
 
+    from qbx import replicas
     rank, world, local = dist_env()
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     torch.cuda.set_device(local)
+    replicas.init("nccl")
     dev = local
 
     s = systems.si512()
@@ -193,8 +189,7 @@ def run_ours(args):
         stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
         start = torch.cuda.Event(enable_timing=True)
         end = torch.cuda.Event(enable_timing=True)
-        if world > 1:
-            torch.distributed.barrier()
+        replicas.barrier(device=f"cuda:{dev}")
         torch.cuda.synchronize()
         if profile:
             ctx.profile(True)
@@ -210,16 +205,13 @@ def run_ours(args):
         end.record(stream)
         end.synchronize()
         torch.cuda.synchronize()
+        replicas.barrier(device=f"cuda:{dev}")
         ms = start.elapsed_time(end) / nsteps
         launches = ctx.launch_count() - n0
         return ms, r, launches
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], device=f"cuda:{dev}", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x, device=f"cuda:{dev}")
 
     # ---- mixed precision (headline)
     mix = capi.from_system(s, device=dev, precision=capi.MIXED, coeffs=c0)
@@ -334,9 +326,49 @@ def run_ours(args):
         mix.profile(False)
     mix.close()
 
+    # ---- the 32-system batch (small cells of uneven size), split over the
+    # ranks, captured steps launched together (qbx_scf_step_batch)
+    batch = None
+    if args.batch_steps > 0:
+        systs = systems.batch()
+        mine = [systs[i] for i in replicas.shard(len(systs), rank, world)]
+        bctx = [capi.from_system(x, device=dev, precision=capi.MIXED) for x in mine]
+        for c in bctx:
+            c.set_step_graph(True)
+        for _ in range(3):
+            capi.scf_step_batch(bctx)          # first use, capture, warm
+        torch.cuda.synchronize()
+        replicas.barrier(device=f"cuda:{dev}")
+        b0 = torch.cuda.Event(enable_timing=True)
+        b1 = torch.cuda.Event(enable_timing=True)
+        b0.record()
+        for _ in range(args.batch_steps):
+            capi.scf_step_batch(bctx)          # returns when every system is done
+        b1.record()
+        b1.synchronize()
+        bms = b0.elapsed_time(b1) / args.batch_steps
+        seq0 = torch.cuda.Event(enable_timing=True)
+        seq1 = torch.cuda.Event(enable_timing=True)
+        seq0.record()
+        for c in bctx:
+            c.scf_step()
+        seq1.record()
+        seq1.synchronize()
+        batch = {"systems": len(systs), "systems_this_rank": len(mine),
+                 "ms_per_batched_step": bms,
+                 "ms_one_after_another": seq0.elapsed_time(seq1),
+                 "what": ("one mixed electronic step of each system (8-64 atoms, 20-30 Ry, "
+                          "bands = 2 x atoms), captured steps launched on one stream each")}
+        for c in bctx:
+            c.close()
+        replicas.barrier(device=f"cuda:{dev}")
+
     ms_mix = max_over_ranks(ms_mix)
     ms_f64 = max_over_ranks(ms_f64)
     ms_e2e = max_over_ranks(ms_e2e)
+    if batch is not None:
+        batch["ms_per_batched_step"] = max_over_ranks(batch["ms_per_batched_step"])
+        batch["ms_one_after_another"] = max_over_ranks(batch["ms_one_after_another"])
 
     if rank == 0:
         cpu = None
@@ -359,6 +391,7 @@ def run_ours(args):
             "step_graph": {"captured": graphs, "launches": graph_launches, "note": graph_note,
                            "eager_ms_per_step": ms_mix_eager},
             "md": md,
+            "batch": batch,
             "mixed_vs_fp64_speedup": ms_f64 / ms_mix,
             "dE_per_atom": de_atom,
             "dE_definition": ("|E_mixed - E_fp64| / atoms for one electronic step of both paths "
@@ -380,9 +413,7 @@ def run_ours(args):
             "clocks": clk,
         }
         print(json.dumps(line))
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    replicas.finalize()
 
 
 def run_profile_case(args):
@@ -419,6 +450,8 @@ def main():
                     help="ionic steps of the molecular-dynamics measurement (0: skip)")
     ap.add_argument("--md-nitscf", type=int, default=1,
                     help="electronic steps per ionic step in the MD measurement")
+    ap.add_argument("--batch-steps", type=int, default=3,
+                    help="timed steps of the 32-system batch measurement (0: skip)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--profile-bands", type=int, default=0,
                     help="run only warm-up + one mixed step of si512 with this many bands "
