@@ -249,7 +249,7 @@ def run_ours(args):
         pass
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     achieved = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9
-    roofline = {"kernel": "kxy_lane<140,140,VPSI> (plane pass of H*psi, register-lane FFTs)",
+    roofline = {"kernel": "kxy_lane_map<140,140> (plane pass of H*psi, register-lane FFTs)",
                 "bound": "hbm",
                 "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                 "frac": achieved / hbm_peak,

@@ -464,9 +464,10 @@ int qbx_set_cell(qbx_context* h, const double cell[9], double ecut, int nst, con
       c.fast_batch = 16;
       if (const char* e = std::getenv("QBX_FAST_BATCH")) c.fast_batch = std::max(0, std::atoi(e));
       if (const char* e = std::getenv("QBX_FAST_LANE_SHAPE"))
-        c.fast_lane_shape = std::max(-1, std::min(4, std::atoi(e)));
+        c.fast_lane_shape = std::max(-1, std::min(6, std::atoi(e)));
       if (const char* e = std::getenv("QBX_FAST_DENSITY_LANE_SHAPE"))
-        c.fast_density_lane_shape = std::atoi(e) == 3 ? 3 : std::atoi(e) == 5 ? 5 : 2;
+        c.fast_density_lane_shape = (std::atoi(e) == 3 || std::atoi(e) == 5 || std::atoi(e) == 6)
+                                        ? std::atoi(e) : 2;
       if (const char* e = std::getenv("QBX_FAST_VPSI_SHAPE"))
         c.fast_vpsi_shape = std::max(0, std::min(2, std::atoi(e)));
     }
@@ -993,7 +994,8 @@ int qbx_autotune(qbx_context* h, char* report, int report_len) {
       for (auto& e : log) r += e.first + ": " + std::to_string(e.second) + " ms\n";
       r += "chosen: lane " + std::to_string(c.fast_lane_shape) + ", warp " +
            std::to_string(c.fast_vpsi_shape) + ", density lane " +
-           std::to_string(c.fast_density_lane_shape) + ", pairs " +
+           std::to_string(c.fast_density_lane_shape) + " x " + std::to_string(c.fast_chunks) +
+           ", pairs " +
            std::to_string(c.fast_batch) + ", rods " + std::to_string(c.fast_rods) + "\n";
       std::strncpy(report, r.c_str(), (size_t)report_len - 1);
       report[report_len - 1] = 0;

@@ -824,7 +824,7 @@ void autotune_fft(Context& ctx, std::vector<std::pair<std::string, double>>* log
     {
       std::vector<std::pair<int, int>> cand;   // (lane shape, warp shape)
       if (ctx.precision == MIXED) {
-        for (int s : {4, 0, 3}) cand.push_back({s, ctx.fast_vpsi_shape});
+        for (int s : {4, 0, 3, 5, 6}) cand.push_back({s, ctx.fast_vpsi_shape});
         for (int s : {0, 1}) cand.push_back({-1, s});
       } else {
         cand.push_back({-1, ctx.fast_vpsi_shape});
@@ -845,13 +845,22 @@ void autotune_fft(Context& ctx, std::vector<std::pair<std::string, double>>* log
     if (ctx.precision == MIXED && ctx.fast_lane_shape >= 0) {
       double best = 1e30;
       int pick = ctx.fast_density_lane_shape;
-      for (int s : {3, 2, 5}) {
+      for (int s : {3, 2, 5, 6}) {
         ctx.fast_density_lane_shape = s;
         const double t = time_ms(dens);
         note("density lane " + std::to_string(s), t);
         if (t < best) { best = t; pick = s; }
       }
       ctx.fast_density_lane_shape = pick;
+      // CTAs per plane (each accumulates its share of the band pairs)
+      int pick_c = ctx.fast_chunks;
+      for (int ch : {4, 8, 12, 16}) {
+        ctx.fast_chunks = ch;
+        const double t = time_ms(dens);
+        note("density CTAs per plane " + std::to_string(ch), t);
+        if (t < best) { best = t; pick_c = ch; }
+      }
+      ctx.fast_chunks = pick_c;
     }
     // 3. band pairs per launch (the stick buffer stays in L2 for small batches)
     {

@@ -483,6 +483,208 @@ kxy_lane(float2* __restrict__ zbuf, int npairs, int pairs_per_cta, DeviceSticks 
   }
 }
 
+// ------------------------------------------------------------ H*psi,
+// sticks read and written through the column map
+// The H*psi plane pass of kxy_lane<VPSI> with the tile's traffic to the
+// sticks taken out: the backward y transform of each occupied column loads
+// its inputs straight from the stick buffer through the (column, y) ->
+// stick map, and the forward y transform stores its outputs straight back
+// the same way.  Per band pair this drops the zero fill of the tile, the
+// scatter of the sticks into it and the gather out of it, and three of the
+// six CTA barriers.  288 threads, MINB CTAs per SM (2: registers capped at
+// 113, lane shape 5; 1: uncapped, lane shape 6).
+template <int N0, int N1, int MINB>
+__global__ void __launch_bounds__(288, MINB)
+kxy_lane_map(float2* __restrict__ zbuf, int npairs, DeviceSticks g,
+             const double2* __restrict__ twx_g, const double2* __restrict__ twy_g,
+             const float* __restrict__ v) {
+  using C = float2;
+  constexpr int LD = pitch(N1);
+  constexpr int TY = lane::lanes_for(N1), MY = N1 / TY;
+  constexpr int TX = lane::lanes_for(N0), MX = N0 / TX;
+  static_assert(TY > 0 && TX > 0, "no register plan for this length");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int ncol = g.ncol, nvec = g.nvec;
+  C* twx = reinterpret_cast<C*>(smem_raw);
+  C* twy = twx + N0;
+  C* P = twy + N1;
+  int* xmap = reinterpret_cast<int*>(P + (size_t)ncol * LD);
+  const int z = blockIdx.x, pl = blockIdx.y;
+  load_tw(twx, twx_g, N0);
+  load_tw(twy, twy_g, N1);
+  for (int x = threadIdx.x; x < N0; x += blockDim.x) xmap[x] = -1;
+  __syncthreads();
+  for (int cidx = threadIdx.x; cidx < ncol; cidx += blockDim.x) xmap[g.col_x[cidx]] = cidx;
+  const int ty = threadIdx.x % TY, gy = threadIdx.x / TY, sy = blockDim.x / TY;
+  const int tx = threadIdx.x % TX, gx = threadIdx.x / TX, sx = blockDim.x / TX;
+  const int mry = lane::bitrev(ty, TY), mrx = lane::bitrev(tx, TX);
+  C* zp = zbuf + ((size_t)pl * g.n2 + z) * nvec;
+  (void)npairs;
+  // backward y on the occupied columns, inputs from the sticks
+#pragma unroll 1
+  for (int base = 0; base < ncol; base += sy) {
+    const int cidx = base + gy;
+    const bool ok = cidx < ncol;
+    const int* cm = g.colmap + (size_t)(ok ? cidx : 0) * N1;
+    C val[MY];
+#pragma unroll
+    for (int k = 0; k < MY; ++k) {
+      const int s = ok ? __ldg(cm + ty + TY * k) : -1;
+      val[k] = s >= 0 ? zp[s] : cmk<C>(0.0, 0.0);
+    }
+    lane::line_n2r<TY, MY, +1>(val, ty, twy);
+    if (ok) {
+      C* col = P + cidx * LD;
+#pragma unroll
+      for (int k2 = 0; k2 < MY; ++k2) col[k2 + MY * mry] = val[k2];
+    }
+  }
+  __syncthreads();
+  // x rows: backward, times V(r), forward
+#pragma unroll 1
+  for (int base = 0; base < N1; base += sx) {
+    const int y = base + gx;
+    const bool ok = y < N1;
+    int txh = tx;
+    asm volatile("" : "+r"(txh));
+    C val[MX];
+#pragma unroll
+    for (int k = 0; k < MX; ++k) {
+      const int cidx = xmap[txh + TX * k];
+      val[k] = (ok && cidx >= 0) ? P[cidx * LD + y] : cmk<C>(0.0, 0.0);
+    }
+    lane::line_n2r<TX, MX, +1>(val, tx, twx);
+    const float* vrow = v + ((size_t)z * N1 + (ok ? y : 0)) * N0 + MX * mrx;
+    asm volatile("" ::: "memory");
+#pragma unroll
+    for (int k2 = 0; k2 < MX; ++k2) {
+      const float vv = ok ? vrow[k2] : 0.f;
+      val[k2].x *= vv;
+      val[k2].y *= vv;
+    }
+    lane::line_r2n<TX, MX, -1>(val, tx, twx);
+    if (ok) {
+      asm volatile("" : "+r"(txh));
+#pragma unroll
+      for (int k = 0; k < MX; ++k) {
+        const int cidx = xmap[txh + TX * k];
+        if (cidx >= 0) P[cidx * LD + y] = val[k];
+      }
+    }
+  }
+  __syncthreads();
+  // forward y, outputs to the sticks
+#pragma unroll 1
+  for (int base = 0; base < ncol; base += sy) {
+    const int cidx = base + gy;
+    const bool ok = cidx < ncol;
+    const C* col = P + (ok ? cidx : 0) * LD;
+    C val[MY];
+#pragma unroll
+    for (int k2 = 0; k2 < MY; ++k2) val[k2] = ok ? col[k2 + MY * mry] : cmk<C>(0.0, 0.0);
+    lane::line_r2n<TY, MY, -1>(val, ty, twy);
+    if (ok) {
+      const int* cm = g.colmap + (size_t)cidx * N1;
+#pragma unroll
+      for (int k = 0; k < MY; ++k) {
+        const int s = __ldg(cm + ty + TY * k);
+        if (s >= 0) zp[s] = val[k];
+      }
+    }
+  }
+}
+
+template <int N0, int N1>
+__host__ size_t xym_smem_bytes(int ncol) {
+  return sizeof(float2) * ((size_t)N0 + N1 + (size_t)ncol * pitch(N1)) + sizeof(int) * (size_t)N0;
+}
+
+// ------------------------------------------------------------ density,
+// sticks read through the column map
+// The density pass of kxy_lane<DENSITY> (whole plane, FP32 accumulator in
+// shared memory) with the y inputs loaded straight from the stick buffer
+// through the column map: no zero fill of the tile and no scatter of the
+// sticks per band pair.  320 threads, one CTA per SM (density shape 6).
+template <int N0, int N1>
+__global__ void __launch_bounds__(320, 1)
+kxy_lane_dmap(const float2* __restrict__ zbuf, int npairs, int pairs_per_cta, DeviceSticks g,
+              const double2* __restrict__ twx_g, const double2* __restrict__ twy_g,
+              double* __restrict__ rho, const double* __restrict__ w, int pair0, int nst) {
+  using C = float2;
+  constexpr int LD = pitch(N1);
+  constexpr int TY = lane::lanes_for(N1), MY = N1 / TY;
+  constexpr int TX = lane::lanes_for(N0), MX = N0 / TX;
+  static_assert(TY > 0 && TX > 0, "no register plan for this length");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int ncol = g.ncol, nvec = g.nvec;
+  C* twx = reinterpret_cast<C*>(smem_raw);
+  C* twy = twx + N0;
+  C* P = twy + N1;
+  float* acc = reinterpret_cast<float*>(P + (size_t)ncol * LD);
+  int* xmap = reinterpret_cast<int*>(acc + (size_t)N0 * N1);
+  const int z = blockIdx.x;
+  load_tw(twx, twx_g, N0);
+  load_tw(twy, twy_g, N1);
+  for (int x = threadIdx.x; x < N0; x += blockDim.x) xmap[x] = -1;
+  for (int t = threadIdx.x; t < N0 * N1; t += blockDim.x) acc[t] = 0.f;
+  __syncthreads();
+  for (int cidx = threadIdx.x; cidx < ncol; cidx += blockDim.x) xmap[g.col_x[cidx]] = cidx;
+  const int ty = threadIdx.x % TY, gy = threadIdx.x / TY, sy = blockDim.x / TY;
+  const int tx = threadIdx.x % TX, gx = threadIdx.x / TX, sx = blockDim.x / TX;
+  const int mry = lane::bitrev(ty, TY), mrx = lane::bitrev(tx, TX);
+  const int pbeg = blockIdx.y * pairs_per_cta;
+  const int pend = min(npairs, pbeg + pairs_per_cta);
+#pragma unroll 1
+  for (int pl = pbeg; pl < pend; ++pl) {
+    const C* zp = zbuf + ((size_t)pl * g.n2 + z) * nvec;
+#pragma unroll 1
+    for (int base = 0; base < ncol; base += sy) {
+      const int cidx = base + gy;
+      const bool ok = cidx < ncol;
+      const int* cm = g.colmap + (size_t)(ok ? cidx : 0) * N1;
+      C val[MY];
+#pragma unroll
+      for (int k = 0; k < MY; ++k) {
+        const int sidx = ok ? __ldg(cm + ty + TY * k) : -1;
+        val[k] = sidx >= 0 ? zp[sidx] : cmk<C>(0.0, 0.0);
+      }
+      lane::line_n2r<TY, MY, +1>(val, ty, twy);
+      if (ok) {
+        C* col = P + cidx * LD;
+#pragma unroll
+        for (int k2 = 0; k2 < MY; ++k2) col[k2 + MY * mry] = val[k2];
+      }
+    }
+    __syncthreads();
+    const int b1 = 2 * (pair0 + pl);
+    const float f1 = (float)w[b1];
+    const float f2 = (b1 + 1 < nst) ? (float)w[b1 + 1] : 0.f;
+#pragma unroll 1
+    for (int base = 0; base < N1; base += sx) {
+      const int y = base + gx;
+      const bool ok = y < N1;
+      int txh = tx;
+      asm volatile("" : "+r"(txh));
+      C val[MX];
+#pragma unroll
+      for (int k = 0; k < MX; ++k) {
+        const int cidx = xmap[txh + TX * k];
+        val[k] = (ok && cidx >= 0) ? P[cidx * LD + y] : cmk<C>(0.0, 0.0);
+      }
+      lane::line_n2r<TX, MX, +1>(val, tx, twx);
+      if (ok) {
+        float* arow = acc + y * N0 + MX * mrx;
+#pragma unroll
+        for (int k2 = 0; k2 < MX; ++k2)
+          arow[k2] += f1 * val[k2].x * val[k2].x + f2 * val[k2].y * val[k2].y;
+      }
+    }
+    __syncthreads();
+  }
+  const size_t pbase = (size_t)z * N1 * N0;
+  for (int t = threadIdx.x; t < N0 * N1; t += blockDim.x) atomicAdd(&rho[pbase + t], (double)acc[t]);
+}
+
 // ------------------------------------------------------------ density,
 // half planes
 // The density pass of kxy_lane over one half of a plane's rows per CTA
@@ -634,6 +836,30 @@ void launch_lane_xy(Context& ctx, const StagedArgs& a, int chunks, int ppc) {
   QBX_LAUNCHED(ctx);
 }
 
+template <int N, int MINB>
+void launch_lane_map(Context& ctx, const StagedArgs& a) {
+  const DeviceSticks& g = ctx.dws;
+  const size_t sm = xym_smem_bytes<N, N>(g.ncol);
+  allow_smem(kxy_lane_map<N, N, MINB>, sm);
+  const int want = (g.ncol * lane::lanes_for(N) + 31) / 32 * 32;
+  const int threads = std::max(64, std::min(288, want));
+  kxy_lane_map<N, N, MINB><<<dim3(N, a.npairs), threads, sm, ctx.stream>>>(
+      (float2*)a.zbuf, a.npairs, g, a.twx, a.twy, (const float*)a.v);
+  QBX_LAUNCHED(ctx);
+}
+
+template <int N>
+void launch_density_map(Context& ctx, const StagedArgs& a, int chunks, int ppc) {
+  const DeviceSticks& g = ctx.dws;
+  const size_t sm = xyl_smem_bytes<N, N, XY_DENSITY>(g.ncol);
+  allow_smem(kxy_lane_dmap<N, N>, sm);
+  const int want = (g.ncol * lane::lanes_for(N) + 31) / 32 * 32;
+  const int threads = std::max(64, std::min(320, want));
+  kxy_lane_dmap<N, N><<<dim3(N, chunks), threads, sm, ctx.stream>>>(
+      (const float2*)a.zbuf, a.npairs, ppc, g, a.twx, a.twy, a.rho, a.w, a.pair0, a.nst);
+  QBX_LAUNCHED(ctx);
+}
+
 template <int N>
 constexpr bool density_half_ok() {
   return N % 2 == 0 && lane::lanes_for(N) >= 2 && lane::lanes_for(N) <= 4;
@@ -679,6 +905,7 @@ void run_cubic(Context& ctx, const StagedArgs& a) {
         chunks = (a.npairs + ppc - 1) / ppc;
         ProfScope ps(ctx, "xy_density");
         if (a.density_lane_shape == 5 && density_half_ok<N>()) launch_density_half<N>(ctx, a, chunks, ppc);
+        else if (a.density_lane_shape == 6) launch_density_map<N>(ctx, a, chunks, ppc);
         else if (a.density_lane_shape == 3) launch_lane_xy<N, XY_DENSITY, 3>(ctx, a, chunks, ppc);
         else launch_lane_xy<N, XY_DENSITY, 2>(ctx, a, chunks, ppc);
         return;
@@ -686,6 +913,8 @@ void run_cubic(Context& ctx, const StagedArgs& a) {
       {
         ProfScope ps(ctx, "xy_vpsi");
         switch (a.lane_shape) {
+          case 5: launch_lane_map<N, 2>(ctx, a); break;
+          case 6: launch_lane_map<N, 1>(ctx, a); break;
           case 1: launch_lane_xy<N, XY_VPSI, 1>(ctx, a, a.npairs, 1); break;
           case 2: launch_lane_xy<N, XY_VPSI, 2>(ctx, a, a.npairs, 1); break;
           case 3: launch_lane_xy<N, XY_VPSI, 3>(ctx, a, a.npairs, 1); break;

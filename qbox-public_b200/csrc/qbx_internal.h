@@ -389,8 +389,10 @@ struct Context {
   int fast_rods = 16;           // rods per CTA of the z kernels
   int fast_warps = 16;          // warps per CTA of the plane kernel (at most)
   int fast_vpsi_shape = 0;      // FP32 H*psi plane CTA shape (0, 1, 2)
-  int fast_lane_shape = 4;      // FP32 register-lane plane kernel shape, -1 = off
-  int fast_density_lane_shape = 3;  // its density shape (2, 3; 5 = half planes)
+  int fast_lane_shape = 4;      // FP32 register-lane plane kernel shape (5: sticks through
+                                // the column map), -1 = off
+  int fast_density_lane_shape = 3;  // its density shape (2, 3; 5 half planes; 6 sticks
+                                    // read through the column map)
   int fast_chunks = 8;          // CTAs per plane in the density pass
   bool fast_fft = true;         // use the specialised kernels when compiled
   float* a32 = nullptr;         // TF32 hi/lo split of the projectors

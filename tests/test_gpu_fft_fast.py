@@ -80,14 +80,15 @@ def test_autotune_keeps_results(precision):
     a.close()
 
 
+@pytest.mark.parametrize("shape", [5, 6])
 @pytest.mark.parametrize("name", ["si8", "si64", "h2o32"])
-def test_density_half_planes(name, monkeypatch):
-    """The half-plane density kernel (two CTAs per plane, y inputs gathered
-    from the sticks) gives the whole-plane kernel's density (FP32, 2e-6 of
-    the largest value)."""
+def test_density_half_planes(name, shape, monkeypatch):
+    """The half-plane density kernel (shape 5: two CTAs per plane) and the
+    whole-plane kernel reading the sticks through the column map (shape 6)
+    give the default kernel's density (FP32, 2e-6 of the largest value)."""
     s = systems.get(name)
     ref = _ctx(s, capi.MIXED, True)
-    monkeypatch.setenv("QBX_FAST_DENSITY_LANE_SHAPE", "5")
+    monkeypatch.setenv("QBX_FAST_DENSITY_LANE_SHAPE", str(shape))
     half = _ctx(s, capi.MIXED, True)
     monkeypatch.delenv("QBX_FAST_DENSITY_LANE_SHAPE")
     ref.update_density()
@@ -96,3 +97,22 @@ def test_density_half_planes(name, monkeypatch):
     np.testing.assert_allclose(rb, ra, rtol=0, atol=2e-6 * np.abs(ra).max())
     ref.close()
     half.close()
+
+
+@pytest.mark.parametrize("shape", [5, 6])
+@pytest.mark.parametrize("name", ["si8", "si64", "h2o32"])
+def test_vpsi_sticks_through_column_map(name, shape, monkeypatch):
+    """The H*psi plane kernel that reads and writes the sticks through the
+    column map (lane shapes 5 and 6) gives the default kernel's H*psi (FP32,
+    2e-6 of the largest value)."""
+    s = systems.get(name)
+    ref = _ctx(s, capi.MIXED, True)
+    monkeypatch.setenv("QBX_FAST_LANE_SHAPE", str(shape))
+    alt = _ctx(s, capi.MIXED, True)
+    monkeypatch.delenv("QBX_FAST_LANE_SHAPE")
+    ra, ha, ea = _run(ref)
+    rb, hb, eb = _run(alt)
+    np.testing.assert_allclose(hb, ha, rtol=0, atol=2e-6 * np.abs(ha).max())
+    assert abs(ea["etotal"] - eb["etotal"]) < 1e-6 * len(s.atoms)
+    ref.close()
+    alt.close()
