@@ -255,9 +255,9 @@ def run_ours(args):
                 "frac": achieved / hbm_peak,
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                 # DRAM bytes per launch: the ncu capture of this kernel
-                # (profiles/kxy_lane_vpsi_si512.md: 336.9 MB for a 16-pair
-                # launch) scaled by the band pairs of this run's launches
-                "traffic": 336.9e6 / 16.0 * (npairs / max(1e-9, n_xy)),
+                # (profiles/kxy_lane_map_vpsi_si512.md: 198.3 MB for a
+                # 32-pair launch) scaled by the band pairs of this run's launches
+                "traffic": 198.3e6 / 32.0 * (npairs / max(1e-9, n_xy)),
                 "algorithmic_bytes_per_launch": per_launch_bytes,
                 "launch_ms": per_launch_ms}
     # GEMM share (FP64 cuBLAS in this build) against the dense FP64 rate
