@@ -145,6 +145,19 @@ int qbx_scf_step(qbx_context* ctx, int compute_forces, double* energies,
 int qbx_scf_step_batch(qbx_context** ctxs, int n, int compute_forces,
                        double* energies);
 
+/* The <wavefunction> element of a Qbox sample file, as Wavefunction::print
+ * writes it with base64 encoding (src/Wavefunction.cpp:919-962,
+ * SlaterDet::print src/SlaterDet.cpp:1382-1549): each band's real values on
+ * the wavefunction basis's own FFT grid (src/Basis.cpp:509-521), x fastest,
+ * base64 in 72-character lines.  The transforms run on the device. */
+int qbx_write_wavefunction(qbx_context* ctx, const char* path);
+/* Reads such an element (written by this library or by the reference) into
+ * the context's coefficients: each grid function transformed forward onto
+ * the basis, the diagonal density matrix as the occupations
+ * (src/WavefunctionHandler.cpp).  The file's grid must be this basis's
+ * grid; only real (Gamma) base64 grid functions. */
+int qbx_read_wavefunction(qbx_context* ctx, const char* path);
+
 /* The ground-state SCF loop of BOSampleStepper::step(0) with atoms fixed
  * (src/BOSampleStepper.cpp:781-1114) and wf_dyn = PSDA: nitscf
  * iterations.  With nite > 0 each iteration mixes the new density into the

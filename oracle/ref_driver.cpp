@@ -18,6 +18,10 @@
 // atoms fixed) with nitscf SCF iterations of nite PSDA steps each and the
 // given charge mixing (charge_mix_coeff, charge_mix_rcut, charge_mix_ndim);
 // its log goes to gs_log.txt and the final coefficients to final_c.bin.
+// wf_dyn = PRINT writes the orthonormalised input wavefunction with the
+// reference's Wavefunction::print (src/Wavefunction.cpp:919-962,
+// SlaterDet::print src/SlaterDet.cpp:1382-1549, base64 encoding) to wf.xml
+// and its coefficients to final_c.bin.
 // wf_dyn = MD runs the reference's own BOSampleStepper::step(nsteps)
 // (src/BOSampleStepper.cpp:165-1428) with atoms_dyn = MD, wf_dyn = PSDA,
 // nitscf electronic steps per ionic step, nite = 0 and the time step dt
@@ -201,6 +205,23 @@ int main(int argc, char** argv)
       c[ig + (size_t)n*mloc] = complex<double>(cin[src], cin[src+1]);
     }
   s.wf.gram();
+
+  if ( wf_dyn == "PRINT" )
+  {
+    ofstream wo((outdir + "/wf.xml").c_str());
+    s.wf.print(wo, "base64", "wavefunction");
+    wo.close();
+    vector<double> out(2*(size_t)ngw*nst);
+    for ( int n = 0; n < nst; n++ )
+      for ( int ig = 0; ig < ngw; ig++ )
+      {
+        const complex<double> v = c[ig + (size_t)n*mloc];
+        const size_t dst = 2*((size_t)n*ngw + perm[ig]);
+        out[dst] = v.real(); out[dst+1] = v.imag();
+      }
+    write_bin(outdir + "/final_c.bin", &out[0], out.size()*sizeof(double));
+    return 0;
+  }
 
   if ( wf_dyn == "GS" )
   {

@@ -6,7 +6,9 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <fstream>
 #include <map>
+#include <sstream>
 #include <new>
 #include <stdexcept>
 #include <thread>
@@ -65,6 +67,8 @@ void free_cell(Context& c) {
   drop_graphs(c);
   free_mixed(c);
   free_mix(c);
+  if (c.have_wgrid) free_sticks(c.dwg);
+  c.have_wgrid = false;
   free_sticks(c.dws);
   free_sticks(c.dvs);
   double** bufs[] = {&c.d_gx_w, &c.d_g2_w, &c.d_gx_v, &c.d_g2i_v, &c.d_c, &c.d_hc, &c.d_c_last,
@@ -778,6 +782,29 @@ int qbx_scf_run(qbx_context* h, int nitscf, int nite, double mix_coeff, double m
                 "bad SCF arguments");
     scf_run(c, nitscf, nite, mix_coeff, mix_rcut, mix_ndim, scf_tol, etotal_int, eigsum,
             nite_done, nitscf_done);
+  });
+}
+
+int qbx_write_wavefunction(qbx_context* h, const char* path) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, false);
+    QBX_REQUIRE(path, 1, "null path");
+    std::ofstream os(path);
+    QBX_REQUIRE(os.good(), 75, std::string("cannot write ") + path);
+    write_wavefunction(c, os);
+    QBX_REQUIRE(os.good(), 75, std::string("write failed: ") + path);
+  });
+}
+
+int qbx_read_wavefunction(qbx_context* h, const char* path) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, false);
+    QBX_REQUIRE(path, 1, "null path");
+    std::ifstream is(path, std::ios::binary);
+    QBX_REQUIRE(is.good(), 75, std::string("cannot read ") + path);
+    std::ostringstream ss;
+    ss << is.rdbuf();
+    read_wavefunction(c, ss.str());
   });
 }
 

@@ -664,18 +664,17 @@ void launch_vpsi(Context& ctx, const double* c, const double* v, double* hc) {
   staged(ctx, OP_VPSI, c, v, nullptr, nullptr, hc);
 }
 
-// full-grid transform of the grid held in ctx.d_grid
-static void grid_fft(Context& ctx, int dir) {
+// full-grid transform of `grid` on the geometry of d (sizes, twiddles)
+static void grid_fft_on(Context& ctx, const DeviceSticks& b, double2* grid, int dir) {
   ProfScope ps(ctx, "grid_fft");
-  const Basis& b = ctx.vb;
   const int n[3] = {b.n0, b.n1, b.n2};
   const int L = 16;
   for (int axis = 0; axis < 3; axis++) {
-    const double2* tw = twiddles(ctx, axis);
+    const double2* tw = b.tw[axis];
     // compile-time lengths: warp FFTs on coalesced tiles (fft_fast.cuh)
     if (ctx.fast_fft &&
-        (fast_grid_lines_a(ctx, (double2*)ctx.d_grid, b.n0, b.n1, b.n2, axis, dir, tw) ||
-         fast_grid_lines_b(ctx, (double2*)ctx.d_grid, b.n0, b.n1, b.n2, axis, dir, tw)))
+        (fast_grid_lines_a(ctx, grid, b.n0, b.n1, b.n2, axis, dir, tw) ||
+         fast_grid_lines_b(ctx, grid, b.n0, b.n1, b.n2, axis, dir, tw)))
       continue;
     const RadixPlan p = make_plan(n[axis]);
     int nblocks;
@@ -685,13 +684,43 @@ static void grid_fft(Context& ctx, int dir) {
     const size_t smem = sizeof(double2) * (size_t)n[axis] * (1 + 2 * L);
     if (dir > 0) {
       allow_smem(k_line_fft<+1>, smem);
-      k_line_fft<+1><<<nblocks, 256, smem, ctx.stream>>>((double2*)ctx.d_grid, b.n0, b.n1, b.n2, axis, p, tw, L);
+      k_line_fft<+1><<<nblocks, 256, smem, ctx.stream>>>(grid, b.n0, b.n1, b.n2, axis, p, tw, L);
     } else {
       allow_smem(k_line_fft<-1>, smem);
-      k_line_fft<-1><<<nblocks, 256, smem, ctx.stream>>>((double2*)ctx.d_grid, b.n0, b.n1, b.n2, axis, p, tw, L);
+      k_line_fft<-1><<<nblocks, 256, smem, ctx.stream>>>(grid, b.n0, b.n1, b.n2, axis, p, tw, L);
     }
     QBX_LAUNCHED(ctx);
   }
+}
+
+// full-grid transform of the density-basis grid held in ctx.d_grid
+static void grid_fft(Context& ctx, int dir) { grid_fft_on(ctx, ctx.dvs, (double2*)ctx.d_grid, dir); }
+
+// One band c (ng coefficients of the half sphere) to its real values on the
+// grid of d (FourierTransform::backward, one band), x fastest, into f.
+void wfgrid_backward(Context& ctx, const DeviceSticks& d, int ng, const double* c, double* f) {
+  const size_t N = (size_t)d.n0 * d.n1 * d.n2;
+  QBX_REQUIRE(N <= ctx.N(), 1, "grid larger than the density grid's workspace");
+  QBX_CUDA(cudaMemsetAsync(ctx.d_grid, 0, N * sizeof(double2), ctx.stream));
+  k_scatter_sphere<<<nblk(ng), 256, 0, ctx.stream>>>((const double2*)c, d.ip, d.im, ng,
+                                                     (double2*)ctx.d_grid);
+  QBX_LAUNCHED(ctx);
+  grid_fft_on(ctx, d, (double2*)ctx.d_grid, +1);
+  k_grid_real<<<nblk(N), 256, 0, ctx.stream>>>((const double2*)ctx.d_grid, N, f);
+  QBX_LAUNCHED(ctx);
+}
+
+// The inverse: real values f on the grid of d to the band's coefficients
+// (FourierTransform::forward with its 1/N, then the half sphere).
+void wfgrid_forward(Context& ctx, const DeviceSticks& d, int ng, const double* f, double* c) {
+  const size_t N = (size_t)d.n0 * d.n1 * d.n2;
+  QBX_REQUIRE(N <= ctx.N(), 1, "grid larger than the density grid's workspace");
+  k_real_to_grid<<<nblk(N), 256, 0, ctx.stream>>>(f, 1.0, N, (double2*)ctx.d_grid);
+  QBX_LAUNCHED(ctx);
+  grid_fft_on(ctx, d, (double2*)ctx.d_grid, -1);
+  k_gather_sphere<<<nblk(ng), 256, 0, ctx.stream>>>((const double2*)ctx.d_grid, d.ip, ng,
+                                                    1.0 / (double)N, (double2*)c);
+  QBX_LAUNCHED(ctx);
 }
 
 static int nblk(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 16); }

@@ -13,6 +13,7 @@
 #include <cusolverDn.h>
 
 #include <complex>
+#include <iosfwd>
 #include <string>
 #include <vector>
 
@@ -267,6 +268,8 @@ struct Context {
 
   Basis wb, vb;                 // wavefunction basis, density basis (4 ecut)
   DeviceSticks dws{}, dvs{};
+  DeviceSticks dwg{};           // the wavefunction basis on its own FFT grid (sample files)
+  bool have_wgrid = false;
   std::string xc = "LDA";
 
   // species and atoms
@@ -567,6 +570,11 @@ void lowdin(Context& ctx);                     // SlaterDet::lowdin of C
 void scf_run(Context& c, int nitscf, int nite, double mix_coeff, double mix_rcut, int mix_ndim,
              double scf_tol, double* etotal_int, double* eigsum, int* nite_done, int* nitscf_done);
 void free_mix(Context& c);
+// sample-file wavefunctions (sample_io.cpp)
+void write_wavefunction(Context& c, std::ostream& os);
+void read_wavefunction(Context& c, const std::string& text);
+void wfgrid_backward(Context& ctx, const DeviceSticks& d, int ng, const double* c, double* f);
+void wfgrid_forward(Context& ctx, const DeviceSticks& d, int ng, const double* f, double* c);
 // molecular dynamics (md.cu)
 void move_atoms(Context& c, const double* tau);
 void md_run(Context& c, int niter, int nitscf, double dt, const double* mass_amu, double* vel,

@@ -38,7 +38,8 @@ SYMBOLS = (
     "qbx_set_gemm_backend", "qbx_split_gemm_tn", "qbx_density_static",
     "qbx_stress", "qbx_get_stress", "qbx_autotune", "qbx_set_wf_dyn", "qbx_jd_update",
     "qbx_scf_step_batch", "qbx_set_step_graph", "qbx_step_graph_info", "qbx_polar",
-    "qbx_move_atoms", "qbx_md_run", "qbx_scf_run",
+    "qbx_move_atoms", "qbx_md_run", "qbx_scf_run", "qbx_write_wavefunction",
+    "qbx_read_wavefunction",
 )
 
 _lib = None
@@ -110,6 +111,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "qbx_get_stress": (_I, [_P, _DP, _DP]),
         "qbx_set_step_graph": (_I, [_P, _I]),
         "qbx_move_atoms": (_I, [_P, _DP]),
+        "qbx_write_wavefunction": (_I, [_P, ctypes.c_char_p]),
+        "qbx_read_wavefunction": (_I, [_P, ctypes.c_char_p]),
         "qbx_scf_run": (_I, [_P, _I, _I, _D, _D, _I, _D, _DP, _DP, _IP, _IP]),
         "qbx_md_run": (_I, [_P, _I, _I, _D, _DP, _DP, _DP, _DP, _DP]),
         "qbx_polar": (_I, [_P, _DP, _D, _I, _I, ctypes.POINTER(_I)]),
@@ -357,6 +360,15 @@ class Context:
         n = done.value
         sums = [eig[i * ns + j] for i in range(n) for j in range(int(nd[i]))]
         return {"etotal_int": eint[:n], "eigenvalue_sum": np.array(sums), "nite_done": nd[:n]}
+
+    def write_wavefunction(self, path: str):
+        """qbx_write_wavefunction: the sample file's <wavefunction> element."""
+        self._ok(self.lib.qbx_write_wavefunction(self.h, path.encode()), "write_wavefunction")
+
+    def read_wavefunction(self, path: str):
+        """qbx_read_wavefunction: coefficients and occupations from a
+        sample file's <wavefunction> element."""
+        self._ok(self.lib.qbx_read_wavefunction(self.h, path.encode()), "read_wavefunction")
 
     def move_atoms(self, tau: np.ndarray):
         """qbx_move_atoms: the same atoms at new positions (species-major)."""

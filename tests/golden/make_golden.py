@@ -11,7 +11,9 @@ a fixed sample of G otherwise), and per-band norms.
 The fixtures pin the numpy oracle (oracle/qbox_np.py) in tests/test_oracle.py.
 ref_<name>_jd.npz holds a JD-stepper run, ref_<name>_md.npz a molecular
 dynamics run and ref_<name>_gs.npz a ground-state SCF run with charge mixing
-of the reference's BOSampleStepper.
+of the reference's BOSampleStepper; ref_<name>_wf.npz the <wavefunction>
+element the reference's Wavefunction::print writes (base64) for a band
+sample, with the coefficients it wrote.
 """
 from __future__ import annotations
 
@@ -132,13 +134,39 @@ def make_gs(name: str, workdir: str) -> str:
     return path
 
 
+# wavefunction output of the reference (Wavefunction::print, base64): system,
+# band sample
+WF_CASES = {"si8": 4}
+
+
+def make_wf(name: str, workdir: str) -> str:
+    """The sample-file <wavefunction> element the reference writes for the
+    orthonormalised seeded coefficients of a band sample, and those
+    coefficients."""
+    import subprocess
+    s = systems.get(name).band_sample(WF_CASES[name])
+    path = inputs.write_system(s, workdir)
+    subprocess.run([inputs.REF_DRIVER, path, "1", workdir, "0", "0", "PRINT"], check=True,
+                   stdout=subprocess.DEVNULL)
+    xml = open(os.path.join(workdir, "wf.xml"), "rb").read()
+    c = np.fromfile(os.path.join(workdir, "final_c.bin")).reshape(s.nbands, -1, 2)
+    fx = dict(nbands=s.nbands, xml=np.frombuffer(xml, dtype=np.uint8),
+              c=c[..., 0] + 1j * c[..., 1])
+    out = os.path.join(os.path.dirname(os.path.abspath(__file__)), f"ref_{name}_wf.npz")
+    np.savez_compressed(out, **fx)
+    return out
+
+
 if __name__ == "__main__":
     import tempfile
     names = sys.argv[1:] or (list(CASES) + [n + "_jd" for n in JD_CASES]
-                             + [n + "_md" for n in MD_CASES] + [n + "_gs" for n in GS_CASES])
+                             + [n + "_md" for n in MD_CASES] + [n + "_gs" for n in GS_CASES]
+                             + [n + "_wf" for n in WF_CASES])
     for n in names:
         with tempfile.TemporaryDirectory() as td:
-            if n.endswith("_gs"):
+            if n.endswith("_wf"):
+                print(make_wf(n[:-3], td))
+            elif n.endswith("_gs"):
                 print(make_gs(n[:-3], td))
             elif n.endswith("_md"):
                 print(make_md(n[:-3], td))
