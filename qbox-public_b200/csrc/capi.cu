@@ -470,7 +470,7 @@ int qbx_set_cell(qbx_context* h, const double cell[9], double ecut, int nst, con
       if (const char* e = std::getenv("QBX_FAST_LANE_SHAPE"))
         c.fast_lane_shape = std::max(-1, std::min(6, std::atoi(e)));
       if (const char* e = std::getenv("QBX_FAST_DENSITY_LANE_SHAPE"))
-        c.fast_density_lane_shape = (std::atoi(e) == 3 || std::atoi(e) == 5 || std::atoi(e) == 6)
+        c.fast_density_lane_shape = (std::atoi(e) == 3 || std::atoi(e) >= 5) && std::atoi(e) <= 7
                                         ? std::atoi(e) : 2;
       if (const char* e = std::getenv("QBX_FAST_VPSI_SHAPE"))
         c.fast_vpsi_shape = std::max(0, std::min(2, std::atoi(e)));

@@ -686,6 +686,193 @@ kxy_lane_dmap(const float2* __restrict__ zbuf, int npairs, int pairs_per_cta, De
 }
 
 // ------------------------------------------------------------ density,
+// accumulator in tensor memory
+// The density pass of kxy_lane<DENSITY> with the FP32 accumulator held in
+// tensor memory (TMEM) instead of shared memory.  A thread accumulates the
+// same points for every band pair (its rows base + gx, its columns
+// MX*bitrev(tx) + k), so each thread keeps them in its own TMEM lane: warp w
+// owns lanes 32*(w%4) .. +31 and a block of columns chosen by w/4, and
+// reads, adds and writes 8 columns at a time (tcgen05.ld/st .32x32b.x8).
+// Freed of the 78 KB shared accumulator, two CTAs fit per SM, each
+// allocating 256 of the SM's 512 TMEM columns.  Density shape 7.
+// load without waiting: r is valid only after tm_wait_ld(r)
+__device__ __forceinline__ void tm_ld8_async(uint32_t taddr, uint32_t (&r)[8]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                 "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+}
+// waits for this thread's loads; r passes through the wait so that no use of
+// it is scheduled before it
+__device__ __forceinline__ void tm_wait_ld(uint32_t (&r)[8]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]),
+                 "+r"(r[6]), "+r"(r[7])
+               :
+               : "memory");
+}
+__device__ __forceinline__ void tm_ld8(uint32_t taddr, uint32_t (&r)[8]) {
+  tm_ld8_async(taddr, r);
+  tm_wait_ld(r);
+}
+__device__ __forceinline__ void tm_st8(uint32_t taddr, const uint32_t (&r)[8]) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr),
+               "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]),
+               "r"(r[7])
+               : "memory");
+}
+__device__ __forceinline__ void tm_wait_st() {
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+
+constexpr int kTmemCols = 256;   // TMEM columns per density CTA (two CTAs per SM)
+
+// TMEM columns per row round of a thread: MX rounded up to the 8-column access
+__host__ __device__ constexpr int tm_round_cols(int mx) { return (mx + 7) / 8 * 8; }
+
+template <int N0, int N1>
+__global__ void __maxnreg__(112)
+kxy_lane_dtm(const float2* __restrict__ zbuf, int npairs, int pairs_per_cta, DeviceSticks g,
+             const double2* __restrict__ twx_g, const double2* __restrict__ twy_g,
+             double* __restrict__ rho, const double* __restrict__ w, int pair0, int nst) {
+  using C = float2;
+  constexpr int LD = pitch(N1);
+  constexpr int TY = lane::lanes_for(N1), MY = N1 / TY;
+  constexpr int TX = lane::lanes_for(N0), MX = N0 / TX;
+  constexpr int CW = tm_round_cols(MX), NCH = CW / 8;
+  static_assert(TY > 0 && TX > 0, "no register plan for this length");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int ncol = g.ncol, nvec = g.nvec;
+  C* twx = reinterpret_cast<C*>(smem_raw);
+  C* twy = twx + N0;
+  C* P = twy + N1;
+  int* xmap = reinterpret_cast<int*>(P + (size_t)ncol * LD);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(xmap + N0);
+  const int z = blockIdx.x;
+  const int warp = threadIdx.x >> 5;
+  const int sx = blockDim.x / TX;
+  const int R = (N1 + sx - 1) / sx;       // row rounds per thread
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(tmem_slot)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  load_tw(twx, twx_g, N0);
+  load_tw(twy, twy_g, N1);
+  for (int x = threadIdx.x; x < N0; x += blockDim.x) xmap[x] = -1;
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tbase = *tmem_slot + ((uint32_t)(32 * (warp & 3)) << 16) +
+                         (uint32_t)((warp >> 2) * R * CW);
+  {
+    const uint32_t zr[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int q = 0; q < R * NCH; ++q) tm_st8(tbase + 8 * q, zr);
+    tm_wait_st();
+  }
+  for (int cidx = threadIdx.x; cidx < ncol; cidx += blockDim.x) xmap[g.col_x[cidx]] = cidx;
+  const int ty = threadIdx.x % TY, gy = threadIdx.x / TY, sy = blockDim.x / TY;
+  const int tx = threadIdx.x % TX, gx = threadIdx.x / TX;
+  const int mry = lane::bitrev(ty, TY), mrx = lane::bitrev(tx, TX);
+  const int pbeg = blockIdx.y * pairs_per_cta;
+  const int pend = min(npairs, pbeg + pairs_per_cta);
+#pragma unroll 1
+  for (int pl = pbeg; pl < pend; ++pl) {
+    const C* zp = zbuf + ((size_t)pl * g.n2 + z) * nvec;
+    for (int t = threadIdx.x; t < ncol * LD; t += blockDim.x) P[t] = cmk<C>(0.0, 0.0);
+    __syncthreads();
+    for (int s2 = threadIdx.x; s2 < nvec; s2 += blockDim.x)
+      P[g.stick_col[s2] * LD + g.stick_y[s2]] = zp[s2];
+    __syncthreads();
+#pragma unroll 1
+    for (int base = 0; base < ncol; base += sy) {
+      const int cidx = base + gy;
+      const bool ok = cidx < ncol;
+      C* col = P + (ok ? cidx : 0) * LD;
+      C val[MY];
+#pragma unroll
+      for (int k = 0; k < MY; ++k) val[k] = ok ? col[ty + TY * k] : cmk<C>(0.0, 0.0);
+      lane::line_n2r<TY, MY, +1>(val, ty, twy);
+      if (ok) {
+#pragma unroll
+        for (int k2 = 0; k2 < MY; ++k2) col[k2 + MY * mry] = val[k2];
+      }
+    }
+    __syncthreads();
+    const int b1 = 2 * (pair0 + pl);
+    const float f1 = (float)w[b1];
+    const float f2 = (b1 + 1 < nst) ? (float)w[b1 + 1] : 0.f;
+    // every warp runs all R rounds (the TMEM accesses are warp-wide); rows
+    // past the end carry zeros
+#pragma unroll 1
+    for (int r = 0; r < R; ++r) {
+      const int y = r * sx + gx;
+      const bool ok = y < N1;
+      int txh = tx;
+      asm volatile("" : "+r"(txh));
+      C val[MX];
+#pragma unroll
+      for (int k = 0; k < MX; ++k) {
+        const int cidx = xmap[txh + TX * k];
+        val[k] = (ok && cidx >= 0) ? P[cidx * LD + y] : cmk<C>(0.0, 0.0);
+      }
+      lane::line_n2r<TX, MX, +1>(val, tx, twx);
+      // read-add-write 8 columns at a time, the next chunk's load in
+      // flight while this one is added
+      const uint32_t trow = tbase + (uint32_t)(r * CW);
+      uint32_t a[8], nx[8];
+      tm_ld8(trow, a);
+#pragma unroll
+      for (int c8 = 0; c8 < NCH; ++c8) {
+        if (c8 + 1 < NCH) tm_ld8_async(trow + 8 * (c8 + 1), nx);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const int k2 = 8 * c8 + j;
+          if (k2 < MX)
+            a[j] = __float_as_uint(__uint_as_float(a[j]) + f1 * val[k2].x * val[k2].x +
+                                   f2 * val[k2].y * val[k2].y);
+        }
+        tm_st8(trow + 8 * c8, a);
+        if (c8 + 1 < NCH) {
+          tm_wait_ld(nx);
+#pragma unroll
+          for (int j = 0; j < 8; ++j) a[j] = nx[j];
+        }
+      }
+    }
+    tm_wait_st();
+    __syncthreads();
+  }
+  // add this CTA's accumulators to the density
+#pragma unroll 1
+  for (int r = 0; r < R; ++r) {
+    const int y = r * sx + gx;
+#pragma unroll
+    for (int c8 = 0; c8 < NCH; ++c8) {
+      uint32_t a[8];
+      tm_ld8(tbase + (uint32_t)(r * CW + 8 * c8), a);
+      if (y < N1) {
+        double* out = rho + ((size_t)z * N1 + y) * N0 + MX * mrx;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const int k2 = 8 * c8 + j;
+          if (k2 < MX) atomicAdd(out + k2, (double)__uint_as_float(a[j]));
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*tmem_slot),
+                 "r"(kTmemCols)
+                 : "memory");
+  }
+}
+
+// ------------------------------------------------------------ density,
 // half planes
 // The density pass of kxy_lane over one half of a plane's rows per CTA
 // (blockIdx.z = 0, 1).  Each half transforms every occupied column along y,
@@ -860,6 +1047,36 @@ void launch_density_map(Context& ctx, const StagedArgs& a, int chunks, int ppc) 
   QBX_LAUNCHED(ctx);
 }
 
+// threads of the TMEM density kernel: one lane group per occupied column,
+// at most 288
+template <int N>
+int density_tmem_threads(const Context& ctx) {
+  const int want = (ctx.dws.ncol * lane::lanes_for(N) + 31) / 32 * 32;
+  return std::max(64, std::min(288, want));
+}
+
+// the TMEM columns every warp needs fit the CTA's 256
+template <int N>
+bool density_tmem_fits(const Context& ctx) {
+  constexpr int TX = lane::lanes_for(N);
+  if (TX == 0) return false;
+  const int threads = density_tmem_threads<N>(ctx);
+  const int sx = threads / TX, R = (N + sx - 1) / sx, nw = threads / 32;
+  return ((nw + 3) / 4) * R * tm_round_cols(N / TX) <= kTmemCols;
+}
+
+template <int N>
+void launch_density_tmem(Context& ctx, const StagedArgs& a, int chunks, int ppc) {
+  const DeviceSticks& g = ctx.dws;
+  const size_t sm = sizeof(float2) * ((size_t)N + N + (size_t)g.ncol * pitch(N)) +
+                    sizeof(int) * (size_t)N + 16;
+  allow_smem(kxy_lane_dtm<N, N>, sm);
+  const int threads = density_tmem_threads<N>(ctx);
+  kxy_lane_dtm<N, N><<<dim3(N, chunks), threads, sm, ctx.stream>>>(
+      (const float2*)a.zbuf, a.npairs, ppc, g, a.twx, a.twy, a.rho, a.w, a.pair0, a.nst);
+  QBX_LAUNCHED(ctx);
+}
+
 template <int N>
 constexpr bool density_half_ok() {
   return N % 2 == 0 && lane::lanes_for(N) >= 2 && lane::lanes_for(N) <= 4;
@@ -906,6 +1123,7 @@ void run_cubic(Context& ctx, const StagedArgs& a) {
         ProfScope ps(ctx, "xy_density");
         if (a.density_lane_shape == 5 && density_half_ok<N>()) launch_density_half<N>(ctx, a, chunks, ppc);
         else if (a.density_lane_shape == 6) launch_density_map<N>(ctx, a, chunks, ppc);
+        else if (a.density_lane_shape == 7 && density_tmem_fits<N>(ctx)) launch_density_tmem<N>(ctx, a, chunks, ppc);
         else if (a.density_lane_shape == 3) launch_lane_xy<N, XY_DENSITY, 3>(ctx, a, chunks, ppc);
         else launch_lane_xy<N, XY_DENSITY, 2>(ctx, a, chunks, ppc);
         return;

@@ -80,12 +80,13 @@ def test_autotune_keeps_results(precision):
     a.close()
 
 
-@pytest.mark.parametrize("shape", [5, 6])
+@pytest.mark.parametrize("shape", [5, 6, 7])
 @pytest.mark.parametrize("name", ["si8", "si64", "h2o32"])
 def test_density_half_planes(name, shape, monkeypatch):
-    """The half-plane density kernel (shape 5: two CTAs per plane) and the
+    """The half-plane density kernel (shape 5: two CTAs per plane), the
     whole-plane kernel reading the sticks through the column map (shape 6)
-    give the default kernel's density (FP32, 2e-6 of the largest value)."""
+    and the kernel accumulating in tensor memory (shape 7) give the default
+    kernel's density (FP32, 2e-6 of the largest value)."""
     s = systems.get(name)
     ref = _ctx(s, capi.MIXED, True)
     monkeypatch.setenv("QBX_FAST_DENSITY_LANE_SHAPE", str(shape))
@@ -116,3 +117,21 @@ def test_vpsi_sticks_through_column_map(name, shape, monkeypatch):
     assert abs(ea["etotal"] - eb["etotal"]) < 1e-6 * len(s.atoms)
     ref.close()
     alt.close()
+
+
+def test_density_tmem_si512(monkeypatch):
+    """The tensor-memory density kernel (shape 7) on the 512-atom cell's
+    140^3 grid, where each thread holds 2 rows x 35 points in 3 column
+    blocks of tensor memory, gives the default kernel's density (FP32, 2e-6
+    of the largest value)."""
+    s = systems.si512().band_sample(32)
+    ref = _ctx(s, capi.MIXED, True)
+    monkeypatch.setenv("QBX_FAST_DENSITY_LANE_SHAPE", "7")
+    tm = _ctx(s, capi.MIXED, True)
+    monkeypatch.delenv("QBX_FAST_DENSITY_LANE_SHAPE")
+    ref.update_density()
+    tm.update_density()
+    ra, rb = ref.density(), tm.density()
+    np.testing.assert_allclose(rb, ra, rtol=0, atol=2e-6 * np.abs(ra).max())
+    ref.close()
+    tm.close()
