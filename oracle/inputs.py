@@ -67,6 +67,11 @@ def write_system(sysdef, workdir: str, c: Optional[np.ndarray] = None) -> str:
         lines.append(f"atom {name}{count[name]} {name} "
                      + " ".join(f"{x:.17e}" for x in pos))
     lines.append(f"coeffs {os.path.join(workdir, 'coeffs.bin')}")
+    for ik, (k, w) in enumerate(sysdef.kpoints or []):
+        p = os.path.join(workdir, f"coeffs_k{ik}.bin")
+        hk = sysdef.kmiller(ik)
+        write_coeffs(p, hk, sysdef.kcoefficients(ik, hk))
+        lines.append(f"kpoint {k[0]:.17e} {k[1]:.17e} {k[2]:.17e} {w:.17e} {p}")
     path = os.path.join(workdir, "system.txt")
     with open(path, "w") as f:
         f.write("\n".join(lines) + "\n")
@@ -172,6 +177,8 @@ def load_outputs(workdir: str) -> Dict:
              "t_vhxc", "t_energy", "t_wf_update"]
     out["energies"] = {n: e[:, i] for i, n in enumerate(names)}
     nst, ngw = meta["nst"], meta["ngw"]
+    nkp = meta.get("nkp", 1)
+    kfiles = os.path.exists(os.path.join(workdir, "final_k0_c.bin"))
     grid = (meta["np2v"], meta["np1v"], meta["np0v"])
     s = 0
     while os.path.exists(os.path.join(workdir, f"step{s}_rhor.bin")):
@@ -179,9 +186,15 @@ def load_outputs(workdir: str) -> Dict:
         d = {}
         d["rhor"] = np.fromfile(pre + "rhor.bin").reshape(grid)
         d["vr"] = np.fromfile(pre + "vr.bin").reshape(grid)
-        for k in ("hc", "c"):
-            a = np.fromfile(pre + f"{k}.bin").reshape(nst, ngw, 2)
-            d[k] = a[..., 0] + 1j * a[..., 1]
+        if kfiles:
+            for ik in range(nkp):
+                for k in ("hc", "c"):
+                    a = np.fromfile(pre + f"k{ik}_{k}.bin").reshape(nst, meta[f"ngw_k{ik}"], 2)
+                    d[f"k{ik}_{k}"] = a[..., 0] + 1j * a[..., 1]
+        else:
+            for k in ("hc", "c"):
+                a = np.fromfile(pre + f"{k}.bin").reshape(nst, ngw, 2)
+                d[k] = a[..., 0] + 1j * a[..., 1]
         out[f"step{s}"] = d
         s += 1
     for s in range(int(e[-1, 0]) + 1):
@@ -191,6 +204,10 @@ def load_outputs(workdir: str) -> Dict:
         fs = os.path.join(workdir, f"step{s}_sigma.txt")
         if os.path.exists(fs):
             out[f"sigma{s}"] = np.loadtxt(fs)
+    for ik in range(nkp if kfiles else 0):
+        a = np.fromfile(os.path.join(workdir, f"final_k{ik}_c.bin")).reshape(
+            nst, meta[f"ngw_k{ik}"], 2)
+        out[f"final_k{ik}_c"] = a[..., 0] + 1j * a[..., 1]
     fc = os.path.join(workdir, "final_c.bin")
     if os.path.exists(fc):
         a = np.fromfile(fc).reshape(nst, ngw, 2)

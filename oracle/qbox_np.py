@@ -936,6 +936,215 @@ class ElectronicStep:
         return out
 
 
+class KPoint:
+    """One k point off Gamma: the complex basis {G: |k+G|^2 < 2 ecut} over the
+    whole sphere (src/Basis.cpp:449-486, update_g :646-690 with kpg), its
+    coefficients c[n, ig] in sorted Miller order, the projector forms at k+G
+    (src/NonLocalPotential.cpp:235-560 with the basis's kpg, kpgi, kpgx) and
+    the PSDA history."""
+
+    def __init__(self, es: "ElectronicStep", k, weight: float, hkl: np.ndarray,
+                 c: np.ndarray):
+        self.k = np.array(k, float)
+        self.weight = float(weight)
+        self.hkl = np.asarray(hkl, np.int64)
+        b = reciprocal(es.cell)
+        self.kpgx = (self.hkl + self.k[None, :]) @ b
+        self.kpg2 = (self.kpgx ** 2).sum(1)
+        self.kpg = np.sqrt(self.kpg2)
+        with np.errstate(divide="ignore"):
+            self.kpgi = np.where(self.kpg > 0, 1.0 / np.where(self.kpg > 0, self.kpg, 1), 0.0)
+        n0, n1, n2 = es.grid_shape
+        h, kk, l = self.hkl[:, 0], self.hkl[:, 1], self.hkl[:, 2]
+        self.ip = ((l % n2) * n1 + (kk % n1)) * n0 + (h % n0)
+        # the first coefficient of the reference's local basis: rod (0,0)
+        # is moved to the front (src/Basis.cpp:587-597), its lowest l first
+        on = np.flatnonzero((h == 0) & (kk == 0))
+        self.first = int(on[np.argmin(l[on])])
+        self.c = np.array(c, complex)
+        self.c_last = None
+        self.dc_last = None
+        s14pi, s34pi = math.sqrt(1.0 / FPI), math.sqrt(3.0 / FPI)
+        self.nl = []
+        for isp, sp in enumerate(es.species):
+            if not sp.proj:
+                continue
+            tw, lp, dfac = [], [], []
+            for iop, (lq, _, _) in enumerate(sp.proj):
+                v, dv = sp.vnlg(iop, self.kpg)
+                if lq == 0:
+                    tw.append(s14pi * v); lp.append(0); dfac.append(sp.dmat[0])
+                else:
+                    for j in range(3):
+                        tw.append(s34pi * self.kpgx[:, j] * self.kpgi * v)
+                        lp.append(1); dfac.append(sp.dmat[1])
+            self.nl.append((isp, np.array(tw), np.array(lp), np.array(dfac)))
+
+
+class KPointStep:
+    """The electronic step of ElectronicStep on a set of k points off Gamma,
+    each a complex SlaterDet (src/SlaterDet.cpp complex branches): one band
+    per FFT, C^H C products, k-weighted sums (src/ChargeDensity.cpp:136-198,
+    src/EnergyFunctional.cpp:440-560, :700-716, src/Wavefunction.cpp:814-830).
+    The density, potentials and the Coulomb and XC energies are the Gamma
+    machinery of an ElectronicStep on the same cell and atoms."""
+
+    def __init__(self, system, cs: Optional[List[np.ndarray]] = None):
+        self.base = ElectronicStep(system)
+        es = self.base
+        self.nst = es.nst
+        self.occ = es.occ
+        self.kpts = []
+        for ik, (k, w) in enumerate(system.kpoints):
+            hkl = system.kmiller(ik)
+            c = system.kcoefficients(ik, hkl) if cs is None else cs[ik]
+            self.kpts.append(KPoint(es, k, w, hkl, c))
+        self.extrapolate = False
+        self.gram()
+
+    # ---- complex SlaterDet operations
+    def gram(self):
+        """src/SlaterDet.cpp:524-533: S = C^H C = L L^H, C <- C L^-H."""
+        for kp in self.kpts:
+            L = np.linalg.cholesky(np.conj(kp.c) @ kp.c.T)
+            kp.c = np.linalg.solve(np.conj(L), kp.c)
+
+    def ortho_align(self, kp):
+        """src/SlaterDet.cpp:877-975: L = chol(C^H C), X = L^-1 C^H C_last,
+        X <- unitary polar factor, C <- C L^-H X."""
+        L = np.linalg.cholesky(np.conj(kp.c) @ kp.c.T)
+        x = np.conj(kp.c) @ kp.c_last.T
+        x = np.linalg.solve(L, x)
+        x = polar_complex(x, 1.e-6, 20)
+        x = np.linalg.solve(np.conj(L).T, x)
+        kp.c = x.T @ kp.c
+
+    def _backward(self, kp, c):
+        z = np.zeros(self.base.N, complex)
+        z[kp.ip] = c
+        return np.fft.ifftn(z.reshape(self.base.wgrid.shape)) * self.base.N
+
+    def _forward(self, kp, f):
+        return (np.fft.fftn(f.reshape(self.base.wgrid.shape)) / self.base.N).ravel()[kp.ip]
+
+    # ---- density (src/SlaterDet.cpp:280-298 complex branch)
+    def update_density(self):
+        es = self.base
+        rho = np.zeros(es.N)
+        for kp in self.kpts:
+            for n in range(self.nst):
+                f = self._backward(kp, kp.c[n]).ravel()
+                rho += kp.weight * self.occ[n] / es.omega * (f.real ** 2 + f.imag ** 2)
+        es.rhor = rho
+        es.total_charge = rho.sum() * es.omega / es.N
+        es.rhog = es.vgrid.forward(es.omega * rho)
+
+    def update_vhxc(self):
+        self.base.update_vhxc()
+
+    def anl(self, kp, isp, tw, lp):
+        """src/NonLocalPotential.cpp:1316-1394 at k: twnl(k+G) (-i)^l
+        exp(-i (k+G).tau)."""
+        tau = self.base.positions[isp]
+        e = np.exp(-1j * (kp.kpgx @ tau.T)).T
+        a = tw[:, None, :] * e[None, :, :]
+        a[lp == 1] *= -1j
+        return a
+
+    def nonlocal_energy(self, kp, hc):
+        """src/NonLocalPotential.cpp:1420-1610, complex branch: F = A^H C,
+        E_nl = sum occ D |F|^2 / Omega, HC += A D F / Omega."""
+        enl = 0.0
+        om_inv = 1.0 / self.base.omega
+        for isp, tw, lp, dfac in kp.nl:
+            a = self.anl(kp, isp, tw, lp)
+            npr, na, ng = a.shape
+            af = a.reshape(npr * na, ng)
+            F = np.conj(af) @ kp.c.T                    # (npr*na, nst)
+            DF = F * np.repeat(dfac, na)[:, None]
+            enl += om_inv * (self.occ[None, :] * (F.real * DF.real + F.imag * DF.imag)).sum()
+            if hc is not None:
+                hc += (om_inv * DF).T @ af
+        return enl
+
+    def energy(self, compute_hpsi=True):
+        es = self.base
+        self.ekin = 0.0
+        self.enl = 0.0
+        for kp in self.kpts:
+            psi2 = (0.5 * self.occ[:, None] * np.abs(kp.c) ** 2).sum(0)
+            self.ekin += kp.weight * (psi2 * kp.kpg2).sum()
+            hc = np.zeros_like(kp.c) if compute_hpsi else None
+            self.enl += kp.weight * self.nonlocal_energy(kp, hc)
+            if compute_hpsi:
+                hc += 0.5 * kp.kpg2[None, :] * kp.c
+                for n in range(self.nst):
+                    f = self._backward(kp, kp.c[n]).ravel() * es.v_r
+                    hc[n] += self._forward(kp, f)
+                kp.hc = hc
+        self.eps, self.exc, self.ehart = es.eps, es.exc, es.ehart
+        self.esr, self.eself = es.esr, es.eself
+        self.ecoul = es.ehart + es.esr - es.eself
+        self.etotal = self.ekin + es.eps + self.enl + self.ecoul + es.exc
+        return self.etotal
+
+    def eigenvalue_sum(self):
+        """Wavefunction::dot (src/Wavefunction.cpp:814-830, complex
+        SlaterDet::dot src/SlaterDet.cpp:1149-1152): sum_k w_k Re tr(C^H HC)."""
+        return sum(kp.weight * (np.conj(kp.c) * kp.hc).real.sum() for kp in self.kpts)
+
+    def kdiag(self, kp):
+        """src/Preconditioner.cpp:88-143 on a complex basis: fac = 1, and the
+        reference still removes half of |c|^2 of the first local coefficient
+        from the norm (its G = 0 correction, here rod (0,0)'s first)."""
+        p2 = np.abs(kp.c) ** 2
+        snorm = p2.sum(1) - 0.5 * p2[:, kp.first]
+        sek = (p2 * kp.kpg2[None, :]).sum(1)
+        ekin = np.where(0.5 * snorm > 0.0, 0.5 * sek / np.where(snorm != 0, snorm, 1), 0.0)
+        ekin = np.where(ekin == 0.0, 1.0, ekin)
+        e = 0.5 * kp.kpg2[None, :]
+        with np.errstate(divide="ignore"):
+            return np.where(e < ekin[:, None], 0.5 / ekin[:, None], 0.5 / e)
+
+    def psda_update(self):
+        """src/PSDAWavefunctionStepper.cpp:46-249, complex branch, per k point
+        (theta of each k point from its own sums)."""
+        for kp in self.kpts:
+            a = np.conj(kp.c) @ kp.hc.T                # A = C^H HC
+            hc = kp.hc - a.T @ kp.c                    # HC - C A
+            dc = -self.kdiag(kp) * hc
+            x = kp.c
+            if self.extrapolate:
+                df = dc - kp.dc_last
+                av = (dc.real * df.real + dc.imag * df.imag).sum()
+                bv = (df.real ** 2 + df.imag ** 2).sum()
+                theta = -av / bv if bv != 0.0 else 0.0
+                if theta < -1.0:
+                    theta = 0.0
+                theta = min(2.0, theta)
+                kp.theta = theta
+                newc = x + theta * (x - kp.c_last) + dc + theta * (dc - kp.dc_last)
+            else:
+                kp.theta = 0.0
+                newc = x + dc
+            kp.c_last = x.copy()
+            kp.dc_last = dc
+            kp.c = newc
+            self.ortho_align(kp)
+        self.extrapolate = True
+
+    def step(self) -> Dict[str, float]:
+        self.update_density()
+        self.update_vhxc()
+        self.energy(True)
+        eig = self.eigenvalue_sum()
+        out = dict(ekin=self.ekin, eps=self.eps, enl=self.enl, ehart=self.ehart,
+                   ecoul=self.ecoul, exc=self.exc, esr=self.esr, eself=self.eself,
+                   etotal=self.etotal, eigenvalue_sum=eig)
+        self.psda_update()
+        return out
+
+
 AMU = 1822.89      # atomic mass unit in electron masses, src/IonicStepper.cpp:40
 
 
@@ -1139,5 +1348,28 @@ def polar(x, tol, maxiter):
         else:
             x = 0.5 * (x + np.linalg.inv(x.T))
         if qn <= tol:      # the update above still runs on the last pass
+            break
+    return x
+
+
+def polar_complex(x, tol, maxiter):
+    """ComplexMatrix::polar (src/Matrix.cpp:2524-2595): Bjorck-Bowie while
+    ||I - X^H X||_F < 1, else the Higham step X <- (X + X^-H)/2.  (The
+    reference's serial ComplexMatrix::transpose leaves the diagonal
+    unconjugated, src/Matrix.cpp:1182-1190; the ScaLAPACK build's pztranc
+    conjugates it; this follows the latter.)"""
+    n = x.shape[0]
+    eye = np.eye(n)
+    for _ in range(maxiter):
+        q = eye - np.conj(x).T @ x
+        qn = math.sqrt((np.abs(q) ** 2).sum())
+        if qn < 1.0:
+            t = eye + 0.75 * q
+            qt = q @ t
+            t = eye + 0.5 * qt
+            x = x @ t
+        else:
+            x = 0.5 * (x + np.linalg.inv(np.conj(x).T))
+        if qn <= tol:
             break
     return x

@@ -28,6 +28,11 @@
 // (a.u.), no thermostat; its printed output goes to md_log.txt, the final
 // positions and velocities to md_tau.txt and md_vel.txt and the final
 // coefficients to final_c.bin.
+// k points: "kpoint kx ky kz weight coeffs.bin" lines in the system file (k in
+// units of the reciprocal vectors) replace the Gamma point by those k points
+// (Wavefunction::add_kpoint, del_kpoint; src/Wavefunction.cpp:400-485), each
+// with its own complex basis and coefficients keyed by Miller index; the
+// PSDA loop then dumps step<N>_k<ik>_{c,hc}.bin and final_k<ik>_c.bin.
 // forces = 1: ionic forces at the dumped steps and the last step; forces = 2:
 // forces and the stress tensor (EnergyFunctional::energy with
 // compute_stress, src/EnergyFunctional.cpp:397-1044), written as
@@ -128,6 +133,8 @@ int main(int argc, char** argv)
   ifstream in(sysfile.c_str());
   if ( !in ) { cerr << "cannot open " << sysfile << endl; return 1; }
   string key, coeff_file;
+  struct KLine { double k[3], w; string path; };
+  vector<KLine> klines;
   double a[9] = {0};
   double ecut_ry = 0.0;
   int nel = 0;
@@ -154,6 +161,11 @@ int main(int argc, char** argv)
       atom_count++;
     }
     else if ( key == "coeffs" ) in >> coeff_file;
+    else if ( key == "kpoint" )
+    {
+      KLine kl; in >> kl.k[0] >> kl.k[1] >> kl.k[2] >> kl.w >> kl.path;
+      klines.push_back(kl);
+    }
     else { cerr << "unknown key " << key << endl; return 1; }
   }
   UnitCell cell(D3vector(a[0],a[1],a[2]), D3vector(a[3],a[4],a[5]),
@@ -162,6 +174,61 @@ int main(int argc, char** argv)
   s.wf.resize(cell, cell, 0.5 * ecut_ry);
   s.wf.set_nel(nel);
   s.wf.update_occ(0.0);
+  if ( !klines.empty() )
+  {
+    for ( size_t i = 0; i < klines.size(); i++ )
+      s.wf.add_kpoint(D3vector(klines[i].k[0],klines[i].k[1],klines[i].k[2]),
+                      klines[i].w);
+    s.wf.del_kpoint(D3vector(0,0,0));
+  }
+  const int nkp = s.wf.nkp();
+
+  // ---- coefficients of each k point, keyed by Miller index ----
+  // perms[ikp][ig] = input row of reference coefficient ig
+  vector<vector<int> > perms(nkp);
+  for ( int ikp = 0; ikp < nkp; ikp++ )
+  {
+    const string path = klines.empty() ? coeff_file : klines[ikp].path;
+    SlaterDet& sdk = *s.wf.sd(0,ikp);
+    const Basis& bk = sdk.basis();
+    const int ngwk = bk.localsize();
+    const int nstk = sdk.nst();
+    ComplexMatrix& ck = sdk.c();
+    FILE* fc = fopen(path.c_str(), "rb");
+    if ( !fc ) { cerr << "cannot open " << path << endl; return 1; }
+    int hdr[2];
+    if ( fread(hdr, sizeof(int), 2, fc) != 2 ) return 1;
+    if ( hdr[0] != ngwk || hdr[1] != nstk )
+    {
+      cerr << "basis mismatch: file ngw=" << hdr[0] << " nb=" << hdr[1]
+           << " reference ngw=" << ngwk << " nst=" << nstk << endl;
+      return 1;
+    }
+    vector<int> hkl(3*ngwk);
+    if ( fread(&hkl[0], sizeof(int), 3*ngwk, fc) != (size_t)(3*ngwk) ) return 1;
+    vector<double> cin(2*(size_t)ngwk*nstk);
+    if ( fread(&cin[0], sizeof(double), cin.size(), fc) != cin.size() ) return 1;
+    fclose(fc);
+    map<Key,int> row_of;
+    for ( int i = 0; i < ngwk; i++ )
+      row_of[Key{hkl[3*i],hkl[3*i+1],hkl[3*i+2]}] = i;
+    vector<int>& pk = perms[ikp];
+    pk.resize(ngwk);
+    for ( int ig = 0; ig < ngwk; ig++ )
+    {
+      Key k{bk.idx(3*ig), bk.idx(3*ig+1), bk.idx(3*ig+2)};
+      map<Key,int>::iterator it = row_of.find(k);
+      if ( it == row_of.end() ) { cerr << "Miller index missing" << endl; return 1; }
+      pk[ig] = it->second;
+    }
+    for ( int n = 0; n < nstk; n++ )
+      for ( int ig = 0; ig < ngwk; ig++ )
+      {
+        const size_t src = 2*((size_t)n*ngwk + pk[ig]);
+        ck[ig + (size_t)n*ck.mloc()] = complex<double>(cin[src], cin[src+1]);
+      }
+  }
+  s.wf.gram();
 
   SlaterDet& sd = *s.wf.sd(0,0);
   const Basis& basis = sd.basis();
@@ -169,42 +236,22 @@ int main(int argc, char** argv)
   const int nst = sd.nst();
   ComplexMatrix& c = sd.c();
   const int mloc = c.mloc();
-
-  // ---- coefficients, keyed by Miller index ----
-  FILE* fc = fopen(coeff_file.c_str(), "rb");
-  if ( !fc ) { cerr << "cannot open " << coeff_file << endl; return 1; }
-  int hdr[2];
-  if ( fread(hdr, sizeof(int), 2, fc) != 2 ) return 1;
-  const int ngw_in = hdr[0], nb_in = hdr[1];
-  if ( ngw_in != ngw || nb_in != nst )
-  {
-    cerr << "basis mismatch: file ngw=" << ngw_in << " nb=" << nb_in
-         << " reference ngw=" << ngw << " nst=" << nst << endl;
-    return 1;
-  }
-  vector<int> hkl(3*ngw);
-  if ( fread(&hkl[0], sizeof(int), 3*ngw, fc) != (size_t)(3*ngw) ) return 1;
-  vector<double> cin(2*(size_t)ngw*nst);
-  if ( fread(&cin[0], sizeof(double), cin.size(), fc) != cin.size() ) return 1;
-  fclose(fc);
-  map<Key,int> row_of;
-  for ( int i = 0; i < ngw; i++ )
-    row_of[Key{hkl[3*i],hkl[3*i+1],hkl[3*i+2]}] = i;
-  vector<int> perm(ngw);  // perm[ig] = input row of reference coefficient ig
-  for ( int ig = 0; ig < ngw; ig++ )
-  {
-    Key k{basis.idx(3*ig), basis.idx(3*ig+1), basis.idx(3*ig+2)};
-    map<Key,int>::iterator it = row_of.find(k);
-    if ( it == row_of.end() ) { cerr << "Miller index missing" << endl; return 1; }
-    perm[ig] = it->second;
-  }
-  for ( int n = 0; n < nst; n++ )
-    for ( int ig = 0; ig < ngw; ig++ )
-    {
-      const size_t src = 2*((size_t)n*ngw + perm[ig]);
-      c[ig + (size_t)n*mloc] = complex<double>(cin[src], cin[src+1]);
-    }
-  s.wf.gram();
+  const vector<int>& perm = perms[0];
+  // coefficients of k point ikp of a wavefunction in the input order
+  auto input_order = [&](const Wavefunction& w, int ikp) {
+    const ComplexMatrix& m = w.sd(0,ikp)->c();
+    const vector<int>& pk = perms[ikp];
+    const int ngwk = (int)pk.size();
+    vector<double> out(2*(size_t)ngwk*nst);
+    for ( int n = 0; n < nst; n++ )
+      for ( int ig = 0; ig < ngwk; ig++ )
+      {
+        const complex<double> v = m[ig + (size_t)n*m.mloc()];
+        const size_t dst = 2*((size_t)n*ngwk + pk[ig]);
+        out[dst] = v.real(); out[dst+1] = v.imag();
+      }
+    return out;
+  };
 
   if ( wf_dyn == "PRINT" )
   {
@@ -319,7 +366,9 @@ int main(int argc, char** argv)
          << "\nnp1v " << vft.np1() << "\nnp2v " << vft.np2()
          << "\nng_v " << cd.vbasis()->localsize()
          << "\nnrods " << basis.nrods() << "\nomega " << cell.volume()
-         << "\nnatoms " << atom_count << "\n";
+         << "\nnatoms " << atom_count << "\nnkp " << nkp << "\n";
+    for ( int ikp = 0; ikp < nkp; ikp++ )
+      meta << "ngw_k" << ikp << " " << perms[ikp].size() << "\n";
   }
 
   stepper->preprocess();
@@ -342,24 +391,15 @@ int main(int argc, char** argv)
       write_bin(pre.str() + "rhor.bin", &cd.rhor[0][0], np012 * sizeof(double));
       write_bin(pre.str() + "vr.bin", &ef.v_r[0][0], np012 * sizeof(double));
       // C and H*C in the input (sorted Miller) order
-      vector<double> out(2*(size_t)ngw*nst);
-      const ComplexMatrix& hc = dwf.sd(0,0)->c();
-      for ( int n = 0; n < nst; n++ )
-        for ( int ig = 0; ig < ngw; ig++ )
-        {
-          const complex<double> v = hc[ig + (size_t)n*mloc];
-          const size_t dst = 2*((size_t)n*ngw + perm[ig]);
-          out[dst] = v.real(); out[dst+1] = v.imag();
-        }
-      write_bin(pre.str() + "hc.bin", &out[0], out.size()*sizeof(double));
-      for ( int n = 0; n < nst; n++ )
-        for ( int ig = 0; ig < ngw; ig++ )
-        {
-          const complex<double> v = c[ig + (size_t)n*mloc];
-          const size_t dst = 2*((size_t)n*ngw + perm[ig]);
-          out[dst] = v.real(); out[dst+1] = v.imag();
-        }
-      write_bin(pre.str() + "c.bin", &out[0], out.size()*sizeof(double));
+      for ( int ikp = 0; ikp < nkp; ikp++ )
+      {
+        ostringstream kp;
+        if ( !klines.empty() ) kp << "k" << ikp << "_";
+        vector<double> out = input_order(dwf, ikp);
+        write_bin(pre.str() + kp.str() + "hc.bin", &out[0], out.size()*sizeof(double));
+        out = input_order(s.wf, ikp);
+        write_bin(pre.str() + kp.str() + "c.bin", &out[0], out.size()*sizeof(double));
+      }
     }
     if ( sstep )
     {
@@ -388,16 +428,14 @@ int main(int argc, char** argv)
     eo.flush();
   }
   // final wavefunctions
+  for ( int ikp = 0; ikp < nkp; ikp++ )
   {
-    vector<double> out(2*(size_t)ngw*nst);
-    for ( int n = 0; n < nst; n++ )
-      for ( int ig = 0; ig < ngw; ig++ )
-      {
-        const complex<double> v = c[ig + (size_t)n*mloc];
-        const size_t dst = 2*((size_t)n*ngw + perm[ig]);
-        out[dst] = v.real(); out[dst+1] = v.imag();
-      }
-    write_bin(outdir + "/final_c.bin", &out[0], out.size()*sizeof(double));
+    ostringstream fn;
+    fn << outdir << "/final_" << (klines.empty() ? "" : "k") ;
+    if ( !klines.empty() ) fn << ikp << "_";
+    fn << "c.bin";
+    vector<double> out = input_order(s.wf, ikp);
+    write_bin(fn.str(), &out[0], out.size()*sizeof(double));
   }
   delete stepper;
   return 0;

@@ -95,6 +95,8 @@ class System:
     xc: str
     seed: int
     nel_override: Optional[int] = None   # electrons when not the ions' total
+    # k points (units of the reciprocal vectors) and weights; None = Gamma
+    kpoints: Optional[List[tuple]] = None
 
     @property
     def ecut(self) -> float:      # Hartree
@@ -117,6 +119,24 @@ class System:
 
     def miller(self) -> np.ndarray:
         return gamma_miller(self.cell, self.ecut)
+
+    def kmiller(self, ik: int) -> np.ndarray:
+        return kpoint_miller(self.cell, self.ecut, self.kpoints[ik][0])
+
+    def kcoefficients(self, ik: int, hkl: Optional[np.ndarray] = None) -> np.ndarray:
+        """(nbands, ngw_k) complex128 for k point ik, keyed by its sorted
+        Miller list (no constraint at G = 0: the basis is complex)."""
+        if hkl is None:
+            hkl = self.kmiller(ik)
+        rng = np.random.default_rng(1000 * self.seed + 7 + ik)
+        ngw = hkl.shape[0]
+        return rng.standard_normal((self.nbands, ngw)) \
+            + 1j * rng.standard_normal((self.nbands, ngw))
+
+    def with_kpoints(self, kpoints, name: Optional[str] = None) -> "System":
+        return dataclasses.replace(self, kpoints=[(tuple(map(float, k)), float(w))
+                                                  for k, w in kpoints],
+                                   name=name or f"{self.name}_k{len(kpoints)}")
 
     def coefficients(self, hkl: Optional[np.ndarray] = None) -> np.ndarray:
         """(nbands, ngw) complex128, keyed by the sorted Miller list."""
@@ -157,6 +177,21 @@ def gamma_miller(cell: np.ndarray, ecut: float) -> np.ndarray:
     gz = h * b[0, 2] + k * b[1, 2] + l * b[2, 2]
     inside = gx * gx + gy * gy + gz * gz < 2.0 * ecut
     hkl = np.stack([h[inside], k[inside], l[inside]], axis=1).astype(np.int32)
+    order = np.lexsort((hkl[:, 2], hkl[:, 1], hkl[:, 0]))
+    return np.ascontiguousarray(hkl[order])
+
+
+def kpoint_miller(cell: np.ndarray, ecut: float, kpoint) -> np.ndarray:
+    """Sorted (h,k,l) of the complex basis at k: {G: |k+G|^2 < 2 ecut} over
+    the whole sphere (the rod set of src/Basis.cpp:449-486)."""
+    b = reciprocal(cell)
+    fac = math.sqrt(2.0 * ecut) / (2.0 * math.pi)
+    m = [int(1.5 + fac * np.linalg.norm(cell[i])) for i in range(3)]
+    h, k, l = np.meshgrid(np.arange(-m[0], m[0] + 1), np.arange(-m[1], m[1] + 1),
+                          np.arange(-m[2], m[2] + 1), indexing="ij")
+    q = np.stack([h.ravel() + kpoint[0], k.ravel() + kpoint[1], l.ravel() + kpoint[2]], 1) @ b
+    inside = (q * q).sum(1) < 2.0 * ecut
+    hkl = np.stack([h.ravel()[inside], k.ravel()[inside], l.ravel()[inside]], 1).astype(np.int32)
     order = np.lexsort((hkl[:, 2], hkl[:, 1], hkl[:, 0]))
     return np.ascontiguousarray(hkl[order])
 
@@ -263,7 +298,20 @@ def batch(nsys: int = 32, seed: int = 3) -> List[System]:
     return out
 
 
-REGISTRY = {"si8": si8, "si64": si64, "si512": si512, "h2o32": h2o32}
+def si8k2() -> System:
+    """si8 at two k points off Gamma (complex bases), LDA."""
+    return si8().with_kpoints([((0.25, 0.25, 0.25), 0.5), ((-0.25, 0.25, 0.25), 0.5)],
+                              "si8k2")
+
+
+def h2o4k2() -> System:
+    """Four water molecules at two k points, PBE, two species."""
+    return h2o32(nmol=4, L=9.0, seed=9, ecut_ry=40.0, nbands=16).with_kpoints(
+        [((0.0, 0.5, 0.0), 0.5), ((0.25, 0.0, 0.5), 0.5)], "h2o4k2")
+
+
+REGISTRY = {"si8": si8, "si64": si64, "si512": si512, "h2o32": h2o32,
+            "si8k2": si8k2, "h2o4k2": h2o4k2}
 
 
 def get(name: str) -> System:

@@ -13,7 +13,9 @@ ref_<name>_jd.npz holds a JD-stepper run, ref_<name>_md.npz a molecular
 dynamics run and ref_<name>_gs.npz a ground-state SCF run with charge mixing
 of the reference's BOSampleStepper; ref_<name>_wf.npz the <wavefunction>
 element the reference's Wavefunction::print writes (base64) for a band
-sample, with the coefficients it wrote.
+sample, with the coefficients it wrote; ref_<name>.npz of a k-point system
+(KPOINT_CASES) the PSDA run on its complex bases, with H*psi and the final
+coefficients of a few bands of each k point.
 """
 from __future__ import annotations
 
@@ -139,6 +141,42 @@ def make_gs(name: str, workdir: str) -> str:
 WF_CASES = {"si8": 4}
 
 
+KPOINT_CASES = {"si8k2": 4, "h2o4k2": 3}
+
+
+def make_kpoint(name: str, nsteps: int, workdir: str) -> str:
+    """PSDA steps of the reference on the k points of a system (complex
+    bases): energies of each step, a density sample, H*psi of the first step
+    and the final coefficients (a few bands at sampled G) of each k point."""
+    s = systems.get(name)
+    out = inputs.run_reference(s, workdir, nsteps, dump_steps=1, threads=os.cpu_count())
+    meta = out["meta"]
+    e = out["energies"]
+    rng = np.random.default_rng(54321)
+    N = meta["np0v"] * meta["np1v"] * meta["np2v"]
+    idx = np.sort(rng.choice(N, NSAMPLE, replace=False))
+    st = out["step0"]
+    fx = dict(grid=np.array([meta["np0v"], meta["np1v"], meta["np2v"]]), nst=meta["nst"],
+              nkp=meta["nkp"], nsteps=nsteps, sample_idx=idx,
+              rhor_sample=st["rhor"].ravel()[idx], rhor_sum=st["rhor"].sum())
+    for ik in range(meta["nkp"]):
+        ngw = meta[f"ngw_k{ik}"]
+        gidx = np.sort(rng.choice(ngw, 512, replace=False))
+        fx[f"k{ik}_ngw"] = ngw
+        fx[f"k{ik}_g_idx"] = gidx
+        fx[f"k{ik}_hc_bands"] = st[f"k{ik}_hc"][:NBANDS_FULL, gidx]
+        fx[f"k{ik}_hc_norm2"] = (np.abs(st[f"k{ik}_hc"]) ** 2).sum(1)
+        fc = out[f"final_k{ik}_c"]
+        fx[f"k{ik}_final_c_bands"] = fc[:NBANDS_FULL, gidx]
+        fx[f"k{ik}_final_c_norm2"] = (np.abs(fc) ** 2).sum(1)
+    for k in ("ekin", "eps", "enl", "ehart", "ecoul", "exc", "esr", "eself",
+              "etotal", "eigenvalue_sum"):
+        fx["e_" + k] = e[k]
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), f"ref_{name}.npz")
+    np.savez_compressed(path, **fx)
+    return path
+
+
 def make_wf(name: str, workdir: str) -> str:
     """The sample-file <wavefunction> element the reference writes for the
     orthonormalised seeded coefficients of a band sample, and those
@@ -161,10 +199,12 @@ if __name__ == "__main__":
     import tempfile
     names = sys.argv[1:] or (list(CASES) + [n + "_jd" for n in JD_CASES]
                              + [n + "_md" for n in MD_CASES] + [n + "_gs" for n in GS_CASES]
-                             + [n + "_wf" for n in WF_CASES])
+                             + [n + "_wf" for n in WF_CASES] + list(KPOINT_CASES))
     for n in names:
         with tempfile.TemporaryDirectory() as td:
-            if n.endswith("_wf"):
+            if n in KPOINT_CASES:
+                print(make_kpoint(n, KPOINT_CASES[n], td))
+            elif n.endswith("_wf"):
                 print(make_wf(n[:-3], td))
             elif n.endswith("_gs"):
                 print(make_gs(n[:-3], td))

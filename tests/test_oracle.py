@@ -207,3 +207,32 @@ def test_oracle_scf_mixing_matches_reference():
     g = fx["g_idx"]
     np.testing.assert_allclose(es.c[:fx["final_c_bands"].shape[0], g], fx["final_c_bands"],
                                rtol=0, atol=1e-11)
+
+
+@pytest.mark.parametrize("name", ["si8k2", "h2o4k2"])
+def test_oracle_kpoints_match_reference(name):
+    """The k-point restatement (complex bases, one band per FFT, C^H C
+    products, k-weighted sums) against the reference's PSDA run on the same k
+    points: every energy term of each step to 1e-10 Ha, the density sample,
+    H*psi and the final coefficients of each k point."""
+    g = golden(name)
+    ks = qbox_np.KPointStep(systems.get(name))
+    assert len(ks.kpts) == int(g["nkp"])
+    for it in range(int(g["nsteps"])):
+        e = ks.step()
+        if it == 0:
+            np.testing.assert_allclose(ks.base.rhor[g["sample_idx"]], g["rhor_sample"],
+                                       rtol=0, atol=1e-13)
+            for ik, kp in enumerate(ks.kpts):
+                assert kp.hkl.shape[0] == int(g[f"k{ik}_ngw"])
+                gi = g[f"k{ik}_g_idx"]
+                np.testing.assert_allclose(kp.hc[:4, gi], g[f"k{ik}_hc_bands"], atol=1e-13)
+                np.testing.assert_allclose((np.abs(kp.hc) ** 2).sum(1), g[f"k{ik}_hc_norm2"],
+                                           rtol=1e-11)
+        for t in TERMS:
+            assert abs(e[t] - g["e_" + t][it]) < 1e-10, (it, t, e[t], g["e_" + t][it])
+    for ik, kp in enumerate(ks.kpts):
+        gi = g[f"k{ik}_g_idx"]
+        np.testing.assert_allclose(kp.c[:4, gi], g[f"k{ik}_final_c_bands"], atol=1e-12)
+        np.testing.assert_allclose((np.abs(kp.c) ** 2).sum(1), g[f"k{ik}_final_c_norm2"],
+                                   rtol=1e-12)
