@@ -119,6 +119,25 @@ int qbx_set_wf_dyn(qbx_context* ctx, const char* wf_dyn);
  * terms the context then holds, as the reference's energy functional does. */
 int qbx_jd_update(qbx_context* ctx);
 
+/* k points off Gamma: Wavefunction::add_kpoint for each of nkp k points
+ * (kpoints: 3 per k point, units of the reciprocal vectors; weights sum to
+ * one) with the Gamma point removed (del_kpoint), src/Wavefunction.cpp:
+ * 400-485.  Each k point gets a complex basis {G: |k+G|^2 < 2 ecut}
+ * (src/Basis.cpp:449-486) and a complex SlaterDet; qbx_gram,
+ * qbx_update_density, qbx_energy (forces and stress excepted),
+ * qbx_eigenvalue_sum, qbx_psda_update and qbx_scf_step then work on the k
+ * points with the reference's k-weighted sums, in FP64.  nkp = 0 returns
+ * to the Gamma point.  Call after qbx_set_cell. */
+int qbx_set_kpoints(qbx_context* ctx, int nkp, const double* kpoints,
+                    const double* weights);
+/* Basis size and Miller indices (3*ngw ints, may be NULL) of k point ikp,
+ * in the order of its coefficients (sorted h, k, l). */
+int qbx_kpoint_basis(const qbx_context* ctx, int ikp, int* ngw, int* hkl);
+/* Coefficients (ngw x nst complex, band-major) and H*psi of k point ikp. */
+int qbx_set_kpoint_coeffs(qbx_context* ctx, int ikp, const double* c);
+int qbx_get_kpoint_coeffs(qbx_context* ctx, int ikp, double* c);
+int qbx_get_kpoint_hpsi(qbx_context* ctx, int ikp, double* hc);
+
 /* One electronic step of the SCF loop with nite = 0
  * (src/BOSampleStepper.cpp:795-977): update_density, update_vhxc,
  * energy(true,...), eigenvalue_sum, PSDA update.  compute_forces: bit 0
@@ -315,6 +334,12 @@ int qbx_autotune(qbx_context* ctx, char* report, int report_len);
  * (if hkl != NULL) the 3*ngw Miller indices in the default order. */
 int qbx_host_basis(const double cell[9], double ecut, int* ngw, int* ngv,
                    int np[3], int* hkl);
+/* Basis::resize of the complex basis at k point k (units of the reciprocal
+ * vectors, src/Basis.cpp:449-486): its size, the index of the reference's
+ * first local coefficient (rod (0,0) moved to the front) and (if hkl !=
+ * NULL) the 3*ngw Miller indices in the library's order (sorted h, k, l). */
+int qbx_host_kbasis(const double cell[9], double ecut, const double k[3], int* ngw,
+                    int* first, int* hkl);
 /* Species::initialize_slpp + Species::dvlocg / vnlg (src/Species.cpp:
  * 1133-1185) evaluated at ng values of |G|: vloc[ng], dvloc[ng],
  * vnl[nproj*ng]. */

@@ -65,6 +65,7 @@ void drop_graphs(Context& c) {
 
 void free_cell(Context& c) {
   drop_graphs(c);
+  free_kpoints(c);
   free_mixed(c);
   free_mix(c);
   if (c.have_wgrid) free_sticks(c.dwg);
@@ -89,6 +90,7 @@ void free_cell(Context& c) {
 
 void free_atoms(Context& c) {
   drop_graphs(c);
+  kpoints_atoms_changed(c);
   if (c.h_fion) { cudaFreeHost(c.h_fion); c.h_fion = nullptr; }
   double** bufs[] = {&c.d_anl, &c.d_fnl, &c.d_dfnl, &c.d_pdfac, &c.d_sfac, &c.d_vps,
                      &c.d_rhops_sp, &c.d_fion, &c.d_dvps, &c.d_vnl, &c.d_dvnl,
@@ -155,6 +157,23 @@ void finish_step(Context& c, bool want_f, bool want_s) {
 // BOSampleStepper's electronic step (src/BOSampleStepper.cpp:795-1114 with
 // nite = 0), every operation on c.stream.
 void step_eager(Context& c, bool want_f, bool want_s, double* energies, double* fion) {
+  if (!c.kpts.empty()) {
+    // k points off Gamma: the same sequence on the complex SlaterDets
+    QBX_REQUIRE(!want_f && !want_s, 1, "forces and stress are not available at k points off Gamma");
+    update_density_k(c);
+    update_vhxc(c);
+    energy_k(c, true);
+    eigsum_k(c);
+    readback(c, false);
+    check_status(c);
+    finish_step(c, false, false);
+    fill_energies(c, energies);
+    psda_update_k(c);
+    readback(c, false);
+    check_status(c);
+    finish_theta(c);
+    return;
+  }
   update_density(c);
   update_vhxc(c);
   energy(c, true, want_f);
@@ -256,7 +275,7 @@ void capture_step(Context& c, bool want_f, StepGraph& g) {
 // runs eagerly (graphs off, JD, stress, profiling, or the first use of the
 // configuration, which sizes the lazily grown buffers before any capture).
 StepGraph* step_graph_for(Context& c, bool want_f, bool want_s) {
-  if (!c.step_graph || c.wf_dyn != 0 || want_s || c.prof.on) return nullptr;
+  if (!c.step_graph || c.wf_dyn != 0 || want_s || c.prof.on || !c.kpts.empty()) return nullptr;
   StepGraph& g = c.graphs[(c.extrapolate ? 1 : 0) + (want_f ? 2 : 0)];
   if (g.exec) return &g;
   if (g.uses++ == 0) return nullptr;
@@ -670,10 +689,57 @@ int qbx_get_hpsi(qbx_context* h, double* hc) {
   return h ? get_coeffs_impl(h, h->c.d_hc, hc, true) : 1;
 }
 
+int qbx_set_kpoints(qbx_context* h, int nkp, const double* kpoints, const double* weights) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, false);
+    QBX_REQUIRE(nkp >= 0 && (nkp == 0 || (kpoints && weights)), 1, "bad k point arguments");
+    drop_graphs(c);
+    set_kpoints(c, nkp, kpoints, weights);
+  });
+}
+
+static KPointSet& kpoint_of(Context& c, int ikp) {
+  QBX_REQUIRE(ikp >= 0 && ikp < (int)c.kpts.size(), 1, "no such k point");
+  return c.kpts[ikp];
+}
+
+int qbx_kpoint_basis(const qbx_context* h, int ikp, int* ngw, int* hkl) {
+  return guarded(const_cast<qbx_context*>(h), [&](Context& c) {
+    const KPointSet& kp = kpoint_of(c, ikp);
+    if (ngw) *ngw = kp.kb.ng;
+    if (hkl) std::memcpy(hkl, kp.kb.hkl.data(), sizeof(int) * kp.kb.hkl.size());
+  });
+}
+
+int qbx_set_kpoint_coeffs(qbx_context* h, int ikp, const double* src) {
+  return guarded(h, [&](Context& c) {
+    KPointSet& kp = kpoint_of(c, ikp);
+    QBX_REQUIRE(src, 1, "null coefficients");
+    const size_t n = 2 * (size_t)kp.kb.ng * c.nst;
+    QBX_CUDA(cudaMemcpyAsync(kp.d_c, src, n * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    QBX_CUDA(cudaStreamSynchronize(c.stream));
+    c.kpts_extrapolate = false;   // a new wavefunction starts a new history
+  });
+}
+
+static int get_kpoint_impl(qbx_context* h, int ikp, bool hpsi, double* dst) {
+  return guarded(h, [&](Context& c) {
+    KPointSet& kp = kpoint_of(c, ikp);
+    QBX_REQUIRE(dst, 1, "null output");
+    const size_t n = 2 * (size_t)kp.kb.ng * c.nst;
+    QBX_CUDA(cudaMemcpyAsync(dst, hpsi ? kp.d_hc : kp.d_c, n * sizeof(double),
+                             cudaMemcpyDeviceToHost, c.stream));
+    QBX_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+int qbx_get_kpoint_coeffs(qbx_context* h, int ikp, double* c) { return get_kpoint_impl(h, ikp, false, c); }
+int qbx_get_kpoint_hpsi(qbx_context* h, int ikp, double* hc) { return get_kpoint_impl(h, ikp, true, hc); }
+
 int qbx_gram(qbx_context* h) {
   return guarded(h, [&](Context& c) {
     check_ready(c, false);
-    gram(c);
+    if (!c.kpts.empty()) gram_k(c);
+    else gram(c);
     readback(c, false);
     check_status(c);
   });
@@ -682,7 +748,8 @@ int qbx_gram(qbx_context* h) {
 int qbx_update_density(qbx_context* h, double* total_charge) {
   return guarded(h, [&](Context& c) {
     check_ready(c, true);
-    update_density(c);
+    if (!c.kpts.empty()) update_density_k(c);
+    else update_density(c);
     readback(c, false);
     finish_density(c);
     if (total_charge) *total_charge = c.total_charge;
@@ -717,7 +784,12 @@ int qbx_get_vr(qbx_context* h, double* vr) {
 int qbx_energy(qbx_context* h, int hpsi, int forces, double* energies, double* fion) {
   return guarded(h, [&](Context& c) {
     check_ready(c, true);
-    energy(c, hpsi != 0, forces != 0);
+    if (!c.kpts.empty()) {
+      QBX_REQUIRE(!forces, 1, "forces are not available at k points off Gamma");
+      energy_k(c, hpsi != 0);
+    } else {
+      energy(c, hpsi != 0, forces != 0);
+    }
     readback(c, forces != 0);
     check_status(c);
     finish_energy(c, forces != 0);
@@ -729,7 +801,8 @@ int qbx_energy(qbx_context* h, int hpsi, int forces, double* energies, double* f
 int qbx_eigenvalue_sum(qbx_context* h, double* eig) {
   return guarded(h, [&](Context& c) {
     check_ready(c, true);
-    launch_eigsum(c);
+    if (!c.kpts.empty()) eigsum_k(c);
+    else launch_eigsum(c);
     readback(c, false);
     finish_eigsum(c);
     if (eig) *eig = c.eigsum;
@@ -739,7 +812,8 @@ int qbx_eigenvalue_sum(qbx_context* h, double* eig) {
 int qbx_psda_update(qbx_context* h) {
   return guarded(h, [&](Context& c) {
     check_ready(c, true);
-    psda_update(c);
+    if (!c.kpts.empty()) psda_update_k(c);
+    else psda_update(c);
     readback(c, false);
     check_status(c);
     finish_theta(c);
@@ -747,7 +821,10 @@ int qbx_psda_update(qbx_context* h) {
 }
 
 int qbx_psda_reset(qbx_context* h) {
-  return guarded(h, [&](Context& c) { c.extrapolate = false; });
+  return guarded(h, [&](Context& c) {
+    c.extrapolate = false;
+    c.kpts_extrapolate = false;
+  });
 }
 
 
@@ -778,6 +855,7 @@ int qbx_scf_run(qbx_context* h, int nitscf, int nite, double mix_coeff, double m
                 int* nite_done, int* nitscf_done) {
   return guarded(h, [&](Context& c) {
     check_ready(c, true);
+    QBX_REQUIRE(c.kpts.empty(), 1, "the charge-mixing SCF loop is not available at k points off Gamma");
     QBX_REQUIRE(nitscf > 0 && nite >= 0 && mix_coeff >= 0.0 && mix_rcut >= 0.0, 1,
                 "bad SCF arguments");
     scf_run(c, nitscf, nite, mix_coeff, mix_rcut, mix_ndim, scf_tol, etotal_int, eigsum,
@@ -788,6 +866,7 @@ int qbx_scf_run(qbx_context* h, int nitscf, int nite, double mix_coeff, double m
 int qbx_write_wavefunction(qbx_context* h, const char* path) {
   return guarded(h, [&](Context& c) {
     check_ready(c, false);
+    QBX_REQUIRE(c.kpts.empty(), 1, "the sample wavefunction writer is not available at k points off Gamma");
     QBX_REQUIRE(path, 1, "null path");
     std::ofstream os(path);
     QBX_REQUIRE(os.good(), 75, std::string("cannot write ") + path);
@@ -799,6 +878,7 @@ int qbx_write_wavefunction(qbx_context* h, const char* path) {
 int qbx_read_wavefunction(qbx_context* h, const char* path) {
   return guarded(h, [&](Context& c) {
     check_ready(c, false);
+    QBX_REQUIRE(c.kpts.empty(), 1, "the sample wavefunction reader is not available at k points off Gamma");
     QBX_REQUIRE(path, 1, "null path");
     std::ifstream is(path, std::ios::binary);
     QBX_REQUIRE(is.good(), 75, std::string("cannot read ") + path);
@@ -820,6 +900,7 @@ int qbx_md_run(qbx_context* h, int niter, int nitscf, double dt, const double* m
                double* vel, double* tau_out, double* ionic, double* scf) {
   return guarded(h, [&](Context& c) {
     check_ready(c, true);
+    QBX_REQUIRE(c.kpts.empty(), 1, "molecular dynamics is not available at k points off Gamma");
     QBX_REQUIRE(niter > 0 && nitscf >= 0 && dt != 0.0 && mass_amu, 1, "bad MD arguments");
     for (size_t is = 0; is < c.species.size(); is++)
       QBX_REQUIRE(mass_amu[is] > 0.0, 1, "species mass must be positive");
@@ -1004,6 +1085,7 @@ int qbx_set_wf_dyn(qbx_context* h, const char* name) {
 int qbx_jd_update(qbx_context* h) {
   return guarded(h, [&](Context& c) {
     check_ready(c, true);
+    QBX_REQUIRE(c.kpts.empty(), 1, "the JD stepper is not available at k points off Gamma");
     jd_update(c);
     readback(c, false);
     check_status(c);
@@ -1038,6 +1120,7 @@ static void copy_stress(const Context& c, double* sigma, double* parts) {
 int qbx_stress(qbx_context* h, double* sigma, double* parts) {
   return guarded(h, [&](Context& c) {
     check_ready(c, true);
+    QBX_REQUIRE(c.kpts.empty(), 1, "the stress tensor is not available at k points off Gamma");
     compute_stress(c);
     readback(c, false);
     check_status(c);
@@ -1183,6 +1266,22 @@ int qbx_host_basis(const double cell[9], double ecut, int* ngw, int* ngv, int np
     if (ngv) *ngv = v.ng;
     if (np) { np[0] = g[0]; np[1] = g[1]; np[2] = g[2]; }
     if (hkl) std::memcpy(hkl, w.hkl.data(), sizeof(int) * w.hkl.size());
+    return 0;
+  } catch (const Error& e) {
+    return e.code;
+  } catch (...) {
+    return 6;
+  }
+}
+
+int qbx_host_kbasis(const double cell[9], double ecut, const double k[3], int* ngw, int* first,
+                    int* hkl) {
+  try {
+    Basis b;
+    build_kbasis(b, cell, ecut, k);
+    if (ngw) *ngw = b.ng;
+    if (first) *first = b.first;
+    if (hkl) std::memcpy(hkl, b.hkl.data(), sizeof(int) * b.hkl.size());
     return 0;
   } catch (const Error& e) {
     return e.code;

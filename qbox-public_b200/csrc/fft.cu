@@ -583,6 +583,154 @@ static void staged_batch(Context& ctx, int op, const double* c, const double* v,
   }
 }
 
+// ------------------------------------------------ complex basis (k != 0)
+// One band per stick line: the basis at k has one rod per (h,k) column and
+// no -G half to fill (BasisMapping::vector_to_zvec and zvec_to_vector of a
+// complex basis, src/BasisMapping.cpp:585-627, 703-750).  zbuf holds band
+// `band0 + slot` in slot, [slot][z][stick] as for band pairs, so the plane
+// kernels run unchanged on the complex sticks.
+__global__ void __launch_bounds__(256)
+k_zfft_bwd_k(const double2* __restrict__ c, int ngw, int band0, DeviceSticks g,
+             const double2* __restrict__ twz, double2* __restrict__ zbuf, int rods_per_cta) {
+  using C = double2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  const int n2 = g.n2;
+  C* A = tw + n2;
+  C* B = A + rods_per_cta * n2;
+  const int r0 = blockIdx.x * rods_per_cta;
+  const int r1 = min(g.nrods, r0 + rods_per_cta);
+  const int nl = r1 - r0;
+  const int pl = blockIdx.y;
+  const double2* cb = c + (size_t)(band0 + pl) * ngw;
+  load_twiddles(tw, twz, n2);
+  const int half = (n2 + 1) / 2;
+  for (int t = threadIdx.x; t < nl * n2; t += blockDim.x) {
+    const int line = t / n2, z = t - line * n2;
+    const int r = r0 + line;
+    const int l = z < half ? z : z - n2;
+    const int lmin = g.rod_lmin[r];
+    C v = make_double2(0.0, 0.0);
+    if (l >= lmin && l < lmin + g.rod_size[r]) v = cb[g.rod_first[r] + (l - lmin)];
+    A[line * n2 + z] = v;
+  }
+  __syncthreads();
+  C* res = fft_lines<+1>(A, B, nl, n2, g.pz, tw);
+  C* out = zbuf + (size_t)pl * n2 * g.nvec;
+  for (int t = threadIdx.x; t < nl * n2; t += blockDim.x) {
+    const int line = t % nl, z = t / nl;
+    out[(size_t)z * g.nvec + r0 + line] = res[line * n2 + z];
+  }
+}
+
+// z transform back and hc = 1/2 |k+G|^2 c + (V psi)(G) / N
+__global__ void __launch_bounds__(256)
+k_zfft_fwd_k(const double2* __restrict__ zbuf, int ngw, int band0, DeviceSticks g,
+             const double2* __restrict__ twz, double scale, const double2* __restrict__ c,
+             const double* __restrict__ g2, double2* __restrict__ hc, int rods_per_cta) {
+  using C = double2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  const int n2 = g.n2;
+  C* A = tw + n2;
+  C* B = A + rods_per_cta * n2;
+  const int r0 = blockIdx.x * rods_per_cta;
+  const int r1 = min(g.nrods, r0 + rods_per_cta);
+  const int nl = r1 - r0;
+  const int pl = blockIdx.y;
+  load_twiddles(tw, twz, n2);
+  const C* in = zbuf + (size_t)pl * n2 * g.nvec;
+  for (int t = threadIdx.x; t < nl * n2; t += blockDim.x) {
+    const int line = t % nl, z = t / nl;
+    A[line * n2 + z] = in[(size_t)z * g.nvec + r0 + line];
+  }
+  __syncthreads();
+  C* res = fft_lines<-1>(A, B, nl, n2, g.pz, tw);
+  const int ig0 = g.rod_first[r0];
+  const int ig1 = g.rod_first[r1 - 1] + g.rod_size[r1 - 1];
+  const size_t boff = (size_t)(band0 + pl) * ngw;
+  for (int ig = ig0 + threadIdx.x; ig < ig1; ig += blockDim.x) {
+    int r = r0;
+    while (r + 1 < r1 && g.rod_first[r + 1] <= ig) ++r;
+    const int l = g.rod_lmin[r] + (ig - g.rod_first[r]);
+    const int z = ((l % n2) + n2) % n2;
+    const C p = res[(r - r0) * n2 + z];
+    const double kin = 0.5 * g2[ig];
+    const double2 a = c[boff + ig];
+    hc[boff + ig] = make_double2(kin * a.x + p.x * scale, kin * a.y + p.y * scale);
+  }
+}
+
+static constexpr int kRodsPerCtaK = 2 * kRodsPerCta;   // one line per rod
+
+// bands of a k point per pass through the context's stick buffer
+static int kbands_per_batch(const Context& ctx, const KPointSet& kp) {
+  const size_t per_band = (size_t)kp.dks.n2 * kp.dks.nvec * sizeof(double2);
+  const int nb = (int)std::min<size_t>((size_t)ctx.nst, ctx.zbuf_bytes / per_band);
+  QBX_REQUIRE(nb >= 1, 20, "stick buffer too small for one band of this k point");
+  return nb;
+}
+
+static void staged_k(Context& ctx, KPointSet& kp, int op, const double* v, double* rho) {
+  const DeviceSticks& g = kp.dks;
+  cudaStream_t st = ctx.stream;
+  double2* zbuf = (double2*)ctx.d_zbuf;
+  const int ngw = kp.kb.ng;
+  const size_t zs = zsmem<double>(g.n2);
+  allow_smem(k_zfft_bwd_k, zs);
+  allow_smem(k_zfft_fwd_k, zs);
+  XYConfig<double> xc = xy_config<double>(g, ctx.device);
+  allow_smem(k_xy<double, OP_DENSITY>, xc.smem);
+  allow_smem(k_xy<double, OP_VPSI>, xc.smem);
+  int sms = 0;
+  QBX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device));
+  const int nbmax = kbands_per_batch(ctx, kp);
+  for (int b0 = 0; b0 < ctx.nst; b0 += nbmax) {
+    const int nb = std::min(nbmax, ctx.nst - b0);
+    dim3 zgrid((g.nrods + kRodsPerCtaK - 1) / kRodsPerCtaK, nb);
+    k_zfft_bwd_k<<<zgrid, 256, zs, st>>>((const double2*)kp.d_c, ngw, b0, g, g.tw[2], zbuf,
+                                         kRodsPerCtaK);
+    QBX_LAUNCHED(ctx);
+    int chunks = std::max(1, (3 * sms + g.n2 - 1) / g.n2);
+    chunks = std::min(chunks, nb);
+    const int ppc = (nb + chunks - 1) / chunks;
+    chunks = (nb + ppc - 1) / ppc;
+    dim3 xgrid(g.n2, chunks);
+    if (op == OP_DENSITY) {
+      // the pair kernel's weights w[2 slot], w[2 slot + 1] are both the band's
+      k_xy<double, OP_DENSITY><<<xgrid, 512, xc.smem, st>>>(zbuf, nb, ppc, g, g.tw[0], g.tw[1],
+                                                           nullptr, rho, kp.d_w2, b0, 2 * ctx.nst,
+                                                           xc.cc, xc.rr);
+      QBX_LAUNCHED(ctx);
+    } else {
+      k_xy<double, OP_VPSI><<<xgrid, 512, xc.smem, st>>>(zbuf, nb, ppc, g, g.tw[0], g.tw[1], v,
+                                                        nullptr, nullptr, b0, 2 * ctx.nst, xc.cc,
+                                                        xc.rr);
+      QBX_LAUNCHED(ctx);
+      const double scale = 1.0 / ((double)g.n0 * g.n1 * g.n2);
+      k_zfft_fwd_k<<<zgrid, 256, zs, st>>>(zbuf, ngw, b0, g, g.tw[2], scale,
+                                           (const double2*)kp.d_c, kp.d_g2, (double2*)kp.d_hc,
+                                           kRodsPerCtaK);
+      QBX_LAUNCHED(ctx);
+    }
+  }
+}
+
+// rho += sum_n weight occ_n / Omega |psi_nk|^2 (SlaterDet::compute_density,
+// complex branch, src/SlaterDet.cpp:280-298)
+void launch_density_k(Context& ctx, KPointSet& kp, double* rho) {
+  ProfScope ps(ctx, "density_k");
+  staged_k(ctx, kp, OP_DENSITY, nullptr, rho);
+}
+
+// hc = 1/2 |k+G|^2 c + FFT_fwd(v FFT_bwd(c)) (SlaterDet::rs_mul_add, complex
+// branch, src/SlaterDet.cpp:458-475, with the kinetic term of
+// EnergyFunctional::energy, src/EnergyFunctional.cpp:789-839)
+void launch_vpsi_k(Context& ctx, KPointSet& kp, const double* v) {
+  ProfScope ps(ctx, "vpsi_k");
+  staged_k(ctx, kp, OP_VPSI, v, nullptr);
+}
+
 static int nblk(size_t n);
 
 __global__ void k_to_float(const double* __restrict__ x, size_t n, float* __restrict__ y) {

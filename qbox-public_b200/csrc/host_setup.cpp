@@ -153,6 +153,105 @@ void build_basis(Basis& b, const double cell[9], double ecut) {
   b.g0 = 0;
 }
 
+// The complex basis at k (units of the reciprocal vectors): the rods of
+// every (h,k) column with some |k+G|^2 < 2 ecut over the whole sphere
+// (src/Basis.cpp:449-486), here in sorted (h,k) order, l ascending; gx, g2,
+// g, gi, g2i hold k+G and its norms (Basis::update_g kpg*, :646-690).
+void build_kbasis(Basis& b, const double cell[9], double ecut, const double kp[3]) {
+  build_basis(b, cell, ecut);   // cell, reciprocal vectors, volume
+  b.complex_basis = true;
+  b.kpoint[0] = kp[0]; b.kpoint[1] = kp[1]; b.kpoint[2] = kp[2];
+  const double two_ecut = 2.0 * ecut;
+  const int hmax = hmax_of(cell, ecut, 0);
+  const int kmax = hmax_of(cell, ecut, 1);
+  const int lmax = hmax_of(cell, ecut, 2);
+  const double* B0 = b.recip;
+  const double* B1 = b.recip + 3;
+  const double* B2 = b.recip + 6;
+  auto q = [&](double h, double k, double l, double* out) {
+    for (int i = 0; i < 3; i++) out[i] = h * B0[i] + k * B1[i] + l * B2[i];
+  };
+  b.rod_h.clear(); b.rod_k.clear(); b.rod_lmin.clear(); b.rod_size.clear();
+  for (int h = -hmax; h <= hmax; h++)
+    for (int k = -kmax; k <= kmax; k++) {
+      int lstart = lmax + 1, lend = -lmax - 1;
+      for (int l = -lmax; l <= lmax; l++) {
+        double v[3];
+        q(kp[0] + h, kp[1] + k, kp[2] + l, v);
+        if (v[0] * v[0] + v[1] * v[1] + v[2] * v[2] < two_ecut) {
+          lstart = std::min(lstart, l);
+          lend = std::max(lend, l);
+        }
+      }
+      if (lend >= lstart) {
+        b.rod_h.push_back(h);
+        b.rod_k.push_back(k);
+        b.rod_lmin.push_back(lstart);
+        b.rod_size.push_back(lend - lstart + 1);
+      }
+    }
+  b.nrods = (int)b.rod_h.size();
+  QBX_REQUIRE(b.nrods > 0, 11, "empty basis at this k point");
+  b.rod_first.resize(b.nrods);
+  int ng = 0;
+  for (int r = 0; r < b.nrods; r++) { b.rod_first[r] = ng; ng += b.rod_size[r]; }
+  b.ng = ng;
+  b.hkl.resize(3 * ng);
+  b.gx.resize(3 * ng);
+  b.g2.resize(ng); b.g.resize(ng); b.gi.resize(ng); b.g2i.resize(ng);
+  b.first = -1;
+  for (int r = 0; r < b.nrods; r++)
+    for (int i = 0; i < b.rod_size[r]; i++) {
+      const int ig = b.rod_first[r] + i;
+      const int h = b.rod_h[r], k = b.rod_k[r], l = b.rod_lmin[r] + i;
+      b.hkl[3 * ig] = h; b.hkl[3 * ig + 1] = k; b.hkl[3 * ig + 2] = l;
+      double v[3];
+      q(kp[0] + h, kp[1] + k, kp[2] + l, v);
+      b.gx[ig] = v[0]; b.gx[ng + ig] = v[1]; b.gx[2 * ng + ig] = v[2];
+      b.g2[ig] = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+      b.g[ig] = std::sqrt(b.g2[ig]);
+      b.gi[ig] = b.g[ig] > 0.0 ? 1.0 / b.g[ig] : 0.0;
+      b.g2i[ig] = b.gi[ig] * b.gi[ig];
+      // the reference moves rod (0,0) to the front of its local basis
+      // (src/Basis.cpp:587-597): its lowest l is the first coefficient
+      if (h == 0 && k == 0 && i == 0) b.first = ig;
+    }
+  QBX_REQUIRE(b.first >= 0, 11, "the basis at this k point has no (0,0) rod");
+  b.g0 = -1;   // no G = 0 coefficient constraint on a complex basis
+}
+
+// Stick geometry of a complex basis on the grid: one stick per rod.
+void set_grid_complex(Basis& b, int n0, int n1, int n2) {
+  b.n0 = n0; b.n1 = n1; b.n2 = n2;
+  b.nvec = b.nrods;
+  b.stick_x.assign(b.nvec, 0);
+  b.stick_y.assign(b.nvec, 0);
+  auto md = [](int v, int n) { return ((v % n) + n) % n; };
+  for (int r = 0; r < b.nrods; r++) {
+    const int h = b.rod_h[r], k = b.rod_k[r];
+    QBX_REQUIRE(2 * std::abs(h) < n0 && 2 * std::abs(k) < n1, 12,
+                "basis does not fit in the FFT grid");
+    QBX_REQUIRE(2 * std::max(std::abs(b.rod_lmin[r]),
+                             std::abs(b.rod_lmin[r] + b.rod_size[r] - 1)) < n2,
+                12, "basis does not fit in the FFT grid");
+    b.stick_x[r] = md(h, n0);
+    b.stick_y[r] = md(k, n1);
+  }
+  std::map<int, int> cols;
+  for (int s = 0; s < b.nvec; s++) cols[b.stick_x[s]] = 0;
+  b.col_x.clear();
+  for (auto& kv : cols) { kv.second = (int)b.col_x.size(); b.col_x.push_back(kv.first); }
+  b.ncol = (int)b.col_x.size();
+  b.stick_col.resize(b.nvec);
+  for (int s = 0; s < b.nvec; s++) b.stick_col[s] = cols[b.stick_x[s]];
+  b.ip.resize(b.ng);
+  b.im.assign(b.ng, 0);
+  for (int ig = 0; ig < b.ng; ig++) {
+    const int h = b.hkl[3 * ig], k = b.hkl[3 * ig + 1], l = b.hkl[3 * ig + 2];
+    b.ip[ig] = md(h, n0) + n0 * (md(k, n1) + n1 * md(l, n2));
+  }
+}
+
 void set_grid(Basis& b, int n0, int n1, int n2) {
   b.n0 = n0; b.n1 = n1; b.n2 = n2;
   b.nvec = 2 * b.nrods - 1;

@@ -11,62 +11,11 @@
 #include <vector>
 
 #include "qbx_internal.h"
+#include "reduce.cuh"
 
 namespace qbx {
 
-static const int kRedBlocks = 592;   // 4 x 148 SMs
-static const int kThreads = 256;
-
-__device__ __forceinline__ double block_sum(double v, double* sh) {
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  __syncthreads();
-  if (lane == 0) sh[wid] = v;
-  __syncthreads();
-  double r = 0.0;
-  if (threadIdx.x == 0)
-    for (int i = 0; i < (int)(blockDim.x >> 5); i++) r += sh[i];
-  return r;   // valid in thread 0
-}
-
-// sum of up to 4 quantities produced by functor F(i, out[4]) over i < n
-template <int K, typename F>
-__global__ void __launch_bounds__(kThreads) k_reduce(F f, size_t n, double* partial) {
-  __shared__ double sh[32];
-  double acc[K];
-#pragma unroll
-  for (int k = 0; k < K; k++) acc[k] = 0.0;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x)
-    f(i, acc);
-#pragma unroll
-  for (int k = 0; k < K; k++) {
-    const double s = block_sum(acc[k], sh);
-    if (threadIdx.x == 0) partial[k * gridDim.x + blockIdx.x] = s;
-  }
-}
-
-template <int K>
-__global__ void k_reduce_final(const double* partial, int nb, double* out) {
-  __shared__ double sh[32];
-  for (int k = 0; k < K; k++) {
-    double a = 0.0;
-    for (int i = threadIdx.x; i < nb; i += blockDim.x) a += partial[k * nb + i];
-    const double s = block_sum(a, sh);
-    if (threadIdx.x == 0) out[k] = s;
-  }
-}
-
-// K sums of f over [0, n) into the scalar slots [slot, slot + K); no host
-// synchronisation (the host reads the slots after the step)
-template <int K, typename F>
-static void reduce(Context& ctx, F f, size_t n, int slot) {
-  const int nb = (int)std::max<size_t>(1, std::min<size_t>(kRedBlocks, (n + kThreads - 1) / kThreads));
-  k_reduce<K><<<nb, kThreads, 0, ctx.stream>>>(f, n, ctx.d_red);
-  QBX_LAUNCHED(ctx);
-  k_reduce_final<K><<<1, kThreads, 0, ctx.stream>>>(ctx.d_red, nb, ctx.d_scalars + slot);
-  QBX_LAUNCHED(ctx);
-}
+using namespace red;
 
 static int blocks_for(size_t n) {
   return (int)std::max<size_t>(1, std::min<size_t>((n + kThreads - 1) / kThreads, 148 * 32));
@@ -710,41 +659,71 @@ __global__ void k_anl(const double* __restrict__ gx, int ngw, const double* __re
   }
 }
 
-void launch_setup_atoms(Context& ctx) {
-  const Basis& vb = ctx.vb;
-  const Basis& wb = ctx.wb;
-  const int ngv = vb.ng, ngw = wb.ng;
-  const int nsp = (int)ctx.species.size();
-  // projector forms twnl = Y_lm(G) V_nl(|G|) (spline of the radial form) do
-  // not depend on the positions: built once per set of atoms, one row of
-  // ngw per (species, projector, m)
-  if (!ctx.d_twnl) {
-    const double s14pi = std::sqrt(1.0 / (4.0 * M_PI));
-    const double s34pi = std::sqrt(3.0 / (4.0 * M_PI));
-    std::vector<double> tw;
-    for (int is = 0; is < nsp; is++) {
-      const SpeciesTables& sp = ctx.species[is];
-      for (size_t iop = 0; iop < sp.proj_l.size(); iop++) {
-        const int l = sp.proj_l[iop];
-        std::vector<double> v(ngw);
-        for (int ig = 0; ig < ngw; ig++) {
-          double val, dv;
-          sp.dvnlg((int)iop, wb.g[ig], val, dv);
-          v[ig] = val;
-        }
-        for (int m = 0; m < 2 * l + 1; m++)
-          for (int ig = 0; ig < ngw; ig++)
-            tw.push_back(l == 0 ? s14pi * v[ig]
-                                : s34pi * wb.gx[(size_t)m * ngw + ig] * wb.gi[ig] * v[ig]);
+// Projector forms twnl = Y_lm(q) V_nl(|q|) (spline of the radial form) on
+// the vectors q of basis b (G, or k+G for a complex basis), one row of ngw
+// per (species, projector, m) (NonLocalPotential::update_twnl,
+// src/NonLocalPotential.cpp:235-560, with the basis's kpg, kpgi, kpgx).
+std::vector<double> twnl_rows(const Context& ctx, const Basis& b) {
+  const double s14pi = std::sqrt(1.0 / (4.0 * M_PI));
+  const double s34pi = std::sqrt(3.0 / (4.0 * M_PI));
+  const int ngw = b.ng;
+  std::vector<double> tw;
+  for (const SpeciesTables& sp : ctx.species) {
+    for (size_t iop = 0; iop < sp.proj_l.size(); iop++) {
+      const int l = sp.proj_l[iop];
+      std::vector<double> v(ngw);
+      for (int ig = 0; ig < ngw; ig++) {
+        double val, dv;
+        sp.dvnlg((int)iop, b.g[ig], val, dv);
+        v[ig] = val;
+      }
+      for (int m = 0; m < 2 * l + 1; m++)
+        for (int ig = 0; ig < ngw; ig++)
+          tw.push_back(l == 0 ? s14pi * v[ig]
+                              : s34pi * b.gx[(size_t)m * ngw + ig] * b.gi[ig] * v[ig]);
+    }
+  }
+  return tw;
+}
+
+// The projector columns anl = twnl (-i)^l exp(-i q.tau) of every atom on the
+// ngw vectors q (device, x, y and z blocks), column order (species,
+// projector, m, atom) as ctx.nproj counts them.
+void build_anl(Context& ctx, const double* d_q, int ngw, const double* d_twnl, double* d_anl) {
+  int col = 0, row = 0, atom0 = 0;
+  for (size_t is = 0; is < ctx.species.size(); is++) {
+    const SpeciesTables& sp = ctx.species[is];
+    const int na = (int)ctx.tau[is].size() / 3;
+    const double* d_tau = ctx.d_tau_all + 3 * (size_t)atom0;
+    for (size_t iop = 0; iop < sp.proj_l.size(); iop++) {
+      const int l = sp.proj_l[iop];
+      for (int m = 0; m < 2 * l + 1; m++, row++) {
+        dim3 grid((ngw + kThreads - 1) / kThreads, na);
+        k_anl<<<grid, kThreads, 0, ctx.stream>>>(d_q, ngw, d_twnl + (size_t)row * ngw, d_tau,
+                                                  na, l, (double2*)d_anl + (size_t)col * ngw);
+        QBX_LAUNCHED(ctx);
+        col += na;
       }
     }
+    atom0 += na;
+  }
+  QBX_REQUIRE(col == ctx.nproj, 30, "projector count mismatch");
+}
+
+void launch_setup_atoms(Context& ctx) {
+  const Basis& vb = ctx.vb;
+  const int ngv = vb.ng, ngw = ctx.wb.ng;
+  const int nsp = (int)ctx.species.size();
+  // the projector forms do not depend on the positions: built once per set
+  // of atoms
+  if (!ctx.d_twnl) {
+    const std::vector<double> tw = twnl_rows(ctx, ctx.wb);
     ctx.d_twnl = tw.empty() ? nullptr : dupload(tw);
   }
   QBX_CUDA(cudaMemsetAsync(ctx.d_vion, 0, 2 * sizeof(double) * ngv, ctx.stream));
   QBX_CUDA(cudaMemsetAsync(ctx.d_rhops, 0, 2 * sizeof(double) * ngv, ctx.stream));
-  int col = 0, row = 0, atom0 = 0;
+  int atom0 = 0;
   for (int is = 0; is < nsp; is++) {
-    const SpeciesTables& sp = ctx.species[is];
     const int na = (int)ctx.tau[is].size() / 3;
     // positions of this species: a slice of the species-major d_tau_all
     const double* d_tau = ctx.d_tau_all + 3 * (size_t)atom0;
@@ -756,21 +735,10 @@ void launch_setup_atoms(Context& ctx) {
                                                          (double2*)ctx.d_vion,
                                                          (double2*)ctx.d_rhops);
     QBX_LAUNCHED(ctx);
-    // projector columns of this species: twnl times the phases
-    for (size_t iop = 0; iop < sp.proj_l.size(); iop++) {
-      const int l = sp.proj_l[iop];
-      for (int m = 0; m < 2 * l + 1; m++, row++) {
-        dim3 grid((ngw + kThreads - 1) / kThreads, na);
-        k_anl<<<grid, kThreads, 0, ctx.stream>>>(ctx.d_gx_w, ngw, ctx.d_twnl + (size_t)row * ngw,
-                                                  d_tau, na, l,
-                                                  (double2*)ctx.d_anl + (size_t)col * ngw);
-        QBX_LAUNCHED(ctx);
-        col += na;
-      }
-    }
     atom0 += na;
   }
-  QBX_REQUIRE(col == ctx.nproj, 30, "projector count mismatch");
+  // projector columns: twnl times the phases
+  if (ctx.nproj) build_anl(ctx, ctx.d_gx_w, ngw, ctx.d_twnl, ctx.d_anl);
 }
 
 // ------------------------------------------------------------ stress

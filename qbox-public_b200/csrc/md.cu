@@ -77,6 +77,7 @@ void move_atoms(Context& c, const double* tau) {
   QBX_CUDA(cudaStreamSynchronize(c.stream));
   launch_setup_atoms(c);
   split_projectors(c);
+  for (KPointSet& kp : c.kpts) kp.anl_ready = false;   // phases at k+G rebuilt on use
   std::vector<double> zv(c.species.size());
   for (size_t is = 0; is < c.species.size(); is++) zv[is] = c.species[is].zval;
   c.esr = esr_energy_forces(c.wb.cell, c.tau, zv, 1.5, c.fion_esr, c.sigma_esr);

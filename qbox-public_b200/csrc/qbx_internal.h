@@ -103,10 +103,17 @@ struct Basis {
   std::vector<int> stick_col;             // compact column of each stick
   std::vector<int> col_x;                 // grid x of each compact column
   std::vector<int> ip, im;                // grid index of +G and -G
+  // complex basis at a k point off Gamma (build_kbasis): gx, g2, g, gi, g2i
+  // hold k+G; one stick per rod; im unused
+  bool complex_basis = false;
+  double kpoint[3] = {0, 0, 0};
+  int first = 0;                          // the reference's first local coefficient
 };
 
 void build_basis(Basis& b, const double cell[9], double ecut);
 void set_grid(Basis& b, int n0, int n1, int n2);
+void build_kbasis(Basis& b, const double cell[9], double ecut, const double kpoint[3]);
+void set_grid_complex(Basis& b, int n0, int n1, int n2);
 bool factorizable(int n);
 int fft_size(const double cell[9], double ecut, int dir);
 void dense_grid(const double cell[9], double ecut_wf, int np[3]);
@@ -255,6 +262,29 @@ struct BatchGraph {
   cudaGraphExec_t exec = nullptr;
   std::vector<long> ids;         // StepGraph ids of the members, in order
   bool failed = false;           // instantiation refused: launch per context
+};
+
+// One k point off Gamma (Wavefunction::add_kpoint): its complex basis and
+// stick geometry, the coefficients and H*psi (ngw x nst complex, column-major
+// like ComplexMatrix), the PSDA history and the projector columns at k+G.
+struct KPointSet {
+  double k[3] = {0, 0, 0};   // units of the reciprocal vectors
+  double weight = 0;
+  Basis kb;
+  DeviceSticks dks{};
+  double* d_c = nullptr;       // 2*ngw*nst
+  double* d_hc = nullptr;
+  double* d_c_last = nullptr;
+  double* d_dc_last = nullptr;
+  double* d_ctmp = nullptr;
+  double* d_g2 = nullptr;      // |k+G|^2
+  double* d_q = nullptr;       // k+G, x, y and z blocks
+  double* d_twnl = nullptr;    // projector forms at k+G
+  double* d_anl = nullptr;     // 2*ngw*nproj
+  double* d_w2 = nullptr;      // weight*occ/Omega twice per band (plane kernel weights)
+  double* d_prec = nullptr;    // nst per-band kinetic energies
+  bool anl_ready = false;
+  double theta = 0;
 };
 
 struct Context {
@@ -432,6 +462,15 @@ struct Context {
   long batch_launches = 0;       // batch graphs launched with this context leading
   int polar_iters = 0;           // iterations of the last eager polar
   double* d_wfv = nullptr;       // wavefunction velocity of the MD extrapolation
+  // k points off Gamma; when set, the electronic step runs on them instead
+  // of the Gamma coefficients
+  std::vector<KPointSet> kpts;
+  bool kpts_extrapolate = false;
+  double* d_fnlk = nullptr;      // 2*nproj*nst complex projections of one k point
+  double* d_znn = nullptr;       // 6 complex nst x nst matrices
+  double* d_zwork = nullptr;     // cuSOLVER workspace of the complex factorisations
+  int zwork_len = 0;             // its length in complex elements
+  int* d_zipiv = nullptr;        // nst pivots + 1 info word
 
   size_t N() const { return (size_t)vb.n0 * vb.n1 * vb.n2; }
 };
@@ -577,6 +616,19 @@ void wfgrid_backward(Context& ctx, const DeviceSticks& d, int ng, const double* 
 void wfgrid_forward(Context& ctx, const DeviceSticks& d, int ng, const double* f, double* c);
 // molecular dynamics (md.cu)
 void move_atoms(Context& c, const double* tau);
+// k points off Gamma (kpoint.cu)
+void set_kpoints(Context& ctx, int nk, const double* k, const double* w);
+void free_kpoints(Context& ctx);
+void kpoints_atoms_changed(Context& ctx);
+void gram_k(Context& ctx);
+void update_density_k(Context& ctx);
+void energy_k(Context& ctx, bool hpsi);
+void eigsum_k(Context& ctx);
+void psda_update_k(Context& ctx);
+std::vector<double> twnl_rows(const Context& ctx, const Basis& b);
+void build_anl(Context& ctx, const double* d_q, int ngw, const double* d_twnl, double* d_anl);
+void launch_density_k(Context& ctx, KPointSet& kp, double* rho);
+void launch_vpsi_k(Context& ctx, KPointSet& kp, const double* v);
 void md_run(Context& c, int niter, int nitscf, double dt, const double* mass_amu, double* vel,
             double* tau_out, double* ionic, double* scf);
 

@@ -25,6 +25,8 @@ ENERGY_NAMES = ("ekin", "eps", "enl", "ehart", "ecoul", "exc", "esr", "eself",
 
 # every entry point of include/qbx.h
 SYMBOLS = (
+    "qbx_set_kpoints", "qbx_kpoint_basis", "qbx_set_kpoint_coeffs",
+    "qbx_get_kpoint_coeffs", "qbx_get_kpoint_hpsi", "qbx_host_kbasis",
     "qbx_version", "qbx_create", "qbx_destroy", "qbx_last_error",
     "qbx_set_precision", "qbx_set_cell", "qbx_basis_sizes", "qbx_basis_miller",
     "qbx_set_coeff_order", "qbx_add_species", "qbx_set_atoms",
@@ -96,6 +98,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "qbx_host_species_eval": (_I, [_I, _D, _I, _DP, _I, _IP, _DP, _I, _DP,
                                        _DP, _DP, _DP]),
         "qbx_host_esr": (_I, [_DP, _I, _IP, _DP, _DP, _DP, _DP]),
+        "qbx_host_kbasis": (_I, [_DP, _D, _DP, _IP, _IP, _IP]),
         "qbx_profile": (_I, [_P, _I]),
         "qbx_profile_get": (_I, [_P, ctypes.c_char_p, _DP, ctypes.POINTER(ctypes.c_long)]),
         "qbx_launch_count": (_I, [_P, ctypes.POINTER(ctypes.c_long)]),
@@ -116,6 +119,11 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "qbx_scf_run": (_I, [_P, _I, _I, _D, _D, _I, _D, _DP, _DP, _IP, _IP]),
         "qbx_md_run": (_I, [_P, _I, _I, _D, _DP, _DP, _DP, _DP, _DP]),
         "qbx_polar": (_I, [_P, _DP, _D, _I, _I, ctypes.POINTER(_I)]),
+        "qbx_set_kpoints": (_I, [_P, _I, _DP, _DP]),
+        "qbx_kpoint_basis": (_I, [_P, _I, _IP, _IP]),
+        "qbx_set_kpoint_coeffs": (_I, [_P, _I, _DP]),
+        "qbx_get_kpoint_coeffs": (_I, [_P, _I, _DP]),
+        "qbx_get_kpoint_hpsi": (_I, [_P, _I, _DP]),
         "qbx_step_graph_info": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_long),
                                      ctypes.POINTER(ctypes.c_long), ctypes.c_char_p, _I]),
     }
@@ -229,6 +237,42 @@ class Context:
     def get_hpsi(self) -> np.ndarray:
         out = np.empty((self.nst, self.ngw), np.complex128)
         self._ok(self.lib.qbx_get_hpsi(self.h, _dp(out.view(np.float64))), "get_hpsi")
+        return out
+
+    # ---- k points off Gamma (complex bases)
+    def set_kpoints(self, kpoints, weights):
+        """Wavefunction::add_kpoint for each k point (units of the
+        reciprocal vectors), the Gamma point removed; [] returns to Gamma."""
+        k = np.ascontiguousarray(np.asarray(kpoints, float).reshape(-1))
+        w = np.ascontiguousarray(np.asarray(weights, float).reshape(-1))
+        nk = w.size
+        self._ok(self.lib.qbx_set_kpoints(self.h, nk, _dp(k) if nk else None,
+                                          _dp(w) if nk else None), "set_kpoints")
+        self.kngw = []
+        for ik in range(nk):
+            n = _I()
+            self._ok(self.lib.qbx_kpoint_basis(self.h, ik, ctypes.byref(n), None), "kpoint_basis")
+            self.kngw.append(n.value)
+
+    def kpoint_miller(self, ik: int) -> np.ndarray:
+        out = np.empty((self.kngw[ik], 3), np.int32)
+        self._ok(self.lib.qbx_kpoint_basis(self.h, ik, None, _ip(out)), "kpoint_basis")
+        return out
+
+    def set_kpoint_coeffs(self, ik: int, c: np.ndarray):
+        a = np.ascontiguousarray(c, np.complex128).view(np.float64)
+        self._ok(self.lib.qbx_set_kpoint_coeffs(self.h, ik, _dp(a)), "set_kpoint_coeffs")
+
+    def get_kpoint_coeffs(self, ik: int) -> np.ndarray:
+        out = np.empty((self.nst, self.kngw[ik]), np.complex128)
+        self._ok(self.lib.qbx_get_kpoint_coeffs(self.h, ik, _dp(out.view(np.float64))),
+                 "get_kpoint_coeffs")
+        return out
+
+    def get_kpoint_hpsi(self, ik: int) -> np.ndarray:
+        out = np.empty((self.nst, self.kngw[ik]), np.complex128)
+        self._ok(self.lib.qbx_get_kpoint_hpsi(self.h, ik, _dp(out.view(np.float64))),
+                 "get_kpoint_hpsi")
         return out
 
     # ---- operations
@@ -492,6 +536,15 @@ def from_system(system, device: int = 0, precision: int = FP64,
     if coeffs is None:
         coeffs = system.coefficients(hkl)
     ctx.set_coeffs(coeffs)
+    if system.kpoints:
+        # the k points replace Gamma; their coefficients are keyed by the
+        # sorted Miller list of each complex basis, the library's own order
+        ctx.set_kpoints([k for k, _ in system.kpoints], [w for _, w in system.kpoints])
+        for ik in range(len(system.kpoints)):
+            hk = system.kmiller(ik)
+            if not np.array_equal(ctx.kpoint_miller(ik), hk):
+                raise QbxError(f"k point {ik}: basis differs from the generator's")
+            ctx.set_kpoint_coeffs(ik, system.kcoefficients(ik, hk))
     if gram:
         ctx.gram()
     return ctx
@@ -512,6 +565,21 @@ def host_basis(cell, ecut: float):
     if rc:
         raise QbxError(f"qbx_host_basis failed: {rc}")
     return ngw.value, ngv.value, (npg[0], npg[1], npg[2]), hkl
+
+
+def host_kbasis(cell, ecut: float, kpoint):
+    """The complex basis at a k point from the library's host code: (Miller
+    indices in coefficient order, index of the reference's first coefficient)."""
+    lib = load()
+    cell = np.ascontiguousarray(np.asarray(cell, float).reshape(9))
+    k = np.ascontiguousarray(np.asarray(kpoint, float).reshape(3))
+    n, first = _I(), _I()
+    rc = lib.qbx_host_kbasis(_dp(cell), ecut, _dp(k), ctypes.byref(n), ctypes.byref(first), None)
+    if rc:
+        raise QbxError(f"qbx_host_kbasis: code {rc}")
+    hkl = np.empty((n.value, 3), np.int32)
+    lib.qbx_host_kbasis(_dp(cell), ecut, _dp(k), None, None, _ip(hkl))
+    return hkl, first.value
 
 
 def host_species_eval(sp, g: np.ndarray):

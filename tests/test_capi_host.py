@@ -84,3 +84,21 @@ def test_host_esr_matches_reference(name):
     np.testing.assert_allclose(f, np.concatenate(f_ref), atol=1e-12)
     g = np.load(os.path.join(ROOT, "tests", "golden", f"ref_{name}.npz"))
     assert abs(e - g["e_esr"][0]) < 1e-10
+
+
+@pytest.mark.parametrize("name", ["si8k2", "h2o4k2"])
+def test_host_kbasis_matches_oracle_and_reference(name):
+    """The complex basis at each k point (host code of the library) equals
+    the oracle's Miller set, has the reference's size (golden fixture) and
+    the reference's first local coefficient (rod (0,0), lowest l)."""
+    from conftest import golden
+    from oracle import qbox_np
+    s = systems.get(name)
+    g = golden(name)
+    base = qbox_np.ElectronicStep(s)
+    for ik, (k, w) in enumerate(s.kpoints):
+        hkl, first = capi.host_kbasis(s.cell, s.ecut, k)
+        np.testing.assert_array_equal(hkl, s.kmiller(ik))
+        assert hkl.shape[0] == int(g[f"k{ik}_ngw"])
+        kp = qbox_np.KPoint(base, k, w, s.kmiller(ik), np.zeros((1, hkl.shape[0])))
+        assert first == kp.first
