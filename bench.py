@@ -363,6 +363,30 @@ def run_ours(args):
             c.close()
         replicas.barrier(device=f"cuda:{dev}")
 
+    # ---- k points off Gamma: si64 at two k points (complex bases, FP64),
+    # ms per electronic step, beside the reference's own time for one step
+    kpts = None
+    if args.kpoint_steps > 0:
+        sk = systems.si64k2()
+        kc = capi.from_system(sk, device=dev, precision=capi.FP64)
+        for _ in range(2):
+            kc.scf_step()
+        stream = torch.cuda.ExternalStream(kc.stream(), device=dev)
+        k0 = torch.cuda.Event(enable_timing=True)
+        k1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        k0.record(stream)
+        for _ in range(args.kpoint_steps):
+            ek = kc.scf_step()
+        k1.record(stream)
+        k1.synchronize()
+        kpts = {"system": "si64 (PBE, 30 Ry, 128 bands) at k = (1/4,1/4,1/4), (-1/4,1/4,1/4), "
+                          "weights 1/2",
+                "ngw_per_kpoint": list(kc.kngw), "precision": "fp64",
+                "ms_per_step": max_over_ranks(k0.elapsed_time(k1) / args.kpoint_steps),
+                "etotal_last": ek["etotal"], "reference_ms_per_step": None}
+        kc.close()
+
     ms_mix = max_over_ranks(ms_mix)
     ms_f64 = max_over_ranks(ms_f64)
     ms_e2e = max_over_ranks(ms_e2e)
@@ -379,6 +403,16 @@ def run_ours(args):
                 cms, sample = reference_step_ms(2, 32, threads)
                 cpu = {"value": cms, "unit": "ms", "cores": threads, "kind": "reference",
                        "sample": sample}
+        if kpts is not None and cpu is not None:
+            # the reference's own k-point step on the host cores (one step,
+            # the sum of its timed phases)
+            from oracle import inputs
+            with tempfile.TemporaryDirectory() as td:
+                out = inputs.run_reference(systems.si64k2(), td, 1, threads=cpu["cores"])
+            e = out["energies"]
+            kpts["reference_ms_per_step"] = 1e3 * float(
+                e["t_charge"][0] + e["t_vhxc"][0] + e["t_energy"][0] + e["t_wf_update"][0])
+            kpts["reference_cores"] = cpu["cores"]
         line = {
             "metric": METRIC, "value": ms_mix, "unit": "ms", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mix,
@@ -392,6 +426,7 @@ def run_ours(args):
                            "eager_ms_per_step": ms_mix_eager},
             "md": md,
             "batch": batch,
+            "kpoints": kpts,
             "mixed_vs_fp64_speedup": ms_f64 / ms_mix,
             "dE_per_atom": de_atom,
             "dE_definition": ("|E_mixed - E_fp64| / atoms for one electronic step of both paths "
@@ -452,6 +487,8 @@ def main():
                     help="electronic steps per ionic step in the MD measurement")
     ap.add_argument("--batch-steps", type=int, default=3,
                     help="timed steps of the 32-system batch measurement (0: skip)")
+    ap.add_argument("--kpoint-steps", type=int, default=3,
+                    help="timed steps of the two-k-point si64 measurement (0: skip)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--profile-bands", type=int, default=0,
                     help="run only warm-up + one mixed step of si512 with this many bands "

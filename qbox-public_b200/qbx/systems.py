@@ -310,8 +310,14 @@ def h2o4k2() -> System:
         [((0.0, 0.5, 0.0), 0.5), ((0.25, 0.0, 0.5), 0.5)], "h2o4k2")
 
 
+def si64k2() -> System:
+    """si64 (PBE, 30 Ry, 128 bands) at two k points off Gamma."""
+    return si64().with_kpoints([((0.25, 0.25, 0.25), 0.5), ((-0.25, 0.25, 0.25), 0.5)],
+                               "si64k2")
+
+
 REGISTRY = {"si8": si8, "si64": si64, "si512": si512, "h2o32": h2o32,
-            "si8k2": si8k2, "h2o4k2": h2o4k2}
+            "si8k2": si8k2, "h2o4k2": h2o4k2, "si64k2": si64k2}
 
 
 def get(name: str) -> System:
