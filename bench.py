@@ -196,12 +196,18 @@ def run_ours(args):
         n0 = ctx.launch_count()
         start.record(stream)
         r = None
-        for _ in range(nsteps):
-            if e2e_bufs is not None:
-                ctx.set_coeffs_async(e2e_bufs[0])
-            r = ctx.scf_step()
-            if e2e_bufs is not None:
-                ctx.get_coeffs_async(e2e_bufs[1])
+        if e2e_bufs is not None:
+            # the streamed SlaterDet: each step uploads its input from pinned
+            # host memory and downloads its result, the copies on their own
+            # streams overlapping the neighbouring steps' compute
+            for _ in range(nsteps):
+                ctx.stream_in(e2e_bufs[0])
+                ctx.scf_step_async()
+                ctx.stream_out(e2e_bufs[1])
+            r = ctx.stream_wait()
+        else:
+            for _ in range(nsteps):
+                r = ctx.scf_step()
         end.record(stream)
         end.synchronize()
         torch.cuda.synchronize()

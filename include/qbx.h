@@ -119,6 +119,21 @@ int qbx_set_wf_dyn(qbx_context* ctx, const char* wf_dyn);
  * terms the context then holds, as the reference's energy functional does. */
 int qbx_jd_update(qbx_context* ctx);
 
+/* Streamed SlaterDet (no counterpart in the reference, whose coefficients
+ * stay in host memory): the coefficients live in pinned host memory and
+ * pass through the GPU every step.  qbx_stream_in enqueues the upload of a
+ * step's input on a copy stream; qbx_scf_step_async enqueues the step (its
+ * captured graph, once qbx_set_step_graph has captured it; otherwise the
+ * synchronous step) after that upload; qbx_stream_out enqueues the download
+ * of the step's result on a second copy stream.  None of them waits for the
+ * GPU, so one step's copies overlap its neighbours' compute; the host
+ * buffers must stay untouched until qbx_stream_wait, which waits for all of
+ * it and returns the last step's energies (and its status as an error). */
+int qbx_stream_in(qbx_context* ctx, const double* c_pinned);
+int qbx_scf_step_async(qbx_context* ctx);
+int qbx_stream_out(qbx_context* ctx, double* c_pinned);
+int qbx_stream_wait(qbx_context* ctx, double* energies);
+
 /* k points off Gamma: Wavefunction::add_kpoint for each of nkp k points
  * (kpoints: 3 per k point, units of the reciprocal vectors; weights sum to
  * one) with the Gamma point removed (del_kpoint), src/Wavefunction.cpp:

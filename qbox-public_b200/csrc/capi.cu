@@ -66,6 +66,11 @@ void drop_graphs(Context& c) {
 void free_cell(Context& c) {
   drop_graphs(c);
   free_kpoints(c);
+  if (c.s_in) cudaStreamSynchronize(c.s_in);
+  if (c.s_out) cudaStreamSynchronize(c.s_out);
+  dfree(c.d_cin);
+  dfree(c.d_cout);
+  c.in_pending = c.finish_pending = false;
   free_mixed(c);
   free_mix(c);
   if (c.have_wgrid) free_sticks(c.dwg);
@@ -374,6 +379,10 @@ void qbx_destroy(qbx_context* h) {
   if (h->c.solver) cusolverDnDestroy(h->c.solver);
   for (auto s : h->c.side)
     if (s) cudaStreamDestroy(s);
+  for (cudaStream_t s : {h->c.s_in, h->c.s_out})
+    if (s) cudaStreamDestroy(s);
+  for (cudaEvent_t e : {h->c.ev_in, h->c.ev_cin_free, h->c.ev_step, h->c.ev_out})
+    if (e) cudaEventDestroy(e);
   if (h->c.stream) cudaStreamDestroy(h->c.stream);
   delete h;
 }
@@ -687,6 +696,108 @@ int qbx_get_coeffs_async(qbx_context* h, double* c) {
 }
 int qbx_get_hpsi(qbx_context* h, double* hc) {
   return h ? get_coeffs_impl(h, h->c.d_hc, hc, true) : 1;
+}
+
+// ---- streamed SlaterDet: copies on their own streams, ordered by events
+static void ensure_streaming(Context& c) {
+  if (!c.s_in) {
+    QBX_CUDA(cudaStreamCreateWithFlags(&c.s_in, cudaStreamNonBlocking));
+    QBX_CUDA(cudaStreamCreateWithFlags(&c.s_out, cudaStreamNonBlocking));
+    for (cudaEvent_t* e : {&c.ev_in, &c.ev_cin_free, &c.ev_step, &c.ev_out})
+      QBX_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  }
+  if (!c.d_cin) {
+    const size_t wf = 2 * (size_t)c.wb.ng * c.nst;
+    c.d_cin = dalloc<double>(wf);
+    c.d_cout = dalloc<double>(wf);
+  }
+}
+
+int qbx_stream_in(qbx_context* h, const double* src) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, false);
+    QBX_REQUIRE(src && c.kpts.empty(), 1, "streamed coefficients need a host buffer at Gamma");
+    ensure_streaming(c);
+    // the previous step has taken its input out of the staging buffer
+    QBX_CUDA(cudaStreamWaitEvent(c.s_in, c.ev_cin_free, 0));
+    QBX_CUDA(cudaMemcpyAsync(c.d_cin, src, 2 * (size_t)c.wb.ng * c.nst * sizeof(double),
+                             cudaMemcpyHostToDevice, c.s_in));
+    QBX_CUDA(cudaEventRecord(c.ev_in, c.s_in));
+    c.in_pending = true;
+  });
+}
+
+int qbx_scf_step_async(qbx_context* h) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, true);
+    QBX_REQUIRE(c.kpts.empty(), 1, "the streamed step is not available at k points off Gamma");
+    ensure_streaming(c);
+    const size_t wf = 2 * (size_t)c.wb.ng * c.nst;
+    if (c.in_pending) {
+      QBX_CUDA(cudaStreamWaitEvent(c.stream, c.ev_in, 0));
+      if (h->d_perm) {
+        k_permute<<<1184, 256, 0, c.stream>>>((const double2*)c.d_cin, h->d_perm, c.wb.ng, c.nst,
+                                              1, (double2*)c.d_c);
+        QBX_LAUNCHED(c);
+      } else {
+        QBX_CUDA(cudaMemcpyAsync(c.d_c, c.d_cin, wf * sizeof(double), cudaMemcpyDeviceToDevice,
+                                 c.stream));
+      }
+      QBX_CUDA(cudaEventRecord(c.ev_cin_free, c.stream));
+      c.in_pending = false;
+    }
+    StepGraph& g = c.graphs[c.extrapolate ? 1 : 0];
+    if (c.step_graph && c.wf_dyn == 0 && !c.prof.on && g.exec) {
+      // captured: launch and return; the host finish (energies, status) of
+      // this step waits for qbx_stream_wait or the next uncaptured step
+      launch_step_graph(c, g);
+      c.extrapolate = true;         // as finish_graph_step leaves it
+      c.finish_pending = true;
+    } else {
+      // not captured (yet): the synchronous step, which may capture
+      QBX_CUDA(cudaStreamSynchronize(c.stream));
+      if (c.finish_pending) finish_graph_step(c, false, c.last_energies, nullptr);
+      c.finish_pending = false;
+      scf_step_any(c, false, false, c.last_energies, nullptr);
+    }
+    // the result to its staging buffer once the previous download is done
+    QBX_CUDA(cudaStreamWaitEvent(c.stream, c.ev_out, 0));
+    if (h->d_perm) {
+      k_permute<<<1184, 256, 0, c.stream>>>((const double2*)c.d_c, h->d_perm, c.wb.ng, c.nst, 0,
+                                            (double2*)c.d_cout);
+      QBX_LAUNCHED(c);
+    } else {
+      QBX_CUDA(cudaMemcpyAsync(c.d_cout, c.d_c, wf * sizeof(double), cudaMemcpyDeviceToDevice,
+                               c.stream));
+    }
+    QBX_CUDA(cudaEventRecord(c.ev_step, c.stream));
+  });
+}
+
+int qbx_stream_out(qbx_context* h, double* dst) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, false);
+    QBX_REQUIRE(dst && c.s_out, 1, "qbx_stream_out before a streamed step");
+    QBX_CUDA(cudaStreamWaitEvent(c.s_out, c.ev_step, 0));
+    QBX_CUDA(cudaMemcpyAsync(dst, c.d_cout, 2 * (size_t)c.wb.ng * c.nst * sizeof(double),
+                             cudaMemcpyDeviceToHost, c.s_out));
+    QBX_CUDA(cudaEventRecord(c.ev_out, c.s_out));
+  });
+}
+
+int qbx_stream_wait(qbx_context* h, double* energies) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, false);
+    QBX_CUDA(cudaStreamSynchronize(c.stream));
+    if (c.s_in) QBX_CUDA(cudaStreamSynchronize(c.s_in));
+    if (c.s_out) QBX_CUDA(cudaStreamSynchronize(c.s_out));
+    if (c.finish_pending) {
+      finish_graph_step(c, false, c.last_energies, nullptr);
+      c.finish_pending = false;
+    }
+    QBX_REQUIRE(std::isfinite(c.last_energies[8]), 41, "streamed step: total energy not finite");
+    if (energies) std::memcpy(energies, c.last_energies, sizeof(double) * QBX_NENERGY);
+  });
 }
 
 int qbx_set_kpoints(qbx_context* h, int nkp, const double* kpoints, const double* weights) {

@@ -462,6 +462,16 @@ struct Context {
   long batch_launches = 0;       // batch graphs launched with this context leading
   int polar_iters = 0;           // iterations of the last eager polar
   double* d_wfv = nullptr;       // wavefunction velocity of the MD extrapolation
+  // streamed SlaterDet (qbx_stream_in / qbx_scf_step_async / qbx_stream_out):
+  // two copy streams, the staging buffers of one step's input and result,
+  // and the events that order them against the compute stream
+  cudaStream_t s_in = nullptr, s_out = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_cin_free = nullptr, ev_step = nullptr, ev_out = nullptr;
+  double* d_cin = nullptr;
+  double* d_cout = nullptr;
+  bool in_pending = false;       // an upload not yet consumed by a step
+  bool finish_pending = false;   // a captured step whose host finish is deferred
+  double last_energies[16] = {0};
   // k points off Gamma; when set, the electronic step runs on them instead
   // of the Gamma coefficients
   std::vector<KPointSet> kpts;

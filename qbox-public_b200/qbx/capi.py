@@ -25,6 +25,7 @@ ENERGY_NAMES = ("ekin", "eps", "enl", "ehart", "ecoul", "exc", "esr", "eself",
 
 # every entry point of include/qbx.h
 SYMBOLS = (
+    "qbx_stream_in", "qbx_scf_step_async", "qbx_stream_out", "qbx_stream_wait",
     "qbx_set_kpoints", "qbx_kpoint_basis", "qbx_set_kpoint_coeffs",
     "qbx_get_kpoint_coeffs", "qbx_get_kpoint_hpsi", "qbx_host_kbasis",
     "qbx_version", "qbx_create", "qbx_destroy", "qbx_last_error",
@@ -119,6 +120,10 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "qbx_scf_run": (_I, [_P, _I, _I, _D, _D, _I, _D, _DP, _DP, _IP, _IP]),
         "qbx_md_run": (_I, [_P, _I, _I, _D, _DP, _DP, _DP, _DP, _DP]),
         "qbx_polar": (_I, [_P, _DP, _D, _I, _I, ctypes.POINTER(_I)]),
+        "qbx_stream_in": (_I, [_P, _DP]),
+        "qbx_scf_step_async": (_I, [_P]),
+        "qbx_stream_out": (_I, [_P, _DP]),
+        "qbx_stream_wait": (_I, [_P, _DP]),
         "qbx_set_kpoints": (_I, [_P, _I, _DP, _DP]),
         "qbx_kpoint_basis": (_I, [_P, _I, _IP, _IP]),
         "qbx_set_kpoint_coeffs": (_I, [_P, _I, _DP]),
@@ -238,6 +243,23 @@ class Context:
         out = np.empty((self.nst, self.ngw), np.complex128)
         self._ok(self.lib.qbx_get_hpsi(self.h, _dp(out.view(np.float64))), "get_hpsi")
         return out
+
+    # ---- streamed SlaterDet: pinned host buffers, copies overlapping compute
+    def stream_in(self, c_pinned: np.ndarray):
+        """Enqueue the upload of a step's input (complex coefficients as a
+        pinned float64 buffer); returns at once."""
+        self._ok(self.lib.qbx_stream_in(self.h, _dp(c_pinned)), "stream_in")
+
+    def scf_step_async(self):
+        self._ok(self.lib.qbx_scf_step_async(self.h), "scf_step_async")
+
+    def stream_out(self, c_pinned: np.ndarray):
+        self._ok(self.lib.qbx_stream_out(self.h, _dp(c_pinned)), "stream_out")
+
+    def stream_wait(self):
+        e = np.zeros(NENERGY)
+        self._ok(self.lib.qbx_stream_wait(self.h, _dp(e)), "stream_wait")
+        return dict(zip(ENERGY_NAMES, e))
 
     # ---- k points off Gamma (complex bases)
     def set_kpoints(self, kpoints, weights):
