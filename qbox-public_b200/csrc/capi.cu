@@ -70,6 +70,9 @@ void free_cell(Context& c) {
   if (c.s_out) cudaStreamSynchronize(c.s_out);
   dfree(c.d_cin);
   dfree(c.d_cout);
+  if (c.d_psir) { cudaFree(c.d_psir); c.d_psir = nullptr; }
+  c.psir_bytes = 0;
+  c.psir_valid = false;
   c.in_pending = c.finish_pending = false;
   free_mixed(c);
   free_mix(c);
@@ -179,9 +182,15 @@ void step_eager(Context& c, bool want_f, bool want_s, double* energies, double* 
     finish_theta(c);
     return;
   }
+  // psi(r) of the density pass is reused by the H*psi pass
+  c.psir_store = true;
   update_density(c);
+  c.psir_store = false;
   update_vhxc(c);
+  c.psir_use = true;
   energy(c, true, want_f);
+  c.psir_use = false;
+  c.psir_valid = false;
   if (want_s) compute_stress(c);
   launch_eigsum(c);
   readback(c, want_f);
@@ -210,14 +219,20 @@ long record_step(Context& c, bool want_f) {
   c.prof.on = false;
   c.capturing = true;
   auto restore = [&]() {
+    c.psir_store = c.psir_use = c.psir_valid = false;
     c.capturing = false;
     c.prof.on = prof;
     c.extrapolate = extrap;
   };
   try {
+    c.psir_store = true;
     update_density(c);
+    c.psir_store = false;
     update_vhxc(c);
+    c.psir_use = true;
     energy(c, true, want_f);
+    c.psir_use = false;
+    c.psir_valid = false;
     launch_eigsum(c);
     psda_update(c);
     enqueue_readback(c, want_f);
@@ -500,6 +515,7 @@ int qbx_set_cell(qbx_context* h, const double cell[9], double ecut, int nst, con
       if (const char* e = std::getenv("QBX_FAST_DENSITY_LANE_SHAPE"))
         c.fast_density_lane_shape = (std::atoi(e) == 3 || std::atoi(e) >= 5) && std::atoi(e) <= 7
                                         ? std::atoi(e) : 2;
+      if (const char* e = std::getenv("QBX_PSIR")) c.psir_mode = std::atoi(e) != 0 ? 1 : 0;
       if (const char* e = std::getenv("QBX_FAST_VPSI_SHAPE"))
         c.fast_vpsi_shape = std::max(0, std::min(2, std::atoi(e)));
     }

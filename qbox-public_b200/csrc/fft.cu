@@ -741,6 +741,25 @@ __global__ void k_to_float(const double* __restrict__ x, size_t n, float* __rest
 
 // The specialised kernels of fft_fast_*.cu in batches of band pairs through
 // ctx.d_zfast; false when the grid has none.
+// the psi(r) buffer (FP32, every band pair on the whole grid), allocated
+// outside stream capture when the device has room for it
+static bool psir_ready(Context& ctx) {
+  if (ctx.psir_mode == 0 || ctx.precision != MIXED || ctx.fast_lane_shape < 0) return false;
+  const size_t need = (size_t)((ctx.nst + 1) / 2) * ctx.N() * sizeof(float2);
+  if (ctx.d_psir && ctx.psir_bytes >= need) return true;
+  if (ctx.capturing) return false;
+  size_t freeb = 0, total = 0;
+  QBX_CUDA(cudaMemGetInfo(&freeb, &total));
+  if (freeb < need + ((size_t)4 << 30)) {
+    if (ctx.psir_mode < 0) ctx.psir_mode = 0;   // no room: recompute psi(r) from now on
+    return false;
+  }
+  if (ctx.d_psir) cudaFree(ctx.d_psir);
+  QBX_CUDA(cudaMalloc(&ctx.d_psir, need));
+  ctx.psir_bytes = need;
+  return true;
+}
+
 static bool staged_fast(Context& ctx, int op, const double* c, const double* v, double* rho,
                         const double* w, double* hc) {
   if (!ctx.fast_fft || !ctx.d_zfast) return false;
@@ -763,6 +782,13 @@ static bool staged_fast(Context& ctx, int op, const double* c, const double* v, 
   a.density_lane_shape = ctx.fast_density_lane_shape;
   a.density_chunks = ctx.fast_chunks;
   a.v = v;
+  a.psir = nullptr;
+  if (op == OP_DENSITY) {
+    ctx.psir_valid = false;
+    if (ctx.psir_store && psir_ready(ctx)) a.psir = ctx.d_psir;
+  } else if (ctx.psir_use && ctx.psir_valid && ctx.psir_src == c) {
+    a.psir = ctx.d_psir;
+  }
   if (op == OP_VPSI && ctx.precision == MIXED) {
     const size_t N = ctx.N();
     k_to_float<<<nblk(N), 256, 0, ctx.stream>>>(v, N, ctx.d_vr32);
@@ -786,6 +812,10 @@ static bool staged_fast(Context& ctx, int op, const double* c, const double* v, 
       return false;
     }
     first = false;
+  }
+  if (op == OP_DENSITY && a.psir) {
+    ctx.psir_valid = true;
+    ctx.psir_src = c;
   }
   return true;
 }

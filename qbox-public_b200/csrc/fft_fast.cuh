@@ -345,12 +345,104 @@ __host__ __device__ constexpr int lane_threads(int shape) {
 }
 __host__ __device__ constexpr int lane_minblocks(int shape) { return (shape == 0 || shape == 4) ? 2 : 1; }
 
+// The real-space band pairs psi(r) kept in HBM between the density pass and
+// the H*psi pass of the same step (FP32, 8 bytes per point and pair: 11 GB
+// at 1 024 bands on a 140^3 grid).  A row's values stay in the register
+// layout of the x transform's output: the value at x = MX*bitrev(tx) + k of
+// lane tx is stored at k*TX + tx, so a warp's 8 rows x 4 lanes write 8 full
+// 32-byte sectors per store, and the H*psi kernel reads each lane's values
+// back into the registers it needs them in.
+template <int N0, int N1, int TX, int MX>
+__device__ __forceinline__ void store_psir(float2* __restrict__ psir, int pair, int n2, int z,
+                                           int y, int tx, const float2 (&val)[MX]) {
+  float2* row = psir + (((size_t)pair * n2 + z) * N1 + y) * N0 + tx;
+#pragma unroll
+  for (int k = 0; k < MX; ++k) row[k * TX] = val[k];
+}
+
+// H*psi plane pass from the stored psi(r): times V(r), forward x, forward y
+// on the occupied columns, outputs to the sticks through the column map (the
+// second half of kxy_lane_map; the backward z and xy transforms of the
+// density pass are not repeated).
+template <int N0, int N1>
+__global__ void __launch_bounds__(288, 1)
+kxy_lane_fwd(float2* __restrict__ zbuf, DeviceSticks g, const double2* __restrict__ twx_g,
+             const double2* __restrict__ twy_g, const float* __restrict__ v,
+             const float2* __restrict__ psir, int pair0) {
+  using C = float2;
+  constexpr int LD = pitch(N1);
+  constexpr int TY = lane::lanes_for(N1), MY = N1 / TY;
+  constexpr int TX = lane::lanes_for(N0), MX = N0 / TX;
+  static_assert(TY > 0 && TX > 0, "no register plan for this length");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int ncol = g.ncol, nvec = g.nvec;
+  C* twx = reinterpret_cast<C*>(smem_raw);
+  C* twy = twx + N0;
+  C* P = twy + N1;
+  int* xmap = reinterpret_cast<int*>(P + (size_t)ncol * LD);
+  const int z = blockIdx.x, pl = blockIdx.y;
+  load_tw(twx, twx_g, N0);
+  load_tw(twy, twy_g, N1);
+  for (int x = threadIdx.x; x < N0; x += blockDim.x) xmap[x] = -1;
+  __syncthreads();
+  for (int cidx = threadIdx.x; cidx < ncol; cidx += blockDim.x) xmap[g.col_x[cidx]] = cidx;
+  __syncthreads();
+  const int ty = threadIdx.x % TY, gy = threadIdx.x / TY, sy = blockDim.x / TY;
+  const int tx = threadIdx.x % TX, gx = threadIdx.x / TX, sx = blockDim.x / TX;
+  const int mry = lane::bitrev(ty, TY), mrx = lane::bitrev(tx, TX);
+  C* zp = zbuf + ((size_t)pl * g.n2 + z) * nvec;
+  const C* pp = psir + ((size_t)(pair0 + pl) * g.n2 + z) * N1 * N0 + tx;
+#pragma unroll 1
+  for (int base = 0; base < N1; base += sx) {
+    const int y = base + gx;
+    const bool ok = y < N1;
+    C val[MX];
+    const C* prow = pp + (size_t)(ok ? y : 0) * N0;
+    const float* vrow = v + ((size_t)z * N1 + (ok ? y : 0)) * N0 + MX * mrx;
+#pragma unroll
+    for (int k = 0; k < MX; ++k) {
+      const C p = ok ? prow[k * TX] : cmk<C>(0.0, 0.0);
+      const float vv = ok ? vrow[k] : 0.f;
+      val[k] = cmk<C>(p.x * vv, p.y * vv);
+    }
+    lane::line_r2n<TX, MX, -1>(val, tx, twx);
+    if (ok) {
+      int txh = tx;
+      asm volatile("" : "+r"(txh));
+#pragma unroll
+      for (int k = 0; k < MX; ++k) {
+        const int cidx = xmap[txh + TX * k];
+        if (cidx >= 0) P[cidx * LD + y] = val[k];
+      }
+    }
+  }
+  __syncthreads();
+#pragma unroll 1
+  for (int base = 0; base < ncol; base += sy) {
+    const int cidx = base + gy;
+    const bool ok = cidx < ncol;
+    const C* col = P + (ok ? cidx : 0) * LD;
+    C val[MY];
+#pragma unroll
+    for (int k2 = 0; k2 < MY; ++k2) val[k2] = ok ? col[k2 + MY * mry] : cmk<C>(0.0, 0.0);
+    lane::line_r2n<TY, MY, -1>(val, ty, twy);
+    if (ok) {
+      const int* cm = g.colmap + (size_t)cidx * N1;
+#pragma unroll
+      for (int k = 0; k < MY; ++k) {
+        const int s = __ldg(cm + ty + TY * k);
+        if (s >= 0) zp[s] = val[k];
+      }
+    }
+  }
+}
+
 template <int N0, int N1, int OP, int SHAPE>
 __global__ void __launch_bounds__(lane_threads(SHAPE), lane_minblocks(SHAPE))
 kxy_lane(float2* __restrict__ zbuf, int npairs, int pairs_per_cta, DeviceSticks g,
          const double2* __restrict__ twx_g, const double2* __restrict__ twy_g,
          const float* __restrict__ v, double* __restrict__ rho, const double* __restrict__ w,
-         int pair0, int nst) {
+         int pair0, int nst, float2* __restrict__ psir) {
   using C = float2;
   constexpr int LD = pitch(N1);
   constexpr int TY = lane::lanes_for(N1), MY = N1 / TY;
@@ -425,6 +517,7 @@ kxy_lane(float2* __restrict__ zbuf, int npairs, int pairs_per_cta, DeviceSticks 
       }
       lane::line_n2r<TX, MX, +1>(val, tx, twx);
       if constexpr (DENS) {
+        if (psir && ok) store_psir<N0, N1, TX, MX>(psir, pair0 + pl, g.n2, z, y, tx, val);
         if (ok) {
           float* arow = acc + y * N0 + MX * mrx;
 #pragma unroll
@@ -609,7 +702,8 @@ template <int N0, int N1>
 __global__ void __launch_bounds__(320, 1)
 kxy_lane_dmap(const float2* __restrict__ zbuf, int npairs, int pairs_per_cta, DeviceSticks g,
               const double2* __restrict__ twx_g, const double2* __restrict__ twy_g,
-              double* __restrict__ rho, const double* __restrict__ w, int pair0, int nst) {
+              double* __restrict__ rho, const double* __restrict__ w, int pair0, int nst,
+              float2* __restrict__ psir) {
   using C = float2;
   constexpr int LD = pitch(N1);
   constexpr int TY = lane::lanes_for(N1), MY = N1 / TY;
@@ -672,6 +766,7 @@ kxy_lane_dmap(const float2* __restrict__ zbuf, int npairs, int pairs_per_cta, De
         val[k] = (ok && cidx >= 0) ? P[cidx * LD + y] : cmk<C>(0.0, 0.0);
       }
       lane::line_n2r<TX, MX, +1>(val, tx, twx);
+      if (psir && ok) store_psir<N0, N1, TX, MX>(psir, pair0 + pl, g.n2, z, y, tx, val);
       if (ok) {
         float* arow = acc + y * N0 + MX * mrx;
 #pragma unroll
@@ -993,6 +1088,7 @@ struct StagedArgs {
   int lane_shape;          // FP32 register-lane plane kernel shape, -1 = not used
   int density_lane_shape;  // its density-pass shape (2, 3; 5 = half planes)
   int density_chunks;      // CTAs per plane in the density pass
+  float2* psir;            // DENSITY: store psi(r) here; VPSI: read it (skip the backward)
 };
 
 template <typename T, int N, int SH>
@@ -1019,7 +1115,7 @@ void launch_lane_xy(Context& ctx, const StagedArgs& a, int chunks, int ppc) {
   }
   kxy_lane<N, N, OP, SH><<<dim3(N, chunks), threads, sm, ctx.stream>>>(
       (float2*)a.zbuf, a.npairs, ppc, g, a.twx, a.twy, (const float*)a.v, a.rho, a.w, a.pair0,
-      a.nst);
+      a.nst, OP == XY_DENSITY ? a.psir : nullptr);
   QBX_LAUNCHED(ctx);
 }
 
@@ -1036,6 +1132,18 @@ void launch_lane_map(Context& ctx, const StagedArgs& a) {
 }
 
 template <int N>
+void launch_lane_fwd(Context& ctx, const StagedArgs& a) {
+  const DeviceSticks& g = ctx.dws;
+  const size_t sm = xym_smem_bytes<N, N>(g.ncol);
+  allow_smem(kxy_lane_fwd<N, N>, sm);
+  const int want = (g.ncol * lane::lanes_for(N) + 31) / 32 * 32;
+  const int threads = std::max(64, std::min(288, want));
+  kxy_lane_fwd<N, N><<<dim3(N, a.npairs), threads, sm, ctx.stream>>>(
+      (float2*)a.zbuf, g, a.twx, a.twy, (const float*)a.v, a.psir, a.pair0);
+  QBX_LAUNCHED(ctx);
+}
+
+template <int N>
 void launch_density_map(Context& ctx, const StagedArgs& a, int chunks, int ppc) {
   const DeviceSticks& g = ctx.dws;
   const size_t sm = xyl_smem_bytes<N, N, XY_DENSITY>(g.ncol);
@@ -1043,7 +1151,7 @@ void launch_density_map(Context& ctx, const StagedArgs& a, int chunks, int ppc) 
   const int want = (g.ncol * lane::lanes_for(N) + 31) / 32 * 32;
   const int threads = std::max(64, std::min(320, want));
   kxy_lane_dmap<N, N><<<dim3(N, chunks), threads, sm, ctx.stream>>>(
-      (const float2*)a.zbuf, a.npairs, ppc, g, a.twx, a.twy, a.rho, a.w, a.pair0, a.nst);
+      (const float2*)a.zbuf, a.npairs, ppc, g, a.twx, a.twy, a.rho, a.w, a.pair0, a.nst, a.psir);
   QBX_LAUNCHED(ctx);
 }
 
@@ -1106,14 +1214,16 @@ void run_cubic(Context& ctx, const StagedArgs& a) {
   const int rpc = a.rods_per_cta;
   const size_t zs = sizeof(C) * ((size_t)N + (size_t)2 * rpc * pitch(N));
   dim3 zgrid((g.nrods + rpc - 1) / rpc, a.npairs);
+  constexpr bool LANE = std::is_same<T, float>::value && lane::lanes_for(N) > 0;
+  // psi(r) of these pairs is stored: the H*psi pass needs no backward
+  const bool from_psir = LANE && a.op == XY_VPSI && a.psir && a.lane_shape >= 0;
   allow_smem(kz_bwd<T, N>, zs);
-  {
+  if (!from_psir) {
     ProfScope ps(ctx, "zfft_bwd");
     kz_bwd<T, N><<<zgrid, kZThreads, zs, st>>>((const double2*)a.c, ngw, a.nst, a.pair0, g, a.twz,
                                                (C*)a.zbuf, rpc);
     QBX_LAUNCHED(ctx);
   }
-  constexpr bool LANE = std::is_same<T, float>::value && lane::lanes_for(N) > 0;
   if constexpr (LANE) {
     if (a.lane_shape >= 0) {
       if (a.op == XY_DENSITY) {
@@ -1121,7 +1231,10 @@ void run_cubic(Context& ctx, const StagedArgs& a) {
         const int ppc = (a.npairs + chunks - 1) / chunks;
         chunks = (a.npairs + ppc - 1) / ppc;
         ProfScope ps(ctx, "xy_density");
-        if (a.density_lane_shape == 5 && density_half_ok<N>()) launch_density_half<N>(ctx, a, chunks, ppc);
+        // psi(r) is stored by the whole-plane kernels (shapes 2, 3, 6)
+        if (a.psir && a.density_lane_shape != 6 && a.density_lane_shape != 2)
+          launch_lane_xy<N, XY_DENSITY, 3>(ctx, a, chunks, ppc);
+        else if (a.density_lane_shape == 5 && density_half_ok<N>()) launch_density_half<N>(ctx, a, chunks, ppc);
         else if (a.density_lane_shape == 6) launch_density_map<N>(ctx, a, chunks, ppc);
         else if (a.density_lane_shape == 7 && density_tmem_fits<N>(ctx)) launch_density_tmem<N>(ctx, a, chunks, ppc);
         else if (a.density_lane_shape == 3) launch_lane_xy<N, XY_DENSITY, 3>(ctx, a, chunks, ppc);
@@ -1130,7 +1243,8 @@ void run_cubic(Context& ctx, const StagedArgs& a) {
       }
       {
         ProfScope ps(ctx, "xy_vpsi");
-        switch (a.lane_shape) {
+        if (from_psir) launch_lane_fwd<N>(ctx, a);
+        else switch (a.lane_shape) {
           case 5: launch_lane_map<N, 2>(ctx, a); break;
           case 6: launch_lane_map<N, 1>(ctx, a); break;
           case 1: launch_lane_xy<N, XY_VPSI, 1>(ctx, a, a.npairs, 1); break;

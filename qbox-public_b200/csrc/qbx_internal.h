@@ -462,6 +462,14 @@ struct Context {
   long batch_launches = 0;       // batch graphs launched with this context leading
   int polar_iters = 0;           // iterations of the last eager polar
   double* d_wfv = nullptr;       // wavefunction velocity of the MD extrapolation
+  // psi(r) of every band pair kept in HBM (FP32) from the density pass to
+  // the H*psi pass of the same step: the step functions set psir_store
+  // around update_density and psir_use around energy
+  float2* d_psir = nullptr;
+  size_t psir_bytes = 0;
+  int psir_mode = -1;            // -1 auto (mixed precision, if it fits), 0 off, 1 on
+  bool psir_store = false, psir_use = false, psir_valid = false;
+  const double* psir_src = nullptr;   // the coefficients psi(r) was made from
   // streamed SlaterDet (qbx_stream_in / qbx_scf_step_async / qbx_stream_out):
   // two copy streams, the staging buffers of one step's input and result,
   // and the events that order them against the compute stream

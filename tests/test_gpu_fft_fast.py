@@ -135,3 +135,27 @@ def test_density_tmem_si512(monkeypatch):
     np.testing.assert_allclose(rb, ra, rtol=0, atol=2e-6 * np.abs(ra).max())
     ref.close()
     tm.close()
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_stored_psi_r_gives_the_recomputed_step(graph, monkeypatch):
+    """psi(r) kept in HBM from the density pass and reused by the H*psi pass
+    of the same step (QBX_PSIR=1) gives the step that transforms every band
+    pair backward twice (QBX_PSIR=0): energies to 1e-12 relative and the
+    coefficients after three steps to 1e-12, eager and captured."""
+    s = systems.si64()
+    ctxs = []
+    for mode in ("1", "0"):
+        monkeypatch.setenv("QBX_PSIR", mode)
+        c = _ctx(s, capi.MIXED, True)
+        c.set_step_graph(graph)
+        ctxs.append(c)
+    monkeypatch.delenv("QBX_PSIR")
+    a, b = ctxs
+    for _ in range(3):
+        ea, eb = a.scf_step(), b.scf_step()
+        for k in ("ekin", "enl", "etotal", "eigenvalue_sum"):
+            assert abs(ea[k] - eb[k]) <= 1e-12 * abs(eb[k]) + 1e-12, (k, ea[k], eb[k])
+    np.testing.assert_allclose(a.get_coeffs(), b.get_coeffs(), rtol=0, atol=1e-12)
+    a.close()
+    b.close()
