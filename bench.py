@@ -155,13 +155,16 @@ def run_reference_arm(args):
 
 
 # ------------------------------------------------------------ our arm
-def algorithmic_bytes_xy_vpsi(ctx, npairs: int, cbytes: int, vbytes: int) -> float:
-    """Per H*psi: for every band pair the plane pass reads and writes every
-    stick value once (2 S c) and reads the potential once (N v bytes)."""
+def algorithmic_bytes_xy_vpsi(ctx, npairs: int, nlaunch: float, cbytes: int, vbytes: int) -> float:
+    """Per H*psi, the H*psi plane kernel that starts from the stored psi(r)
+    (kxy_lane_fwd): every band pair's psi(r) read once (N c bytes), its sticks
+    written once (S c bytes), and the potential read once per launch
+    (N v bytes)."""
     n0, n1, n2 = ctx.grid
+    N = n0 * n1 * n2
     nvec = 2 * nrods(ctx) - 1
     S = nvec * n2
-    return npairs * (2.0 * S * cbytes + float(vbytes) * n0 * n1 * n2)
+    return npairs * float(N + S) * cbytes + nlaunch * float(vbytes) * N
 
 
 def nrods(ctx) -> int:
@@ -245,7 +248,7 @@ def run_ours(args):
     npairs = (s.nbands + 1) // 2
     # one xy_vpsi launch per batch of band pairs
     t_xy, n_xy = prof["xy_vpsi"]["ms_per_step"], prof["xy_vpsi"]["launches_per_step"]
-    bytes_hpsi = algorithmic_bytes_xy_vpsi(mix, npairs, 8, 4)
+    bytes_hpsi = algorithmic_bytes_xy_vpsi(mix, npairs, n_xy, 8, 4)
     per_launch_bytes = bytes_hpsi / max(1e-9, n_xy)
     per_launch_ms = t_xy / max(1e-9, n_xy)
     peaks = {}
@@ -255,15 +258,16 @@ def run_ours(args):
         pass
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     achieved = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9
-    roofline = {"kernel": "kxy_lane_map<140,140> (plane pass of H*psi, register-lane FFTs)",
+    roofline = {"kernel": "kxy_lane_fwd<140,140> (H*psi plane pass from the stored psi(r): "
+                          "times V, forward x and y register-lane FFTs)",
                 "bound": "hbm",
                 "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                 "frac": achieved / hbm_peak,
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                 # DRAM bytes per launch: the ncu capture of this kernel
-                # (profiles/kxy_lane_map_vpsi_si512.md: 198.3 MB for a
-                # 32-pair launch) scaled by the band pairs of this run's launches
-                "traffic": 198.3e6 / 32.0 * (npairs / max(1e-9, n_xy)),
+                # (profiles/kxy_lane_fwd_si512.md: 424.0 MB for a 16-pair
+                # launch) scaled by the band pairs of this run's launches
+                "traffic": 424.0e6 / 16.0 * (npairs / max(1e-9, n_xy)),
                 "algorithmic_bytes_per_launch": per_launch_bytes,
                 "launch_ms": per_launch_ms}
     # GEMM share (FP64 cuBLAS in this build) against the dense FP64 rate

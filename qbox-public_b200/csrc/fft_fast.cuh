@@ -365,7 +365,7 @@ __device__ __forceinline__ void store_psir(float2* __restrict__ psir, int pair, 
 // second half of kxy_lane_map; the backward z and xy transforms of the
 // density pass are not repeated).
 template <int N0, int N1>
-__global__ void __launch_bounds__(288, 1)
+__global__ void __maxnreg__(112)
 kxy_lane_fwd(float2* __restrict__ zbuf, DeviceSticks g, const double2* __restrict__ twx_g,
              const double2* __restrict__ twy_g, const float* __restrict__ v,
              const float2* __restrict__ psir, int pair0) {
