@@ -513,7 +513,7 @@ int qbx_set_cell(qbx_context* h, const double cell[9], double ecut, int nst, con
       if (const char* e = std::getenv("QBX_FAST_LANE_SHAPE"))
         c.fast_lane_shape = std::max(-1, std::min(6, std::atoi(e)));
       if (const char* e = std::getenv("QBX_FAST_DENSITY_LANE_SHAPE"))
-        c.fast_density_lane_shape = (std::atoi(e) == 3 || std::atoi(e) >= 5) && std::atoi(e) <= 7
+        c.fast_density_lane_shape = (std::atoi(e) == 3 || std::atoi(e) >= 5) && std::atoi(e) <= 8
                                         ? std::atoi(e) : 2;
       if (const char* e = std::getenv("QBX_PSIR")) c.psir_mode = std::atoi(e) != 0 ? 1 : 0;
       if (const char* e = std::getenv("QBX_FAST_VPSI_SHAPE"))

@@ -1052,7 +1052,7 @@ void autotune_fft(Context& ctx, std::vector<std::pair<std::string, double>>* log
     if (ctx.precision == MIXED && ctx.fast_lane_shape >= 0) {
       double best = 1e30;
       int pick = ctx.fast_density_lane_shape;
-      for (int s : {3, 2, 5, 6, 7}) {
+      for (int s : {3, 2, 5, 6, 7, 8}) {
         ctx.fast_density_lane_shape = s;
         const double t = time_ms(dens);
         note("density lane " + std::to_string(s), t);

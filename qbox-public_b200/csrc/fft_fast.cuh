@@ -781,6 +781,135 @@ kxy_lane_dmap(const float2* __restrict__ zbuf, int npairs, int pairs_per_cta, De
 }
 
 // ------------------------------------------------------------ density,
+// next band pair's sticks queued during the x rows
+// The density pass of kxy_lane<DENSITY> (whole plane, FP32 accumulator in
+// shared memory, psi(r) optionally stored) with two tiles: P holds the
+// sticks of a pair at their (column, y) places and zeros everywhere else,
+// and the backward y transform writes its output to a second tile Q instead
+// of in place.  P's zeros therefore survive, so P is cleared once per CTA
+// instead of once per pair, and as soon as the y transform has read P the
+// next pair's sticks are copied into it with cp.async (8 bytes per stick,
+// straight to its place in the tile) while the x rows of the current pair
+// run from Q.  Each thread keeps the tile offsets of its sticks in
+// registers (at most kDqSticks per thread).  Density shape 8: 288 threads,
+// one CTA per SM; at 140^3 the two tiles, the accumulator and the tables
+// take 227 840 of the 232 448 bytes a CTA may hold.
+constexpr int kDqSticks = 16;
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+template <int N0, int N1>
+__host__ size_t xydq_smem_bytes(int ncol) {
+  return sizeof(float2) * ((size_t)N0 + N1 + (size_t)2 * ncol * pitch(N1)) +
+         sizeof(float) * (size_t)N0 * N1 + sizeof(int) * (size_t)N0;
+}
+
+template <int N0, int N1>
+__global__ void __launch_bounds__(288, 1)
+kxy_lane_dq(const float2* __restrict__ zbuf, int npairs, int pairs_per_cta, DeviceSticks g,
+            const double2* __restrict__ twx_g, const double2* __restrict__ twy_g,
+            double* __restrict__ rho, const double* __restrict__ w, int pair0, int nst,
+            float2* __restrict__ psir) {
+  using C = float2;
+  constexpr int LD = pitch(N1);
+  constexpr int TY = lane::lanes_for(N1), MY = N1 / TY;
+  constexpr int TX = lane::lanes_for(N0), MX = N0 / TX;
+  static_assert(TY > 0 && TX > 0, "no register plan for this length");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int ncol = g.ncol, nvec = g.nvec;
+  C* twx = reinterpret_cast<C*>(smem_raw);
+  C* twy = twx + N0;
+  C* P = twy + N1;
+  C* Q = P + (size_t)ncol * LD;
+  float* acc = reinterpret_cast<float*>(Q + (size_t)ncol * LD);
+  int* xmap = reinterpret_cast<int*>(acc + (size_t)N0 * N1);
+  const int z = blockIdx.x;
+  load_tw(twx, twx_g, N0);
+  load_tw(twy, twy_g, N1);
+  for (int x = threadIdx.x; x < N0; x += blockDim.x) xmap[x] = -1;
+  for (int t = threadIdx.x; t < N0 * N1; t += blockDim.x) acc[t] = 0.f;
+  for (int t = threadIdx.x; t < ncol * LD; t += blockDim.x) P[t] = cmk<C>(0.0, 0.0);
+  // tile offsets of this thread's sticks s = threadIdx.x + j * blockDim.x
+  int soff[kDqSticks];
+#pragma unroll
+  for (int j = 0; j < kDqSticks; ++j) {
+    const int s = threadIdx.x + j * blockDim.x;
+    soff[j] = s < nvec ? g.stick_col[s] * LD + g.stick_y[s] : -1;
+  }
+  __syncthreads();
+  for (int cidx = threadIdx.x; cidx < ncol; cidx += blockDim.x) xmap[g.col_x[cidx]] = cidx;
+  const int ty = threadIdx.x % TY, gy = threadIdx.x / TY, sy = blockDim.x / TY;
+  const int tx = threadIdx.x % TX, gx = threadIdx.x / TX, sx = blockDim.x / TX;
+  const int mry = lane::bitrev(ty, TY), mrx = lane::bitrev(tx, TX);
+  const int pbeg = blockIdx.y * pairs_per_cta;
+  const int pend = min(npairs, pbeg + pairs_per_cta);
+  auto queue_sticks = [&](int pl) {
+    const C* zp = zbuf + ((size_t)pl * g.n2 + z) * nvec + threadIdx.x;
+#pragma unroll
+    for (int j = 0; j < kDqSticks; ++j)
+      if (soff[j] >= 0) cp_async8(P + soff[j], zp + (size_t)j * blockDim.x);
+    cp_async_commit();
+  };
+  if (pbeg < pend) queue_sticks(pbeg);
+#pragma unroll 1
+  for (int pl = pbeg; pl < pend; ++pl) {
+    cp_async_wait_all();
+    __syncthreads();   // P holds pair pl's sticks; the previous x rows are done with Q
+    // backward y on the occupied columns: P (natural) -> Q (m-distributed)
+#pragma unroll 1
+    for (int base = 0; base < ncol; base += sy) {
+      const int cidx = base + gy;
+      const bool ok = cidx < ncol;
+      const C* col = P + (ok ? cidx : 0) * LD;
+      C val[MY];
+#pragma unroll
+      for (int k = 0; k < MY; ++k) val[k] = ok ? col[ty + TY * k] : cmk<C>(0.0, 0.0);
+      lane::line_n2r<TY, MY, +1>(val, ty, twy);
+      if (ok) {
+        C* qcol = Q + cidx * LD;
+#pragma unroll
+        for (int k2 = 0; k2 < MY; ++k2) qcol[k2 + MY * mry] = val[k2];
+      }
+    }
+    __syncthreads();   // P is free: the next pair's sticks stream in under the x rows
+    if (pl + 1 < pend) queue_sticks(pl + 1);
+    const int b1 = 2 * (pair0 + pl);
+    const float f1 = (float)w[b1];
+    const float f2 = (b1 + 1 < nst) ? (float)w[b1 + 1] : 0.f;
+#pragma unroll 1
+    for (int base = 0; base < N1; base += sx) {
+      const int y = base + gx;
+      const bool ok = y < N1;
+      int txh = tx;
+      asm volatile("" : "+r"(txh));
+      C val[MX];
+#pragma unroll
+      for (int k = 0; k < MX; ++k) {
+        const int cidx = xmap[txh + TX * k];
+        val[k] = (ok && cidx >= 0) ? Q[cidx * LD + y] : cmk<C>(0.0, 0.0);
+      }
+      lane::line_n2r<TX, MX, +1>(val, tx, twx);
+      if (psir && ok) store_psir<N0, N1, TX, MX>(psir, pair0 + pl, g.n2, z, y, tx, val);
+      if (ok) {
+        float* arow = acc + y * N0 + MX * mrx;
+#pragma unroll
+        for (int k2 = 0; k2 < MX; ++k2)
+          arow[k2] += f1 * val[k2].x * val[k2].x + f2 * val[k2].y * val[k2].y;
+      }
+    }
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  const size_t pbase = (size_t)z * N1 * N0;
+  for (int t = threadIdx.x; t < N0 * N1; t += blockDim.x) atomicAdd(&rho[pbase + t], (double)acc[t]);
+}
+
+// ------------------------------------------------------------ density,
 // accumulator in tensor memory
 // The density pass of kxy_lane<DENSITY> with the FP32 accumulator held in
 // tensor memory (TMEM) instead of shared memory.  A thread accumulates the
@@ -1155,6 +1284,25 @@ void launch_density_map(Context& ctx, const StagedArgs& a, int chunks, int ppc) 
   QBX_LAUNCHED(ctx);
 }
 
+// false (nothing launched) when the two tiles do not fit a CTA's shared
+// memory or a thread would hold more than kDqSticks sticks
+template <int N>
+bool launch_density_dq(Context& ctx, const StagedArgs& a, int chunks, int ppc) {
+  const DeviceSticks& g = ctx.dws;
+  const size_t sm = xydq_smem_bytes<N, N>(g.ncol);
+  const int want = (g.ncol * lane::lanes_for(N) + 31) / 32 * 32;
+  const int threads = std::max(64, std::min(288, want));
+  int dev = 0, optin = 0;
+  QBX_CUDA(cudaGetDevice(&dev));
+  QBX_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  if (sm > (size_t)optin || g.nvec > kDqSticks * threads) return false;
+  allow_smem(kxy_lane_dq<N, N>, sm);
+  kxy_lane_dq<N, N><<<dim3(N, chunks), threads, sm, ctx.stream>>>(
+      (const float2*)a.zbuf, a.npairs, ppc, g, a.twx, a.twy, a.rho, a.w, a.pair0, a.nst, a.psir);
+  QBX_LAUNCHED(ctx);
+  return true;
+}
+
 // threads of the TMEM density kernel: one lane group per occupied column,
 // at most 288
 template <int N>
@@ -1231,9 +1379,14 @@ void run_cubic(Context& ctx, const StagedArgs& a) {
         const int ppc = (a.npairs + chunks - 1) / chunks;
         chunks = (a.npairs + ppc - 1) / ppc;
         ProfScope ps(ctx, "xy_density");
-        // psi(r) is stored by the whole-plane kernels (shapes 2, 3, 6)
-        if (a.psir && a.density_lane_shape != 6 && a.density_lane_shape != 2)
+        // psi(r) is stored by the whole-plane kernels (shapes 2, 3, 6, 8)
+        if (a.psir && a.density_lane_shape != 6 && a.density_lane_shape != 2 &&
+            a.density_lane_shape != 8)
           launch_lane_xy<N, XY_DENSITY, 3>(ctx, a, chunks, ppc);
+        else if (a.density_lane_shape == 8) {
+          if (!launch_density_dq<N>(ctx, a, chunks, ppc))
+            launch_lane_xy<N, XY_DENSITY, 3>(ctx, a, chunks, ppc);
+        }
         else if (a.density_lane_shape == 5 && density_half_ok<N>()) launch_density_half<N>(ctx, a, chunks, ppc);
         else if (a.density_lane_shape == 6) launch_density_map<N>(ctx, a, chunks, ppc);
         else if (a.density_lane_shape == 7 && density_tmem_fits<N>(ctx)) launch_density_tmem<N>(ctx, a, chunks, ppc);

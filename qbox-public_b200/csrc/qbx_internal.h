@@ -425,7 +425,8 @@ struct Context {
   int fast_lane_shape = 4;      // FP32 register-lane plane kernel shape (5: sticks through
                                 // the column map), -1 = off
   int fast_density_lane_shape = 3;  // its density shape (2, 3; 5 half planes; 6 sticks
-                                    // read through the column map; 7 TMEM accumulator)
+                                    // read through the column map; 7 TMEM accumulator;
+                                    // 8 next pair's sticks queued with cp.async)
   int fast_chunks = 8;          // CTAs per plane in the density pass
   bool fast_fft = true;         // use the specialised kernels when compiled
   float* a32 = nullptr;         // TF32 hi/lo split of the projectors

@@ -80,13 +80,14 @@ def test_autotune_keeps_results(precision):
     a.close()
 
 
-@pytest.mark.parametrize("shape", [5, 6, 7])
+@pytest.mark.parametrize("shape", [5, 6, 7, 8])
 @pytest.mark.parametrize("name", ["si8", "si64", "h2o32"])
 def test_density_half_planes(name, shape, monkeypatch):
     """The half-plane density kernel (shape 5: two CTAs per plane), the
-    whole-plane kernel reading the sticks through the column map (shape 6)
-    and the kernel accumulating in tensor memory (shape 7) give the default
-    kernel's density (FP32, 2e-6 of the largest value)."""
+    whole-plane kernel reading the sticks through the column map (shape 6),
+    the kernel accumulating in tensor memory (shape 7) and the kernel that
+    queues the next band pair's sticks with cp.async (shape 8) give the
+    default kernel's density (FP32, 2e-6 of the largest value)."""
     s = systems.get(name)
     ref = _ctx(s, capi.MIXED, True)
     monkeypatch.setenv("QBX_FAST_DENSITY_LANE_SHAPE", str(shape))
@@ -135,6 +136,31 @@ def test_density_tmem_si512(monkeypatch):
     np.testing.assert_allclose(rb, ra, rtol=0, atol=2e-6 * np.abs(ra).max())
     ref.close()
     tm.close()
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_density_queued_sticks_si512(graph, monkeypatch):
+    """Density shape 8 on the 512-atom cell's 140^3 grid, where its two
+    tiles, accumulator and tables fill 227 840 bytes of shared memory: the
+    step that stores psi(r) from it gives the default kernel's energies
+    (1e-12 relative) and coefficients after two steps (1e-12), eager and
+    captured."""
+    s = systems.si512().band_sample(32)
+    ctxs = []
+    for shape in ("8", "3"):
+        monkeypatch.setenv("QBX_FAST_DENSITY_LANE_SHAPE", shape)
+        c = _ctx(s, capi.MIXED, True)
+        c.set_step_graph(graph)
+        ctxs.append(c)
+    monkeypatch.delenv("QBX_FAST_DENSITY_LANE_SHAPE")
+    a, b = ctxs
+    for _ in range(3 if graph else 2):
+        ea, eb = a.scf_step(), b.scf_step()
+        for k in ("ekin", "enl", "etotal", "eigenvalue_sum"):
+            assert abs(ea[k] - eb[k]) <= 1e-12 * abs(eb[k]) + 1e-12, (k, ea[k], eb[k])
+    np.testing.assert_allclose(a.get_coeffs(), b.get_coeffs(), rtol=0, atol=1e-12)
+    a.close()
+    b.close()
 
 
 @pytest.mark.parametrize("graph", [False, True])
