@@ -781,6 +781,7 @@ static bool staged_fast(Context& ctx, int op, const double* c, const double* v, 
   a.lane_shape = ctx.fast_lane_shape;
   a.density_lane_shape = ctx.fast_density_lane_shape;
   a.density_chunks = ctx.fast_chunks;
+  a.fwd_pairs_per_cta = ctx.fast_fwd_ppc;
   a.v = v;
   a.psir = nullptr;
   if (op == OP_DENSITY) {

@@ -360,15 +360,25 @@ __device__ __forceinline__ void store_psir(float2* __restrict__ psir, int pair, 
   for (int k = 0; k < MX; ++k) row[k * TX] = val[k];
 }
 
+// L2 prefetch of a contiguous range (16-byte aligned start, size a multiple
+// of 16 bytes): one instruction streams it from HBM while the CTA works on
+// something else.
+__device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"(bytes) : "memory");
+}
+
 // H*psi plane pass from the stored psi(r): times V(r), forward x, forward y
 // on the occupied columns, outputs to the sticks through the column map (the
 // second half of kxy_lane_map; the backward z and xy transforms of the
-// density pass are not repeated).
+// density pass are not repeated).  A CTA takes pairs_per_cta band pairs of
+// one plane; while it works on one pair, the next pair's psi(r) plane (one
+// contiguous N0*N1*8-byte block) is prefetched into L2 by one bulk
+// instruction, so the x rows' loads find it there.
 template <int N0, int N1>
 __global__ void __maxnreg__(112)
 kxy_lane_fwd(float2* __restrict__ zbuf, DeviceSticks g, const double2* __restrict__ twx_g,
              const double2* __restrict__ twy_g, const float* __restrict__ v,
-             const float2* __restrict__ psir, int pair0) {
+             const float2* __restrict__ psir, int pair0, int npairs, int pairs_per_cta) {
   using C = float2;
   constexpr int LD = pitch(N1);
   constexpr int TY = lane::lanes_for(N1), MY = N1 / TY;
@@ -380,7 +390,12 @@ kxy_lane_fwd(float2* __restrict__ zbuf, DeviceSticks g, const double2* __restric
   C* twy = twx + N0;
   C* P = twy + N1;
   int* xmap = reinterpret_cast<int*>(P + (size_t)ncol * LD);
-  const int z = blockIdx.x, pl = blockIdx.y;
+  const int z = blockIdx.x;
+  const int pbeg = blockIdx.y * pairs_per_cta;
+  const int pend = min(npairs, pbeg + pairs_per_cta);
+  constexpr size_t kPlane = (size_t)N1 * N0;
+  auto psir_plane = [&](int pl) { return psir + ((size_t)(pair0 + pl) * g.n2 + z) * kPlane; };
+  if (threadIdx.x == 0 && pbeg < pend) prefetch_l2(psir_plane(pbeg), (unsigned)(kPlane * sizeof(C)));
   load_tw(twx, twx_g, N0);
   load_tw(twy, twy_g, N1);
   for (int x = threadIdx.x; x < N0; x += blockDim.x) xmap[x] = -1;
@@ -390,8 +405,12 @@ kxy_lane_fwd(float2* __restrict__ zbuf, DeviceSticks g, const double2* __restric
   const int ty = threadIdx.x % TY, gy = threadIdx.x / TY, sy = blockDim.x / TY;
   const int tx = threadIdx.x % TX, gx = threadIdx.x / TX, sx = blockDim.x / TX;
   const int mry = lane::bitrev(ty, TY), mrx = lane::bitrev(tx, TX);
+#pragma unroll 1
+  for (int pl = pbeg; pl < pend; ++pl) {
+  if (threadIdx.x == 0 && pl + 1 < pend)
+    prefetch_l2(psir_plane(pl + 1), (unsigned)(kPlane * sizeof(C)));
   C* zp = zbuf + ((size_t)pl * g.n2 + z) * nvec;
-  const C* pp = psir + ((size_t)(pair0 + pl) * g.n2 + z) * N1 * N0 + tx;
+  const C* pp = psir_plane(pl) + tx;
 #pragma unroll 1
   for (int base = 0; base < N1; base += sx) {
     const int y = base + gx;
@@ -434,6 +453,8 @@ kxy_lane_fwd(float2* __restrict__ zbuf, DeviceSticks g, const double2* __restric
         if (s >= 0) zp[s] = val[k];
       }
     }
+  }
+  __syncthreads();   // the y columns are read out of P before the next pair's x rows
   }
 }
 
@@ -1218,6 +1239,7 @@ struct StagedArgs {
   int density_lane_shape;  // its density-pass shape (2, 3; 5 = half planes)
   int density_chunks;      // CTAs per plane in the density pass
   float2* psir;            // DENSITY: store psi(r) here; VPSI: read it (skip the backward)
+  int fwd_pairs_per_cta;   // VPSI from psi(r): band pairs per CTA of kxy_lane_fwd
 };
 
 template <typename T, int N, int SH>
@@ -1267,8 +1289,10 @@ void launch_lane_fwd(Context& ctx, const StagedArgs& a) {
   allow_smem(kxy_lane_fwd<N, N>, sm);
   const int want = (g.ncol * lane::lanes_for(N) + 31) / 32 * 32;
   const int threads = std::max(64, std::min(288, want));
-  kxy_lane_fwd<N, N><<<dim3(N, a.npairs), threads, sm, ctx.stream>>>(
-      (float2*)a.zbuf, g, a.twx, a.twy, (const float*)a.v, a.psir, a.pair0);
+  const int ppc = std::max(1, std::min(a.npairs, a.fwd_pairs_per_cta));
+  const int chunks = (a.npairs + ppc - 1) / ppc;
+  kxy_lane_fwd<N, N><<<dim3(N, chunks), threads, sm, ctx.stream>>>(
+      (float2*)a.zbuf, g, a.twx, a.twy, (const float*)a.v, a.psir, a.pair0, a.npairs, ppc);
   QBX_LAUNCHED(ctx);
 }
 

@@ -428,6 +428,7 @@ struct Context {
                                     // read through the column map; 7 TMEM accumulator;
                                     // 8 next pair's sticks queued with cp.async)
   int fast_chunks = 8;          // CTAs per plane in the density pass
+  int fast_fwd_ppc = 2;         // band pairs per CTA of the H*psi plane kernel from psi(r)
   bool fast_fft = true;         // use the specialised kernels when compiled
   float* a32 = nullptr;         // TF32 hi/lo split of the projectors
   float* a32lo = nullptr;

@@ -163,6 +163,29 @@ def test_density_queued_sticks_si512(graph, monkeypatch):
     b.close()
 
 
+@pytest.mark.parametrize("ppc", ["3", "16"])
+def test_hpsi_from_psi_r_pairs_per_cta(ppc, monkeypatch):
+    """The H*psi plane kernel from the stored psi(r) with several band pairs
+    per CTA (3: a launch's 16 pairs end in a partial CTA; 16: one CTA per
+    plane), each prefetching the next pair's psi(r) plane into L2, gives the
+    one-pair-per-CTA kernel's step: energies to 1e-12 relative and the
+    coefficients after two steps to 1e-12."""
+    s = systems.si64()
+    ctxs = []
+    for mode in (ppc, "1"):
+        monkeypatch.setenv("QBX_FWD_PAIRS_PER_CTA", mode)
+        ctxs.append(_ctx(s, capi.MIXED, True))
+    monkeypatch.delenv("QBX_FWD_PAIRS_PER_CTA")
+    a, b = ctxs
+    for _ in range(2):
+        ea, eb = a.scf_step(), b.scf_step()
+        for k in ("ekin", "enl", "etotal", "eigenvalue_sum"):
+            assert abs(ea[k] - eb[k]) <= 1e-12 * abs(eb[k]) + 1e-12, (k, ea[k], eb[k])
+    np.testing.assert_allclose(a.get_coeffs(), b.get_coeffs(), rtol=0, atol=1e-12)
+    a.close()
+    b.close()
+
+
 @pytest.mark.parametrize("graph", [False, True])
 def test_stored_psi_r_gives_the_recomputed_step(graph, monkeypatch):
     """psi(r) kept in HBM from the density pass and reused by the H*psi pass
