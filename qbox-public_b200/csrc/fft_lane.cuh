@@ -160,11 +160,24 @@ __host__ __device__ constexpr int bitrev(int t, int T) {
   return r;
 }
 
-// W_{2h}^{e} with DIR sign, e in [0, h), h in {1, 2}
-template <int DIR, typename C> __device__ __forceinline__ C w2h(C x, int e, int h) {
-  if (h == 1 || e == 0) return x;
-  // h == 2, e == 1: W_4 = DIR i
-  return reg::cmuli<DIR>(x);
+// One butterfly of a cross-lane stage: the lower lane of the pair keeps
+// a + b, the upper one b - a, both as s*a + b with s = +-1 per lane (an
+// exact fused multiply-add), so every lane runs the same two instructions
+// instead of forming both results and selecting one.
+template <typename C> __device__ __forceinline__ C lane_bfly(C a, C b, float s) {
+  using Real = decltype(a.x);
+  C r;
+  r.x = (Real)s * a.x + b.x;
+  r.y = (Real)s * a.y + b.y;
+  return r;
+}
+// x or x * (DIR i), chosen per lane
+template <int DIR, typename C> __device__ __forceinline__ C rot_if(C x, bool rot) {
+  const C r = reg::cmuli<DIR>(x);
+  C o;
+  o.x = rot ? r.x : x.x;
+  o.y = rot ? r.y : x.y;
+  return o;
 }
 
 // T-point DFT across the lanes t = 0..T-1 of a group, one value per lane:
@@ -176,8 +189,9 @@ __device__ __forceinline__ C group_dft_n2r(C a, int t) {
   for (int h = T / 2; h >= 1; h >>= 1) {
     const C b = shfl_xor(a, h);
     const int j = t & (2 * h - 1);
-    if (j < h) a = cadd(a, b);
-    else a = w2h<DIR>(csub(b, a), j - h, h);
+    a = lane_bfly(a, b, j < h ? 1.f : -1.f);
+    // W_{2h}^{j-h} on the upper lanes: only W_4^1 = DIR i is not 1
+    if (h == 2) a = rot_if<DIR>(a, j == 3);
   }
   return a;
 }
@@ -191,10 +205,9 @@ __device__ __forceinline__ C group_dft_r2n(C a, int t) {
   for (int h = 1; h <= T / 2; h <<= 1) {
     const int j = t & (2 * h - 1);
     // the upper element of each butterfly is twiddled before the exchange
-    if (j >= h) a = w2h<DIR>(a, j - h, h);
+    if (h == 2) a = rot_if<DIR>(a, j == 3);
     const C b = shfl_xor(a, h);
-    if (j < h) a = cadd(a, b);
-    else a = csub(b, a);
+    a = lane_bfly(a, b, j < h ? 1.f : -1.f);
   }
   return a;
 }
