@@ -782,6 +782,7 @@ static bool staged_fast(Context& ctx, int op, const double* c, const double* v, 
   a.density_lane_shape = ctx.fast_density_lane_shape;
   a.density_chunks = ctx.fast_chunks;
   a.fwd_pairs_per_cta = ctx.fast_fwd_ppc;
+  a.zlane = ctx.fast_zlane;
   a.v = v;
   a.psir = nullptr;
   if (op == OP_DENSITY) {
@@ -1086,17 +1087,22 @@ void autotune_fft(Context& ctx, std::vector<std::pair<std::string, double>>* log
       }
       ctx.fast_batch = pick;
     }
-    // 4. rods per CTA of the z kernels
+    // 4. z-stick kernels (register lanes or a warp per stick) and rods per CTA
     {
       double best = 1e30;
-      int pick = ctx.fast_rods;
-      for (int r : {8, 16, 24}) {
-        ctx.fast_rods = r;
-        const double t = time_ms(vpsi);
-        note("rods per z CTA " + std::to_string(r), t);
-        if (t < best) { best = t; pick = r; }
+      int pick = ctx.fast_rods, pick_z = ctx.fast_zlane;
+      for (int zl : {1, 0}) {
+        if (zl == 0 && ctx.precision != MIXED) continue;
+        if (ctx.precision == MIXED) ctx.fast_zlane = zl;
+        for (int r : {8, 16, 24}) {
+          ctx.fast_rods = r;
+          const double t = time_ms(vpsi);
+          note("z lanes " + std::to_string(ctx.fast_zlane) + " rods per z CTA " + std::to_string(r), t);
+          if (t < best) { best = t; pick = r; pick_z = ctx.fast_zlane; }
+        }
       }
       ctx.fast_rods = pick;
+      ctx.fast_zlane = pick_z;
     }
   } catch (...) {
     cudaEventDestroy(e0);

@@ -180,6 +180,146 @@ kz_fwd(const typename reg::CT<T>::c* __restrict__ zbuf, int ngw, int nst, int pa
   }
 }
 
+// ------------------------------------------------------------ z sticks,
+// register lanes (FP32)
+// The z transforms of kz_bwd / kz_fwd with each stick's line held in the
+// registers of a group of lane::lanes_for(N2) lanes (fft_lane.cuh) instead
+// of a warp working through shared-memory stages.  A CTA takes the sticks of
+// rods_per_cta rods (2 rods_per_cta - 1 sticks, or 2 rods_per_cta) for one
+// band pair, one lane group per stick.
+//
+// Backward: lane t of a group loads the stick's values at z = t + T k
+// straight from the two bands' coefficients, transforms, and stores its
+// outputs z = k2 + M bitrev(t) to the sticks: for each k2 a warp's 8 groups
+// write T runs of 8 consecutive sticks.  No shared memory but the twiddles.
+template <int N2, int MINB>
+__global__ void __launch_bounds__(256, MINB)
+kz_bwd_lane(const double2* __restrict__ c, int ngw, int nst, int pair0, DeviceSticks g,
+            const double2* __restrict__ twz, float2* __restrict__ zbuf, int rods_per_cta) {
+  using C = float2;
+  constexpr int T = lane::lanes_for(N2), M = N2 / T;
+  static_assert(T > 0, "no register plan for this length");
+  __shared__ C tw[N2];
+  const int r0 = blockIdx.x * rods_per_cta;
+  const int r1 = min(g.nrods, r0 + rods_per_cta);
+  const int s0 = (r0 == 0) ? 0 : 2 * r0 - 1;
+  const int nl = (2 * r1 - 1) - s0;
+  const int pl = blockIdx.y;
+  const int b1 = 2 * (pair0 + pl);
+  const double2* c1 = c + (size_t)b1 * ngw;
+  const double2* c2 = (b1 + 1 < nst) ? c + (size_t)(b1 + 1) * ngw : nullptr;
+  load_tw(tw, twz, N2);
+  __syncthreads();
+  const int t = threadIdx.x % T, mr = lane::bitrev(t, T);
+  constexpr int half = (N2 + 1) / 2;
+  C* out = zbuf + (size_t)pl * N2 * g.nvec;
+  // rounds uniform across the CTA, so that every lane takes part in the shuffles
+#pragma unroll 1
+  for (int base = 0; base < nl; base += blockDim.x / T) {
+    const int line = base + threadIdx.x / T;
+    const bool ok = line < nl;
+    const int s = s0 + (ok ? line : 0);
+    const int r = (s + 1) >> 1;
+    const int lmin = g.rod_lmin[r], size = g.rod_size[r], first = g.rod_first[r];
+    const bool rod0 = (r == 0);
+    const bool mstick = ((s & 1) == 0);   // the -G stick of a rod r > 0
+    C v[M];
+#pragma unroll
+    for (int k = 0; k < M; ++k) {
+      const int z = t + T * k;
+      const int lz = z < half ? z : z - N2;
+      const bool minus = rod0 ? (lz <= 0) : mstick;
+      const int l = minus ? -lz : lz;
+      double vx = 0.0, vy = 0.0;
+      if (ok && l >= lmin && l < lmin + size) {
+        const double2 p = c1[first + (l - lmin)];
+        const double2 q = c2 ? c2[first + (l - lmin)] : make_double2(0.0, 0.0);
+        if (!minus) { vx = p.x - q.y; vy = p.y + q.x; }
+        else        { vx = p.x + q.y; vy = q.x - p.y; }
+      }
+      v[k] = cmk<C>(vx, vy);
+    }
+    lane::line_n2r<T, M, +1>(v, t, tw);
+    if (ok) {
+#pragma unroll
+      for (int k2 = 0; k2 < M; ++k2) out[(size_t)(k2 + M * mr) * g.nvec + s] = v[k2];
+    }
+  }
+}
+
+// Forward: lane t loads z = k2 + M bitrev(t) of its stick (the distribution
+// the backward kernel stored), transforms back to natural order, and puts the
+// line into shared memory, from which one warp per rod unpacks the pair and
+// adds the kinetic term exactly as kz_fwd does.
+template <int N2>
+__global__ void __launch_bounds__(256)
+kz_fwd_lane(const float2* __restrict__ zbuf, int ngw, int nst, int pair0, DeviceSticks g,
+            const double2* __restrict__ twz, double scale, const double2* __restrict__ c,
+            const double* __restrict__ g2, double2* __restrict__ hc, int rods_per_cta) {
+  using C = float2;
+  constexpr int T = lane::lanes_for(N2), M = N2 / T;
+  constexpr int LD = pitch(N2);
+  static_assert(T > 0, "no register plan for this length");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  C* lines = tw + N2;
+  const int r0 = blockIdx.x * rods_per_cta;
+  const int r1 = min(g.nrods, r0 + rods_per_cta);
+  const int s0 = (r0 == 0) ? 0 : 2 * r0 - 1;
+  const int nl = (2 * r1 - 1) - s0;
+  const int pl = blockIdx.y;
+  const int b1 = 2 * (pair0 + pl);
+  const bool two = (b1 + 1 < nst);
+  load_tw(tw, twz, N2);
+  __syncthreads();
+  const int t = threadIdx.x % T, mr = lane::bitrev(t, T);
+  const C* in = zbuf + (size_t)pl * N2 * g.nvec;
+#pragma unroll 1
+  for (int base = 0; base < nl; base += blockDim.x / T) {
+    const int line = base + threadIdx.x / T;
+    const bool ok = line < nl;
+    const int s = s0 + (ok ? line : 0);
+    C v[M];
+#pragma unroll
+    for (int k2 = 0; k2 < M; ++k2)
+      v[k2] = ok ? in[(size_t)(k2 + M * mr) * g.nvec + s] : cmk<C>(0.0, 0.0);
+    lane::line_r2n<T, M, -1>(v, t, tw);
+    if (ok) {
+      C* buf = lines + line * LD;
+#pragma unroll
+      for (int k = 0; k < M; ++k) buf[t + T * k] = v[k];
+    }
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int r = r0 + warp; r < r1; r += nw) {
+    const int lmin = g.rod_lmin[r], size = g.rod_size[r], first = g.rod_first[r];
+    const int sp = (r == 0) ? 0 : 2 * r - 1 - s0;
+    const int sm = (r == 0) ? 0 : 2 * r - s0;
+    for (int e = lane; e < size; e += 32) {
+      const int l = lmin + e;
+      const int zp = ((l % N2) + N2) % N2;
+      const int zm = ((-l % N2) + N2) % N2;
+      const C P = lines[sp * LD + zp];
+      const C Mv = lines[sm * LD + zm];
+      // c1 = (Z(G) + conj Z(-G))/2, c2 = -i (Z(G) - conj Z(-G))/2
+      const double px = P.x, py = P.y, mx = Mv.x, my = Mv.y;
+      const double c1x = 0.5 * (px + mx) * scale, c1y = 0.5 * (py - my) * scale;
+      const double c2x = 0.5 * (py + my) * scale, c2y = 0.5 * (mx - px) * scale;
+      const int ig = first + e;
+      const double kin = 0.5 * g2[ig];
+      const size_t i1 = (size_t)b1 * ngw + ig;
+      const double2 a = c[i1];
+      hc[i1] = make_double2(kin * a.x + c1x, kin * a.y + c1y);
+      if (two) {
+        const size_t i2 = i1 + ngw;
+        const double2 b = c[i2];
+        hc[i2] = make_double2(kin * b.x + c2x, kin * b.y + c2y);
+      }
+    }
+  }
+}
+
 // ------------------------------------------------------------ xy plane
 enum { XY_DENSITY = 0, XY_VPSI = 1 };
 
@@ -1240,6 +1380,9 @@ struct StagedArgs {
   int density_chunks;      // CTAs per plane in the density pass
   float2* psir;            // DENSITY: store psi(r) here; VPSI: read it (skip the backward)
   int fwd_pairs_per_cta;   // VPSI from psi(r): band pairs per CTA of kxy_lane_fwd
+  int zlane;               // FP32 z sticks in register lanes: 0 off; 1 both directions
+                           // (backward capped for 2 CTAs per SM); 2 both, uncapped; 3
+                           // forward only
 };
 
 template <typename T, int N, int SH>
@@ -1389,12 +1532,28 @@ void run_cubic(Context& ctx, const StagedArgs& a) {
   constexpr bool LANE = std::is_same<T, float>::value && lane::lanes_for(N) > 0;
   // psi(r) of these pairs is stored: the H*psi pass needs no backward
   const bool from_psir = LANE && a.op == XY_VPSI && a.psir && a.lane_shape >= 0;
-  allow_smem(kz_bwd<T, N>, zs);
+  // z sticks in register lanes: one lane group per stick of the CTA's rods
+  const bool zlane = LANE && a.zlane;
+  const int zl_threads = std::min(256, (lane::lanes_for(N) * 2 * rpc + 31) / 32 * 32);
   if (!from_psir) {
     ProfScope ps(ctx, "zfft_bwd");
-    kz_bwd<T, N><<<zgrid, kZThreads, zs, st>>>((const double2*)a.c, ngw, a.nst, a.pair0, g, a.twz,
-                                               (C*)a.zbuf, rpc);
-    QBX_LAUNCHED(ctx);
+    if constexpr (LANE) {
+      if (zlane && a.zlane != 3) {
+        if (a.zlane == 2)
+          kz_bwd_lane<N, 1><<<zgrid, zl_threads, 0, st>>>((const double2*)a.c, ngw, a.nst, a.pair0,
+                                                          g, a.twz, (float2*)a.zbuf, rpc);
+        else
+          kz_bwd_lane<N, 2><<<zgrid, zl_threads, 0, st>>>((const double2*)a.c, ngw, a.nst, a.pair0,
+                                                          g, a.twz, (float2*)a.zbuf, rpc);
+        QBX_LAUNCHED(ctx);
+      }
+    }
+    if (!zlane || a.zlane == 3) {
+      allow_smem(kz_bwd<T, N>, zs);
+      kz_bwd<T, N><<<zgrid, kZThreads, zs, st>>>((const double2*)a.c, ngw, a.nst, a.pair0, g,
+                                                 a.twz, (C*)a.zbuf, rpc);
+      QBX_LAUNCHED(ctx);
+    }
   }
   if constexpr (LANE) {
     if (a.lane_shape >= 0) {
@@ -1431,12 +1590,20 @@ void run_cubic(Context& ctx, const StagedArgs& a) {
           default: launch_lane_xy<N, XY_VPSI, 0>(ctx, a, a.npairs, 1); break;
         }
       }
-      allow_smem(kz_fwd<T, N>, zs);
       const double scale = 1.0 / ((double)N * N * N);
       ProfScope ps(ctx, "zfft_fwd");
-      kz_fwd<T, N><<<zgrid, kZThreads, zs, st>>>((const C*)a.zbuf, ngw, a.nst, a.pair0, g, a.twz,
-                                                 scale, (const double2*)a.c, ctx.d_g2_w,
-                                                 (double2*)a.hc, rpc);
+      if (zlane) {
+        const size_t zls = sizeof(float2) * ((size_t)N + (size_t)2 * rpc * pitch(N));
+        allow_smem(kz_fwd_lane<N>, zls);
+        kz_fwd_lane<N><<<zgrid, zl_threads, zls, st>>>((const float2*)a.zbuf, ngw, a.nst, a.pair0,
+                                                       g, a.twz, scale, (const double2*)a.c,
+                                                       ctx.d_g2_w, (double2*)a.hc, rpc);
+      } else {
+        allow_smem(kz_fwd<T, N>, zs);
+        kz_fwd<T, N><<<zgrid, kZThreads, zs, st>>>((const C*)a.zbuf, ngw, a.nst, a.pair0, g,
+                                                   a.twz, scale, (const double2*)a.c, ctx.d_g2_w,
+                                                   (double2*)a.hc, rpc);
+      }
       QBX_LAUNCHED(ctx);
       return;
     }

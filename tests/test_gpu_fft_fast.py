@@ -163,6 +163,27 @@ def test_density_queued_sticks_si512(graph, monkeypatch):
     b.close()
 
 
+@pytest.mark.parametrize("name", ["si8", "si64", "h2o32"])
+def test_z_sticks_in_register_lanes(name, monkeypatch):
+    """The z-stick transforms held in register lanes (kz_bwd_lane,
+    kz_fwd_lane) give the warp-per-stick kernels' density and H*psi (FP32,
+    2e-6 of the largest value) and total energy (1e-6 Ha per atom)."""
+    s = systems.get(name)
+    ctxs = []
+    for mode in ("1", "0"):
+        monkeypatch.setenv("QBX_ZLANE", mode)
+        ctxs.append(_ctx(s, capi.MIXED, True))
+    monkeypatch.delenv("QBX_ZLANE")
+    a, b = ctxs
+    ra, ha, ea = _run(a)
+    rb, hb, eb = _run(b)
+    np.testing.assert_allclose(ra, rb, rtol=0, atol=2e-6 * np.abs(rb).max())
+    np.testing.assert_allclose(ha, hb, rtol=0, atol=2e-6 * np.abs(hb).max())
+    assert abs(ea["etotal"] - eb["etotal"]) < 1e-6 * len(s.atoms)
+    a.close()
+    b.close()
+
+
 @pytest.mark.parametrize("ppc", ["3", "16"])
 def test_hpsi_from_psi_r_pairs_per_cta(ppc, monkeypatch):
     """The H*psi plane kernel from the stored psi(r) with several band pairs
