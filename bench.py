@@ -157,7 +157,7 @@ def run_reference_arm(args):
 # ------------------------------------------------------------ our arm
 def algorithmic_bytes_xy_vpsi(ctx, npairs: int, nlaunch: float, cbytes: int, vbytes: int) -> float:
     """Per H*psi, the H*psi plane kernel that starts from the stored psi(r)
-    (kxy_lane_fwd): every band pair's psi(r) read once (N c bytes), its sticks
+    (kxy_lane_fwd_staged): every band pair's psi(r) read once (N c bytes), its sticks
     written once (S c bytes), and the potential read once per launch
     (N v bytes)."""
     n0, n1, n2 = ctx.grid
@@ -258,8 +258,9 @@ def run_ours(args):
         pass
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     achieved = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9
-    roofline = {"kernel": "kxy_lane_fwd<140,140> (H*psi plane pass from the stored psi(r): "
-                          "times V, forward x and y register-lane FFTs)",
+    roofline = {"kernel": "kxy_lane_fwd_staged<140,140> (H*psi plane pass from the stored "
+                          "psi(r), rows staged by cp.async: times V, forward x and y "
+                          "register-lane FFTs)",
                 "bound": "hbm",
                 "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                 "frac": achieved / hbm_peak,

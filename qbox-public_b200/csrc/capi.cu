@@ -516,6 +516,7 @@ int qbx_set_cell(qbx_context* h, const double cell[9], double ecut, int nst, con
         c.fast_density_lane_shape = (std::atoi(e) == 3 || std::atoi(e) >= 5) && std::atoi(e) <= 8
                                         ? std::atoi(e) : 2;
       if (const char* e = std::getenv("QBX_PSIR")) c.psir_mode = std::atoi(e) != 0 ? 1 : 0;
+      if (const char* e = std::getenv("QBX_FWD_STAGED")) c.fast_fwd_staged = std::atoi(e) != 0 ? 1 : 0;
       if (const char* e = std::getenv("QBX_ZLANE")) c.fast_zlane = std::max(0, std::min(3, std::atoi(e)));
       if (const char* e = std::getenv("QBX_FWD_PAIRS_PER_CTA"))
         c.fast_fwd_ppc = std::max(1, std::min(64, std::atoi(e)));

@@ -783,6 +783,7 @@ static bool staged_fast(Context& ctx, int op, const double* c, const double* v, 
   a.density_chunks = ctx.fast_chunks;
   a.fwd_pairs_per_cta = ctx.fast_fwd_ppc;
   a.zlane = ctx.fast_zlane;
+  a.fwd_staged = ctx.fast_fwd_staged;
   a.v = v;
   a.psir = nullptr;
   if (op == OP_DENSITY) {

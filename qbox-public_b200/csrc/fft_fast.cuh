@@ -66,6 +66,16 @@ __device__ __forceinline__ void load_tw(C* dst, const double2* src, int n) {
 
 __host__ __device__ constexpr int pitch(int n) { return (n % 2 == 0) ? n + 1 : n; }
 
+// cp.async: asynchronous copies from global into shared memory, completed by
+// cp_async_wait_all (this thread's copies) and made visible to the CTA by a
+// barrier after it
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // ------------------------------------------------------------ z backward
 template <typename T, int N2>
 __global__ void __launch_bounds__(kZThreads)
@@ -598,9 +608,129 @@ kxy_lane_fwd(float2* __restrict__ zbuf, DeviceSticks g, const double2* __restric
   }
 }
 
+// The same H*psi pass with each round of x rows (blockDim/T rows of psi(r)
+// and of V(r)) staged in shared memory by cp.async: while a round's line
+// transforms run from registers, the next round's rows (or the next band
+// pair's first rows) stream in, so the loads of psi(r) no longer stall the
+// transforms.  One CTA per SM (at 140^3 the tables, the column tile and a
+// 72-row stage take 197 080 bytes).
+template <int N0, int N1>
+__host__ size_t xyfs_smem_bytes(int ncol, int rows) {
+  return sizeof(float2) * ((size_t)N0 + N1 + (size_t)ncol * pitch(N1)) + sizeof(int) * (size_t)N0 +
+         (sizeof(float2) + sizeof(float)) * (size_t)N0 * rows;
+}
+
+template <int N0, int N1>
+__global__ void __launch_bounds__(288, 1)
+kxy_lane_fwd_staged(float2* __restrict__ zbuf, DeviceSticks g, const double2* __restrict__ twx_g,
+                    const double2* __restrict__ twy_g, const float* __restrict__ v,
+                    const float2* __restrict__ psir, int pair0, int npairs, int pairs_per_cta) {
+  using C = float2;
+  constexpr int LD = pitch(N1);
+  constexpr int TY = lane::lanes_for(N1), MY = N1 / TY;
+  constexpr int TX = lane::lanes_for(N0), MX = N0 / TX;
+  static_assert(TY > 0 && TX > 0, "no register plan for this length");
+  static_assert((N0 * sizeof(float)) % 16 == 0, "rows of V(r) must be whole 16-byte chunks");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int ncol = g.ncol, nvec = g.nvec;
+  const int sx = blockDim.x / TX;                 // rows per round
+  C* twx = reinterpret_cast<C*>(smem_raw);
+  C* twy = twx + N0;
+  C* Sp = twy + N1;                               // staged psi(r) rows: sx x N0
+  float* Sv = reinterpret_cast<float*>(Sp + (size_t)sx * N0);   // staged V rows
+  C* P = reinterpret_cast<C*>(Sv + (size_t)sx * N0);
+  int* xmap = reinterpret_cast<int*>(P + (size_t)ncol * LD);
+  const int z = blockIdx.x;
+  const int pbeg = blockIdx.y * pairs_per_cta;
+  const int pend = min(npairs, pbeg + pairs_per_cta);
+  constexpr size_t kPlane = (size_t)N1 * N0;
+  constexpr int kChunkP = N0 * (int)sizeof(C) / 16, kChunkV = N0 * (int)sizeof(float) / 16;
+  // rows y0 .. y0+sx-1 of pair pl into the stage (16-byte chunks)
+  auto stage = [&](int pl, int y0) {
+    const int nr = min(sx, N1 - y0);
+    const char* gp = reinterpret_cast<const char*>(psir + ((size_t)(pair0 + pl) * g.n2 + z) * kPlane +
+                                                   (size_t)y0 * N0);
+    const char* gv = reinterpret_cast<const char*>(v + ((size_t)z * N1 + y0) * N0);
+    char* sp = reinterpret_cast<char*>(Sp);
+    char* sv = reinterpret_cast<char*>(Sv);
+    for (int i = threadIdx.x; i < nr * kChunkP; i += blockDim.x) {
+      const unsigned s = (unsigned)__cvta_generic_to_shared(sp + 16 * (size_t)i);
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gp + 16 * (size_t)i)
+                   : "memory");
+    }
+    for (int i = threadIdx.x; i < nr * kChunkV; i += blockDim.x) {
+      const unsigned s = (unsigned)__cvta_generic_to_shared(sv + 16 * (size_t)i);
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gv + 16 * (size_t)i)
+                   : "memory");
+    }
+    cp_async_commit();
+  };
+  if (pbeg < pend) stage(pbeg, 0);
+  load_tw(twx, twx_g, N0);
+  load_tw(twy, twy_g, N1);
+  for (int x = threadIdx.x; x < N0; x += blockDim.x) xmap[x] = -1;
+  __syncthreads();
+  for (int cidx = threadIdx.x; cidx < ncol; cidx += blockDim.x) xmap[g.col_x[cidx]] = cidx;
+  const int ty = threadIdx.x % TY, gy = threadIdx.x / TY, sy = blockDim.x / TY;
+  const int tx = threadIdx.x % TX, gx = threadIdx.x / TX;
+  const int mry = lane::bitrev(ty, TY), mrx = lane::bitrev(tx, TX);
+#pragma unroll 1
+  for (int pl = pbeg; pl < pend; ++pl) {
+    C* zp = zbuf + ((size_t)pl * g.n2 + z) * nvec;
+#pragma unroll 1
+    for (int y0 = 0; y0 < N1; y0 += sx) {
+      cp_async_wait_all();
+      __syncthreads();   // the round is staged; P and xmap are ready
+      const int y = y0 + gx;
+      const bool ok = y < N1;
+      C val[MX];
+#pragma unroll
+      for (int k = 0; k < MX; ++k) {
+        const C p = ok ? Sp[gx * N0 + tx + TX * k] : cmk<C>(0.0, 0.0);
+        const float vv = ok ? Sv[gx * N0 + MX * mrx + k] : 0.f;
+        val[k] = cmk<C>(p.x * vv, p.y * vv);
+      }
+      __syncthreads();   // the stage is free: queue the next round under this one's transforms
+      if (y0 + sx < N1) stage(pl, y0 + sx);
+      else if (pl + 1 < pend) stage(pl + 1, 0);
+      lane::line_r2n<TX, MX, -1>(val, tx, twx);
+      if (ok) {
+        int txh = tx;
+        asm volatile("" : "+r"(txh));
+#pragma unroll
+        for (int k = 0; k < MX; ++k) {
+          const int cidx = xmap[txh + TX * k];
+          if (cidx >= 0) P[cidx * LD + y] = val[k];
+        }
+      }
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int base = 0; base < ncol; base += sy) {
+      const int cidx = base + gy;
+      const bool ok = cidx < ncol;
+      const C* col = P + (ok ? cidx : 0) * LD;
+      C val[MY];
+#pragma unroll
+      for (int k2 = 0; k2 < MY; ++k2) val[k2] = ok ? col[k2 + MY * mry] : cmk<C>(0.0, 0.0);
+      lane::line_r2n<TY, MY, -1>(val, ty, twy);
+      if (ok) {
+        const int* cm = g.colmap + (size_t)cidx * N1;
+#pragma unroll
+        for (int k = 0; k < MY; ++k) {
+          const int s = __ldg(cm + ty + TY * k);
+          if (s >= 0) zp[s] = val[k];
+        }
+      }
+    }
+  }
+  cp_async_wait_all();
+}
+
 template <int N0, int N1, int OP, int SHAPE>
 __global__ void __launch_bounds__(lane_threads(SHAPE), lane_minblocks(SHAPE))
-kxy_lane(float2* __restrict__ zbuf, int npairs, int pairs_per_cta, DeviceSticks g,
+kxy_lane(
+float2* __restrict__ zbuf, int npairs, int pairs_per_cta, DeviceSticks g,
          const double2* __restrict__ twx_g, const double2* __restrict__ twy_g,
          const float* __restrict__ v, double* __restrict__ rho, const double* __restrict__ w,
          int pair0, int nst, float2* __restrict__ psir) {
@@ -957,12 +1087,6 @@ kxy_lane_dmap(const float2* __restrict__ zbuf, int npairs, int pairs_per_cta, De
 // take 227 840 of the 232 448 bytes a CTA may hold.
 constexpr int kDqSticks = 16;
 
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 template <int N0, int N1>
 __host__ size_t xydq_smem_bytes(int ncol) {
@@ -1380,6 +1504,7 @@ struct StagedArgs {
   int density_chunks;      // CTAs per plane in the density pass
   float2* psir;            // DENSITY: store psi(r) here; VPSI: read it (skip the backward)
   int fwd_pairs_per_cta;   // VPSI from psi(r): band pairs per CTA of kxy_lane_fwd
+  int fwd_staged;          // VPSI from psi(r): rounds of rows staged by cp.async
   int zlane;               // FP32 z sticks in register lanes: 0 off; 1 both directions
                            // (backward capped for 2 CTAs per SM); 2 both, uncapped; 3
                            // forward only
@@ -1437,6 +1562,31 @@ void launch_lane_fwd(Context& ctx, const StagedArgs& a) {
   kxy_lane_fwd<N, N><<<dim3(N, chunks), threads, sm, ctx.stream>>>(
       (float2*)a.zbuf, g, a.twx, a.twy, (const float*)a.v, a.psir, a.pair0, a.npairs, ppc);
   QBX_LAUNCHED(ctx);
+}
+
+// false (nothing launched) when the length has no 16-byte row chunks or the
+// stage does not fit a CTA's shared memory
+template <int N>
+bool launch_lane_fwd_staged(Context& ctx, const StagedArgs& a) {
+  if constexpr (N % 4 != 0) {
+    return false;
+  } else {
+    const DeviceSticks& g = ctx.dws;
+    const int want = (g.ncol * lane::lanes_for(N) + 31) / 32 * 32;
+    const int threads = std::max(64, std::min(288, want));
+    const size_t sm = xyfs_smem_bytes<N, N>(g.ncol, threads / lane::lanes_for(N));
+    int dev = 0, optin = 0;
+    QBX_CUDA(cudaGetDevice(&dev));
+    QBX_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    if (sm > (size_t)optin) return false;
+    allow_smem(kxy_lane_fwd_staged<N, N>, sm);
+    const int ppc = std::max(1, std::min(a.npairs, a.fwd_pairs_per_cta));
+    const int chunks = (a.npairs + ppc - 1) / ppc;
+    kxy_lane_fwd_staged<N, N><<<dim3(N, chunks), threads, sm, ctx.stream>>>(
+        (float2*)a.zbuf, g, a.twx, a.twy, (const float*)a.v, a.psir, a.pair0, a.npairs, ppc);
+    QBX_LAUNCHED(ctx);
+    return true;
+  }
 }
 
 template <int N>
@@ -1579,7 +1729,9 @@ void run_cubic(Context& ctx, const StagedArgs& a) {
       }
       {
         ProfScope ps(ctx, "xy_vpsi");
-        if (from_psir) launch_lane_fwd<N>(ctx, a);
+        if (from_psir) {
+          if (!a.fwd_staged || !launch_lane_fwd_staged<N>(ctx, a)) launch_lane_fwd<N>(ctx, a);
+        }
         else switch (a.lane_shape) {
           case 5: launch_lane_map<N, 2>(ctx, a); break;
           case 6: launch_lane_map<N, 1>(ctx, a); break;

@@ -429,6 +429,7 @@ struct Context {
                                     // 8 next pair's sticks queued with cp.async)
   int fast_chunks = 8;          // CTAs per plane in the density pass
   int fast_fwd_ppc = 2;         // band pairs per CTA of the H*psi plane kernel from psi(r)
+  int fast_fwd_staged = 1;      // that kernel with its rows staged by cp.async
   int fast_zlane = 1;           // FP32 z sticks in register lanes (0: warp per stick;
                                 // 2: backward uncapped; 3: forward only)
   bool fast_fft = true;         // use the specialised kernels when compiled

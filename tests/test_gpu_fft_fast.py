@@ -184,19 +184,24 @@ def test_z_sticks_in_register_lanes(name, monkeypatch):
     b.close()
 
 
+@pytest.mark.parametrize("staged", ["0", "1"])
 @pytest.mark.parametrize("ppc", ["3", "16"])
-def test_hpsi_from_psi_r_pairs_per_cta(ppc, monkeypatch):
+@pytest.mark.parametrize("name", ["si64", "si512_32"])
+def test_hpsi_from_psi_r_pairs_per_cta(name, ppc, staged, monkeypatch):
     """The H*psi plane kernel from the stored psi(r) with several band pairs
     per CTA (3: a launch's 16 pairs end in a partial CTA; 16: one CTA per
-    plane), each prefetching the next pair's psi(r) plane into L2, gives the
+    plane), each prefetching the next pair's psi(r) plane into L2 or (staged)
+    copying its rounds of rows into shared memory with cp.async, gives the
     one-pair-per-CTA kernel's step: energies to 1e-12 relative and the
     coefficients after two steps to 1e-12."""
-    s = systems.si64()
+    s = systems.si64() if name == "si64" else systems.si512().band_sample(32)
     ctxs = []
-    for mode in (ppc, "1"):
+    for mode, st in ((ppc, staged), ("1", "0")):
         monkeypatch.setenv("QBX_FWD_PAIRS_PER_CTA", mode)
+        monkeypatch.setenv("QBX_FWD_STAGED", st)
         ctxs.append(_ctx(s, capi.MIXED, True))
     monkeypatch.delenv("QBX_FWD_PAIRS_PER_CTA")
+    monkeypatch.delenv("QBX_FWD_STAGED")
     a, b = ctxs
     for _ in range(2):
         ea, eb = a.scf_step(), b.scf_step()
