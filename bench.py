@@ -266,9 +266,9 @@ def run_ours(args):
                 "frac": achieved / hbm_peak,
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                 # DRAM bytes per launch: the ncu capture of this kernel
-                # (profiles/kxy_lane_fwd_si512.md: 424.0 MB for a 16-pair
-                # launch) scaled by the band pairs of this run's launches
-                "traffic": 424.0e6 / 16.0 * (npairs / max(1e-9, n_xy)),
+                # (profiles/kxy_lane_fwd_staged_si512.md: 420.5 MB for a
+                # 16-pair launch) scaled by the band pairs of this run's launches
+                "traffic": 420.5e6 / 16.0 * (npairs / max(1e-9, n_xy)),
                 "algorithmic_bytes_per_launch": per_launch_bytes,
                 "launch_ms": per_launch_ms}
     # GEMM share (FP64 cuBLAS in this build) against the dense FP64 rate
@@ -306,6 +306,20 @@ def run_ours(args):
     pin_in.numpy()[:] = cur.view(np.float64).ravel()
     ne2e = max(2, min(args.steps, 5))
     ms_e2e, _, _ = timed(mix, ne2e, e2e_bufs=(pin_in.numpy(), pin_out.numpy()))
+    # the host link alone: one copy of the same bytes each way (the end-to-end
+    # step cannot be faster than the slower direction)
+    link = {}
+    dev_buf = torch.empty(nb // 8, dtype=torch.float64, device=f"cuda:{dev}")
+    for name, (dst, src) in (("h2d_gbs", (dev_buf, pin_in)), ("d2h_gbs", (pin_out, dev_buf))):
+        c0 = torch.cuda.Event(enable_timing=True)
+        c1 = torch.cuda.Event(enable_timing=True)
+        dst.copy_(src, non_blocking=True)
+        c0.record()
+        dst.copy_(src, non_blocking=True)
+        c1.record()
+        c1.synchronize()
+        link[name] = nb / (c0.elapsed_time(c1) * 1e-3) / 1e9
+    del dev_buf
 
     # ---- molecular dynamics of the same cell (dt = 20 a.u., forces every
     # ionic step, captured electronic steps): ms per ionic step
@@ -454,7 +468,9 @@ def run_ours(args):
             "fft_tuning": tuning_mix.strip().splitlines()[-1],
             "cpu_baseline": cpu,
             "e2e": {"value": ms_e2e, "unit": "ms", "h2d_bytes_per_step": nb,
-                    "d2h_bytes_per_step": nb},
+                    "d2h_bytes_per_step": nb,
+                    "host_link": {k: round(v, 1) for k, v in link.items()},
+                    "copy_floor_ms": nb / (min(link.values()) * 1e9) * 1e3},
             "gpu_launches": launches,
             "clocks": clk,
         }
