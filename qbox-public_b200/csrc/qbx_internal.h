@@ -659,13 +659,15 @@ void md_run(Context& c, int niter, int nitscf, double dt, const double* mass_amu
 void split_bf16(Context& ctx, const double* x, size_t n, void* hi, void* lo);
 void overlap_diag_f64(Context& ctx, const double* c, int K, int n, double* S);
 // C = alpha * op(A) op(B) + beta * C, C column-major with ld m
+// lower: only the tiles holding the lower triangle of a square C are
+// formed (the tcgen05 backend; the others form all of C)
 void split_gemm(Context& ctx, bool ta, bool tb, int m, int n, int k, double alpha,
                 const void* ahi, const void* alo, int lda, const void* bhi, const void* blo,
-                int ldb, double beta, double* C);
+                int ldb, double beta, double* C, bool lower = false);
 bool tc_gemm_supported(const Context& ctx, bool ta, bool tb, int m, int n, int k);
 void tc_split_gemm(Context& ctx, bool ta, bool tb, int m, int n, int k, double alpha,
                    const void* ahi, const void* alo, int lda, const void* bhi, const void* blo,
-                   int ldb, double beta, double* C);
+                   int ldb, double beta, double* C, bool lower = false);
 int tc_check_error(Context& ctx);   // nonzero if a tcgen05 GEMM wait ran out
 void split_bf16_2d(Context& ctx, const double* x, int rows, int cols, int ldx, void* hi, void* lo,
                    int ldp);

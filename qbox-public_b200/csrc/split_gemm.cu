@@ -113,9 +113,9 @@ static void cublas_split(Context& ctx, bool ta, bool tb, int m, int n, int k, co
 
 void split_gemm(Context& ctx, bool ta, bool tb, int m, int n, int k, double alpha,
                 const void* ahi, const void* alo, int lda, const void* bhi, const void* blo,
-                int ldb, double beta, double* C) {
+                int ldb, double beta, double* C, bool lower) {
   if (ctx.gemm_backend == 1 && tc_gemm_supported(ctx, ta, tb, m, n, k)) {
-    tc_split_gemm(ctx, ta, tb, m, n, k, alpha, ahi, alo, lda, bhi, blo, ldb, beta, C);
+    tc_split_gemm(ctx, ta, tb, m, n, k, alpha, ahi, alo, lda, bhi, blo, ldb, beta, C, lower);
     return;
   }
   float* D = (float*)ctx.d_acc32;

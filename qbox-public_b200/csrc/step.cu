@@ -29,8 +29,9 @@ static void overlap_cholesky(Context& ctx, const double* c, double* S, int statu
   const int n = ctx.nst, K = 2 * ctx.wb.ng;
   const double two = 2.0, zero = 0.0;
   if (split >= 0) {
+    // lower triangle only, as the FP64 path's syrk: potrf reads nothing else
     split_gemm(ctx, true, false, n, n, K, 2.0, ctx.cs_hi[split], ctx.cs_lo[split], ctx.ldp,
-               ctx.cs_hi[split], ctx.cs_lo[split], ctx.ldp, 0.0, S);
+               ctx.cs_hi[split], ctx.cs_lo[split], ctx.ldp, 0.0, S, true);
     launch_rank1_fix(ctx, S, n, c, K, c, K, n, n, -1.0, true);
     overlap_diag_f64(ctx, c, K, n, S);
   } else {

@@ -155,7 +155,14 @@ k_tc_split_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant
                 const __grid_constant__ CUtensorMap mb_hi, const __grid_constant__ CUtensorMap mb_lo,
                 int M, int N, int nkb, int kb_per_split, float* __restrict__ ws,
                 double* __restrict__ C, int ldc, double alpha, double beta,
-                int* __restrict__ err) {
+                int* __restrict__ err, int lower) {
+  // lower: a tile whose every column is right of its every row holds only
+  // the strict upper triangle and is not formed (the whole CTA leaves before
+  // it allocates anything)
+  {
+    const int tm0 = (ws ? blockIdx.x : blockIdx.y) * BM, tn0 = (ws ? blockIdx.y : blockIdx.x) * BN;
+    if (lower && tn0 >= tm0 + BM) return;
+  }
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint64_t* full = (uint64_t*)(base + STAGES * STAGE_BYTES);
@@ -370,14 +377,17 @@ static CUtensorMap kmajor_map(const void* ptr, int k, int cols, int ld, int kind
 }
 
 // out(col * ldc + row) = alpha * sum_s ws(s, col * M + row) + beta * out, in FP64
+// (lower: only the tiles the GEMM formed, those that meet the lower triangle)
 __global__ void k_reduce_splits2d(const float* __restrict__ ws, int nsplit, int M, int N,
-                                  double alpha, double beta, double* __restrict__ out, int ldc) {
+                                  double alpha, double beta, double* __restrict__ out, int ldc,
+                                  int lower) {
   const size_t n = (size_t)M * N;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
+    const size_t col = i / M, row = i - col * M;
+    if (lower && (col / tc::BN) * tc::BN >= (row / tc::BM) * tc::BM + tc::BM) continue;
     double s = 0.0;
     for (int z = 0; z < nsplit; z++) s += (double)ws[(size_t)z * n + i];
-    const size_t col = i / M, row = i - col * M;
     double* o = out + col * ldc + row;
     *o = alpha * s + (beta != 0.0 ? beta * *o : 0.0);
   }
@@ -395,7 +405,7 @@ bool tc_gemm_supported(const Context& ctx, bool ta, bool tb, int m, int n, int k
 // only when the output has too few tiles to fill the GPU.
 static void tc_gemm_tn(Context& ctx, int kind, int m, int n, int k, double alpha, const void* ahi,
                        const void* alo, int lda, const void* bhi, const void* blo, int ldb,
-                       double beta, double* C, int ldc) {
+                       double beta, double* C, int ldc, bool lower = false) {
   const size_t es = kind == tc::KIND_BF16 ? 2 : 4;
   QBX_REQUIRE(m > 0 && n > 0 && k > 0 && ldc >= m, 54, "bad tcgen05 GEMM shape");
   QBX_REQUIRE((lda * es) % 16 == 0 && (ldb * es) % 16 == 0, 54,
@@ -409,7 +419,9 @@ static void tc_gemm_tn(Context& ctx, int kind, int m, int n, int k, double alpha
   const int bk = tc::bk_of(kind);
   const int nkb = (k + bk - 1) / bk;
   const int tm = (m + tc::BM - 1) / tc::BM, tn = (n + tc::BN - 1) / tc::BN;
-  const int tiles = tm * tn;
+  QBX_REQUIRE(!lower || m == n, 54, "lower-triangle GEMM of a non-square output");
+  // tiles formed: with lower, those on or below the diagonal of tiles
+  const int tiles = lower ? tm * (tm + 1) / 2 : tm * tn;
   int sms = 148;
   QBX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device));
   // split K so that about two CTAs per SM are in flight; the partials (FP32)
@@ -437,27 +449,27 @@ static void tc_gemm_tn(Context& ctx, int kind, int m, int n, int k, double alpha
   if (kind == tc::KIND_BF16) {
     allow_smem(tc::k_tc_split_gemm<tc::KIND_BF16>, tc::SMEM_BYTES);
     tc::k_tc_split_gemm<tc::KIND_BF16><<<grid, tc::THREADS, tc::SMEM_BYTES, ctx.stream>>>(
-        mah, mal, mbh, mbl, m, n, nkb, kbps, ws, C, ldc, alpha, beta, err);
+        mah, mal, mbh, mbl, m, n, nkb, kbps, ws, C, ldc, alpha, beta, err, lower ? 1 : 0);
   } else {
     allow_smem(tc::k_tc_split_gemm<tc::KIND_TF32>, tc::SMEM_BYTES);
     tc::k_tc_split_gemm<tc::KIND_TF32><<<grid, tc::THREADS, tc::SMEM_BYTES, ctx.stream>>>(
-        mah, mal, mbh, mbl, m, n, nkb, kbps, ws, C, ldc, alpha, beta, err);
+        mah, mal, mbh, mbl, m, n, nkb, kbps, ws, C, ldc, alpha, beta, err, lower ? 1 : 0);
   }
   QBX_LAUNCHED(ctx);
   if (splits > 1) {
     const size_t nn = (size_t)m * n;
     const int nb = (int)std::min<size_t>((nn + 255) / 256, (size_t)sms * 16);
     k_reduce_splits2d<<<nb, 256, 0, ctx.stream>>>((const float*)ctx.d_tc_ws, splits, m, n, alpha,
-                                                  beta, C, ldc);
+                                                  beta, C, ldc, lower ? 1 : 0);
     QBX_LAUNCHED(ctx);
   }
 }
 
 void tc_split_gemm(Context& ctx, bool ta, bool tb, int m, int n, int k, double alpha,
                    const void* ahi, const void* alo, int lda, const void* bhi, const void* blo,
-                   int ldb, double beta, double* C) {
+                   int ldb, double beta, double* C, bool lower) {
   QBX_REQUIRE(tc_gemm_supported(ctx, ta, tb, m, n, k), 54, "shape not supported by tcgen05 GEMM");
-  tc_gemm_tn(ctx, tc::KIND_BF16, m, n, k, alpha, ahi, alo, lda, bhi, blo, ldb, beta, C, m);
+  tc_gemm_tn(ctx, tc::KIND_BF16, m, n, k, alpha, ahi, alo, lda, bhi, blo, ldb, beta, C, m, lower);
 }
 
 void tc_gemm_kind_tn(Context& ctx, int kind, int m, int n, int k, double alpha, const void* ahi,
