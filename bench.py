@@ -33,6 +33,11 @@ import tempfile
 import threading
 import time
 
+# The 32-system batch runs one stream per system: let the device give each its
+# own hardware queue (the default of 8 serialises streams onto shared queues).
+# Read once, when this process creates its CUDA context.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.join(ROOT, "qbox-public_b200")
 for p in (PKG, ROOT):
