@@ -338,11 +338,21 @@ __global__ void k_precondition(double2* __restrict__ hc, const double* __restric
   }
 }
 
-struct AndersonF {
-  const double2* f; const double2* fl; int ngw;
+// The preconditioned residual and the Anderson sums in one pass: dc = -K r
+// (as k_precondition) is written over the residual and, in the same visit,
+// enters <dc, dc - dc_last> and |dc - dc_last|^2 (weight 2 off G = 0, the
+// real view of the half sphere; src/PSDAWavefunctionStepper.cpp:129-179)
+struct PrecondAndersonF {
+  double2* hc; const double2* fl; const double* g2; const double* ekin; int ngw;
   __device__ void operator()(size_t i, double* a) const {
-    const int ig = (int)(i % (size_t)ngw);
-    const double2 x = f[i], y = fl[i];
+    const int b = (int)(i / ngw), ig = (int)(i - (size_t)b * ngw);
+    const double e = 0.5 * g2[ig];
+    const double en = ekin[b];
+    const double k = (e < en) ? 0.5 / en : 0.5 / e;
+    const double2 r = hc[i];
+    const double2 x = make_double2(-k * r.x, -k * r.y);
+    hc[i] = x;
+    const double2 y = fl[i];
     const double dx = x.x - y.x, dy = x.y - y.y;
     const double w = (ig == 0) ? 1.0 : 2.0;
     a[0] += w * (x.x * dx + x.y * dy);
@@ -386,12 +396,15 @@ __global__ void k_psda_update(double2* __restrict__ c, double2* __restrict__ c_l
 // Stepper.cpp:82-212): precondition, Anderson theta, step.
 void launch_psda_elementwise(Context& ctx) {
   const size_t n = (size_t)ctx.wb.ng * ctx.nst;
-  k_precondition<<<blocks_for(n), kThreads, 0, ctx.stream>>>((double2*)ctx.d_hc, ctx.d_g2_w,
-                                                              ctx.d_prec, ctx.wb.ng, n);
-  QBX_LAUNCHED(ctx);
-  if (ctx.extrapolate)
-    reduce<2>(ctx, AndersonF{(const double2*)ctx.d_hc, (const double2*)ctx.d_dc_last, ctx.wb.ng},
+  if (ctx.extrapolate) {
+    reduce<2>(ctx, PrecondAndersonF{(double2*)ctx.d_hc, (const double2*)ctx.d_dc_last,
+                                    ctx.d_g2_w, ctx.d_prec, ctx.wb.ng},
               n, SLOT_ANDERSON);
+  } else {
+    k_precondition<<<blocks_for(n), kThreads, 0, ctx.stream>>>((double2*)ctx.d_hc, ctx.d_g2_w,
+                                                                ctx.d_prec, ctx.wb.ng, n);
+    QBX_LAUNCHED(ctx);
+  }
   // theta is formed on the device from the two sums
   k_psda_update<<<blocks_for(n), kThreads, 0, ctx.stream>>>(
       (double2*)ctx.d_c, (double2*)ctx.d_c_last, (double2*)ctx.d_dc_last,
