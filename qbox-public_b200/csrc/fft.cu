@@ -1095,7 +1095,7 @@ void autotune_fft(Context& ctx, std::vector<std::pair<std::string, double>>* log
       for (int zl : {1, 0}) {
         if (zl == 0 && ctx.precision != MIXED) continue;
         if (ctx.precision == MIXED) ctx.fast_zlane = zl;
-        for (int r : {8, 16, 24}) {
+        for (int r : {8, 16, 24, 32}) {
           ctx.fast_rods = r;
           const double t = time_ms(vpsi);
           note("z lanes " + std::to_string(ctx.fast_zlane) + " rods per z CTA " + std::to_string(r), t);
