@@ -311,6 +311,74 @@ int qbx_set_gemm_backend(qbx_context* ctx, int backend);
 int qbx_split_gemm_tn(qbx_context* ctx, int m, int n, int k, const double* a,
                       const double* b, double* d, int backend);
 
+/* ---- The reference's classes on the caller's host arrays.
+ * A C++ caller that keeps Qbox's FourierTransform, SlaterDet and
+ * NonLocalPotential objects (their headers unchanged) implements their
+ * methods with these calls; coefficient arrays are ngw complex values per
+ * band, band after band, in the context's coefficient order (the caller's,
+ * when qbx_set_coeff_order was given); grids hold np0*np1*np2 values, x
+ * fastest (FourierTransform::index, src/FourierTransform.h:167-168). */
+
+/* FourierTransform(const Basis& basis, int np0, int np1, int np2)
+ * (src/FourierTransform.h:105-110, src/FourierTransform.cpp:97-114) on any
+ * basis: hkl holds the Miller index of each of the ngw coefficients in the
+ * caller's order; real_basis != 0 for a Gamma half sphere (each coefficient
+ * also stands for -G with the conjugate value).  The basis must fit in the
+ * grid as Basis::fits_in_grid requires (src/Basis.cpp:139-144), else error
+ * 12.  The transforms run on `device` as full-grid line FFTs; coefficients
+ * and grids cross the host link on every call. */
+typedef struct qbx_ft qbx_ft;
+int qbx_ft_create(qbx_ft** ft, int device, int ngw, const int* hkl, int real_basis, int np0,
+                  int np1, int np2);
+void qbx_ft_destroy(qbx_ft* ft);
+const char* qbx_ft_last_error(qbx_ft* ft);
+/* FourierTransform::backward(c, f) (src/FourierTransform.h:112,
+ * src/FourierTransform.cpp:159-170): f(r) = sum_G c(G) exp(iG.r) on the
+ * grid, -G with the conjugate on a real basis; unscaled. */
+int qbx_ft_backward(qbx_ft* ft, const double* c, double* f);
+/* FourierTransform::backward(c1, c2, f) (src/FourierTransform.h:117-118,
+ * src/FourierTransform.cpp:187-200): f = psi_1 + i psi_2 for two bands of a
+ * real basis (src/BasisMapping.cpp:666-700). */
+int qbx_ft_backward2(qbx_ft* ft, const double* c1, const double* c2, double* f);
+/* FourierTransform::forward(f, c) (src/FourierTransform.h:114,
+ * src/FourierTransform.cpp:147-157): c(G) = 1/N sum_r f(r) exp(-iG.r).  The
+ * reference overwrites f; here f is left as it was. */
+int qbx_ft_forward(qbx_ft* ft, double* f, double* c);
+/* FourierTransform::forward(f, c1, c2) (src/FourierTransform.h:120-121,
+ * src/FourierTransform.cpp:173-184): the two real functions of f = psi_1 +
+ * i psi_2 (src/BasisMapping.cpp:716-750); real basis only. */
+int qbx_ft_forward2(qbx_ft* ft, double* f, double* c1, double* c2);
+
+/* SlaterDet::compute_density(ft, weight, rho) (src/SlaterDet.h:66,
+ * src/SlaterDet.cpp:225-298) of the context's SlaterDet on the context's
+ * grid: rho[i] += weight * sum_n occ_n/Omega |psi_n(r_i)|^2, rho a HOST array
+ * of np0*np1*np2 doubles (the staged two-band transforms of the
+ * electronic step, in the context's precision). */
+int qbx_compute_density(qbx_context* ctx, double weight, double* rho);
+/* SlaterDet::rs_mul_add(ft, v, sdp) (src/SlaterDet.h:68,
+ * src/SlaterDet.cpp:410-477): sdp.c += FFT_fwd(v(r) FFT_bwd(c)) for every
+ * band; v a HOST array of np0*np1*np2 doubles, dc the HOST coefficients of
+ * sdp (nst bands), added into. */
+int qbx_rs_mul_add(qbx_context* ctx, const double* v, double* dc);
+/* NonLocalPotential::energy(compute_hpsi, dsd, compute_forces, fion,
+ * compute_stress, sigma_enl) (src/NonLocalPotential.h:65-67,
+ * src/NonLocalPotential.cpp:1258-2069) alone: E_nl into *enl; with
+ * compute_hpsi the nonlocal H*C added into dc (HOST, nst bands); with
+ * compute_forces the nonlocal forces (3 per atom, species-major) written to
+ * fion; with compute_stress sigma_enl[6] (xx yy zz xy yz xz). */
+int qbx_nonlocal_energy(qbx_context* ctx, int compute_hpsi, double* dc, int compute_forces,
+                        double* fion, int compute_stress, double* sigma_enl, double* enl);
+/* SlaterDet::ortho_align(const SlaterDet& sd) (src/SlaterDet.h:76,
+ * src/SlaterDet.cpp:768-876): orthonormalises the context's C and aligns it
+ * with sd, given as HOST coefficients (nst bands).  sd is held in the
+ * stepper's last-step buffer, so the PSDA history restarts (as after
+ * qbx_set_coeffs). */
+int qbx_ortho_align(qbx_context* ctx, const double* c_sd);
+/* SlaterDet::dot(const SlaterDet& sd) (src/SlaterDet.h:77,
+ * src/SlaterDet.cpp:1122-1153) at Gamma: tr(C^T C_sd) over the real view,
+ * +G and -G once each, *d = 2 sum - sum of the G=0 terms. */
+int qbx_dot(qbx_context* ctx, const double* c_sd, double* d);
+
 /* Size of the device array behind qbx_density_static: 32 MiB. */
 #define QBX_STATIC_SCRATCH_BYTES ((size_t)32 << 20)
 
@@ -325,14 +393,17 @@ int qbx_split_gemm_tn(qbx_context* ctx, int m, int n, int k, const double* a,
  * occupations, or NULL for 2 per band.  The z-stick scratch, twiddle and
  * weight tables come from one static device array of QBX_STATIC_SCRATCH_BYTES
  * that every GPU loading the library holds until exit; the call allocates
- * nothing and returns error 62 when one band pair's z-sticks do not fit:
+ * nothing.  Error 62 covers every limit of that array, and the message names
+ * which one was hit: (1) an FFT length above 4096; (2) the three twiddle
+ * tables and the nst band weights above 1 MiB (about 130 000 bands at the
+ * grid lengths used here); (3) one band pair's z-sticks above 31 MiB:
  * np2 * (2*nrods-1) complex values per pair (FP32 in the mixed precision,
- * FP64 otherwise) must fit in 31 MiB, about 4 M values in FP32.  The first
- * call on a device looks up the array's device address
- * (cudaGetSymbolAddress), so make it before any stream capture.  All calls
- * share the array and it keeps the last call's contents; calls that overlap
- * on one GPU race.  Runs on the context's stream and returns after it has
- * finished. */
+ * FP64 otherwise), about 4 M values in FP32.  Every call looks up the
+ * array's address in the CUDA context current on the calling thread
+ * (cudaGetSymbolAddress, which allocates nothing).  All calls share the
+ * array and it keeps the last call's contents; calls that overlap on one
+ * GPU race.  Runs on the context's stream and synchronizes that stream
+ * before returning. */
 int qbx_density_static(qbx_context* ctx, const double* d_c, int nst,
                        const double* occ, double* d_rho);
 

@@ -85,7 +85,7 @@ void free_cell(Context& c) {
                      &c.d_exc, &c.d_vx2, &c.d_grad, &c.d_rhog, &c.d_vion, &c.d_rhops,
                      &c.d_vtmp_g, &c.d_vtmp_g2, &c.d_nn, &c.d_nn2, &c.d_nn3, &c.d_nn4,
                      &c.d_solver_work, &c.d_red, &c.d_scalars, &c.d_prec, &c.d_jd_h,
-                     &c.d_jd_w, &c.d_jd_work, &c.d_wfv};
+                     &c.d_jd_w, &c.d_jd_work, &c.d_wfv, &c.d_xsd, &c.d_xgrid};
   for (double** b : bufs) dfree(*b);
   dfree(c.d_ipiv);
   dfree(c.d_info);
@@ -350,6 +350,9 @@ int qbx_create(qbx_context** out, int device, int precision) {
   // leave C orthonormal only to ~1e-5); the H*C updates use BF16 splits,
   // ~20% faster, whose ~1e-5 relative error only enters the step direction
   if (const char* e = std::getenv("QBX_TALL_KIND")) h->c.tall_kind = std::atoi(e) == 0 ? 0 : 1;
+  if (const char* e = std::getenv("QBX_TC_CHUNK")) h->c.tc_chunk = std::max(1, std::min(64, std::atoi(e)));
+  if (const char* e = std::getenv("QBX_TC_EPW")) h->c.tc_epw = std::atoi(e) == 4 ? 4 : 8;
+  if (const char* e = std::getenv("QBX_TC_CORR_MUL")) h->c.tc_corr_mul = std::max(0, std::min(64, std::atoi(e)));
   if (const char* e = std::getenv("QBX_TALL_KIND_HC")) h->c.tall_kind_hc = std::atoi(e) == 1 ? 1 : 0;
   // batches of captured steps: one graph launch per context on its own
   // stream (default; 9.8 ms for 32 small systems) or one graph with every
@@ -1277,6 +1280,182 @@ int qbx_ft_backward_pair(qbx_context* h, int n1, int n2, double* f) {
     const double* c2 = n2 >= 0 ? c.d_c + 2 * (size_t)n2 * c.wb.ng : nullptr;
     wb_backward_pair(c, c1, c2, c.d_grad);   // complex grid in the first 2N of d_grad
     QBX_CUDA(cudaMemcpyAsync(f, c.d_grad, 2 * N * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    QBX_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+// ---------------------------------------------- class-level entry points
+// SlaterDet and NonLocalPotential operations on the caller's host arrays
+// (coefficients in the caller's row order when qbx_set_coeff_order was
+// given, grids x fastest), for callers that keep the reference's classes.
+
+namespace {
+
+__global__ void k_sub_kinetic(double2* __restrict__ hc, const double2* __restrict__ c,
+                              const double* __restrict__ g2, int ng, int nst) {
+  const size_t n = (size_t)ng * nst;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const double k = 0.5 * g2[t % ng];
+    const double2 a = c[t];
+    hc[t].x -= k * a.x;
+    hc[t].y -= k * a.y;
+  }
+}
+
+// d = 2 sum_n sum_i a_n[i] b_n[i] - sum_n a_n[0] b_n[0] over the real view
+// (2 ng doubles per band), the G = 0 row at internal index 0
+__global__ void k_sd_dot(const double* __restrict__ a, const double* __restrict__ b, int ng,
+                         int nst, double* __restrict__ out) {
+  __shared__ double sh[32];
+  const size_t n = 2 * (size_t)ng * nst;
+  double s = 0.0;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const size_t i = t % (2 * (size_t)ng);
+    const double p = a[t] * b[t];
+    s += i == 0 ? p : 2.0 * p;   // the first real element of each band once
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += sh[w];
+    atomicAdd(out, t);
+  }
+}
+
+double* lazy_wf(Context& c, double*& p) {
+  if (!p) p = dalloc<double>(2 * (size_t)c.wb.ng * c.nst);
+  return p;
+}
+
+// host (caller order) -> device (internal order)
+void upload_wf(qbx_context* h, const double* src, double* dst) {
+  Context& c = h->c;
+  const size_t wf = 2 * (size_t)c.wb.ng * c.nst;
+  if (h->d_perm) {
+    QBX_CUDA(cudaMemcpyAsync(c.d_ctmp, src, wf * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    k_permute<<<1184, 256, 0, c.stream>>>((const double2*)c.d_ctmp, h->d_perm, c.wb.ng, c.nst, 1,
+                                          (double2*)dst);
+    QBX_LAUNCHED(c);
+  } else {
+    QBX_CUDA(cudaMemcpyAsync(dst, src, wf * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+  }
+}
+
+// device (internal order) -> host vector (caller order)
+std::vector<double> download_wf(qbx_context* h, const double* dsrc) {
+  Context& c = h->c;
+  const size_t wf = 2 * (size_t)c.wb.ng * c.nst;
+  std::vector<double> out(wf);
+  const double* src = dsrc;
+  if (h->d_perm) {
+    k_permute<<<1184, 256, 0, c.stream>>>((const double2*)dsrc, h->d_perm, c.wb.ng, c.nst, 0,
+                                          (double2*)c.d_ctmp);
+    QBX_LAUNCHED(c);
+    src = c.d_ctmp;
+  }
+  QBX_CUDA(cudaMemcpyAsync(out.data(), src, wf * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  QBX_CUDA(cudaStreamSynchronize(c.stream));
+  return out;
+}
+
+}  // namespace
+
+int qbx_compute_density(qbx_context* h, double weight, double* rho) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, false);
+    QBX_REQUIRE(c.kpts.empty(), 1, "qbx_compute_density works on the Gamma SlaterDet");
+    QBX_REQUIRE(rho, 1, "null density array");
+    const size_t N = c.N();
+    if (!c.d_xgrid) c.d_xgrid = dalloc<double>(N);
+    launch_density(c, c.d_c, c.d_xgrid);
+    std::vector<double> tmp(N);
+    QBX_CUDA(cudaMemcpyAsync(tmp.data(), c.d_xgrid, N * sizeof(double), cudaMemcpyDeviceToHost,
+                             c.stream));
+    QBX_CUDA(cudaStreamSynchronize(c.stream));
+    for (size_t i = 0; i < N; i++) rho[i] += weight * tmp[i];
+  });
+}
+
+int qbx_rs_mul_add(qbx_context* h, const double* v, double* dc) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, false);
+    QBX_REQUIRE(c.kpts.empty(), 1, "qbx_rs_mul_add works on the Gamma SlaterDet");
+    QBX_REQUIRE(v && dc, 1, "null potential or output array");
+    const size_t N = c.N();
+    if (!c.d_xgrid) c.d_xgrid = dalloc<double>(N);
+    double* out = lazy_wf(c, c.d_xsd);
+    QBX_CUDA(cudaMemcpyAsync(c.d_xgrid, v, N * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    launch_vpsi(c, c.d_c, c.d_xgrid, out);   // 1/2 G^2 c + V psi
+    k_sub_kinetic<<<1184, 256, 0, c.stream>>>((double2*)out, (const double2*)c.d_c, c.d_g2_w,
+                                              c.wb.ng, c.nst);
+    QBX_LAUNCHED(c);
+    const std::vector<double> add = download_wf(h, out);
+    for (size_t i = 0; i < add.size(); i++) dc[i] += add[i];
+  });
+}
+
+int qbx_nonlocal_energy(qbx_context* h, int compute_hpsi, double* dc, int compute_forces,
+                        double* fion, int compute_stress, double* sigma_enl, double* enl) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, true);
+    QBX_REQUIRE(c.kpts.empty(), 1, "qbx_nonlocal_energy works on the Gamma SlaterDet");
+    QBX_REQUIRE(!compute_hpsi || dc, 1, "null H*psi array");
+    QBX_REQUIRE(!compute_forces || fion, 1, "null force array");
+    QBX_REQUIRE(!compute_stress || sigma_enl, 1, "null stress array");
+    double* out = compute_hpsi ? lazy_wf(c, c.d_xsd) : nullptr;
+    nonlocal_only(c, compute_hpsi != 0, out);
+    size_t natoms = 0;
+    for (auto& t : c.tau) natoms += t.size() / 3;
+    if (compute_forces) {
+      QBX_CUDA(cudaMemsetAsync(c.d_fion, 0, sizeof(double) * 3 * natoms, c.stream));
+      if (c.nproj) launch_nl_forces(c, c.d_fion);
+    }
+    if (compute_stress) compute_stress_nl(c);
+    readback(c, compute_forces != 0);
+    check_status(c);
+    const double e_nl = c.nproj ? c.h_scalars[SLOT_ENL] : 0.0;
+    if (enl) *enl = e_nl;
+    if (compute_forces) std::memcpy(fion, c.h_fion, sizeof(double) * 3 * natoms);
+    if (compute_stress) nl_stress_part(c, e_nl, sigma_enl);
+    if (compute_hpsi) {
+      const std::vector<double> add = download_wf(h, out);
+      for (size_t i = 0; i < add.size(); i++) dc[i] += add[i];
+    }
+  });
+}
+
+int qbx_ortho_align(qbx_context* h, const double* c_ref) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, false);
+    QBX_REQUIRE(c.kpts.empty(), 1, "qbx_ortho_align works on the Gamma SlaterDet");
+    QBX_REQUIRE(c_ref, 1, "null coefficient array");
+    upload_wf(h, c_ref, c.d_c_last);
+    if (c.precision == MIXED)
+      split_bf16_2d(c, c.d_c_last, 2 * c.wb.ng, c.nst, 2 * c.wb.ng, c.cs_hi[0], c.cs_lo[0], c.ldp);
+    ortho_align(c);
+    // the stepper's last-step buffer now holds the caller's SlaterDet
+    c.extrapolate = false;
+    readback(c, false);
+    check_status(c);
+  });
+}
+
+int qbx_dot(qbx_context* h, const double* c_other, double* d) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, false);
+    QBX_REQUIRE(c.kpts.empty(), 1, "qbx_dot works on the Gamma SlaterDet");
+    QBX_REQUIRE(c_other && d, 1, "null coefficient or result pointer");
+    double* other = lazy_wf(c, c.d_xsd);
+    upload_wf(h, c_other, other);
+    double* acc = c.d_scalars + SLOT_SCRATCH;
+    QBX_CUDA(cudaMemsetAsync(acc, 0, sizeof(double), c.stream));
+    k_sd_dot<<<1184, 256, 0, c.stream>>>(c.d_c, other, c.wb.ng, c.nst, acc);
+    QBX_LAUNCHED(c);
+    QBX_CUDA(cudaMemcpyAsync(d, acc, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     QBX_CUDA(cudaStreamSynchronize(c.stream));
   });
 }

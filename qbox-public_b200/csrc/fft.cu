@@ -430,6 +430,28 @@ __global__ void k_gather_sphere(const double2* __restrict__ grid, const int* __r
   }
 }
 
+// complex basis: only +G is stored (BasisMapping::vector_to_zvec,
+// src/BasisMapping.cpp:655-663)
+__global__ void k_scatter_plus(const double2* __restrict__ c, const int* __restrict__ ip, int ng,
+                               double2* __restrict__ grid) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ng; i += gridDim.x * blockDim.x)
+    grid[ip[i]] = c[i];
+}
+
+// two real functions out of one complex transform
+// (BasisMapping::zvec_to_doublevector, src/BasisMapping.cpp:716-750), with
+// the forward transform's 1/N applied to the grid values
+__global__ void k_gather_pair(const double2* __restrict__ grid, const int* __restrict__ ip,
+                              const int* __restrict__ im, int ng, double scale,
+                              double2* __restrict__ c1, double2* __restrict__ c2) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ng; i += gridDim.x * blockDim.x) {
+    const double2 p = grid[ip[i]], m = grid[im[i]];
+    const double a = p.x * scale, b = p.y * scale, c = m.x * scale, d = m.y * scale;
+    c1[i] = make_double2(0.5 * (a + c), 0.5 * (b - d));
+    c2[i] = make_double2(0.5 * (b + d), 0.5 * (c - a));
+  }
+}
+
 __global__ void k_real_to_grid(const double* __restrict__ f, double scale, size_t n,
                                double2* __restrict__ grid) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
@@ -905,6 +927,70 @@ void wfgrid_forward(Context& ctx, const DeviceSticks& d, int ng, const double* f
 }
 
 static int nblk(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 16); }
+
+// ----------------------------------------------- a caller's basis and grid
+// The grid of a FourierTransform built on any basis (its Miller indices in
+// the caller's order): sizes, twiddle tables, radix plans and the grid
+// index of +G and (real basis) -G of each coefficient.  The transforms are
+// full-grid line passes; the staged z-stick kernels serve the contexts'
+// own bases.
+void upload_grid_map(DeviceSticks& d, int n0, int n1, int n2, const std::vector<int>& ip,
+                     const std::vector<int>& im) {
+  free_sticks(d);
+  d = DeviceSticks{};
+  d.n0 = n0; d.n1 = n1; d.n2 = n2;
+  d.ip = dupload(ip);
+  if (!im.empty()) d.im = dupload(im);
+  d.px = make_plan(n0);
+  d.py = make_plan(n1);
+  d.pz = make_plan(n2);
+  const int n[3] = {n0, n1, n2};
+  for (int a = 0; a < 3; a++) {
+    std::vector<double2> t = twiddle_table(n[a]);
+    d.tw[a] = dalloc<double2>(n[a]);
+    h2d_sync(d.tw[a], t.data(), n[a] * sizeof(double2));
+  }
+}
+
+// FourierTransform::backward (src/FourierTransform.cpp:159-200): one band
+// (c2 == nullptr) or the pair c1 + i c2 (real basis) from the basis to the
+// complex grid, unscaled synthesis
+void basis_ft_backward(Context& ctx, const DeviceSticks& d, int ng, bool real_basis,
+                       const double* c1, const double* c2, double* grid) {
+  const size_t N = (size_t)d.n0 * d.n1 * d.n2;
+  QBX_CUDA(cudaMemsetAsync(grid, 0, N * sizeof(double2), ctx.stream));
+  if (!real_basis) {
+    k_scatter_plus<<<nblk(ng), 256, 0, ctx.stream>>>((const double2*)c1, d.ip, ng,
+                                                     (double2*)grid);
+  } else if (c2) {
+    k_scatter_pair<<<nblk(ng), 256, 0, ctx.stream>>>((const double2*)c1, (const double2*)c2, d.ip,
+                                                     d.im, ng, (double2*)grid);
+  } else {
+    k_scatter_sphere<<<nblk(ng), 256, 0, ctx.stream>>>((const double2*)c1, d.ip, d.im, ng,
+                                                       (double2*)grid);
+  }
+  QBX_LAUNCHED(ctx);
+  grid_fft_on(ctx, d, (double2*)grid, +1);
+}
+
+// FourierTransform::forward (src/FourierTransform.cpp:147-196): the grid is
+// transformed in place (the reference also overwrites f), scaled by 1/N and
+// gathered onto the basis; with c2 the two real functions are unpacked
+void basis_ft_forward(Context& ctx, const DeviceSticks& d, int ng, bool real_basis, double* grid,
+                      double* c1, double* c2) {
+  const size_t N = (size_t)d.n0 * d.n1 * d.n2;
+  grid_fft_on(ctx, d, (double2*)grid, -1);
+  const double scale = 1.0 / (double)N;
+  if (c2) {
+    QBX_REQUIRE(real_basis, 1, "the two-band forward transform needs a real basis");
+    k_gather_pair<<<nblk(ng), 256, 0, ctx.stream>>>((const double2*)grid, d.ip, d.im, ng, scale,
+                                                    (double2*)c1, (double2*)c2);
+  } else {
+    k_gather_sphere<<<nblk(ng), 256, 0, ctx.stream>>>((const double2*)grid, d.ip, ng, scale,
+                                                      (double2*)c1);
+  }
+  QBX_LAUNCHED(ctx);
+}
 
 void vb_backward(Context& ctx, const double* coef, double* real_out) {
   const size_t N = ctx.N();

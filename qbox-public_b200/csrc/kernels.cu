@@ -891,9 +891,8 @@ enum : int { SS_EKIN = SLOT_STRESS, SS_EPS = SLOT_STRESS + 6, SS_EHART = SLOT_ST
 static_assert(SS_ENL + 6 <= SLOT_SCRATCH, "stress slots overlap the scratch slots");
 
 void compute_stress(Context& ctx) {
-  static const int vi[6] = {0, 1, 2, 0, 1, 0}, vj[6] = {0, 1, 2, 1, 2, 2};
   const double om_inv = 1.0 / ctx.wb.omega;
-  const int ngw = ctx.wb.ng, ngv = ctx.vb.ng, nst = ctx.nst, np = ctx.nproj;
+  const int ngw = ctx.wb.ng, ngv = ctx.vb.ng, nst = ctx.nst;
   const int nsp = (int)ctx.species.size();
   const size_t N = ctx.N();
   reduce<6>(ctx, EkinStressF{(const double2*)ctx.d_c, ctx.d_gx_w, ctx.d_occ, ngw},
@@ -909,6 +908,15 @@ void compute_stress(Context& ctx) {
     reduce<1>(ctx, LdaStressF{ctx.d_exc, ctx.d_rhor, ctx.d_vxc}, N, SS_EXC);
   else
     reduce<6>(ctx, GgaStressF{ctx.d_grad, ctx.d_vx2, N}, N, SS_EXC);
+  compute_stress_nl(ctx);
+}
+
+// The nonlocal part alone (src/NonLocalPotential.cpp:1790-2069): per Voigt
+// component the strain derivative of the projector forms times the phases,
+// dF = 2 A_ij^T C, contracted with D F / Omega into the SS_ENL slots.
+void compute_stress_nl(Context& ctx) {
+  static const int vi[6] = {0, 1, 2, 0, 1, 0}, vj[6] = {0, 1, 2, 1, 2, 2};
+  const int ngw = ctx.wb.ng, nst = ctx.nst, np = ctx.nproj;
   QBX_CUDA(cudaMemsetAsync(ctx.d_scalars + SS_ENL, 0, 6 * sizeof(double), ctx.stream));
   if (np) {
     const int K = 2 * ngw;
@@ -939,6 +947,14 @@ void compute_stress(Context& ctx) {
                 SS_ENL + k);
     }
   }
+}
+
+// sigma_enl of NonLocalPotential::energy (src/NonLocalPotential.cpp:2057-2066)
+// from E_nl and the SS_ENL slots read back after compute_stress_nl
+void nl_stress_part(const Context& ctx, double enl, double* sigma_enl) {
+  const double om_inv = 1.0 / ctx.wb.omega;
+  for (int k = 0; k < 6; k++)
+    sigma_enl[k] = ((k < 3 ? enl : 0.0) + ctx.h_scalars[SS_ENL + k]) * om_inv;
 }
 
 // The stress parts from the slots of compute_stress and the energies of the

@@ -35,17 +35,16 @@ constexpr int kMaxLen = 4096;   // longest FFT length whose table fits
 
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
-// Device address of g_scratch per device, taken once with that device current.
-static void* g_scratch_ptr[64] = {nullptr};
-
-void* scratch_address(int device) {
-  QBX_REQUIRE(device >= 0 && device < 64, 61, "device index out of range for the static scratch");
-  if (!g_scratch_ptr[device]) {
-    void* p = nullptr;
-    QBX_CUDA(cudaGetSymbolAddress(&p, g_scratch));
-    g_scratch_ptr[device] = p;
-  }
-  return g_scratch_ptr[device];
+// Device address of g_scratch in the CUDA context current on the calling
+// thread.  A __device__ symbol's address belongs to a context, not to a
+// device ordinal (a plug-in's own driver-API context on the same device, or
+// the context made after a cudaDeviceReset, places the array elsewhere), so
+// it is looked up on every call; the lookup allocates nothing.
+void* scratch_address() {
+  void* p = nullptr;
+  QBX_CUDA(cudaGetSymbolAddress(&p, g_scratch));
+  QBX_REQUIRE(p != nullptr, 61, "no device address for the static scratch array");
+  return p;
 }
 
 // exp(+2 pi i k/n) for the three axis lengths, and the band weights
@@ -90,7 +89,7 @@ extern "C" int qbx_density_static(qbx_context* h, const double* d_c, int nst, co
                 "one band pair's z-sticks (" + std::to_string(per_pair) +
                     " bytes) exceed the static scratch of " +
                     std::to_string(kScratchBytes - kTableBytes) + " bytes");
-    unsigned char* base = (unsigned char*)scratch_address(c.device);
+    unsigned char* base = (unsigned char*)scratch_address();
     double2* twx = (double2*)base;
     double2* twy = twx + n0;
     double2* twz = twy + n1;

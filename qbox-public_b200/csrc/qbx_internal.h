@@ -331,6 +331,8 @@ struct Context {
   double* d_c_last = nullptr;
   double* d_dc_last = nullptr;
   double* d_ctmp = nullptr;     // scratch copy of C
+  double* d_xsd = nullptr;      // a caller's SlaterDet (class-level entry points), lazy
+  double* d_xgrid = nullptr;    // a caller's grid function (class-level entry points), lazy
   double* d_occ = nullptr;      // nst
   double* d_anl = nullptr;      // 2*ngw*nproj  (complex projectors x phase)
   double* d_fnl = nullptr;      // nproj*nst
@@ -402,6 +404,10 @@ struct Context {
 
   // mixed precision: BF16 hi/lo splits of the GEMM operands
   int gemm_backend = 1;         // 0: cuBLAS BF16 products, 1: own tcgen05 kernel
+  int tc_chunk = 2;             // tcgen05 GEMM: K blocks per TMEM chain of the hi*hi term
+  int tc_corr_mul = 8;          // tcgen05 GEMM: hi*lo + lo*hi chains this many times longer,
+                                // in accumulators of their own (0: in the hi*hi chain)
+  int tc_epw = 8;               // tcgen05 GEMM: epilogue warps (4 or 8)
   void* d_acc32 = nullptr;      // FP32 product accumulator
   size_t acc32_elems = 0;
   void* cs_hi[2] = {nullptr, nullptr};   // splits of C (0: at energy, 1: after the step)
@@ -587,6 +593,11 @@ void launch_nl_forces(Context& ctx, double* fion);
 // stress tensor of the state of the last energy(): SLOT_STRESS; then
 // finish_stress gives ctx.sigma, ctx.sigma_parts
 void compute_stress(Context& ctx);
+void compute_stress_nl(Context& ctx);            // the nonlocal part alone (SS_ENL slots)
+void nl_stress_part(const Context& ctx, double enl, double* sigma_enl);   // after readback
+// NonLocalPotential::energy on its own: E_nl into its slot and, with hpsi,
+// the nonlocal part of H*C written to out (device, K x nst)
+void nonlocal_only(Context& ctx, bool hpsi, double* out);
 void launch_identity_axpy(Context& ctx, double* t, const double* q, int n,
                           double alpha);       // t = I + alpha*q
 void launch_symmetrize_lower(Context& ctx, double* q, int n);
@@ -636,6 +647,12 @@ void free_mix(Context& c);
 void write_wavefunction(Context& c, std::ostream& os);
 void read_wavefunction(Context& c, const std::string& text);
 void wfgrid_backward(Context& ctx, const DeviceSticks& d, int ng, const double* c, double* f);
+void upload_grid_map(DeviceSticks& d, int n0, int n1, int n2, const std::vector<int>& ip,
+                     const std::vector<int>& im);
+void basis_ft_backward(Context& ctx, const DeviceSticks& d, int ng, bool real_basis,
+                       const double* c1, const double* c2, double* grid);
+void basis_ft_forward(Context& ctx, const DeviceSticks& d, int ng, bool real_basis, double* grid,
+                      double* c1, double* c2);
 void wfgrid_forward(Context& ctx, const DeviceSticks& d, int ng, const double* f, double* c);
 // molecular dynamics (md.cu)
 void move_atoms(Context& c, const double* tau);

@@ -459,6 +459,23 @@ static void nonlocal(Context& ctx, bool hpsi) {
   }
 }
 
+void nonlocal_only(Context& ctx, bool hpsi, double* out) {
+  const int K = 2 * ctx.wb.ng;
+  if (mixed(ctx))
+    split_bf16_2d(ctx, ctx.d_c, K, ctx.nst, K, ctx.cs_hi[0], ctx.cs_lo[0], ctx.ldp);
+  if (hpsi)
+    QBX_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * (size_t)K * ctx.nst, ctx.stream));
+  double* saved = ctx.d_hc;
+  ctx.d_hc = out;
+  try {
+    nonlocal(ctx, hpsi);
+  } catch (...) {
+    ctx.d_hc = saved;
+    throw;
+  }
+  ctx.d_hc = saved;
+}
+
 // EnergyFunctional::energy (src/EnergyFunctional.cpp:397-1044)
 void energy(Context& ctx, bool hpsi, bool forces) {
   ProfScope ps(ctx, "energy");

@@ -49,9 +49,15 @@ constexpr int STAGES = 3;
 constexpr int TILE_BYTES = BM * 128;              // 16 KB per operand tile
 constexpr int STAGE_BYTES = 4 * TILE_BYTES;       // A_hi, A_lo, B_hi, B_lo
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /* align */ + 256 /* barriers */;
-constexpr int THREADS = 256;
-constexpr uint32_t TMEM_COLS = 2 * BN;           // two accumulators, used in turn
-constexpr int CHUNK = 8;                          // K blocks per accumulator fill
+// warps 0-3: TMA producer, MMA issuer, two idle; then EPW epilogue warps,
+// EPW/4 per TMEM lane quarter (warp w reads lanes 32*(w%4) .. 32*(w%4)+31),
+// each holding BN*4/EPW columns of the tile
+__host__ __device__ constexpr int threads_of(int epw) { return 128 + 32 * epw; }
+// TMEM: two accumulators used in turn (256 columns); with the correction
+// terms kept apart (sep), a second pair for hi*lo + lo*hi (512 columns)
+// TMEM: two hi*hi accumulators used in turn (256 columns); with the
+// correction terms kept apart (sep), two more for hi*lo + lo*hi (512 columns)
+__host__ __device__ constexpr uint32_t tmem_cols_of(int sep) { return sep ? 4 * BN : 2 * BN; }
 constexpr long long WAIT_LIMIT = 1ll << 24;       // bounded spins per wait
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -129,6 +135,18 @@ __device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t da, uint64_t db, 
   }
 }
 
+// 16 consecutive TMEM columns of this warp's 32 lanes (one per thread);
+// the caller waits with tcgen05.wait::ld before reading r
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t* r) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
@@ -141,21 +159,28 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
 }
 
 // Accumulation: the MMA warp fills one of two 128-column TMEM accumulators
-// with CHUNK K blocks (512 products of each split term per element) and
-// commits it; the epilogue warps add that accumulator into FP32 registers
-// and hand it back, while the MMA warp fills the other one.  FP32 chains
-// thus stay short (CHUNK*4 MMA steps in TMEM, then one register add per
-// chunk) instead of one TMEM chain over the whole K slice.
+// with `chunk` K blocks (64 * chunk products of each split term per
+// element) and commits it; the epilogue warps add that accumulator into FP32
+// registers (round to nearest) and hand it back, while the MMA warp fills
+// the other one.  The tensor core's own FP32 additions into TMEM do not
+// round to nearest: each one can shift the running sum toward zero by up to
+// an ulp, so a long chain biases a coherent inner product low (at 145 838
+// rows and 96 additions per chain that bias reached 1.7e-6 of F = A^T C,
+// 3e-6 of E_nl).  Short chains keep that bias down.  With corr_mul > 0 the
+// small terms hi*lo + lo*hi (2^-8 of the sum) go to a second pair of
+// accumulators whose chains are corr_mul times longer, so that the large
+// hi*hi chain carries one MMA per K step of 16 and the epilogue drains the
+// small terms only every corr_mul chunks.
 // Output: with ws != nullptr the FP32 tile of split-K slice z goes to
 // ws[z][col * M + row]; otherwise (no K split) C[col * ldc + row] =
 // alpha * D + beta * C in FP64.  Rows >= M and columns >= N are not stored.
-template <int KIND>
-__global__ void __launch_bounds__(THREADS, 1)
+template <int KIND, int EPW>
+__global__ void __launch_bounds__(threads_of(EPW), 1)
 k_tc_split_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant__ CUtensorMap ma_lo,
                 const __grid_constant__ CUtensorMap mb_hi, const __grid_constant__ CUtensorMap mb_lo,
                 int M, int N, int nkb, int kb_per_split, float* __restrict__ ws,
                 double* __restrict__ C, int ldc, double alpha, double beta,
-                int* __restrict__ err, int lower) {
+                int* __restrict__ err, int lower, int chunk, int corr_mul) {
   // lower: a tile whose every column is right of its every row holds only
   // the strict upper triangle and is not formed (the whole CTA leaves before
   // it allocates anything)
@@ -169,7 +194,9 @@ k_tc_split_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant
   uint64_t* empty = full + STAGES;
   uint64_t* tfull = empty + STAGES;      // accumulator b filled
   uint64_t* tfree = tfull + 2;           // accumulator b drained by the epilogue
-  uint32_t* tmem_slot = (uint32_t*)(tfree + 2);
+  uint64_t* cfull = tfree + 2;           // correction accumulator b filled
+  uint64_t* cfree = cfull + 2;           // correction accumulator b drained
+  uint32_t* tmem_slot = (uint32_t*)(cfree + 2);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // without a K split the N tiles of one M tile are adjacent in the grid, so
@@ -178,7 +205,10 @@ k_tc_split_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant
   const int kb0 = blockIdx.z * kb_per_split;
   const int kb1 = min(nkb, kb0 + kb_per_split);
   const int niter = max(0, kb1 - kb0);
-  const int nchunk = (niter + CHUNK - 1) / CHUNK;
+  const int nchunk = (niter + chunk - 1) / chunk;
+  const int sep = corr_mul > 0 ? 1 : 0;
+  const int cchunk = chunk * (sep ? corr_mul : 1);   // K blocks per correction chain
+  const uint32_t tmem_cols = tmem_cols_of(sep);
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; s++) {
@@ -187,14 +217,16 @@ k_tc_split_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant
     }
     for (int b = 0; b < 2; b++) {
       mbar_init(&tfull[b], 1);
-      mbar_init(&tfree[b], 4);           // one arrival per epilogue warp
+      mbar_init(&tfree[b], EPW);         // one arrival per epilogue warp
+      mbar_init(&cfull[b], 1);
+      mbar_init(&cfree[b], EPW);
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(tmem_slot)),
-                 "r"(TMEM_COLS)
+                 "r"(tmem_cols)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -219,10 +251,17 @@ k_tc_split_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant
   } else if (warp == 1 && lane == 0) {
     // ---------------- MMA issuer
     for (int it = 0; it < niter; ++it) {
-      const int c = it / CHUNK, b = c & 1;
-      const bool chunk_start = (it % CHUNK) == 0;
+      const int c = it / chunk, b = c & 1;
+      const int cc = it / cchunk, cb = cc & 1;
+      const bool chunk_start = (it % chunk) == 0;
+      const bool corr_start = (it % cchunk) == 0;
       if (chunk_start && c >= 2 && !mbar_wait(&tfree[b], (uint32_t)(((c >> 1) - 1) & 1))) {
         atomicExch(err, 4);
+        break;
+      }
+      if (sep && corr_start && cc >= 2 &&
+          !mbar_wait(&cfree[cb], (uint32_t)(((cc >> 1) - 1) & 1))) {
+        atomicExch(err, 5);
         break;
       }
       const int s = it % STAGES;
@@ -235,25 +274,44 @@ k_tc_split_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant
       const uint64_t dbh = smem_desc(st + 2 * TILE_BYTES);
       const uint64_t dbl = smem_desc(st + 3 * TILE_BYTES);
       const uint32_t tacc = tmem + (uint32_t)(b * BN);
+      const uint32_t tcor = sep ? tmem + (uint32_t)((2 + cb) * BN) : tacc;
       // 4 MMAs of 32 bytes of K each (16 BF16 or 8 TF32)
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         const uint64_t off = (uint64_t)(k * 32) >> 4;
         const uint32_t accumulate = (chunk_start && k == 0) ? 0u : 1u;
+        const uint32_t cacc = sep ? ((corr_start && k == 0) ? 0u : 1u) : 1u;
         umma<KIND>(tacc, dah + off, dbh + off, accumulate);
-        umma<KIND>(tacc, dah + off, dbl + off, 1u);
-        umma<KIND>(tacc, dal + off, dbh + off, 1u);
+        umma<KIND>(tcor, dah + off, dbl + off, cacc);
+        umma<KIND>(tcor, dal + off, dbh + off, 1u);
       }
       umma_commit(&empty[s]);
-      if ((it % CHUNK) == CHUNK - 1 || it == niter - 1) umma_commit(&tfull[b]);
+      if ((it % chunk) == chunk - 1 || it == niter - 1) umma_commit(&tfull[b]);
+      if (sep && ((it % cchunk) == cchunk - 1 || it == niter - 1)) umma_commit(&cfull[cb]);
     }
   } else if (warp >= 4) {
     // ---------------- epilogue: drain each chunk into FP32 registers
-    const int wq = warp - 4;                       // TMEM lanes 32*wq .. 32*wq+31
+    constexpr int COLS = BN * 4 / EPW;             // columns of this warp
+    const int wq = warp & 3;                       // TMEM lanes 32*wq .. 32*wq+31
+    const int cbase = ((warp - 4) >> 2) * COLS;    // first column of this warp
     const int row = m0 + wq * 32 + lane;
-    float acc[BN];
+    const uint32_t tlane = tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)cbase;
+    float acc[COLS];
 #pragma unroll
-    for (int j = 0; j < BN; ++j) acc[j] = 0.0f;
+    for (int j = 0; j < COLS; ++j) acc[j] = 0.0f;
+    // acc += this warp's columns of one accumulator, 64 columns (four loads
+    // in flight) per wait
+    auto drain = [&](uint32_t col0) {
+#pragma unroll
+      for (int c0 = 0; c0 < COLS; c0 += 64) {
+        uint32_t r[64];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) tmem_ld16(tlane + col0 + (uint32_t)(c0 + 16 * q), r + 16 * q);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int j = 0; j < 64; ++j) acc[c0 + j] += __uint_as_float(r[j]);
+      }
+    };
     bool ok = true;
     for (int c = 0; c < nchunk && ok; ++c) {
       const int b = c & 1;
@@ -263,31 +321,30 @@ k_tc_split_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-#pragma unroll
-      for (int c0 = 0; c0 < BN; c0 += 16) {
-        uint32_t r[16];
-        const uint32_t taddr = tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)(b * BN + c0);
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-            "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
-              "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
-              "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-            : "r"(taddr));
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-        for (int j = 0; j < 16; ++j) acc[c0 + j] += __uint_as_float(r[j]);
-      }
+      drain((uint32_t)(b * BN));
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       __syncwarp();
       if (lane == 0) mbar_arrive(&tfree[b]);
+      if (sep && ((c + 1) % corr_mul == 0 || c == nchunk - 1)) {
+        const int cc = c / corr_mul, cb = cc & 1;
+        if (!mbar_wait(&cfull[cb], (uint32_t)((cc >> 1) & 1))) {
+          atomicExch(err, 6);
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        drain((uint32_t)((2 + cb) * BN));
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&cfree[cb]);
+      }
     }
     if (ws) {
       float* out = ws + (size_t)blockIdx.z * M * N;
       if (row < M) {
 #pragma unroll
-        for (int j = 0; j < BN; ++j) {
-          const int col = n0 + j;
+        for (int j = 0; j < COLS; ++j) {
+          const int col = n0 + cbase + j;
           if (col < N) out[(size_t)col * M + row] = ok ? acc[j] : 0.0f;
         }
       }
@@ -298,8 +355,8 @@ k_tc_split_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant
         // writer, so the result does not depend on their order); no load
         // round trips in the epilogue
 #pragma unroll
-        for (int j = 0; j < BN; ++j) {
-          const int col = n0 + j;
+        for (int j = 0; j < COLS; ++j) {
+          const int col = n0 + cbase + j;
           if (col < N) atomicAdd(crow + (size_t)col * ldc, alpha * (double)acc[j]);
         }
       } else {
@@ -308,18 +365,18 @@ k_tc_split_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant
       // load at a time would leave the epilogue waiting 128 round trips)
       constexpr int G = 16;
 #pragma unroll
-      for (int j0 = 0; j0 < BN; j0 += G) {
+      for (int j0 = 0; j0 < COLS; j0 += G) {
         double old[G];
         if (beta != 0.0) {
 #pragma unroll
           for (int j = 0; j < G; ++j) {
-            const int col = n0 + j0 + j;
+            const int col = n0 + cbase + j0 + j;
             old[j] = col < N ? crow[(size_t)col * ldc] : 0.0;
           }
         }
 #pragma unroll
         for (int j = 0; j < G; ++j) {
-          const int col = n0 + j0 + j;
+          const int col = n0 + cbase + j0 + j;
           if (col < N)
             crow[(size_t)col * ldc] = alpha * (double)acc[j0 + j] + (beta != 0.0 ? beta * old[j] : 0.0);
         }
@@ -331,7 +388,7 @@ k_tc_split_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant
   if (warp == 1) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                 "r"(TMEM_COLS)
+                 "r"(tmem_cols)
                  : "memory");
   }
 }
@@ -443,17 +500,22 @@ static void tc_gemm_tn(Context& ctx, int kind, int m, int n, int k, double alpha
     }
   }
   int* err = ctx.d_status + ST_TC_ERR;   // wait-timeout flag, sticky
+  const int chunk = std::max(1, ctx.tc_chunk), corr_mul = std::max(0, ctx.tc_corr_mul);
   float* ws = splits > 1 ? (float*)ctx.d_tc_ws : nullptr;
   QBX_REQUIRE(splits > 1 ? tn <= 65535 : tm <= 65535, 54, "too many tiles for the grid");
   dim3 grid = splits > 1 ? dim3(tm, tn, splits) : dim3(tn, tm, 1);
+  auto launch = [&](auto kern, int epw) {
+    allow_smem(kern, tc::SMEM_BYTES);
+    kern<<<grid, tc::threads_of(epw), tc::SMEM_BYTES, ctx.stream>>>(
+        mah, mal, mbh, mbl, m, n, nkb, kbps, ws, C, ldc, alpha, beta, err, lower ? 1 : 0,
+        chunk, corr_mul);
+  };
   if (kind == tc::KIND_BF16) {
-    allow_smem(tc::k_tc_split_gemm<tc::KIND_BF16>, tc::SMEM_BYTES);
-    tc::k_tc_split_gemm<tc::KIND_BF16><<<grid, tc::THREADS, tc::SMEM_BYTES, ctx.stream>>>(
-        mah, mal, mbh, mbl, m, n, nkb, kbps, ws, C, ldc, alpha, beta, err, lower ? 1 : 0);
+    if (ctx.tc_epw == 8) launch(tc::k_tc_split_gemm<tc::KIND_BF16, 8>, 8);
+    else launch(tc::k_tc_split_gemm<tc::KIND_BF16, 4>, 4);
   } else {
-    allow_smem(tc::k_tc_split_gemm<tc::KIND_TF32>, tc::SMEM_BYTES);
-    tc::k_tc_split_gemm<tc::KIND_TF32><<<grid, tc::THREADS, tc::SMEM_BYTES, ctx.stream>>>(
-        mah, mal, mbh, mbl, m, n, nkb, kbps, ws, C, ldc, alpha, beta, err, lower ? 1 : 0);
+    if (ctx.tc_epw == 8) launch(tc::k_tc_split_gemm<tc::KIND_TF32, 8>, 8);
+    else launch(tc::k_tc_split_gemm<tc::KIND_TF32, 4>, 4);
   }
   QBX_LAUNCHED(ctx);
   if (splits > 1) {

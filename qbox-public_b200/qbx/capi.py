@@ -43,6 +43,9 @@ SYMBOLS = (
     "qbx_scf_step_batch", "qbx_set_step_graph", "qbx_step_graph_info", "qbx_polar",
     "qbx_move_atoms", "qbx_md_run", "qbx_scf_run", "qbx_write_wavefunction",
     "qbx_read_wavefunction",
+    "qbx_ft_create", "qbx_ft_destroy", "qbx_ft_last_error", "qbx_ft_backward",
+    "qbx_ft_backward2", "qbx_ft_forward", "qbx_ft_forward2", "qbx_compute_density",
+    "qbx_rs_mul_add", "qbx_nonlocal_energy", "qbx_ortho_align", "qbx_dot",
 )
 
 _lib = None
@@ -131,6 +134,18 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "qbx_get_kpoint_hpsi": (_I, [_P, _I, _DP]),
         "qbx_step_graph_info": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_long),
                                      ctypes.POINTER(ctypes.c_long), ctypes.c_char_p, _I]),
+        "qbx_ft_create": (_I, [ctypes.POINTER(_P), _I, _I, _IP, _I, _I, _I, _I]),
+        "qbx_ft_destroy": (None, [_P]),
+        "qbx_ft_last_error": (ctypes.c_char_p, [_P]),
+        "qbx_ft_backward": (_I, [_P, _DP, _DP]),
+        "qbx_ft_backward2": (_I, [_P, _DP, _DP, _DP]),
+        "qbx_ft_forward": (_I, [_P, _DP, _DP]),
+        "qbx_ft_forward2": (_I, [_P, _DP, _DP, _DP]),
+        "qbx_compute_density": (_I, [_P, _D, _DP]),
+        "qbx_rs_mul_add": (_I, [_P, _DP, _DP]),
+        "qbx_nonlocal_energy": (_I, [_P, _I, _DP, _I, _DP, _I, _DP, _DP]),
+        "qbx_ortho_align": (_I, [_P, _DP]),
+        "qbx_dot": (_I, [_P, _DP, _DP]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -509,9 +524,64 @@ class Context:
         (default coefficient order) into a device grid, using the library's
         static scratch array; pointers are raw device addresses."""
         o = None if occ is None else np.ascontiguousarray(occ, dtype=float)
+        if o is not None and o.size != nst:
+            raise ValueError(f"density_static: {o.size} occupations for {nst} bands")
         self._ok(self.lib.qbx_density_static(self.h, ctypes.c_void_p(c_dev_ptr), nst,
                                              _dp(o), ctypes.c_void_p(rho_dev_ptr)),
                  "density_static")
+
+    # ---- the reference's class methods on host arrays
+    def compute_density(self, weight: float, rho: np.ndarray):
+        """SlaterDet::compute_density: rho += weight * sum_n occ_n/Omega
+        |psi_n|^2 (rho: float64 array of the grid size, x fastest)."""
+        assert rho.dtype == np.float64 and rho.flags["C_CONTIGUOUS"]
+        assert rho.size == self.grid[0] * self.grid[1] * self.grid[2]
+        self._ok(self.lib.qbx_compute_density(self.h, float(weight), _dp(rho)),
+                 "compute_density")
+
+    def rs_mul_add(self, v: np.ndarray, dc: np.ndarray):
+        """SlaterDet::rs_mul_add: dc += FFT_fwd(v FFT_bwd(c)) (dc: complex
+        (nst, ngw), modified in place)."""
+        vv = np.ascontiguousarray(v, float)
+        assert vv.size == self.grid[0] * self.grid[1] * self.grid[2]
+        assert dc.dtype == np.complex128 and dc.flags["C_CONTIGUOUS"]
+        assert dc.shape == (self.nst, self.ngw)
+        self._ok(self.lib.qbx_rs_mul_add(self.h, _dp(vv), _dp(dc.view(np.float64))),
+                 "rs_mul_add")
+
+    def nonlocal_energy(self, dc: Optional[np.ndarray] = None, forces: bool = False,
+                        stress: bool = False):
+        """NonLocalPotential::energy: returns {"enl", "fion" (natoms x 3),
+        "sigma_enl" (6)}; with dc the nonlocal H*C is added into it."""
+        if dc is not None:
+            assert dc.dtype == np.complex128 and dc.flags["C_CONTIGUOUS"]
+            assert dc.shape == (self.nst, self.ngw)
+        f = np.zeros(3 * max(1, self.natoms))
+        sig = np.zeros(6)
+        e = _D()
+        self._ok(self.lib.qbx_nonlocal_energy(
+            self.h, int(dc is not None), _dp(dc.view(np.float64)) if dc is not None else None,
+            int(forces), _dp(f), int(stress), _dp(sig), ctypes.byref(e)), "nonlocal_energy")
+        out = {"enl": e.value}
+        if forces:
+            out["fion"] = f[:3 * self.natoms].reshape(-1, 3)
+        if stress:
+            out["sigma_enl"] = sig
+        return out
+
+    def ortho_align(self, c_ref: np.ndarray):
+        """SlaterDet::ortho_align(sd) with sd's coefficients c_ref."""
+        a = np.ascontiguousarray(c_ref, np.complex128)
+        assert a.shape == (self.nst, self.ngw)
+        self._ok(self.lib.qbx_ortho_align(self.h, _dp(a.view(np.float64))), "ortho_align")
+
+    def dot(self, c_other: np.ndarray) -> float:
+        """SlaterDet::dot(sd) at Gamma."""
+        a = np.ascontiguousarray(c_other, np.complex128)
+        assert a.shape == (self.nst, self.ngw)
+        d = _D()
+        self._ok(self.lib.qbx_dot(self.h, _dp(a.view(np.float64)), ctypes.byref(d)), "dot")
+        return d.value
 
     def stream(self) -> int:
         return self.lib.qbx_stream(self.h)
@@ -521,6 +591,78 @@ class Context:
 
     def get_coeffs_async(self, out_pinned: np.ndarray):
         self._ok(self.lib.qbx_get_coeffs_async(self.h, _dp(out_pinned)), "get_coeffs_async")
+
+
+class FourierTransform:
+    """qbx_ft: the reference's FourierTransform(basis, np0, np1, np2) on a
+    caller's basis (Miller indices in the caller's order) and grid."""
+
+    def __init__(self, hkl: np.ndarray, grid, real_basis: bool = True, device: int = 0):
+        self.lib = load()
+        idx = np.ascontiguousarray(np.asarray(hkl, np.int32).reshape(-1, 3))
+        self.ngw = idx.shape[0]
+        self.grid = tuple(int(x) for x in grid)
+        h = _P()
+        rc = self.lib.qbx_ft_create(ctypes.byref(h), device, self.ngw, _ip(idx),
+                                    int(real_basis), *self.grid)
+        if rc:
+            raise QbxError(f"qbx_ft_create failed with code {rc}")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.qbx_ft_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ok(self, rc, what):
+        if rc:
+            msg = self.lib.qbx_ft_last_error(self.h)
+            raise QbxError(f"{what}: code {rc}: {msg.decode() if msg else ''}")
+
+    @property
+    def N(self):
+        return self.grid[0] * self.grid[1] * self.grid[2]
+
+    def _c(self, c):
+        a = np.ascontiguousarray(c, np.complex128)
+        assert a.size == self.ngw
+        return a
+
+    def backward(self, c: np.ndarray, c2: Optional[np.ndarray] = None) -> np.ndarray:
+        """Complex grid (np2, np1, np0) of one band, or of c + i c2."""
+        f = np.empty(self.N, np.complex128)
+        a = self._c(c)
+        if c2 is None:
+            self._ok(self.lib.qbx_ft_backward(self.h, _dp(a.view(np.float64)),
+                                              _dp(f.view(np.float64))), "ft_backward")
+        else:
+            b = self._c(c2)
+            self._ok(self.lib.qbx_ft_backward2(self.h, _dp(a.view(np.float64)),
+                                               _dp(b.view(np.float64)),
+                                               _dp(f.view(np.float64))), "ft_backward2")
+        return f.reshape(self.grid[2], self.grid[1], self.grid[0])
+
+    def forward(self, f: np.ndarray, two: bool = False):
+        """Coefficients of a complex grid (1/N scaling); two=True unpacks
+        two real functions."""
+        g = np.ascontiguousarray(f, np.complex128).reshape(-1)
+        assert g.size == self.N
+        c1 = np.empty(self.ngw, np.complex128)
+        if not two:
+            self._ok(self.lib.qbx_ft_forward(self.h, _dp(g.view(np.float64)),
+                                             _dp(c1.view(np.float64))), "ft_forward")
+            return c1
+        c2 = np.empty(self.ngw, np.complex128)
+        self._ok(self.lib.qbx_ft_forward2(self.h, _dp(g.view(np.float64)),
+                                          _dp(c1.view(np.float64)), _dp(c2.view(np.float64))),
+                 "ft_forward2")
+        return c1, c2
 
 
 def scf_step_batch(contexts, stress: bool = False, forces: bool = False):

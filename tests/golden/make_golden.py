@@ -15,7 +15,10 @@ of the reference's BOSampleStepper; ref_<name>_wf.npz the <wavefunction>
 element the reference's Wavefunction::print writes (base64) for a band
 sample, with the coefficients it wrote; ref_<name>.npz of a k-point system
 (KPOINT_CASES) the PSDA run on its complex bases, with H*psi and the final
-coefficients of a few bands of each k point.
+coefficients of a few bands of each k point.  ref_si512_b32.npz is a 32-band
+sample of the 512-atom cell (its 140^3 grid and 2048 projectors),
+ref_si64_30.npz a 30-step PSDA run of the 64-atom PBE cell and
+ref_batch4.npz four systems of the 32-system batch.
 """
 from __future__ import annotations
 
@@ -36,10 +39,11 @@ NSAMPLE = 2048
 NBANDS_FULL = 4
 
 
-def make(name: str, nsteps: int, workdir: str) -> str:
-    s = systems.get(name)
+def make(name: str, nsteps: int, workdir: str, s=None, stress: bool = True) -> str:
+    if s is None:
+        s = systems.get(name)
     out = inputs.run_reference(s, workdir, nsteps, dump_steps=1, forces=True,
-                               stress=True, threads=os.cpu_count())
+                               stress=stress, threads=os.cpu_count())
     meta = out["meta"]
     e = out["energies"]
     rng = np.random.default_rng(12345)
@@ -63,8 +67,10 @@ def make(name: str, nsteps: int, workdir: str) -> str:
         final_c_bands=out["final_c"][:NBANDS_FULL, gidx],
         final_c_norm2=(np.abs(out["final_c"]) ** 2).sum(1),
         fion_first=out["fion0"], fion_last=out[f"fion{nsteps - 1}"],
-        sigma_first=out["sigma0"], sigma_last=out[f"sigma{nsteps - 1}"],
     )
+    if stress:
+        fx["sigma_first"] = out["sigma0"]
+        fx["sigma_last"] = out[f"sigma{nsteps - 1}"]
     for k in ("ekin", "eps", "enl", "ehart", "ecoul", "exc", "esr", "eself",
               "etotal", "eigenvalue_sum"):
         fx["e_" + k] = e[k]
@@ -90,6 +96,59 @@ def make_jd(name: str, nsteps: int, workdir: str) -> str:
 
 
 JD_CASES = {"si8": 6}
+
+# Band samples of a large cell: the 512-atom cell's 140^3 grid, its 2048
+# projectors and its plane-wave basis with only a few bands (name: system,
+# bands, steps), so that the length-140 kernels are pinned to the reference.
+SAMPLE_CASES = {"si512_b32": ("si512", 32, 3)}
+
+# Long PSDA trajectories, energies of every step and the final coefficients
+# of a few bands (name: system, steps)
+LONG_CASES = {"si64_30": ("si64", 30)}
+
+# Systems of the 32-system batch (their indices) and the steps run for each
+BATCH_PICK = (0, 9, 18, 27)
+BATCH_STEPS = 2
+
+
+def make_long(name: str, workdir: str) -> str:
+    """Energies of every step of a long PSDA run and the final coefficients
+    of a few bands at sampled G."""
+    sysname, nsteps = LONG_CASES[name]
+    s = systems.get(sysname)
+    out = inputs.run_reference(s, workdir, nsteps, threads=os.cpu_count())
+    e = out["energies"]
+    ngw = out["final_c"].shape[1]
+    gidx = np.sort(np.random.default_rng(12345).choice(ngw, 512, replace=False))
+    fx = dict(nsteps=nsteps, g_idx=gidx, final_c_bands=out["final_c"][:NBANDS_FULL, gidx],
+              final_c_norm2=(np.abs(out["final_c"]) ** 2).sum(1))
+    for k in ("ekin", "eps", "enl", "ehart", "ecoul", "exc", "esr", "eself",
+              "etotal", "eigenvalue_sum"):
+        fx["e_" + k] = e[k]
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), f"ref_{name}.npz")
+    np.savez_compressed(path, **fx)
+    return path
+
+
+def make_batch(workdir: str) -> str:
+    """A few systems of the 32-system batch (uneven cells, cutoffs and band
+    counts, LDA): energies of each of BATCH_STEPS steps and the forces of
+    the first step, keyed s<index>_."""
+    fx = dict(picked=np.array(BATCH_PICK), nsteps=BATCH_STEPS)
+    allsys = systems.batch()
+    for i in BATCH_PICK:
+        s = allsys[i]
+        sub = os.path.join(workdir, f"s{i}")
+        out = inputs.run_reference(s, sub, BATCH_STEPS, dump_steps=1, forces=True,
+                                   threads=os.cpu_count())
+        e = out["energies"]
+        for k in ("ekin", "eps", "enl", "ehart", "ecoul", "exc", "esr", "eself",
+                  "etotal", "eigenvalue_sum"):
+            fx[f"s{i}_e_{k}"] = e[k]
+        fx[f"s{i}_fion_first"] = out["fion0"]
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ref_batch4.npz")
+    np.savez_compressed(path, **fx)
+    return path
 
 # MD: (ionic steps, electronic steps per ionic step, dt in a.u.)
 MD_CASES = {"si8": (3, 2, 20.0)}
@@ -199,10 +258,19 @@ if __name__ == "__main__":
     import tempfile
     names = sys.argv[1:] or (list(CASES) + [n + "_jd" for n in JD_CASES]
                              + [n + "_md" for n in MD_CASES] + [n + "_gs" for n in GS_CASES]
-                             + [n + "_wf" for n in WF_CASES] + list(KPOINT_CASES))
+                             + [n + "_wf" for n in WF_CASES] + list(KPOINT_CASES)
+                             + list(SAMPLE_CASES) + list(LONG_CASES) + ["batch4"])
     for n in names:
         with tempfile.TemporaryDirectory() as td:
-            if n in KPOINT_CASES:
+            if n in SAMPLE_CASES:
+                sysname, nb, nsteps = SAMPLE_CASES[n]
+                print(make(n, nsteps, td, s=systems.get(sysname).band_sample(nb),
+                           stress=False))
+            elif n in LONG_CASES:
+                print(make_long(n, td))
+            elif n == "batch4":
+                print(make_batch(td))
+            elif n in KPOINT_CASES:
                 print(make_kpoint(n, KPOINT_CASES[n], td))
             elif n.endswith("_wf"):
                 print(make_wf(n[:-3], td))

@@ -52,6 +52,44 @@ def test_density_static_matches_update_density(name, precision):
     ctx.close()
 
 
+@pytest.mark.parametrize("precision", [capi.FP64, capi.MIXED])
+def test_density_static_odd_band_count_allocates_nothing(precision):
+    """nst = nbands - 1 (odd): the last band pair has one band.  The result
+    must equal qbx_update_density of a context holding those nst bands, and
+    after the first call (which may load the library's kernels) a call must
+    leave the device's free memory unchanged."""
+    import dataclasses
+    import torch
+    s = systems.si64()
+    ctx = capi.from_system(s, precision=precision)
+    ctx.set_coeff_order(None)
+    c_all = ctx.get_coeffs()
+    nst = s.nbands - 1
+    s_odd = dataclasses.replace(s, nbands=nst, nel_override=2 * nst)
+    ref_ctx = capi.from_system(s_odd, precision=precision, coeffs=None, gram=False)
+    ref_ctx.set_coeff_order(None)
+    ref_ctx.set_coeffs(c_all[:nst])
+    ref_ctx.update_density()
+    ref = ref_ctx.density()
+    ref_ctx.close()
+    c = torch.from_numpy(c_all[:nst].view(np.float64).copy()).cuda()
+    rho = torch.empty(ref.size, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    tol = (1e-12 if precision == capi.FP64 else 2e-6) * np.abs(ref).max()
+    ctx.density_static(c.data_ptr(), nst, rho.data_ptr())
+    for _ in range(2):
+        rho.fill_(np.nan)
+        torch.cuda.synchronize()
+        free0, _ = torch.cuda.mem_get_info()
+        ctx.density_static(c.data_ptr(), nst, rho.data_ptr())
+        free1, _ = torch.cuda.mem_get_info()
+        assert free1 == free0, (free0, free1)
+        np.testing.assert_allclose(rho.cpu().numpy(), ref, rtol=0, atol=tol)
+    with pytest.raises(ValueError, match="occupations"):
+        ctx.density_static(c.data_ptr(), nst, rho.data_ptr(), np.full(s.nbands, 2.0))
+    ctx.close()
+
+
 def test_density_static_rejects_bad_arguments():
     s = systems.si8()
     ctx = capi.from_system(s)
