@@ -78,21 +78,26 @@ def write_system(sysdef, workdir: str, c: Optional[np.ndarray] = None) -> str:
     return path
 
 
+GPU_FT_DRIVER = os.path.join(HERE, "_ref", "ref_driver_gpuft")
+
+
 def run_reference(sysdef, workdir: str, nsteps: int, dump_steps: int = 0,
                   forces: bool = False, wf_dyn: str = "PSDA",
-                  threads: Optional[int] = None, c=None, stress: bool = False) -> Dict:
+                  threads: Optional[int] = None, c=None, stress: bool = False,
+                  driver: str = REF_DRIVER) -> Dict:
     """Run the compiled reference on sysdef; returns parsed outputs.  With
     stress=True (implies forces) the stress tensor of the force steps is
-    read as out["sigma"][step]."""
-    if not os.path.exists(REF_DRIVER):
-        raise FileNotFoundError("oracle/_ref/ref_driver not built "
-                                "(make -C oracle)")
+    read as out["sigma"][step].  driver=GPU_FT_DRIVER runs the same
+    reference build with the GPU FourierTransform of qbox-public_b200/qbox_shim
+    in place of its own (make -C oracle gpu_ft)."""
+    if not os.path.exists(driver):
+        raise FileNotFoundError(f"{driver} not built (make -C oracle)")
     path = write_system(sysdef, workdir, c)
     env = dict(os.environ)
     if threads:
         env["OMP_NUM_THREADS"] = str(threads)
         env["OPENBLAS_NUM_THREADS"] = str(threads)
-    subprocess.run([REF_DRIVER, path, str(nsteps), workdir, str(dump_steps),
+    subprocess.run([driver, path, str(nsteps), workdir, str(dump_steps),
                     "2" if stress else ("1" if forces else "0"), wf_dyn], check=True, env=env,
                    stdout=subprocess.DEVNULL)
     return load_outputs(workdir)
