@@ -196,9 +196,10 @@ def run_reference_arm(args):
     line = {
         "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": world, "steps": 1,
         "warmup": 0, "ms_per_step": ms, "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "scaling": "strong" if args.shard else "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
         "impl": "reference",
-        "config": bench_config(world),
+        "config": bench_config(world, args.shard),
         "precision": "FP64 (the reference's CPU build, single task, OpenMP + OpenBLAS threads)",
         "steps_requested": args.steps, "warmup_requested": args.warmup,
         "cpu_baseline": {"value": ms, "unit": "ms", "cores": threads, "kind": "reference",
@@ -208,11 +209,14 @@ def run_reference_arm(args):
     print(json.dumps(line))
 
 
-def bench_config(world: int) -> dict:
+def bench_config(world: int, shard: bool = False) -> dict:
     """The workload both arms run (identical in both JSON lines)."""
+    par = "single GPU"
+    if world > 1:
+        par = f"band pairs sharded over {world} GPUs" if shard else "replicas"
     return {"workload": WORKLOAD,
             "l2": "inputs larger than L2 (1.19 GB wavefunctions per step)",
-            "parallelism": "replicas" if world > 1 else "single GPU"}
+            "parallelism": par}
 
 
 # ------------------------------------------------------------ our arm
@@ -283,12 +287,24 @@ def run_ours(args):
     def max_over_ranks(x):
         return replicas.max_over_ranks(x, device=f"cuda:{dev}")
 
+    sharded = args.shard and world > 1
+
+    def maybe_shard(ctx):
+        # --shard: the band pairs of the one cell split over the ranks (NCCL
+        # allreduce of the density, broadcast of the H*psi blocks); the
+        # sharded step runs eagerly
+        if sharded:
+            from qbx import sharding
+            sharding.shard_band_pairs(ctx, device=f"cuda:{dev}")
+        else:
+            ctx.set_step_graph(True)
+
     # ---- mixed precision (headline)
     mix = capi.from_system(s, device=dev, precision=capi.MIXED, coeffs=c0)
     mix.scf_step()
     tuning_mix = mix.autotune()
     # the step runs as a captured CUDA graph (captured during the warm-up)
-    mix.set_step_graph(True)
+    maybe_shard(mix)
     for _ in range(args.warmup):
         mix.scf_step()
     clocks = ClockSampler(dev)
@@ -346,7 +362,7 @@ def run_ours(args):
     f64 = capi.from_system(s, device=dev, precision=capi.FP64, coeffs=c0)
     f64.scf_step()
     f64.autotune()
-    f64.set_step_graph(True)
+    maybe_shard(f64)
     for _ in range(args.warmup):
         f64.scf_step()
     ms_f64, r_f64, _ = timed(f64, args.steps)
@@ -434,7 +450,7 @@ def run_ours(args):
 
         ms_md, out_md = md_leg(mix)
         f64md = capi.from_system(s, device=dev, precision=capi.FP64, coeffs=c_md, gram=False)
-        f64md.set_step_graph(True)
+        maybe_shard(f64md)
         ms_md64, out_md64 = md_leg(f64md)
         f64md.close()
         ec = out_md["ionic"][:, 2]
@@ -568,12 +584,13 @@ def run_ours(args):
         line = {
             "metric": METRIC, "value": ms_mix, "unit": "ms", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mix,
-            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "higher_is_better": False, "scaling": "strong" if sharded else "weak",
+            "vs_baseline": None,
             "dtype": ("mixed: FP32 FFTs and real-space work; BF16x3 (inner products) and "
                       "TF32x3 (rotation) split products on tcgen05 with FP32 accumulation; "
                       "FP64 Cholesky, polar, phases and reductions"),
             "data": "synthetic",
-            "config": bench_config(world),
+            "config": bench_config(world, sharded),
             "precision": "mixed",
             "step_graph": {"captured": graphs, "launches": graph_launches, "note": graph_note,
                            "eager_ms_per_step": ms_mix_eager},
@@ -626,6 +643,8 @@ def run_profile_case(args):
     ctx.scf_step()
     if args.profile_tune:
         ctx.autotune()
+    if args.profile_graph:
+        ctx.set_step_graph(True)     # the profiled step is the captured graph
     for _ in range(args.warmup):
         ctx.scf_step()
     ctx.synchronize()
@@ -650,11 +669,16 @@ def main():
     ap.add_argument("--kpoint-steps", type=int, default=3,
                     help="timed steps of the two-k-point si64 measurement (0: skip)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--shard", action="store_true",
+                    help="with several GPUs: split the band pairs of the one cell over them "
+                         "(strong scaling) instead of running independent replicas")
     ap.add_argument("--profile-bands", type=int, default=0,
                     help="run only warm-up + one mixed step of si512 with this many bands "
                          "(a case for profilers); prints nothing")
     ap.add_argument("--profile-tune", action="store_true",
                     help="with --profile-bands: autotune the FFT configuration first")
+    ap.add_argument("--profile-graph", action="store_true",
+                    help="with --profile-bands: profile the captured step (graph launch)")
     args = ap.parse_args()
     if args.profile_bands:
         run_profile_case(args)

@@ -379,6 +379,31 @@ int qbx_ortho_align(qbx_context* ctx, const double* c_sd);
  * +G and -G once each, *d = 2 sum - sum of the G=0 terms. */
 int qbx_dot(qbx_context* ctx, const double* c_sd, double* d);
 
+/* ---- Band pairs of one SlaterDet split over GPUs: the reference's state
+ * axis (nstb of MPIdata::set, src/MPIdata.cpp:55-121, the columns of c_ in
+ * src/SlaterDet.cpp:84-93) for the FFT work of the step.  Each of nranks
+ * processes (one GPU each) builds the same context (cell, species, atoms,
+ * coefficients) and calls qbx_set_band_shard with its rank and the group's
+ * NCCL unique id, which one rank makes with qbx_nccl_unique_id and the
+ * caller passes to the others by its own means.  From then on each GPU
+ * transforms a contiguous range of about npairs/nranks band pairs in
+ * update_density and in the local part of H*psi; the density is summed over
+ * the GPUs (ncclAllReduce, src/ChargeDensity.cpp:166) and the H*psi bands
+ * are broadcast from their owners, so every GPU continues the step with the
+ * whole of both and computes the same products on the same data.  Every
+ * rank must make the same calls in the same order.  Gamma only; exclusive
+ * with qbx_set_step_graph.  nranks = 1 with an id runs the collectives on a
+ * group of one; nranks = 1 with id = NULL switches sharding off.  libnccl.so.2
+ * is loaded at the first call (error 70 if it cannot be). */
+#define QBX_NCCL_ID_BYTES 128
+int qbx_nccl_unique_id(unsigned char id[QBX_NCCL_ID_BYTES]);
+int qbx_set_band_shard(qbx_context* ctx, int rank, int nranks,
+                       const unsigned char id[QBX_NCCL_ID_BYTES]);
+/* Host-only: the band pairs [first_pair, end_pair) that rank of nranks
+ * transforms for nst bands (pair p = bands 2p and 2p+1): contiguous ranges
+ * whose sizes differ by one at most. */
+int qbx_shard_pairs(int nst, int rank, int nranks, int* first_pair, int* end_pair);
+
 /* Size of the device array behind qbx_density_static: 32 MiB. */
 #define QBX_STATIC_SCRATCH_BYTES ((size_t)32 << 20)
 

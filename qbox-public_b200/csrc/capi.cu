@@ -386,6 +386,10 @@ void qbx_destroy(qbx_context* h) {
   if (!h) return;
   cudaSetDevice(h->c.device);
   if (h->c.stream) cudaStreamSynchronize(h->c.stream);
+  try {
+    shard_release(h->c);
+  } catch (...) {
+  }
   free_atoms(h->c);
   free_cell(h->c);
   dfree(h->d_perm);
@@ -1059,6 +1063,7 @@ int qbx_polar(qbx_context* h, double* x, double tol, int maxiter, int graph, int
 
 int qbx_set_step_graph(qbx_context* h, int on) {
   return guarded(h, [&](Context& c) {
+    QBX_REQUIRE(!on || !c.shard_comm, 1, "captured steps and band sharding are exclusive");
     c.step_graph = on != 0;
     c.graph_note.clear();
     drop_graphs(c);

@@ -821,16 +821,18 @@ static bool staged_fast(Context& ctx, int op, const double* c, const double* v, 
     a.v = ctx.d_vr32;
   }
   const size_t limit = (size_t)max_smem_optin(ctx.device);
-  const int npairs = (ctx.nst + 1) / 2;
+  int plo = 0, phi = 0;
+  shard_pairs(ctx, plo, phi);            // this GPU's band pairs
+  const int npairs = phi - plo;
   const size_t per_pair = (ctx.precision == MIXED ? sizeof(float2) : sizeof(double2)) *
                           (size_t)g.n2 * g.nvec;
-  int batch = (int)std::min<size_t>(npairs, ctx.zfast_bytes / per_pair);
+  int batch = (int)std::min<size_t>(std::max(npairs, 1), ctx.zfast_bytes / per_pair);
   if (ctx.fast_batch > 0) batch = std::min(batch, ctx.fast_batch);
   QBX_REQUIRE(batch >= 1, 21, "stick buffer of the specialised FFTs holds no band pair");
   bool first = true;
-  for (int p0 = 0; p0 < npairs; p0 += batch) {
+  for (int p0 = plo; p0 < phi; p0 += batch) {
     a.pair0 = p0;
-    a.npairs = std::min(batch, npairs - p0);
+    a.npairs = std::min(batch, phi - p0);
     const bool ok = fast_staged_a(ctx, a, limit) || fast_staged_b(ctx, a, limit);
     if (!ok) {
       QBX_REQUIRE(first, 21, "specialised FFT kernels unavailable after the first batch");
@@ -848,9 +850,10 @@ static bool staged_fast(Context& ctx, int op, const double* c, const double* v, 
 static void staged(Context& ctx, int op, const double* c, const double* v, double* rho,
                    const double* w, double* hc) {
   if (staged_fast(ctx, op, c, v, rho, w, hc)) return;
-  const int npairs = (ctx.nst + 1) / 2;
-  for (int p0 = 0; p0 < npairs; p0 += ctx.pair_batch) {
-    const int np = std::min(ctx.pair_batch, npairs - p0);
+  int plo = 0, phi = 0;
+  shard_pairs(ctx, plo, phi);
+  for (int p0 = plo; p0 < phi; p0 += ctx.pair_batch) {
+    const int np = std::min(ctx.pair_batch, phi - p0);
     if (ctx.precision == MIXED)
       staged_batch<float>(ctx, op, c, v, rho, w, hc, p0, np);
     else
@@ -858,13 +861,18 @@ static void staged(Context& ctx, int op, const double* c, const double* v, doubl
   }
 }
 
+// With the band pairs split over GPUs (qbx_set_band_shard) each GPU
+// transforms its own pairs; the density is then summed over the GPUs and
+// the H*psi blocks gathered, so every GPU continues with the whole of both.
 void launch_density(Context& ctx, const double* c, double* rho) {
   QBX_CUDA(cudaMemsetAsync(rho, 0, ctx.N() * sizeof(double), ctx.stream));
   staged(ctx, OP_DENSITY, c, nullptr, rho, density_weights(ctx), nullptr);
+  if (ctx.shard_comm) shard_sum(ctx, rho, ctx.N());
 }
 
 void launch_vpsi(Context& ctx, const double* c, const double* v, double* hc) {
   staged(ctx, OP_VPSI, c, v, nullptr, nullptr, hc);
+  if (ctx.shard_comm) shard_gather_bands(ctx, hc);
 }
 
 // full-grid transform of `grid` on the geometry of d (sizes, twiddles)

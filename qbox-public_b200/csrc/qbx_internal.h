@@ -408,6 +408,11 @@ struct Context {
   int tc_corr_mul = 8;          // tcgen05 GEMM: hi*lo + lo*hi chains this many times longer,
                                 // in accumulators of their own (0: in the hi*hi chain)
   int tc_epw = 8;               // tcgen05 GEMM: epilogue warps (4 or 8)
+
+  // band pairs split over GPUs (qbx_set_band_shard): this GPU's rank among
+  // shard_n, and the NCCL communicator (ncclComm_t) of the group
+  int shard_rank = 0, shard_n = 1;
+  void* shard_comm = nullptr;
   void* d_acc32 = nullptr;      // FP32 product accumulator
   size_t acc32_elems = 0;
   void* cs_hi[2] = {nullptr, nullptr};   // splits of C (0: at energy, 1: after the step)
@@ -593,6 +598,13 @@ void launch_nl_forces(Context& ctx, double* fion);
 // stress tensor of the state of the last energy(): SLOT_STRESS; then
 // finish_stress gives ctx.sigma, ctx.sigma_parts
 void compute_stress(Context& ctx);
+// band-pair sharding (shard.cu): this GPU's pairs [lo, hi); the sum of a
+// device array over the GPUs; the gather of every GPU's bands of a
+// band-major K x nst block; the communicator's release
+void shard_pairs(const Context& ctx, int& lo, int& hi);
+void shard_sum(Context& ctx, double* x, size_t n);
+void shard_gather_bands(Context& ctx, double* x);
+void shard_release(Context& ctx);
 void compute_stress_nl(Context& ctx);            // the nonlocal part alone (SS_ENL slots)
 void nl_stress_part(const Context& ctx, double enl, double* sigma_enl);   // after readback
 // NonLocalPotential::energy on its own: E_nl into its slot and, with hpsi,

@@ -46,7 +46,10 @@ SYMBOLS = (
     "qbx_ft_create", "qbx_ft_destroy", "qbx_ft_last_error", "qbx_ft_backward",
     "qbx_ft_backward2", "qbx_ft_forward", "qbx_ft_forward2", "qbx_compute_density",
     "qbx_rs_mul_add", "qbx_nonlocal_energy", "qbx_ortho_align", "qbx_dot",
+    "qbx_nccl_unique_id", "qbx_set_band_shard", "qbx_shard_pairs",
 )
+
+NCCL_ID_BYTES = 128
 
 _lib = None
 
@@ -146,6 +149,9 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "qbx_nonlocal_energy": (_I, [_P, _I, _DP, _I, _DP, _I, _DP, _DP]),
         "qbx_ortho_align": (_I, [_P, _DP]),
         "qbx_dot": (_I, [_P, _DP, _DP]),
+        "qbx_nccl_unique_id": (_I, [ctypes.c_char_p]),
+        "qbx_set_band_shard": (_I, [_P, _I, _I, ctypes.c_char_p]),
+        "qbx_shard_pairs": (_I, [_I, _I, _I, _IP, _IP]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -583,6 +589,13 @@ class Context:
         self._ok(self.lib.qbx_dot(self.h, _dp(a.view(np.float64)), ctypes.byref(d)), "dot")
         return d.value
 
+    def set_band_shard(self, rank: int, nranks: int, nccl_id: Optional[bytes]):
+        """qbx_set_band_shard: this GPU transforms its share of the band
+        pairs; densities and H*psi blocks are exchanged over NCCL."""
+        if nccl_id is not None:
+            assert len(nccl_id) == NCCL_ID_BYTES
+        self._ok(self.lib.qbx_set_band_shard(self.h, rank, nranks, nccl_id), "set_band_shard")
+
     def stream(self) -> int:
         return self.lib.qbx_stream(self.h)
 
@@ -591,6 +604,27 @@ class Context:
 
     def get_coeffs_async(self, out_pinned: np.ndarray):
         self._ok(self.lib.qbx_get_coeffs_async(self.h, _dp(out_pinned)), "get_coeffs_async")
+
+
+def nccl_unique_id() -> bytes:
+    """qbx_nccl_unique_id: a new NCCL group id (made on one rank, passed to
+    the others by the caller)."""
+    lib = load()
+    buf = ctypes.create_string_buffer(NCCL_ID_BYTES)
+    rc = lib.qbx_nccl_unique_id(buf)
+    if rc:
+        raise QbxError(f"qbx_nccl_unique_id failed with code {rc}")
+    return buf.raw
+
+
+def shard_pairs(nst: int, rank: int, nranks: int):
+    """qbx_shard_pairs: the band pairs [first, end) of rank among nranks."""
+    lib = load()
+    a, b = _I(), _I()
+    rc = lib.qbx_shard_pairs(nst, rank, nranks, ctypes.byref(a), ctypes.byref(b))
+    if rc:
+        raise QbxError(f"qbx_shard_pairs: code {rc}")
+    return a.value, b.value
 
 
 class FourierTransform:
