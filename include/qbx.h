@@ -374,6 +374,14 @@ int qbx_nonlocal_energy(qbx_context* ctx, int compute_hpsi, double* dc, int comp
  * stepper's last-step buffer, so the PSDA history restarts (as after
  * qbx_set_coeffs). */
 int qbx_ortho_align(qbx_context* ctx, const double* c_sd);
+/* Wavefunction::diag(dwf, eigvec) (src/Wavefunction.h:115,
+ * src/Wavefunction.cpp:834-917) at Gamma: the subspace Hamiltonian
+ * h = 2 C^T (H C) - c0 hc0^T from the H*C of the last qbx_energy with
+ * compute_hpsi, its nst eigenvalues (ascending) into eig (HOST); with
+ * eigvec != 0 the context's C becomes C Z (Z the eigenvectors) and its H*C
+ * the previous C, as the reference overwrites dwf; the PSDA history
+ * restarts.  FP64 products in both precisions. */
+int qbx_diag(qbx_context* ctx, int eigvec, double* eig);
 /* SlaterDet::dot(const SlaterDet& sd) (src/SlaterDet.h:77,
  * src/SlaterDet.cpp:1122-1153) at Gamma: tr(C^T C_sd) over the real view,
  * +G and -G once each, *d = 2 sum - sum of the G=0 terms. */

@@ -846,6 +846,18 @@ class ElectronicStep:
         self.sigma = sum(parts.values())
         return self.sigma
 
+    def diag(self, eigvec=True):
+        """src/Wavefunction.cpp:834-917 (real basis): h = 2 C^T HC - c0 hc0^T,
+        eigenvalues by syev; with eigvec C <- C Z and dwf (hc) <- the old
+        C.  Returns the eigenvalues."""
+        h = self.real_dot(self.c, self.hc)
+        w, z = np.linalg.eigh(h)
+        if eigvec:
+            old = self.c.copy()
+            self.c = z.T @ old
+            self.hc = old
+        return w
+
     def eigenvalue_sum(self):
         """Wavefunction::dot (src/SlaterDet.cpp:1122-1153)."""
         d = 2.0 * (np.conj(self.c) * self.hc).real.sum()

@@ -22,6 +22,10 @@
 // reference's Wavefunction::print (src/Wavefunction.cpp:919-962,
 // SlaterDet::print src/SlaterDet.cpp:1382-1549, base64 encoding) to wf.xml
 // and its coefficients to final_c.bin.
+// wf_dyn = DIAG runs the PSDA steps, then once more update_density,
+// update_vhxc and energy(true) and the subspace diagonalisation
+// Wavefunction::diag(dwf, true) (src/Wavefunction.cpp:834-917); it writes
+// the eigenvalues (diag_eig.txt) and the rotated coefficients (final_c.bin).
 // wf_dyn = MD runs the reference's own BOSampleStepper::step(nsteps)
 // (src/BOSampleStepper.cpp:165-1428) with atoms_dyn = MD, wf_dyn = PSDA,
 // nitscf electronic steps per ionic step, nite = 0 and the time step dt
@@ -426,6 +430,18 @@ int main(int argc, char** argv)
        << ef.etotal() << " " << eigsum << " " << (t1-t0) << " " << (t2-t1)
        << " " << (t3-t2) << " " << (t4-t3) << "\n";
     eo.flush();
+  }
+  if ( wf_dyn == "DIAG" )
+  {
+    cd.update_density();
+    ef.update_vhxc(false);
+    ef.energy(true, dwf, false, fion, false, sigma);
+    s.wf.diag(dwf, true);
+    ofstream ev((outdir + "/diag_eig.txt").c_str());
+    ev << setprecision(17);
+    const vector<double>& eig = s.wf.sd(0,0)->eig();
+    for ( size_t n = 0; n < eig.size(); n++ )
+      ev << eig[n] << "\n";
   }
   // final wavefunctions
   for ( int ikp = 0; ikp < nkp; ikp++ )

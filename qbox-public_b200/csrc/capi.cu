@@ -1449,6 +1449,23 @@ int qbx_ortho_align(qbx_context* h, const double* c_ref) {
   });
 }
 
+int qbx_diag(qbx_context* h, int eigvec, double* eig) {
+  return guarded(h, [&](Context& c) {
+    check_ready(c, false);
+    QBX_REQUIRE(c.kpts.empty(), 1, "qbx_diag works on the Gamma SlaterDet");
+    QBX_REQUIRE(eig, 1, "null eigenvalue array");
+    double* w = dalloc<double>(c.nst);
+    try {
+      diag(c, eigvec != 0, w);
+      QBX_CUDA(cudaMemcpy(eig, w, sizeof(double) * c.nst, cudaMemcpyDeviceToHost));
+    } catch (...) {
+      dfree(w);
+      throw;
+    }
+    dfree(w);
+  });
+}
+
 int qbx_dot(qbx_context* h, const double* c_other, double* d) {
   return guarded(h, [&](Context& c) {
     check_ready(c, false);

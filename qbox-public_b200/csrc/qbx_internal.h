@@ -610,6 +610,9 @@ void nl_stress_part(const Context& ctx, double enl, double* sigma_enl);   // aft
 // NonLocalPotential::energy on its own: E_nl into its slot and, with hpsi,
 // the nonlocal part of H*C written to out (device, K x nst)
 void nonlocal_only(Context& ctx, bool hpsi, double* out);
+// Wavefunction::diag: eigenvalues of C^T H C into w (device, nst); with
+// eigvec C <- C Z and H*C <- the previous C
+void diag(Context& ctx, bool eigvec, double* w);
 void launch_identity_axpy(Context& ctx, double* t, const double* q, int n,
                           double alpha);       // t = I + alpha*q
 void launch_symmetrize_lower(Context& ctx, double* q, int n);

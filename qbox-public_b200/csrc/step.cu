@@ -526,6 +526,47 @@ void psda_update(Context& ctx) {
   ctx.extrapolate = true;
 }
 
+// Wavefunction::diag(dwf, eigvec) (src/Wavefunction.cpp:834-917), real
+// basis: h = 2 C^T (H C) - c0 hc0^T (the H C of the last energy()), its
+// eigenvalues by syevd into w (device, nst); with eigvec the eigenvectors Z
+// rotate C <- C Z and H*C takes the previous C, as the reference overwrites
+// dwf with it.  The products are FP64 in both precisions.
+void diag(Context& ctx, bool eigvec, double* w) {
+  ProfScope ps(ctx, "diag");
+  const int n = ctx.nst, K = 2 * ctx.wb.ng;
+  const double one = 1.0, two = 2.0, zero = 0.0;
+  double* h = ctx.d_nn;
+  QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, ctx.d_c, K, ctx.d_hc, K,
+                       &zero, h, n));
+  launch_rank1_fix(ctx, h, n, ctx.d_c, K, ctx.d_hc, K, n, n, -1.0, false);
+  int lwork = 0;
+  const cusolverEigMode_t mode = eigvec ? CUSOLVER_EIG_MODE_VECTOR : CUSOLVER_EIG_MODE_NOVECTOR;
+  QBX_SOLVER(cusolverDnDsyevd_bufferSize(ctx.solver, mode, CUBLAS_FILL_MODE_LOWER, n, h, n, w,
+                                         &lwork));
+  double* work = dalloc<double>(std::max(1, lwork));
+  try {
+    QBX_SOLVER(cusolverDnDsyevd(ctx.solver, mode, CUBLAS_FILL_MODE_LOWER, n, h, n, w, work, lwork,
+                                ctx.d_info));
+    int info = 0;
+    QBX_CUDA(cudaMemcpyAsync(&info, ctx.d_info, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+    QBX_CUDA(cudaStreamSynchronize(ctx.stream));
+    QBX_REQUIRE(info == 0, 41, "syevd of the subspace Hamiltonian failed (info=" +
+                                   std::to_string(info) + ")");
+    if (eigvec) {
+      QBX_CUDA(cudaMemcpyAsync(ctx.d_hc, ctx.d_c, sizeof(double) * (size_t)K * n,
+                               cudaMemcpyDeviceToDevice, ctx.stream));
+      QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, K, n, n, &one, ctx.d_hc, K, h, n,
+                           &zero, ctx.d_c, K));
+      ctx.extrapolate = false;
+    }
+    QBX_CUDA(cudaStreamSynchronize(ctx.stream));
+  } catch (...) {
+    dfree(work);
+    throw;
+  }
+  dfree(work);
+}
+
 // JDWavefunctionStepper::update (src/JDWavefunctionStepper.cpp:47-376),
 // real basis: Y = C, HY = H C; residual R = HY - Y (Y^T HY); Z = -K R made
 // orthogonal to Y and orthonormal (gram); H Z by a second energy(); the

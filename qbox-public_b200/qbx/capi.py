@@ -46,7 +46,7 @@ SYMBOLS = (
     "qbx_ft_create", "qbx_ft_destroy", "qbx_ft_last_error", "qbx_ft_backward",
     "qbx_ft_backward2", "qbx_ft_forward", "qbx_ft_forward2", "qbx_compute_density",
     "qbx_rs_mul_add", "qbx_nonlocal_energy", "qbx_ortho_align", "qbx_dot",
-    "qbx_nccl_unique_id", "qbx_set_band_shard", "qbx_shard_pairs",
+    "qbx_nccl_unique_id", "qbx_set_band_shard", "qbx_shard_pairs", "qbx_diag",
 )
 
 NCCL_ID_BYTES = 128
@@ -152,6 +152,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "qbx_nccl_unique_id": (_I, [ctypes.c_char_p]),
         "qbx_set_band_shard": (_I, [_P, _I, _I, ctypes.c_char_p]),
         "qbx_shard_pairs": (_I, [_I, _I, _I, _IP, _IP]),
+        "qbx_diag": (_I, [_P, _I, _DP]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -580,6 +581,13 @@ class Context:
         a = np.ascontiguousarray(c_ref, np.complex128)
         assert a.shape == (self.nst, self.ngw)
         self._ok(self.lib.qbx_ortho_align(self.h, _dp(a.view(np.float64))), "ortho_align")
+
+    def diag(self, eigvec: bool = True) -> np.ndarray:
+        """Wavefunction::diag after energy(hpsi=True): the eigenvalues of
+        C^T H C; with eigvec C becomes its eigenvectors."""
+        w = np.zeros(self.nst)
+        self._ok(self.lib.qbx_diag(self.h, int(eigvec), _dp(w)), "diag")
+        return w
 
     def dot(self, c_other: np.ndarray) -> float:
         """SlaterDet::dot(sd) at Gamma."""

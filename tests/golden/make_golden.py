@@ -18,7 +18,8 @@ sample, with the coefficients it wrote; ref_<name>.npz of a k-point system
 coefficients of a few bands of each k point.  ref_si512_b32.npz is a 32-band
 sample of the 512-atom cell (its 140^3 grid and 2048 projectors),
 ref_si64_30.npz a 30-step PSDA run of the 64-atom PBE cell and
-ref_batch4.npz four systems of the 32-system batch.
+ref_batch4.npz four systems of the 32-system batch; ref_si64_diag.npz the
+subspace diagonalisation (Wavefunction::diag) after three PSDA steps.
 """
 from __future__ import annotations
 
@@ -105,6 +106,26 @@ SAMPLE_CASES = {"si512_b32": ("si512", 32, 3)}
 # Long PSDA trajectories, energies of every step and the final coefficients
 # of a few bands (name: system, steps)
 LONG_CASES = {"si64_30": ("si64", 30)}
+
+# Subspace diagonalisation after a few PSDA steps (name: steps)
+DIAG_CASES = {"si64": 3}
+
+
+def make_diag(name: str, workdir: str) -> str:
+    """Wavefunction::diag(dwf, true) after the PSDA steps: eigenvalues, and
+    the rotated coefficients of a few bands at sampled G."""
+    nsteps = DIAG_CASES[name]
+    s = systems.get(name)
+    out = inputs.run_reference(s, workdir, nsteps, wf_dyn="DIAG", threads=os.cpu_count())
+    eig = np.loadtxt(os.path.join(workdir, "diag_eig.txt"))
+    fc = out["final_c"]
+    gidx = np.sort(np.random.default_rng(12345).choice(fc.shape[1], 512, replace=False))
+    fx = dict(nsteps=nsteps, eig=eig, g_idx=gidx, final_c_bands=fc[:, gidx],
+              e_etotal=out["energies"]["etotal"])
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), f"ref_{name}_diag.npz")
+    np.savez_compressed(path, **fx)
+    return path
+
 
 # Systems of the 32-system batch (their indices) and the steps run for each
 BATCH_PICK = (0, 9, 18, 27)
@@ -259,7 +280,8 @@ if __name__ == "__main__":
     names = sys.argv[1:] or (list(CASES) + [n + "_jd" for n in JD_CASES]
                              + [n + "_md" for n in MD_CASES] + [n + "_gs" for n in GS_CASES]
                              + [n + "_wf" for n in WF_CASES] + list(KPOINT_CASES)
-                             + list(SAMPLE_CASES) + list(LONG_CASES) + ["batch4"])
+                             + list(SAMPLE_CASES) + list(LONG_CASES) + ["batch4"]
+                             + [n + "_diag" for n in DIAG_CASES])
     for n in names:
         with tempfile.TemporaryDirectory() as td:
             if n in SAMPLE_CASES:
@@ -270,6 +292,8 @@ if __name__ == "__main__":
                 print(make_long(n, td))
             elif n == "batch4":
                 print(make_batch(td))
+            elif n.endswith("_diag"):
+                print(make_diag(n[:-5], td))
             elif n in KPOINT_CASES:
                 print(make_kpoint(n, KPOINT_CASES[n], td))
             elif n.endswith("_wf"):

@@ -150,3 +150,26 @@ def test_ortho_align_and_dot():
     es.ortho_align(c_ref)
     np.testing.assert_allclose(ctx.get_coeffs(), es.c, atol=1e-10)
     ctx.close()
+
+
+def test_diag_matches_reference():
+    """Wavefunction::diag(dwf, true) after three PSDA steps of the 64-atom
+    cell (tests/golden/ref_si64_diag.npz, the reference's own run):
+    eigenvalues to 1e-10 Ha, rotated coefficients to 1e-7 up to the sign of
+    each band (the smallest eigenvalue gap is 7e-4 Ha)."""
+    from conftest import golden
+    g = golden("si64_diag")
+    s = systems.si64()
+    ctx = capi.from_system(s)
+    for _ in range(int(g["nsteps"])):
+        ctx.scf_step()
+    ctx.update_density()
+    ctx.update_vhxc()
+    ctx.energy(hpsi=True)
+    w = ctx.diag(eigvec=True)
+    np.testing.assert_allclose(w, g["eig"], atol=1e-10)
+    c = ctx.get_coeffs()[:, g["g_idx"]]
+    ref = g["final_c_bands"]
+    sign = np.sign((c.conj() * ref).sum(1).real)
+    np.testing.assert_allclose(c * sign[:, None], ref, atol=1e-7)
+    ctx.close()

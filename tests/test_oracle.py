@@ -236,3 +236,21 @@ def test_oracle_kpoints_match_reference(name):
         np.testing.assert_allclose(kp.c[:4, gi], g[f"k{ik}_final_c_bands"], atol=1e-12)
         np.testing.assert_allclose((np.abs(kp.c) ** 2).sum(1), g[f"k{ik}_final_c_norm2"],
                                    rtol=1e-12)
+
+
+def test_oracle_diag_matches_reference():
+    """ElectronicStep.diag against the reference's Wavefunction::diag after
+    three PSDA steps of the 64-atom cell: eigenvalues 1e-10 Ha, rotated
+    coefficients 1e-7 up to the sign of each band."""
+    g = golden("si64_diag")
+    es = qbox_np.ElectronicStep(systems.si64())
+    for _ in range(int(g["nsteps"])):
+        es.step()
+    es.update_density()
+    es.update_vhxc()
+    es.energy(True)
+    w = es.diag(True)
+    np.testing.assert_allclose(w, g["eig"], atol=1e-10)
+    c = es.c[:, g["g_idx"]]
+    sign = np.sign((c.conj() * g["final_c_bands"]).sum(1).real)
+    np.testing.assert_allclose(c * sign[:, None], g["final_c_bands"], atol=1e-7)
