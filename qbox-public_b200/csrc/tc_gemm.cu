@@ -481,9 +481,30 @@ static void tc_gemm_tn(Context& ctx, int kind, int m, int n, int k, double alpha
   const int tiles = lower ? tm * (tm + 1) / 2 : tm * tn;
   int sms = 148;
   QBX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device));
-  // split K so that about two CTAs per SM are in flight; the partials (FP32)
-  // are summed in FP64 afterwards
-  int splits = std::max(1, std::min(nkb, (2 * sms + tiles - 1) / tiles));
+  // Split K when the output has few tiles: one CTA per SM runs at a time
+  // (its three pipeline stages fill the shared memory), so the CTAs should
+  // fill whole waves of sms (a product of fewer than sms/16 tiles gets one
+  // wave of short K slices).  Otherwise, of 1..16 splits with K slices of at
+  // least 16 blocks, take the one whose waves are fullest, a larger count only for 2 %
+  // more (a 64-tile n x n product: 9 splits, 576 CTAs in 3.9 waves, where
+  // rounding two CTAs per SM up gave 320 CTAs in 2.2 waves).  The FP32
+  // partials are summed in FP64 afterwards.
+  int splits = 1;
+  if (tiles * 16 < sms) {
+    // a small product: one wave of short K slices
+    splits = std::max(1, std::min(nkb, (sms + tiles - 1) / tiles));
+  } else if (tiles < 4 * sms) {
+    double best = -1.0;
+    for (int sp = 1; sp <= 16 && (nkb + sp - 1) / sp >= 16; sp++) {
+      const long work = (long)tiles * sp;
+      const long waves = (work + sms - 1) / sms;
+      const double eff = (double)work / (double)(waves * sms);
+      if (eff > best + 0.02) {
+        best = eff;
+        splits = sp;
+      }
+    }
+  }
   const int kbps = (nkb + splits - 1) / splits;
   splits = (nkb + kbps - 1) / kbps;
   if (splits > 1) {
