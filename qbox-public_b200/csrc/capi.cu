@@ -214,7 +214,7 @@ void step_eager(Context& c, bool want_f, bool want_s, double* energies, double* 
 // recording changes (profiling, the extrapolation flag, the launch count) is
 // put back afterwards; returns the number of this library's kernels recorded.
 long record_step(Context& c, bool want_f) {
-  const bool prof = c.prof.on, extrap = c.extrapolate;
+  const bool prof = c.prof.on, extrap = c.extrapolate, kextrap = c.kpts_extrapolate;
   const long n0 = c.nlaunch;
   c.prof.on = false;
   c.capturing = true;
@@ -223,8 +223,22 @@ long record_step(Context& c, bool want_f) {
     c.capturing = false;
     c.prof.on = prof;
     c.extrapolate = extrap;
+    c.kpts_extrapolate = kextrap;
   };
   try {
+    if (!c.kpts.empty()) {
+      // k points off Gamma: the same sequence on the complex SlaterDets
+      update_density_k(c);
+      update_vhxc(c);
+      energy_k(c, true);
+      eigsum_k(c);
+      psda_update_k(c);
+      enqueue_readback(c, false);
+      restore();
+      const long k = c.nlaunch - n0;
+      c.nlaunch = n0;
+      return k;
+    }
     c.psir_store = true;
     update_density(c);
     c.psir_store = false;
@@ -295,8 +309,10 @@ void capture_step(Context& c, bool want_f, StepGraph& g) {
 // runs eagerly (graphs off, JD, stress, profiling, or the first use of the
 // configuration, which sizes the lazily grown buffers before any capture).
 StepGraph* step_graph_for(Context& c, bool want_f, bool want_s) {
-  if (!c.step_graph || c.wf_dyn != 0 || want_s || c.prof.on || !c.kpts.empty()) return nullptr;
-  StepGraph& g = c.graphs[(c.extrapolate ? 1 : 0) + (want_f ? 2 : 0)];
+  if (!c.step_graph || c.wf_dyn != 0 || want_s || c.prof.on) return nullptr;
+  if (!c.kpts.empty() && want_f) return nullptr;
+  const bool extrap = c.kpts.empty() ? c.extrapolate : c.kpts_extrapolate;
+  StepGraph& g = c.graphs[(extrap ? 1 : 0) + (want_f ? 2 : 0)];
   if (g.exec) return &g;
   if (g.uses++ == 0) return nullptr;
   try {
@@ -324,7 +340,8 @@ void finish_graph_step(Context& c, bool want_f, double* energies, double* fion) 
   finish_step(c, want_f, false);
   fill_energies(c, energies);
   finish_theta(c);
-  c.extrapolate = true;
+  if (c.kpts.empty()) c.extrapolate = true;
+  else c.kpts_extrapolate = true;
   if (want_f && fion) std::memcpy(fion, c.fion.data(), sizeof(double) * c.fion.size());
 }
 

@@ -628,6 +628,10 @@ void launch_frob2(Context& ctx, const double* q, int n) {
   reduce<1>(ctx, Sq{q}, (size_t)n * n, SLOT_FROB);
 }
 
+void launch_sumsq(Context& ctx, const double* x, size_t len, int slot) {
+  reduce<1>(ctx, Sq{x}, len, slot);
+}
+
 // ------------------------------------------------------ per-geometry setup
 // S(G) = sum_a exp(-i G.tau_a) on the density sphere
 __global__ void k_sfac(const double* __restrict__ gx, int ng, const double* __restrict__ tau,

@@ -196,77 +196,122 @@ void ensure_zwork(Context& ctx) {
   QBX_CUDA(cudaMalloc(&ctx.d_zipiv, sizeof(int) * (n + 1)));
 }
 
-int read_info(Context& ctx) {
-  int info = 0;
-  QBX_CUDA(cudaMemcpyAsync(&info, ctx.d_zipiv + ctx.nst, sizeof(int), cudaMemcpyDeviceToHost,
-                           ctx.stream));
-  QBX_CUDA(cudaStreamSynchronize(ctx.stream));
-  return info;
-}
-
-// S = C^H C = L L^H into znn(0) (lower triangle), Cholesky on the device
-void overlap_cholesky_k(Context& ctx, const double* c, int ngw) {
+// S = C^H C = L L^H into znn(0) (lower triangle), Cholesky on the device; its
+// info code goes to the status word `status`, checked when the step's
+// scalars are read back (no host read inside a step)
+void overlap_cholesky_k(Context& ctx, const double* c, int ngw, int status) {
   const int n = ctx.nst;
   const double one = 1.0, zero = 0.0;
   double* L = znn(ctx, 0);
   QBX_BLAS(cublasZherk(ctx.blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_C, n, ngw, &one, zc(c), ngw,
                        &zero, zc(L), n));
   QBX_SOLVER(cusolverDnZpotrf(ctx.solver, CUBLAS_FILL_MODE_LOWER, n, zc(L), n, zc(ctx.d_zwork),
-                              ctx.zwork_len, ctx.d_zipiv + n));
-  const int info = read_info(ctx);
-  QBX_REQUIRE(info == 0, 40, "Cholesky of the k-point overlap matrix: matrix not positive "
-                             "definite (info=" + std::to_string(info) + ")");
+                              ctx.zwork_len, ctx.d_status + status));
+}
+
+// t = P I for the row interchanges of an LU factorisation (ipiv 1-based,
+// applied in order), one thread per column, complex
+__global__ void k_zpivoted_identity(double2* __restrict__ t, const int* __restrict__ ipiv, int n) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  double2* col = t + (size_t)j * n;
+  for (int i = 0; i < n; i++) col[i] = make_double2(i == j ? 1.0 : 0.0, 0.0);
+  for (int i = 0; i < n; i++) {
+    const int p = ipiv[i] - 1;
+    if (p != i && p >= 0 && p < n) {
+      const double2 a = col[i];
+      col[i] = col[p];
+      col[p] = a;
+    }
+  }
 }
 
 // ComplexMatrix::polar (src/Matrix.cpp:2524-2595): Bjorck-Bowie steps while
 // ||I - X^H X||_F < 1, else the Higham step X <- (X + X^-H) / 2 (X^-H with
-// the conjugated diagonal, as the ScaLAPACK build's pztranc gives it); the
-// norm is read back after each step.
-void polar_k(Context& ctx, double* x, double tol, int maxiter) {
+// the conjugated diagonal, as the ScaLAPACK build's pztranc gives it).
+// q = I - X^H X and SLOT_FROB = ||q||_F^2
+static void polar_q_k(Context& ctx, const double* x, double* q) {
   const int n = ctx.nst;
   const size_t nn = (size_t)n * n;
+  QBX_CUDA(cudaMemsetAsync(q, 0, 2 * nn * sizeof(double), ctx.stream));
+  k_zaxpy_identity<<<nblk(nn), 256, 0, ctx.stream>>>((double2*)q, n, 1.0, 0.0);
+  QBX_LAUNCHED(ctx);
+  QBX_BLAS(cublasZgemm(ctx.blas, CUBLAS_OP_C, CUBLAS_OP_N, n, n, n, &kMone, zc(x), n, zc(x), n,
+                       &kOne, zc(q), n));
+  launch_sumsq(ctx, q, 2 * nn, SLOT_FROB);
+}
+
+// x <- x (I + q/2 (I + 3q/4))
+static void polar_bjorck_k(Context& ctx, double* x, const double* q, double* t, double* qt,
+                           double* xp) {
+  const int n = ctx.nst;
+  const size_t nn = (size_t)n * n;
+  QBX_CUDA(cudaMemcpyAsync(t, q, 2 * nn * sizeof(double), cudaMemcpyDeviceToDevice, ctx.stream));
+  k_zaxpy_identity<<<nblk(nn), 256, 0, ctx.stream>>>((double2*)t, n, 1.0, 0.75);
+  QBX_LAUNCHED(ctx);
+  QBX_BLAS(cublasZgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &kOne, zc(q), n, zc(t), n,
+                       &kZero, zc(qt), n));
+  k_zaxpy_identity<<<nblk(nn), 256, 0, ctx.stream>>>((double2*)qt, n, 1.0, 0.5);
+  QBX_LAUNCHED(ctx);
+  QBX_BLAS(cublasZgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &kOne, zc(x), n, zc(qt), n,
+                       &kZero, zc(xp), n));
+  QBX_CUDA(cudaMemcpyAsync(x, xp, 2 * nn * sizeof(double), cudaMemcpyDeviceToDevice, ctx.stream));
+}
+
+// x <- (x + x^-H)/2: x^-H by an LU factorisation of x^H (P x^H = L U) and the
+// two triangular solves of U^-1 L^-1 P (getrs would allocate stream-ordered
+// memory at some sizes, which a conditional graph body cannot hold)
+static void polar_higham_k(Context& ctx, double* x, double* t, double* qt) {
+  const int n = ctx.nst;
+  const size_t nn = (size_t)n * n;
+  QBX_BLAS(cublasZgeam(ctx.blas, CUBLAS_OP_C, CUBLAS_OP_N, n, n, &kOne, zc(x), n, &kZero, zc(x), n,
+                       zc(t), n));
+  QBX_SOLVER(cusolverDnZgetrf(ctx.solver, n, n, zc(t), n, zc(ctx.d_zwork), ctx.d_zipiv,
+                              ctx.d_status + ST_INFO_POLAR));
+  k_zpivoted_identity<<<(n + 127) / 128, 128, 0, ctx.stream>>>((double2*)qt, ctx.d_zipiv, n);
+  QBX_LAUNCHED(ctx);
+  QBX_BLAS(cublasZtrsm(ctx.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
+                       CUBLAS_DIAG_UNIT, n, n, &kOne, zc(t), n, zc(qt), n));
+  QBX_BLAS(cublasZtrsm(ctx.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N,
+                       CUBLAS_DIAG_NON_UNIT, n, n, &kOne, zc(t), n, zc(qt), n));
+  k_zaverage<<<nblk(nn), 256, 0, ctx.stream>>>((double2*)x, (const double2*)qt, nn);
+  QBX_LAUNCHED(ctx);
+}
+
+// Eagerly the norm is read back after each q; inside a captured step the
+// loop is a WHILE conditional node whose body decides on the device and runs
+// the chosen step in an IF/ELSE node, as the Gamma polar does.
+void polar_k(Context& ctx, double* x, double tol, int maxiter) {
   double* q = znn(ctx, 2);
   double* t = znn(ctx, 3);
   double* qt = znn(ctx, 4);
   double* xp = znn(ctx, 5);
-  for (int iter = 0; iter < maxiter; iter++) {
-    QBX_CUDA(cudaMemsetAsync(q, 0, 2 * nn * sizeof(double), ctx.stream));
-    k_zaxpy_identity<<<nblk(nn), 256, 0, ctx.stream>>>((double2*)q, n, 1.0, 0.0);
-    QBX_LAUNCHED(ctx);
-    QBX_BLAS(cublasZgemm(ctx.blas, CUBLAS_OP_C, CUBLAS_OP_N, n, n, n, &kMone, zc(x), n, zc(x), n,
-                         &kOne, zc(q), n));
-    double qn = 0.0;
-    QBX_BLAS(cublasDznrm2(ctx.blas, (int)nn, zc(q), 1, &qn));
-    if (qn < 1.0) {
-      // t = I + 0.75 q; qt = q t; t = I + 0.5 qt; x <- x t
-      QBX_CUDA(cudaMemcpyAsync(t, q, 2 * nn * sizeof(double), cudaMemcpyDeviceToDevice, ctx.stream));
-      k_zaxpy_identity<<<nblk(nn), 256, 0, ctx.stream>>>((double2*)t, n, 1.0, 0.75);
-      QBX_LAUNCHED(ctx);
-      QBX_BLAS(cublasZgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &kOne, zc(q), n, zc(t), n,
-                           &kZero, zc(qt), n));
-      k_zaxpy_identity<<<nblk(nn), 256, 0, ctx.stream>>>((double2*)qt, n, 1.0, 0.5);
-      QBX_LAUNCHED(ctx);
-      QBX_BLAS(cublasZgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &kOne, zc(x), n, zc(qt), n,
-                           &kZero, zc(xp), n));
-      QBX_CUDA(cudaMemcpyAsync(x, xp, 2 * nn * sizeof(double), cudaMemcpyDeviceToDevice, ctx.stream));
-    } else {
-      // t = X^H; t <- t^-1 (LU, then solve against the identity); x <- (x + t)/2
-      QBX_BLAS(cublasZgeam(ctx.blas, CUBLAS_OP_C, CUBLAS_OP_N, n, n, &kOne, zc(x), n, &kZero,
-                           zc(x), n, zc(t), n));
-      QBX_SOLVER(cusolverDnZgetrf(ctx.solver, n, n, zc(t), n, zc(ctx.d_zwork), ctx.d_zipiv,
-                                  ctx.d_zipiv + n));
-      const int info = read_info(ctx);
-      QBX_REQUIRE(info == 0, 42, "LU factor of the k-point polar iterate is singular");
-      QBX_CUDA(cudaMemsetAsync(qt, 0, 2 * nn * sizeof(double), ctx.stream));
-      k_zaxpy_identity<<<nblk(nn), 256, 0, ctx.stream>>>((double2*)qt, n, 1.0, 0.0);
-      QBX_LAUNCHED(ctx);
-      QBX_SOLVER(cusolverDnZgetrs(ctx.solver, CUBLAS_OP_N, n, n, zc(t), n, ctx.d_zipiv, zc(qt), n,
-                                  ctx.d_zipiv + n));
-      k_zaverage<<<nblk(nn), 256, 0, ctx.stream>>>((double2*)x, (const double2*)qt, nn);
-      QBX_LAUNCHED(ctx);
+  if (!ctx.capturing) {
+    for (int iter = 0; iter < maxiter; iter++) {
+      polar_q_k(ctx, x, q);
+      const double qn = std::sqrt(read_slot(ctx, SLOT_FROB));
+      if (qn < 1.0) polar_bjorck_k(ctx, x, q, t, qt, xp);
+      else polar_higham_k(ctx, x, t, qt);
+      if (qn <= tol) break;
     }
-    if (qn <= tol) break;
+    return;
   }
+  int* iters = ctx.d_status + ST_POLAR_ITERS;
+  QBX_CUDA(cudaMemsetAsync(iters, 0, sizeof(int), ctx.stream));
+  cudaGraphConditionalHandle loop;
+  QBX_CUDA(cudaGraphConditionalHandleCreate(&loop, capture_graph(ctx.stream), 1,
+                                            cudaGraphCondAssignDefault));
+  cudaGraph_t body = add_conditional(ctx.stream, loop, cudaGraphCondTypeWhile, 1)[0];
+  capture_body(ctx, body, ctx.side[0], [&]() {
+    polar_q_k(ctx, x, q);
+    cudaGraphConditionalHandle branch;
+    QBX_CUDA(cudaGraphConditionalHandleCreate(&branch, capture_graph(ctx.stream), 0, 0));
+    launch_polar_decide(ctx, tol, maxiter, iters, loop, branch);
+    cudaGraph_t* arms = add_conditional(ctx.stream, branch, cudaGraphCondTypeIf, 2);
+    cudaGraph_t bjorck = arms[0], higham = arms[1];
+    capture_body(ctx, bjorck, ctx.side[1], [&]() { polar_bjorck_k(ctx, x, q, t, qt, xp); });
+    capture_body(ctx, higham, ctx.side[1], [&]() { polar_higham_k(ctx, x, t, qt); });
+  });
 }
 
 // SlaterDet::ortho_align, complex branch (src/SlaterDet.cpp:877-975)
@@ -275,7 +320,7 @@ void ortho_align_k(Context& ctx, KPointSet& kp) {
   const int n = ctx.nst, K = kp.kb.ng;
   double* L = znn(ctx, 0);
   double* X = znn(ctx, 1);
-  overlap_cholesky_k(ctx, kp.d_c, K);
+  overlap_cholesky_k(ctx, kp.d_c, K, ST_INFO_ORTHO);
   QBX_BLAS(cublasZgemm(ctx.blas, CUBLAS_OP_C, CUBLAS_OP_N, n, n, K, &kOne, zc(kp.d_c), K,
                        zc(kp.d_c_last), K, &kZero, zc(X), n));
   QBX_BLAS(cublasZtrsm(ctx.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
@@ -375,7 +420,7 @@ void gram_k(Context& ctx) {
   const int n = ctx.nst;
   for (KPointSet& kp : ctx.kpts) {
     const int K = kp.kb.ng;
-    overlap_cholesky_k(ctx, kp.d_c, K);
+    overlap_cholesky_k(ctx, kp.d_c, K, ST_INFO_GRAM);
     QBX_BLAS(cublasZtrsm(ctx.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_C,
                          CUBLAS_DIAG_NON_UNIT, K, n, &kOne, zc(znn(ctx, 0)), n, zc(kp.d_c), K));
   }

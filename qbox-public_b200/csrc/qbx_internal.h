@@ -14,6 +14,7 @@
 
 #include <complex>
 #include <iosfwd>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -618,6 +619,18 @@ void launch_identity_axpy(Context& ctx, double* t, const double* q, int n,
 void launch_symmetrize_lower(Context& ctx, double* q, int n);
 void launch_avg_transpose(Context& ctx, double* x, const double* t, int n);
 void launch_frob2(Context& ctx, const double* q, int n);   // SLOT_FROB = ||q||_F^2
+void launch_sumsq(Context& ctx, const double* x, size_t len, int slot);   // sum of x_i^2
+// Conditional graph nodes of a step being captured (step.cu): the graph
+// captured on s; a conditional node of the given type after s's current
+// dependencies (returns its bodies); f captured into body on stream s; the
+// polar loop's decision from SLOT_FROB (Bjorck-Bowie branch when the norm
+// is below one; another iteration while above tol and under maxiter).
+cudaGraph_t capture_graph(cudaStream_t s);
+cudaGraph_t* add_conditional(cudaStream_t s, cudaGraphConditionalHandle h,
+                             cudaGraphConditionalNodeType type, unsigned size);
+void capture_body(Context& ctx, cudaGraph_t body, cudaStream_t s, const std::function<void()>& f);
+void launch_polar_decide(Context& ctx, double tol, int maxiter, int* iters,
+                         cudaGraphConditionalHandle loop, cudaGraphConditionalHandle branch);
 
 // ------------------------------------------------ scalars of a step (scalars.cu)
 // Copies the slots and status words (and d_fion when `fion`) to their pinned

@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <functional>
 
 #include "qbx_internal.h"
 
@@ -118,7 +119,7 @@ static void polar_higham(Context& ctx, double* x, double* t, double* qt) {
 
 // After q of an iteration: choose the branch (1: Bjorck-Bowie, 0: Higham)
 // and whether another iteration follows, as the host loop below does.
-__global__ void k_polar_decide(const double* __restrict__ frob2, double tol, int maxiter,
+__global__ void k_polar_decide_gamma(const double* __restrict__ frob2, double tol, int maxiter,
                                int* __restrict__ iters, cudaGraphConditionalHandle loop,
                                cudaGraphConditionalHandle branch) {
   const double qn = sqrt(*frob2);
@@ -130,7 +131,7 @@ __global__ void k_polar_decide(const double* __restrict__ frob2, double tol, int
 
 // ------------------------------------------------ conditional graph nodes
 // The graph being captured on stream s.
-static cudaGraph_t capture_graph(cudaStream_t s) {
+cudaGraph_t capture_graph(cudaStream_t s) {
   cudaStreamCaptureStatus st;
   cudaGraph_t g = nullptr;
   QBX_CUDA(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, nullptr, nullptr));
@@ -140,8 +141,8 @@ static cudaGraph_t capture_graph(cudaStream_t s) {
 
 // Appends a conditional node of the given type after the current capture
 // dependencies of s, makes it the only dependency, and returns its bodies.
-static cudaGraph_t* add_conditional(cudaStream_t s, cudaGraphConditionalHandle h,
-                                    cudaGraphConditionalNodeType type, unsigned size) {
+cudaGraph_t* add_conditional(cudaStream_t s, cudaGraphConditionalHandle h,
+                             cudaGraphConditionalNodeType type, unsigned size) {
   cudaStreamCaptureStatus st;
   cudaGraph_t g = nullptr;
   const cudaGraphNode_t* deps = nullptr;
@@ -160,8 +161,7 @@ static cudaGraph_t* add_conditional(cudaStream_t s, cudaGraphConditionalHandle h
 }
 
 // Runs f with ctx.stream (and cuBLAS/cuSOLVER) on s, capturing into body.
-template <typename F>
-static void capture_into(Context& ctx, cudaGraph_t body, cudaStream_t s, F f) {
+void capture_body(Context& ctx, cudaGraph_t body, cudaStream_t s, const std::function<void()>& f) {
   cudaStream_t saved = ctx.stream;
   QBX_CUDA(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0,
                                          cudaStreamCaptureModeRelaxed));
@@ -210,18 +210,25 @@ static void polar(Context& ctx, double* x, double tol, int maxiter) {
   QBX_CUDA(cudaGraphConditionalHandleCreate(&loop, capture_graph(ctx.stream), 1,
                                             cudaGraphCondAssignDefault));
   cudaGraph_t body = add_conditional(ctx.stream, loop, cudaGraphCondTypeWhile, 1)[0];
-  capture_into(ctx, body, ctx.side[0], [&]() {
+  capture_body(ctx, body, ctx.side[0], [&]() {
     polar_q(ctx, x, q);
     cudaGraphConditionalHandle branch;
     QBX_CUDA(cudaGraphConditionalHandleCreate(&branch, capture_graph(ctx.stream), 0, 0));
-    k_polar_decide<<<1, 1, 0, ctx.stream>>>(ctx.d_scalars + SLOT_FROB, tol, maxiter, iters, loop,
-                                            branch);
+    k_polar_decide_gamma<<<1, 1, 0, ctx.stream>>>(ctx.d_scalars + SLOT_FROB, tol, maxiter, iters,
+                                                  loop, branch);
     QBX_LAUNCHED(ctx);
     cudaGraph_t* arms = add_conditional(ctx.stream, branch, cudaGraphCondTypeIf, 2);
     cudaGraph_t bjorck = arms[0], higham = arms[1];
-    capture_into(ctx, bjorck, ctx.side[1], [&]() { polar_bjorck(ctx, x, q, t, qt, xp); });
-    capture_into(ctx, higham, ctx.side[1], [&]() { polar_higham(ctx, x, t, qt); });
+    capture_body(ctx, bjorck, ctx.side[1], [&]() { polar_bjorck(ctx, x, q, t, qt, xp); });
+    capture_body(ctx, higham, ctx.side[1], [&]() { polar_higham(ctx, x, t, qt); });
   });
+}
+
+void launch_polar_decide(Context& ctx, double tol, int maxiter, int* iters,
+                         cudaGraphConditionalHandle loop, cudaGraphConditionalHandle branch) {
+  k_polar_decide_gamma<<<1, 1, 0, ctx.stream>>>(ctx.d_scalars + SLOT_FROB, tol, maxiter, iters,
+                                                loop, branch);
+  QBX_LAUNCHED(ctx);
 }
 
 // The orthogonal polar factor of x (nst x nst, device) in place, eagerly or

@@ -105,3 +105,31 @@ def test_kpoint_errors_and_return_to_gamma():
     assert abs(ea["etotal"] - eb["etotal"]) < 1e-10
     ctx.close()
     ref.close()
+
+
+@pytest.mark.parametrize("name", ["si8k2", "h2o4k2"])
+def test_kpoint_step_captured_equals_eager(name):
+    """The k-point step as one CUDA graph (qbx_set_step_graph): the complex
+    polar iteration in WHILE/IF conditional nodes, the Cholesky status in a
+    device word.  Captured from its second use; every step equals the eager
+    step of a twin context to 1e-12 Ha, and the reference's energies to 1e-8
+    Ha over the fixture's steps."""
+    g = golden(name)
+    s = systems.get(name)
+    eager = capi.from_system(s, precision=capi.FP64)
+    graph = capi.from_system(s, precision=capi.FP64)
+    graph.set_step_graph(True)
+    nsteps = int(g["nsteps"])
+    for it in range(nsteps):
+        ra = eager.scf_step()
+        rb = graph.scf_step()
+        for k in TERMS:
+            assert abs(ra[k] - rb[k]) < 1e-12 * max(1.0, abs(ra[k])), (it, k, ra[k], rb[k])
+            assert abs(rb[k] - g["e_" + k][it]) < 1e-8 * max(1.0, abs(g["e_" + k][it])), (it, k)
+    captured, launches, _ = graph.step_graph_info()
+    assert captured >= 1 and launches >= 1, (captured, launches)
+    for ik in range(len(s.kpoints)):
+        np.testing.assert_allclose(graph.get_kpoint_coeffs(ik), eager.get_kpoint_coeffs(ik),
+                                   atol=1e-12)
+    eager.close()
+    graph.close()
