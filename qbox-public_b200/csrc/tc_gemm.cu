@@ -53,8 +53,6 @@ constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /* align */ + 256 /* barr
 // EPW/4 per TMEM lane quarter (warp w reads lanes 32*(w%4) .. 32*(w%4)+31),
 // each holding BN*4/EPW columns of the tile
 __host__ __device__ constexpr int threads_of(int epw) { return 128 + 32 * epw; }
-// TMEM: two accumulators used in turn (256 columns); with the correction
-// terms kept apart (sep), a second pair for hi*lo + lo*hi (512 columns)
 // TMEM: two hi*hi accumulators used in turn (256 columns); with the
 // correction terms kept apart (sep), two more for hi*lo + lo*hi (512 columns)
 __host__ __device__ constexpr uint32_t tmem_cols_of(int sep) { return sep ? 4 * BN : 2 * BN; }
