@@ -382,10 +382,10 @@ def run_ours(args):
     pin_out = torch.empty(nb // 8, dtype=torch.float64, pin_memory=True)
     cur = mix.get_coeffs()
     pin_in.numpy()[:] = cur.view(np.float64).ravel()
-    # ten streamed steps (two per timed step, at most 20): the first upload and
-    # the last download have no neighbouring step to overlap, and over more
-    # steps that fill and drain weighs less per step
-    ne2e = max(2, min(2 * args.steps, 20))
+    # two streamed steps per timed step, at most 40: the first upload and the
+    # last download have no neighbouring step to overlap (about 43 ms in
+    # all), and over more steps that fill and drain weighs less per step
+    ne2e = max(2, min(2 * args.steps, 40))
     # warm-up of the streamed path: its first call allocates the device
     # staging buffers (2 x 1.19 GB) and the copy streams
     for _ in range(2):
