@@ -541,6 +541,7 @@ int qbx_set_cell(qbx_context* h, const double cell[9], double ecut, int nst, con
                                         ? std::atoi(e) : 2;
       if (const char* e = std::getenv("QBX_PSIR")) c.psir_mode = std::atoi(e) != 0 ? 1 : 0;
       if (const char* e = std::getenv("QBX_FWD_STAGED")) c.fast_fwd_staged = std::atoi(e) != 0 ? 1 : 0;
+      if (const char* e = std::getenv("QBX_FFT_PRUNE")) c.fast_prune = std::atoi(e) != 0 ? 1 : 0;
       if (const char* e = std::getenv("QBX_ZLANE")) c.fast_zlane = std::max(0, std::min(3, std::atoi(e)));
       if (const char* e = std::getenv("QBX_FWD_PAIRS_PER_CTA"))
         c.fast_fwd_ppc = std::max(1, std::min(64, std::atoi(e)));
@@ -1262,7 +1263,10 @@ int qbx_autotune(qbx_context* h, char* report, int report_len) {
            std::to_string(c.fast_density_lane_shape) + " x " + std::to_string(c.fast_chunks) +
            ", pairs " +
            std::to_string(c.fast_batch) + ", rods " + std::to_string(c.fast_rods) +
-           ", z lanes " + std::to_string(c.fast_zlane) + "\n";
+           ", z lanes " + std::to_string(c.fast_zlane) + ", pruned xy " +
+           std::to_string(c.fast_prune && c.dws.xw <= prune_width(c.dws.n0) &&
+                          c.dws.yw <= prune_width(c.dws.n1)) +
+           " z " + std::to_string(c.fast_prune && c.dws.zw <= prune_width(c.dws.n2)) + "\n";
       std::strncpy(report, r.c_str(), (size_t)report_len - 1);
       report[report_len - 1] = 0;
     }

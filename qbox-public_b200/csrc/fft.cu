@@ -26,6 +26,7 @@
 //
 // All 1-D FFTs are mixed-radix (2,3,4,5,7,11) self-sorting Stockham passes
 // over shared memory with a twiddle table exp(+2 pi i k/n) built in FP64.
+#include <algorithm>
 #include <cstdio>
 #include <vector>
 
@@ -495,6 +496,12 @@ void upload_sticks(DeviceSticks& d, const Basis& b) {
     for (int s = 0; s < b.nvec; s++) cm[(size_t)b.stick_col[s] * b.n1 + b.stick_y[s]] = s;
     d.colmap = dupload(cm);
   }
+  auto dist = [](int x, int n) { x = ((x % n) + n) % n; return std::min(x, n - x); };
+  d.xw = d.yw = d.zw = 0;
+  for (int x : b.col_x) d.xw = std::max(d.xw, dist(x, b.n0));
+  for (int y : b.stick_y) d.yw = std::max(d.yw, dist(y, b.n1));
+  for (int r = 0; r < b.nrods; r++)
+    d.zw = std::max({d.zw, std::abs(b.rod_lmin[r]), std::abs(b.rod_lmin[r] + b.rod_size[r] - 1)});
   d.px = make_plan(b.n0);
   d.py = make_plan(b.n1);
   d.pz = make_plan(b.n2);
@@ -806,6 +813,7 @@ static bool staged_fast(Context& ctx, int op, const double* c, const double* v, 
   a.fwd_pairs_per_cta = ctx.fast_fwd_ppc;
   a.zlane = ctx.fast_zlane;
   a.fwd_staged = ctx.fast_fwd_staged;
+  a.prune = ctx.fast_prune;
   a.v = v;
   a.psir = nullptr;
   if (op == OP_DENSITY) {

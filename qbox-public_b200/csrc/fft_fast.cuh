@@ -202,7 +202,15 @@ kz_fwd(const typename reg::CT<T>::c* __restrict__ zbuf, int ngw, int nst, int pa
 // straight from the two bands' coefficients, transforms, and stores its
 // outputs z = k2 + M bitrev(t) to the sticks: for each k2 a warp's 8 groups
 // write T runs of 8 consecutive sticks.  No shared memory but the twiddles.
-template <int N2, int MINB>
+// Lane register k of a line held by T lanes (points t + T k, t < T) holds a
+// point within prune_width(N) of 0 for some lane: the registers for which
+// this is false carry only points outside the sphere, which the pruned
+// kernels neither load nor store.
+template <int N, int T> __host__ __device__ constexpr bool keep_reg(int k) {
+  return T * k <= prune_width(N) || T * k + T - 1 >= N - prune_width(N);
+}
+
+template <int N2, int MINB, bool PRUNE = false>
 __global__ void __launch_bounds__(256, MINB)
 kz_bwd_lane(const double2* __restrict__ c, int ngw, int nst, int pair0, DeviceSticks g,
             const double2* __restrict__ twz, float2* __restrict__ zbuf, int rods_per_cta) {
@@ -236,6 +244,10 @@ kz_bwd_lane(const double2* __restrict__ c, int ngw, int nst, int pair0, DeviceSt
     C v[M];
 #pragma unroll
     for (int k = 0; k < M; ++k) {
+      if (PRUNE && !keep_reg<N2, T>(k)) {
+        v[k] = cmk<C>(0.0, 0.0);
+        continue;
+      }
       const int z = t + T * k;
       const int lz = z < half ? z : z - N2;
       const bool minus = rod0 ? (lz <= 0) : mstick;
@@ -261,7 +273,7 @@ kz_bwd_lane(const double2* __restrict__ c, int ngw, int nst, int pair0, DeviceSt
 // the backward kernel stored), transforms back to natural order, and puts the
 // line into shared memory, from which one warp per rod unpacks the pair and
 // adds the kinetic term exactly as kz_fwd does.
-template <int N2>
+template <int N2, bool PRUNE = false>
 __global__ void __launch_bounds__(256)
 kz_fwd_lane(const float2* __restrict__ zbuf, int ngw, int nst, int pair0, DeviceSticks g,
             const double2* __restrict__ twz, double scale, const double2* __restrict__ c,
@@ -297,7 +309,8 @@ kz_fwd_lane(const float2* __restrict__ zbuf, int ngw, int nst, int pair0, Device
     if (ok) {
       C* buf = lines + line * LD;
 #pragma unroll
-      for (int k = 0; k < M; ++k) buf[t + T * k] = v[k];
+      for (int k = 0; k < M; ++k)
+        if (!PRUNE || keep_reg<N2, T>(k)) buf[t + T * k] = v[k];
     }
   }
   __syncthreads();
@@ -620,7 +633,7 @@ __host__ size_t xyfs_smem_bytes(int ncol, int rows) {
          (sizeof(float2) + sizeof(float)) * (size_t)N0 * rows;
 }
 
-template <int N0, int N1>
+template <int N0, int N1, bool PRUNE = false>
 __global__ void __launch_bounds__(288, 1)
 kxy_lane_fwd_staged(float2* __restrict__ zbuf, DeviceSticks g, const double2* __restrict__ twx_g,
                     const double2* __restrict__ twy_g, const float* __restrict__ v,
@@ -699,6 +712,7 @@ kxy_lane_fwd_staged(float2* __restrict__ zbuf, DeviceSticks g, const double2* __
         asm volatile("" : "+r"(txh));
 #pragma unroll
         for (int k = 0; k < MX; ++k) {
+          if (PRUNE && !keep_reg<N0, TX>(k)) continue;   // no column there
           const int cidx = xmap[txh + TX * k];
           if (cidx >= 0) P[cidx * LD + y] = val[k];
         }
@@ -718,6 +732,7 @@ kxy_lane_fwd_staged(float2* __restrict__ zbuf, DeviceSticks g, const double2* __
         const int* cm = g.colmap + (size_t)cidx * N1;
 #pragma unroll
         for (int k = 0; k < MY; ++k) {
+          if (PRUNE && !keep_reg<N1, TY>(k)) continue;   // no stick there
           const int s = __ldg(cm + ty + TY * k);
           if (s >= 0) zp[s] = val[k];
         }
@@ -1094,7 +1109,7 @@ __host__ size_t xydq_smem_bytes(int ncol) {
          sizeof(float) * (size_t)N0 * N1 + sizeof(int) * (size_t)N0;
 }
 
-template <int N0, int N1>
+template <int N0, int N1, bool PRUNE = false>
 __global__ void __launch_bounds__(288, 1)
 kxy_lane_dq(const float2* __restrict__ zbuf, int npairs, int pairs_per_cta, DeviceSticks g,
             const double2* __restrict__ twx_g, const double2* __restrict__ twy_g,
@@ -1153,7 +1168,8 @@ kxy_lane_dq(const float2* __restrict__ zbuf, int npairs, int pairs_per_cta, Devi
       const C* col = P + (ok ? cidx : 0) * LD;
       C val[MY];
 #pragma unroll
-      for (int k = 0; k < MY; ++k) val[k] = ok ? col[ty + TY * k] : cmk<C>(0.0, 0.0);
+      for (int k = 0; k < MY; ++k)
+        val[k] = ok && (!PRUNE || keep_reg<N1, TY>(k)) ? col[ty + TY * k] : cmk<C>(0.0, 0.0);
       lane::line_n2r<TY, MY, +1>(val, ty, twy);
       if (ok) {
         C* qcol = Q + cidx * LD;
@@ -1175,6 +1191,10 @@ kxy_lane_dq(const float2* __restrict__ zbuf, int npairs, int pairs_per_cta, Devi
       C val[MX];
 #pragma unroll
       for (int k = 0; k < MX; ++k) {
+        if (PRUNE && !keep_reg<N0, TX>(k)) {   // no column there
+          val[k] = cmk<C>(0.0, 0.0);
+          continue;
+        }
         const int cidx = xmap[txh + TX * k];
         val[k] = (ok && cidx >= 0) ? Q[cidx * LD + y] : cmk<C>(0.0, 0.0);
       }
@@ -1505,10 +1525,20 @@ struct StagedArgs {
   float2* psir;            // DENSITY: store psi(r) here; VPSI: read it (skip the backward)
   int fwd_pairs_per_cta;   // VPSI from psi(r): band pairs per CTA of kxy_lane_fwd
   int fwd_staged;          // VPSI from psi(r): rounds of rows staged by cp.async
+  int prune;               // FP32 lane kernels skip the points beyond prune_width
   int zlane;               // FP32 z sticks in register lanes: 0 off; 1 both directions
                            // (backward capped for 2 CTAs per SM); 2 both, uncapped; 3
                            // forward only
 };
+
+// the pruned plane kernels need every stick column and stick row within
+// prune_width of 0, the pruned z kernels every rod
+template <int N> bool xy_prunable(const StagedArgs& a, const DeviceSticks& g) {
+  return a.prune && g.xw <= prune_width(N) && g.yw <= prune_width(N);
+}
+template <int N> bool z_prunable(const StagedArgs& a, const DeviceSticks& g) {
+  return a.prune && g.zw <= prune_width(N);
+}
 
 template <typename T, int N, int SH>
 void launch_vpsi_xy(Context& ctx, const StagedArgs& a) {
@@ -1579,11 +1609,15 @@ bool launch_lane_fwd_staged(Context& ctx, const StagedArgs& a) {
     QBX_CUDA(cudaGetDevice(&dev));
     QBX_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     if (sm > (size_t)optin) return false;
-    allow_smem(kxy_lane_fwd_staged<N, N>, sm);
     const int ppc = std::max(1, std::min(a.npairs, a.fwd_pairs_per_cta));
     const int chunks = (a.npairs + ppc - 1) / ppc;
-    kxy_lane_fwd_staged<N, N><<<dim3(N, chunks), threads, sm, ctx.stream>>>(
-        (float2*)a.zbuf, g, a.twx, a.twy, (const float*)a.v, a.psir, a.pair0, a.npairs, ppc);
+    auto run = [&](auto kern) {
+      allow_smem(kern, sm);
+      kern<<<dim3(N, chunks), threads, sm, ctx.stream>>>(
+          (float2*)a.zbuf, g, a.twx, a.twy, (const float*)a.v, a.psir, a.pair0, a.npairs, ppc);
+    };
+    if (xy_prunable<N>(a, g)) run(kxy_lane_fwd_staged<N, N, true>);
+    else run(kxy_lane_fwd_staged<N, N, false>);
     QBX_LAUNCHED(ctx);
     return true;
   }
@@ -1613,9 +1647,14 @@ bool launch_density_dq(Context& ctx, const StagedArgs& a, int chunks, int ppc) {
   QBX_CUDA(cudaGetDevice(&dev));
   QBX_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
   if (sm > (size_t)optin || g.nvec > kDqSticks * threads) return false;
-  allow_smem(kxy_lane_dq<N, N>, sm);
-  kxy_lane_dq<N, N><<<dim3(N, chunks), threads, sm, ctx.stream>>>(
-      (const float2*)a.zbuf, a.npairs, ppc, g, a.twx, a.twy, a.rho, a.w, a.pair0, a.nst, a.psir);
+  auto run = [&](auto kern) {
+    allow_smem(kern, sm);
+    kern<<<dim3(N, chunks), threads, sm, ctx.stream>>>((const float2*)a.zbuf, a.npairs, ppc, g,
+                                                       a.twx, a.twy, a.rho, a.w, a.pair0, a.nst,
+                                                       a.psir);
+  };
+  if (xy_prunable<N>(a, g)) run(kxy_lane_dq<N, N, true>);
+  else run(kxy_lane_dq<N, N, false>);
   QBX_LAUNCHED(ctx);
   return true;
 }
@@ -1689,12 +1728,18 @@ void run_cubic(Context& ctx, const StagedArgs& a) {
     ProfScope ps(ctx, "zfft_bwd");
     if constexpr (LANE) {
       if (zlane && a.zlane != 3) {
-        if (a.zlane == 2)
-          kz_bwd_lane<N, 1><<<zgrid, zl_threads, 0, st>>>((const double2*)a.c, ngw, a.nst, a.pair0,
-                                                          g, a.twz, (float2*)a.zbuf, rpc);
-        else
-          kz_bwd_lane<N, 2><<<zgrid, zl_threads, 0, st>>>((const double2*)a.c, ngw, a.nst, a.pair0,
-                                                          g, a.twz, (float2*)a.zbuf, rpc);
+        auto run = [&](auto kern) {
+          kern<<<zgrid, zl_threads, 0, st>>>((const double2*)a.c, ngw, a.nst, a.pair0, g, a.twz,
+                                             (float2*)a.zbuf, rpc);
+        };
+        const bool pz = z_prunable<N>(a, g);
+        if (a.zlane == 2) {
+          if (pz) run(kz_bwd_lane<N, 1, true>);
+          else run(kz_bwd_lane<N, 1, false>);
+        } else {
+          if (pz) run(kz_bwd_lane<N, 2, true>);
+          else run(kz_bwd_lane<N, 2, false>);
+        }
         QBX_LAUNCHED(ctx);
       }
     }
@@ -1746,10 +1791,14 @@ void run_cubic(Context& ctx, const StagedArgs& a) {
       ProfScope ps(ctx, "zfft_fwd");
       if (zlane) {
         const size_t zls = sizeof(float2) * ((size_t)N + (size_t)2 * rpc * pitch(N));
-        allow_smem(kz_fwd_lane<N>, zls);
-        kz_fwd_lane<N><<<zgrid, zl_threads, zls, st>>>((const float2*)a.zbuf, ngw, a.nst, a.pair0,
-                                                       g, a.twz, scale, (const double2*)a.c,
-                                                       ctx.d_g2_w, (double2*)a.hc, rpc);
+        auto run = [&](auto kern) {
+          allow_smem(kern, zls);
+          kern<<<zgrid, zl_threads, zls, st>>>((const float2*)a.zbuf, ngw, a.nst, a.pair0, g,
+                                               a.twz, scale, (const double2*)a.c, ctx.d_g2_w,
+                                               (double2*)a.hc, rpc);
+        };
+        if (z_prunable<N>(a, g)) run(kz_fwd_lane<N, true>);
+        else run(kz_fwd_lane<N, false>);
       } else {
         allow_smem(kz_fwd<T, N>, zs);
         kz_fwd<T, N><<<zgrid, kZThreads, zs, st>>>((const C*)a.zbuf, ngw, a.nst, a.pair0, g,

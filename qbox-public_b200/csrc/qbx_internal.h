@@ -134,7 +134,16 @@ struct DeviceSticks {
   double2* tw[3];    // exp(+2 pi i k/n) for the x, y, z lengths (owned here,
                      // so contexts of different grids never share tables)
   int* colmap;       // ncol x n1: the stick at (compact column, y), -1 if none
+  // widest occupied distance from 0 (mod n) of the stick columns' x, the
+  // sticks' y and the rods' z: the pruned plane and z kernels skip the lane
+  // registers that only hold points beyond prune_width(n)
+  int xw, yw, zw;
 };
+
+// Points of a line of length n that the pruned kernels keep: x with
+// min(x, n - x) <= prune_width(n).  A wavefunction basis on the grid Qbox
+// builds for its density (n >= 4 hmax + 1) always fits.
+__host__ __device__ constexpr int prune_width(int n) { return (n - 1) / 4; }
 
 // -------------------------------------------------------------- species
 // G-space tables of one species, as the reference's Species holds them after
@@ -442,6 +451,8 @@ struct Context {
   int fast_chunks = 8;          // CTAs per plane in the density pass
   int fast_fwd_ppc = 2;         // band pairs per CTA of the H*psi plane kernel from psi(r)
   int fast_fwd_staged = 1;      // that kernel with its rows staged by cp.async
+  int fast_prune = 1;           // FP32 lane kernels skip the points beyond the sphere
+                                // (prune_width) where the basis allows it
   int fast_zlane = 1;           // FP32 z sticks in register lanes (0: warp per stick;
                                 // 2: backward uncapped; 3: forward only)
   bool fast_fft = true;         // use the specialised kernels when compiled

@@ -234,3 +234,36 @@ def test_stored_psi_r_gives_the_recomputed_step(graph, monkeypatch):
     np.testing.assert_allclose(a.get_coeffs(), b.get_coeffs(), rtol=0, atol=1e-12)
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("name", ["si8", "si64", "h2o32", "si512_32"])
+def test_pruned_lane_kernels(name, monkeypatch):
+    """The FP32 lane kernels that skip the lane registers beyond the sphere
+    (QBX_FFT_PRUNE=1: the H*psi plane pass stores only the columns and
+    sticks within prune_width, the z passes load and store only the z
+    within it, the density pass loads only the columns and rows within it)
+    give the unpruned kernels' density and H*psi (2e-6 of the largest value),
+    and their two-step trajectory: energies to 1e-8 Ha per atom and the
+    coefficients to 1e-7.  The density pass is the queued-sticks kernel
+    (shape 8) and the H*psi pass the staged one, as at 140^3."""
+    s = systems.si512().band_sample(32) if name == "si512_32" else systems.get(name)
+    ctxs = []
+    monkeypatch.setenv("QBX_FAST_DENSITY_LANE_SHAPE", "8")
+    for mode in ("1", "0"):
+        monkeypatch.setenv("QBX_FFT_PRUNE", mode)
+        ctxs.append(_ctx(s, capi.MIXED, True))
+    monkeypatch.delenv("QBX_FFT_PRUNE")
+    monkeypatch.delenv("QBX_FAST_DENSITY_LANE_SHAPE")
+    a, b = ctxs
+    ra, ha, ea = _run(a)
+    rb, hb, eb = _run(b)
+    np.testing.assert_allclose(ra, rb, rtol=0, atol=2e-6 * np.abs(rb).max())
+    np.testing.assert_allclose(ha, hb, rtol=0, atol=2e-6 * np.abs(hb).max())
+    natoms = len(s.atoms)
+    for _ in range(2):
+        ea, eb = a.scf_step(), b.scf_step()
+        for k in ("ekin", "enl", "etotal", "eigenvalue_sum"):
+            assert abs(ea[k] - eb[k]) <= 1e-8 * natoms, (k, ea[k], eb[k])
+    np.testing.assert_allclose(a.get_coeffs(), b.get_coeffs(), rtol=0, atol=1e-7)
+    a.close()
+    b.close()
