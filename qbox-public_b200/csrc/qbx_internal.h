@@ -418,6 +418,7 @@ struct Context {
   int tc_corr_mul = 8;          // tcgen05 GEMM: hi*lo + lo*hi chains this many times longer,
                                 // in accumulators of their own (0: in the hi*hi chain)
   int tc_epw = 8;               // tcgen05 GEMM: epilogue warps (4 or 8)
+  int tc_pair = 0;              // tcgen05 GEMM: 256-row tiles on CTA pairs (cta_group::2)
 
   // band pairs split over GPUs (qbx_set_band_shard): this GPU's rank among
   // shard_n, and the NCCL communicator (ncclComm_t) of the group

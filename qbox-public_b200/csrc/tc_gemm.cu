@@ -391,6 +391,355 @@ k_tc_split_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant
   }
 }
 
+// ------------------------------------------------------------ CTA pairs
+// The same product on 256 x 128 tiles, computed by a cluster of two CTAs on
+// two SMs with tcgen05.mma.cta_group::2.  CTA r of the pair loads its own 128
+// rows of A and half of B's 128 columns (columns 64 r .. 64 r + 63) into its
+// shared memory; the pair's first CTA issues the MMAs, which read A and B
+// from both CTAs' shared memory and accumulate rows 128 r .. 128 r + 127 of
+// the tile in CTA r's TMEM.  Per SM a K block moves 48 KB of operands
+// instead of 64 KB, the MMAs read a quarter less from each SM's shared
+// memory, and four pipeline stages fit.
+//   - both CTAs' TMA loads complete on the first CTA's stage barrier, whose
+//     expected bytes the first CTA sets for the pair;
+//   - the first CTA's MMA commits arrive on the same barrier of both CTAs
+//     (stage free, accumulator filled);
+//   - the epilogue warps of both CTAs drain their own TMEM and hand the
+//     accumulator back on the first CTA's barrier.
+// The accumulation chains, the epilogue and the outputs are those of
+// k_tc_split_gemm.  Every mbarrier wait is bounded; both CTAs meet at a
+// cluster barrier after the barriers are set up and again before TMEM is
+// freed, and every path (a timed-out wait included) reaches both.
+constexpr int PAIR_STAGES = 4;
+constexpr int HALF_TILE_BYTES = (BN / 2) * 128;                           // 64 rows of B: 8 KB
+constexpr int PAIR_STAGE_BYTES = 2 * TILE_BYTES + 2 * HALF_TILE_BYTES;   // 48 KB
+constexpr int PAIR_SMEM_BYTES = PAIR_STAGES * PAIR_STAGE_BYTES + 1024 + 256;
+
+// instruction descriptor of the pair's 256 x 128 MMA
+__host__ __device__ constexpr uint32_t idesc_pair_of(int kind) {
+  const uint32_t fmt = kind == KIND_BF16 ? 1u : 2u;
+  return (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(BN >> 3) << 17) |
+         ((uint32_t)((2 * BM) >> 4) << 24);
+}
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+
+// shared::cluster address of this shared variable in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t cluster_addr(const void* p, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(rank));
+  return r;
+}
+
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile(
+      "barrier.cluster.arrive.release.aligned;\n\t"
+      "barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t addr) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(addr)
+               : "memory");
+}
+
+// bounded wait, acquiring at cluster scope (the barrier's arrivals come from
+// the other CTA of the pair or from the pair's MMAs)
+__device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, uint32_t parity) {
+  const uint32_t a = smem_u32(bar);
+  for (long long it = 0; it < WAIT_LIMIT; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// TMA load into this CTA's shared memory, its bytes counted on the pair's
+// barrier at cluster address bar (no multicast: each CTA loads its own tiles)
+__device__ __forceinline__ void tma_load_2d_pair(void* dst, const CUtensorMap* map, uint32_t bar,
+                                                 int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes "
+      "[%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(dst)),
+      "l"((uint64_t)map), "r"(bar), "r"(x), "r"(y)
+      : "memory");
+}
+
+template <int KIND>
+__device__ __forceinline__ void umma_pair(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t acc) {
+  if constexpr (KIND == KIND_BF16) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(idesc_pair_of(KIND_BF16)), "r"(acc)
+        : "memory");
+  } else {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(idesc_pair_of(KIND_TF32)), "r"(acc)
+        : "memory");
+  }
+}
+
+// one arrival on the barrier at this offset in both CTAs of the pair when
+// the MMAs issued so far have completed
+__device__ __forceinline__ void umma_commit_pair(uint64_t* bar) {
+  asm volatile(
+      "{\n\t.reg .b16 m;\n\t"
+      "mov.b16 m, 3;\n\t"
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 "
+      "[%0], m;\n\t}" ::"r"(smem_u32(bar))
+      : "memory");
+}
+
+template <int KIND, int EPW>
+__global__ void __launch_bounds__(threads_of(EPW), 1)
+k_tc_pair_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant__ CUtensorMap ma_lo,
+               const __grid_constant__ CUtensorMap mb_hi, const __grid_constant__ CUtensorMap mb_lo,
+               int M, int N, int nkb, int kb_per_split, float* __restrict__ ws,
+               double* __restrict__ C, int ldc, double alpha, double beta,
+               int* __restrict__ err, int lower, int chunk, int corr_mul) {
+  // the pair is M tiles 2p and 2p + 1, CTA ranks 0 and 1 of a cluster along
+  // x.  Without a K split, x runs over (N tile, rank) and y over the pairs,
+  // so the N tiles that share a pair's A tiles run together and A streams
+  // from HBM once.
+  const int mt = ws ? (int)blockIdx.x : 2 * (int)blockIdx.y + (int)(blockIdx.x & 1);
+  const int nt = ws ? (int)blockIdx.y : (int)(blockIdx.x >> 1);
+  const int m0 = mt * BM, n0 = nt * BN;
+  // lower: a pair whose every row lies above the tile's first column holds
+  // only the strict upper triangle; both CTAs leave before anything is set up
+  if (lower && n0 >= (mt & ~1) * BM + 2 * BM) return;
+  const uint32_t rank = cluster_rank();
+  const bool lead = rank == 0;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t* full = (uint64_t*)(base + PAIR_STAGES * PAIR_STAGE_BYTES);
+  uint64_t* empty = full + PAIR_STAGES;
+  uint64_t* tfull = empty + PAIR_STAGES;
+  uint64_t* tfree = tfull + 2;
+  uint64_t* cfull = tfree + 2;
+  uint64_t* cfree = cfull + 2;
+  uint32_t* tmem_slot = (uint32_t*)(cfree + 2);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int kb0 = blockIdx.z * kb_per_split;
+  const int kb1 = min(nkb, kb0 + kb_per_split);
+  const int niter = max(0, kb1 - kb0);
+  const int nchunk = (niter + chunk - 1) / chunk;
+  const int sep = corr_mul > 0 ? 1 : 0;
+  const int cchunk = chunk * (sep ? corr_mul : 1);
+  const uint32_t tmem_cols = tmem_cols_of(sep);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < PAIR_STAGES; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; b++) {
+      mbar_init(&tfull[b], 1);
+      mbar_init(&tfree[b], 2 * EPW);    // the epilogue warps of both CTAs
+      mbar_init(&cfull[b], 1);
+      mbar_init(&cfree[b], 2 * EPW);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(tmem_cols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  }
+  __syncthreads();
+  cluster_sync_all();   // both CTAs' barriers exist before any arrival crosses the pair
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // ---------------- TMA producer (both CTAs)
+    bool ok = true;
+    for (int it = 0; it < niter; ++it) {
+      const int s = it % PAIR_STAGES;
+      const uint32_t ph = (uint32_t)((it / PAIR_STAGES) & 1);
+      if (!mbar_wait_cluster(&empty[s], ph ^ 1u)) {
+        atomicExch(err, 1);
+        ok = false;
+        break;
+      }
+      unsigned char* st = base + s * PAIR_STAGE_BYTES;
+      const uint32_t fb = cluster_addr(&full[s], 0);
+      if (lead) mbar_expect_tx(&full[s], 2 * PAIR_STAGE_BYTES);
+      const int kx = (kb0 + it) * bk_of(KIND);
+      const int nb = n0 + (int)rank * (BN / 2);
+      tma_load_2d_pair(st, &ma_hi, fb, kx, m0);
+      tma_load_2d_pair(st + TILE_BYTES, &ma_lo, fb, kx, m0);
+      tma_load_2d_pair(st + 2 * TILE_BYTES, &mb_hi, fb, kx, nb);
+      tma_load_2d_pair(st + 2 * TILE_BYTES + HALF_TILE_BYTES, &mb_lo, fb, kx, nb);
+    }
+    // every stage's last release (a commit of the first CTA's MMAs) has
+    // arrived here before this CTA can leave
+    for (int it = niter; it < niter + PAIR_STAGES && ok; ++it) {
+      const int s = it % PAIR_STAGES;
+      if (!mbar_wait_cluster(&empty[s], (uint32_t)(((it / PAIR_STAGES) & 1) ^ 1))) {
+        atomicExch(err, 7);
+        ok = false;
+      }
+    }
+  } else if (warp == 1 && lane == 0 && lead) {
+    // ---------------- MMA issuer (first CTA)
+    for (int it = 0; it < niter; ++it) {
+      const int c = it / chunk, b = c & 1;
+      const int cc = it / cchunk, cb = cc & 1;
+      const bool chunk_start = (it % chunk) == 0;
+      const bool corr_start = (it % cchunk) == 0;
+      if (chunk_start && c >= 2 &&
+          !mbar_wait_cluster(&tfree[b], (uint32_t)(((c >> 1) - 1) & 1))) {
+        atomicExch(err, 4);
+        break;
+      }
+      if (sep && corr_start && cc >= 2 &&
+          !mbar_wait_cluster(&cfree[cb], (uint32_t)(((cc >> 1) - 1) & 1))) {
+        atomicExch(err, 5);
+        break;
+      }
+      const int s = it % PAIR_STAGES;
+      const uint32_t ph = (uint32_t)((it / PAIR_STAGES) & 1);
+      if (!mbar_wait_cluster(&full[s], ph)) { atomicExch(err, 2); break; }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      unsigned char* st = base + s * PAIR_STAGE_BYTES;
+      const uint64_t dah = smem_desc(st);
+      const uint64_t dal = smem_desc(st + TILE_BYTES);
+      const uint64_t dbh = smem_desc(st + 2 * TILE_BYTES);
+      const uint64_t dbl = smem_desc(st + 2 * TILE_BYTES + HALF_TILE_BYTES);
+      const uint32_t tacc = tmem + (uint32_t)(b * BN);
+      const uint32_t tcor = sep ? tmem + (uint32_t)((2 + cb) * BN) : tacc;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const uint64_t off = (uint64_t)(k * 32) >> 4;
+        const uint32_t accumulate = (chunk_start && k == 0) ? 0u : 1u;
+        const uint32_t cacc = sep ? ((corr_start && k == 0) ? 0u : 1u) : 1u;
+        umma_pair<KIND>(tacc, dah + off, dbh + off, accumulate);
+        umma_pair<KIND>(tcor, dah + off, dbl + off, cacc);
+        umma_pair<KIND>(tcor, dal + off, dbh + off, 1u);
+      }
+      umma_commit_pair(&empty[s]);
+      if ((it % chunk) == chunk - 1 || it == niter - 1) umma_commit_pair(&tfull[b]);
+      if (sep && ((it % cchunk) == cchunk - 1 || it == niter - 1)) umma_commit_pair(&cfull[cb]);
+    }
+  } else if (warp >= 4) {
+    // ---------------- epilogue (both CTAs): drain this CTA's TMEM rows
+    constexpr int COLS = BN * 4 / EPW;
+    const int wq = warp & 3;
+    const int cbase = ((warp - 4) >> 2) * COLS;
+    const int row = m0 + wq * 32 + lane;
+    const uint32_t tlane = tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)cbase;
+    float acc[COLS];
+#pragma unroll
+    for (int j = 0; j < COLS; ++j) acc[j] = 0.0f;
+    auto drain = [&](uint32_t col0) {
+#pragma unroll
+      for (int c0 = 0; c0 < COLS; c0 += 64) {
+        uint32_t r[64];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) tmem_ld16(tlane + col0 + (uint32_t)(c0 + 16 * q), r + 16 * q);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int j = 0; j < 64; ++j) acc[c0 + j] += __uint_as_float(r[j]);
+      }
+    };
+    bool ok = true;
+    for (int c = 0; c < nchunk && ok; ++c) {
+      const int b = c & 1;
+      if (!mbar_wait_cluster(&tfull[b], (uint32_t)((c >> 1) & 1))) {
+        atomicExch(err, 3);
+        ok = false;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      drain((uint32_t)(b * BN));
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive_remote(cluster_addr(&tfree[b], 0));
+      if (sep && ((c + 1) % corr_mul == 0 || c == nchunk - 1)) {
+        const int cc = c / corr_mul, cb = cc & 1;
+        if (!mbar_wait_cluster(&cfull[cb], (uint32_t)((cc >> 1) & 1))) {
+          atomicExch(err, 6);
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        drain((uint32_t)((2 + cb) * BN));
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) mbar_arrive_remote(cluster_addr(&cfree[cb], 0));
+      }
+    }
+    if (ws) {
+      float* out = ws + (size_t)blockIdx.z * M * N;
+      if (row < M) {
+#pragma unroll
+        for (int j = 0; j < COLS; ++j) {
+          const int col = n0 + cbase + j;
+          if (col < N) out[(size_t)col * M + row] = ok ? acc[j] : 0.0f;
+        }
+      }
+    } else if (row < M && ok) {
+      double* crow = C + row;
+      if (beta == 1.0) {
+#pragma unroll
+        for (int j = 0; j < COLS; ++j) {
+          const int col = n0 + cbase + j;
+          if (col < N) atomicAdd(crow + (size_t)col * ldc, alpha * (double)acc[j]);
+        }
+      } else {
+        constexpr int G = 16;
+#pragma unroll
+        for (int j0 = 0; j0 < COLS; j0 += G) {
+          double old[G];
+          if (beta != 0.0) {
+#pragma unroll
+            for (int j = 0; j < G; ++j) {
+              const int col = n0 + cbase + j0 + j;
+              old[j] = col < N ? crow[(size_t)col * ldc] : 0.0;
+            }
+          }
+#pragma unroll
+          for (int j = 0; j < G; ++j) {
+            const int col = n0 + cbase + j0 + j;
+            if (col < N)
+              crow[(size_t)col * ldc] =
+                  alpha * (double)acc[j0 + j] + (beta != 0.0 ? beta * old[j] : 0.0);
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // the pair's MMAs have read both CTAs' shared memory and every arrival has
+  // landed before either CTA frees its TMEM or leaves
+  cluster_sync_all();
+  if (warp == 1) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(tmem_cols)
+                 : "memory");
+  }
+}
+
 }  // namespace tc
 
 // ------------------------------------------------------------------ host
@@ -415,12 +764,13 @@ static EncodeTiledFn encode_fn() {
 // K-major matrix of BF16 or TF32 (FP32) elements: rows = k (contiguous, ld
 // elements), cols = m; box of one 128-byte row of K by 128 columns, 128-byte
 // swizzle.  Columns past `cols` and K past `k` read as zero.
-static CUtensorMap kmajor_map(const void* ptr, int k, int cols, int ld, int kind) {
+static CUtensorMap kmajor_map(const void* ptr, int k, int cols, int ld, int kind,
+                              int box_cols = tc::BM) {
   CUtensorMap map;
   const size_t es = kind == tc::KIND_BF16 ? 2 : 4;
   const cuuint64_t dims[2] = {(cuuint64_t)k, (cuuint64_t)cols};
   const cuuint64_t strides[1] = {(cuuint64_t)ld * es};
-  const cuuint32_t box[2] = {(cuuint32_t)tc::bk_of(kind), (cuuint32_t)tc::BM};
+  const cuuint32_t box[2] = {(cuuint32_t)tc::bk_of(kind), (cuuint32_t)box_cols};
   const cuuint32_t estr[2] = {1, 1};
   const CUresult r = encode_fn()(
       &map, kind == tc::KIND_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
@@ -521,20 +871,53 @@ static void tc_gemm_tn(Context& ctx, int kind, int m, int n, int k, double alpha
   int* err = ctx.d_status + ST_TC_ERR;   // wait-timeout flag, sticky
   const int chunk = std::max(1, ctx.tc_chunk), corr_mul = std::max(0, ctx.tc_corr_mul);
   float* ws = splits > 1 ? (float*)ctx.d_tc_ws : nullptr;
-  QBX_REQUIRE(splits > 1 ? tn <= 65535 : tm <= 65535, 54, "too many tiles for the grid");
-  dim3 grid = splits > 1 ? dim3(tm, tn, splits) : dim3(tn, tm, 1);
-  auto launch = [&](auto kern, int epw) {
-    allow_smem(kern, tc::SMEM_BYTES);
-    kern<<<grid, tc::threads_of(epw), tc::SMEM_BYTES, ctx.stream>>>(
-        mah, mal, mbh, mbl, m, n, nkb, kbps, ws, C, ldc, alpha, beta, err, lower ? 1 : 0,
-        chunk, corr_mul);
-  };
-  if (kind == tc::KIND_BF16) {
-    if (ctx.tc_epw == 8) launch(tc::k_tc_split_gemm<tc::KIND_BF16, 8>, 8);
-    else launch(tc::k_tc_split_gemm<tc::KIND_BF16, 4>, 4);
+  if (ctx.tc_pair) {
+    // CTA pairs: B in half tiles of 64 columns, M tiles padded to an even count
+    const CUtensorMap mbh2 = kmajor_map(bhi, k, n, ldb, kind, tc::BN / 2);
+    const CUtensorMap mbl2 = kmajor_map(blo, k, n, ldb, kind, tc::BN / 2);
+    const int tm2 = (tm + 1) & ~1;
+    QBX_REQUIRE(splits > 1 ? tn <= 65535 : tm2 / 2 <= 65535, 54, "too many tiles for the grid");
+    const dim3 grid2 = splits > 1 ? dim3(tm2, tn, splits) : dim3(2 * tn, tm2 / 2, 1);
+    auto launch2 = [&](auto kern, int epw) {
+      allow_smem(kern, tc::PAIR_SMEM_BYTES);
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = grid2;
+      cfg.blockDim = dim3(tc::threads_of(epw));
+      cfg.dynamicSmemBytes = tc::PAIR_SMEM_BYTES;
+      cfg.stream = ctx.stream;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = 2;   // a cta_group::2 pair is a cluster along x
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = 1;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      QBX_CUDA(cudaLaunchKernelEx(&cfg, kern, mah, mal, mbh2, mbl2, m, n, nkb, kbps, ws, C, ldc,
+                                  alpha, beta, err, lower ? 1 : 0, chunk, corr_mul));
+    };
+    if (kind == tc::KIND_BF16) {
+      if (ctx.tc_epw == 8) launch2(tc::k_tc_pair_gemm<tc::KIND_BF16, 8>, 8);
+      else launch2(tc::k_tc_pair_gemm<tc::KIND_BF16, 4>, 4);
+    } else {
+      if (ctx.tc_epw == 8) launch2(tc::k_tc_pair_gemm<tc::KIND_TF32, 8>, 8);
+      else launch2(tc::k_tc_pair_gemm<tc::KIND_TF32, 4>, 4);
+    }
   } else {
-    if (ctx.tc_epw == 8) launch(tc::k_tc_split_gemm<tc::KIND_TF32, 8>, 8);
-    else launch(tc::k_tc_split_gemm<tc::KIND_TF32, 4>, 4);
+    QBX_REQUIRE(splits > 1 ? tn <= 65535 : tm <= 65535, 54, "too many tiles for the grid");
+    const dim3 grid = splits > 1 ? dim3(tm, tn, splits) : dim3(tn, tm, 1);
+    auto launch = [&](auto kern, int epw) {
+      allow_smem(kern, tc::SMEM_BYTES);
+      kern<<<grid, tc::threads_of(epw), tc::SMEM_BYTES, ctx.stream>>>(
+          mah, mal, mbh, mbl, m, n, nkb, kbps, ws, C, ldc, alpha, beta, err, lower ? 1 : 0,
+          chunk, corr_mul);
+    };
+    if (kind == tc::KIND_BF16) {
+      if (ctx.tc_epw == 8) launch(tc::k_tc_split_gemm<tc::KIND_BF16, 8>, 8);
+      else launch(tc::k_tc_split_gemm<tc::KIND_BF16, 4>, 4);
+    } else {
+      if (ctx.tc_epw == 8) launch(tc::k_tc_split_gemm<tc::KIND_TF32, 8>, 8);
+      else launch(tc::k_tc_split_gemm<tc::KIND_TF32, 4>, 4);
+    }
   }
   QBX_LAUNCHED(ctx);
   if (splits > 1) {

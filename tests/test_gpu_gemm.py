@@ -1,5 +1,7 @@
 """The tcgen05 split-precision GEMM against numpy (FP64) and against the
 same split products through cuBLAS, through the C ABI."""
+import os
+
 import numpy as np
 import pytest
 
@@ -11,6 +13,19 @@ pytestmark = pytest.mark.gpu
 @pytest.fixture(scope="module")
 def ctx():
     c = capi.Context()
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="module")
+def ctx_pair():
+    """A context whose tcgen05 GEMMs run on CTA pairs, 256 x 128 tiles
+    (QBX_TC_PAIR=1), instead of one CTA per 128 x 128 tile."""
+    os.environ["QBX_TC_PAIR"] = "1"
+    try:
+        c = capi.Context()
+    finally:
+        os.environ.pop("QBX_TC_PAIR", None)
     yield c
     c.close()
 
@@ -56,3 +71,49 @@ def test_tcgen05_tf32_split_gemm(ctx, m, n, k):
     d = ctx.split_gemm_tn(a, b, backend=2)
     scale = np.abs(ref).max()
     assert np.abs(d - ref).max() < 2e-6 * scale
+
+
+@pytest.mark.parametrize("m,n,k,backend", [(128, 128, 64, 1), (384, 256, 5000, 1),
+                                           (1024, 1024, 23848, 1), (2048, 1024, 20000, 1),
+                                           (300, 130, 1000, 2), (145838, 256, 1024, 2),
+                                           (1000, 1024, 2048, 2)])
+def test_cta_pair_gemm_matches_single_cta(ctx, ctx_pair, m, n, k, backend):
+    """The CTA-pair kernel (cta_group::2, 256 x 128 tiles, B split between
+    the two CTAs' shared memory) gives the one-CTA kernel's products: the
+    same K blocks in the same accumulation chains, so they agree to 1e-6 of
+    the largest value; both stay within the split-precision bound of the
+    FP64 product.  The shapes cover an odd number of M tiles (the pair's
+    second CTA reads zeros), partial tiles, the split-K and the direct
+    (tall update) epilogues, BF16 and TF32."""
+    rng = np.random.default_rng(7 * m + n + k)
+    a = rng.standard_normal((k, m)) / np.sqrt(k)
+    b = rng.standard_normal((k, n)) / np.sqrt(k)
+    ref = a.T @ b
+    d2 = ctx_pair.split_gemm_tn(a, b, backend=backend)
+    d1 = ctx.split_gemm_tn(a, b, backend=backend)
+    scale = np.abs(ref).max()
+    assert np.abs(d2 - d1).max() <= 1e-6 * scale
+    bound = 2e-5 if backend == 1 else 2e-6
+    assert np.abs(d2 - ref).max() < bound * scale + 1e-6
+
+
+def test_cta_pair_gemm_step_si512_sample(monkeypatch):
+    """Two mixed electronic steps of a 32-band sample of the 512-atom cell
+    with every tcgen05 GEMM on CTA pairs (the lower-triangle overlaps, the
+    split-K inner products, the tall updates) give the one-CTA steps'
+    energies to 1e-8 Ha per atom and coefficients to 1e-7."""
+    from qbx import systems
+    s = systems.si512().band_sample(32)
+    ctxs = []
+    for mode in ("1", "0"):
+        monkeypatch.setenv("QBX_TC_PAIR", mode)
+        ctxs.append(capi.from_system(s, precision=capi.MIXED))
+    monkeypatch.delenv("QBX_TC_PAIR")
+    a, b = ctxs
+    for _ in range(2):
+        ea, eb = a.scf_step(), b.scf_step()
+        for key in ("ekin", "enl", "etotal", "eigenvalue_sum"):
+            assert abs(ea[key] - eb[key]) <= 1e-8 * len(s.atoms), (key, ea[key], eb[key])
+    np.testing.assert_allclose(a.get_coeffs(), b.get_coeffs(), rtol=0, atol=1e-7)
+    a.close()
+    b.close()
