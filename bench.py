@@ -342,10 +342,10 @@ def run_ours(args):
                 "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                 "frac": achieved / hbm_peak,
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
-                # DRAM bytes per launch: the ncu capture of this kernel
-                # (profiles/kxy_lane_fwd_staged_si512.md: 420.5 MB for a
+                # DRAM bytes per launch: the ncu capture of the pruned kernel
+                # (profiles/kxy_lane_fwd_staged_si512.md: 416.1 MB for a
                 # 16-pair launch) scaled by the band pairs of this run's launches
-                "traffic": 420.5e6 / 16.0 * (npairs / max(1e-9, n_xy)),
+                "traffic": 416.1e6 / 16.0 * (npairs / max(1e-9, n_xy)),
                 "algorithmic_bytes_per_launch": per_launch_bytes,
                 "launch_ms": per_launch_ms}
     # GEMM share: the split-precision products of the mixed step (BF16 and
