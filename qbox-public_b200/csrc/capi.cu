@@ -369,7 +369,8 @@ int qbx_create(qbx_context** out, int device, int precision) {
   if (const char* e = std::getenv("QBX_TALL_KIND")) h->c.tall_kind = std::atoi(e) == 0 ? 0 : 1;
   if (const char* e = std::getenv("QBX_TC_CHUNK")) h->c.tc_chunk = std::max(1, std::min(64, std::atoi(e)));
   if (const char* e = std::getenv("QBX_TC_EPW")) h->c.tc_epw = std::atoi(e) == 4 ? 4 : 8;
-  if (const char* e = std::getenv("QBX_TC_PAIR")) h->c.tc_pair = std::atoi(e) != 0 ? 1 : 0;
+  if (const char* e = std::getenv("QBX_TC_PAIR")) h->c.tc_pair = std::max(0, std::min(2, std::atoi(e)));
+  if (const char* e = std::getenv("QBX_TC_PAIR_EPW")) h->c.tc_pair_epw = std::atoi(e) == 8 ? 8 : 16;
   if (const char* e = std::getenv("QBX_TC_CORR_MUL")) h->c.tc_corr_mul = std::max(0, std::min(64, std::atoi(e)));
   if (const char* e = std::getenv("QBX_TALL_KIND_HC")) h->c.tall_kind_hc = std::atoi(e) == 1 ? 1 : 0;
   // batches of captured steps: one graph launch per context on its own

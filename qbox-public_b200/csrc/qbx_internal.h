@@ -418,7 +418,9 @@ struct Context {
   int tc_corr_mul = 8;          // tcgen05 GEMM: hi*lo + lo*hi chains this many times longer,
                                 // in accumulators of their own (0: in the hi*hi chain)
   int tc_epw = 8;               // tcgen05 GEMM: epilogue warps (4 or 8)
-  int tc_pair = 0;              // tcgen05 GEMM: 256-row tiles on CTA pairs (cta_group::2)
+  int tc_pair = 2;              // tcgen05 GEMM on CTA pairs (cta_group::2): 0 off (one CTA per
+                                // 128 x 128 tile), 1 256 x 128 tiles, 2 256 x 256 tiles
+  int tc_pair_epw = 16;         // epilogue warps of the 256 x 256 pair tiles (8 or 16)
 
   // band pairs split over GPUs (qbx_set_band_shard): this GPU's rank among
   // shard_n, and the NCCL communicator (ncclComm_t) of the group

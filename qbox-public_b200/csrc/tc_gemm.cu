@@ -410,15 +410,20 @@ k_tc_split_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant
 // k_tc_split_gemm.  Every mbarrier wait is bounded; both CTAs meet at a
 // cluster barrier after the barriers are set up and again before TMEM is
 // freed, and every path (a timed-out wait included) reaches both.
-constexpr int PAIR_STAGES = 4;
-constexpr int HALF_TILE_BYTES = (BN / 2) * 128;                           // 64 rows of B: 8 KB
-constexpr int PAIR_STAGE_BYTES = 2 * TILE_BYTES + 2 * HALF_TILE_BYTES;   // 48 KB
-constexpr int PAIR_SMEM_BYTES = PAIR_STAGES * PAIR_STAGE_BYTES + 1024 + 256;
+// The pair's tile is 256 rows by BNT = 128 or 256 columns; each CTA holds
+// BNT / 2 rows of B per stage.  With BNT = 256 two accumulators fill the 512
+// TMEM columns, so the correction terms share the hi*hi chain (corr_mul 0).
+template <int BNT> struct PairCfg {
+  static constexpr int HALF_BYTES = (BNT / 2) * 128;                     // 8 or 16 KB
+  static constexpr int STAGE_BYTES = 2 * TILE_BYTES + 2 * HALF_BYTES;   // 48 or 64 KB
+  static constexpr int STAGES = BNT == 128 ? 4 : 3;
+  static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+};
 
-// instruction descriptor of the pair's 256 x 128 MMA
-__host__ __device__ constexpr uint32_t idesc_pair_of(int kind) {
+// instruction descriptor of the pair's 256 x BNT MMA
+__host__ __device__ constexpr uint32_t idesc_pair_of(int kind, int bnt) {
   const uint32_t fmt = kind == KIND_BF16 ? 1u : 2u;
-  return (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(BN >> 3) << 17) |
+  return (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(bnt >> 3) << 17) |
          ((uint32_t)((2 * BM) >> 4) << 24);
 }
 
@@ -475,21 +480,21 @@ __device__ __forceinline__ void tma_load_2d_pair(void* dst, const CUtensorMap* m
       : "memory");
 }
 
-template <int KIND>
+template <int KIND, int BNT>
 __device__ __forceinline__ void umma_pair(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t acc) {
   if constexpr (KIND == KIND_BF16) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-        "l"(da), "l"(db), "r"(idesc_pair_of(KIND_BF16)), "r"(acc)
+        "l"(da), "l"(db), "r"(idesc_pair_of(KIND_BF16, BNT)), "r"(acc)
         : "memory");
   } else {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::2.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-        "l"(da), "l"(db), "r"(idesc_pair_of(KIND_TF32)), "r"(acc)
+        "l"(da), "l"(db), "r"(idesc_pair_of(KIND_TF32, BNT)), "r"(acc)
         : "memory");
   }
 }
@@ -505,7 +510,7 @@ __device__ __forceinline__ void umma_commit_pair(uint64_t* bar) {
       : "memory");
 }
 
-template <int KIND, int EPW>
+template <int KIND, int EPW, int BNT>
 __global__ void __launch_bounds__(threads_of(EPW), 1)
 k_tc_pair_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant__ CUtensorMap ma_lo,
                const __grid_constant__ CUtensorMap mb_hi, const __grid_constant__ CUtensorMap mb_lo,
@@ -518,7 +523,8 @@ k_tc_pair_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant_
   // from HBM once.
   const int mt = ws ? (int)blockIdx.x : 2 * (int)blockIdx.y + (int)(blockIdx.x & 1);
   const int nt = ws ? (int)blockIdx.y : (int)(blockIdx.x >> 1);
-  const int m0 = mt * BM, n0 = nt * BN;
+  using P = PairCfg<BNT>;
+  const int m0 = mt * BM, n0 = nt * BNT;
   // lower: a pair whose every row lies above the tile's first column holds
   // only the strict upper triangle; both CTAs leave before anything is set up
   if (lower && n0 >= (mt & ~1) * BM + 2 * BM) return;
@@ -526,9 +532,9 @@ k_tc_pair_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant_
   const bool lead = rank == 0;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  uint64_t* full = (uint64_t*)(base + PAIR_STAGES * PAIR_STAGE_BYTES);
-  uint64_t* empty = full + PAIR_STAGES;
-  uint64_t* tfull = empty + PAIR_STAGES;
+  uint64_t* full = (uint64_t*)(base + P::STAGES * P::STAGE_BYTES);
+  uint64_t* empty = full + P::STAGES;
+  uint64_t* tfull = empty + P::STAGES;
   uint64_t* tfree = tfull + 2;
   uint64_t* cfull = tfree + 2;
   uint64_t* cfree = cfull + 2;
@@ -538,13 +544,13 @@ k_tc_pair_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant_
   const int kb0 = blockIdx.z * kb_per_split;
   const int kb1 = min(nkb, kb0 + kb_per_split);
   const int niter = max(0, kb1 - kb0);
-  const int nchunk = (niter + chunk - 1) / chunk;
   const int sep = corr_mul > 0 ? 1 : 0;
+  const int nchunk = (niter + chunk - 1) / chunk;
   const int cchunk = chunk * (sep ? corr_mul : 1);
-  const uint32_t tmem_cols = tmem_cols_of(sep);
+  const uint32_t tmem_cols = (uint32_t)(sep ? 4 * BNT : 2 * BNT);
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < PAIR_STAGES; s++) {
+    for (int s = 0; s < P::STAGES; s++) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
@@ -573,34 +579,80 @@ k_tc_pair_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant_
     // ---------------- TMA producer (both CTAs)
     bool ok = true;
     for (int it = 0; it < niter; ++it) {
-      const int s = it % PAIR_STAGES;
-      const uint32_t ph = (uint32_t)((it / PAIR_STAGES) & 1);
+      const int s = it % P::STAGES;
+      const uint32_t ph = (uint32_t)((it / P::STAGES) & 1);
       if (!mbar_wait_cluster(&empty[s], ph ^ 1u)) {
         atomicExch(err, 1);
         ok = false;
         break;
       }
-      unsigned char* st = base + s * PAIR_STAGE_BYTES;
+      unsigned char* st = base + s * P::STAGE_BYTES;
       const uint32_t fb = cluster_addr(&full[s], 0);
-      if (lead) mbar_expect_tx(&full[s], 2 * PAIR_STAGE_BYTES);
+      if (lead) mbar_expect_tx(&full[s], 2 * P::STAGE_BYTES);
       const int kx = (kb0 + it) * bk_of(KIND);
-      const int nb = n0 + (int)rank * (BN / 2);
+      const int nb = n0 + (int)rank * (BNT / 2);
       tma_load_2d_pair(st, &ma_hi, fb, kx, m0);
       tma_load_2d_pair(st + TILE_BYTES, &ma_lo, fb, kx, m0);
       tma_load_2d_pair(st + 2 * TILE_BYTES, &mb_hi, fb, kx, nb);
-      tma_load_2d_pair(st + 2 * TILE_BYTES + HALF_TILE_BYTES, &mb_lo, fb, kx, nb);
+      tma_load_2d_pair(st + 2 * TILE_BYTES + P::HALF_BYTES, &mb_lo, fb, kx, nb);
     }
     // every stage's last release (a commit of the first CTA's MMAs) has
     // arrived here before this CTA can leave
-    for (int it = niter; it < niter + PAIR_STAGES && ok; ++it) {
-      const int s = it % PAIR_STAGES;
-      if (!mbar_wait_cluster(&empty[s], (uint32_t)(((it / PAIR_STAGES) & 1) ^ 1))) {
+    for (int it = niter; it < niter + P::STAGES && ok; ++it) {
+      const int s = it % P::STAGES;
+      if (!mbar_wait_cluster(&empty[s], (uint32_t)(((it / P::STAGES) & 1) ^ 1))) {
         atomicExch(err, 7);
         ok = false;
       }
     }
   } else if (warp == 1 && lane == 0 && lead) {
     // ---------------- MMA issuer (first CTA)
+    if (!sep) {
+      // One accumulator chain per `chunk` K blocks holding all three terms.
+      // Each K block issues its small hi*lo and lo*hi products before its
+      // hi*hi products, so the chain's first block adds its small terms to a
+      // sum 2^8 times smaller than the whole (the TMEM additions truncate,
+      // and their error scales with the running sum).
+      for (int c = 0; c < nchunk; ++c) {
+        const int b = c & 1;
+        const int it0 = c * chunk, it1 = min(niter, it0 + chunk);
+        if (c >= 2 && !mbar_wait_cluster(&tfree[b], (uint32_t)(((c >> 1) - 1) & 1))) {
+          atomicExch(err, 4);
+          break;
+        }
+        const uint32_t tacc = tmem + (uint32_t)(b * BNT);
+        uint32_t accumulate = 0u;
+        bool ok = true;
+        for (int it = it0; it < it1; ++it) {
+          const int s = it % P::STAGES;
+          if (!mbar_wait_cluster(&full[s], (uint32_t)((it / P::STAGES) & 1))) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          unsigned char* st = base + s * P::STAGE_BYTES;
+          const uint64_t dah = smem_desc(st);
+          const uint64_t dal = smem_desc(st + TILE_BYTES);
+          const uint64_t dbh = smem_desc(st + 2 * TILE_BYTES);
+          const uint64_t dbl = smem_desc(st + 2 * TILE_BYTES + P::HALF_BYTES);
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const uint64_t off = (uint64_t)(k * 32) >> 4;
+            umma_pair<KIND, BNT>(tacc, dah + off, dbl + off, accumulate);
+            accumulate = 1u;
+            umma_pair<KIND, BNT>(tacc, dal + off, dbh + off, 1u);
+          }
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const uint64_t off = (uint64_t)(k * 32) >> 4;
+            umma_pair<KIND, BNT>(tacc, dah + off, dbh + off, 1u);
+          }
+          umma_commit_pair(&empty[s]);
+        }
+        if (!ok) { atomicExch(err, 2); break; }
+        umma_commit_pair(&tfull[b]);
+      }
+    } else
     for (int it = 0; it < niter; ++it) {
       const int c = it / chunk, b = c & 1;
       const int cc = it / cchunk, cb = cc & 1;
@@ -616,25 +668,25 @@ k_tc_pair_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant_
         atomicExch(err, 5);
         break;
       }
-      const int s = it % PAIR_STAGES;
-      const uint32_t ph = (uint32_t)((it / PAIR_STAGES) & 1);
+      const int s = it % P::STAGES;
+      const uint32_t ph = (uint32_t)((it / P::STAGES) & 1);
       if (!mbar_wait_cluster(&full[s], ph)) { atomicExch(err, 2); break; }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      unsigned char* st = base + s * PAIR_STAGE_BYTES;
+      unsigned char* st = base + s * P::STAGE_BYTES;
       const uint64_t dah = smem_desc(st);
       const uint64_t dal = smem_desc(st + TILE_BYTES);
       const uint64_t dbh = smem_desc(st + 2 * TILE_BYTES);
-      const uint64_t dbl = smem_desc(st + 2 * TILE_BYTES + HALF_TILE_BYTES);
-      const uint32_t tacc = tmem + (uint32_t)(b * BN);
-      const uint32_t tcor = sep ? tmem + (uint32_t)((2 + cb) * BN) : tacc;
+      const uint64_t dbl = smem_desc(st + 2 * TILE_BYTES + P::HALF_BYTES);
+      const uint32_t tacc = tmem + (uint32_t)(b * BNT);
+      const uint32_t tcor = sep ? tmem + (uint32_t)((2 + cb) * BNT) : tacc;
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         const uint64_t off = (uint64_t)(k * 32) >> 4;
         const uint32_t accumulate = (chunk_start && k == 0) ? 0u : 1u;
         const uint32_t cacc = sep ? ((corr_start && k == 0) ? 0u : 1u) : 1u;
-        umma_pair<KIND>(tacc, dah + off, dbh + off, accumulate);
-        umma_pair<KIND>(tcor, dah + off, dbl + off, cacc);
-        umma_pair<KIND>(tcor, dal + off, dbh + off, 1u);
+        umma_pair<KIND, BNT>(tacc, dah + off, dbh + off, accumulate);
+        umma_pair<KIND, BNT>(tcor, dah + off, dbl + off, cacc);
+        umma_pair<KIND, BNT>(tcor, dal + off, dbh + off, 1u);
       }
       umma_commit_pair(&empty[s]);
       if ((it % chunk) == chunk - 1 || it == niter - 1) umma_commit_pair(&tfull[b]);
@@ -642,7 +694,10 @@ k_tc_pair_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant_
     }
   } else if (warp >= 4) {
     // ---------------- epilogue (both CTAs): drain this CTA's TMEM rows
-    constexpr int COLS = BN * 4 / EPW;
+    constexpr int COLS = BNT * 4 / EPW;
+    // TMEM columns per wait: four loads in flight, or one where the tile's
+    // register copy leaves no room for more
+    constexpr int LDW = (COLS > 64 || EPW > 8) ? 16 : 64;
     const int wq = warp & 3;
     const int cbase = ((warp - 4) >> 2) * COLS;
     const int row = m0 + wq * 32 + lane;
@@ -652,13 +707,14 @@ k_tc_pair_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant_
     for (int j = 0; j < COLS; ++j) acc[j] = 0.0f;
     auto drain = [&](uint32_t col0) {
 #pragma unroll
-      for (int c0 = 0; c0 < COLS; c0 += 64) {
-        uint32_t r[64];
+      for (int c0 = 0; c0 < COLS; c0 += LDW) {
+        uint32_t r[LDW];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) tmem_ld16(tlane + col0 + (uint32_t)(c0 + 16 * q), r + 16 * q);
+        for (int q = 0; q < LDW / 16; ++q)
+          tmem_ld16(tlane + col0 + (uint32_t)(c0 + 16 * q), r + 16 * q);
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-        for (int j = 0; j < 64; ++j) acc[c0 + j] += __uint_as_float(r[j]);
+        for (int j = 0; j < LDW; ++j) acc[c0 + j] += __uint_as_float(r[j]);
       }
     };
     bool ok = true;
@@ -670,7 +726,7 @@ k_tc_pair_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant_
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      drain((uint32_t)(b * BN));
+      drain((uint32_t)(b * BNT));
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       __syncwarp();
       if (lane == 0) mbar_arrive_remote(cluster_addr(&tfree[b], 0));
@@ -682,7 +738,7 @@ k_tc_pair_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant_
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        drain((uint32_t)((2 + cb) * BN));
+        drain((uint32_t)((2 + cb) * BNT));
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncwarp();
         if (lane == 0) mbar_arrive_remote(cluster_addr(&cfree[cb], 0));
@@ -706,7 +762,7 @@ k_tc_pair_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant_
           if (col < N) atomicAdd(crow + (size_t)col * ldc, alpha * (double)acc[j]);
         }
       } else {
-        constexpr int G = 16;
+        constexpr int G = (COLS > 64 || EPW > 8) ? 4 : 16;   // loads in flight per group
 #pragma unroll
         for (int j0 = 0; j0 < COLS; j0 += G) {
           double old[G];
@@ -823,10 +879,16 @@ static void tc_gemm_tn(Context& ctx, int kind, int m, int n, int k, double alpha
   const CUtensorMap mbl = kmajor_map(blo, k, n, ldb, kind);
   const int bk = tc::bk_of(kind);
   const int nkb = (k + bk - 1) / bk;
-  const int tm = (m + tc::BM - 1) / tc::BM, tn = (n + tc::BN - 1) / tc::BN;
+  // tile width: 256 columns for CTA pairs with QBX_TC_PAIR=2, else 128
+  const int bnt = ctx.tc_pair == 2 ? 256 : tc::BN;
+  const int tm = (m + tc::BM - 1) / tc::BM, tn = (n + bnt - 1) / bnt;
   QBX_REQUIRE(!lower || m == n, 54, "lower-triangle GEMM of a non-square output");
-  // tiles formed: with lower, those on or below the diagonal of tiles
-  const int tiles = lower ? tm * (tm + 1) / 2 : tm * tn;
+  // tiles formed: with lower, those that meet the lower triangle
+  int tiles = tm * tn;
+  if (lower) {
+    tiles = 0;
+    for (int i = 0; i < tm; i++) tiles += std::min(tn, ((i + 1) * tc::BM + bnt - 1) / bnt);
+  }
   int sms = 148;
   QBX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device));
   // Split K when the output has few tiles: one CTA per SM runs at a time
@@ -872,18 +934,21 @@ static void tc_gemm_tn(Context& ctx, int kind, int m, int n, int k, double alpha
   const int chunk = std::max(1, ctx.tc_chunk), corr_mul = std::max(0, ctx.tc_corr_mul);
   float* ws = splits > 1 ? (float*)ctx.d_tc_ws : nullptr;
   if (ctx.tc_pair) {
-    // CTA pairs: B in half tiles of 64 columns, M tiles padded to an even count
-    const CUtensorMap mbh2 = kmajor_map(bhi, k, n, ldb, kind, tc::BN / 2);
-    const CUtensorMap mbl2 = kmajor_map(blo, k, n, ldb, kind, tc::BN / 2);
+    // CTA pairs: B in half tiles of bnt / 2 columns, M tiles padded to an
+    // even count; 256-column tiles keep the correction terms in the hi*hi
+    // chain and use eight epilogue warps
+    const CUtensorMap mbh2 = kmajor_map(bhi, k, n, ldb, kind, bnt / 2);
+    const CUtensorMap mbl2 = kmajor_map(blo, k, n, ldb, kind, bnt / 2);
+    const int cm = bnt == 256 ? 0 : corr_mul;
     const int tm2 = (tm + 1) & ~1;
     QBX_REQUIRE(splits > 1 ? tn <= 65535 : tm2 / 2 <= 65535, 54, "too many tiles for the grid");
     const dim3 grid2 = splits > 1 ? dim3(tm2, tn, splits) : dim3(2 * tn, tm2 / 2, 1);
-    auto launch2 = [&](auto kern, int epw) {
-      allow_smem(kern, tc::PAIR_SMEM_BYTES);
+    auto launch2 = [&](auto kern, int epw, int smem) {
+      allow_smem(kern, smem);
       cudaLaunchConfig_t cfg = {};
       cfg.gridDim = grid2;
       cfg.blockDim = dim3(tc::threads_of(epw));
-      cfg.dynamicSmemBytes = tc::PAIR_SMEM_BYTES;
+      cfg.dynamicSmemBytes = smem;
       cfg.stream = ctx.stream;
       cudaLaunchAttribute at[1];
       at[0].id = cudaLaunchAttributeClusterDimension;
@@ -893,14 +958,21 @@ static void tc_gemm_tn(Context& ctx, int kind, int m, int n, int k, double alpha
       cfg.attrs = at;
       cfg.numAttrs = 1;
       QBX_CUDA(cudaLaunchKernelEx(&cfg, kern, mah, mal, mbh2, mbl2, m, n, nkb, kbps, ws, C, ldc,
-                                  alpha, beta, err, lower ? 1 : 0, chunk, corr_mul));
+                                  alpha, beta, err, lower ? 1 : 0, chunk, cm));
     };
+    constexpr int S128 = tc::PairCfg<128>::SMEM_BYTES, S256 = tc::PairCfg<256>::SMEM_BYTES;
     if (kind == tc::KIND_BF16) {
-      if (ctx.tc_epw == 8) launch2(tc::k_tc_pair_gemm<tc::KIND_BF16, 8>, 8);
-      else launch2(tc::k_tc_pair_gemm<tc::KIND_BF16, 4>, 4);
+      if (bnt == 256 && ctx.tc_pair_epw == 16)
+        launch2(tc::k_tc_pair_gemm<tc::KIND_BF16, 16, 256>, 16, S256);
+      else if (bnt == 256) launch2(tc::k_tc_pair_gemm<tc::KIND_BF16, 8, 256>, 8, S256);
+      else if (ctx.tc_epw == 8) launch2(tc::k_tc_pair_gemm<tc::KIND_BF16, 8, 128>, 8, S128);
+      else launch2(tc::k_tc_pair_gemm<tc::KIND_BF16, 4, 128>, 4, S128);
     } else {
-      if (ctx.tc_epw == 8) launch2(tc::k_tc_pair_gemm<tc::KIND_TF32, 8>, 8);
-      else launch2(tc::k_tc_pair_gemm<tc::KIND_TF32, 4>, 4);
+      if (bnt == 256 && ctx.tc_pair_epw == 16)
+        launch2(tc::k_tc_pair_gemm<tc::KIND_TF32, 16, 256>, 16, S256);
+      else if (bnt == 256) launch2(tc::k_tc_pair_gemm<tc::KIND_TF32, 8, 256>, 8, S256);
+      else if (ctx.tc_epw == 8) launch2(tc::k_tc_pair_gemm<tc::KIND_TF32, 8, 128>, 8, S128);
+      else launch2(tc::k_tc_pair_gemm<tc::KIND_TF32, 4, 128>, 4, S128);
     }
   } else {
     QBX_REQUIRE(splits > 1 ? tn <= 65535 : tm <= 65535, 54, "too many tiles for the grid");
