@@ -307,7 +307,9 @@ int qbx_set_gemm_backend(qbx_context* ctx, int backend);
 /* One split-precision product D (m x n) = A^T B of host FP64 matrices A
  * (k x m) and B (k x n), column-major, for checking the products on their
  * own: backend 0 = BF16 splits through cuBLAS, 1 = BF16 splits through the
- * library's tcgen05 kernel, 2 = TF32 splits through the tcgen05 kernel. */
+ * library's tcgen05 kernel, 2 = TF32 splits through the tcgen05 kernel, 3 / 4
+ * = BF16 / TF32 splits with A read as an MN-major operand (the form of the
+ * tall updates; needs the default 256 x 256 CTA-pair kernel). */
 int qbx_split_gemm_tn(qbx_context* ctx, int m, int n, int k, const double* a,
                       const double* b, double* d, int backend);
 

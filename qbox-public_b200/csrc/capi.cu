@@ -371,6 +371,7 @@ int qbx_create(qbx_context** out, int device, int precision) {
   if (const char* e = std::getenv("QBX_TC_EPW")) h->c.tc_epw = std::atoi(e) == 4 ? 4 : 8;
   if (const char* e = std::getenv("QBX_TC_PAIR")) h->c.tc_pair = std::max(0, std::min(2, std::atoi(e)));
   if (const char* e = std::getenv("QBX_TC_PAIR_EPW")) h->c.tc_pair_epw = std::atoi(e) == 8 ? 8 : 16;
+  if (const char* e = std::getenv("QBX_TC_TF32_MN")) h->c.tc_tf32_mn = std::atoi(e) != 0 ? 1 : 0;
   if (const char* e = std::getenv("QBX_TC_CORR_MUL")) h->c.tc_corr_mul = std::max(0, std::min(64, std::atoi(e)));
   if (const char* e = std::getenv("QBX_TALL_KIND_HC")) h->c.tall_kind_hc = std::atoi(e) == 1 ? 1 : 0;
   // batches of captured steps: one graph launch per context on its own
@@ -1538,7 +1539,7 @@ int qbx_split_gemm_tn(qbx_context* h, int m, int n, int k, const double* a, cons
                       double* d, int backend) {
   return guarded(h, [&](Context& c) {
     QBX_REQUIRE(m > 0 && n > 0 && k > 0 && a && b && d, 1, "bad GEMM arguments");
-    QBX_REQUIRE(backend >= 0 && backend <= 2, 1, "backend must be 0, 1 or 2");
+    QBX_REQUIRE(backend >= 0 && backend <= 4, 1, "backend must be 0 to 4");
     double *da = dalloc<double>((size_t)k * m), *db = dalloc<double>((size_t)k * n);
     double* dd = dalloc<double>((size_t)m * n);
     void *ah = nullptr, *al = nullptr, *bh = nullptr, *bl = nullptr, *acc = nullptr;
@@ -1557,7 +1558,21 @@ int qbx_split_gemm_tn(qbx_context* h, int m, int n, int k, const double* a, cons
     try {
       h2d_sync(da, a, sizeof(double) * k * m);
       h2d_sync(db, b, sizeof(double) * k * n);
-      if (backend == 2) {
+      if (backend == 3 || backend == 4) {
+        // A as an MN-major operand (its transposed split, m contiguous), B
+        // K-major: the tall-update form, BF16 (3) or TF32 (4) splits
+        const int kind = backend == 3 ? TALL_BF16 : TALL_TF32;
+        const size_t es = backend == 3 ? 2 : 4;
+        const int ldm = (m + 63) / 64 * 64, ldk = (k + 63) / 64 * 64;
+        QBX_CUDA(cudaMalloc(&ah, (size_t)ldm * k * es));
+        QBX_CUDA(cudaMalloc(&al, (size_t)ldm * k * es));
+        QBX_CUDA(cudaMalloc(&bh, (size_t)ldk * n * es));
+        QBX_CUDA(cudaMalloc(&bl, (size_t)ldk * n * es));
+        split_t(c, kind, da, k, m, k, ah, al, ldm);
+        split_plain(c, kind, db, k, n, k, bh, bl, ldk);
+        QBX_CUDA(cudaMemsetAsync(dd, 0, sizeof(double) * m * n, c.stream));
+        tc_gemm_kind_nn_mn(c, kind, m, n, k, 1.0, ah, al, ldm, bh, bl, ldk, 0.0, dd, m);
+      } else if (backend == 2) {
         // TF32 splits through the tcgen05 kind::tf32 kernel
         const int ldk = pad4(k);
         QBX_CUDA(cudaMalloc(&ah, (size_t)ldk * m * 4));

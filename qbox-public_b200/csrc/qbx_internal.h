@@ -421,6 +421,8 @@ struct Context {
   int tc_pair = 2;              // tcgen05 GEMM on CTA pairs (cta_group::2): 0 off (one CTA per
                                 // 128 x 128 tile), 1 256 x 128 tiles, 2 256 x 256 tiles
   int tc_pair_epw = 16;         // epilogue warps of the 256 x 256 pair tiles (8 or 16)
+  int tc_tf32_mn = 1;           // TF32 tall updates read the plain split MN-major (else a
+                                // transposed split)
 
   // band pairs split over GPUs (qbx_set_band_shard): this GPU's rank among
   // shard_n, and the NCCL communicator (ncclComm_t) of the group
@@ -751,6 +753,12 @@ void split_t(Context& ctx, int kind, const double* x, int rows, int cols, int ld
 void tc_gemm_kind_tn(Context& ctx, int kind, int m, int n, int k, double alpha, const void* ahi,
                      const void* alo, int lda, const void* bhi, const void* blo, int ldb,
                      double beta, double* C, int ldc);
+// C (m x n) = alpha * A B + beta * C with A given as its plain split (m
+// contiguous, lda between columns) and B (k x n) K-major: the tall update
+// without a transposed copy of A (CTA pairs on 256 x 256 tiles)
+void tc_gemm_kind_nn_mn(Context& ctx, int kind, int m, int n, int k, double alpha, const void* ahi,
+                        const void* alo, int lda, const void* bhi, const void* blo, int ldb,
+                        double beta, double* C, int ldc);
 void tc_tf32_gemm_tn(Context& ctx, int m, int n, int k, double alpha, const float* ahi,
                      const float* alo, int lda, const float* bhi, const float* blo, int ldb,
                      double beta, double* C, int ldc);

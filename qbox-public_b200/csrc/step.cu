@@ -275,15 +275,28 @@ int polar_entry(Context& ctx, double* x, double tol, int maxiter, bool graph) {
 }
 
 // out += alpha * c * M for the FP64 wavefunction block c (K x n) and an n x n
-// matrix M: the tcgen05 kernel on the transposed split of c (BF16 or TF32
-// hi/lo of the given kind), or three cuBLAS TF32 products on its plain
+// matrix M: the tcgen05 kernel on the split of c (BF16 or TF32 hi/lo of the
+// given kind: its plain split, read MN-major, with the 256 x 256 CTA pairs;
+// else its transposed split), or three cuBLAS TF32 products on its plain
 // split.  out may be c itself: both read the split copy of c.
 static void tall_update(Context& ctx, int kind, const double* c, const double* M, double alpha,
-                        double* out) {
+                        double* out, const void* c_hi = nullptr, const void* c_lo = nullptr) {
   const int n = ctx.nst, K = 2 * ctx.wb.ng;
   if (ctx.gemm_backend == 1) {
     const int ld = Context::tall_ld_of(kind, n);
     split_plain(ctx, kind, M, n, n, n, ctx.tm_hi, ctx.tm_lo, ld);   // M is K-major as stored
+    if (ctx.tc_pair == 2 && (kind == TALL_BF16 || ctx.tc_tf32_mn)) {
+      // the CTA-pair kernel reads c's plain split as an MN-major operand:
+      // the caller's (c_hi, c_lo: this kind, ld ldp) or one made here
+      if (!c_hi) {
+        split_plain(ctx, kind, c, K, n, K, ctx.ct_hi, ctx.ct_lo, ctx.ldp);
+        c_hi = ctx.ct_hi;
+        c_lo = ctx.ct_lo;
+      }
+      tc_gemm_kind_nn_mn(ctx, kind, K, n, n, alpha, c_hi, c_lo, ctx.ldp, ctx.tm_hi, ctx.tm_lo, ld,
+                         1.0, out, K);
+      return;
+    }
     split_t(ctx, kind, c, K, n, K, ctx.ct_hi, ctx.ct_lo, ld);
     tc_gemm_kind_tn(ctx, kind, K, n, n, alpha, ctx.ct_hi, ctx.ct_lo, ld, ctx.tm_hi, ctx.tm_lo, ld,
                     1.0, out, K);
@@ -518,7 +531,10 @@ void psda_update(Context& ctx) {
       split_gemm(ctx, true, false, n, n, K, 2.0, ctx.cs_hi[0], ctx.cs_lo[0], ctx.ldp, ctx.hs_hi,
                  ctx.hs_lo, ctx.ldp, 0.0, A);
       launch_rank1_fix(ctx, A, n, ctx.d_c, K, ctx.d_hc, K, n, n, -1.0, false);
-      tall_update(ctx, ctx.tall_kind_hc, ctx.d_c, A, -1.0, ctx.d_hc);
+      // C's BF16 split from energy() is the MN-major operand when the kinds agree
+      const bool bf = ctx.tall_kind_hc == TALL_BF16;
+      tall_update(ctx, ctx.tall_kind_hc, ctx.d_c, A, -1.0, ctx.d_hc, bf ? ctx.cs_hi[0] : nullptr,
+                  bf ? ctx.cs_lo[0] : nullptr);
     } else {
       QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, K, &two, ctx.d_c, K, ctx.d_hc,
                            K, &zero, A, n));
@@ -691,8 +707,11 @@ void alloc_mixed(Context& ctx) {
   // tall-update splits: room for either kind (TF32 4 bytes at ld pad4,
   // BF16 2 bytes at ld pad8)
   auto tall_bytes = [](size_t rows, size_t cols) { return (size_t)pad8((int)rows) * cols * 4; };
-  QBX_CUDA(cudaMalloc(&ctx.ct_hi, tall_bytes(n, K)));
-  QBX_CUDA(cudaMalloc(&ctx.ct_lo, tall_bytes(n, K)));
+  // ct holds the transposed split of a wavefunction block, or its plain
+  // split (ld ldp) for the MN-major tall updates
+  const size_t ct_bytes = std::max(tall_bytes(n, K), (size_t)ctx.ldp * n * 4);
+  QBX_CUDA(cudaMalloc(&ctx.ct_hi, ct_bytes));
+  QBX_CUDA(cudaMalloc(&ctx.ct_lo, ct_bytes));
   QBX_CUDA(cudaMalloc(&ctx.tm_hi, tall_bytes(std::max(np, n), n)));
   QBX_CUDA(cudaMalloc(&ctx.tm_lo, tall_bytes(std::max(np, n), n)));
   if (np) {

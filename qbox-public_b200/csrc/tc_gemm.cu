@@ -105,6 +105,21 @@ __device__ __forceinline__ uint64_t smem_desc(const void* tile) {
   return ((addr & 0x3FFFF) >> 4) | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
 }
 
+// MN-major operand tile (M contiguous): boxes of 128 bytes of M by the K
+// block, each K row one 128-byte swizzled row; BF16 tiles in 8-row groups
+// 1024 bytes apart (stride byte offset), the boxes (128 bytes of M each)
+// `box_bytes` apart (leading byte offset).
+// TF32 tiles use the 128-byte swizzle with 32-byte atoms (layout type 1):
+// groups of 4 K rows, 512 bytes apart.
+template <int KIND>
+__device__ __forceinline__ uint64_t smem_desc_mn(const void* tile, uint32_t box_bytes) {
+  const uint64_t addr = smem_u32(tile);
+  constexpr uint64_t sbo = KIND == KIND_BF16 ? 1024 : 512;
+  constexpr uint64_t layout = KIND == KIND_BF16 ? 2 : 1;
+  return ((addr & 0x3FFFF) >> 4) | ((uint64_t)(box_bytes >> 4) << 16) | ((sbo >> 4) << 32) |
+         (1ull << 46) | (layout << 61);
+}
+
 // Instruction descriptor: F32 accumulate (bits 4-5 = 1), A and B formats
 // (bits 7-9, 10-12: BF16 = 1 for kind::f16, TF32 = 2 for kind::tf32), both
 // K-major, N >> 3 at bit 17, M >> 4 at bit 24.
@@ -420,11 +435,12 @@ template <int BNT> struct PairCfg {
   static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
 };
 
-// instruction descriptor of the pair's 256 x BNT MMA
-__host__ __device__ constexpr uint32_t idesc_pair_of(int kind, int bnt) {
+// instruction descriptor of the pair's 256 x BNT MMA; amn: A is MN-major
+// (bit 15)
+__host__ __device__ constexpr uint32_t idesc_pair_of(int kind, int bnt, bool amn = false) {
   const uint32_t fmt = kind == KIND_BF16 ? 1u : 2u;
-  return (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(bnt >> 3) << 17) |
-         ((uint32_t)((2 * BM) >> 4) << 24);
+  return (1u << 4) | (fmt << 7) | (fmt << 10) | ((amn ? 1u : 0u) << 15) |
+         ((uint32_t)(bnt >> 3) << 17) | ((uint32_t)((2 * BM) >> 4) << 24);
 }
 
 __device__ __forceinline__ uint32_t cluster_rank() {
@@ -480,21 +496,21 @@ __device__ __forceinline__ void tma_load_2d_pair(void* dst, const CUtensorMap* m
       : "memory");
 }
 
-template <int KIND, int BNT>
+template <int KIND, int BNT, bool AMN = false>
 __device__ __forceinline__ void umma_pair(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t acc) {
   if constexpr (KIND == KIND_BF16) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-        "l"(da), "l"(db), "r"(idesc_pair_of(KIND_BF16, BNT)), "r"(acc)
+        "l"(da), "l"(db), "r"(idesc_pair_of(KIND_BF16, BNT, AMN)), "r"(acc)
         : "memory");
   } else {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::2.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-        "l"(da), "l"(db), "r"(idesc_pair_of(KIND_TF32, BNT)), "r"(acc)
+        "l"(da), "l"(db), "r"(idesc_pair_of(KIND_TF32, BNT, AMN)), "r"(acc)
         : "memory");
   }
 }
@@ -510,7 +526,11 @@ __device__ __forceinline__ void umma_commit_pair(uint64_t* bar) {
       : "memory");
 }
 
-template <int KIND, int EPW, int BNT>
+// AMN: A is MN-major in global memory (its M rows contiguous, as the
+// columns of a SlaterDet are): the tall updates then read the plain split of
+// the wavefunction block instead of a transposed copy.  Its 128 rows per K
+// block arrive as boxes of 128 bytes of M.
+template <int KIND, int EPW, int BNT, bool AMN>
 __global__ void __launch_bounds__(threads_of(EPW), 1)
 k_tc_pair_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant__ CUtensorMap ma_lo,
                const __grid_constant__ CUtensorMap mb_hi, const __grid_constant__ CUtensorMap mb_lo,
@@ -524,6 +544,12 @@ k_tc_pair_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant_
   const int mt = ws ? (int)blockIdx.x : 2 * (int)blockIdx.y + (int)(blockIdx.x & 1);
   const int nt = ws ? (int)blockIdx.y : (int)(blockIdx.x >> 1);
   using P = PairCfg<BNT>;
+  // A descriptors and the step of one MMA's K slice (32 bytes of K within a
+  // K-major row; 16 or 8 rows of 128 bytes down an MN-major tile), in the
+  // descriptor's 16-byte address units
+  constexpr uint32_t A_BOX = AMN ? TILE_BYTES / (BM / (128 / (KIND == KIND_BF16 ? 2 : 4))) : 0;
+  auto a_desc = [](const void* t) { return AMN ? smem_desc_mn<KIND>(t, A_BOX) : smem_desc(t); };
+  constexpr uint64_t AK = AMN ? (uint64_t)(KIND == KIND_BF16 ? 16 : 8) * 128 / 16 : 32 / 16;
   const int m0 = mt * BM, n0 = nt * BNT;
   // lower: a pair whose every row lies above the tile's first column holds
   // only the strict upper triangle; both CTAs leave before anything is set up
@@ -591,8 +617,19 @@ k_tc_pair_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant_
       if (lead) mbar_expect_tx(&full[s], 2 * P::STAGE_BYTES);
       const int kx = (kb0 + it) * bk_of(KIND);
       const int nb = n0 + (int)rank * (BNT / 2);
-      tma_load_2d_pair(st, &ma_hi, fb, kx, m0);
-      tma_load_2d_pair(st + TILE_BYTES, &ma_lo, fb, kx, m0);
+      if constexpr (AMN) {
+        // M boxes of 128 bytes: 64 BF16 or 32 TF32 rows, K block deep
+        constexpr int MW = 128 / (KIND == KIND_BF16 ? 2 : 4);
+        constexpr int BOX = TILE_BYTES / (BM / MW);
+#pragma unroll
+        for (int q = 0; q < BM / MW; ++q) {
+          tma_load_2d_pair(st + q * BOX, &ma_hi, fb, m0 + q * MW, kx);
+          tma_load_2d_pair(st + TILE_BYTES + q * BOX, &ma_lo, fb, m0 + q * MW, kx);
+        }
+      } else {
+        tma_load_2d_pair(st, &ma_hi, fb, kx, m0);
+        tma_load_2d_pair(st + TILE_BYTES, &ma_lo, fb, kx, m0);
+      }
       tma_load_2d_pair(st + 2 * TILE_BYTES, &mb_hi, fb, kx, nb);
       tma_load_2d_pair(st + 2 * TILE_BYTES + P::HALF_BYTES, &mb_lo, fb, kx, nb);
     }
@@ -631,21 +668,21 @@ k_tc_pair_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant_
           }
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
           unsigned char* st = base + s * P::STAGE_BYTES;
-          const uint64_t dah = smem_desc(st);
-          const uint64_t dal = smem_desc(st + TILE_BYTES);
+          const uint64_t dah = a_desc(st);
+          const uint64_t dal = a_desc(st + TILE_BYTES);
           const uint64_t dbh = smem_desc(st + 2 * TILE_BYTES);
           const uint64_t dbl = smem_desc(st + 2 * TILE_BYTES + P::HALF_BYTES);
 #pragma unroll
           for (int k = 0; k < 4; ++k) {
             const uint64_t off = (uint64_t)(k * 32) >> 4;
-            umma_pair<KIND, BNT>(tacc, dah + off, dbl + off, accumulate);
+            umma_pair<KIND, BNT, AMN>(tacc, dah + k * AK, dbl + off, accumulate);
             accumulate = 1u;
-            umma_pair<KIND, BNT>(tacc, dal + off, dbh + off, 1u);
+            umma_pair<KIND, BNT, AMN>(tacc, dal + k * AK, dbh + off, 1u);
           }
 #pragma unroll
           for (int k = 0; k < 4; ++k) {
             const uint64_t off = (uint64_t)(k * 32) >> 4;
-            umma_pair<KIND, BNT>(tacc, dah + off, dbh + off, 1u);
+            umma_pair<KIND, BNT, AMN>(tacc, dah + k * AK, dbh + off, 1u);
           }
           umma_commit_pair(&empty[s]);
         }
@@ -673,8 +710,8 @@ k_tc_pair_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant_
       if (!mbar_wait_cluster(&full[s], ph)) { atomicExch(err, 2); break; }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       unsigned char* st = base + s * P::STAGE_BYTES;
-      const uint64_t dah = smem_desc(st);
-      const uint64_t dal = smem_desc(st + TILE_BYTES);
+      const uint64_t dah = a_desc(st);
+      const uint64_t dal = a_desc(st + TILE_BYTES);
       const uint64_t dbh = smem_desc(st + 2 * TILE_BYTES);
       const uint64_t dbl = smem_desc(st + 2 * TILE_BYTES + P::HALF_BYTES);
       const uint32_t tacc = tmem + (uint32_t)(b * BNT);
@@ -684,9 +721,9 @@ k_tc_pair_gemm(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant_
         const uint64_t off = (uint64_t)(k * 32) >> 4;
         const uint32_t accumulate = (chunk_start && k == 0) ? 0u : 1u;
         const uint32_t cacc = sep ? ((corr_start && k == 0) ? 0u : 1u) : 1u;
-        umma_pair<KIND, BNT>(tacc, dah + off, dbh + off, accumulate);
-        umma_pair<KIND, BNT>(tcor, dah + off, dbl + off, cacc);
-        umma_pair<KIND, BNT>(tcor, dal + off, dbh + off, 1u);
+        umma_pair<KIND, BNT, AMN>(tacc, dah + k * AK, dbh + off, accumulate);
+        umma_pair<KIND, BNT, AMN>(tcor, dah + k * AK, dbl + off, cacc);
+        umma_pair<KIND, BNT, AMN>(tcor, dal + k * AK, dbh + off, 1u);
       }
       umma_commit_pair(&empty[s]);
       if ((it % chunk) == chunk - 1 || it == niter - 1) umma_commit_pair(&tfull[b]);
@@ -837,6 +874,24 @@ static CUtensorMap kmajor_map(const void* ptr, int k, int cols, int ld, int kind
   return map;
 }
 
+// MN-major matrix (M contiguous, ld elements between K rows): boxes of 128
+// bytes of M by one K block, 128-byte swizzle (with 32-byte atoms for TF32)
+static CUtensorMap mn_map(const void* ptr, int m, int k, int ld, int kind) {
+  CUtensorMap map;
+  const size_t es = kind == tc::KIND_BF16 ? 2 : 4;
+  const cuuint64_t dims[2] = {(cuuint64_t)m, (cuuint64_t)k};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * es};
+  const cuuint32_t box[2] = {(cuuint32_t)(128 / es), (cuuint32_t)tc::bk_of(kind)};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = encode_fn()(
+      &map, kind == tc::KIND_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+      2, const_cast<void*>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+      kind == tc::KIND_BF16 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B,
+      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  QBX_REQUIRE(r == CUDA_SUCCESS, 53, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+  return map;
+}
+
 // out(col * ldc + row) = alpha * sum_s ws(s, col * M + row) + beta * out, in FP64
 // (lower: only the tiles the GEMM formed, those that meet the lower triangle)
 __global__ void k_reduce_splits2d(const float* __restrict__ ws, int nsplit, int M, int N,
@@ -864,17 +919,20 @@ bool tc_gemm_supported(const Context& ctx, bool ta, bool tb, int m, int n, int k
 // C (m x n, ld ldc) = alpha * A^T B + beta * C, A (k x m) and B (k x n)
 // K-major splits of the given kind.  The K dimension is split across CTAs
 // only when the output has too few tiles to fill the GPU.
+// amn: A is MN-major (m contiguous, lda between its k rows), CTA pairs on
+// 256 x 256 tiles only.
 static void tc_gemm_tn(Context& ctx, int kind, int m, int n, int k, double alpha, const void* ahi,
                        const void* alo, int lda, const void* bhi, const void* blo, int ldb,
-                       double beta, double* C, int ldc, bool lower = false) {
+                       double beta, double* C, int ldc, bool lower = false, bool amn = false) {
   const size_t es = kind == tc::KIND_BF16 ? 2 : 4;
   QBX_REQUIRE(m > 0 && n > 0 && k > 0 && ldc >= m, 54, "bad tcgen05 GEMM shape");
   QBX_REQUIRE((lda * es) % 16 == 0 && (ldb * es) % 16 == 0, 54,
               "leading dimension not 16-byte aligned");
   QBX_REQUIRE(((uintptr_t)ahi | (uintptr_t)alo | (uintptr_t)bhi | (uintptr_t)blo) % 16 == 0, 54,
               "operand not 16-byte aligned");
-  const CUtensorMap mah = kmajor_map(ahi, k, m, lda, kind);
-  const CUtensorMap mal = kmajor_map(alo, k, m, lda, kind);
+  QBX_REQUIRE(!amn || ctx.tc_pair == 2, 54, "an MN-major A needs the 256 x 256 CTA-pair kernel");
+  const CUtensorMap mah = amn ? mn_map(ahi, m, k, lda, kind) : kmajor_map(ahi, k, m, lda, kind);
+  const CUtensorMap mal = amn ? mn_map(alo, m, k, lda, kind) : kmajor_map(alo, k, m, lda, kind);
   const CUtensorMap mbh = kmajor_map(bhi, k, n, ldb, kind);
   const CUtensorMap mbl = kmajor_map(blo, k, n, ldb, kind);
   const int bk = tc::bk_of(kind);
@@ -961,18 +1019,21 @@ static void tc_gemm_tn(Context& ctx, int kind, int m, int n, int k, double alpha
                                   alpha, beta, err, lower ? 1 : 0, chunk, cm));
     };
     constexpr int S128 = tc::PairCfg<128>::SMEM_BYTES, S256 = tc::PairCfg<256>::SMEM_BYTES;
+    const bool e16 = ctx.tc_pair_epw == 16;
     if (kind == tc::KIND_BF16) {
-      if (bnt == 256 && ctx.tc_pair_epw == 16)
-        launch2(tc::k_tc_pair_gemm<tc::KIND_BF16, 16, 256>, 16, S256);
-      else if (bnt == 256) launch2(tc::k_tc_pair_gemm<tc::KIND_BF16, 8, 256>, 8, S256);
-      else if (ctx.tc_epw == 8) launch2(tc::k_tc_pair_gemm<tc::KIND_BF16, 8, 128>, 8, S128);
-      else launch2(tc::k_tc_pair_gemm<tc::KIND_BF16, 4, 128>, 4, S128);
+      if (amn && e16) launch2(tc::k_tc_pair_gemm<tc::KIND_BF16, 16, 256, true>, 16, S256);
+      else if (amn) launch2(tc::k_tc_pair_gemm<tc::KIND_BF16, 8, 256, true>, 8, S256);
+      else if (bnt == 256 && e16) launch2(tc::k_tc_pair_gemm<tc::KIND_BF16, 16, 256, false>, 16, S256);
+      else if (bnt == 256) launch2(tc::k_tc_pair_gemm<tc::KIND_BF16, 8, 256, false>, 8, S256);
+      else if (ctx.tc_epw == 8) launch2(tc::k_tc_pair_gemm<tc::KIND_BF16, 8, 128, false>, 8, S128);
+      else launch2(tc::k_tc_pair_gemm<tc::KIND_BF16, 4, 128, false>, 4, S128);
     } else {
-      if (bnt == 256 && ctx.tc_pair_epw == 16)
-        launch2(tc::k_tc_pair_gemm<tc::KIND_TF32, 16, 256>, 16, S256);
-      else if (bnt == 256) launch2(tc::k_tc_pair_gemm<tc::KIND_TF32, 8, 256>, 8, S256);
-      else if (ctx.tc_epw == 8) launch2(tc::k_tc_pair_gemm<tc::KIND_TF32, 8, 128>, 8, S128);
-      else launch2(tc::k_tc_pair_gemm<tc::KIND_TF32, 4, 128>, 4, S128);
+      if (amn && e16) launch2(tc::k_tc_pair_gemm<tc::KIND_TF32, 16, 256, true>, 16, S256);
+      else if (amn) launch2(tc::k_tc_pair_gemm<tc::KIND_TF32, 8, 256, true>, 8, S256);
+      else if (bnt == 256 && e16) launch2(tc::k_tc_pair_gemm<tc::KIND_TF32, 16, 256, false>, 16, S256);
+      else if (bnt == 256) launch2(tc::k_tc_pair_gemm<tc::KIND_TF32, 8, 256, false>, 8, S256);
+      else if (ctx.tc_epw == 8) launch2(tc::k_tc_pair_gemm<tc::KIND_TF32, 8, 128, false>, 8, S128);
+      else launch2(tc::k_tc_pair_gemm<tc::KIND_TF32, 4, 128, false>, 4, S128);
     }
   } else {
     QBX_REQUIRE(splits > 1 ? tn <= 65535 : tm <= 65535, 54, "too many tiles for the grid");
@@ -1013,6 +1074,13 @@ void tc_gemm_kind_tn(Context& ctx, int kind, int m, int n, int k, double alpha, 
                      double beta, double* C, int ldc) {
   tc_gemm_tn(ctx, kind == TALL_TF32 ? tc::KIND_TF32 : tc::KIND_BF16, m, n, k, alpha, ahi, alo, lda,
              bhi, blo, ldb, beta, C, ldc);
+}
+
+void tc_gemm_kind_nn_mn(Context& ctx, int kind, int m, int n, int k, double alpha, const void* ahi,
+                        const void* alo, int lda, const void* bhi, const void* blo, int ldb,
+                        double beta, double* C, int ldc) {
+  tc_gemm_tn(ctx, kind == TALL_TF32 ? tc::KIND_TF32 : tc::KIND_BF16, m, n, k, alpha, ahi, alo, lda,
+             bhi, blo, ldb, beta, C, ldc, false, true);
 }
 
 void tc_tf32_gemm_tn(Context& ctx, int m, int n, int k, double alpha, const float* ahi,

@@ -138,3 +138,22 @@ def test_cta_pair_gemm_step_si512_sample(pair, monkeypatch):
     np.testing.assert_allclose(a.get_coeffs(), b.get_coeffs(), rtol=0, atol=ctol)
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("m,n,k,backend", [(128, 256, 1024, 3), (145838, 1024, 1024, 3),
+                                           (300, 130, 1000, 4), (145838, 1024, 1024, 4),
+                                           (1000, 256, 2048, 3)])
+def test_tall_update_with_mn_major_a(ctx_default, m, n, k, backend):
+    """The tall-update form of the CTA-pair kernel: A read as an MN-major
+    operand (its rows contiguous, as the plain split of a wavefunction block
+    lies), B K-major.  BF16 (3) and TF32 (4) splits against the FP64
+    product, within the split-precision bound; partial tiles and the
+    512-atom shape (145 838 rows, 1 024 bands)."""
+    rng = np.random.default_rng(11 * m + n + k)
+    a = rng.standard_normal((k, m)) / np.sqrt(k)
+    b = rng.standard_normal((k, n)) / np.sqrt(k)
+    d = ctx_default.split_gemm_tn(a, b, backend=backend)
+    ref = a.T @ b
+    scale = np.abs(ref).max()
+    bound = 2e-5 if backend == 3 else 2e-6
+    assert np.abs(d - ref).max() < bound * scale + 1e-6
