@@ -732,6 +732,10 @@ void tc_split_gemm(Context& ctx, bool ta, bool tb, int m, int n, int k, double a
 int tc_check_error(Context& ctx);   // nonzero if a tcgen05 GEMM wait ran out
 void split_bf16_2d(Context& ctx, const double* x, int rows, int cols, int ldx, void* hi, void* lo,
                    int ldp);
+// both splits of one block in one pass: BF16 hi/lo (ld ldb, padding rows
+// zero) and TF32 hi/lo (ld ldt)
+void split_bf16_tf32(Context& ctx, const double* x, int rows, int cols, int ldx, void* bhi,
+                     void* blo, int ldb, float* thi, float* tlo, int ldt);
 void split_tf32(Context& ctx, const double* x, int rows, int cols, int ldx, float* hi, float* lo,
                 int ldy);
 void tf32x3_gemm_nn(Context& ctx, int m, int n, int k, double alpha, const float* Ahi,

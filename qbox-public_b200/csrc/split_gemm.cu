@@ -76,13 +76,6 @@ __global__ void k_split_bf16_2d(const double* __restrict__ x, int rows, int cols
   }
 }
 
-void split_bf16_2d(Context& ctx, const double* x, int rows, int cols, int ldx, void* hi, void* lo,
-                   int ldp) {
-  const size_t n = (size_t)ldp * cols;
-  k_split_bf16_2d<<<nblocks(n), 256, 0, ctx.stream>>>(x, rows, cols, ldx, (__nv_bfloat16*)hi,
-                                                      (__nv_bfloat16*)lo, ldp);
-  QBX_LAUNCHED(ctx);
-}
 
 void split_bf16(Context& ctx, const double* x, size_t n, void* hi, void* lo) {
   k_split_bf16<<<nblocks(n), 256, 0, ctx.stream>>>(x, n, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo);
@@ -142,6 +135,84 @@ __device__ __forceinline__ float tf32_round(float x) {
   return __uint_as_float(u);
 }
 
+// The splits of a column-major FP64 block, four consecutive rows a thread
+// (two 16-byte loads, 8- or 16-byte stores), one column per grid row, so no
+// index division: BF16 hi/lo (ld ldb, the padding rows up to ldb zero) and/or
+// TF32 hi/lo (ld ldt, rows < rows only).  Needs x 16-byte aligned, ldx even
+// and ldb, ldt multiples of 4.
+template <bool BF, bool TF>
+__global__ void k_split2d_v4(const double* __restrict__ x, int rows, int ldx,
+                             __nv_bfloat16* __restrict__ bhi, __nv_bfloat16* __restrict__ blo,
+                             int ldb, float* __restrict__ thi, float* __restrict__ tlo, int ldt,
+                             int span) {
+  const int c = blockIdx.y;
+  const double* xc = x + (size_t)c * ldx;
+  for (int r = 4 * (blockIdx.x * blockDim.x + threadIdx.x); r < span;
+       r += 4 * gridDim.x * blockDim.x) {
+    double v[4];
+    if (r + 3 < rows) {
+      const double2 a = *reinterpret_cast<const double2*>(xc + r);
+      const double2 b = *reinterpret_cast<const double2*>(xc + r + 2);
+      v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+    } else {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) v[q] = r + q < rows ? xc[r + q] : 0.0;
+    }
+    if constexpr (BF) {
+      __nv_bfloat16 h[4], l[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        h[q] = __double2bfloat16(v[q]);
+        l[q] = __double2bfloat16(v[q] - (double)__bfloat162float(h[q]));
+      }
+      if (r < ldb) {
+        *reinterpret_cast<uint2*>(bhi + (size_t)c * ldb + r) = *reinterpret_cast<uint2*>(h);
+        *reinterpret_cast<uint2*>(blo + (size_t)c * ldb + r) = *reinterpret_cast<uint2*>(l);
+      }
+    }
+    if constexpr (TF) {
+      float h[4], l[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        h[q] = tf32_round((float)v[q]);
+        l[q] = tf32_round((float)(v[q] - (double)h[q]));
+      }
+      if (r + 3 < rows) {
+        *reinterpret_cast<float4*>(thi + (size_t)c * ldt + r) = make_float4(h[0], h[1], h[2], h[3]);
+        *reinterpret_cast<float4*>(tlo + (size_t)c * ldt + r) = make_float4(l[0], l[1], l[2], l[3]);
+      } else {
+        for (int q = 0; q < 4 && r + q < rows; ++q) {
+          thi[(size_t)c * ldt + r + q] = h[q];
+          tlo[(size_t)c * ldt + r + q] = l[q];
+        }
+      }
+    }
+  }
+}
+
+static bool v4_ok(const double* x, int ldx, int ld_out) {
+  return ((uintptr_t)x % 16) == 0 && ldx % 2 == 0 && ld_out % 4 == 0;
+}
+
+// grid of the v4 kernel: columns in y, rows / 4 threads in x (capped)
+static dim3 v4_grid(int span, int cols) {
+  const int per = (span + 1023) / 1024;   // 256 threads x 4 rows
+  return dim3((unsigned)std::max(1, std::min(per, 64)), (unsigned)cols);
+}
+
+void split_bf16_2d(Context& ctx, const double* x, int rows, int cols, int ldx, void* hi, void* lo,
+                   int ldp) {
+  if (v4_ok(x, ldx, ldp) && ((uintptr_t)hi | (uintptr_t)lo) % 8 == 0 && cols <= 65535) {
+    k_split2d_v4<true, false><<<v4_grid(ldp, cols), 256, 0, ctx.stream>>>(
+        x, rows, ldx, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo, ldp, nullptr, nullptr, 4, ldp);
+  } else {
+    const size_t n = (size_t)ldp * cols;
+    k_split_bf16_2d<<<nblocks(n), 256, 0, ctx.stream>>>(x, rows, cols, ldx, (__nv_bfloat16*)hi,
+                                                        (__nv_bfloat16*)lo, ldp);
+  }
+  QBX_LAUNCHED(ctx);
+}
+
 __global__ void k_split_tf32(const double* __restrict__ x, int rows, int cols, int ldx,
                              float* __restrict__ hi, float* __restrict__ lo, int ldy) {
   const size_t n = (size_t)rows * cols;
@@ -157,8 +228,24 @@ __global__ void k_split_tf32(const double* __restrict__ x, int rows, int cols, i
 
 void split_tf32(Context& ctx, const double* x, int rows, int cols, int ldx, float* hi, float* lo,
                 int ldy) {
-  const size_t n = (size_t)rows * cols;
-  k_split_tf32<<<nblocks(n), 256, 0, ctx.stream>>>(x, rows, cols, ldx, hi, lo, ldy);
+  if (v4_ok(x, ldx, ldy) && ((uintptr_t)hi | (uintptr_t)lo) % 16 == 0 && cols <= 65535) {
+    k_split2d_v4<false, true><<<v4_grid(rows, cols), 256, 0, ctx.stream>>>(
+        x, rows, ldx, nullptr, nullptr, 4, hi, lo, ldy, rows);
+  } else {
+    const size_t n = (size_t)rows * cols;
+    k_split_tf32<<<nblocks(n), 256, 0, ctx.stream>>>(x, rows, cols, ldx, hi, lo, ldy);
+  }
+  QBX_LAUNCHED(ctx);
+}
+
+void split_bf16_tf32(Context& ctx, const double* x, int rows, int cols, int ldx, void* bhi,
+                     void* blo, int ldb, float* thi, float* tlo, int ldt) {
+  QBX_REQUIRE(v4_ok(x, ldx, ldb) && ldt % 4 == 0 && ldb >= rows && ldt >= rows && cols <= 65535 &&
+                  ((uintptr_t)bhi | (uintptr_t)blo) % 8 == 0 &&
+                  ((uintptr_t)thi | (uintptr_t)tlo) % 16 == 0,
+              50, "split of a block into BF16 and TF32: unaligned operands");
+  k_split2d_v4<true, true><<<v4_grid(ldb, cols), 256, 0, ctx.stream>>>(
+      x, rows, ldx, (__nv_bfloat16*)bhi, (__nv_bfloat16*)blo, ldb, thi, tlo, ldt, ldb);
   QBX_LAUNCHED(ctx);
 }
 

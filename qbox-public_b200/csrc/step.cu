@@ -319,8 +319,16 @@ void ortho_align(Context& ctx) {
   if (!mx)
     QBX_CUDA(cudaMemcpyAsync(ctx.d_ctmp, ctx.d_c, sizeof(double) * (size_t)K * n,
                              cudaMemcpyDeviceToDevice, ctx.stream));
-  // in the mixed path slot 0 holds the split of C_last (made in energy())
-  if (mx) split_bf16_2d(ctx, ctx.d_c, K, n, K, ctx.cs_hi[1], ctx.cs_lo[1], ctx.ldp);
+  // in the mixed path slot 0 holds the split of C_last (made in energy());
+  // where the rotation reads C's plain TF32 split, both splits of C are made
+  // in one pass
+  const bool both = mx && ctx.gemm_backend == 1 && ctx.tc_pair == 2 && ctx.tc_tf32_mn &&
+                    ctx.tall_kind == TALL_TF32;
+  if (both)
+    split_bf16_tf32(ctx, ctx.d_c, K, n, K, ctx.cs_hi[1], ctx.cs_lo[1], ctx.ldp, (float*)ctx.ct_hi,
+                    (float*)ctx.ct_lo, ctx.ldp);
+  else if (mx)
+    split_bf16_2d(ctx, ctx.d_c, K, n, K, ctx.cs_hi[1], ctx.cs_lo[1], ctx.ldp);
   overlap_cholesky(ctx, ctx.d_c, L, ST_INFO_ORTHO, mx ? 1 : -1);
   // B = 2 C^T C_last - c0 c_last0^T
   {
@@ -345,7 +353,8 @@ void ortho_align(Context& ctx) {
     double* T = ctx.d_nn3;
     launch_identity_axpy(ctx, T, X, n, -1.0);
     // rotation: TF32 splits, so that C stays orthonormal to ~1e-7
-    tall_update(ctx, ctx.tall_kind, ctx.d_c, T, -1.0, ctx.d_c);
+    tall_update(ctx, ctx.tall_kind, ctx.d_c, T, -1.0, ctx.d_c, both ? ctx.ct_hi : nullptr,
+                both ? ctx.ct_lo : nullptr);
   } else {
     QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, K, n, n, &one, ctx.d_ctmp, K, X, n,
                          &zero, ctx.d_c, K));
