@@ -429,6 +429,8 @@ struct Context {
   int shard_rank = 0, shard_n = 1;
   void* shard_comm = nullptr;
   void* d_acc32 = nullptr;      // FP32 product accumulator
+  double* d_colred = nullptr;   // per-column partial sums of the fused split kernels
+  size_t colred_elems = 0;
   size_t acc32_elems = 0;
   void* cs_hi[2] = {nullptr, nullptr};   // splits of C (0: at energy, 1: after the step)
   void* cs_lo[2] = {nullptr, nullptr};
@@ -736,6 +738,13 @@ void split_bf16_2d(Context& ctx, const double* x, int rows, int cols, int ldx, v
 // zero) and TF32 hi/lo (ld ldt)
 void split_bf16_tf32(Context& ctx, const double* x, int rows, int cols, int ldx, void* bhi,
                      void* blo, int ldb, float* thi, float* tlo, int ldt);
+// the BF16 split of a wavefunction block (rows = 2 ngw) with the kinetic sum
+// sum_n occ_n sum_G g2(G) |c_n(G)|^2 of the same pass into *out
+void split_bf16_ekin(Context& ctx, const double* x, int rows, int cols, int ldx, void* hi,
+                     void* lo, int ldp, const double* g2, const double* occ, double* out);
+// diag(S) = 2 C^T C - c0 c0^T on the diagonal, exact in FP64, from the
+// column sums of the last split_bf16_tf32 of c
+void overlap_diag_from_split(Context& ctx, const double* c, int K, int n, int ldp, double* S);
 void split_tf32(Context& ctx, const double* x, int rows, int cols, int ldx, float* hi, float* lo,
                 int ldy);
 void tf32x3_gemm_nn(Context& ctx, int m, int n, int k, double alpha, const float* Ahi,

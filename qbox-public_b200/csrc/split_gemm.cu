@@ -15,6 +15,7 @@
 #include <algorithm>
 
 #include "qbx_internal.h"
+#include "reduce.cuh"
 #include <cuda_bf16.h>
 
 namespace qbx {
@@ -140,13 +141,19 @@ __device__ __forceinline__ float tf32_round(float x) {
 // index division: BF16 hi/lo (ld ldb, the padding rows up to ldb zero) and/or
 // TF32 hi/lo (ld ldt, rows < rows only).  Needs x 16-byte aligned, ldx even
 // and ldb, ldt multiples of 4.
-template <bool BF, bool TF>
+// RED also sums, per column, the squares of its FP64 values (1) or the
+// squares weighted by g2[row / 2] (2, the kinetic sum of a band over its
+// complex coefficients) into part[column * gridDim.x + blockIdx.x]: fixed
+// partials that the finishing kernels add in order.
+template <bool BF, bool TF, int RED = 0>
 __global__ void k_split2d_v4(const double* __restrict__ x, int rows, int ldx,
                              __nv_bfloat16* __restrict__ bhi, __nv_bfloat16* __restrict__ blo,
                              int ldb, float* __restrict__ thi, float* __restrict__ tlo, int ldt,
-                             int span) {
+                             int span, const double* __restrict__ g2 = nullptr,
+                             double* __restrict__ part = nullptr) {
   const int c = blockIdx.y;
   const double* xc = x + (size_t)c * ldx;
+  double acc = 0.0;
   for (int r = 4 * (blockIdx.x * blockDim.x + threadIdx.x); r < span;
        r += 4 * gridDim.x * blockDim.x) {
     double v[4];
@@ -157,6 +164,16 @@ __global__ void k_split2d_v4(const double* __restrict__ x, int rows, int ldx,
     } else {
 #pragma unroll
       for (int q = 0; q < 4; ++q) v[q] = r + q < rows ? xc[r + q] : 0.0;
+    }
+    if constexpr (RED == 1) {
+      acc += v[0] * v[0] + v[1] * v[1] + v[2] * v[2] + v[3] * v[3];
+    } else if constexpr (RED == 2) {
+      // rows r .. r + 3 are the real and imaginary parts of coefficients
+      // r / 2 and r / 2 + 1 (r even); rows past `rows` are zero
+      if (r < rows) {
+        const double w0 = g2[r >> 1], w1 = r + 2 < rows ? g2[(r >> 1) + 1] : 0.0;
+        acc += (v[0] * v[0] + v[1] * v[1]) * w0 + (v[2] * v[2] + v[3] * v[3]) * w1;
+      }
     }
     if constexpr (BF) {
       __nv_bfloat16 h[4], l[4];
@@ -187,6 +204,11 @@ __global__ void k_split2d_v4(const double* __restrict__ x, int rows, int ldx,
         }
       }
     }
+  }
+  if constexpr (RED != 0) {
+    __shared__ double sh[32];
+    const double t = red::block_sum(acc, sh);
+    if (threadIdx.x == 0) part[(size_t)c * gridDim.x + blockIdx.x] = t;
   }
 }
 
@@ -238,14 +260,64 @@ void split_tf32(Context& ctx, const double* x, int rows, int cols, int ldx, floa
   QBX_LAUNCHED(ctx);
 }
 
+// diag(S)_c = 2 sum of the squares of column c - x(0, c)^2, from the
+// partials of k_split2d_v4<..., 1> (one thread per column, partials in order)
+__global__ void k_diag_from_partials(const double* __restrict__ part, int nb,
+                                     const double* __restrict__ x, int ldx, int cols,
+                                     double* __restrict__ S, int lds) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cols) return;
+  double t = 0.0;
+  for (int b = 0; b < nb; b++) t += part[(size_t)c * nb + b];
+  const double x0 = x[(size_t)c * ldx];
+  S[(size_t)c * lds + c] = 2.0 * t - x0 * x0;
+}
+
+// sum over columns of w[c] times the column's partials, into out[0]
+__global__ void k_weighted_from_partials(const double* __restrict__ part, int nb,
+                                         const double* __restrict__ w, int cols,
+                                         double* __restrict__ out) {
+  __shared__ double sh[32];
+  double a = 0.0;
+  for (int c = threadIdx.x; c < cols; c += blockDim.x) {
+    double t = 0.0;
+    for (int b = 0; b < nb; b++) t += part[(size_t)c * nb + b];
+    a += w[c] * t;
+  }
+  const double s = red::block_sum(a, sh);
+  if (threadIdx.x == 0) out[0] = s;
+}
+
+void split_bf16_ekin(Context& ctx, const double* x, int rows, int cols, int ldx, void* hi,
+                     void* lo, int ldp, const double* g2, const double* occ, double* out) {
+  QBX_REQUIRE(v4_ok(x, ldx, ldp) && ((uintptr_t)hi | (uintptr_t)lo) % 8 == 0 && cols <= 65535 &&
+                  rows % 2 == 0 && (size_t)cols * 64 <= ctx.colred_elems,
+              50, "split with the kinetic sums: unaligned operands or no room for the partials");
+  const dim3 g = v4_grid(ldp, cols);
+  k_split2d_v4<true, false, 2><<<g, 256, 0, ctx.stream>>>(
+      x, rows, ldx, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo, ldp, nullptr, nullptr, 4, ldp, g2,
+      ctx.d_colred);
+  QBX_LAUNCHED(ctx);
+  k_weighted_from_partials<<<1, 256, 0, ctx.stream>>>(ctx.d_colred, (int)g.x, occ, cols, out);
+  QBX_LAUNCHED(ctx);
+}
+
 void split_bf16_tf32(Context& ctx, const double* x, int rows, int cols, int ldx, void* bhi,
                      void* blo, int ldb, float* thi, float* tlo, int ldt) {
   QBX_REQUIRE(v4_ok(x, ldx, ldb) && ldt % 4 == 0 && ldb >= rows && ldt >= rows && cols <= 65535 &&
                   ((uintptr_t)bhi | (uintptr_t)blo) % 8 == 0 &&
                   ((uintptr_t)thi | (uintptr_t)tlo) % 16 == 0,
               50, "split of a block into BF16 and TF32: unaligned operands");
-  k_split2d_v4<true, true><<<v4_grid(ldb, cols), 256, 0, ctx.stream>>>(
-      x, rows, ldx, (__nv_bfloat16*)bhi, (__nv_bfloat16*)blo, ldb, thi, tlo, ldt, ldb);
+  QBX_REQUIRE((size_t)cols * 64 <= ctx.colred_elems, 50, "no room for the column partials");
+  k_split2d_v4<true, true, 1><<<v4_grid(ldb, cols), 256, 0, ctx.stream>>>(
+      x, rows, ldx, (__nv_bfloat16*)bhi, (__nv_bfloat16*)blo, ldb, thi, tlo, ldt, ldb, nullptr,
+      ctx.d_colred);
+  QBX_LAUNCHED(ctx);
+}
+
+void overlap_diag_from_split(Context& ctx, const double* c, int K, int n, int ldp, double* S) {
+  const int nb = (int)v4_grid(ldp, n).x;
+  k_diag_from_partials<<<(n + 127) / 128, 128, 0, ctx.stream>>>(ctx.d_colred, nb, c, K, n, S, n);
   QBX_LAUNCHED(ctx);
 }
 

@@ -25,7 +25,8 @@ static bool mixed(const Context& ctx) { return ctx.precision == MIXED; }
 // diagonal is recomputed exactly in FP64.  The factorisation's info code
 // goes to the status word `status` (checked when the step's scalars are
 // read back: a matrix that is not positive definite is an error there).
-static void overlap_cholesky(Context& ctx, const double* c, double* S, int status, int split) {
+static void overlap_cholesky(Context& ctx, const double* c, double* S, int status, int split,
+                             bool diag_from_split = false) {
   ProfScope ps(ctx, "overlap_cholesky");
   const int n = ctx.nst, K = 2 * ctx.wb.ng;
   const double two = 2.0, zero = 0.0;
@@ -34,7 +35,8 @@ static void overlap_cholesky(Context& ctx, const double* c, double* S, int statu
     split_gemm(ctx, true, false, n, n, K, 2.0, ctx.cs_hi[split], ctx.cs_lo[split], ctx.ldp,
                ctx.cs_hi[split], ctx.cs_lo[split], ctx.ldp, 0.0, S, true);
     launch_rank1_fix(ctx, S, n, c, K, c, K, n, n, -1.0, true);
-    overlap_diag_f64(ctx, c, K, n, S);
+    if (diag_from_split) overlap_diag_from_split(ctx, c, K, n, ctx.ldp, S);
+    else overlap_diag_f64(ctx, c, K, n, S);
   } else {
     QBX_BLAS(cublasDsyrk(ctx.blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, n, K, &two, c, K, &zero,
                          S, n));
@@ -329,7 +331,7 @@ void ortho_align(Context& ctx) {
                     (float*)ctx.ct_lo, ctx.ldp);
   else if (mx)
     split_bf16_2d(ctx, ctx.d_c, K, n, K, ctx.cs_hi[1], ctx.cs_lo[1], ctx.ldp);
-  overlap_cholesky(ctx, ctx.d_c, L, ST_INFO_ORTHO, mx ? 1 : -1);
+  overlap_cholesky(ctx, ctx.d_c, L, ST_INFO_ORTHO, mx ? 1 : -1, both);
   // B = 2 C^T C_last - c0 c_last0^T
   {
     ProfScope ps(ctx, "gemm_overlap_last");
@@ -508,10 +510,16 @@ void nonlocal_only(Context& ctx, bool hpsi, double* out) {
 // EnergyFunctional::energy (src/EnergyFunctional.cpp:397-1044)
 void energy(Context& ctx, bool hpsi, bool forces) {
   ProfScope ps(ctx, "energy");
-  if (mixed(ctx))
-    split_bf16_2d(ctx, ctx.d_c, 2 * ctx.wb.ng, ctx.nst, 2 * ctx.wb.ng, ctx.cs_hi[0], ctx.cs_lo[0],
-                  ctx.ldp);
-  launch_ekin(ctx);
+  if (mixed(ctx) && ctx.d_colred) {
+    // the split for the inner products and the kinetic sum in one pass over C
+    split_bf16_ekin(ctx, ctx.d_c, 2 * ctx.wb.ng, ctx.nst, 2 * ctx.wb.ng, ctx.cs_hi[0],
+                    ctx.cs_lo[0], ctx.ldp, ctx.d_g2_w, ctx.d_occ, ctx.d_scalars + SLOT_EKIN);
+  } else {
+    if (mixed(ctx))
+      split_bf16_2d(ctx, ctx.d_c, 2 * ctx.wb.ng, ctx.nst, 2 * ctx.wb.ng, ctx.cs_hi[0],
+                    ctx.cs_lo[0], ctx.ldp);
+    launch_ekin(ctx);
+  }
   if (hpsi) {
     ProfScope pv(ctx, "vpsi");
     launch_vpsi(ctx, ctx.d_c, ctx.d_vr, ctx.d_hc);   // hc = 1/2 G^2 c + V psi
@@ -672,6 +680,8 @@ void free_mixed(Context& ctx) {
                    &ctx.d_tc_ws};
   for (void** b : bufs)
     if (*b) { cudaFree(*b); *b = nullptr; }
+  dfree(ctx.d_colred);
+  ctx.colred_elems = 0;
   dfree(ctx.c32);
   dfree(ctx.c32lo);
   dfree(ctx.a32);
@@ -696,6 +706,8 @@ void alloc_mixed(Context& ctx) {
   const size_t small = std::max(np * n, n * n);
   ctx.acc32_elems = std::max(wf, std::max(np * n, std::max(K * np, n * n)));
   QBX_CUDA(cudaMalloc(&ctx.d_acc32, ctx.acc32_elems * sizeof(float)));
+  ctx.colred_elems = 64 * n;
+  ctx.d_colred = dalloc<double>(ctx.colred_elems);
   for (int s = 0; s < 2; s++) {
     QBX_CUDA(cudaMalloc(&ctx.cs_hi[s], wf * 2));
     QBX_CUDA(cudaMalloc(&ctx.cs_lo[s], wf * 2));
