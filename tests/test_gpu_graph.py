@@ -139,3 +139,28 @@ def test_polar_matches_oracle(name, graph):
         assert np.abs(got.T @ got - np.eye(s.nbands)).max() < 1e-9, kind
         assert 1 <= iters <= 20, (kind, iters)
     ctx.close()
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_polar_mixed_higham_by_cholesky(graph):
+    """The mixed path's Higham steps form x^-T from the Cholesky factor of
+    x^T x instead of a pivoted LU of x^T: the polar factor is the oracle's
+    to 1e-8 and orthogonal to 1e-9, for the near-orthogonal case, the
+    symmetric one (polar factor I) and a rotated one with singular values
+    from 0.1 to 3, eagerly and captured."""
+    from oracle import qbox_np
+    s = systems.get("si64")
+    ctx = capi.from_system(s, precision=capi.MIXED)
+    n = s.nbands
+    cases = _polar_cases(n, 11)
+    rng = np.random.default_rng(5)
+    u, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    v, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    cases["rotated"] = u @ np.diag(np.linspace(0.1, 3.0, n)) @ v.T
+    for kind, x in cases.items():
+        ref = qbox_np.polar(x.copy(), 1e-6, 20)
+        got, iters = ctx.polar(x, 1e-6, 20, graph=graph)
+        np.testing.assert_allclose(got, ref, rtol=0, atol=1e-8, err_msg=kind)
+        assert np.abs(got.T @ got - np.eye(n)).max() < 1e-9, kind
+        assert 1 <= iters <= 20, (kind, iters)
+    ctx.close()
