@@ -466,6 +466,28 @@ __global__ void k_grid_real(const double2* __restrict__ grid, size_t n, double* 
     f[i] = grid[i].x;
 }
 
+// both parts of a grid of two packed real fields
+__global__ void k_grid_split(const double2* __restrict__ grid, size_t n, double* __restrict__ f0,
+                             double* __restrict__ f1) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const double2 v = grid[i];
+    f0[i] = v.x;
+    f1[i] = v.y;
+  }
+}
+
+// grid = f0 w + i f1 w (f1 may be null)
+__global__ void k_real2_mul_to_grid(const double* __restrict__ f0, const double* __restrict__ f1,
+                                    const double* __restrict__ w, size_t n,
+                                    double2* __restrict__ grid) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const double x = w[i];
+    grid[i] = make_double2(f0[i] * x, f1 ? f1[i] * x : 0.0);
+  }
+}
+
 // ------------------------------------------------------------ launchers
 static std::vector<double2> twiddle_table(int n) {
   std::vector<double2> t(n);
@@ -1016,6 +1038,36 @@ void vb_backward(Context& ctx, const double* coef, double* real_out) {
   QBX_LAUNCHED(ctx);
   grid_fft(ctx, +1);
   k_grid_real<<<nblk(N), 256, 0, ctx.stream>>>((const double2*)ctx.d_grid, N, real_out);
+  QBX_LAUNCHED(ctx);
+}
+
+void vb_backward_pair(Context& ctx, const double* a, const double* b, double* out0, double* out1) {
+  const size_t N = ctx.N();
+  QBX_CUDA(cudaMemsetAsync(ctx.d_grid, 0, N * sizeof(double2), ctx.stream));
+  k_scatter_pair<<<nblk(ctx.vb.ng), 256, 0, ctx.stream>>>((const double2*)a, (const double2*)b,
+                                                          ctx.dvs.ip, ctx.dvs.im, ctx.vb.ng,
+                                                          (double2*)ctx.d_grid);
+  QBX_LAUNCHED(ctx);
+  grid_fft(ctx, +1);
+  k_grid_split<<<nblk(N), 256, 0, ctx.stream>>>((const double2*)ctx.d_grid, N, out0, out1);
+  QBX_LAUNCHED(ctx);
+}
+
+void vb_forward_real_pair(Context& ctx, const double* f0, const double* f1, const double* w,
+                          double* c0, double* c1) {
+  const size_t N = ctx.N();
+  k_real2_mul_to_grid<<<nblk(N), 256, 0, ctx.stream>>>(f0, f1, w, N, (double2*)ctx.d_grid);
+  QBX_LAUNCHED(ctx);
+  grid_fft(ctx, -1);
+  if (f1) {
+    k_gather_pair<<<nblk(ctx.vb.ng), 256, 0, ctx.stream>>>((const double2*)ctx.d_grid, ctx.dvs.ip,
+                                                           ctx.dvs.im, ctx.vb.ng, 1.0 / (double)N,
+                                                           (double2*)c0, (double2*)c1);
+  } else {
+    k_gather_sphere<<<nblk(ctx.vb.ng), 256, 0, ctx.stream>>>((const double2*)ctx.d_grid, ctx.dvs.ip,
+                                                             ctx.vb.ng, 1.0 / (double)N,
+                                                             (double2*)c0);
+  }
   QBX_LAUNCHED(ctx);
 }
 

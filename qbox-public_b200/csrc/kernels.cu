@@ -145,6 +145,18 @@ __global__ void k_mul_igx(const double2* __restrict__ in, const double* __restri
   }
 }
 
+// out(G) = sum_j i gx_j(G) in_j(G)
+__global__ void k_sum_igx3(const double2* __restrict__ a, const double2* __restrict__ b,
+                           const double2* __restrict__ c, const double* __restrict__ gx, int ng,
+                           double2* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ng; i += gridDim.x * blockDim.x) {
+    const double g0 = gx[i], g1 = gx[(size_t)ng + i], g2 = gx[2 * (size_t)ng + i];
+    const double2 u = a[i], v = b[i], w = c[i];
+    const double re = g0 * u.x + g1 * v.x + g2 * w.x, im = g0 * u.y + g1 * v.y + g2 * w.y;
+    out[i] = make_double2(-im, re);
+  }
+}
+
 __global__ void k_mul(const double* __restrict__ a, const double* __restrict__ b, size_t n,
                       double* __restrict__ out) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
@@ -185,33 +197,34 @@ void launch_xc(Context& ctx) {
     reduce<1>(ctx, DotF{ctx.d_rhor, ctx.d_vxc}, N, SLOT_EXC + 2);   // for dxc
     return;
   }
-  // PBE: grad rho by three backward transforms of i G_j rho(G)/Omega
+  // PBE: grad rho as the backward transforms of i G_j rho(G)/Omega, two real
+  // components packed into one complex transform
   const int ngv = ctx.vb.ng;
+  double* xg[3] = {ctx.d_xc_g, ctx.d_xc_g + 2 * (size_t)ngv, ctx.d_xc_g + 4 * (size_t)ngv};
   for (int j = 0; j < 3; j++) {
     k_mul_igx<<<blocks_for(ngv), kThreads, 0, ctx.stream>>>(
         (const double2*)ctx.d_rhog, ctx.d_gx_v + (size_t)j * ngv, ngv, 1.0 / om,
-        (double2*)ctx.d_vtmp_g);
+        (double2*)xg[j]);
     QBX_LAUNCHED(ctx);
-    vb_backward(ctx, ctx.d_vtmp_g, ctx.d_grad + j * N);
   }
+  vb_backward_pair(ctx, xg[0], xg[1], ctx.d_grad, ctx.d_grad + N);
+  vb_backward(ctx, xg[2], ctx.d_grad + 2 * N);
   k_pbe<<<nb, kThreads, 0, ctx.stream>>>(ctx.d_rhor, ctx.d_grad, N, ctx.d_vxc, ctx.d_vx2,
                                          ctx.d_exc);
   QBX_LAUNCHED(ctx);
   // sum e_xc and sum rho v1 (the latter for the XC stress)
   reduce<2>(ctx, SumRhoV1F{ctx.d_exc, ctx.d_rhor, ctx.d_vxc}, N, SLOT_EXC);
-  // vxc += sum_j backward(i G_j forward(grad_j vxc2))
-  for (int j = 0; j < 3; j++) {
-    k_mul<<<nb, kThreads, 0, ctx.stream>>>(ctx.d_grad + j * N, ctx.d_vx2, N, ctx.d_exc);
-    QBX_LAUNCHED(ctx);
-    vb_forward_real(ctx, ctx.d_exc, 1.0, ctx.d_vtmp_g);
-    k_mul_igx<<<blocks_for(ngv), kThreads, 0, ctx.stream>>>(
-        (const double2*)ctx.d_vtmp_g, ctx.d_gx_v + (size_t)j * ngv, ngv, 1.0,
-        (double2*)ctx.d_vtmp_g);
-    QBX_LAUNCHED(ctx);
-    vb_backward(ctx, ctx.d_vtmp_g, ctx.d_exc);
-    k_axpy<<<nb, kThreads, 0, ctx.stream>>>(ctx.d_vxc, ctx.d_exc, N);
-    QBX_LAUNCHED(ctx);
-  }
+  // vxc += backward(sum_j i G_j forward(grad_j vxc2)): the forward transforms
+  // two real fields to a complex one, the sum in G space before one backward
+  vb_forward_real_pair(ctx, ctx.d_grad, ctx.d_grad + N, ctx.d_vx2, xg[0], xg[1]);
+  vb_forward_real_pair(ctx, ctx.d_grad + 2 * N, nullptr, ctx.d_vx2, xg[2], nullptr);
+  k_sum_igx3<<<blocks_for(ngv), kThreads, 0, ctx.stream>>>(
+      (const double2*)xg[0], (const double2*)xg[1], (const double2*)xg[2], ctx.d_gx_v, ngv,
+      (double2*)ctx.d_vtmp_g);
+  QBX_LAUNCHED(ctx);
+  vb_backward(ctx, ctx.d_vtmp_g, ctx.d_exc);
+  k_axpy<<<nb, kThreads, 0, ctx.stream>>>(ctx.d_vxc, ctx.d_exc, N);
+  QBX_LAUNCHED(ctx);
   reduce<1>(ctx, DotF{ctx.d_rhor, ctx.d_vxc}, N, SLOT_EXC + 2);   // for dxc
 }
 

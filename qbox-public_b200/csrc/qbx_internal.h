@@ -360,6 +360,7 @@ struct Context {
   double* d_rhops = nullptr;    // 2*ngv (sum of S*rhops)
   double* d_vtmp_g = nullptr;   // 2*ngv scratch
   double* d_vtmp_g2 = nullptr;  // 2*ngv scratch
+  double* d_xc_g = nullptr;     // 3 x 2*ngv: the GGA's density-basis coefficients
   double* d_sfac = nullptr;     // 2*ngv*nsp
   double* d_vps = nullptr;      // ngv*nsp
   double* d_rhops_sp = nullptr; // ngv*nsp
@@ -588,6 +589,13 @@ void launch_vpsi(Context& ctx, const double* c, const double* v, double* hc);
 // vbasis transforms on the full grid
 void vb_backward(Context& ctx, const double* coef, double* real_out);   // real part
 void vb_forward_real(Context& ctx, const double* f, double scale, double* coef);
+// two real fields in one complex transform: out0 + i out1 from the
+// coefficients a and b (both of real fields, half sphere)
+void vb_backward_pair(Context& ctx, const double* a, const double* b, double* out0, double* out1);
+// the coefficients of f0 w and f1 w (f1 may be null) from one complex
+// transform, with the 1/N of the forward transform
+void vb_forward_real_pair(Context& ctx, const double* f0, const double* f1, const double* w,
+                          double* c0, double* c1);
 // wavefunction-basis single transforms through the full-grid path (tests)
 void wb_backward_pair(Context& ctx, const double* c1, const double* c2, double* grid_out);
 
