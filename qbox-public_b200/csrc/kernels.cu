@@ -544,16 +544,65 @@ void launch_nl_forces(Context& ctx, double* fion) {
   }
 }
 
+// Cell and reciprocal vectors (rows) for the phase tables of the kernels
+// below.
+struct CellRows {
+  double a[9];
+  double b[9];
+};
+
+// exp(-i G.tau) for the density-basis vector (x, y, z) from three tables of
+// exp(-i 2 pi h u_j) (u_j = tau.b_j / 2 pi the fractional coordinates, h the
+// Miller index G.a_j / 2 pi), as the reference's StructureFactor builds its
+// phases (src/StructureFactor.cpp:95-151): two complex products per vector
+// instead of a sine and cosine.  Indices outside the tables fall back to
+// sincos.
+__device__ __forceinline__ double2 phase_from_tables(const double2* tab, int hmax,
+                                                     const CellRows& cr, double x, double y,
+                                                     double z, double tx, double ty, double tz) {
+  const double inv2pi = 0.15915494309189533577;
+  const int W = 2 * hmax + 1;
+  const int h0 = __double2int_rn((x * cr.a[0] + y * cr.a[1] + z * cr.a[2]) * inv2pi);
+  const int h1 = __double2int_rn((x * cr.a[3] + y * cr.a[4] + z * cr.a[5]) * inv2pi);
+  const int h2 = __double2int_rn((x * cr.a[6] + y * cr.a[7] + z * cr.a[8]) * inv2pi);
+  if (abs(h0) > hmax || abs(h1) > hmax || abs(h2) > hmax) {
+    double sn, cs;
+    sincos(x * tx + y * ty + z * tz, &sn, &cs);
+    return make_double2(cs, -sn);
+  }
+  const double2 p = tab[h0 + hmax], q = tab[W + h1 + hmax], r = tab[2 * W + h2 + hmax];
+  const double2 pq = make_double2(p.x * q.x - p.y * q.y, p.x * q.y + p.y * q.x);
+  return make_double2(pq.x * r.x - pq.y * r.y, pq.x * r.y + pq.y * r.x);
+}
+
+// the three tables of one atom: tab[j W + h + hmax] = exp(-i 2 pi h u_j)
+__device__ __forceinline__ void phase_tables(double2* tab, int hmax, const CellRows& cr,
+                                             double tx, double ty, double tz) {
+  const int W = 2 * hmax + 1;
+  for (int t = threadIdx.x; t < 3 * W; t += blockDim.x) {
+    const int j = t / W, h = t - j * W - hmax;
+    const double u2 = (tx * cr.b[3 * j] + ty * cr.b[3 * j + 1] + tz * cr.b[3 * j + 2]) *
+                      0.31830988618379067154;   // 2 u = tau.b_j / pi
+    double sn, cs;
+    sincospi((double)h * u2, &sn, &cs);
+    tab[t] = make_double2(cs, -sn);
+  }
+}
+
 // Forces of the local pseudopotential and the Hartree term of the Gaussian
-// pseudocharges (src/EnergyFunctional.cpp:841-930), one CTA per atom.
+// pseudocharges (src/EnergyFunctional.cpp:841-930), one CTA per atom, its
+// phases from the atom's tables in shared memory.
 __global__ void k_local_force(const double* __restrict__ gx, const double2* __restrict__ rhogt,
                               const double2* __restrict__ rhog, const double* __restrict__ vps,
                               const double* __restrict__ rhops, const double* __restrict__ g2i,
                               int ng, double om_inv, const double* __restrict__ tau, double fac,
-                              int atom0, double* __restrict__ fion) {
+                              int atom0, double* __restrict__ fion, CellRows cr, int hmax) {
   __shared__ double sh[32];
+  extern __shared__ double2 tab[];   // 3 (2 hmax + 1)
   const int ia = blockIdx.x;
   const double tx = tau[3 * ia], ty = tau[3 * ia + 1], tz = tau[3 * ia + 2];
+  phase_tables(tab, hmax, cr, tx, ty, tz);
+  __syncthreads();
   const double fpi = 4.0 * M_PI;
   double s0 = 0.0, s1 = 0.0, s2 = 0.0;
   for (int i = threadIdx.x; i < ng; i += blockDim.x) {
@@ -564,8 +613,8 @@ __global__ void k_local_force(const double* __restrict__ gx, const double2* __re
     // vtemp = t conj(rhogt) + vps conj(rhoelg)
     const double vr = t * rt.x + vps[i] * re.x;
     const double vi = -t * rt.y - vps[i] * re.y;
-    double sn, cs;
-    sincos(x * tx + y * ty + z * tz, &sn, &cs);
+    const double2 ph = phase_from_tables(tab, hmax, cr, x, y, z, tx, ty, tz);
+    const double cs = ph.x, sn = -ph.y;
     // exp(-i G.tau) = cs - i sn
     const double tmp = cs * vi + (-sn) * vr;
     s0 += tmp * x; s1 += tmp * y; s2 += tmp * z;
@@ -580,6 +629,22 @@ __global__ void k_local_force(const double* __restrict__ gx, const double2* __re
   }
 }
 
+static CellRows cell_rows(const Context& ctx) {
+  CellRows cr;
+  for (int i = 0; i < 9; i++) {
+    cr.a[i] = ctx.vb.cell[i];
+    cr.b[i] = ctx.vb.recip[i];
+  }
+  return cr;
+}
+// largest Miller index of the density grid
+static int phase_hmax(const Context& ctx) {
+  return std::max(ctx.vb.n0, std::max(ctx.vb.n1, ctx.vb.n2)) / 2 + 1;
+}
+static size_t phase_table_bytes(const Context& ctx) {
+  return sizeof(double2) * 3 * (2 * (size_t)phase_hmax(ctx) + 1);
+}
+
 void launch_local_forces(Context& ctx, double* fion) {
   const int ngv = ctx.vb.ng;
   int atom0 = 0;
@@ -587,10 +652,11 @@ void launch_local_forces(Context& ctx, double* fion) {
     const int na = (int)ctx.tau[is].size() / 3;
     if (na == 0) continue;
     // positions of this species: a slice of the species-major d_tau_all
-    k_local_force<<<na, kThreads, 0, ctx.stream>>>(
+    k_local_force<<<na, kThreads, phase_table_bytes(ctx), ctx.stream>>>(
         ctx.d_gx_v, (const double2*)ctx.d_vtmp_g2, (const double2*)ctx.d_rhog,
         ctx.d_vps + is * (size_t)ngv, ctx.d_rhops_sp + is * (size_t)ngv, ctx.d_g2i_v, ngv,
-        1.0 / ctx.vb.omega, ctx.d_tau_all + 3 * (size_t)atom0, -2.0 * ctx.vb.omega, atom0, fion);
+        1.0 / ctx.vb.omega, ctx.d_tau_all + 3 * (size_t)atom0, -2.0 * ctx.vb.omega, atom0, fion,
+        cell_rows(ctx), phase_hmax(ctx));
     QBX_LAUNCHED(ctx);
     atom0 += na;
   }
@@ -657,6 +723,32 @@ __global__ void k_sfac(const double* __restrict__ gx, int ng, const double* __re
       sincos(x * tau[3 * a] + y * tau[3 * a + 1] + z * tau[3 * a + 2], &sn, &cs);
       re += cs;
       im -= sn;
+    }
+    s[i] = make_double2(re, im);
+  }
+}
+
+// the phase tables of every atom of a species, tab[a 3W + j W + h + hmax]
+__global__ void k_phase_tables(const double* __restrict__ tau, CellRows cr, int hmax,
+                               double2* __restrict__ tab) {
+  const int a = blockIdx.x;
+  phase_tables(tab + (size_t)a * 3 * (2 * hmax + 1), hmax, cr, tau[3 * a], tau[3 * a + 1],
+               tau[3 * a + 2]);
+}
+
+// S(G) = sum_a exp(-i G.tau_a) from the atoms' phase tables
+__global__ void k_sfac_tab(const double* __restrict__ gx, int ng, const double* __restrict__ tau,
+                           int na, const double2* __restrict__ tab, CellRows cr, int hmax,
+                           double2* __restrict__ s) {
+  const int W3 = 3 * (2 * hmax + 1);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ng; i += gridDim.x * blockDim.x) {
+    const double x = gx[i], y = gx[ng + i], z = gx[2 * ng + i];
+    double re = 0.0, im = 0.0;
+    for (int a = 0; a < na; a++) {
+      const double2 ph = phase_from_tables(tab + (size_t)a * W3, hmax, cr, x, y, z, tau[3 * a],
+                                           tau[3 * a + 1], tau[3 * a + 2]);
+      re += ph.x;
+      im += ph.y;
     }
     s[i] = make_double2(re, im);
   }
@@ -758,7 +850,16 @@ void launch_setup_atoms(Context& ctx) {
     // positions of this species: a slice of the species-major d_tau_all
     const double* d_tau = ctx.d_tau_all + 3 * (size_t)atom0;
     double2* sf = (double2*)ctx.d_sfac + (size_t)is * ngv;
-    k_sfac<<<blocks_for(ngv), kThreads, 0, ctx.stream>>>(ctx.d_gx_v, ngv, d_tau, na, sf);
+    if ((size_t)na * phase_table_bytes(ctx) <= ctx.phase_tab_bytes) {
+      k_phase_tables<<<na, 128, 0, ctx.stream>>>(d_tau, cell_rows(ctx), phase_hmax(ctx),
+                                                (double2*)ctx.d_phase_tab);
+      QBX_LAUNCHED(ctx);
+      k_sfac_tab<<<blocks_for(ngv), kThreads, 0, ctx.stream>>>(
+          ctx.d_gx_v, ngv, d_tau, na, (const double2*)ctx.d_phase_tab, cell_rows(ctx),
+          phase_hmax(ctx), sf);
+    } else {
+      k_sfac<<<blocks_for(ngv), kThreads, 0, ctx.stream>>>(ctx.d_gx_v, ngv, d_tau, na, sf);
+    }
     QBX_LAUNCHED(ctx);
     k_vion<<<blocks_for(ngv), kThreads, 0, ctx.stream>>>(sf, ctx.d_vps + (size_t)is * ngv,
                                                          ctx.d_rhops_sp + (size_t)is * ngv, ngv,

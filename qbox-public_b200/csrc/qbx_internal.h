@@ -408,6 +408,8 @@ struct Context {
   double* d_dvnl = nullptr;     // nrad*ngw: dV_nl/dG
   int* d_pcol = nullptr;        // 4*nproj: (l, m, radial row, atom) per column
   double* d_tau_all = nullptr;  // 3*natoms
+  double* d_phase_tab = nullptr;   // per atom exp(-i 2 pi h u_j) tables (structure factors)
+  size_t phase_tab_bytes = 0;
   double* d_twnl = nullptr;     // projector forms Y_lm V_nl, one ngw row per (species, l, m)
   double* d_astress = nullptr;  // 2*ngw*nproj: a strain-derivative projector block
   void* sa_hi = nullptr;        // its BF16 split (mixed path)
