@@ -102,9 +102,10 @@ void free_atoms(Context& c) {
   if (c.h_fion) { cudaFreeHost(c.h_fion); c.h_fion = nullptr; }
   double** bufs[] = {&c.d_anl, &c.d_fnl, &c.d_dfnl, &c.d_pdfac, &c.d_sfac, &c.d_vps,
                      &c.d_rhops_sp, &c.d_fion, &c.d_dvps, &c.d_vnl, &c.d_dvnl,
-                     &c.d_tau_all, &c.d_astress, &c.d_twnl, &c.d_phase_tab};
+                     &c.d_tau_all, &c.d_astress, &c.d_twnl, &c.d_phase_tab, &c.d_fpart};
   for (double** b : bufs) dfree(*b);
   c.phase_tab_bytes = 0;
+  c.fpart_elems = 0;
   dfree(c.d_patom);
   dfree(c.d_pcol);
   if (c.sa_hi) { cudaFree(c.sa_hi); c.sa_hi = nullptr; }
@@ -675,6 +676,8 @@ int qbx_set_atoms(qbx_context* h, const int* na, const double* tau) {
       const int hmax = std::max(c.vb.n0, std::max(c.vb.n1, c.vb.n2)) / 2 + 1;
       c.phase_tab_bytes = (size_t)std::max(1, natoms) * 3 * (2 * (size_t)hmax + 1) * 16;
       c.d_phase_tab = dalloc<double>(c.phase_tab_bytes / sizeof(double));
+      c.fpart_elems = 3 * (size_t)std::max(1, natoms) * 16;
+      c.d_fpart = dalloc<double>(c.fpart_elems);
     }
     c.d_fion = dalloc<double>(3 * std::max(1, natoms));
     QBX_CUDA(cudaMallocHost(&c.h_fion, 3 * std::max(1, natoms) * sizeof(double)));

@@ -629,6 +629,71 @@ __global__ void k_local_force(const double* __restrict__ gx, const double2* __re
   }
 }
 
+// The same forces for kLfAtoms atoms per CTA and one slice of the G vectors
+// per grid row: the per-G factors are formed once for the CTA's atoms, and
+// the slices' partial sums go to part[(atom 3 + j) nslice + slice], added in
+// order by k_local_force_finish.
+constexpr int kLfAtoms = 8;
+__global__ void __launch_bounds__(256)
+k_local_force_multi(const double* __restrict__ gx, const double2* __restrict__ rhogt,
+                    const double2* __restrict__ rhog, const double* __restrict__ vps,
+                    const double* __restrict__ rhops, const double* __restrict__ g2i, int ng,
+                    double om_inv, const double* __restrict__ tau, int na, CellRows cr, int hmax,
+                    double* __restrict__ part) {
+  __shared__ double sh[32];
+  extern __shared__ double2 tabs[];   // kLfAtoms x 3 (2 hmax + 1)
+  const int W3 = 3 * (2 * hmax + 1);
+  const int a0 = blockIdx.x * kLfAtoms, nat = min(kLfAtoms, na - a0);
+  for (int a = 0; a < nat; a++)
+    phase_tables(tabs + (size_t)a * W3, hmax, cr, tau[3 * (a0 + a)], tau[3 * (a0 + a) + 1],
+                 tau[3 * (a0 + a) + 2]);
+  __syncthreads();
+  const int nslice = gridDim.y;
+  const int per = (ng + nslice - 1) / nslice;
+  const int g0 = blockIdx.y * per, g1 = min(ng, g0 + per);
+  const double fpi = 4.0 * M_PI;
+  double s[kLfAtoms][3];
+#pragma unroll
+  for (int a = 0; a < kLfAtoms; a++) s[a][0] = s[a][1] = s[a][2] = 0.0;
+  for (int i = g0 + threadIdx.x; i < g1; i += blockDim.x) {
+    const double x = gx[i], y = gx[ng + i], z = gx[2 * ng + i];
+    const double2 rt = rhogt[i];
+    const double2 re = make_double2(rhog[i].x * om_inv, rhog[i].y * om_inv);
+    const double t = fpi * rhops[i] * g2i[i];
+    const double vr = t * rt.x + vps[i] * re.x;
+    const double vi = -t * rt.y - vps[i] * re.y;
+#pragma unroll
+    for (int a = 0; a < kLfAtoms; a++) {
+      if (a < nat) {
+        const int ia = a0 + a;
+        const double2 ph = phase_from_tables(tabs + (size_t)a * W3, hmax, cr, x, y, z, tau[3 * ia],
+                                             tau[3 * ia + 1], tau[3 * ia + 2]);
+        // exp(-i G.tau) = ph.x + i ph.y = cs - i sn
+        const double tmp = ph.x * vi + ph.y * vr;
+        s[a][0] += tmp * x;
+        s[a][1] += tmp * y;
+        s[a][2] += tmp * z;
+      }
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < kLfAtoms; a++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      const double v = block_sum(s[a][j], sh);
+      if (threadIdx.x == 0 && a < nat) part[((size_t)(a0 + a) * 3 + j) * nslice + blockIdx.y] = v;
+    }
+}
+
+__global__ void k_local_force_finish(const double* __restrict__ part, int na, int nslice,
+                                     double fac, int atom0, double* __restrict__ fion) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= 3 * na) return;
+  double t = 0.0;
+  for (int sl = 0; sl < nslice; sl++) t += part[(size_t)k * nslice + sl];
+  fion[3 * (size_t)atom0 + k] += fac * t;
+}
+
 static CellRows cell_rows(const Context& ctx) {
   CellRows cr;
   for (int i = 0; i < 9; i++) {
@@ -652,11 +717,26 @@ void launch_local_forces(Context& ctx, double* fion) {
     const int na = (int)ctx.tau[is].size() / 3;
     if (na == 0) continue;
     // positions of this species: a slice of the species-major d_tau_all
-    k_local_force<<<na, kThreads, phase_table_bytes(ctx), ctx.stream>>>(
-        ctx.d_gx_v, (const double2*)ctx.d_vtmp_g2, (const double2*)ctx.d_rhog,
-        ctx.d_vps + is * (size_t)ngv, ctx.d_rhops_sp + is * (size_t)ngv, ctx.d_g2i_v, ngv,
-        1.0 / ctx.vb.omega, ctx.d_tau_all + 3 * (size_t)atom0, -2.0 * ctx.vb.omega, atom0, fion,
-        cell_rows(ctx), phase_hmax(ctx));
+    constexpr int kSlices = 16;
+    if ((size_t)na * 3 * kSlices <= ctx.fpart_elems) {
+      const size_t sm = kLfAtoms * phase_table_bytes(ctx);
+      allow_smem(k_local_force_multi, sm);
+      dim3 grid((na + kLfAtoms - 1) / kLfAtoms, kSlices);
+      k_local_force_multi<<<grid, kThreads, sm, ctx.stream>>>(
+          ctx.d_gx_v, (const double2*)ctx.d_vtmp_g2, (const double2*)ctx.d_rhog,
+          ctx.d_vps + is * (size_t)ngv, ctx.d_rhops_sp + is * (size_t)ngv, ctx.d_g2i_v, ngv,
+          1.0 / ctx.vb.omega, ctx.d_tau_all + 3 * (size_t)atom0, na, cell_rows(ctx),
+          phase_hmax(ctx), ctx.d_fpart);
+      QBX_LAUNCHED(ctx);
+      k_local_force_finish<<<(3 * na + 127) / 128, 128, 0, ctx.stream>>>(
+          ctx.d_fpart, na, kSlices, -2.0 * ctx.vb.omega, atom0, fion);
+    } else {
+      k_local_force<<<na, kThreads, phase_table_bytes(ctx), ctx.stream>>>(
+          ctx.d_gx_v, (const double2*)ctx.d_vtmp_g2, (const double2*)ctx.d_rhog,
+          ctx.d_vps + is * (size_t)ngv, ctx.d_rhops_sp + is * (size_t)ngv, ctx.d_g2i_v, ngv,
+          1.0 / ctx.vb.omega, ctx.d_tau_all + 3 * (size_t)atom0, -2.0 * ctx.vb.omega, atom0,
+          fion, cell_rows(ctx), phase_hmax(ctx));
+    }
     QBX_LAUNCHED(ctx);
     atom0 += na;
   }

@@ -156,7 +156,7 @@ void md_run(Context& c, int niter, int nitscf, double dt, const double* mass_amu
       ProfScope ps(c, "md_extrapolate");
       if (it == 0) {
         extrapolate(c, dt, 0);
-        gram(c);
+        gram(c, true);
       } else {
         align_to_c(c, c.d_wfv);
         extrapolate(c, 0.0, 1);
@@ -174,7 +174,7 @@ void md_run(Context& c, int niter, int nitscf, double dt, const double* mass_amu
   // (src/BOSampleStepper.cpp:1351-1420)
   align_to_c(c, c.d_wfv);
   extrapolate(c, 1.0 / dt, 2);
-  gram(c);
+  gram(c, true);
   forces_here();
   compute_v();
   if (vel) std::memcpy(vel, v0.data(), v0.size() * sizeof(double));

@@ -410,6 +410,8 @@ struct Context {
   double* d_tau_all = nullptr;  // 3*natoms
   double* d_phase_tab = nullptr;   // per atom exp(-i 2 pi h u_j) tables (structure factors)
   size_t phase_tab_bytes = 0;
+  double* d_fpart = nullptr;    // slice partials of the local forces (3 natoms x 16)
+  size_t fpart_elems = 0;
   double* d_twnl = nullptr;     // projector forms Y_lm V_nl, one ngw row per (species, l, m)
   double* d_astress = nullptr;  // 2*ngw*nproj: a strain-derivative projector block
   void* sa_hi = nullptr;        // its BF16 split (mixed path)
@@ -681,7 +683,7 @@ void check_status(Context& ctx);
 void bind_stream(Context& ctx, cudaStream_t s);
 
 // ------------------------------------------------ the step and its callers
-void gram(Context& ctx);
+void gram(Context& ctx, bool split_overlap = false);
 void ortho_align(Context& ctx);
 void update_density(Context& ctx);
 void update_vhxc(Context& ctx);

@@ -46,9 +46,26 @@ static void overlap_cholesky(Context& ctx, const double* c, double* S, int statu
                               ctx.solver_lwork, ctx.d_status + status));
 }
 
-// SlaterDet::gram (src/SlaterDet.cpp:480-534): C <- C L^-T
-void gram(Context& ctx) {
+static void rotate(Context& ctx, double* x, const double* M);
+
+// SlaterDet::gram (src/SlaterDet.cpp:480-534): C <- C L^-T.  With
+// split_overlap in the mixed path (the MD extrapolation), the overlap is the
+// split BF16 product with its FP64 diagonal and C L^-T the split TF32
+// rotation C - C (I - L^-T), as in ortho_align; otherwise FP64 throughout.
+void gram(Context& ctx, bool split_overlap) {
   launch_cleanup(ctx, ctx.d_c);
+  if (split_overlap && mixed(ctx)) {
+    const int n = ctx.nst, K = 2 * ctx.wb.ng;
+    const double one = 1.0;
+    split_bf16_2d(ctx, ctx.d_c, K, n, K, ctx.cs_hi[1], ctx.cs_lo[1], ctx.ldp);
+    overlap_cholesky(ctx, ctx.d_c, ctx.d_nn, ST_INFO_GRAM, 1);
+    double* X = ctx.d_nn2;
+    launch_identity_axpy(ctx, X, X, n, 0.0);
+    QBX_BLAS(cublasDtrsm(ctx.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T,
+                         CUBLAS_DIAG_NON_UNIT, n, n, &one, ctx.d_nn, n, X, n));   // L^-T
+    rotate(ctx, ctx.d_c, X);
+    return;
+  }
   overlap_cholesky(ctx, ctx.d_c, ctx.d_nn, ST_INFO_GRAM, -1);
   const double one = 1.0;
   QBX_BLAS(cublasDtrsm(ctx.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T,
