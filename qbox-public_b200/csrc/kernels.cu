@@ -351,12 +351,12 @@ __global__ void k_precondition(double2* __restrict__ hc, const double* __restric
   }
 }
 
-// The preconditioned residual and the Anderson sums in one pass: dc = -K r
-// (as k_precondition) is written over the residual and, in the same visit,
-// enters <dc, dc - dc_last> and |dc - dc_last|^2 (weight 2 off G = 0, the
-// real view of the half sphere; src/PSDAWavefunctionStepper.cpp:129-179)
+// The Anderson sums of the preconditioned residual dc = -K r (formed as
+// k_precondition forms it, not stored: the update forms it again from r):
+// <dc, dc - dc_last> and |dc - dc_last|^2 (weight 2 off G = 0, the real view
+// of the half sphere; src/PSDAWavefunctionStepper.cpp:129-179)
 struct PrecondAndersonF {
-  double2* hc; const double2* fl; const double* g2; const double* ekin; int ngw;
+  const double2* hc; const double2* fl; const double* g2; const double* ekin; int ngw;
   __device__ void operator()(size_t i, double* a) const {
     const int b = (int)(i / ngw), ig = (int)(i - (size_t)b * ngw);
     const double e = 0.5 * g2[ig];
@@ -364,7 +364,6 @@ struct PrecondAndersonF {
     const double k = (e < en) ? 0.5 / en : 0.5 / e;
     const double2 r = hc[i];
     const double2 x = make_double2(-k * r.x, -k * r.y);
-    hc[i] = x;
     const double2 y = fl[i];
     const double dx = x.x - y.x, dy = x.y - y.y;
     const double w = (ig == 0) ? 1.0 : 2.0;
@@ -381,15 +380,25 @@ __device__ __forceinline__ double anderson_theta(const double* ab) {
   return fmin(2.0, theta);
 }
 
+// The step, one band per grid row: dc = -K r from the residual r (hc), then
+// c <- c + theta (c - c_last) + dc + theta (dc - dc_last), and the last c and
+// dc kept for the next step.
 __global__ void k_psda_update(double2* __restrict__ c, double2* __restrict__ c_last,
-                              double2* __restrict__ dc_last, const double2* __restrict__ dc,
-                              size_t n, const double* __restrict__ ab, int extrapolate,
+                              double2* __restrict__ dc_last, const double2* __restrict__ r,
+                              const double* __restrict__ g2, const double* __restrict__ ekin,
+                              int ngw, const double* __restrict__ ab, int extrapolate,
                               double* __restrict__ theta_out) {
   const double theta = extrapolate ? anderson_theta(ab) : 0.0;
-  if (blockIdx.x == 0 && threadIdx.x == 0) *theta_out = theta;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x) {
-    const double2 x = c[i], f = dc[i];
+  const int b = blockIdx.y;
+  if (b == 0 && blockIdx.x == 0 && threadIdx.x == 0) *theta_out = theta;
+  const double en = ekin[b];
+  const size_t off = (size_t)b * ngw;
+  for (int ig = blockIdx.x * blockDim.x + threadIdx.x; ig < ngw; ig += gridDim.x * blockDim.x) {
+    const size_t i = off + ig;
+    const double e = 0.5 * g2[ig];
+    const double k = (e < en) ? 0.5 / en : 0.5 / e;
+    const double2 rv = r[i];
+    const double2 x = c[i], f = make_double2(-k * rv.x, -k * rv.y);
     double2 nc;
     if (extrapolate) {
       const double2 xl = c_last[i], fl = dc_last[i];
@@ -409,20 +418,18 @@ __global__ void k_psda_update(double2* __restrict__ c, double2* __restrict__ c_l
 // Stepper.cpp:82-212): precondition, Anderson theta, step.
 void launch_psda_elementwise(Context& ctx) {
   const size_t n = (size_t)ctx.wb.ng * ctx.nst;
-  if (ctx.extrapolate) {
-    reduce<2>(ctx, PrecondAndersonF{(double2*)ctx.d_hc, (const double2*)ctx.d_dc_last,
+  if (ctx.extrapolate)
+    reduce<2>(ctx, PrecondAndersonF{(const double2*)ctx.d_hc, (const double2*)ctx.d_dc_last,
                                     ctx.d_g2_w, ctx.d_prec, ctx.wb.ng},
               n, SLOT_ANDERSON);
-  } else {
-    k_precondition<<<blocks_for(n), kThreads, 0, ctx.stream>>>((double2*)ctx.d_hc, ctx.d_g2_w,
-                                                                ctx.d_prec, ctx.wb.ng, n);
-    QBX_LAUNCHED(ctx);
-  }
-  // theta is formed on the device from the two sums
-  k_psda_update<<<blocks_for(n), kThreads, 0, ctx.stream>>>(
+  // theta is formed on the device from the two sums; the residual stays in hc
+  const int ngw = ctx.wb.ng;
+  dim3 grid((unsigned)std::max(1, std::min((ngw + kThreads - 1) / kThreads, 16)),
+            (unsigned)ctx.nst);
+  k_psda_update<<<grid, kThreads, 0, ctx.stream>>>(
       (double2*)ctx.d_c, (double2*)ctx.d_c_last, (double2*)ctx.d_dc_last,
-      (const double2*)ctx.d_hc, n, ctx.d_scalars + SLOT_ANDERSON, ctx.extrapolate ? 1 : 0,
-      ctx.d_scalars + SLOT_THETA);
+      (const double2*)ctx.d_hc, ctx.d_g2_w, ctx.d_prec, ngw, ctx.d_scalars + SLOT_ANDERSON,
+      ctx.extrapolate ? 1 : 0, ctx.d_scalars + SLOT_THETA);
   QBX_LAUNCHED(ctx);
 }
 
