@@ -83,7 +83,7 @@ void free_cell(Context& c) {
   double** bufs[] = {&c.d_gx_w, &c.d_g2_w, &c.d_gx_v, &c.d_g2i_v, &c.d_c, &c.d_hc, &c.d_c_last,
                      &c.d_dc_last, &c.d_ctmp, &c.d_occ, &c.d_rhor, &c.d_vr, &c.d_vxc,
                      &c.d_exc, &c.d_vx2, &c.d_grad, &c.d_rhog, &c.d_vion, &c.d_rhops,
-                     &c.d_vtmp_g, &c.d_vtmp_g2, &c.d_xc_g, &c.d_nn, &c.d_nn2, &c.d_nn3, &c.d_nn4,
+                     &c.d_vtmp_g, &c.d_vtmp_g2, &c.d_xc_g, &c.d_nn, &c.d_nn2, &c.d_nn3, &c.d_nn4, &c.d_nn5,
                      &c.d_solver_work, &c.d_red, &c.d_scalars, &c.d_prec, &c.d_jd_h,
                      &c.d_jd_w, &c.d_jd_work, &c.d_wfv, &c.d_xsd, &c.d_xgrid};
   for (double** b : bufs) dfree(*b);
@@ -506,6 +506,7 @@ int qbx_set_cell(qbx_context* h, const double cell[9], double ecut, int nst, con
     c.d_nn2 = dalloc<double>(nn);
     c.d_nn3 = dalloc<double>(nn);
     c.d_nn4 = dalloc<double>(3 * nn);
+    c.d_nn5 = dalloc<double>(nn);
     c.d_ipiv = dalloc<int>(nst);
     c.d_info = dalloc<int>(1);
     int lw1 = 0, lw2 = 0;

@@ -372,6 +372,7 @@ struct Context {
   double* d_nn2 = nullptr;
   double* d_nn3 = nullptr;
   double* d_nn4 = nullptr;
+  double* d_nn5 = nullptr;      // n x n: L^-1 of ortho_align's overlap (mixed path)
   int* d_ipiv = nullptr;
   int* d_info = nullptr;
   double* d_solver_work = nullptr;

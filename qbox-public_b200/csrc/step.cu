@@ -390,11 +390,26 @@ void ortho_align(Context& ctx) {
                            ctx.d_c_last, K, &zero, X, n));
   }
   launch_rank1_fix(ctx, X, n, ctx.d_c, K, ctx.d_c_last, K, n, n, -1.0, false);
-  QBX_BLAS(cublasDtrsm(ctx.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
-                       CUBLAS_DIAG_NON_UNIT, n, n, &one, L, n, X, n));
-  polar(ctx, X, 1.e-6, 20);
-  QBX_BLAS(cublasDtrsm(ctx.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T,
-                       CUBLAS_DIAG_NON_UNIT, n, n, &one, L, n, X, n));
+  if (mx) {
+    // L^-1 once (one triangular solve of I), then two products in place of
+    // the two solves with L and L^T (each solve as slow as the inverse)
+    double* Li = ctx.d_nn5;
+    double* T = L;   // L is not read after L^-1 is formed
+    launch_identity_axpy(ctx, Li, Li, n, 0.0);
+    QBX_BLAS(cublasDtrsm(ctx.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
+                         CUBLAS_DIAG_NON_UNIT, n, n, &one, L, n, Li, n));
+    QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &one, Li, n, X, n, &zero, T,
+                         n));
+    polar(ctx, T, 1.e-6, 20);
+    QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, n, &one, Li, n, T, n, &zero, X,
+                         n));
+  } else {
+    QBX_BLAS(cublasDtrsm(ctx.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
+                         CUBLAS_DIAG_NON_UNIT, n, n, &one, L, n, X, n));
+    polar(ctx, X, 1.e-6, 20);
+    QBX_BLAS(cublasDtrsm(ctx.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T,
+                         CUBLAS_DIAG_NON_UNIT, n, n, &one, L, n, X, n));
+  }
   ProfScope ps(ctx, "gemm_rotate");
   if (mx) {
     // C <- C - C (I - X): the split-precision error only touches the
