@@ -486,7 +486,8 @@ __device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, uint32_t parity
 }
 
 // TMA load into this CTA's shared memory, its bytes counted on the pair's
-// barrier at cluster address bar (no multicast: each CTA loads its own tiles)
+// barrier at cluster address bar (each CTA loads only its own tiles from this
+// GPU's memory)
 __device__ __forceinline__ void tma_load_2d_pair(void* dst, const CUtensorMap* map, uint32_t bar,
                                                  int x, int y) {
   asm volatile(
