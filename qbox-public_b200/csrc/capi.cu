@@ -201,7 +201,7 @@ void step_eager(Context& c, bool want_f, bool want_s, double* energies, double* 
   fill_energies(c, energies);
   if (want_f && fion) std::memcpy(fion, c.fion.data(), sizeof(double) * c.fion.size());
   if (c.wf_dyn == 1) jd_update(c);
-  else psda_update(c);
+  else psda_update(c, PSDA_PREC_FROM_ENERGY);   // energy() ran on this C
   readback(c, false);
   check_status(c);
   finish_theta(c);
@@ -249,8 +249,7 @@ long record_step(Context& c, bool want_f) {
     energy(c, true, want_f);
     c.psir_use = false;
     c.psir_valid = false;
-    launch_eigsum(c);
-    psda_update(c);
+    psda_update(c, PSDA_PREC_FROM_ENERGY | PSDA_EIGSUM);
     enqueue_readback(c, want_f);
   } catch (...) {
     restore();
@@ -374,6 +373,7 @@ int qbx_create(qbx_context** out, int device, int precision) {
   if (const char* e = std::getenv("QBX_TC_PAIR")) h->c.tc_pair = std::max(0, std::min(2, std::atoi(e)));
   if (const char* e = std::getenv("QBX_TC_PAIR_EPW")) h->c.tc_pair_epw = std::atoi(e) == 8 ? 8 : 16;
   if (const char* e = std::getenv("QBX_TC_TF32_MN")) h->c.tc_tf32_mn = std::atoi(e) != 0 ? 1 : 0;
+  if (const char* e = std::getenv("QBX_STEP_FUSE")) h->c.step_fuse = std::atoi(e) != 0 ? 1 : 0;
   if (const char* e = std::getenv("QBX_TC_CORR_MUL")) h->c.tc_corr_mul = std::max(0, std::min(64, std::atoi(e)));
   if (const char* e = std::getenv("QBX_TALL_KIND_HC")) h->c.tall_kind_hc = std::atoi(e) == 1 ? 1 : 0;
   // batches of captured steps: one graph launch per context on its own

@@ -12,6 +12,7 @@
 
 #include "qbx_internal.h"
 #include "reduce.cuh"
+#include "split.cuh"
 
 namespace qbx {
 
@@ -414,9 +415,73 @@ __global__ void k_psda_update(double2* __restrict__ c, double2* __restrict__ c_l
   }
 }
 
+// k_psda_update with the splits of the new C that ortho_align reads written
+// in the same pass: SlaterDet::cleanup (Im c(G=0) = 0, src/SlaterDet.cpp:
+// 1341-1356) applied to the new C, then its BF16 hi/lo (ld ldb, padding rows
+// zero) and TF32 hi/lo (ld ldt) splits, and per band the partial sums of its
+// squares for the overlap's diagonal.  Four rows (two coefficients) a thread,
+// one band per grid row, with the grid and partial layout of the split
+// kernel k_split2d_v4<true, true, 1> (part[band * gridDim.x + blockIdx.x]).
+// rows = 2 ngw; all four FP64 blocks have ld rows.
+__global__ void __launch_bounds__(256)
+k_psda_update_split(double* __restrict__ c, double* __restrict__ c_last,
+                    double* __restrict__ dc_last, const double* __restrict__ r,
+                    const double* __restrict__ g2, const double* __restrict__ ekin, int rows,
+                    const double* __restrict__ ab, int extrapolate, double* __restrict__ theta_out,
+                    __nv_bfloat16* __restrict__ bhi, __nv_bfloat16* __restrict__ blo, int ldb,
+                    float* __restrict__ thi, float* __restrict__ tlo, int ldt,
+                    double* __restrict__ part) {
+  const double theta = extrapolate ? anderson_theta(ab) : 0.0;
+  const int b = blockIdx.y;
+  if (b == 0 && blockIdx.x == 0 && threadIdx.x == 0) *theta_out = theta;
+  const double en = ekin[b];
+  const size_t off = (size_t)b * rows;
+  double acc = 0.0;
+  for (int q = 4 * (blockIdx.x * blockDim.x + threadIdx.x); q < ldb;
+       q += 4 * gridDim.x * blockDim.x) {
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int row = q + 2 * h;   // real part of coefficient row / 2
+      if (row < rows) {
+        const size_t i = off + row;
+        const double e = 0.5 * g2[row >> 1];
+        const double k = (e < en) ? 0.5 / en : 0.5 / e;
+        const double2 rv = *reinterpret_cast<const double2*>(r + i);
+        const double2 x = *reinterpret_cast<const double2*>(c + i);
+        const double2 f = make_double2(-k * rv.x, -k * rv.y);
+        double2 nc;
+        if (extrapolate) {
+          const double2 xl = *reinterpret_cast<const double2*>(c_last + i);
+          const double2 fl = *reinterpret_cast<const double2*>(dc_last + i);
+          nc.x = x.x + theta * (x.x - xl.x) + f.x + theta * (f.x - fl.x);
+          nc.y = x.y + theta * (x.y - xl.y) + f.y + theta * (f.y - fl.y);
+        } else {
+          nc.x = x.x + f.x;
+          nc.y = x.y + f.y;
+        }
+        if (row == 0) nc.y = 0.0;
+        *reinterpret_cast<double2*>(c + i) = nc;
+        *reinterpret_cast<double2*>(c_last + i) = x;
+        *reinterpret_cast<double2*>(dc_last + i) = f;
+        v[2 * h] = nc.x;
+        v[2 * h + 1] = nc.y;
+      }
+    }
+    acc += v[0] * v[0] + v[1] * v[1] + v[2] * v[2] + v[3] * v[3];
+    store_splits4<true, true>(v, q, rows, b, bhi, blo, ldb, thi, tlo, ldt);
+  }
+  __shared__ double sh[32];
+  const double t = block_sum(acc, sh);
+  if (threadIdx.x == 0) part[(size_t)b * gridDim.x + blockIdx.x] = t;
+}
+
 // PSDAWavefunctionStepper::update after the residual (src/PSDAWavefunction
-// Stepper.cpp:82-212): precondition, Anderson theta, step.
-void launch_psda_elementwise(Context& ctx) {
+// Stepper.cpp:82-212): precondition, Anderson theta, step.  With split_c
+// (the mixed path where ortho_align reads C's BF16 and TF32 splits) the step
+// also cleans up the new C and writes those splits and the column partials
+// (cs_hi/lo[1], ct_hi/lo, d_colred), as split_bf16_tf32 would.
+void launch_psda_elementwise(Context& ctx, bool split_c) {
   const size_t n = (size_t)ctx.wb.ng * ctx.nst;
   if (ctx.extrapolate)
     reduce<2>(ctx, PrecondAndersonF{(const double2*)ctx.d_hc, (const double2*)ctx.d_dc_last,
@@ -424,6 +489,20 @@ void launch_psda_elementwise(Context& ctx) {
               n, SLOT_ANDERSON);
   // theta is formed on the device from the two sums; the residual stays in hc
   const int ngw = ctx.wb.ng;
+  if (split_c) {
+    const int ldp = ctx.ldp, nst = ctx.nst;
+    const int nb = std::max(1, std::min((ldp + 1023) / 1024, 64));   // as the split kernel's grid
+    QBX_REQUIRE(ldp % 4 == 0 && ldp >= 2 * ngw && nst <= 65535 &&
+                    (size_t)nb * nst <= ctx.colred_elems && ctx.cs_hi[1] && ctx.ct_hi,
+                50, "PSDA step with the splits of C: no split buffers or partials");
+    k_psda_update_split<<<dim3((unsigned)nb, (unsigned)nst), 256, 0, ctx.stream>>>(
+        ctx.d_c, ctx.d_c_last, ctx.d_dc_last, ctx.d_hc, ctx.d_g2_w, ctx.d_prec, 2 * ngw,
+        ctx.d_scalars + SLOT_ANDERSON, ctx.extrapolate ? 1 : 0, ctx.d_scalars + SLOT_THETA,
+        (__nv_bfloat16*)ctx.cs_hi[1], (__nv_bfloat16*)ctx.cs_lo[1], ldp, (float*)ctx.ct_hi,
+        (float*)ctx.ct_lo, ldp, ctx.d_colred);
+    QBX_LAUNCHED(ctx);
+    return;
+  }
   dim3 grid((unsigned)std::max(1, std::min((ngw + kThreads - 1) / kThreads, 16)),
             (unsigned)ctx.nst);
   k_psda_update<<<grid, kThreads, 0, ctx.stream>>>(

@@ -429,6 +429,9 @@ struct Context {
   int tc_pair_epw = 16;         // epilogue warps of the 256 x 256 pair tiles (8 or 16)
   int tc_tf32_mn = 1;           // TF32 tall updates read the plain split MN-major (else a
                                 // transposed split)
+  int step_fuse = 1;            // mixed PSDA step: band energies of the preconditioner, the
+                                // eigenvalue sum and C's splits made inside neighbouring
+                                // passes (0: each in a pass of its own)
 
   // band pairs split over GPUs (qbx_set_band_shard): this GPU's rank among
   // shard_n, and the NCCL communicator (ncclComm_t) of the group
@@ -618,7 +621,9 @@ void launch_setup_atoms(Context& ctx);         // sfac, vion, rhops, anl
 void launch_ekin(Context& ctx);                // SLOT_EKIN
 void launch_eigsum(Context& ctx);              // SLOT_EIG
 void launch_precond_update(Context& ctx);      // d_prec
-void launch_psda_elementwise(Context& ctx);    // residual->step; SLOT_THETA
+// residual -> step; SLOT_THETA.  split_c: also C's cleanup and the splits
+// that ortho_align reads when ortho_splits_both (one pass)
+void launch_psda_elementwise(Context& ctx, bool split_c = false);
 void launch_precondition_into(Context& ctx, const double* r, double* z);   // z = -K r
 void launch_cleanup(Context& ctx, double* c);  // Im c(G=0) = 0
 void launch_rank1_fix(Context& ctx, double* m, int ldm, const double* x, int ldx,
@@ -685,11 +690,22 @@ void bind_stream(Context& ctx, cudaStream_t s);
 
 // ------------------------------------------------ the step and its callers
 void gram(Context& ctx, bool split_overlap = false);
-void ortho_align(Context& ctx);
+// c_split_done: the caller has cleaned up C and written the splits that
+// ortho_splits_both names (launch_psda_elementwise with split_c)
+void ortho_align(Context& ctx, bool c_split_done = false);
+// ortho_align reads C's BF16 and TF32 splits, made in one pass
+bool ortho_splits_both(const Context& ctx);
 void update_density(Context& ctx);
 void update_vhxc(Context& ctx);
 void energy(Context& ctx, bool hpsi, bool forces);
-void psda_update(Context& ctx);
+// psda_update's fusions, for callers that ran energy() on the same C just
+// before: PSDA_PREC_FROM_ENERGY takes the preconditioner's band energies
+// from energy()'s split pass (mixed path), PSDA_EIGSUM forms the eigenvalue
+// sum (SLOT_EIG) in the split of H C (mixed path; launch_eigsum otherwise)
+enum : unsigned { PSDA_PREC_FROM_ENERGY = 1u, PSDA_EIGSUM = 2u };
+void psda_update(Context& ctx, unsigned fuse = 0);
+// energy()'s mixed path forms the preconditioner's band energies too
+bool energy_forms_prec(const Context& ctx);
 void jd_update(Context& ctx);
 void polar_factor(Context& ctx, double* x, double tol, int maxiter);
 int polar_entry(Context& ctx, double* x, double tol, int maxiter, bool graph);
@@ -752,9 +768,15 @@ void split_bf16_2d(Context& ctx, const double* x, int rows, int cols, int ldx, v
 void split_bf16_tf32(Context& ctx, const double* x, int rows, int cols, int ldx, void* bhi,
                      void* blo, int ldb, float* thi, float* tlo, int ldt);
 // the BF16 split of a wavefunction block (rows = 2 ngw) with the kinetic sum
-// sum_n occ_n sum_G g2(G) |c_n(G)|^2 of the same pass into *out
+// sum_n occ_n sum_G g2(G) |c_n(G)|^2 of the same pass into *out; with prec,
+// also each band's kinetic energy for the preconditioner into prec[cols]
 void split_bf16_ekin(Context& ctx, const double* x, int rows, int cols, int ldx, void* hi,
-                     void* lo, int ldp, const double* g2, const double* occ, double* out);
+                     void* lo, int ldp, const double* g2, const double* occ, double* out,
+                     double* prec = nullptr);
+// the BF16 split of a wavefunction block x (rows = 2 ngw) with the sum over
+// its columns of 2 Re <x_n, y_n> - x_n(0) y_n(0) (y of x's layout) into *out
+void split_bf16_dot(Context& ctx, const double* x, const double* y, int rows, int cols, int ldx,
+                    void* hi, void* lo, int ldp, double* out);
 // diag(S) = 2 C^T C - c0 c0^T on the diagonal, exact in FP64, from the
 // column sums of the last split_bf16_tf32 of c
 void overlap_diag_from_split(Context& ctx, const double* c, int K, int n, int ldp, double* S);

@@ -382,7 +382,7 @@ void scf_run(Context& c, int nitscf, int nite, double mix_coeff, double mix_rcut
       if (ite > 0) eig_m = eig;
       eig = c.eigsum;
       if (eigsum) eigsum[(size_t)it * nsteps + ite] = eig;
-      psda_update(c);
+      psda_update(c, PSDA_PREC_FROM_ENERGY);   // energy() ran on this C
       if (ite > 0) conv = std::fabs(eig - eig_m) < 0.01 * delta_ehart;
       ite++;
     }

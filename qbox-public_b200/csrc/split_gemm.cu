@@ -16,7 +16,7 @@
 
 #include "qbx_internal.h"
 #include "reduce.cuh"
-#include <cuda_bf16.h>
+#include "split.cuh"
 
 namespace qbx {
 
@@ -128,32 +128,28 @@ void split_gemm(Context& ctx, bool ta, bool tb, int m, int n, int k, double alph
 // first), then added into the FP64 output: relative error ~3e-7 per element,
 // that of an FP32 product, against ~1e-5 for three BF16 products.
 
-// round an FP32 value to TF32 (10 explicit mantissa bits), nearest with
-// ties away from zero; finite inputs only
-__device__ __forceinline__ float tf32_round(float x) {
-  unsigned u = __float_as_uint(x);
-  u = (u + 0x1000u) & 0xffffe000u;
-  return __uint_as_float(u);
-}
-
 // The splits of a column-major FP64 block, four consecutive rows a thread
 // (two 16-byte loads, 8- or 16-byte stores), one column per grid row, so no
 // index division: BF16 hi/lo (ld ldb, the padding rows up to ldb zero) and/or
 // TF32 hi/lo (ld ldt, rows < rows only).  Needs x 16-byte aligned, ldx even
 // and ldb, ldt multiples of 4.
-// RED also sums, per column, the squares of its FP64 values (1) or the
+// RED also sums, per column, the squares of its FP64 values (1), the
 // squares weighted by g2[row / 2] (2, the kinetic sum of a band over its
-// complex coefficients) into part[column * gridDim.x + blockIdx.x]: fixed
-// partials that the finishing kernels add in order.
+// complex coefficients), both of these (3: the weighted sum first, the plain
+// one in a second partial array cols x gridDim.x further on), or the
+// products with the same column of a second block y of x's layout (4) into
+// part[column * gridDim.x + blockIdx.x]: fixed partials that the finishing
+// kernels add in order.
 template <bool BF, bool TF, int RED = 0>
 __global__ void k_split2d_v4(const double* __restrict__ x, int rows, int ldx,
                              __nv_bfloat16* __restrict__ bhi, __nv_bfloat16* __restrict__ blo,
                              int ldb, float* __restrict__ thi, float* __restrict__ tlo, int ldt,
                              int span, const double* __restrict__ g2 = nullptr,
-                             double* __restrict__ part = nullptr) {
+                             double* __restrict__ part = nullptr,
+                             const double* __restrict__ y = nullptr) {
   const int c = blockIdx.y;
   const double* xc = x + (size_t)c * ldx;
-  double acc = 0.0;
+  double acc = 0.0, acc2 = 0.0;
   for (int r = 4 * (blockIdx.x * blockDim.x + threadIdx.x); r < span;
        r += 4 * gridDim.x * blockDim.x) {
     double v[4];
@@ -167,48 +163,37 @@ __global__ void k_split2d_v4(const double* __restrict__ x, int rows, int ldx,
     }
     if constexpr (RED == 1) {
       acc += v[0] * v[0] + v[1] * v[1] + v[2] * v[2] + v[3] * v[3];
-    } else if constexpr (RED == 2) {
+    } else if constexpr (RED == 2 || RED == 3) {
       // rows r .. r + 3 are the real and imaginary parts of coefficients
       // r / 2 and r / 2 + 1 (r even); rows past `rows` are zero
       if (r < rows) {
         const double w0 = g2[r >> 1], w1 = r + 2 < rows ? g2[(r >> 1) + 1] : 0.0;
-        acc += (v[0] * v[0] + v[1] * v[1]) * w0 + (v[2] * v[2] + v[3] * v[3]) * w1;
+        const double s0 = v[0] * v[0] + v[1] * v[1], s1 = v[2] * v[2] + v[3] * v[3];
+        acc += s0 * w0 + s1 * w1;
+        if constexpr (RED == 3) acc2 += s0 + s1;
       }
-    }
-    if constexpr (BF) {
-      __nv_bfloat16 h[4], l[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        h[q] = __double2bfloat16(v[q]);
-        l[q] = __double2bfloat16(v[q] - (double)__bfloat162float(h[q]));
-      }
-      if (r < ldb) {
-        *reinterpret_cast<uint2*>(bhi + (size_t)c * ldb + r) = *reinterpret_cast<uint2*>(h);
-        *reinterpret_cast<uint2*>(blo + (size_t)c * ldb + r) = *reinterpret_cast<uint2*>(l);
-      }
-    }
-    if constexpr (TF) {
-      float h[4], l[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        h[q] = tf32_round((float)v[q]);
-        l[q] = tf32_round((float)(v[q] - (double)h[q]));
-      }
+    } else if constexpr (RED == 4) {
+      const double* yc = y + (size_t)c * ldx;
       if (r + 3 < rows) {
-        *reinterpret_cast<float4*>(thi + (size_t)c * ldt + r) = make_float4(h[0], h[1], h[2], h[3]);
-        *reinterpret_cast<float4*>(tlo + (size_t)c * ldt + r) = make_float4(l[0], l[1], l[2], l[3]);
+        const double2 a = *reinterpret_cast<const double2*>(yc + r);
+        const double2 b = *reinterpret_cast<const double2*>(yc + r + 2);
+        acc += v[0] * a.x + v[1] * a.y + v[2] * b.x + v[3] * b.y;
       } else {
-        for (int q = 0; q < 4 && r + q < rows; ++q) {
-          thi[(size_t)c * ldt + r + q] = h[q];
-          tlo[(size_t)c * ldt + r + q] = l[q];
-        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          if (r + q < rows) acc += v[q] * yc[r + q];
       }
     }
+    store_splits4<BF, TF>(v, r, rows, c, bhi, blo, ldb, thi, tlo, ldt);
   }
   if constexpr (RED != 0) {
     __shared__ double sh[32];
     const double t = red::block_sum(acc, sh);
     if (threadIdx.x == 0) part[(size_t)c * gridDim.x + blockIdx.x] = t;
+    if constexpr (RED == 3) {
+      const double t2 = red::block_sum(acc2, sh);
+      if (threadIdx.x == 0) part[((size_t)gridDim.y + c) * gridDim.x + blockIdx.x] = t2;
+    }
   }
 }
 
@@ -288,17 +273,90 @@ __global__ void k_weighted_from_partials(const double* __restrict__ part, int nb
   if (threadIdx.x == 0) out[0] = s;
 }
 
+// From the partials of k_split2d_v4<..., 3> of a wavefunction block x: the
+// occupation-weighted kinetic sum into out[0] (as k_weighted_from_partials)
+// and each band's kinetic energy for the preconditioner,
+// prec_n = sum |c|^2 G^2 / (2 sum |c|^2 - |c_0|^2) on the half sphere, 1 where
+// that is not positive (Preconditioner::update, src/Preconditioner.cpp:88-143;
+// the same formula as the one-band-per-CTA kernel of the FP64 path).  One CTA
+// of up to 1 024 threads, one column a thread per pass.
+__global__ void k_ekin_prec_from_partials(const double* __restrict__ part, int nb,
+                                          const double* __restrict__ w, int cols,
+                                          const double* __restrict__ x, int ldx,
+                                          double* __restrict__ out, double* __restrict__ prec) {
+  __shared__ double sh[32];
+  const double* part2 = part + (size_t)cols * nb;
+  double a = 0.0;
+  for (int c = threadIdx.x; c < cols; c += blockDim.x) {
+    double te = 0.0, tn = 0.0;
+    for (int b = 0; b < nb; b++) {
+      te += part[(size_t)c * nb + b];
+      tn += part2[(size_t)c * nb + b];
+    }
+    a += w[c] * te;
+    const double re = x[(size_t)c * ldx], im = x[(size_t)c * ldx + 1];
+    const double bn = 2.0 * (tn - 0.5 * (re * re + im * im)), be = 2.0 * te;
+    double e = (0.5 * bn > 0.0) ? 0.5 * be / bn : 0.0;
+    if (e == 0.0) e = 1.0;
+    prec[c] = e;
+  }
+  const double s = red::block_sum(a, sh);
+  if (threadIdx.x == 0) out[0] = s;
+}
+
+// sum over columns of 2 (column's partials) - x(0, c) y(0, c), from the
+// partials of k_split2d_v4<..., 4>: 2 Re <x_c, y_c> on the half sphere with
+// G = 0 counted once, summed over the columns
+__global__ void k_dot_from_partials(const double* __restrict__ part, int nb, int cols,
+                                    const double* __restrict__ x, const double* __restrict__ y,
+                                    int ldx, double* __restrict__ out) {
+  __shared__ double sh[32];
+  double a = 0.0;
+  for (int c = threadIdx.x; c < cols; c += blockDim.x) {
+    double t = 0.0;
+    for (int b = 0; b < nb; b++) t += part[(size_t)c * nb + b];
+    a += 2.0 * t - x[(size_t)c * ldx] * y[(size_t)c * ldx];
+  }
+  const double s = red::block_sum(a, sh);
+  if (threadIdx.x == 0) out[0] = s;
+}
+
 void split_bf16_ekin(Context& ctx, const double* x, int rows, int cols, int ldx, void* hi,
-                     void* lo, int ldp, const double* g2, const double* occ, double* out) {
+                     void* lo, int ldp, const double* g2, const double* occ, double* out,
+                     double* prec) {
   QBX_REQUIRE(v4_ok(x, ldx, ldp) && ((uintptr_t)hi | (uintptr_t)lo) % 8 == 0 && cols <= 65535 &&
-                  rows % 2 == 0 && (size_t)cols * 64 <= ctx.colred_elems,
+                  rows % 2 == 0 && (size_t)cols * (prec ? 128 : 64) <= ctx.colred_elems,
               50, "split with the kinetic sums: unaligned operands or no room for the partials");
   const dim3 g = v4_grid(ldp, cols);
-  k_split2d_v4<true, false, 2><<<g, 256, 0, ctx.stream>>>(
-      x, rows, ldx, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo, ldp, nullptr, nullptr, 4, ldp, g2,
-      ctx.d_colred);
+  if (prec) {
+    k_split2d_v4<true, false, 3><<<g, 256, 0, ctx.stream>>>(
+        x, rows, ldx, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo, ldp, nullptr, nullptr, 4, ldp, g2,
+        ctx.d_colred);
+    QBX_LAUNCHED(ctx);
+    k_ekin_prec_from_partials<<<1, 1024, 0, ctx.stream>>>(ctx.d_colred, (int)g.x, occ, cols, x,
+                                                          ldx, out, prec);
+  } else {
+    k_split2d_v4<true, false, 2><<<g, 256, 0, ctx.stream>>>(
+        x, rows, ldx, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo, ldp, nullptr, nullptr, 4, ldp, g2,
+        ctx.d_colred);
+    QBX_LAUNCHED(ctx);
+    k_weighted_from_partials<<<1, 256, 0, ctx.stream>>>(ctx.d_colred, (int)g.x, occ, cols, out);
+  }
   QBX_LAUNCHED(ctx);
-  k_weighted_from_partials<<<1, 256, 0, ctx.stream>>>(ctx.d_colred, (int)g.x, occ, cols, out);
+}
+
+void split_bf16_dot(Context& ctx, const double* x, const double* y, int rows, int cols, int ldx,
+                    void* hi, void* lo, int ldp, double* out) {
+  QBX_REQUIRE(v4_ok(x, ldx, ldp) && ((uintptr_t)y % 16) == 0 &&
+                  ((uintptr_t)hi | (uintptr_t)lo) % 8 == 0 && cols <= 65535 &&
+                  (size_t)cols * 64 <= ctx.colred_elems,
+              50, "split with the column products: unaligned operands or no room for the partials");
+  const dim3 g = v4_grid(ldp, cols);
+  k_split2d_v4<true, false, 4><<<g, 256, 0, ctx.stream>>>(
+      x, rows, ldx, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo, ldp, nullptr, nullptr, 4, ldp, nullptr,
+      ctx.d_colred, y);
+  QBX_LAUNCHED(ctx);
+  k_dot_from_partials<<<1, 1024, 0, ctx.stream>>>(ctx.d_colred, (int)g.x, cols, x, y, ldx, out);
   QBX_LAUNCHED(ctx);
 }
 

@@ -358,25 +358,30 @@ static void tall_update(Context& ctx, int kind, const double* c, const double* M
 }
 
 // SlaterDet::ortho_align (src/SlaterDet.cpp:768-876)
-void ortho_align(Context& ctx) {
+bool ortho_splits_both(const Context& ctx) {
+  return mixed(ctx) && ctx.gemm_backend == 1 && ctx.tc_pair == 2 && ctx.tc_tf32_mn &&
+         ctx.tall_kind == TALL_TF32 && ctx.d_colred;
+}
+
+void ortho_align(Context& ctx, bool c_split_done) {
   const int n = ctx.nst, K = 2 * ctx.wb.ng;
   const double one = 1.0, two = 2.0, zero = 0.0;
-  launch_cleanup(ctx, ctx.d_c);
+  const bool mx = mixed(ctx);
+  // in the mixed path slot 0 holds the split of C_last (made in energy());
+  // where the rotation reads C's plain TF32 split, both splits of C are made
+  // in one pass (or by the PSDA step that formed C)
+  const bool both = ortho_splits_both(ctx);
+  QBX_REQUIRE(!c_split_done || both, 50, "ortho_align: C's splits were made for another path");
+  if (!c_split_done) launch_cleanup(ctx, ctx.d_c);
   double* L = ctx.d_nn;
   double* X = ctx.d_nn2;
-  const bool mx = mixed(ctx);
   if (!mx)
     QBX_CUDA(cudaMemcpyAsync(ctx.d_ctmp, ctx.d_c, sizeof(double) * (size_t)K * n,
                              cudaMemcpyDeviceToDevice, ctx.stream));
-  // in the mixed path slot 0 holds the split of C_last (made in energy());
-  // where the rotation reads C's plain TF32 split, both splits of C are made
-  // in one pass
-  const bool both = mx && ctx.gemm_backend == 1 && ctx.tc_pair == 2 && ctx.tc_tf32_mn &&
-                    ctx.tall_kind == TALL_TF32;
-  if (both)
+  if (both && !c_split_done)
     split_bf16_tf32(ctx, ctx.d_c, K, n, K, ctx.cs_hi[1], ctx.cs_lo[1], ctx.ldp, (float*)ctx.ct_hi,
                     (float*)ctx.ct_lo, ctx.ldp);
-  else if (mx)
+  else if (mx && !both)
     split_bf16_2d(ctx, ctx.d_c, K, n, K, ctx.cs_hi[1], ctx.cs_lo[1], ctx.ldp);
   overlap_cholesky(ctx, ctx.d_c, L, ST_INFO_ORTHO, mx ? 1 : -1, both);
   // B = 2 C^T C_last - c0 c_last0^T
@@ -569,13 +574,17 @@ void nonlocal_only(Context& ctx, bool hpsi, double* out) {
   ctx.d_hc = saved;
 }
 
+bool energy_forms_prec(const Context& ctx) { return mixed(ctx) && ctx.d_colred && ctx.step_fuse; }
+
 // EnergyFunctional::energy (src/EnergyFunctional.cpp:397-1044)
 void energy(Context& ctx, bool hpsi, bool forces) {
   ProfScope ps(ctx, "energy");
-  if (mixed(ctx) && ctx.d_colred) {
-    // the split for the inner products and the kinetic sum in one pass over C
+  if (energy_forms_prec(ctx)) {
+    // the split for the inner products, the kinetic sum and the
+    // preconditioner's band energies in one pass over C
     split_bf16_ekin(ctx, ctx.d_c, 2 * ctx.wb.ng, ctx.nst, 2 * ctx.wb.ng, ctx.cs_hi[0],
-                    ctx.cs_lo[0], ctx.ldp, ctx.d_g2_w, ctx.d_occ, ctx.d_scalars + SLOT_EKIN);
+                    ctx.cs_lo[0], ctx.ldp, ctx.d_g2_w, ctx.d_occ, ctx.d_scalars + SLOT_EKIN,
+                    ctx.d_prec);
   } else {
     if (mixed(ctx))
       split_bf16_2d(ctx, ctx.d_c, 2 * ctx.wb.ng, ctx.nst, 2 * ctx.wb.ng, ctx.cs_hi[0],
@@ -598,15 +607,21 @@ void energy(Context& ctx, bool hpsi, bool forces) {
 }
 
 // PSDAWavefunctionStepper::update (src/PSDAWavefunctionStepper.cpp:46-249)
-void psda_update(Context& ctx) {
+void psda_update(Context& ctx, unsigned fuse) {
   ProfScope ps(ctx, "psda_update");
   const int n = ctx.nst, K = 2 * ctx.wb.ng;
   const double one = 1.0, two = 2.0, zero = 0.0, mone = -1.0;
   double* A = ctx.d_nn;
+  const bool eig_in_split = (fuse & PSDA_EIGSUM) && mixed(ctx) && ctx.d_colred && ctx.step_fuse;
+  if ((fuse & PSDA_EIGSUM) && !eig_in_split) launch_eigsum(ctx);
   {
     ProfScope pg(ctx, "gemm_residual");
     if (mixed(ctx)) {
-      split_bf16_2d(ctx, ctx.d_hc, K, n, K, ctx.hs_hi, ctx.hs_lo, ctx.ldp);
+      if (eig_in_split)
+        split_bf16_dot(ctx, ctx.d_hc, ctx.d_c, K, n, K, ctx.hs_hi, ctx.hs_lo, ctx.ldp,
+                       ctx.d_scalars + SLOT_EIG);
+      else
+        split_bf16_2d(ctx, ctx.d_hc, K, n, K, ctx.hs_hi, ctx.hs_lo, ctx.ldp);
       split_gemm(ctx, true, false, n, n, K, 2.0, ctx.cs_hi[0], ctx.cs_lo[0], ctx.ldp, ctx.hs_hi,
                  ctx.hs_lo, ctx.ldp, 0.0, A);
       launch_rank1_fix(ctx, A, n, ctx.d_c, K, ctx.d_hc, K, n, n, -1.0, false);
@@ -622,9 +637,11 @@ void psda_update(Context& ctx) {
                            &one, ctx.d_hc, K));
     }
   }
-  launch_precond_update(ctx);
-  launch_psda_elementwise(ctx);
-  ortho_align(ctx);
+  if (!((fuse & PSDA_PREC_FROM_ENERGY) && energy_forms_prec(ctx))) launch_precond_update(ctx);
+  // the step writes the new C's splits for ortho_align in the same pass
+  const bool split_c = ortho_splits_both(ctx) && ctx.step_fuse;
+  launch_psda_elementwise(ctx, split_c);
+  ortho_align(ctx, split_c);
   ctx.extrapolate = true;
 }
 
@@ -768,7 +785,7 @@ void alloc_mixed(Context& ctx) {
   const size_t small = std::max(np * n, n * n);
   ctx.acc32_elems = std::max(wf, std::max(np * n, std::max(K * np, n * n)));
   QBX_CUDA(cudaMalloc(&ctx.d_acc32, ctx.acc32_elems * sizeof(float)));
-  ctx.colred_elems = 64 * n;
+  ctx.colred_elems = 128 * n;   // up to two partial arrays of 64 per column
   ctx.d_colred = dalloc<double>(ctx.colred_elems);
   for (int s = 0; s < 2; s++) {
     QBX_CUDA(cudaMalloc(&ctx.cs_hi[s], wf * 2));
