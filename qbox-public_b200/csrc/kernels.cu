@@ -419,10 +419,10 @@ __global__ void k_psda_update(double2* __restrict__ c, double2* __restrict__ c_l
 // in the same pass: SlaterDet::cleanup (Im c(G=0) = 0, src/SlaterDet.cpp:
 // 1341-1356) applied to the new C, then its BF16 hi/lo (ld ldb, padding rows
 // zero) and TF32 hi/lo (ld ldt) splits, and per band the partial sums of its
-// squares for the overlap's diagonal.  Four rows (two coefficients) a thread,
-// one band per grid row, with the grid and partial layout of the split
-// kernel k_split2d_v4<true, true, 1> (part[band * gridDim.x + blockIdx.x]).
-// rows = 2 ngw; all four FP64 blocks have ld rows.
+// squares for the overlap's diagonal (part[band * gridDim.x + blockIdx.x],
+// gridDim.x as the split kernel's grid, which overlap_diag_from_split
+// expects).  One coefficient (two rows) a thread, one band per grid row;
+// rows = 2 ngw, all four FP64 blocks have ld rows.
 __global__ void __launch_bounds__(256)
 k_psda_update_split(double* __restrict__ c, double* __restrict__ c_last,
                     double* __restrict__ dc_last, const double* __restrict__ r,
@@ -435,41 +435,43 @@ k_psda_update_split(double* __restrict__ c, double* __restrict__ c_last,
   const int b = blockIdx.y;
   if (b == 0 && blockIdx.x == 0 && threadIdx.x == 0) *theta_out = theta;
   const double en = ekin[b];
-  const size_t off = (size_t)b * rows;
+  const int ngw = rows >> 1, half = ldb >> 1;
   double acc = 0.0;
-  for (int q = 4 * (blockIdx.x * blockDim.x + threadIdx.x); q < ldb;
-       q += 4 * gridDim.x * blockDim.x) {
-    double v[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int row = q + 2 * h;   // real part of coefficient row / 2
-      if (row < rows) {
-        const size_t i = off + row;
-        const double e = 0.5 * g2[row >> 1];
-        const double k = (e < en) ? 0.5 / en : 0.5 / e;
-        const double2 rv = *reinterpret_cast<const double2*>(r + i);
-        const double2 x = *reinterpret_cast<const double2*>(c + i);
-        const double2 f = make_double2(-k * rv.x, -k * rv.y);
-        double2 nc;
-        if (extrapolate) {
-          const double2 xl = *reinterpret_cast<const double2*>(c_last + i);
-          const double2 fl = *reinterpret_cast<const double2*>(dc_last + i);
-          nc.x = x.x + theta * (x.x - xl.x) + f.x + theta * (f.x - fl.x);
-          nc.y = x.y + theta * (x.y - xl.y) + f.y + theta * (f.y - fl.y);
-        } else {
-          nc.x = x.x + f.x;
-          nc.y = x.y + f.y;
-        }
-        if (row == 0) nc.y = 0.0;
-        *reinterpret_cast<double2*>(c + i) = nc;
-        *reinterpret_cast<double2*>(c_last + i) = x;
-        *reinterpret_cast<double2*>(dc_last + i) = f;
-        v[2 * h] = nc.x;
-        v[2 * h + 1] = nc.y;
+  for (int ig = blockIdx.x * blockDim.x + threadIdx.x; ig < half;
+       ig += gridDim.x * blockDim.x) {
+    double2 nc = make_double2(0.0, 0.0);   // the padding rows split to zero
+    if (ig < ngw) {
+      const size_t i = (size_t)b * ngw + ig;   // in double2 units
+      const double e = 0.5 * g2[ig];
+      const double k = (e < en) ? 0.5 / en : 0.5 / e;
+      const double2 rv = reinterpret_cast<const double2*>(r)[i];
+      const double2 x = reinterpret_cast<const double2*>(c)[i];
+      const double2 f = make_double2(-k * rv.x, -k * rv.y);
+      if (extrapolate) {
+        const double2 xl = reinterpret_cast<const double2*>(c_last)[i];
+        const double2 fl = reinterpret_cast<const double2*>(dc_last)[i];
+        nc.x = x.x + theta * (x.x - xl.x) + f.x + theta * (f.x - fl.x);
+        nc.y = x.y + theta * (x.y - xl.y) + f.y + theta * (f.y - fl.y);
+      } else {
+        nc.x = x.x + f.x;
+        nc.y = x.y + f.y;
       }
+      if (ig == 0) nc.y = 0.0;
+      reinterpret_cast<double2*>(c)[i] = nc;
+      reinterpret_cast<double2*>(c_last)[i] = x;
+      reinterpret_cast<double2*>(dc_last)[i] = f;
+      acc += nc.x * nc.x + nc.y * nc.y;
+      float2 th, tl;
+      split_tf32(nc.x, th.x, tl.x);
+      split_tf32(nc.y, th.y, tl.y);
+      *reinterpret_cast<float2*>(thi + (size_t)b * ldt + 2 * ig) = th;
+      *reinterpret_cast<float2*>(tlo + (size_t)b * ldt + 2 * ig) = tl;
     }
-    acc += v[0] * v[0] + v[1] * v[1] + v[2] * v[2] + v[3] * v[3];
-    store_splits4<true, true>(v, q, rows, b, bhi, blo, ldb, thi, tlo, ldt);
+    __nv_bfloat162 bh, bl;
+    split_bf16(nc.x, bh.x, bl.x);
+    split_bf16(nc.y, bh.y, bl.y);
+    *reinterpret_cast<__nv_bfloat162*>(bhi + (size_t)b * ldb + 2 * ig) = bh;
+    *reinterpret_cast<__nv_bfloat162*>(blo + (size_t)b * ldb + 2 * ig) = bl;
   }
   __shared__ double sh[32];
   const double t = block_sum(acc, sh);

@@ -273,59 +273,51 @@ __global__ void k_weighted_from_partials(const double* __restrict__ part, int nb
   if (threadIdx.x == 0) out[0] = s;
 }
 
-// From the partials of k_split2d_v4<..., 3> of a wavefunction block x: the
-// occupation-weighted kinetic sum into out[0] (as k_weighted_from_partials)
-// and each band's kinetic energy for the preconditioner,
-// prec_n = sum |c|^2 G^2 / (2 sum |c|^2 - |c_0|^2) on the half sphere, 1 where
+// Per column c of the partials of k_split2d_v4<..., 3> of a wavefunction
+// block x: w[c] times its kinetic sum into wt[c] (added over the columns by
+// k_reduce_final) and the band's kinetic energy for the preconditioner,
+// prec_c = sum |c|^2 G^2 / (2 sum |c|^2 - |c_0|^2) on the half sphere, 1 where
 // that is not positive (Preconditioner::update, src/Preconditioner.cpp:88-143;
-// the same formula as the one-band-per-CTA kernel of the FP64 path).  One CTA
-// of up to 1 024 threads, one column a thread per pass.
-__global__ void k_ekin_prec_from_partials(const double* __restrict__ part, int nb,
-                                          const double* __restrict__ w, int cols,
-                                          const double* __restrict__ x, int ldx,
-                                          double* __restrict__ out, double* __restrict__ prec) {
-  __shared__ double sh[32];
+// the formula of the one-band-per-CTA kernel of the FP64 path).  One thread
+// per column.
+__global__ void k_ekin_prec_columns(const double* __restrict__ part, int nb,
+                                    const double* __restrict__ w, int cols,
+                                    const double* __restrict__ x, int ldx,
+                                    double* __restrict__ wt, double* __restrict__ prec) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cols) return;
   const double* part2 = part + (size_t)cols * nb;
-  double a = 0.0;
-  for (int c = threadIdx.x; c < cols; c += blockDim.x) {
-    double te = 0.0, tn = 0.0;
-    for (int b = 0; b < nb; b++) {
-      te += part[(size_t)c * nb + b];
-      tn += part2[(size_t)c * nb + b];
-    }
-    a += w[c] * te;
-    const double re = x[(size_t)c * ldx], im = x[(size_t)c * ldx + 1];
-    const double bn = 2.0 * (tn - 0.5 * (re * re + im * im)), be = 2.0 * te;
-    double e = (0.5 * bn > 0.0) ? 0.5 * be / bn : 0.0;
-    if (e == 0.0) e = 1.0;
-    prec[c] = e;
+  double te = 0.0, tn = 0.0;
+  for (int b = 0; b < nb; b++) {
+    te += part[(size_t)c * nb + b];
+    tn += part2[(size_t)c * nb + b];
   }
-  const double s = red::block_sum(a, sh);
-  if (threadIdx.x == 0) out[0] = s;
+  wt[c] = w[c] * te;
+  const double re = x[(size_t)c * ldx], im = x[(size_t)c * ldx + 1];
+  const double bn = 2.0 * (tn - 0.5 * (re * re + im * im)), be = 2.0 * te;
+  double e = (0.5 * bn > 0.0) ? 0.5 * be / bn : 0.0;
+  if (e == 0.0) e = 1.0;
+  prec[c] = e;
 }
 
-// sum over columns of 2 (column's partials) - x(0, c) y(0, c), from the
-// partials of k_split2d_v4<..., 4>: 2 Re <x_c, y_c> on the half sphere with
-// G = 0 counted once, summed over the columns
-__global__ void k_dot_from_partials(const double* __restrict__ part, int nb, int cols,
-                                    const double* __restrict__ x, const double* __restrict__ y,
-                                    int ldx, double* __restrict__ out) {
-  __shared__ double sh[32];
-  double a = 0.0;
-  for (int c = threadIdx.x; c < cols; c += blockDim.x) {
-    double t = 0.0;
-    for (int b = 0; b < nb; b++) t += part[(size_t)c * nb + b];
-    a += 2.0 * t - x[(size_t)c * ldx] * y[(size_t)c * ldx];
-  }
-  const double s = red::block_sum(a, sh);
-  if (threadIdx.x == 0) out[0] = s;
+// Per column c of the partials of k_split2d_v4<..., 4>: 2 (column's sum) -
+// x(0, c) y(0, c) into wt[c], i.e. 2 Re <x_c, y_c> on the half sphere with
+// G = 0 counted once.  One thread per column.
+__global__ void k_dot_columns(const double* __restrict__ part, int nb, int cols,
+                              const double* __restrict__ x, const double* __restrict__ y, int ldx,
+                              double* __restrict__ wt) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cols) return;
+  double t = 0.0;
+  for (int b = 0; b < nb; b++) t += part[(size_t)c * nb + b];
+  wt[c] = 2.0 * t - x[(size_t)c * ldx] * y[(size_t)c * ldx];
 }
 
 void split_bf16_ekin(Context& ctx, const double* x, int rows, int cols, int ldx, void* hi,
                      void* lo, int ldp, const double* g2, const double* occ, double* out,
                      double* prec) {
   QBX_REQUIRE(v4_ok(x, ldx, ldp) && ((uintptr_t)hi | (uintptr_t)lo) % 8 == 0 && cols <= 65535 &&
-                  rows % 2 == 0 && (size_t)cols * (prec ? 128 : 64) <= ctx.colred_elems,
+                  rows % 2 == 0 && (size_t)cols * (prec ? 129 : 64) <= ctx.colred_elems,
               50, "split with the kinetic sums: unaligned operands or no room for the partials");
   const dim3 g = v4_grid(ldp, cols);
   if (prec) {
@@ -333,8 +325,11 @@ void split_bf16_ekin(Context& ctx, const double* x, int rows, int cols, int ldx,
         x, rows, ldx, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo, ldp, nullptr, nullptr, 4, ldp, g2,
         ctx.d_colred);
     QBX_LAUNCHED(ctx);
-    k_ekin_prec_from_partials<<<1, 1024, 0, ctx.stream>>>(ctx.d_colred, (int)g.x, occ, cols, x,
-                                                          ldx, out, prec);
+    double* wt = ctx.d_colred + (size_t)2 * cols * g.x;   // after the two partial arrays
+    k_ekin_prec_columns<<<(cols + 127) / 128, 128, 0, ctx.stream>>>(ctx.d_colred, (int)g.x, occ,
+                                                                    cols, x, ldx, wt, prec);
+    QBX_LAUNCHED(ctx);
+    red::k_reduce_final<1><<<1, 256, 0, ctx.stream>>>(wt, cols, out);
   } else {
     k_split2d_v4<true, false, 2><<<g, 256, 0, ctx.stream>>>(
         x, rows, ldx, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo, ldp, nullptr, nullptr, 4, ldp, g2,
@@ -349,14 +344,18 @@ void split_bf16_dot(Context& ctx, const double* x, const double* y, int rows, in
                     void* hi, void* lo, int ldp, double* out) {
   QBX_REQUIRE(v4_ok(x, ldx, ldp) && ((uintptr_t)y % 16) == 0 &&
                   ((uintptr_t)hi | (uintptr_t)lo) % 8 == 0 && cols <= 65535 &&
-                  (size_t)cols * 64 <= ctx.colred_elems,
+                  (size_t)cols * 65 <= ctx.colred_elems,
               50, "split with the column products: unaligned operands or no room for the partials");
   const dim3 g = v4_grid(ldp, cols);
   k_split2d_v4<true, false, 4><<<g, 256, 0, ctx.stream>>>(
       x, rows, ldx, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo, ldp, nullptr, nullptr, 4, ldp, nullptr,
       ctx.d_colred, y);
   QBX_LAUNCHED(ctx);
-  k_dot_from_partials<<<1, 1024, 0, ctx.stream>>>(ctx.d_colred, (int)g.x, cols, x, y, ldx, out);
+  double* wt = ctx.d_colred + (size_t)cols * g.x;   // after the partials
+  k_dot_columns<<<(cols + 127) / 128, 128, 0, ctx.stream>>>(ctx.d_colred, (int)g.x, cols, x, y,
+                                                            ldx, wt);
+  QBX_LAUNCHED(ctx);
+  red::k_reduce_final<1><<<1, 256, 0, ctx.stream>>>(wt, cols, out);
   QBX_LAUNCHED(ctx);
 }
 

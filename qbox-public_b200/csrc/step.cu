@@ -785,7 +785,7 @@ void alloc_mixed(Context& ctx) {
   const size_t small = std::max(np * n, n * n);
   ctx.acc32_elems = std::max(wf, std::max(np * n, std::max(K * np, n * n)));
   QBX_CUDA(cudaMalloc(&ctx.d_acc32, ctx.acc32_elems * sizeof(float)));
-  ctx.colred_elems = 128 * n;   // up to two partial arrays of 64 per column
+  ctx.colred_elems = 129 * n;   // up to two partial arrays of 64 per column, then one total
   ctx.d_colred = dalloc<double>(ctx.colred_elems);
   for (int s = 0; s < 2; s++) {
     QBX_CUDA(cudaMalloc(&ctx.cs_hi[s], wf * 2));
