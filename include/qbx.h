@@ -310,6 +310,15 @@ int qbx_set_gemm_backend(qbx_context* ctx, int backend);
  * library's tcgen05 kernel, 2 = TF32 splits through the tcgen05 kernel, 3 / 4
  * = BF16 / TF32 splits with A read as an MN-major operand (the form of the
  * tall updates; needs the default 256 x 256 CTA-pair kernel). */
+/* No counterpart in the reference (it applies its Cholesky factors with
+ * ScaLAPACK triangular solves, src/SlaterDet.cpp:1272-1314).  li = l^-1 for a
+ * lower-triangular n x n HOST matrix l (column-major; its upper triangle is
+ * not read), through the routine that ortho_align and the polar iteration's
+ * Cholesky step of the mixed path use: blocked (32 x 32 diagonal inverses,
+ * then FP64 GEMMs doubling the block) for n = 32 x a power of two, *blocked
+ * = 1; otherwise one triangular solve of I, *blocked = 0 (blocked may be
+ * NULL).  For checking that routine on its own. */
+int qbx_lower_inverse(qbx_context* ctx, int n, const double* l, double* li, int* blocked);
 int qbx_split_gemm_tn(qbx_context* ctx, int m, int n, int k, const double* a,
                       const double* b, double* d, int backend);
 

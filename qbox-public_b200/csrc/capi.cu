@@ -1092,6 +1092,25 @@ int qbx_polar(qbx_context* h, double* x, double tol, int maxiter, int graph, int
   });
 }
 
+int qbx_lower_inverse(qbx_context* h, int n, const double* l, double* li, int* blocked) {
+  return guarded(h, [&](Context& c) {
+    QBX_REQUIRE(n > 0 && l && li, 1, "bad triangular-inverse arguments");
+    const size_t nn = (size_t)n * n;
+    double *dl = dalloc<double>(nn), *dli = dalloc<double>(nn), *dw = dalloc<double>(nn / 4 + 1);
+    try {
+      QBX_CUDA(cudaMemcpyAsync(dl, l, nn * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+      lower_inverse(c, dl, n, dli, dw);
+      QBX_CUDA(cudaMemcpyAsync(li, dli, nn * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+      QBX_CUDA(cudaStreamSynchronize(c.stream));
+    } catch (...) {
+      dfree(dl); dfree(dli); dfree(dw);
+      throw;
+    }
+    dfree(dl); dfree(dli); dfree(dw);
+    if (blocked) *blocked = lower_inverse_blocked(n) ? 1 : 0;
+  });
+}
+
 int qbx_set_step_graph(qbx_context* h, int on) {
   return guarded(h, [&](Context& c) {
     QBX_REQUIRE(!on || !c.shard_comm, 1, "captured steps and band sharding are exclusive");

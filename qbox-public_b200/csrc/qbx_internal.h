@@ -708,6 +708,10 @@ void psda_update(Context& ctx, unsigned fuse = 0);
 bool energy_forms_prec(const Context& ctx);
 void jd_update(Context& ctx);
 void polar_factor(Context& ctx, double* x, double tol, int maxiter);
+// Li = L^-1 of a lower-triangular n x n L (ld n), blocked for n = 32 x a power
+// of two (work: n * n / 4 doubles), else a triangular solve of I
+bool lower_inverse_blocked(int n);
+void lower_inverse(Context& ctx, const double* L, int n, double* Li, double* work);
 int polar_entry(Context& ctx, double* x, double tol, int maxiter, bool graph);
 // one electronic step (captured graph or eager), energies/fion as qbx_scf_step
 void scf_step_any(Context& c, bool want_f, bool want_s, double* energies, double* fion);

@@ -136,10 +136,70 @@ static void polar_higham(Context& ctx, double* x, double* t, double* qt) {
   launch_avg_transpose(ctx, x, t, n);
 }
 
+// ------------------------------------------------ inverse of a lower triangle
+// The inverses of the diagonal 32 x 32 blocks of a lower-triangular L (ld n)
+// into the same blocks of Li: one warp per block, thread j forms column j by
+// forward substitution, x_i = (delta_ij - sum_{k<i} L_ik x_k) / L_ii with
+// x_k = 0 above the diagonal, in FP64.  Only the lower triangle of L is read.
+__global__ void __launch_bounds__(32) k_tri_inv_diag32(const double* __restrict__ L, int n,
+                                                       double* __restrict__ Li) {
+  __shared__ double sl[32][33];
+  const int k0 = 32 * blockIdx.x, j = threadIdx.x;
+  for (int c = 0; c < 32; c++) sl[j][c] = L[(size_t)(k0 + c) * n + k0 + j];
+  __syncwarp();
+  double x[32];
+#pragma unroll
+  for (int i = 0; i < 32; i++) {
+    double s = (i == j) ? 1.0 : 0.0;
+#pragma unroll
+    for (int k = 0; k < i; k++) s -= sl[i][k] * x[k];
+    x[i] = (i < j) ? 0.0 : s / sl[i][i];
+  }
+  __syncwarp();
+#pragma unroll
+  for (int i = 0; i < 32; i++) sl[i][j] = x[i];
+  __syncwarp();
+  for (int c = 0; c < 32; c++) Li[(size_t)(k0 + c) * n + k0 + j] = sl[j][c];
+}
+
+// Li = L^-1 for a lower-triangular n x n L (column-major, ld n; its upper
+// triangle is not read), for n = 32 x a power of two: the diagonal 32 x 32
+// blocks inverted directly, then, doubling the block size b, each pair of
+// neighbouring inverted blocks A^-1 (upper left) and C^-1 (lower right) with
+// the block B of L below A gets the off-diagonal block -C^-1 B A^-1 of the
+// inverse: two strided-batched FP64 GEMMs per level, all pairs of a level in
+// one call.  work holds n * n / 4 doubles.  Other n (or none of the blocked
+// form): one triangular solve of I, as cuBLAS's trsm.
+bool lower_inverse_blocked(int n) { return n >= 32 && n % 32 == 0 && ((n / 32) & (n / 32 - 1)) == 0; }
+
+void lower_inverse(Context& ctx, const double* L, int n, double* Li, double* work) {
+  const double one = 1.0, zero = 0.0, mone = -1.0;
+  if (!lower_inverse_blocked(n)) {
+    launch_identity_axpy(ctx, Li, Li, n, 0.0);
+    QBX_BLAS(cublasDtrsm(ctx.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
+                         CUBLAS_DIAG_NON_UNIT, n, n, &one, L, n, Li, n));
+    return;
+  }
+  QBX_CUDA(cudaMemsetAsync(Li, 0, sizeof(double) * n * n, ctx.stream));
+  k_tri_inv_diag32<<<n / 32, 32, 0, ctx.stream>>>(L, n, Li);
+  QBX_LAUNCHED(ctx);
+  for (int b = 32; b < n; b *= 2) {
+    const int pairs = n / (2 * b);
+    const long long st = 2LL * b * (n + 1);   // one pair's diagonal block to the next
+    // work_p = B_p A_p^-1
+    QBX_BLAS(cublasDgemmStridedBatched(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, b, b, b, &one, L + b,
+                                       n, st, Li, n, st, &zero, work, b, (long long)b * b, pairs));
+    // the block of Li below A_p^-1: -C_p^-1 work_p
+    QBX_BLAS(cublasDgemmStridedBatched(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, b, b, b, &mone,
+                                       Li + b + (size_t)b * n, n, st, work, b, (long long)b * b,
+                                       &zero, Li + b, n, st, pairs));
+  }
+}
+
 // The same Higham step for the mixed path, with x^-T = x (x^T x)^-1 formed
 // from the Cholesky factor of x^T x = I - q (q of this iteration, full):
 // S = L L^T, W = L^-1, S^-1 = W^T W, x <- x (I + S^-1) / 2.  One Cholesky
-// factor and one triangular solve instead of a pivoted LU and two solves
+// factor and one triangular inverse instead of a pivoted LU and two solves
 // (cuSOLVER's pivoted getrf took 2.1 ms at n = 1 024, the whole step 0.8 ms).
 // x^T x squares x's condition number; the Bjorck-Bowie steps that follow
 // converge to the same polar factor in FP64.
@@ -150,9 +210,7 @@ static void polar_higham_chol(Context& ctx, double* x, const double* q, double* 
   launch_identity_axpy(ctx, qt, q, n, -1.0);    // S = I - q = x^T x
   QBX_SOLVER(cusolverDnDpotrf(ctx.solver, CUBLAS_FILL_MODE_LOWER, n, qt, n, ctx.d_solver_work,
                               ctx.solver_lwork, ctx.d_status + ST_INFO_POLAR));
-  launch_identity_axpy(ctx, t, t, n, 0.0);      // t = I
-  QBX_BLAS(cublasDtrsm(ctx.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
-                       CUBLAS_DIAG_NON_UNIT, n, n, &one, qt, n, t, n));   // t = L^-1
+  lower_inverse(ctx, qt, n, t, xp);              // t = L^-1 (xp is free until the syrk)
   QBX_BLAS(cublasDsyrk(ctx.blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, n, n, &one, t, n, &zero,
                        xp, n));                  // S^-1 = W^T W (lower)
   launch_symmetrize_lower(ctx, xp, n);
@@ -400,9 +458,7 @@ void ortho_align(Context& ctx, bool c_split_done) {
     // the two solves with L and L^T (each solve as slow as the inverse)
     double* Li = ctx.d_nn5;
     double* T = L;   // L is not read after L^-1 is formed
-    launch_identity_axpy(ctx, Li, Li, n, 0.0);
-    QBX_BLAS(cublasDtrsm(ctx.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
-                         CUBLAS_DIAG_NON_UNIT, n, n, &one, L, n, Li, n));
+    lower_inverse(ctx, L, n, Li, ctx.d_nn3);   // d_nn3 is free until the rotation
     QBX_BLAS(cublasDgemm(ctx.blas, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &one, Li, n, X, n, &zero, T,
                          n));
     polar(ctx, T, 1.e-6, 20);

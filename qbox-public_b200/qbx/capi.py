@@ -47,6 +47,7 @@ SYMBOLS = (
     "qbx_ft_backward2", "qbx_ft_forward", "qbx_ft_forward2", "qbx_compute_density",
     "qbx_rs_mul_add", "qbx_nonlocal_energy", "qbx_ortho_align", "qbx_dot",
     "qbx_nccl_unique_id", "qbx_set_band_shard", "qbx_shard_pairs", "qbx_diag",
+    "qbx_lower_inverse",
 )
 
 NCCL_ID_BYTES = 128
@@ -112,6 +113,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "qbx_stream": (_P, [_P]),
         "qbx_set_gemm_backend": (_I, [_P, _I]),
         "qbx_split_gemm_tn": (_I, [_P, _I, _I, _I, _DP, _DP, _DP, _I]),
+        "qbx_lower_inverse": (_I, [_P, _I, _DP, _DP, _IP]),
         "qbx_density_static": (_I, [_P, ctypes.c_void_p, _I, _DP, ctypes.c_void_p]),
         "qbx_stress": (_I, [_P, _DP, _DP]),
         "qbx_autotune": (_I, [_P, ctypes.c_char_p, _I]),
@@ -414,6 +416,16 @@ class Context:
         self._ok(self.lib.qbx_split_gemm_tn(self.h, m, n, k, _dp(at), _dp(bt), _dp(out),
                                             backend), "split_gemm_tn")
         return out.T
+
+    def lower_inverse(self, l: np.ndarray):
+        """qbx_lower_inverse: (l^-1, blocked) for a lower-triangular n x n l."""
+        n = l.shape[0]
+        lt = np.ascontiguousarray(np.asarray(l, float).T)   # column-major
+        out = np.empty((n, n))
+        blocked = ctypes.c_int(0)
+        self._ok(self.lib.qbx_lower_inverse(self.h, n, _dp(lt), _dp(out), ctypes.byref(blocked)),
+                 "lower_inverse")
+        return out.T, bool(blocked.value)
 
     def set_wf_dyn(self, name: str):
         """qbx_set_wf_dyn: "PSDA" or "JD" for the update of scf_step."""
