@@ -493,7 +493,7 @@ void launch_psda_elementwise(Context& ctx, bool split_c) {
   const int ngw = ctx.wb.ng;
   if (split_c) {
     const int ldp = ctx.ldp, nst = ctx.nst;
-    const int nb = std::max(1, std::min((ldp + 1023) / 1024, 64));   // as the split kernel's grid
+    const int nb = split_blocks_per_column(ldp);   // the partials overlap_diag_from_split adds
     QBX_REQUIRE(ldp % 4 == 0 && ldp >= 2 * ngw && nst <= 65535 &&
                     (size_t)nb * nst <= ctx.colred_elems && ctx.cs_hi[1] && ctx.ct_hi,
                 50, "PSDA step with the splits of C: no split buffers or partials");

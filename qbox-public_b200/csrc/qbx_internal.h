@@ -781,6 +781,9 @@ void split_bf16_ekin(Context& ctx, const double* x, int rows, int cols, int ldx,
 // its columns of 2 Re <x_n, y_n> - x_n(0) y_n(0) (y of x's layout) into *out
 void split_bf16_dot(Context& ctx, const double* x, const double* y, int rows, int cols, int ldx,
                     void* hi, void* lo, int ldp, double* out);
+// CTAs per column of the split kernels over span rows (at most 64): the
+// number of column partials that the finishing kernels add
+int split_blocks_per_column(int span);
 // diag(S) = 2 C^T C - c0 c0^T on the diagonal, exact in FP64, from the
 // column sums of the last split_bf16_tf32 of c
 void overlap_diag_from_split(Context& ctx, const double* c, int K, int n, int ldp, double* S);

@@ -201,10 +201,14 @@ static bool v4_ok(const double* x, int ldx, int ld_out) {
   return ((uintptr_t)x % 16) == 0 && ldx % 2 == 0 && ld_out % 4 == 0;
 }
 
+int split_blocks_per_column(int span) {
+  const int per = (span + 1023) / 1024;   // 256 threads x 4 rows
+  return std::max(1, std::min(per, 64));
+}
+
 // grid of the v4 kernel: columns in y, rows / 4 threads in x (capped)
 static dim3 v4_grid(int span, int cols) {
-  const int per = (span + 1023) / 1024;   // 256 threads x 4 rows
-  return dim3((unsigned)std::max(1, std::min(per, 64)), (unsigned)cols);
+  return dim3((unsigned)split_blocks_per_column(span), (unsigned)cols);
 }
 
 void split_bf16_2d(Context& ctx, const double* x, int rows, int cols, int ldx, void* hi, void* lo,
